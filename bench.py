@@ -1,0 +1,394 @@
+"""MD-Bench short-range timestep on B200: atom-steps/s, mixed FP32 vs FP64.
+
+One bench step = one rebuild period of the reference loop (reneigh_every = 20
+MD timesteps: 19 plain steps and one step with wrap, ghost map, binning and
+list build), thermo sampled every nstat = 100 steps as the reference does.
+
+Headline (``value``): LJ, fcc 64^3 cells = 1,048,576 atoms, reduced density
+0.8442, T 1.44, cutoff 2.5 + skin 0.3, full Verlet lists, mixed precision.
+The same run reports the FP64 path on the same workload and both EAM paths on
+Cu fcc 32^3 cells (131,072 atoms, a = 3.615 A, 1600 K, funcfl Cu_u3), with
+the mixed path's force error and 1000-step energy drift against FP64.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+With N > 1 (torchrun) every rank runs one independent replica (the path has
+no data-path collective on one node); value is the sum over ranks, timing the
+max over ranks.
+"""
+import argparse
+import json
+import os
+import shutil
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "md-bench_b200"))
+
+LJ_CELLS = 64
+EAM_CELLS = 32
+EAM_A = 3.615
+EAM_T = 1600.0
+EAM_FILE = os.path.join(ROOT, "tests", "golden", "data", "Cu_u3.eam")
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "MDBench-VL")
+METRIC = "atom-steps/s, LJ+EAM mixed-FP32 vs FP64 on 1 B200 at stated force error"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50, help="timed bench steps (20 MD steps each)")
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-variants", action="store_true", help="headline only")
+    ap.add_argument("--profile", choices=["lj_mixed", "lj_fp64", "eam_mixed", "eam_fp64",
+                                          "lj_mixed_half", "lj_fp64_half"],
+                    help="run one variant only (W+K bench steps + force timing), for ncu")
+    ap.add_argument("--cells", type=int, default=None, help="fcc cells per side (profiling)")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+class Clocks:
+    """nvidia-smi clock and throttle-reason sampling during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.p = None
+        if shutil.which("nvidia-smi"):
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "-i", str(device),
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        out, _ = self.p.communicate(timeout=10)
+        rows = [r.split(",") for r in out.strip().splitlines() if r.count(",") == 5]
+        if not rows:
+            return None
+        sm = [float(r[0]) for r in rows if r[0].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4)
+                          if r[2 + k].strip().lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(rows[0][1]) if rows[0][1].strip().isdigit() else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+def lj_workload(mdb, precision, device, cells=None, half=0):
+    c = cells or LJ_CELLS
+    hp = mdb.host_params(nx=c, ny=c, nz=c, half_neigh=half)
+    x, v, t = mdb.create_fcc(hp)
+    s = mdb.system_from_host(hp, len(t), precision=precision, device=device)
+    return s, (x, v, t)
+
+
+def eam_workload(mdb, precision, device, cells=None, half=0):
+    c = cells or EAM_CELLS
+    tab = mdb.read_funcfl(EAM_FILE)
+    hp = mdb.host_params(eam=tab, nx=c, ny=c, nz=c, rho=4.0 / EAM_A ** 3, temp=EAM_T)
+    x, v, t = mdb.create_fcc(hp)
+    # the reference reads this configuration from a dump (-i): cutneigh/2 bins
+    hp.from_file = 1
+    s = mdb.system_from_host(hp, len(t), eam=tab, precision=precision, device=device)
+    return s, (x, v, t)
+
+
+def time_run(torch, s, steps, warmup, rebuild_every, first=0):
+    """Device time of `steps` bench steps, events on the library's stream."""
+    stream = torch.cuda.ExternalStream(s.stream)
+    n = first
+    samples = []
+    for _ in range(warmup):
+        samples += s.run(rebuild_every, first_step=n)
+        n += rebuild_every
+    s.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    l0 = s.launches
+    e0.record(stream)
+    for _ in range(steps):
+        samples += s.run(rebuild_every, first_step=n)
+        n += rebuild_every
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / 1e3, s.launches - l0, samples, n
+
+
+def force_kernel_time(torch, s, reps=20):
+    """Average duration of one force launch (no energy), on the launching stream."""
+    stream = torch.cuda.ExternalStream(s.stream)
+    for _ in range(3):
+        s.compute_force()
+    s.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        s.compute_force()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / reps
+
+
+def algorithmic_bytes(kind, precision, natoms, mean_list):
+    """Bytes one force launch must move (per atom: list + count + own position +
+    one read of each neighbour position + force write; EAM: two list passes,
+    rho/fp arrays)."""
+    pos = 32 if precision == "fp64" else 16
+    if kind == "lj":
+        per = 4 * mean_list + 4 + pos + pos + 24
+    else:
+        per = 2 * (4 * mean_list + 4 + pos) + pos + 8 + 8 + 24
+    return per * natoms, per
+
+
+def rel_force_err(a, b):
+    rms = np.sqrt(np.mean(np.sum(b * b, axis=1)))
+    d = np.sqrt(np.sum((a - b) ** 2, axis=1))
+    return float(np.sqrt(np.mean(d * d)) / rms), float(d.max() / rms)
+
+
+def measure(torch, mdb, kind, precision, args, device, half=0):
+    make = lj_workload if kind == "lj" else eam_workload
+    s, (x, v, t) = make(mdb, precision, device, args.cells, half)
+    s.set_atoms(x, v, t)
+    s.setup()
+    th0 = s.thermo()
+    nat = len(t)
+    every = s.params.reneigh_every
+    secs, launches, samples, nsteps = time_run(torch, s, args.steps, args.warmup, every)
+    mean_list = float(s.numneigh().mean())
+    return dict(system=s, natoms=nat, secs=secs, launches=launches, samples=samples,
+                nsteps=nsteps, th0=th0, mean_list=mean_list,
+                value=nat * every * args.steps / secs, ms_per_step=1e3 * secs / args.steps,
+                init=(x, v, t))
+
+
+def e2e(torch, s, init, steps, every):
+    """Same metric through the public C ABI with host buffers: each step uploads
+    the atoms from pinned host memory, runs setup + one rebuild period, and
+    reads positions, velocities and forces back."""
+    x, v, t = init
+    n = len(t)
+    hx = torch.from_numpy(np.ascontiguousarray(x)).pin_memory().numpy()
+    hv = torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy()
+    ht = torch.from_numpy(np.ascontiguousarray(t)).pin_memory().numpy()
+    bi = hx.nbytes + hv.nbytes + ht.nbytes
+    bo = 3 * 3 * 8 * n + 4 * n
+    s.synchronize()
+    t0 = time.perf_counter()
+    for k in range(steps):
+        s.set_atoms(hx, hv, ht)
+        s.setup()
+        s.run(every, first_step=0)
+        s.atoms()
+    s.synchronize()
+    secs = time.perf_counter() - t0
+    return dict(value=n * every * steps / secs, unit="atom-steps/s", h2d_bytes_per_step=bi,
+                d2h_bytes_per_step=bo)
+
+
+def cpu_baseline(kind_sample_steps=20):
+    """The reference CPU build on this host (all cores), bounded sample."""
+    cores = os.cpu_count() or 1
+    if os.path.exists(REF_BIN):
+        env = dict(os.environ, OMP_NUM_THREADS=str(cores), OMP_SCHEDULE="static",
+                   OMP_PROC_BIND="close")
+        out = subprocess.run([REF_BIN, "-nx", str(LJ_CELLS), "-ny", str(LJ_CELLS), "-nz",
+                              str(LJ_CELLS), "-n", str(kind_sample_steps)], env=env,
+                             capture_output=True, text=True, timeout=900).stdout
+        for line in out.splitlines():
+            if "atom updates/us" in line:
+                val = float(line.split("|")[1].split()[0]) * 1e6
+                return dict(value=val, unit="atom-steps/s", cores=cores, kind="reference",
+                            sample=f"reference VL FP64 strict build, LJ {LJ_CELLS}^3 "
+                                   f"(1,048,576 atoms), {kind_sample_steps} steps incl. one "
+                                   "rebuild, OpenMP static")
+        raise RuntimeError("reference run printed no performance line")
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # checker only: timed as the CPU baseline
+    o = oracle.Oracle(nx=32, ny=32, nz=32)
+    o.lattice()
+    o.setup()
+    o.force()
+    t0 = time.perf_counter()
+    o.run(kind_sample_steps)
+    secs = time.perf_counter() - t0
+    return dict(value=32 ** 3 * 4 * kind_sample_steps / secs, unit="atom-steps/s", cores=1,
+                kind="port", sample=f"C restatement, LJ 32^3, {kind_sample_steps} steps")
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return
+    steps = 20 * max(args.steps // 5, 1)
+    cb = cpu_baseline(steps)
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"],
+            "unit": "atom-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"lj-fcc-{LJ_CELLS}^3-verletlist-full", "natoms": 1048576,
+                       "md_steps": steps},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return reference_arm(args, rank)
+    import torch
+    import mdb
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    if args.profile:
+        kind, prec = args.profile.split("_")[:2]
+        half = 1 if args.profile.endswith("_half") else 0
+        m = measure(torch, mdb, kind, prec, args, local, half)
+        kt = force_kernel_time(torch, m["system"], reps=3)
+        print(json.dumps({"profile": args.profile, "natoms": m["natoms"],
+                          "value": m["value"], "ms_per_step": m["ms_per_step"],
+                          "force_ms": kt * 1e3, "mean_list": m["mean_list"],
+                          "launches": m["launches"]}), flush=True)
+        return
+
+    # headline: LJ 1M atoms, mixed precision
+    barrier()
+    clk = Clocks(local)
+    head = measure(torch, mdb, "lj", "mixed", args, local)
+    clocks = clk.stop()
+    secs = head["secs"]
+    if dist:
+        tt = torch.tensor([secs], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        secs = float(tt.item())
+    value = head["natoms"] * 20 * args.steps * world / secs
+
+    s = head["system"]
+    kt = force_kernel_time(torch, s)
+    alg, per_atom = algorithmic_bytes("lj", "mixed", head["natoms"], head["mean_list"])
+    hbm, src = peaks()
+    achieved = alg / kt / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tj = json.load(f)
+        if "lj_mixed_bytes_per_atom" in tj:
+            traffic = tj["lj_mixed_bytes_per_atom"] * head["natoms"]
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+            "frac": round(achieved / hbm, 4), "traffic": traffic,
+            "kernel": "k_lj_mixed (full list, uniform types)",
+            "kernel_ms": round(kt * 1e3, 4), "bytes_per_atom": round(per_atom, 1),
+            "peak_source": src}
+
+    extra = {}
+    if not args.no_variants and rank == 0:
+        fp = measure(torch, mdb, "lj", "fp64", args, local)
+        # mixed force error against FP64 on the same (melted) state
+        x, v, f64, t = fp["system"].atoms()
+        fp["system"].set_atoms(x, v, t)
+        fp["system"].setup()
+        _, _, f64, _ = fp["system"].atoms()
+        s.set_atoms(x, v, t)
+        s.setup()
+        rms, mx = rel_force_err(s.atoms()[2], f64)
+
+        def drift(m):
+            e = [m["th0"]["E"]] + [q["E"] for q in m["samples"]]
+            return float((e[-1] - e[0]) / abs(e[0]))
+
+        em = measure(torch, mdb, "eam", "mixed", args, local)
+        ef = measure(torch, mdb, "eam", "fp64", args, local)
+        xe, ve, fe, te = ef["system"].atoms()
+        ef["system"].set_atoms(xe, ve, te)
+        ef["system"].setup()
+        em["system"].set_atoms(xe, ve, te)
+        em["system"].setup()
+        erms, emx = rel_force_err(em["system"].atoms()[2], ef["system"].atoms()[2])
+        extra = {
+            "variants": {
+                "lj_mixed": {"value": head["value"], "ms_per_step": head["ms_per_step"],
+                             "force_rms_rel_err": rms, "force_max_rel_err": mx,
+                             "energy_drift": drift(head), "md_steps": head["nsteps"]},
+                "lj_fp64": {"value": fp["value"], "ms_per_step": fp["ms_per_step"],
+                            "energy_drift": drift(fp), "md_steps": fp["nsteps"]},
+                "eam_mixed": {"value": em["value"], "ms_per_step": em["ms_per_step"],
+                              "natoms": em["natoms"], "force_rms_rel_err": erms,
+                              "force_max_rel_err": emx, "energy_drift": drift(em)},
+                "eam_fp64": {"value": ef["value"], "ms_per_step": ef["ms_per_step"],
+                             "natoms": ef["natoms"], "energy_drift": drift(ef)},
+            },
+            "mixed_over_fp64": {"lj": head["value"] / fp["value"],
+                                "eam": em["value"] / ef["value"]},
+        }
+
+    e2 = e2e(torch, s, head["init"], max(args.steps // 5, 3), 20)
+    if dist:
+        tt = torch.tensor([e2["value"]], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.SUM)
+        e2["value"] = float(tt.item())
+    cb = cpu_baseline() if (rank == 0 and world == 1) else None
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32-mixed",
+                "data": "synthetic",
+                "config": {"workload": f"lj-fcc-{LJ_CELLS}^3-verletlist-full-mixed",
+                           "natoms_per_gpu": head["natoms"], "md_steps_per_bench_step": 20,
+                           "rebuild_every": 20, "thermo_every": 100, "density": 0.8442,
+                           "cutoff": 2.5, "skin": 0.3,
+                           "l2": "inputs larger than L2 (Verlet list %.0f MB)"
+                                 % (head["mean_list"] * 4 * head["natoms"] / 1e6),
+                           "parallelism": f"replicas{world}"},
+                "roofline": roof, "cpu_baseline": cb, "e2e": e2, "clocks": clocks,
+                "gpu_launches": head["launches"]}
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

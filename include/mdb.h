@@ -1,0 +1,172 @@
+/*
+ * mdb.h - C ABI of libmdb, the B200 (sm_100a) implementation of MD-Bench's
+ * short-range timestep: binning and Verlet lists, ghost/PBC setup and update,
+ * Lennard-Jones (full/half lists, single and multi-type) and three-pass EAM
+ * forces, the velocity-Verlet integrator and the thermo reductions.
+ *
+ * The reference binds its kernels through global function pointers
+ * (verletlist/force.h:16-17, neighbor.h:80-81, pbc.h:15-17, integrate.h:12-14)
+ * and a CUDA shim (common/device.h:26-50). Each hook below names the reference
+ * interface it replaces. All state lives in an opaque context that owns its
+ * device memory and one CUDA stream; every call is stream-ordered on that
+ * stream and returns an int status (0 = success) instead of exiting the
+ * process as the reference's cuda_assert does (common/deviceCuda.cu:14-20).
+ * A context is not thread-safe; distinct contexts are independent.
+ *
+ * Arrays crossing this boundary are plain host pointers in the reference's
+ * default layout: positions, velocities and forces as AoS triples
+ * (verletlist/atom.h:78-88, ATOM_POSITION_AOS), types as int.
+ */
+#ifndef MDB_H
+#define MDB_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define MDB_OK           0
+#define MDB_ERR_ARG      1 /* invalid argument or unsupported configuration */
+#define MDB_ERR_CUDA     2 /* a CUDA runtime call failed (context unusable) */
+#define MDB_ERR_OVERFLOW 3 /* a device buffer overflowed and could not grow */
+#define MDB_ERR_TIMEOUT  4 /* a bounded device wait expired */
+#define MDB_ERR_NOMEM    5 /* device or host allocation failed */
+#define MDB_ERR_STATE    6 /* call out of order (e.g. force before atoms) */
+
+/* ---- enumerations ---------------------------------------------------------- */
+#define MDB_FF_LJ  0 /* enum forcetype FF_LJ, verletlist/force.h:20 */
+#define MDB_FF_EAM 1 /* FF_EAM */
+
+#define MDB_PREC_FP64       0 /* FP64 throughout; reproduces the reference bit for bit */
+#define MDB_PREC_MIXED      1 /* FP32 pair forces on exact relative coordinates, FP32 sums */
+#define MDB_PREC_MIXED_COMP 2 /* as MIXED with compensated (two-float) force sums */
+
+#define MDB_BINS_LATTICE 0 /* nbin = max(1, 5/6 * n cells), verletlist/neighbor.c:67-69 */
+#define MDB_BINS_FILE    1 /* bin size = cutneigh/2, verletlist/neighbor.c:123-141 */
+
+/* ---- parameters (the subset of Parameter, common/parameter.h:76-119, that
+ *      the timestep reads) -------------------------------------------------- */
+typedef struct {
+    int force_field;   /* MDB_FF_LJ or MDB_FF_EAM */
+    int half_neigh;    /* 0 full list, 1 half list (LJ only) */
+    int precision;     /* MDB_PREC_* */
+    int bin_rule;      /* MDB_BINS_* */
+    int nx, ny, nz;    /* unit cells (MDB_BINS_LATTICE) */
+    int pbc_x, pbc_y, pbc_z;
+    int ntypes;        /* LJ types; per-type tables below (NULL: epsilon, sigma) */
+    int reneigh_every; /* rebuild period in steps (reference default 20) */
+    int nstat;         /* thermo sample period in steps (reference default 100) */
+    int maxneighs;     /* initial list capacity per atom; 0 -> 100 as the reference */
+    int natoms;        /* total atoms for the thermo degrees of freedom */
+    int device;        /* CUDA device ordinal */
+    double xprd, yprd, zprd; /* box lengths; the box starts at the origin */
+    double dt;
+    double dtforce;    /* as the reference computes it (0.5*dt, EAM: /mass/mvv2e) */
+    double mass;
+    double cutforce;
+    double cutneigh;   /* cutforce + skin */
+    double epsilon, sigma;
+    const double* epsilon_per_type; /* ntypes entries or NULL */
+    const double* sigma_per_type;   /* ntypes entries or NULL */
+} MdbParams;
+
+/* EAM tables: 7-coefficient cubic rows as common/eam_utils.c:224-284 lays them
+ * out (coefficients 0..2 derivative, 3..6 value); one element. */
+typedef struct {
+    int nrho, nr;
+    int nrho_tot, nr_tot;
+    double rdr, rdrho;
+    double cut, mass;
+    const double* frho_spline; /* nrho_tot */
+    const double* rhor_spline; /* nr_tot */
+    const double* z2r_spline;  /* nr_tot */
+} MdbEamTables;
+
+/* Thermo sample: T and P exactly as computeThermo prints them
+ * (common/thermo.c:60-100; P is the reference's kinetic-only pressure), plus
+ * totals of kinetic, potential and total energy (not in the reference). */
+typedef struct {
+    int step;
+    double temperature;
+    double pressure;
+    double ke;
+    double pe;
+    double etotal;
+} MdbThermo;
+
+typedef struct MdbCtx MdbCtx;
+
+/* ---- context ----------------------------------------------------------------
+ * Replaces initDevice (verletlist/device_spec.c:12-48) and the allocateGPU /
+ * memcpyToGPU family (common/device.h:26-50). */
+int mdb_create(const MdbParams* params, MdbCtx** out);
+int mdb_destroy(MdbCtx* ctx);
+const char* mdb_status_string(int status);
+const char* mdb_last_error(const MdbCtx* ctx);
+void* mdb_stream(MdbCtx* ctx); /* the context's cudaStream_t */
+int mdb_synchronize(MdbCtx* ctx);
+
+/* EAM tables (from mdb_eam_read_funcfl or any other source). */
+int mdb_set_eam(MdbCtx* ctx, const MdbEamTables* tables);
+
+/* Reads a funcfl file and builds the splines as initEam does
+ * (common/eam_utils.c:22-284). Arrays are malloc'd; free with
+ * mdb_eam_free. */
+int mdb_eam_read_funcfl(const char* path, MdbEamTables* out);
+void mdb_eam_free(MdbEamTables* t);
+
+/* Local atoms, AoS host arrays. Replaces copyDataToCUDADevice /
+ * copyDataFromCUDADevice (verletlist/forceCuda.cu:331-343). */
+int mdb_set_atoms(MdbCtx* ctx, int nlocal, const double* x, const double* v, const int* type);
+int mdb_get_atoms(MdbCtx* ctx, double* x, double* v, double* f, int* type);
+
+/* ---- hooks ------------------------------------------------------------------ */
+/* setupPbc (verletlist/pbc.c:103-232): ghost map in the reference order. */
+int mdb_setup_pbc(MdbCtx* ctx);
+/* updatePbc (verletlist/pbc.c:42-58, pbcCuda.cu:51-74): ghost positions. */
+int mdb_update_pbc(MdbCtx* ctx);
+/* updateAtomsPbc (verletlist/pbc.c:62-87): wrap local atoms into the box. */
+int mdb_update_atoms_pbc(MdbCtx* ctx);
+/* buildNeighbor (verletlist/neighbor.c:260-352, neighborCuda.cu:259-364):
+ * binning + list, growing the list capacity on overflow. */
+int mdb_build_neighbor(MdbCtx* ctx);
+/* computeForce (verletlist/force.h:16-17): LJ full/half or EAM per params. */
+int mdb_compute_force(MdbCtx* ctx);
+/* The same forces plus the potential energy that mdb_thermo then reports (the
+ * reference computes no energy; this variant is not part of its hook set). */
+int mdb_compute_force_energy(MdbCtx* ctx);
+/* initialIntegrate / finalIntegrate (verletlist/integrate.c:21-42). */
+int mdb_initial_integrate(MdbCtx* ctx);
+int mdb_final_integrate(MdbCtx* ctx);
+/* computeThermo (common/thermo.c:60-100) of the current state. */
+int mdb_thermo(MdbCtx* ctx, MdbThermo* out);
+
+/* setup tail of verletlist/main.c:96-111 for atoms already set:
+ * setupPbc, updatePbc, buildNeighbor, computeForce. */
+int mdb_setup(MdbCtx* ctx);
+
+/* The timestep loop of verletlist/main.c:371-419 for steps
+ * first_step .. first_step+nsteps-1, each step captured in CUDA graphs.
+ * A thermo sample (with potential energy) is taken after every step n with
+ * (n+1) % nstat == 0, as the reference prints them; up to max_samples (at most
+ * 64 per call) are returned in samples. */
+int mdb_run(MdbCtx* ctx, int first_step, int nsteps, MdbThermo* samples, int max_samples,
+    int* nsamples);
+
+/* ---- introspection (tests, tools) ----------------------------------------- */
+int mdb_get_counts(MdbCtx* ctx, int* nlocal, int* nghost, int* maxneighs);
+int mdb_get_positions_all(MdbCtx* ctx, double* x); /* (nlocal+nghost) x 3 */
+int mdb_get_ghosts(MdbCtx* ctx, int* border_map, int* pbc_xyz);
+/* Row-major copy: neighbors[i*ld + k], k < numneigh[i], in build order. */
+int mdb_get_neighbor_list(MdbCtx* ctx, int* numneigh, int* neighbors, int ld);
+/* ints: nbinx nbiny nbinz mbinx mbiny mbinz pad_x pad_y pad_z nstencil;
+ * dbls: binsizex binsizey binsizez bininvx bininvy bininvz cutneigh. */
+int mdb_get_bin_geometry(MdbCtx* ctx, int* ints, double* dbls, int* stencil, int max_stencil);
+int mdb_get_eam_fp(MdbCtx* ctx, double* fp); /* nlocal + nghost */
+/* Kernel launches issued by this context since creation (instrumentation). */
+long long mdb_launch_count(const MdbCtx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MDB_H */

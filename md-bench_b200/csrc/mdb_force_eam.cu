@@ -1,0 +1,359 @@
+// EAM forces over Verlet lists (computeForceEam, verletlist/force_eam.c:19-228)
+// as three kernels: (1) density rho_i and fp_i = F'(rho_i) per local atom,
+// (2) fp copied to the ghosts through the ghost map (the mid-step halo),
+// (3) pair forces from rho', phi' and fp_i + fp_j.
+//
+// Spline tables are re-laid out as rows of 8 coefficients (one 64-byte row
+// per grid point instead of 56 bytes) so a row is two aligned sectors.
+// FP64 path: -fmad=false, bit-identical to the reference's strict build.
+// Mixed path: pair terms and spline rows in FP32 on exact fixed-point pair
+// differences; the density (embedding) sum, F'(rho) and all energy sums FP64.
+#include "mdb_internal.cuh"
+
+namespace mdb {
+
+static constexpr int EAM_THREADS = 128;
+static constexpr int EUNROLL     = 4;
+
+template <bool ENERGY>
+__global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_fp64(int nlocal,
+    const double4* __restrict__ x, const int* __restrict__ numneigh,
+    const int* __restrict__ neighbors, int ld, double cutforcesq, EamDev e,
+    double* __restrict__ fp, double* __restrict__ epart)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double eng  = 0.0;
+    if (i < nlocal) {
+        const double4 xi = x[i];
+        const int n      = numneigh[i];
+        const int* nb    = neighbors + i;
+        double rhoi      = 0.0;
+        auto pair        = [&](const double4& xj) {
+            double delx = xi.x - xj.x;
+            double dely = xi.y - xj.y;
+            double delz = xi.z - xj.z;
+            double rsq  = delx * delx + dely * dely + delz * delz;
+            if (rsq < cutforcesq) {
+                double p = sqrt(rsq) * e.rdr + 1.0;
+                int m    = (int)(p);
+                m        = m < e.nr - 1 ? m : e.nr - 1;
+                p -= m;
+                p              = p < 1.0 ? p : 1.0;
+                const double* c = e.rhor + 8 * m;
+                rhoi += ((__ldg(c + 3) * p + __ldg(c + 4)) * p + __ldg(c + 5)) * p + __ldg(c + 6);
+            }
+        };
+        int k = 0;
+        for (; k + EUNROLL <= n; k += EUNROLL) {
+            int j[EUNROLL];
+            double4 xj[EUNROLL];
+#pragma unroll
+            for (int u = 0; u < EUNROLL; u++)
+                j[u] = __ldcs(nb + (size_t)(k + u) * ld);
+#pragma unroll
+            for (int u = 0; u < EUNROLL; u++)
+                xj[u] = ldg4(x + j[u]);
+#pragma unroll
+            for (int u = 0; u < EUNROLL; u++)
+                pair(xj[u]);
+        }
+        for (; k < n; k++)
+            pair(ldg4(x + __ldcs(nb + (size_t)k * ld)));
+        double p = 1.0 * rhoi * e.rdrho + 1.0;
+        int m    = (int)(p);
+        m        = m < e.nrho - 1 ? m : e.nrho - 1;
+        m        = m > 1 ? m : 1;
+        p -= m;
+        p               = p < 1.0 ? p : 1.0;
+        const double* c = e.frho + 8 * m;
+        fp[i]           = (__ldg(c + 0) * p + __ldg(c + 1)) * p + __ldg(c + 2);
+        if (ENERGY) eng = ((__ldg(c + 3) * p + __ldg(c + 4)) * p + __ldg(c + 5)) * p + __ldg(c + 6);
+    }
+    if (ENERGY) {
+        double s = block_sum(eng);
+        if (threadIdx.x == 0) epart[blockIdx.x] = s;
+    }
+}
+
+__global__ void k_eam_fp_ghost(int nlocal, double* __restrict__ fp,
+    const int* __restrict__ border_map, const int* __restrict__ counters)
+{
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= counters[CNT_NGHOST]) return;
+    fp[nlocal + g] = fp[border_map[g]];
+}
+
+template <bool ENERGY>
+__global__ void __launch_bounds__(EAM_THREADS) k_eam_force_fp64(int nlocal,
+    const double4* __restrict__ x, const int* __restrict__ numneigh,
+    const int* __restrict__ neighbors, int ld, double cutforcesq, EamDev e,
+    const double* __restrict__ fp, double* __restrict__ fx, double* __restrict__ fy,
+    double* __restrict__ fz, double* __restrict__ epart)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double eng  = 0.0;
+    if (i < nlocal) {
+        const double4 xi = x[i];
+        const int n      = numneigh[i];
+        const int* nb    = neighbors + i;
+        const double fpi = fp[i];
+        double fix = 0.0, fiy = 0.0, fiz = 0.0;
+        auto pair = [&](int j, const double4& xj) {
+            double delx = xi.x - xj.x;
+            double dely = xi.y - xj.y;
+            double delz = xi.z - xj.z;
+            double rsq  = delx * delx + dely * dely + delz * delz;
+            if (rsq < cutforcesq) {
+                double r = sqrt(rsq);
+                double p = r * e.rdr + 1.0;
+                int m    = (int)(p);
+                m        = m < e.nr - 1 ? m : e.nr - 1;
+                p -= m;
+                p                = p < 1.0 ? p : 1.0;
+                const double* cr = e.rhor + 8 * m;
+                const double* cz = e.z2r + 8 * m;
+                double rhoip     = (__ldg(cr + 0) * p + __ldg(cr + 1)) * p + __ldg(cr + 2);
+                double z2p       = (__ldg(cz + 0) * p + __ldg(cz + 1)) * p + __ldg(cz + 2);
+                double z2 = ((__ldg(cz + 3) * p + __ldg(cz + 4)) * p + __ldg(cz + 5)) * p +
+                            __ldg(cz + 6);
+                double recip = 1.0 / r;
+                double phi   = z2 * recip;
+                double phip  = z2p * recip - phi * recip;
+                double psip  = fpi * rhoip + __ldg(fp + j) * rhoip + phip;
+                double fpair = -psip * recip;
+                fix += delx * fpair;
+                fiy += dely * fpair;
+                fiz += delz * fpair;
+                if (ENERGY) eng += 0.5 * phi;
+            }
+        };
+        int k = 0;
+        for (; k + EUNROLL <= n; k += EUNROLL) {
+            int j[EUNROLL];
+            double4 xj[EUNROLL];
+#pragma unroll
+            for (int u = 0; u < EUNROLL; u++)
+                j[u] = __ldcs(nb + (size_t)(k + u) * ld);
+#pragma unroll
+            for (int u = 0; u < EUNROLL; u++)
+                xj[u] = ldg4(x + j[u]);
+#pragma unroll
+            for (int u = 0; u < EUNROLL; u++)
+                pair(j[u], xj[u]);
+        }
+        for (; k < n; k++) {
+            int j = __ldcs(nb + (size_t)k * ld);
+            pair(j, ldg4(x + j));
+        }
+        fx[i] = fix;
+        fy[i] = fiy;
+        fz[i] = fiz;
+    }
+    if (ENERGY) {
+        double s = block_sum(eng);
+        if (threadIdx.x == 0) epart[blockIdx.x] = s;
+    }
+}
+
+// ---- mixed ------------------------------------------------------------------
+__device__ __forceinline__ void qdelta(const int4& a, const int4& b, const QScale& qs,
+    float& dx, float& dy, float& dz)
+{
+    dx = (float)(int)((unsigned)a.x - (unsigned)b.x) * qs.ix;
+    dy = (float)(int)((unsigned)a.y - (unsigned)b.y) * qs.iy;
+    dz = (float)(int)((unsigned)a.z - (unsigned)b.z) * qs.iz;
+}
+
+template <bool ENERGY>
+__global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_mixed(int nlocal,
+    const int4* __restrict__ xq, QScale qs, const int* __restrict__ numneigh,
+    const int* __restrict__ neighbors, int ld, float cutforcesq, EamDev e,
+    double* __restrict__ fp, double* __restrict__ epart)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double eng  = 0.0;
+    if (i < nlocal) {
+        const int4 qi = xq[i];
+        const int n   = numneigh[i];
+        const int* nb = neighbors + i;
+        const float rdr = (float)e.rdr;
+        double rhoi   = 0.0; // FP64 embedding (density) sum
+        auto pair     = [&](const int4& qj) {
+            float dx, dy, dz;
+            qdelta(qi, qj, qs, dx, dy, dz);
+            float rsq = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
+            if (rsq < cutforcesq) {
+                float p = __fmaf_rn(sqrtf(rsq), rdr, 1.0f);
+                int m   = (int)p;
+                m       = m < e.nr - 1 ? m : e.nr - 1;
+                p -= (float)m;
+                p              = p < 1.0f ? p : 1.0f;
+                const float4 c = __ldg(reinterpret_cast<const float4*>(e.rhor32 + 8 * m) + 0);
+                const float4 d = __ldg(reinterpret_cast<const float4*>(e.rhor32 + 8 * m) + 1);
+                // coefficients 3..6 are c.w, d.x, d.y, d.z
+                rhoi += (double)__fmaf_rn(__fmaf_rn(__fmaf_rn(c.w, p, d.x), p, d.y), p, d.z);
+            }
+        };
+        int k = 0;
+        for (; k + EUNROLL <= n; k += EUNROLL) {
+            int j[EUNROLL];
+            int4 qj[EUNROLL];
+#pragma unroll
+            for (int u = 0; u < EUNROLL; u++)
+                j[u] = __ldcs(nb + (size_t)(k + u) * ld);
+#pragma unroll
+            for (int u = 0; u < EUNROLL; u++)
+                qj[u] = __ldg(xq + j[u]);
+#pragma unroll
+            for (int u = 0; u < EUNROLL; u++)
+                pair(qj[u]);
+        }
+        for (; k < n; k++)
+            pair(__ldg(xq + __ldcs(nb + (size_t)k * ld)));
+        double p = 1.0 * rhoi * e.rdrho + 1.0;
+        int m    = (int)(p);
+        m        = m < e.nrho - 1 ? m : e.nrho - 1;
+        m        = m > 1 ? m : 1;
+        p -= m;
+        p               = p < 1.0 ? p : 1.0;
+        const double* c = e.frho + 8 * m;
+        fp[i]           = (__ldg(c + 0) * p + __ldg(c + 1)) * p + __ldg(c + 2);
+        if (ENERGY) eng = ((__ldg(c + 3) * p + __ldg(c + 4)) * p + __ldg(c + 5)) * p + __ldg(c + 6);
+    }
+    if (ENERGY) {
+        double s = block_sum(eng);
+        if (threadIdx.x == 0) epart[blockIdx.x] = s;
+    }
+}
+
+template <bool ENERGY>
+__global__ void __launch_bounds__(EAM_THREADS) k_eam_force_mixed(int nlocal,
+    const int4* __restrict__ xq, QScale qs, const int* __restrict__ numneigh,
+    const int* __restrict__ neighbors, int ld, float cutforcesq, EamDev e,
+    const double* __restrict__ fp, double* __restrict__ fx, double* __restrict__ fy,
+    double* __restrict__ fz, double* __restrict__ epart)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double eng  = 0.0;
+    if (i < nlocal) {
+        const int4 qi   = xq[i];
+        const int n     = numneigh[i];
+        const int* nb   = neighbors + i;
+        const float fpi = (float)fp[i];
+        const float rdr = (float)e.rdr;
+        float fix = 0.f, fiy = 0.f, fiz = 0.f;
+        auto pair = [&](int j, const int4& qj) {
+            float dx, dy, dz;
+            qdelta(qi, qj, qs, dx, dy, dz);
+            float rsq = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
+            if (rsq < cutforcesq) {
+                float r = sqrtf(rsq);
+                float p = __fmaf_rn(r, rdr, 1.0f);
+                int m   = (int)p;
+                m       = m < e.nr - 1 ? m : e.nr - 1;
+                p -= (float)m;
+                p               = p < 1.0f ? p : 1.0f;
+                const float4 r0 = __ldg(reinterpret_cast<const float4*>(e.rhor32 + 8 * m));
+                const float4 z0 = __ldg(reinterpret_cast<const float4*>(e.z2r32 + 8 * m) + 0);
+                const float4 z1 = __ldg(reinterpret_cast<const float4*>(e.z2r32 + 8 * m) + 1);
+                float rhoip = __fmaf_rn(__fmaf_rn(r0.x, p, r0.y), p, r0.z);
+                float z2p   = __fmaf_rn(__fmaf_rn(z0.x, p, z0.y), p, z0.z);
+                float z2 = __fmaf_rn(__fmaf_rn(__fmaf_rn(z0.w, p, z1.x), p, z1.y), p, z1.z);
+                float recip = __frcp_rn(r);
+                float phi   = z2 * recip;
+                float phip  = __fmaf_rn(z2p, recip, -phi * recip);
+                float fpj   = (float)__ldg(fp + j);
+                float psip  = __fmaf_rn(fpi + fpj, rhoip, phip);
+                float fpair = -psip * recip;
+                fix         = __fmaf_rn(dx, fpair, fix);
+                fiy         = __fmaf_rn(dy, fpair, fiy);
+                fiz         = __fmaf_rn(dz, fpair, fiz);
+                if (ENERGY) eng += 0.5 * (double)phi;
+            }
+        };
+        int k = 0;
+        for (; k + EUNROLL <= n; k += EUNROLL) {
+            int j[EUNROLL];
+            int4 qj[EUNROLL];
+#pragma unroll
+            for (int u = 0; u < EUNROLL; u++)
+                j[u] = __ldcs(nb + (size_t)(k + u) * ld);
+#pragma unroll
+            for (int u = 0; u < EUNROLL; u++)
+                qj[u] = __ldg(xq + j[u]);
+#pragma unroll
+            for (int u = 0; u < EUNROLL; u++)
+                pair(j[u], qj[u]);
+        }
+        for (; k < n; k++) {
+            int j = __ldcs(nb + (size_t)k * ld);
+            pair(j, __ldg(xq + j));
+        }
+        fx[i] = (double)fix;
+        fy[i] = (double)fiy;
+        fz[i] = (double)fiz;
+    }
+    if (ENERGY) {
+        double s = block_sum(eng);
+        if (threadIdx.x == 0) epart[blockIdx.x] = s;
+    }
+}
+
+static void fp_ghost(cudaStream_t s, int nlocal, int ghost_cap, double* fp,
+    const int* border_map, const int* counters)
+{
+    if (ghost_cap <= 0) return;
+    k_eam_fp_ghost<<<mdb_blocks(ghost_cap, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(nlocal, fp,
+        border_map, counters);
+    g_launches++;
+}
+
+void launch_eam_fp64(cudaStream_t s, int energy, int nlocal, int ghost_cap, const double4* x,
+    const int* numneigh, const int* neighbors, int ld, double cutforcesq, EamDev eam,
+    const int* border_map, const int* counters, double* fp, double* fx, double* fy,
+    double* fz, double* epart_rho, double* epart_pair)
+{
+    if (nlocal <= 0) return;
+    int nb = mdb_blocks(nlocal, EAM_THREADS);
+    if (energy)
+        k_eam_rho_fp64<true><<<nb, EAM_THREADS, 0, s>>>(nlocal, x, numneigh, neighbors, ld,
+            cutforcesq, eam, fp, epart_rho);
+    else
+        k_eam_rho_fp64<false><<<nb, EAM_THREADS, 0, s>>>(nlocal, x, numneigh, neighbors, ld,
+            cutforcesq, eam, fp, epart_rho);
+    g_launches++;
+    fp_ghost(s, nlocal, ghost_cap, fp, border_map, counters);
+    if (energy)
+        k_eam_force_fp64<true><<<nb, EAM_THREADS, 0, s>>>(nlocal, x, numneigh, neighbors, ld,
+            cutforcesq, eam, fp, fx, fy, fz, epart_pair);
+    else
+        k_eam_force_fp64<false><<<nb, EAM_THREADS, 0, s>>>(nlocal, x, numneigh, neighbors, ld,
+            cutforcesq, eam, fp, fx, fy, fz, epart_pair);
+    g_launches++;
+}
+
+void launch_eam_mixed(cudaStream_t s, int energy, int nlocal, int ghost_cap, const int4* xq,
+    QScale qs, const int* numneigh, const int* neighbors, int ld, float cutforcesq,
+    EamDev eam, const int* border_map, const int* counters, double* fp, double* fx,
+    double* fy, double* fz, double* epart_rho, double* epart_pair)
+{
+    if (nlocal <= 0) return;
+    int nb = mdb_blocks(nlocal, EAM_THREADS);
+    if (energy)
+        k_eam_rho_mixed<true><<<nb, EAM_THREADS, 0, s>>>(nlocal, xq, qs, numneigh, neighbors,
+            ld, cutforcesq, eam, fp, epart_rho);
+    else
+        k_eam_rho_mixed<false><<<nb, EAM_THREADS, 0, s>>>(nlocal, xq, qs, numneigh, neighbors,
+            ld, cutforcesq, eam, fp, epart_rho);
+    g_launches++;
+    fp_ghost(s, nlocal, ghost_cap, fp, border_map, counters);
+    if (energy)
+        k_eam_force_mixed<true><<<nb, EAM_THREADS, 0, s>>>(nlocal, xq, qs, numneigh,
+            neighbors, ld, cutforcesq, eam, fp, fx, fy, fz, epart_pair);
+    else
+        k_eam_force_mixed<false><<<nb, EAM_THREADS, 0, s>>>(nlocal, xq, qs, numneigh,
+            neighbors, ld, cutforcesq, eam, fp, fx, fy, fz, epart_pair);
+    g_launches++;
+}
+
+} // namespace mdb

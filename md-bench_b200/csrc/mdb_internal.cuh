@@ -1,0 +1,167 @@
+// Internal declarations shared by the libmdb translation units.
+// Device data layout (HBM), per context:
+//   x       double4[nall_cap]  positions of locals then ghosts; .w holds the type
+//                              id as raw int bits (never used arithmetically)
+//   xq      int4[nall_cap]     mixed path: positions in 32-bit fixed point
+//                              (fraction of the box, wraps modulo the box), .w type
+//   vx,vy,vz / fx,fy,fz        SoA doubles over locals
+//   neighbors int32 [maxneighs][ld]  SoA (k-major) so a warp reads 128 B per k
+//   numneigh  int32 [nlocal]
+//   bins: CSR (bin_start[mbins+1], bin_atoms[nall]) with atoms of a bin in
+//         ascending index order, so lists come out in the reference order
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "mdb.h"
+
+#define MDB_MAX_TYPES   8
+#define MDB_MAX_STENCIL 1331 /* (2*5+1)^3 */
+
+// device counters (int slots)
+enum {
+    CNT_NGHOST       = 0, // ghosts in use (clamped to capacity)
+    CNT_NGHOST_TOTAL = 1, // ghosts requested by the last setupPbc
+    CNT_MAXNEED      = 2, // largest numneigh seen when a row overflowed
+    CNT_BADBIN       = 3, // atoms found outside the bin grid
+    CNT_SLOTS        = 8
+};
+
+struct BinGeom {
+    int nbinx, nbiny, nbinz;
+    int mbinx, mbiny, mbinz;
+    int pad_x, pad_y, pad_z;
+    int nstencil, mbins;
+    double binsizex, binsizey, binsizez;
+    double bininvx, bininvy, bininvz;
+    double xlo, ylo, zlo; // fabs(0 - pad*binsize) + 1e-9, verletlist/neighbor.c:361-366
+};
+
+struct LJTable {
+    int ntypes;
+    int uniform; // every type pair has the same epsilon and sigma6
+    double eps[MDB_MAX_TYPES * MDB_MAX_TYPES];
+    double sig6[MDB_MAX_TYPES * MDB_MAX_TYPES];
+};
+
+struct LJTableF {
+    int ntypes;
+    int uniform;
+    float eps[MDB_MAX_TYPES * MDB_MAX_TYPES];
+    float sig6[MDB_MAX_TYPES * MDB_MAX_TYPES];
+};
+
+struct QScale { // fixed-point position scale: q = x * s (mod 2^32), dx = dq * inv
+    double sx, sy, sz;
+    float ix, iy, iz;
+};
+
+struct EamDev {
+    int nrho, nr;
+    double rdr, rdrho;
+    const double* frho; // rows of 8 doubles (coefficients 0..6 + pad)
+    const double* rhor;
+    const double* z2r;
+    const float* frho32;
+    const float* rhor32;
+    const float* z2r32;
+};
+
+// ---- launch helpers (implemented in the .cu files) --------------------------
+namespace mdb {
+
+// scan: out[0..n] exclusive prefix sums of in[0..n-1]; out[n] = total.
+// scratch must hold scan_scratch_ints(n) ints.
+int scan_scratch_ints(int n);
+void scan_exclusive(const int* in, int* out, int n, int* scratch, cudaStream_t s);
+
+// integrator / pbc / thermo (mdb_vl.cu)
+void launch_initial_integrate(cudaStream_t s, int n, double dtf, double dt, double4* x,
+    double* vx, double* vy, double* vz, const double* fx, const double* fy, const double* fz,
+    int4* xq, QScale qs);
+void launch_final_integrate(cudaStream_t s, int n, double dtf, double* vx, double* vy,
+    double* vz, const double* fx, const double* fy, const double* fz);
+void launch_pack_atoms(cudaStream_t s, int n, const double* xa, const double* va,
+    const int* ta, double4* x, double* vx, double* vy, double* vz);
+void launch_unpack_atoms(cudaStream_t s, int n, const double4* x, const double* vx,
+    const double* vy, const double* vz, const double* fx, const double* fy, const double* fz,
+    double* xa, double* va, double* fa, int* ta);
+void launch_wrap(cudaStream_t s, int n, double4* x, double xprd, double yprd, double zprd);
+void launch_ghost_count(cudaStream_t s, int n, const double4* x, double cut, double xprd,
+    double yprd, double zprd, int px, int py, int pz, int* cnt);
+void launch_ghost_write(cudaStream_t s, int n, int ghost_cap, double4* x, int4* xq,
+    double cut, double xprd, double yprd, double zprd, int px, int py, int pz, const int* off,
+    int* border_map, int* pbc_code, int* counters);
+void launch_ghost_update(cudaStream_t s, int nlocal, int ghost_cap, double4* x,
+    const int* border_map, const int* pbc_code, double xprd, double yprd, double zprd,
+    const int* counters);
+void launch_ghost_update_q(cudaStream_t s, int nlocal, int ghost_cap, int4* xq,
+    const int* border_map, const int* counters);
+void launch_quantize(cudaStream_t s, int n, const double4* x, int4* xq, QScale qs);
+void launch_bin_count(cudaStream_t s, int nlocal, int nall_cap, const double4* x, BinGeom g,
+    int* atom_bin, int* atom_slot, int* bin_count, int* counters);
+void launch_bin_scatter(cudaStream_t s, int nlocal, int nall_cap, const int* atom_bin,
+    const int* atom_slot, const int* bin_start, int* bin_atoms, const int* counters);
+void launch_bin_sort(cudaStream_t s, int mbins, const int* bin_start, int* bin_atoms);
+void launch_build_list(cudaStream_t s, int nlocal, const double4* x, BinGeom g,
+    const int* stencil, const int* atom_bin, const int* bin_start, const int* bin_atoms,
+    double cutneighsq, int half, int maxneighs, int ld, int* neighbors, int* numneigh,
+    int* counters);
+int ke_partial_blocks(int n);
+void launch_ke_partial(cudaStream_t s, int n, const double* vx, const double* vy,
+    const double* vz, double mass, double* partials);
+void launch_reduce_partials(cudaStream_t s, int nparts, const double* partials, double* out);
+
+// block-wide sum; the result is valid in thread 0 (all threads must call)
+__device__ __forceinline__ double block_sum(double v)
+{
+    __shared__ double ws[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) ws[warp] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (warp == 0) {
+        t = lane < (int)(blockDim.x >> 5) ? ws[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1)
+            t += __shfl_down_sync(0xffffffffu, t, o);
+    }
+    __syncthreads();
+    return t;
+}
+
+__device__ __forceinline__ int type_of(const double4& p) { return (int)__double_as_longlong(p.w); }
+
+// read-only 32-byte position load as two 16-byte non-coherent loads of one sector
+__device__ __forceinline__ double4 ldg4(const double4* p)
+{
+    const double2* q = reinterpret_cast<const double2*>(p);
+    double2 a = __ldg(q), b = __ldg(q + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// forces (mdb_force_lj.cu, mdb_force_eam.cu)
+int force_partial_blocks(int n);
+void launch_lj_fp64(cudaStream_t s, int half, int energy, int nlocal, const double4* x,
+    const int* numneigh, const int* neighbors, int ld, double cutforcesq, const LJTable& tab,
+    double* fx, double* fy, double* fz, double* epart);
+void launch_lj_mixed(cudaStream_t s, int comp, int half, int energy, int nlocal,
+    const int4* xq, QScale qs, const int* numneigh, const int* neighbors, int ld,
+    float cutforcesq, const LJTableF& tab, double* fx, double* fy, double* fz, double* epart);
+void launch_eam_fp64(cudaStream_t s, int energy, int nlocal, int ghost_cap, const double4* x,
+    const int* numneigh, const int* neighbors, int ld, double cutforcesq, EamDev eam,
+    const int* border_map, const int* counters, double* fp, double* fx, double* fy,
+    double* fz, double* epart_rho, double* epart_pair);
+void launch_eam_mixed(cudaStream_t s, int energy, int nlocal, int ghost_cap, const int4* xq,
+    QScale qs, const int* numneigh, const int* neighbors, int ld, float cutforcesq,
+    EamDev eam, const int* border_map, const int* counters, double* fp, double* fx,
+    double* fy, double* fz, double* epart_rho, double* epart_pair);
+
+extern long long g_launches; // launches issued through these helpers (all contexts)
+
+} // namespace mdb
+
+#define MDB_NTHREADS 256
+static inline int mdb_blocks(long long n, int t) { return (int)((n + t - 1) / t); }

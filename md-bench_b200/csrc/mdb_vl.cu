@@ -1,0 +1,521 @@
+// Verlet-list scheme kernels other than the forces: integrator, periodic
+// images (ghost map and update), binning, list build and the thermo sums.
+// Compiled with -fmad=false: every FP64 expression rounds exactly as the
+// reference's strict build evaluates it, which keeps the FP64 path
+// bit-identical to the reference (see the parity tests).
+#include "mdb_internal.cuh"
+
+namespace mdb {
+
+long long g_launches = 0;
+
+__device__ __forceinline__ int4 quantize(const double4& p, const QScale& qs)
+{
+    int4 q;
+    q.x = (int)(unsigned int)(unsigned long long)__double2ll_rn(p.x * qs.sx);
+    q.y = (int)(unsigned int)(unsigned long long)__double2ll_rn(p.y * qs.sy);
+    q.z = (int)(unsigned int)(unsigned long long)__double2ll_rn(p.z * qs.sz);
+    q.w = type_of(p);
+    return q;
+}
+
+// ---- integrator: verletlist/integrate.c:21-42 -------------------------------
+__global__ void k_initial_integrate(int n, double dtf, double dt, double4* __restrict__ x,
+    double* __restrict__ vx, double* __restrict__ vy, double* __restrict__ vz,
+    const double* __restrict__ fx, const double* __restrict__ fy,
+    const double* __restrict__ fz, int4* __restrict__ xq, QScale qs)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double a = vx[i] + dtf * fx[i];
+    double b = vy[i] + dtf * fy[i];
+    double c = vz[i] + dtf * fz[i];
+    vx[i]     = a;
+    vy[i]     = b;
+    vz[i]     = c;
+    double4 p = x[i];
+    p.x       = p.x + dt * a;
+    p.y       = p.y + dt * b;
+    p.z       = p.z + dt * c;
+    x[i]      = p;
+    if (xq) xq[i] = quantize(p, qs);
+}
+
+__global__ void k_final_integrate(int n, double dtf, double* __restrict__ vx,
+    double* __restrict__ vy, double* __restrict__ vz, const double* __restrict__ fx,
+    const double* __restrict__ fy, const double* __restrict__ fz)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    vx[i] = vx[i] + dtf * fx[i];
+    vy[i] = vy[i] + dtf * fy[i];
+    vz[i] = vz[i] + dtf * fz[i];
+}
+
+void launch_initial_integrate(cudaStream_t s, int n, double dtf, double dt, double4* x,
+    double* vx, double* vy, double* vz, const double* fx, const double* fy, const double* fz,
+    int4* xq, QScale qs)
+{
+    if (n <= 0) return;
+    k_initial_integrate<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(n, dtf, dt, x,
+        vx, vy, vz, fx, fy, fz, xq, qs);
+    g_launches++;
+}
+
+void launch_final_integrate(cudaStream_t s, int n, double dtf, double* vx, double* vy,
+    double* vz, const double* fx, const double* fy, const double* fz)
+{
+    if (n <= 0) return;
+    k_final_integrate<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(n, dtf, vx, vy, vz,
+        fx, fy, fz);
+    g_launches++;
+}
+
+// ---- host-layout transfer: AoS triples <-> device layout ---------------------
+__global__ void k_pack_atoms(int n, const double* __restrict__ xa, const double* __restrict__ va,
+    const int* __restrict__ ta, double4* __restrict__ x, double* __restrict__ vx,
+    double* __restrict__ vy, double* __restrict__ vz)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    x[i]  = make_double4(xa[3 * i], xa[3 * i + 1], xa[3 * i + 2],
+         __longlong_as_double((long long)ta[i]));
+    vx[i] = va[3 * i];
+    vy[i] = va[3 * i + 1];
+    vz[i] = va[3 * i + 2];
+}
+
+__global__ void k_unpack_atoms(int n, const double4* __restrict__ x,
+    const double* __restrict__ vx, const double* __restrict__ vy,
+    const double* __restrict__ vz, const double* __restrict__ fx,
+    const double* __restrict__ fy, const double* __restrict__ fz, double* __restrict__ xa,
+    double* __restrict__ va, double* __restrict__ fa, int* __restrict__ ta)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double4 p     = x[i];
+    xa[3 * i]     = p.x;
+    xa[3 * i + 1] = p.y;
+    xa[3 * i + 2] = p.z;
+    ta[i]         = type_of(p);
+    va[3 * i]     = vx[i];
+    va[3 * i + 1] = vy[i];
+    va[3 * i + 2] = vz[i];
+    fa[3 * i]     = fx[i];
+    fa[3 * i + 1] = fy[i];
+    fa[3 * i + 2] = fz[i];
+}
+
+void launch_pack_atoms(cudaStream_t s, int n, const double* xa, const double* va,
+    const int* ta, double4* x, double* vx, double* vy, double* vz)
+{
+    if (n <= 0) return;
+    k_pack_atoms<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(n, xa, va, ta, x, vx, vy,
+        vz);
+    g_launches++;
+}
+
+void launch_unpack_atoms(cudaStream_t s, int n, const double4* x, const double* vx,
+    const double* vy, const double* vz, const double* fx, const double* fy, const double* fz,
+    double* xa, double* va, double* fa, int* ta)
+{
+    if (n <= 0) return;
+    k_unpack_atoms<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(n, x, vx, vy, vz, fx,
+        fy, fz, xa, va, fa, ta);
+    g_launches++;
+}
+
+// ---- wrap: updateAtomsPbcCPU, verletlist/pbc.c:62-87 ------------------------
+__global__ void k_wrap(int n, double4* __restrict__ x, double xprd, double yprd, double zprd)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double4 p = x[i];
+    if (p.x < 0.0) p.x += xprd;
+    else if (p.x >= xprd) p.x -= xprd;
+    if (p.y < 0.0) p.y += yprd;
+    else if (p.y >= yprd) p.y -= yprd;
+    if (p.z < 0.0) p.z += zprd;
+    else if (p.z >= zprd) p.z -= zprd;
+    x[i] = p;
+}
+
+void launch_wrap(cudaStream_t s, int n, double4* x, double xprd, double yprd, double zprd)
+{
+    if (n <= 0) return;
+    k_wrap<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(n, x, xprd, yprd, zprd);
+    g_launches++;
+}
+
+// ---- ghost map: setupPbc, verletlist/pbc.c:103-232 ---------------------------
+// The 26 image candidates of one atom, enumerated in the reference's order
+// (6 faces, 8 corners, 12 edges). For each candidate `visit(sx, sy, sz)` is
+// called when the atom lies within cutneigh of the faces it crosses.
+template <typename F>
+__device__ __forceinline__ void for_each_image(double x, double y, double z, double c,
+    double xp, double yp, double zp, int px, int py, int pz, F visit)
+{
+    const bool xl = x < c, xh = x >= (xp - c);
+    const bool yl = y < c, yh = y >= (yp - c);
+    const bool zl = z < c, zh = z >= (zp - c);
+    if (px) {
+        if (xl) visit(+1, 0, 0);
+        if (xh) visit(-1, 0, 0);
+    }
+    if (py) {
+        if (yl) visit(0, +1, 0);
+        if (yh) visit(0, -1, 0);
+    }
+    if (pz) {
+        if (zl) visit(0, 0, +1);
+        if (zh) visit(0, 0, -1);
+    }
+    if (px && py && pz) {
+        if (xl && yl && zl) visit(+1, +1, +1);
+        if (xl && yh && zl) visit(+1, -1, +1);
+        if (xl && yl && zh) visit(+1, +1, -1);
+        if (xl && yh && zh) visit(+1, -1, -1);
+        if (xh && yl && zl) visit(-1, +1, +1);
+        if (xh && yh && zl) visit(-1, -1, +1);
+        if (xh && yl && zh) visit(-1, +1, -1);
+        if (xh && yh && zh) visit(-1, -1, -1);
+    }
+    if (px && pz) {
+        if (xl && zl) visit(+1, 0, +1);
+        if (xl && zh) visit(+1, 0, -1);
+        if (xh && zl) visit(-1, 0, +1);
+        if (xh && zh) visit(-1, 0, -1);
+    }
+    if (py && pz) {
+        if (yl && zl) visit(0, +1, +1);
+        if (yl && zh) visit(0, +1, -1);
+        if (yh && zl) visit(0, -1, +1);
+        if (yh && zh) visit(0, -1, -1);
+    }
+    if (px && py) {
+        if (yl && xl) visit(+1, +1, 0);
+        if (yl && xh) visit(-1, +1, 0);
+        if (yh && xl) visit(+1, -1, 0);
+        if (yh && xh) visit(-1, -1, 0);
+    }
+}
+
+__global__ void k_ghost_count(int n, const double4* __restrict__ x, double c, double xp,
+    double yp, double zp, int px, int py, int pz, int* __restrict__ cnt)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double4 p = x[i];
+    int k     = 0;
+    for_each_image(p.x, p.y, p.z, c, xp, yp, zp, px, py, pz, [&](int, int, int) { k++; });
+    cnt[i] = k;
+}
+
+__device__ __forceinline__ int pack_shift(int sx, int sy, int sz)
+{
+    return (sx + 1) | ((sy + 1) << 2) | ((sz + 1) << 4);
+}
+
+__global__ void k_ghost_write(int n, int ghost_cap, double4* __restrict__ x,
+    int4* __restrict__ xq, double c, double xp, double yp, double zp, int px, int py, int pz,
+    const int* __restrict__ off, int* __restrict__ border_map, int* __restrict__ pbc_code)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double4 p = x[i];
+    int g     = off[i];
+    int4 q    = xq ? xq[i] : make_int4(0, 0, 0, 0);
+    for_each_image(p.x, p.y, p.z, c, xp, yp, zp, px, py, pz, [&](int sx, int sy, int sz) {
+        if (g < ghost_cap) {
+            border_map[g] = i;
+            pbc_code[g]   = pack_shift(sx, sy, sz);
+            double4 gp;
+            gp.x         = p.x + sx * xp;
+            gp.y         = p.y + sy * yp;
+            gp.z         = p.z + sz * zp;
+            gp.w         = p.w;
+            x[n + g]     = gp;
+            if (xq) xq[n + g] = q;
+        }
+        g++;
+    });
+}
+
+__global__ void k_ghost_finalize(int n, int ghost_cap, const int* __restrict__ off,
+    int* __restrict__ counters)
+{
+    int total                  = off[n];
+    counters[CNT_NGHOST_TOTAL] = total;
+    counters[CNT_NGHOST]       = total < ghost_cap ? total : ghost_cap;
+}
+
+void launch_ghost_count(cudaStream_t s, int n, const double4* x, double cut, double xprd,
+    double yprd, double zprd, int px, int py, int pz, int* cnt)
+{
+    if (n <= 0) return;
+    k_ghost_count<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(n, x, cut, xprd, yprd,
+        zprd, px, py, pz, cnt);
+    g_launches++;
+}
+
+void launch_ghost_write(cudaStream_t s, int n, int ghost_cap, double4* x, int4* xq,
+    double cut, double xprd, double yprd, double zprd, int px, int py, int pz, const int* off,
+    int* border_map, int* pbc_code, int* counters)
+{
+    k_ghost_finalize<<<1, 1, 0, s>>>(n, ghost_cap, off, counters);
+    g_launches++;
+    if (n <= 0) return;
+    k_ghost_write<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(n, ghost_cap, x, xq,
+        cut, xprd, yprd, zprd, px, py, pz, off, border_map, pbc_code);
+    g_launches++;
+}
+
+// ---- ghost update: updatePbcCPU, verletlist/pbc.c:42-58 ----------------------
+__global__ void k_ghost_update(int nlocal, int ghost_cap, double4* __restrict__ x,
+    const int* __restrict__ border_map, const int* __restrict__ pbc_code, double xp,
+    double yp, double zp, const int* __restrict__ counters)
+{
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= counters[CNT_NGHOST]) return;
+    int b     = border_map[g];
+    int code  = pbc_code[g];
+    int sx    = (code & 3) - 1, sy = ((code >> 2) & 3) - 1, sz = ((code >> 4) & 3) - 1;
+    double4 p = x[b];
+    double4 q;
+    q.x           = p.x + sx * xp;
+    q.y           = p.y + sy * yp;
+    q.z           = p.z + sz * zp;
+    q.w           = p.w;
+    x[nlocal + g] = q;
+}
+
+__global__ void k_ghost_update_q(int nlocal, int4* __restrict__ xq,
+    const int* __restrict__ border_map, const int* __restrict__ counters)
+{
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= counters[CNT_NGHOST]) return;
+    xq[nlocal + g] = xq[border_map[g]];
+}
+
+void launch_ghost_update(cudaStream_t s, int nlocal, int ghost_cap, double4* x,
+    const int* border_map, const int* pbc_code, double xprd, double yprd, double zprd,
+    const int* counters)
+{
+    if (ghost_cap <= 0) return;
+    k_ghost_update<<<mdb_blocks(ghost_cap, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(nlocal,
+        ghost_cap, x, border_map, pbc_code, xprd, yprd, zprd, counters);
+    g_launches++;
+}
+
+void launch_ghost_update_q(cudaStream_t s, int nlocal, int ghost_cap, int4* xq,
+    const int* border_map, const int* counters)
+{
+    if (ghost_cap <= 0) return;
+    k_ghost_update_q<<<mdb_blocks(ghost_cap, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(nlocal, xq,
+        border_map, counters);
+    g_launches++;
+}
+
+__global__ void k_quantize(int n, const double4* __restrict__ x, int4* __restrict__ xq,
+    QScale qs)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    xq[i] = quantize(x[i], qs);
+}
+
+void launch_quantize(cudaStream_t s, int n, const double4* x, int4* xq, QScale qs)
+{
+    if (n <= 0) return;
+    k_quantize<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(n, x, xq, qs);
+    g_launches++;
+}
+
+// ---- binning: coord2bin + binatoms, verletlist/neighbor.c:355-464 ------------
+__device__ __forceinline__ int coord2bin(const double4& p, const BinGeom& g)
+{
+    int ix = (int)((p.x + g.xlo) * g.bininvx);
+    int iy = (int)((p.y + g.ylo) * g.bininvy);
+    int iz = (int)((p.z + g.zlo) * g.bininvz);
+    if (ix < 0 || iy < 0 || iz < 0 || ix >= g.mbinx || iy >= g.mbiny || iz >= g.mbinz)
+        return -1;
+    return iz * g.mbiny * g.mbinx + iy * g.mbinx + ix;
+}
+
+__global__ void k_bin_count(int nlocal, int nall_cap, const double4* __restrict__ x,
+    BinGeom g, int* __restrict__ atom_bin, int* __restrict__ atom_slot,
+    int* __restrict__ bin_count, int* __restrict__ counters)
+{
+    int i    = blockIdx.x * blockDim.x + threadIdx.x;
+    int nall = nlocal + counters[CNT_NGHOST];
+    if (i >= nall) return;
+    int b = coord2bin(x[i], g);
+    if (b < 0) {
+        atomicAdd(&counters[CNT_BADBIN], 1);
+        atom_bin[i] = -1;
+        return;
+    }
+    atom_bin[i]  = b;
+    atom_slot[i] = atomicAdd(&bin_count[b], 1);
+}
+
+__global__ void k_bin_scatter(int nlocal, const int* __restrict__ atom_bin,
+    const int* __restrict__ atom_slot, const int* __restrict__ bin_start,
+    int* __restrict__ bin_atoms, const int* __restrict__ counters)
+{
+    int i    = blockIdx.x * blockDim.x + threadIdx.x;
+    int nall = nlocal + counters[CNT_NGHOST];
+    if (i >= nall) return;
+    int b = atom_bin[i];
+    if (b < 0) return;
+    bin_atoms[bin_start[b] + atom_slot[i]] = i;
+}
+
+// Atoms of a bin in ascending index order: the order binatoms produces when it
+// fills bins in one serial pass (verletlist/neighbor.c:443-454).
+__global__ void k_bin_sort(int mbins, const int* __restrict__ bin_start, int* __restrict__ bin_atoms)
+{
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= mbins) return;
+    int s = bin_start[b], e = bin_start[b + 1];
+    for (int k = s + 1; k < e; k++) {
+        int v = bin_atoms[k];
+        int m = k - 1;
+        while (m >= s && bin_atoms[m] > v) {
+            bin_atoms[m + 1] = bin_atoms[m];
+            m--;
+        }
+        bin_atoms[m + 1] = v;
+    }
+}
+
+void launch_bin_count(cudaStream_t s, int nlocal, int nall_cap, const double4* x, BinGeom g,
+    int* atom_bin, int* atom_slot, int* bin_count, int* counters)
+{
+    k_bin_count<<<mdb_blocks(nall_cap, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(nlocal, nall_cap,
+        x, g, atom_bin, atom_slot, bin_count, counters);
+    g_launches++;
+}
+
+void launch_bin_scatter(cudaStream_t s, int nlocal, int nall_cap, const int* atom_bin,
+    const int* atom_slot, const int* bin_start, int* bin_atoms, const int* counters)
+{
+    k_bin_scatter<<<mdb_blocks(nall_cap, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(nlocal, atom_bin,
+        atom_slot, bin_start, bin_atoms, counters);
+    g_launches++;
+}
+
+void launch_bin_sort(cudaStream_t s, int mbins, const int* bin_start, int* bin_atoms)
+{
+    k_bin_sort<<<mdb_blocks(mbins, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(mbins, bin_start,
+        bin_atoms);
+    g_launches++;
+}
+
+// ---- list build: buildNeighborCPU, verletlist/neighbor.c:260-352 -------------
+// One thread per local atom walks the stencil in the reference order and the
+// atoms of each bin in index order, so row i holds exactly the reference's
+// neighbours in the reference's order. Rows are stored k-major (SoA).
+__global__ void __launch_bounds__(128) k_build_list(int nlocal, const double4* __restrict__ x,
+    BinGeom g, const int* __restrict__ stencil, const int* __restrict__ atom_bin,
+    const int* __restrict__ bin_start, const int* __restrict__ bin_atoms, double cutneighsq,
+    int half, int maxneighs, int ld, int* __restrict__ neighbors, int* __restrict__ numneigh,
+    int* __restrict__ counters)
+{
+    __shared__ int st[MDB_MAX_STENCIL];
+    for (int k = threadIdx.x; k < g.nstencil; k += blockDim.x)
+        st[k] = stencil[k];
+    __syncthreads();
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nlocal) return;
+    const double4 xi = x[i];
+    const int ibin   = atom_bin[i];
+    int n            = 0;
+    if (ibin >= 0) {
+        for (int k = 0; k < g.nstencil; k++) {
+            int jbin = ibin + st[k];
+            if (jbin < 0 || jbin >= g.mbins) continue;
+            int beg = __ldg(&bin_start[jbin]);
+            int end = __ldg(&bin_start[jbin + 1]);
+            for (int m = beg; m < end; m++) {
+                int j = __ldg(&bin_atoms[m]);
+                if (j == i) continue;
+                if (half && j < i) continue;
+                double4 xj  = ldg4(&x[j]);
+                double delx = xi.x - xj.x;
+                double dely = xi.y - xj.y;
+                double delz = xi.z - xj.z;
+                double rsq  = delx * delx + dely * dely + delz * delz;
+                if (rsq <= cutneighsq) {
+                    if (n < maxneighs) neighbors[(size_t)n * ld + i] = j;
+                    n++;
+                }
+            }
+        }
+    }
+    // the stored count never exceeds the row capacity, so no consumer can read
+    // past the list; the true count of an overflowing row goes to the host,
+    // which grows the list and rebuilds before any force is computed
+    numneigh[i] = n < maxneighs ? n : maxneighs;
+    if (n > maxneighs) atomicMax(&counters[CNT_MAXNEED], n);
+}
+
+void launch_build_list(cudaStream_t s, int nlocal, const double4* x, BinGeom g,
+    const int* stencil, const int* atom_bin, const int* bin_start, const int* bin_atoms,
+    double cutneighsq, int half, int maxneighs, int ld, int* neighbors, int* numneigh,
+    int* counters)
+{
+    if (nlocal <= 0) return;
+    k_build_list<<<mdb_blocks(nlocal, 128), 128, 0, s>>>(nlocal, x, g, stencil, atom_bin,
+        bin_start, bin_atoms, cutneighsq, half, maxneighs, ld, neighbors, numneigh, counters);
+    g_launches++;
+}
+
+// ---- thermo: sum of v.v per block, then one fixed-order reduction ------------
+static constexpr int KE_THREADS = 256;
+static constexpr int KE_MAX_BLOCKS = 1184; // 8 x 148 SMs
+
+int ke_partial_blocks(int n)
+{
+    int b = mdb_blocks(n, KE_THREADS);
+    return b < KE_MAX_BLOCKS ? (b > 0 ? b : 1) : KE_MAX_BLOCKS;
+}
+
+__global__ void k_ke_partial(int n, const double* __restrict__ vx,
+    const double* __restrict__ vy, const double* __restrict__ vz, double mass,
+    double* __restrict__ part)
+{
+    // sum of (vx^2 + vy^2 + vz^2) * mass, common/thermo.c:74-77
+    double t = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double a = vx[i], b = vy[i], c = vz[i];
+        t += (a * a + b * b + c * c) * mass;
+    }
+    t = block_sum(t);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+__global__ void k_reduce_partials(int nparts, const double* __restrict__ part,
+    double* __restrict__ out)
+{
+    double t = 0.0;
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x)
+        t += part[i];
+    t = block_sum(t);
+    if (threadIdx.x == 0) *out = t;
+}
+
+void launch_ke_partial(cudaStream_t s, int n, const double* vx, const double* vy,
+    const double* vz, double mass, double* partials)
+{
+    k_ke_partial<<<ke_partial_blocks(n), KE_THREADS, 0, s>>>(n, vx, vy, vz, mass, partials);
+    g_launches++;
+}
+
+void launch_reduce_partials(cudaStream_t s, int nparts, const double* partials, double* out)
+{
+    k_reduce_partials<<<1, 1024, 0, s>>>(nparts, partials, out);
+    g_launches++;
+}
+
+} // namespace mdb

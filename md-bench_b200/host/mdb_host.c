@@ -1,0 +1,368 @@
+/*
+ * Host-side setup for libmdb (see include/mdb_host.h). Compiled with
+ * -ffp-contract=off so that the generated lattice and velocities are the
+ * reference's to the last bit.
+ */
+#include "mdb_host.h"
+
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define HMAX(a, b) ((a) > (b) ? (a) : (b))
+#define HMIN(a, b) ((a) < (b) ? (a) : (b))
+
+void mdbh_defaults(MdbHostParams* p)
+{
+    memset(p, 0, sizeof *p);
+    p->force_field   = MDB_FF_LJ;
+    p->precision     = MDB_PREC_FP64;
+    p->epsilon       = 1.0;
+    p->sigma         = 1.0;
+    p->rho           = 0.8442;
+    p->ntypes        = 4;
+    p->ntimes        = 200;
+    p->dt            = 0.005;
+    p->nx = p->ny = p->nz = 32;
+    p->pbc_x = p->pbc_y = p->pbc_z = 1;
+    p->cutforce      = 2.5;
+    p->skin          = 0.3;
+    p->temp          = 1.44;
+    p->nstat         = 100;
+    p->mass          = 1.0;
+    p->reneigh_every = 20;
+}
+
+static char* trim_comment(char* line)
+{
+    char* h = strchr(line, '#');
+    if (h) *h = '\0';
+    return line;
+}
+
+int mdbh_read_types(MdbHostParams* p, const char* path)
+{
+    FILE* fp = fopen(path, "r");
+    if (!fp) return MDB_ERR_ARG;
+    char line[4096];
+    int t = 0;
+    while (fgets(line, sizeof line, fp)) {
+        char* save = NULL;
+        char* e    = strtok_r(trim_comment(line), " \t\n\r", &save);
+        if (!e) continue;
+        char* s = strtok_r(NULL, " \t\n\r", &save);
+        if (!s || t >= MDBH_MAX_TYPES) {
+            fclose(fp);
+            return MDB_ERR_ARG;
+        }
+        p->epsilon_per_type[t] = atof(e);
+        p->sigma_per_type[t]   = atof(s);
+        t++;
+    }
+    fclose(fp);
+    if (t == 0) return MDB_ERR_ARG;
+    p->ntypes    = t;
+    p->has_types = 1;
+    return MDB_OK;
+}
+
+int mdbh_read_params(MdbHostParams* p, const char* path)
+{
+    FILE* fp = fopen(path, "r");
+    if (!fp) return MDB_ERR_ARG;
+    char line[4096];
+    char types_file[4096] = { 0 };
+    int explicit_lj       = 0;
+    while (fgets(line, sizeof line, fp)) {
+        char* save = NULL;
+        char* key  = strtok_r(trim_comment(line), " \t\n\r", &save);
+        char* val  = key ? strtok_r(NULL, " \t\n\r", &save) : NULL;
+        if (!key || !val) continue;
+#define RP(name, conv)                                                                  \
+    if (strcmp(key, #name) == 0) {                                                      \
+        p->name = conv(val);                                                            \
+        continue;                                                                       \
+    }
+        if (strcmp(key, "force_field") == 0) {
+            p->force_field = strncmp(val, "eam", 3) == 0 ? MDB_FF_EAM : MDB_FF_LJ;
+            continue;
+        }
+        if (strcmp(key, "types_file") == 0) {
+            snprintf(types_file, sizeof types_file, "%s", val);
+            continue;
+        }
+        if (!strcmp(key, "epsilon") || !strcmp(key, "sigma") || !strcmp(key, "ntypes"))
+            explicit_lj = 1;
+        RP(epsilon, atof)
+        RP(sigma, atof)
+        RP(rho, atof)
+        RP(dt, atof)
+        RP(cutforce, atof)
+        RP(skin, atof)
+        RP(temp, atof)
+        RP(mass, atof)
+        RP(ntypes, atoi)
+        RP(ntimes, atoi)
+        RP(nx, atoi)
+        RP(ny, atoi)
+        RP(nz, atoi)
+        RP(pbc_x, atoi)
+        RP(pbc_y, atoi)
+        RP(pbc_z, atoi)
+        RP(nstat, atoi)
+        RP(reneigh_every, atoi)
+        RP(half_neigh, atoi)
+#undef RP
+    }
+    fclose(fp);
+    /* common/parameter.c:262-273: a types file excludes epsilon/sigma/ntypes */
+    if (types_file[0]) {
+        if (explicit_lj) return MDB_ERR_ARG;
+        return mdbh_read_types(p, types_file);
+    }
+    return MDB_OK;
+}
+
+void mdbh_apply_eam(MdbHostParams* p, const MdbEamTables* t)
+{
+    p->force_field = MDB_FF_EAM;
+    p->mass        = t->mass;
+    p->cutforce    = t->cut;
+    p->temp        = 600.0;
+    p->dt          = 0.001;
+    p->rho         = 0.07041125;
+}
+
+void mdbh_finalize(MdbHostParams* p)
+{
+    p->lattice = pow((4.0 / p->rho), (1.0 / 3.0));
+    if (!p->from_file) {
+        p->xprd = p->nx * p->lattice;
+        p->yprd = p->ny * p->lattice;
+        p->zprd = p->nz * p->lattice;
+    }
+    if (p->force_field == MDB_FF_EAM) {
+        p->cutneigh = p->cutforce + 1.0;                /* common/eam_utils.c:31 */
+        p->dtforce  = 0.5 * p->dt / p->mass;            /* common/eam_utils.c:35 */
+        p->dtforce /= 1.036427e-04;                     /* common/thermo.c:56 */
+    } else {
+        p->cutneigh = p->cutforce + p->skin;            /* verletlist/main.c:305 */
+        p->dtforce  = 0.5 * p->dt;                      /* common/parameter.c:276 */
+    }
+}
+
+/* Park-Miller minimal standard generator (Schrage), common/util.c:24-33. */
+static double park_miller(int* seed)
+{
+    const int a = 16807, m = 2147483647, q = 127773, r = 2836;
+    int k       = (*seed) / q;
+    *seed       = a * (*seed - k * q) - r * k;
+    if (*seed < 0) *seed += m;
+    return (1.0 / m) * (*seed);
+}
+
+int mdbh_create_fcc(const MdbHostParams* p, double** xo, double** vo, int** to)
+{
+    const int nx = p->nx, ny = p->ny, nz = p->nz;
+    if (nx < 1 || ny < 1 || nz < 1 || p->ntypes < 1) return -MDB_ERR_ARG;
+    long long natoms = 4LL * nx * ny * nz;
+    if (natoms > 0x7fffffffLL) return -MDB_ERR_ARG;
+    double* x = malloc(sizeof(double) * 3 * natoms);
+    double* v = malloc(sizeof(double) * 3 * natoms);
+    int* type = malloc(sizeof(int) * natoms);
+    if (!x || !v || !type) {
+        free(x);
+        free(v);
+        free(type);
+        return -MDB_ERR_NOMEM;
+    }
+    const double xhi = p->xprd, yhi = p->yprd, zhi = p->zprd;
+    double alat      = pow((4.0 / p->rho), (1.0 / 3.0));
+    int ilo = HMAX((int)(0.0 / (0.5 * alat) - 1), 0);
+    int ihi = HMIN((int)(xhi / (0.5 * alat) + 1), 2 * nx - 1);
+    int jlo = HMAX((int)(0.0 / (0.5 * alat) - 1), 0);
+    int jhi = HMIN((int)(yhi / (0.5 * alat) + 1), 2 * ny - 1);
+    int klo = HMAX((int)(0.0 / (0.5 * alat) - 1), 0);
+    int khi = HMIN((int)(zhi / (0.5 * alat) + 1), 2 * nz - 1);
+
+    /* traversal in 8x8x8 sub-boxes, verletlist/atom.c:170-245 */
+    srand(1);
+    int n = 0, sx = 0, sy = 0, sz = 0, ox = 0, oy = 0, oz = 0;
+    const int sub = 8;
+    while (oz * sub <= khi) {
+        int k = oz * sub + sz, j = oy * sub + sy, i = ox * sub + sx;
+        if (((i + j + k) % 2 == 0) && i >= ilo && i <= ihi && j >= jlo && j <= jhi && k >= klo &&
+            k <= khi) {
+            double xt = 0.5 * alat * i, yt = 0.5 * alat * j, zt = 0.5 * alat * k;
+            if (xt >= 0.0 && xt < xhi && yt >= 0.0 && yt < yhi && zt >= 0.0 && zt < zhi &&
+                n < natoms) {
+                int seed = k * (2 * ny) * (2 * nx) + j * (2 * nx) + i + 1;
+                for (int d = 0; d < 3; d++) {
+                    for (int m = 0; m < 5; m++)
+                        park_miller(&seed);
+                    v[3 * n + d] = park_miller(&seed);
+                }
+                x[3 * n + 0] = xt;
+                x[3 * n + 1] = yt;
+                x[3 * n + 2] = zt;
+                type[n]      = rand() % p->ntypes;
+                n++;
+            }
+        }
+        if (++sx == sub) { sx = 0; sy++; }
+        if (sy == sub) { sy = 0; sz++; }
+        if (sz == sub) { sz = 0; ox++; }
+        if (ox * sub > ihi) { ox = 0; oy++; }
+        if (oy * sub > jhi) { oy = 0; oz++; }
+    }
+
+    /* adjustThermo: remove centre-of-mass motion, rescale to temp */
+    double mvv2e = p->force_field == MDB_FF_EAM ? 1.036427e-04 : 1.0;
+    double dof   = p->force_field == MDB_FF_EAM ? (natoms * 3 - 3) * 8.617343e-05
+                                                : (double)(natoms * 3 - 3);
+    double t_scale = mvv2e / dof;
+    double vt[3]   = { 0.0, 0.0, 0.0 };
+    for (int i = 0; i < n; i++)
+        for (int d = 0; d < 3; d++)
+            vt[d] += v[3 * i + d];
+    for (int d = 0; d < 3; d++)
+        vt[d] = vt[d] / natoms;
+    for (int i = 0; i < n; i++)
+        for (int d = 0; d < 3; d++)
+            v[3 * i + d] -= vt[d];
+    double t = 0.0;
+    for (int i = 0; i < n; i++)
+        t += (v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2]) *
+             p->mass;
+    t *= t_scale;
+    double factor = sqrt(p->temp / t);
+    for (int i = 0; i < 3 * n; i++)
+        v[i] *= factor;
+    *xo = x;
+    *vo = v;
+    *to = type;
+    return n;
+}
+
+int mdbh_read_dmp(MdbHostParams* p, const char* path, double** xo, double** vo, int** to)
+{
+    FILE* fp = fopen(path, "r");
+    if (!fp) return -MDB_ERR_ARG;
+    char line[4096];
+    int natoms = 0, read = 0, have_ts = 0;
+    double lo[3] = { 0, 0, 0 }, hi[3] = { 0, 0, 0 };
+    double *x = NULL, *v = NULL;
+    int* type = NULL;
+    int bad   = 0;
+    while (!bad && fgets(line, sizeof line, fp)) {
+        if (strncmp(line, "ITEM: ", 6) != 0) {
+            bad = 1;
+            break;
+        }
+        const char* item = line + 6;
+        if (strncmp(item, "TIMESTEP", 8) == 0) {
+            bad     = !fgets(line, sizeof line, fp);
+            have_ts = 1;
+        } else if (strncmp(item, "NUMBER OF ATOMS", 15) == 0) {
+            bad    = !fgets(line, sizeof line, fp);
+            natoms = atoi(line);
+            if (natoms <= 0) bad = 1;
+        } else if (strncmp(item, "BOX BOUNDS pp pp pp", 19) == 0) {
+            for (int d = 0; d < 3 && !bad; d++) {
+                if (!fgets(line, sizeof line, fp) || sscanf(line, "%lf %lf", &lo[d], &hi[d]) != 2)
+                    bad = 1;
+            }
+        } else if (strncmp(item, "ATOMS id type x y z vx vy vz", 28) == 0) {
+            if (natoms <= 0) {
+                bad = 1;
+                break;
+            }
+            x    = calloc(3 * (size_t)natoms, sizeof(double));
+            v    = calloc(3 * (size_t)natoms, sizeof(double));
+            type = calloc((size_t)natoms, sizeof(int));
+            for (int i = 0; i < natoms && !bad; i++) {
+                int id, t;
+                double a[6];
+                if (!fgets(line, sizeof line, fp) ||
+                    sscanf(line, "%d %d %lf %lf %lf %lf %lf %lf", &id, &t, &a[0], &a[1], &a[2],
+                        &a[3], &a[4], &a[5]) != 8 ||
+                    id < 1 || id > natoms) {
+                    bad = 1;
+                    break;
+                }
+                id--;
+                type[id] = t;
+                for (int d = 0; d < 3; d++) {
+                    x[3 * id + d] = a[d];
+                    v[3 * id + d] = a[3 + d];
+                }
+                read++;
+            }
+            break;
+        } else {
+            bad = 1;
+        }
+    }
+    fclose(fp);
+    if (bad || !have_ts || read != natoms) {
+        free(x);
+        free(v);
+        free(type);
+        return -MDB_ERR_ARG;
+    }
+    p->xprd      = hi[0] - lo[0];
+    p->yprd      = hi[1] - lo[1];
+    p->zprd      = hi[2] - lo[2];
+    p->from_file = 1;
+    *xo          = x;
+    *vo          = v;
+    *to          = type;
+    return natoms;
+}
+
+int mdbh_write_dmp(const char* path, int n, const double* x, const double* v, const int* type,
+    double xprd, double yprd, double zprd)
+{
+    FILE* fp = fopen(path, "w");
+    if (!fp) return MDB_ERR_ARG;
+    fprintf(fp, "ITEM: TIMESTEP\n0\nITEM: NUMBER OF ATOMS\n%d\nITEM: BOX BOUNDS pp pp pp\n", n);
+    fprintf(fp, "0.0 %.17g\n0.0 %.17g\n0.0 %.17g\n", xprd, yprd, zprd);
+    fprintf(fp, "ITEM: ATOMS id type x y z vx vy vz\n");
+    for (int i = 0; i < n; i++)
+        fprintf(fp, "%d %d %.17g %.17g %.17g %.17g %.17g %.17g\n", i + 1, type[i], x[3 * i],
+            x[3 * i + 1], x[3 * i + 2], v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+    return fclose(fp) == 0 ? MDB_OK : MDB_ERR_ARG;
+}
+
+void mdbh_mdb_params(const MdbHostParams* p, int natoms, MdbParams* o)
+{
+    memset(o, 0, sizeof *o);
+    o->force_field      = p->force_field;
+    o->half_neigh       = p->half_neigh;
+    o->precision        = p->precision;
+    o->bin_rule         = p->from_file ? MDB_BINS_FILE : MDB_BINS_LATTICE;
+    o->nx               = p->nx;
+    o->ny               = p->ny;
+    o->nz               = p->nz;
+    o->pbc_x            = p->pbc_x;
+    o->pbc_y            = p->pbc_y;
+    o->pbc_z            = p->pbc_z;
+    o->ntypes           = p->ntypes;
+    o->reneigh_every    = p->reneigh_every;
+    o->nstat            = p->nstat;
+    o->maxneighs        = 100;
+    o->natoms           = natoms;
+    o->xprd             = p->xprd;
+    o->yprd             = p->yprd;
+    o->zprd             = p->zprd;
+    o->dt               = p->dt;
+    o->dtforce          = p->dtforce;
+    o->mass             = p->mass;
+    o->cutforce         = p->cutforce;
+    o->cutneigh         = p->cutneigh;
+    o->epsilon          = p->epsilon;
+    o->sigma            = p->sigma;
+    o->epsilon_per_type = p->has_types ? p->epsilon_per_type : NULL;
+    o->sigma_per_type   = p->has_types ? p->sigma_per_type : NULL;
+}

@@ -1,0 +1,462 @@
+"""Python binding of libmdb (the B200 MD-Bench timestep) over its C ABI.
+
+This mirrors the reference's plugin surface (computeForce, buildNeighbor,
+updatePbc, updateAtomsPbc, initialIntegrate, finalIntegrate, computeThermo)
+one call per hook, plus the whole graph-captured loop (``System.run``).
+Everything runs on the GPU; there is no CPU fallback: importing this module
+without the built ``libmdb.so`` or calling it without a CUDA device raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmdb.so")
+
+FF_LJ, FF_EAM = 0, 1
+PREC_FP64, PREC_MIXED, PREC_MIXED_COMP = 0, 1, 2
+BINS_LATTICE, BINS_FILE = 0, 1
+PRECISIONS = {"fp64": PREC_FP64, "mixed": PREC_MIXED, "mixed_comp": PREC_MIXED_COMP}
+
+
+class MdbError(RuntimeError):
+    pass
+
+
+class MdbParams(C.Structure):
+    _fields_ = [
+        ("force_field", C.c_int), ("half_neigh", C.c_int), ("precision", C.c_int),
+        ("bin_rule", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("pbc_x", C.c_int), ("pbc_y", C.c_int), ("pbc_z", C.c_int), ("ntypes", C.c_int),
+        ("reneigh_every", C.c_int), ("nstat", C.c_int), ("maxneighs", C.c_int),
+        ("natoms", C.c_int), ("device", C.c_int),
+        ("xprd", C.c_double), ("yprd", C.c_double), ("zprd", C.c_double),
+        ("dt", C.c_double), ("dtforce", C.c_double), ("mass", C.c_double),
+        ("cutforce", C.c_double), ("cutneigh", C.c_double),
+        ("epsilon", C.c_double), ("sigma", C.c_double),
+        ("epsilon_per_type", C.POINTER(C.c_double)),
+        ("sigma_per_type", C.POINTER(C.c_double)),
+    ]
+
+
+class MdbEamTables(C.Structure):
+    _fields_ = [
+        ("nrho", C.c_int), ("nr", C.c_int), ("nrho_tot", C.c_int), ("nr_tot", C.c_int),
+        ("rdr", C.c_double), ("rdrho", C.c_double), ("cut", C.c_double), ("mass", C.c_double),
+        ("frho_spline", C.POINTER(C.c_double)), ("rhor_spline", C.POINTER(C.c_double)),
+        ("z2r_spline", C.POINTER(C.c_double)),
+    ]
+
+
+class MdbHostParams(C.Structure):
+    _fields_ = [
+        ("force_field", C.c_int), ("half_neigh", C.c_int), ("precision", C.c_int),
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("ntypes", C.c_int),
+        ("ntimes", C.c_int), ("nstat", C.c_int), ("reneigh_every", C.c_int),
+        ("pbc_x", C.c_int), ("pbc_y", C.c_int), ("pbc_z", C.c_int), ("has_types", C.c_int),
+        ("epsilon", C.c_double), ("sigma", C.c_double), ("rho", C.c_double),
+        ("temp", C.c_double), ("mass", C.c_double), ("dt", C.c_double),
+        ("cutforce", C.c_double), ("skin", C.c_double),
+        ("epsilon_per_type", C.c_double * 8), ("sigma_per_type", C.c_double * 8),
+        ("xprd", C.c_double), ("yprd", C.c_double), ("zprd", C.c_double),
+        ("from_file", C.c_int),
+        ("lattice", C.c_double), ("cutneigh", C.c_double), ("dtforce", C.c_double),
+    ]
+
+
+class MdbThermo(C.Structure):
+    _fields_ = [("step", C.c_int), ("temperature", C.c_double), ("pressure", C.c_double),
+                ("ke", C.c_double), ("pe", C.c_double), ("etotal", C.c_double)]
+
+    def as_dict(self):
+        return dict(step=self.step, T=self.temperature, P=self.pressure, KE=self.ke,
+                    PE=self.pe, E=self.etotal)
+
+
+# every symbol include/mdb.h declares
+EXPORTS = [
+    "mdb_create", "mdb_destroy", "mdb_status_string", "mdb_last_error", "mdb_stream",
+    "mdb_synchronize", "mdb_set_eam", "mdb_eam_read_funcfl", "mdb_eam_free", "mdb_set_atoms",
+    "mdb_get_atoms", "mdb_setup_pbc", "mdb_update_pbc", "mdb_update_atoms_pbc",
+    "mdb_build_neighbor", "mdb_compute_force", "mdb_compute_force_energy",
+    "mdb_initial_integrate", "mdb_final_integrate", "mdb_thermo", "mdb_setup", "mdb_run", "mdb_get_counts",
+    "mdb_get_positions_all", "mdb_get_ghosts", "mdb_get_neighbor_list",
+    "mdb_get_bin_geometry", "mdb_get_eam_fp", "mdb_launch_count",
+]
+# every symbol include/mdb_host.h declares
+HOST_EXPORTS = [
+    "mdbh_defaults", "mdbh_read_params", "mdbh_read_types", "mdbh_apply_eam",
+    "mdbh_finalize", "mdbh_create_fcc", "mdbh_read_dmp", "mdbh_write_dmp", "mdbh_mdb_params",
+]
+
+_lib = None
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+def load():
+    """Load libmdb.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise MdbError(f"{LIB_PATH} is missing: build it with `make -C md-bench_b200`")
+    lib = C.CDLL(LIB_PATH)
+    vp, ip = C.c_void_p, C.c_int
+    sig = {
+        "mdb_create": ([C.POINTER(MdbParams), C.POINTER(vp)], ip),
+        "mdb_destroy": ([vp], ip),
+        "mdb_status_string": ([ip], C.c_char_p),
+        "mdb_last_error": ([vp], C.c_char_p),
+        "mdb_stream": ([vp], vp),
+        "mdb_synchronize": ([vp], ip),
+        "mdb_set_eam": ([vp, C.POINTER(MdbEamTables)], ip),
+        "mdb_eam_read_funcfl": ([C.c_char_p, C.POINTER(MdbEamTables)], ip),
+        "mdb_eam_free": ([C.POINTER(MdbEamTables)], None),
+        "mdb_set_atoms": ([vp, ip, _dp, _dp, _ip], ip),
+        "mdb_get_atoms": ([vp, vp, vp, vp, vp], ip),
+        "mdb_thermo": ([vp, C.POINTER(MdbThermo)], ip),
+        "mdb_run": ([vp, ip, ip, C.POINTER(MdbThermo), ip, C.POINTER(ip)], ip),
+        "mdb_get_counts": ([vp, C.POINTER(ip), C.POINTER(ip), C.POINTER(ip)], ip),
+        "mdb_get_positions_all": ([vp, _dp], ip),
+        "mdb_get_ghosts": ([vp, _ip, _ip], ip),
+        "mdb_get_neighbor_list": ([vp, _ip, vp, ip], ip),
+        "mdb_get_bin_geometry": ([vp, _ip, _dp, _ip, ip], ip),
+        "mdb_get_eam_fp": ([vp, _dp], ip),
+        "mdb_launch_count": ([vp], C.c_longlong),
+    }
+    for name in ("mdb_setup_pbc", "mdb_update_pbc", "mdb_update_atoms_pbc",
+                 "mdb_build_neighbor", "mdb_compute_force", "mdb_compute_force_energy",
+                 "mdb_initial_integrate", "mdb_final_integrate", "mdb_setup"):
+        sig[name] = ([vp], ip)
+    hp = C.POINTER(MdbHostParams)
+    pd, pi = C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.POINTER(C.c_int))
+    sig.update({
+        "mdbh_defaults": ([hp], None),
+        "mdbh_read_params": ([hp, C.c_char_p], ip),
+        "mdbh_read_types": ([hp, C.c_char_p], ip),
+        "mdbh_apply_eam": ([hp, C.POINTER(MdbEamTables)], None),
+        "mdbh_finalize": ([hp], None),
+        "mdbh_create_fcc": ([hp, pd, pd, pi], ip),
+        "mdbh_read_dmp": ([hp, C.c_char_p, pd, pd, pi], ip),
+        "mdbh_write_dmp": ([C.c_char_p, ip, _dp, _dp, _ip, C.c_double, C.c_double,
+                            C.c_double], ip),
+        "mdbh_mdb_params": ([hp, ip, C.POINTER(MdbParams)], None),
+    })
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = lib
+    return lib
+
+
+_libc = C.CDLL(None)
+_libc.free.argtypes = [C.c_void_p]
+
+
+def host_params(**kw):
+    """Reference defaults (mdbh_defaults) with overrides, e.g. nx=64, half_neigh=1.
+
+    ``eam`` (tables from :func:`read_funcfl`) applies initEam's overrides;
+    ``types`` = (epsilon_per_type, sigma_per_type) sets a types file's content.
+    Call :func:`finalize` (done by the builders below) before use."""
+    lib = load()
+    p = MdbHostParams()
+    lib.mdbh_defaults(C.byref(p))
+    eam = kw.pop("eam", None)
+    types = kw.pop("types", None)
+    if isinstance(kw.get("precision"), str):
+        kw["precision"] = PRECISIONS[kw["precision"]]
+    if eam is not None:
+        t, _keep = _eam_struct(eam)
+        lib.mdbh_apply_eam(C.byref(p), C.byref(t))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    if types is not None:
+        eps, sig = types
+        p.ntypes = len(eps)
+        p.has_types = 1
+        for i, (e, s) in enumerate(zip(eps, sig)):
+            p.epsilon_per_type[i] = e
+            p.sigma_per_type[i] = s
+    return p
+
+
+def _take(ptr, n, dtype, shape):
+    a = np.ctypeslib.as_array(ptr, (n,)).astype(dtype, copy=True).reshape(shape)
+    _libc.free(C.cast(ptr, C.c_void_p))
+    return a
+
+
+def create_fcc(hp):
+    """createAtom + adjustThermo on the host: (x, v, type) as numpy arrays."""
+    lib = load()
+    lib.mdbh_finalize(C.byref(hp))
+    xp, vp, tp = C.POINTER(C.c_double)(), C.POINTER(C.c_double)(), C.POINTER(C.c_int)()
+    n = lib.mdbh_create_fcc(C.byref(hp), C.byref(xp), C.byref(vp), C.byref(tp))
+    if n < 0:
+        raise MdbError(f"mdbh_create_fcc failed ({-n})")
+    return (_take(xp, 3 * n, np.float64, (n, 3)), _take(vp, 3 * n, np.float64, (n, 3)),
+            _take(tp, n, np.int32, (n,)))
+
+
+def read_dmp(hp, path):
+    """readAtom_dmp: sets hp's box and from_file; returns (x, v, type)."""
+    lib = load()
+    xp, vp, tp = C.POINTER(C.c_double)(), C.POINTER(C.c_double)(), C.POINTER(C.c_int)()
+    n = lib.mdbh_read_dmp(C.byref(hp), path.encode(), C.byref(xp), C.byref(vp), C.byref(tp))
+    if n < 0:
+        raise MdbError(f"cannot read dump {path}")
+    lib.mdbh_finalize(C.byref(hp))
+    return (_take(xp, 3 * n, np.float64, (n, 3)), _take(vp, 3 * n, np.float64, (n, 3)),
+            _take(tp, n, np.int32, (n,)))
+
+
+def write_dmp(path, x, v, t, box):
+    lib = load()
+    rc = lib.mdbh_write_dmp(path.encode(), len(t), np.ascontiguousarray(x, np.float64).ravel(),
+                            np.ascontiguousarray(v, np.float64).ravel(),
+                            np.ascontiguousarray(t, np.int32), *box)
+    if rc:
+        raise MdbError(f"cannot write dump {path}")
+
+
+def _eam_struct(t):
+    keep = [np.ascontiguousarray(t[k], dtype=np.float64)
+            for k in ("frho_spline", "rhor_spline", "z2r_spline")]
+    ptr = [a.ctypes.data_as(C.POINTER(C.c_double)) for a in keep]
+    s = MdbEamTables(nrho=t["nrho"], nr=t["nr"], nrho_tot=t["nrho_tot"], nr_tot=t["nr_tot"],
+                     rdr=t["rdr"], rdrho=t["rdrho"], cut=t["cut"], mass=t["mass"],
+                     frho_spline=ptr[0], rhor_spline=ptr[1], z2r_spline=ptr[2])
+    return s, keep
+
+
+def system_from_host(hp, natoms, eam=None, device=0, **overrides):
+    """A :class:`System` configured exactly as the reference configures itself."""
+    lib = load()
+    lib.mdbh_finalize(C.byref(hp))
+    mp = MdbParams()
+    lib.mdbh_mdb_params(C.byref(hp), natoms, C.byref(mp))
+    kw = {f: getattr(mp, f) for f, _ in MdbParams._fields_
+          if f not in ("epsilon_per_type", "sigma_per_type")}
+    kw["pbc"] = (kw.pop("pbc_x"), kw.pop("pbc_y"), kw.pop("pbc_z"))
+    kw["device"] = device
+    if hp.has_types:
+        kw["epsilon_per_type"] = list(hp.epsilon_per_type)[:hp.ntypes]
+        kw["sigma_per_type"] = list(hp.sigma_per_type)[:hp.ntypes]
+    kw.update(overrides)
+    return System(eam=eam, **kw)
+
+
+def read_funcfl(path):
+    """EAM tables from a funcfl file (mdb_eam_read_funcfl) as numpy arrays."""
+    lib = load()
+    t = MdbEamTables()
+    rc = lib.mdb_eam_read_funcfl(path.encode(), C.byref(t))
+    if rc:
+        raise MdbError(f"cannot read EAM file {path}: {lib.mdb_status_string(rc).decode()}")
+    out = dict(nrho=t.nrho, nr=t.nr, nrho_tot=t.nrho_tot, nr_tot=t.nr_tot, rdr=t.rdr,
+               rdrho=t.rdrho, cut=t.cut, mass=t.mass,
+               frho_spline=np.ctypeslib.as_array(t.frho_spline, (t.nrho_tot,)).copy(),
+               rhor_spline=np.ctypeslib.as_array(t.rhor_spline, (t.nr_tot,)).copy(),
+               z2r_spline=np.ctypeslib.as_array(t.z2r_spline, (t.nr_tot,)).copy())
+    lib.mdb_eam_free(C.byref(t))
+    return out
+
+
+class System:
+    """One device-resident MD system (an ``MdbCtx``)."""
+
+    def __init__(self, *, xprd, yprd, zprd, cutforce, cutneigh, dt, dtforce, natoms,
+                 mass=1.0, force_field=FF_LJ, half_neigh=0, precision=PREC_FP64,
+                 bin_rule=BINS_LATTICE, nx=0, ny=0, nz=0, ntypes=1, epsilon=1.0, sigma=1.0,
+                 epsilon_per_type=None, sigma_per_type=None, reneigh_every=20, nstat=100,
+                 maxneighs=100, pbc=(1, 1, 1), device=0, eam=None):
+        self.lib = load()
+        if isinstance(precision, str):
+            precision = PRECISIONS[precision]
+        p = MdbParams(force_field=force_field, half_neigh=half_neigh, precision=precision,
+                      bin_rule=bin_rule, nx=nx, ny=ny, nz=nz, pbc_x=pbc[0], pbc_y=pbc[1],
+                      pbc_z=pbc[2], ntypes=ntypes, reneigh_every=reneigh_every, nstat=nstat,
+                      maxneighs=maxneighs, natoms=natoms, device=device, xprd=xprd,
+                      yprd=yprd, zprd=zprd, dt=dt, dtforce=dtforce, mass=mass,
+                      cutforce=cutforce, cutneigh=cutneigh, epsilon=epsilon, sigma=sigma)
+        keep = []
+        if epsilon_per_type is not None:
+            e = np.ascontiguousarray(epsilon_per_type, dtype=np.float64)
+            s = np.ascontiguousarray(sigma_per_type, dtype=np.float64)
+            keep += [e, s]
+            p.epsilon_per_type = e.ctypes.data_as(C.POINTER(C.c_double))
+            p.sigma_per_type = s.ctypes.data_as(C.POINTER(C.c_double))
+        h = C.c_void_p()
+        rc = self.lib.mdb_create(C.byref(p), C.byref(h))
+        if rc:
+            raise MdbError(f"mdb_create failed: {self.lib.mdb_status_string(rc).decode()}")
+        self.h = h
+        self.params = p
+        self.nlocal = 0
+        if eam is not None:
+            self.set_eam(eam)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mdb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _ck(self, rc, what):
+        if rc:
+            msg = self.lib.mdb_last_error(self.h)
+            raise MdbError(f"{what}: {self.lib.mdb_status_string(rc).decode()}"
+                           f" ({msg.decode() if msg else ''})")
+
+    # -- data ---------------------------------------------------------------
+    def set_eam(self, t):
+        self._eam_keep = [np.ascontiguousarray(t[k], dtype=np.float64)
+                          for k in ("frho_spline", "rhor_spline", "z2r_spline")]
+        ptr = [a.ctypes.data_as(C.POINTER(C.c_double)) for a in self._eam_keep]
+        tab = MdbEamTables(nrho=t["nrho"], nr=t["nr"], nrho_tot=t["nrho_tot"],
+                           nr_tot=t["nr_tot"], rdr=t["rdr"], rdrho=t["rdrho"], cut=t["cut"],
+                           mass=t["mass"], frho_spline=ptr[0], rhor_spline=ptr[1],
+                           z2r_spline=ptr[2])
+        self._ck(self.lib.mdb_set_eam(self.h, C.byref(tab)), "mdb_set_eam")
+
+    def set_atoms(self, x, v, type_):
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+        v = np.ascontiguousarray(v, dtype=np.float64).reshape(-1)
+        t = np.ascontiguousarray(type_, dtype=np.int32)
+        self._ck(self.lib.mdb_set_atoms(self.h, len(t), x, v, t), "mdb_set_atoms")
+        self.nlocal = len(t)
+
+    def atoms(self):
+        n = self.nlocal
+        x = np.zeros((n, 3)); v = np.zeros((n, 3)); f = np.zeros((n, 3))
+        t = np.zeros(n, dtype=np.int32)
+        ptr = lambda a: a.ctypes.data_as(C.c_void_p)
+        self._ck(self.lib.mdb_get_atoms(self.h, ptr(x), ptr(v), ptr(f), ptr(t)),
+                 "mdb_get_atoms")
+        return x, v, f, t
+
+    def counts(self):
+        nl, ng, mx = C.c_int(), C.c_int(), C.c_int()
+        self._ck(self.lib.mdb_get_counts(self.h, C.byref(nl), C.byref(ng), C.byref(mx)),
+                 "mdb_get_counts")
+        return nl.value, ng.value, mx.value
+
+    def positions_all(self):
+        nl, ng, _ = self.counts()
+        x = np.zeros((nl + ng) * 3)
+        self._ck(self.lib.mdb_get_positions_all(self.h, x), "mdb_get_positions_all")
+        return x.reshape(-1, 3)
+
+    def ghosts(self):
+        _, ng, _ = self.counts()
+        bm = np.zeros(max(ng, 1), dtype=np.int32)
+        pb = np.zeros(max(3 * ng, 3), dtype=np.int32)
+        self._ck(self.lib.mdb_get_ghosts(self.h, bm, pb), "mdb_get_ghosts")
+        return bm[:ng], pb[:3 * ng].reshape(ng, 3)
+
+    def neighbor_list(self):
+        nl, _, mx = self.counts()
+        nn = np.zeros(nl, dtype=np.int32)
+        nb = np.zeros(nl * mx, dtype=np.int32)
+        self._ck(self.lib.mdb_get_neighbor_list(self.h, nn, nb.ctypes.data_as(C.c_void_p), mx),
+                 "mdb_get_neighbor_list")
+        return nn, nb.reshape(nl, mx)
+
+    def numneigh(self):
+        nl, _, _ = self.counts()
+        nn = np.zeros(nl, dtype=np.int32)
+        self._ck(self.lib.mdb_get_neighbor_list(self.h, nn, None, 0), "mdb_get_neighbor_list")
+        return nn
+
+    def bin_geometry(self):
+        ints = np.zeros(10, dtype=np.int32)
+        dbls = np.zeros(7)
+        st = np.zeros(4096, dtype=np.int32)
+        self._ck(self.lib.mdb_get_bin_geometry(self.h, ints, dbls, st, 4096),
+                 "mdb_get_bin_geometry")
+        keys_i = ["nbinx", "nbiny", "nbinz", "mbinx", "mbiny", "mbinz", "pad_x", "pad_y",
+                  "pad_z", "nstencil"]
+        keys_d = ["binsizex", "binsizey", "binsizez", "bininvx", "bininvy", "bininvz",
+                  "cutneigh"]
+        g = {k: int(v) for k, v in zip(keys_i, ints)}
+        g.update({k: float(v) for k, v in zip(keys_d, dbls)})
+        g["stencil"] = st[:g["nstencil"]].copy()
+        return g
+
+    def eam_fp(self):
+        nl, ng, _ = self.counts()
+        fp = np.zeros(nl + ng)
+        self._ck(self.lib.mdb_get_eam_fp(self.h, fp), "mdb_get_eam_fp")
+        return fp
+
+    # -- hooks --------------------------------------------------------------
+    def setup(self):
+        self._ck(self.lib.mdb_setup(self.h), "mdb_setup")
+
+    def setup_pbc(self):
+        self._ck(self.lib.mdb_setup_pbc(self.h), "mdb_setup_pbc")
+
+    def update_pbc(self):
+        self._ck(self.lib.mdb_update_pbc(self.h), "mdb_update_pbc")
+
+    def update_atoms_pbc(self):
+        self._ck(self.lib.mdb_update_atoms_pbc(self.h), "mdb_update_atoms_pbc")
+
+    def build_neighbor(self):
+        self._ck(self.lib.mdb_build_neighbor(self.h), "mdb_build_neighbor")
+
+    def compute_force(self, energy=False):
+        if energy:
+            self._ck(self.lib.mdb_compute_force_energy(self.h), "mdb_compute_force_energy")
+        else:
+            self._ck(self.lib.mdb_compute_force(self.h), "mdb_compute_force")
+
+    def initial_integrate(self):
+        self._ck(self.lib.mdb_initial_integrate(self.h), "mdb_initial_integrate")
+
+    def final_integrate(self):
+        self._ck(self.lib.mdb_final_integrate(self.h), "mdb_final_integrate")
+
+    def thermo(self):
+        t = MdbThermo()
+        self._ck(self.lib.mdb_thermo(self.h, C.byref(t)), "mdb_thermo")
+        return t.as_dict()
+
+    def step(self, n):
+        """One timestep with index n through the individual hooks."""
+        reneigh = (n + 1) % self.params.reneigh_every == 0
+        self.initial_integrate()
+        if reneigh:
+            self.update_atoms_pbc()
+            self.setup_pbc()
+            self.update_pbc()
+            self.build_neighbor()
+        else:
+            self.update_pbc()
+        self.compute_force()
+        self.final_integrate()
+
+    def run(self, nsteps, first_step=0, max_samples=64):
+        """Graph-captured loop; returns the thermo samples."""
+        buf = (MdbThermo * max(max_samples, 1))()
+        ns = C.c_int()
+        self._ck(self.lib.mdb_run(self.h, first_step, nsteps, buf, max_samples, C.byref(ns)),
+                 "mdb_run")
+        return [buf[k].as_dict() for k in range(ns.value)]
+
+    def synchronize(self):
+        self._ck(self.lib.mdb_synchronize(self.h), "mdb_synchronize")
+
+    @property
+    def stream(self):
+        return self.lib.mdb_stream(self.h)
+
+    @property
+    def launches(self):
+        return self.lib.mdb_launch_count(self.h)
