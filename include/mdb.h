@@ -153,6 +153,21 @@ int mdb_setup(MdbCtx* ctx);
 int mdb_run(MdbCtx* ctx, int first_step, int nsteps, MdbThermo* samples, int max_samples,
     int* nsamples);
 
+/* ---- allocation-free entry point -------------------------------------------
+ * No counterpart in the reference. For callers that keep their own device
+ * arrays and cannot allocate device memory (inside their own stream capture,
+ * under an allocator that owns the device, in a loop that must not call
+ * cudaMalloc): sum over n atoms of mass * (vx^2 + vy^2 + vz^2), the sum that
+ * computeThermo turns into T (common/thermo.c:74-77; T = sum * mvv2e / dof).
+ * d_v: n AoS velocity triples in device memory; d_out: one double in device
+ * memory; stream: a cudaStream_t (NULL = legacy default stream). Asynchronous.
+ * Allocates nothing: partial sums go to a static 32 KiB device array that
+ * every call on a device shares (overlapping calls on the GPU race; each call
+ * rewrites every slot it reads, so no clearing is needed). At most 8,388,608
+ * atoms per call (MDB_ERR_ARG beyond). The first call on a device looks up the
+ * array's device address; make that first call before any stream capture. */
+int mdb_kinetic_sum_noalloc(const double* d_v, int n, double mass, double* d_out, void* stream);
+
 /* ---- introspection (tests, tools) ----------------------------------------- */
 int mdb_get_counts(MdbCtx* ctx, int* nlocal, int* nghost, int* maxneighs);
 int mdb_get_positions_all(MdbCtx* ctx, double* x); /* (nlocal+nghost) x 3 */

@@ -82,7 +82,7 @@ EXPORTS = [
     "mdb_build_neighbor", "mdb_compute_force", "mdb_compute_force_energy",
     "mdb_initial_integrate", "mdb_final_integrate", "mdb_thermo", "mdb_setup", "mdb_run", "mdb_get_counts",
     "mdb_get_positions_all", "mdb_get_ghosts", "mdb_get_neighbor_list",
-    "mdb_get_bin_geometry", "mdb_get_eam_fp", "mdb_launch_count",
+    "mdb_get_bin_geometry", "mdb_get_eam_fp", "mdb_launch_count", "mdb_kinetic_sum_noalloc",
 ]
 # every symbol include/mdb_host.h declares
 HOST_EXPORTS = [
@@ -125,6 +125,7 @@ def load():
         "mdb_get_bin_geometry": ([vp, _ip, _dp, _ip, ip], ip),
         "mdb_get_eam_fp": ([vp, _dp], ip),
         "mdb_launch_count": ([vp], C.c_longlong),
+        "mdb_kinetic_sum_noalloc": ([vp, ip, C.c_double, vp, vp], ip),
     }
     for name in ("mdb_setup_pbc", "mdb_update_pbc", "mdb_update_atoms_pbc",
                  "mdb_build_neighbor", "mdb_compute_force", "mdb_compute_force_energy",
