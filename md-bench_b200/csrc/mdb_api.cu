@@ -35,22 +35,27 @@ struct MdbCtx {
 
     BinGeom g;
     std::vector<int> stencil;
+    std::vector<int4> stencil4;
     LJTable tab;
     LJTableF tabf;
-    QScale qs;
+    CellFrame cf;
+    ShiftTable shift;
     double cutforcesq = 0, cutneighsq = 0;
     double mvv2e = 1, dof_boltz = 1, t_scale = 1, p_scale = 1;
 
     // device buffers
     double4* x  = nullptr;
-    int4* xq    = nullptr;
+    float4* xr  = nullptr; // mixed path: cell-relative FP32 positions
+    int* qcell  = nullptr; // mixed path: cell of each atom
     double *vx = nullptr, *vy = nullptr, *vz = nullptr;
     double *fx = nullptr, *fy = nullptr, *fz = nullptr;
     int *border_map = nullptr, *pbc_code = nullptr;
     int *ghost_cnt = nullptr, *ghost_off = nullptr;
     int *atom_bin = nullptr, *atom_slot = nullptr;
     int *bin_count = nullptr, *bin_start = nullptr, *bin_atoms = nullptr;
-    int* stencil_d = nullptr;
+    int *bin_lcount = nullptr, *loc_start = nullptr; // locals per bin, their offsets
+    int* local_order = nullptr;                      // row t of the list -> atom
+    int4* stencil_d  = nullptr;                      // {flat offset, dx, dy, dz}
     int *numneigh = nullptr, *neighbors = nullptr;
     int* counters = nullptr;
     int* scan_scratch = nullptr;
@@ -206,12 +211,16 @@ static int setup_bins(MdbCtx* ctx)
     if (mb > (1LL << 30)) return fail(ctx, MDB_ERR_ARG, "bin grid too large");
     g.mbins = (int)mb;
     ctx->stencil.clear();
+    ctx->stencil4.clear();
     double cutsq = cut * cut;
     for (int k = -nextz; k <= nextz; k++)
         for (int j = -nexty; j <= nexty; j++)
             for (int i = -nextx; i <= nextx; i++)
-                if (bindist(g, i, j, k) < cutsq)
-                    ctx->stencil.push_back(k * g.mbiny * g.mbinx + j * g.mbinx + i);
+                if (bindist(g, i, j, k) < cutsq) {
+                    int flat = k * g.mbiny * g.mbinx + j * g.mbinx + i;
+                    ctx->stencil.push_back(flat);
+                    ctx->stencil4.push_back(make_int4(flat, i, j, k));
+                }
     g.nstencil = (int)ctx->stencil.size();
     if (g.nstencil > MDB_MAX_STENCIL) return fail(ctx, MDB_ERR_ARG, "stencil too large");
     g.xlo = fabs(0.0 - g.pad_x * g.binsizex) + 1e-9;
@@ -314,22 +323,25 @@ extern "C" int mdb_create(const MdbParams* params, MdbCtx** out)
         goto bad;
     }
     ctx->mixed = p.precision != MDB_PREC_FP64;
-    if (ctx->mixed && (p.xprd <= 2 * p.cutneigh || p.yprd <= 2 * p.cutneigh ||
-                          p.zprd <= 2 * p.cutneigh)) {
-        rc = fail(ctx, MDB_ERR_ARG,
-            "mixed precision needs every box length above twice the neighbour cutoff");
-        goto bad;
-    }
     ctx->cutforcesq = p.cutforce * p.cutforce;
     ctx->cutneighsq = p.cutneigh * p.cutneigh;
     {
-        const double two32 = 4294967296.0;
-        ctx->qs.sx         = two32 / p.xprd;
-        ctx->qs.sy         = two32 / p.yprd;
-        ctx->qs.sz         = two32 / p.zprd;
-        ctx->qs.ix         = (float)(p.xprd / two32);
-        ctx->qs.iy         = (float)(p.yprd / two32);
-        ctx->qs.iz         = (float)(p.zprd / two32);
+        // mixed-path cells: the smallest power of two G with 2 G >= cutneigh, so
+        // any listed pair lies within two cells per axis (code range -2..2)
+        double g = 1.0 / 1024;
+        while (2 * g < p.cutneigh)
+            g *= 2;
+        ctx->cf.g    = g;
+        ctx->cf.ginv = 1.0 / g;
+        for (int c = 0; c < MDB_NCODES; c++) {
+            int dx = c % 5 - 2, dy = (c / 5) % 5 - 2, dz = c / 25 - 2;
+            ctx->shift.s[c] = make_float4((float)(dx * g), (float)(dy * g), (float)(dz * g), 0.f);
+        }
+        double lmax = std::max(p.xprd, std::max(p.yprd, p.zprd)) + 2 * p.cutneigh;
+        if (ctx->mixed && lmax * ctx->cf.ginv > 1000) {
+            rc = fail(ctx, MDB_ERR_ARG, "box too large for the mixed path's cell index");
+            goto bad;
+        }
     }
     if ((rc = setup_bins(ctx)) != MDB_OK) goto bad;
     if ((rc = setup_types(ctx, p.ntypes)) != MDB_OK) goto bad;
@@ -354,8 +366,13 @@ extern "C" int mdb_create(const MdbParams* params, MdbCtx** out)
             rc = fail(ctx, MDB_ERR_NOMEM, "device allocation", e);
             goto bad;
         }
+        if ((e = dalloc(&ctx->bin_lcount, ctx->g.mbins)) != cudaSuccess ||
+            (e = dalloc(&ctx->loc_start, ctx->g.mbins + 1)) != cudaSuccess) {
+            rc = fail(ctx, MDB_ERR_NOMEM, "device allocation", e);
+            goto bad;
+        }
         cudaMemset(ctx->counters, 0, CNT_SLOTS * sizeof(int));
-        cudaMemcpy(ctx->stencil_d, ctx->stencil.data(), sizeof(int) * ctx->g.nstencil,
+        cudaMemcpy(ctx->stencil_d, ctx->stencil4.data(), sizeof(int4) * ctx->g.nstencil,
             cudaMemcpyHostToDevice);
         if ((e = cudaGetLastError()) != cudaSuccess) {
             rc = fail(ctx, MDB_ERR_CUDA, "setup copy", e);
@@ -373,7 +390,9 @@ bad:
 static void free_atom_buffers(MdbCtx* ctx)
 {
     dfree(ctx->x);
-    dfree(ctx->xq);
+    dfree(ctx->xr);
+    dfree(ctx->qcell);
+    dfree(ctx->local_order);
     dfree(ctx->vx);
     dfree(ctx->vy);
     dfree(ctx->vz);
@@ -409,6 +428,8 @@ extern "C" int mdb_destroy(MdbCtx* ctx)
     dfree(ctx->stencil_d);
     dfree(ctx->bin_count);
     dfree(ctx->bin_start);
+    dfree(ctx->bin_lcount);
+    dfree(ctx->loc_start);
     dfree(ctx->eam_frho);
     dfree(ctx->eam_rhor);
     dfree(ctx->eam_z2r);
@@ -444,14 +465,13 @@ static int alloc_ghost_sized(MdbCtx* ctx, int ghost_cap)
     dfree(ctx->x);
     ctx->x = nx;
     if (ctx->mixed) {
-        int4* nq;
-        CK(dalloc(&nq, nall));
-        if (ctx->xq) {
-            CK(cudaMemcpyAsync(nq, ctx->xq, sizeof(int4) * ctx->nlocal, cudaMemcpyDeviceToDevice, s));
-            CK(cudaStreamSynchronize(s));
-        }
-        dfree(ctx->xq);
-        ctx->xq = nq;
+        if ((long long)nall > (long long)MDB_IDX_MASK)
+            return fail(ctx, MDB_ERR_ARG, "mixed path limited to 2^25 atoms including ghosts");
+        // cells and relative positions are recomputed by every rebuild
+        dfree(ctx->xr);
+        dfree(ctx->qcell);
+        CK(dalloc(&ctx->xr, nall));
+        CK(dalloc(&ctx->qcell, nall));
     }
     dfree(ctx->border_map);
     dfree(ctx->pbc_code);
@@ -515,6 +535,7 @@ extern "C" int mdb_set_atoms(MdbCtx* ctx, int nlocal, const double* x, const dou
         CK(dalloc(&ctx->ghost_cnt, nlocal + 1));
         CK(dalloc(&ctx->ghost_off, nlocal + 1));
         CK(dalloc(&ctx->numneigh, nlocal));
+        CK(dalloc(&ctx->local_order, nlocal));
         CK(dalloc(&ctx->stage, 9 * (size_t)nlocal));
         CK(dalloc(&ctx->stage_t, nlocal));
         int nscan         = std::max(scan_scratch_ints(nlocal), scan_scratch_ints(ctx->g.mbins));
@@ -532,7 +553,6 @@ extern "C" int mdb_set_atoms(MdbCtx* ctx, int nlocal, const double* x, const dou
         double shell = (ctx->p.xprd + 2 * c) * (ctx->p.yprd + 2 * c) * (ctx->p.zprd + 2 * c) - vol;
         int gcap     = (int)std::min(2.0e9, 1.25 * dens * shell + 1024);
         ctx->x       = nullptr;
-        ctx->xq      = nullptr;
         if ((rc = alloc_ghost_sized(ctx, gcap)) != MDB_OK) return rc;
         if ((rc = alloc_list(ctx, ctx->maxneighs)) != MDB_OK) return rc;
     }
@@ -551,7 +571,8 @@ extern "C" int mdb_set_atoms(MdbCtx* ctx, int nlocal, const double* x, const dou
     }
     if (ctx->mixed) {
         long long m = launch_mark();
-        launch_quantize(s, nlocal, ctx->x, ctx->xq, ctx->qs);
+        launch_cells(s, nlocal, ctx->nall_cap, ctx->x, ctx->xr, ctx->qcell, ctx->cf,
+            ctx->counters, 1);
         launch_account(ctx, m);
     }
     CK(cudaStreamSynchronize(s));
@@ -586,7 +607,8 @@ extern "C" int mdb_get_atoms(MdbCtx* ctx, double* x, double* v, double* f, int* 
 static void enq_initial(MdbCtx* ctx)
 {
     launch_initial_integrate(ctx->s, ctx->nlocal, ctx->p.dtforce, ctx->p.dt, ctx->x, ctx->vx,
-        ctx->vy, ctx->vz, ctx->fx, ctx->fy, ctx->fz, ctx->mixed ? ctx->xq : nullptr, ctx->qs);
+        ctx->vy, ctx->vz, ctx->fx, ctx->fy, ctx->fz, ctx->mixed ? ctx->xr : nullptr,
+        ctx->qcell, ctx->cf);
 }
 
 static void enq_final(MdbCtx* ctx)
@@ -595,14 +617,21 @@ static void enq_final(MdbCtx* ctx)
         ctx->fx, ctx->fy, ctx->fz);
 }
 
+// finalIntegrate of the previous step fused with initialIntegrate of this one
+static void enq_final_initial(MdbCtx* ctx)
+{
+    launch_final_initial_integrate(ctx->s, ctx->nlocal, ctx->p.dtforce, ctx->p.dt, ctx->x,
+        ctx->vx, ctx->vy, ctx->vz, ctx->fx, ctx->fy, ctx->fz, ctx->mixed ? ctx->xr : nullptr,
+        ctx->qcell, ctx->cf);
+}
+
+// Mixed path: only the cell-relative FP32 ghost positions are refreshed
+// between rebuilds (the FP64 ghost positions are rebuilt with the ghost map).
 static void enq_ghost_update(MdbCtx* ctx)
 {
-    if (ctx->mixed)
-        launch_ghost_update_q(ctx->s, ctx->nlocal, ctx->ghost_cap, ctx->xq, ctx->border_map,
-            ctx->counters);
-    else
-        launch_ghost_update(ctx->s, ctx->nlocal, ctx->ghost_cap, ctx->x, ctx->border_map,
-            ctx->pbc_code, ctx->p.xprd, ctx->p.yprd, ctx->p.zprd, ctx->counters);
+    launch_ghost_update(ctx->s, ctx->nlocal, ctx->ghost_cap, ctx->x, ctx->border_map,
+        ctx->pbc_code, ctx->p.xprd, ctx->p.yprd, ctx->p.zprd, ctx->counters,
+        ctx->mixed ? ctx->xr : nullptr, ctx->qcell, ctx->cf);
 }
 
 static void enq_force(MdbCtx* ctx, bool energy)
@@ -613,13 +642,14 @@ static void enq_force(MdbCtx* ctx, bool energy)
     double* ep1    = ctx->partials + ctx->npart;
     if (ctx->p.force_field == MDB_FF_EAM) {
         if (ctx->mixed)
-            launch_eam_mixed(s, energy, n, ctx->ghost_cap, ctx->xq, ctx->qs, ctx->numneigh,
-                ctx->neighbors, ctx->ld, (float)ctx->cutforcesq, ctx->eam, ctx->border_map,
-                ctx->counters, ctx->fp, ctx->fx, ctx->fy, ctx->fz, ep0, ep1);
+            launch_eam_mixed(s, energy, n, ctx->ghost_cap, ctx->local_order, ctx->xr,
+                ctx->shift, ctx->numneigh, ctx->neighbors, ctx->ld, (float)ctx->cutforcesq,
+                ctx->eam, ctx->border_map, ctx->counters, ctx->fp, ctx->fx, ctx->fy, ctx->fz,
+                ep0, ep1);
         else
-            launch_eam_fp64(s, energy, n, ctx->ghost_cap, ctx->x, ctx->numneigh, ctx->neighbors,
-                ctx->ld, ctx->cutforcesq, ctx->eam, ctx->border_map, ctx->counters, ctx->fp,
-                ctx->fx, ctx->fy, ctx->fz, ep0, ep1);
+            launch_eam_fp64(s, energy, n, ctx->ghost_cap, ctx->local_order, ctx->x,
+                ctx->numneigh, ctx->neighbors, ctx->ld, ctx->cutforcesq, ctx->eam,
+                ctx->border_map, ctx->counters, ctx->fp, ctx->fx, ctx->fy, ctx->fz, ep0, ep1);
         return;
     }
     if (ctx->p.half_neigh) {
@@ -629,11 +659,11 @@ static void enq_force(MdbCtx* ctx, bool energy)
     }
     if (ctx->mixed)
         launch_lj_mixed(s, ctx->p.precision == MDB_PREC_MIXED_COMP, ctx->p.half_neigh, energy, n,
-            ctx->xq, ctx->qs, ctx->numneigh, ctx->neighbors, ctx->ld, (float)ctx->cutforcesq,
-            ctx->tabf, ctx->fx, ctx->fy, ctx->fz, ep0);
+            ctx->local_order, ctx->xr, ctx->shift, ctx->numneigh, ctx->neighbors, ctx->ld,
+            (float)ctx->cutforcesq, ctx->tabf, ctx->fx, ctx->fy, ctx->fz, ep0);
     else
-        launch_lj_fp64(s, ctx->p.half_neigh, energy, n, ctx->x, ctx->numneigh, ctx->neighbors,
-            ctx->ld, ctx->cutforcesq, ctx->tab, ctx->fx, ctx->fy, ctx->fz, ep0);
+        launch_lj_fp64(s, ctx->p.half_neigh, energy, n, ctx->local_order, ctx->x, ctx->numneigh,
+            ctx->neighbors, ctx->ld, ctx->cutforcesq, ctx->tab, ctx->fx, ctx->fy, ctx->fz, ep0);
 }
 
 // Rebuild sequence after the initial integration of a reneighbour step:
@@ -646,32 +676,44 @@ static void enq_ghosts(MdbCtx* ctx)
     launch_ghost_count(s, ctx->nlocal, ctx->x, p.cutneigh, p.xprd, p.yprd, p.zprd, p.pbc_x,
         p.pbc_y, p.pbc_z, ctx->ghost_cnt);
     scan_exclusive(ctx->ghost_cnt, ctx->ghost_off, ctx->nlocal, ctx->scan_scratch, s);
-    launch_ghost_write(s, ctx->nlocal, ctx->ghost_cap, ctx->x, ctx->mixed ? ctx->xq : nullptr,
-        p.cutneigh, p.xprd, p.yprd, p.zprd, p.pbc_x, p.pbc_y, p.pbc_z, ctx->ghost_off,
-        ctx->border_map, ctx->pbc_code, ctx->counters);
+    launch_ghost_write(s, ctx->nlocal, ctx->ghost_cap, ctx->x, p.cutneigh, p.xprd, p.yprd,
+        p.zprd, p.pbc_x, p.pbc_y, p.pbc_z, ctx->ghost_off, ctx->border_map, ctx->pbc_code,
+        ctx->counters);
+    // mixed path: cells (fixed until the next rebuild) of locals and ghosts
+    if (ctx->mixed)
+        launch_cells(s, ctx->nlocal, ctx->nall_cap, ctx->x, ctx->xr, ctx->qcell, ctx->cf,
+            ctx->counters, 0);
 }
 
 static void enq_list(MdbCtx* ctx)
 {
     cudaStream_t s = ctx->s;
     cudaMemsetAsync(ctx->bin_count, 0, sizeof(int) * ctx->g.mbins, s);
+    cudaMemsetAsync(ctx->bin_lcount, 0, sizeof(int) * ctx->g.mbins, s);
     launch_bin_count(s, ctx->nlocal, ctx->nall_cap, ctx->x, ctx->g, ctx->atom_bin,
-        ctx->atom_slot, ctx->bin_count, ctx->counters);
+        ctx->atom_slot, ctx->bin_count, ctx->bin_lcount, ctx->counters);
     scan_exclusive(ctx->bin_count, ctx->bin_start, ctx->g.mbins, ctx->scan_scratch, s);
+    scan_exclusive(ctx->bin_lcount, ctx->loc_start, ctx->g.mbins, ctx->scan_scratch, s);
     launch_bin_scatter(s, ctx->nlocal, ctx->nall_cap, ctx->atom_bin, ctx->atom_slot,
         ctx->bin_start, ctx->bin_atoms, ctx->counters);
-    launch_bin_sort(s, ctx->g.mbins, ctx->bin_start, ctx->bin_atoms);
-    launch_build_list(s, ctx->nlocal, ctx->x, ctx->g, ctx->stencil_d, ctx->atom_bin,
-        ctx->bin_start, ctx->bin_atoms, ctx->cutneighsq, ctx->p.half_neigh, ctx->maxneighs,
-        ctx->ld, ctx->neighbors, ctx->numneigh, ctx->counters);
+    launch_bin_sort(s, ctx->g.mbins, ctx->bin_start, ctx->bin_atoms, ctx->loc_start,
+        ctx->local_order);
+    launch_build_list(s, ctx->nlocal, ctx->x, ctx->g, ctx->stencil_d, ctx->local_order,
+        ctx->atom_bin, ctx->bin_start, ctx->bin_atoms, ctx->cutneighsq, ctx->p.half_neigh,
+        ctx->maxneighs, ctx->ld, ctx->neighbors, ctx->numneigh, ctx->counters,
+        ctx->mixed ? ctx->qcell : nullptr);
+}
+
+static void clear_rebuild_counters(MdbCtx* ctx)
+{
+    // CNT_MAXNEED, CNT_BADBIN, CNT_BADCELL
+    cudaMemsetAsync(ctx->counters + CNT_MAXNEED, 0, 3 * sizeof(int), ctx->s);
 }
 
 static void enq_rebuild(MdbCtx* ctx)
 {
-    cudaStream_t s = ctx->s;
-    cudaMemsetAsync(ctx->counters + CNT_MAXNEED, 0, 2 * sizeof(int), s);
-    launch_wrap(s, ctx->nlocal, ctx->x, ctx->p.xprd, ctx->p.yprd, ctx->p.zprd);
-    if (ctx->mixed) launch_quantize(s, ctx->nlocal, ctx->x, ctx->xq, ctx->qs);
+    clear_rebuild_counters(ctx);
+    launch_wrap(ctx->s, ctx->nlocal, ctx->x, ctx->p.xprd, ctx->p.yprd, ctx->p.zprd);
     enq_ghosts(ctx);
     enq_list(ctx);
 }
@@ -679,7 +721,7 @@ static void enq_rebuild(MdbCtx* ctx)
 // setup() of verletlist/main.c:96-111 builds ghosts and lists without wrapping.
 static void enq_rebuild_nowrap(MdbCtx* ctx)
 {
-    cudaMemsetAsync(ctx->counters + CNT_MAXNEED, 0, 2 * sizeof(int), ctx->s);
+    clear_rebuild_counters(ctx);
     enq_ghosts(ctx);
     enq_list(ctx);
 }
@@ -695,6 +737,8 @@ static int check_rebuild(MdbCtx* ctx)
     if (e != cudaSuccess) return -fail(ctx, MDB_ERR_CUDA, "rebuild check", e);
     const int* h = ctx->h_counters;
     if (h[CNT_BADBIN] > 0) return -fail(ctx, MDB_ERR_OVERFLOW, "atom outside the bin grid");
+    if (h[CNT_BADCELL] > 0)
+        return -fail(ctx, MDB_ERR_OVERFLOW, "mixed path: listed pair more than two cells apart");
     int again = 0;
     if (h[CNT_NGHOST_TOTAL] > ctx->ghost_cap) {
         int rc = alloc_ghost_sized(ctx, (int)(h[CNT_NGHOST_TOTAL] * 1.2) + 1024);
@@ -789,11 +833,11 @@ extern "C" int mdb_update_pbc(MdbCtx* ctx)
     NEED_ATOMS();
     if (!ctx->have_ghosts) return fail(ctx, MDB_ERR_STATE, "setup_pbc not run");
     long long m = launch_mark();
+    // FP64 ghost positions, and on the mixed path also their relative copies
     launch_ghost_update(ctx->s, ctx->nlocal, ctx->ghost_cap, ctx->x, ctx->border_map,
-        ctx->pbc_code, ctx->p.xprd, ctx->p.yprd, ctx->p.zprd, ctx->counters);
-    if (ctx->mixed)
-        launch_ghost_update_q(ctx->s, ctx->nlocal, ctx->ghost_cap, ctx->xq, ctx->border_map,
-            ctx->counters);
+        ctx->pbc_code, ctx->p.xprd, ctx->p.yprd, ctx->p.zprd, ctx->counters, nullptr, nullptr,
+        ctx->cf);
+    if (ctx->mixed) enq_ghost_update(ctx);
     launch_account(ctx, m);
     return MDB_OK;
 }
@@ -803,7 +847,9 @@ extern "C" int mdb_update_atoms_pbc(MdbCtx* ctx)
     NEED_ATOMS();
     long long m = launch_mark();
     launch_wrap(ctx->s, ctx->nlocal, ctx->x, ctx->p.xprd, ctx->p.yprd, ctx->p.zprd);
-    if (ctx->mixed) launch_quantize(ctx->s, ctx->nlocal, ctx->x, ctx->xq, ctx->qs);
+    if (ctx->mixed)
+        launch_cells(ctx->s, ctx->nlocal, ctx->nall_cap, ctx->x, ctx->xr, ctx->qcell, ctx->cf,
+            ctx->counters, 1);
     launch_account(ctx, m);
     return MDB_OK;
 }
@@ -814,7 +860,7 @@ extern "C" int mdb_build_neighbor(MdbCtx* ctx)
     if (!ctx->have_ghosts) return fail(ctx, MDB_ERR_STATE, "setup_pbc not run");
     for (int attempt = 0; attempt < 8; attempt++) {
         long long m = launch_mark();
-        cudaMemsetAsync(ctx->counters + CNT_MAXNEED, 0, 2 * sizeof(int), ctx->s);
+        clear_rebuild_counters(ctx);
         enq_list(ctx);
         launch_account(ctx, m);
         int r = check_rebuild(ctx);
@@ -923,12 +969,14 @@ extern "C" int mdb_setup(MdbCtx* ctx)
     return compute_force(ctx, true);
 }
 
+// A plain step (no rebuild, no sample) whose predecessor left its final
+// integration pending: finalIntegrate(n-1) + initialIntegrate(n) in one
+// kernel, ghost update, force. Its own final integration is left pending.
 static void enq_plain_step(MdbCtx* ctx)
 {
-    enq_initial(ctx);
+    enq_final_initial(ctx);
     enq_ghost_update(ctx);
     enq_force(ctx, false);
-    enq_final(ctx);
 }
 
 extern "C" int mdb_run(MdbCtx* ctx, int first_step, int nsteps, MdbThermo* samples,
@@ -941,20 +989,31 @@ extern "C" int mdb_run(MdbCtx* ctx, int first_step, int nsteps, MdbThermo* sampl
     int nslot = 0;
     std::vector<int> slot_step;
     const int last = first_step + nsteps - 1;
+    // finalIntegrate of step n is deferred and fused with initialIntegrate of
+    // step n+1 unless a thermo sample, a rebuild step or the end of the run
+    // needs it on its own
+    bool pending_final = false;
     for (int n = first_step; n <= last; n++) {
         bool reneigh = (n + 1) % ctx->p.reneigh_every == 0;
         bool sample  = max_samples > 0 && (n + 1) % ctx->p.nstat == 0;
-        if (!reneigh && !sample) {
+        if (!reneigh && !sample && pending_final) {
             if (!ctx->g_plain.exec) {
                 int rc = capture(ctx, ctx->g_plain, enq_plain_step);
                 if (rc) return rc;
             }
             int rc = launch_graph(ctx, ctx->g_plain);
             if (rc) return rc;
+            if (n == last) {
+                long long m = launch_mark();
+                enq_final(ctx);
+                launch_account(ctx, m);
+            }
             continue;
         }
         long long m = launch_mark();
-        enq_initial(ctx);
+        if (pending_final) enq_final_initial(ctx);
+        else enq_initial(ctx);
+        pending_final = false;
         launch_account(ctx, m);
         if (reneigh) {
             int rc = do_rebuild(ctx, true);
@@ -966,7 +1025,11 @@ extern "C" int mdb_run(MdbCtx* ctx, int first_step, int nsteps, MdbThermo* sampl
         }
         m = launch_mark();
         enq_force(ctx, sample);
-        enq_final(ctx);
+        if (sample || n == last) {
+            enq_final(ctx);
+        } else {
+            pending_final = true;
+        }
         if (sample && nslot < ctx->nred_slots && nslot < max_samples) {
             enq_thermo(ctx, nslot, true);
             slot_step.push_back(n + 1);
@@ -1101,17 +1164,23 @@ extern "C" int mdb_get_neighbor_list(MdbCtx* ctx, int* numneigh, int* neighbors,
 {
     NEED_ATOMS();
     if (!ctx->have_list) return fail(ctx, MDB_ERR_STATE, "no neighbour list");
+    // rows are stored per list row t; atom local_order[t] owns row t. Mixed-path
+    // entries carry a cell-offset code above the index bits, masked off here.
     int n = ctx->nlocal;
-    std::vector<int> nn(n);
+    std::vector<int> nn(n), order(n);
     CK(cudaStreamSynchronize(ctx->s));
     CK(cudaMemcpy(nn.data(), ctx->numneigh, sizeof(int) * n, cudaMemcpyDeviceToHost));
-    if (numneigh) memcpy(numneigh, nn.data(), sizeof(int) * n);
+    CK(cudaMemcpy(order.data(), ctx->local_order, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    if (numneigh)
+        for (int t = 0; t < n; t++)
+            numneigh[order[t]] = nn[t];
     if (neighbors) {
+        const int mask = ctx->mixed ? MDB_IDX_MASK : -1;
         std::vector<int> all((size_t)ctx->maxneighs * ctx->ld);
         CK(cudaMemcpy(all.data(), ctx->neighbors, sizeof(int) * all.size(), cudaMemcpyDeviceToHost));
-        for (int i = 0; i < n; i++)
-            for (int k = 0; k < nn[i] && k < ld && k < ctx->maxneighs; k++)
-                neighbors[(size_t)i * ld + k] = all[(size_t)k * ctx->ld + i];
+        for (int t = 0; t < n; t++)
+            for (int k = 0; k < nn[t] && k < ld && k < ctx->maxneighs; k++)
+                neighbors[(size_t)order[t] * ld + k] = all[(size_t)k * ctx->ld + t] & mask;
     }
     return MDB_OK;
 }

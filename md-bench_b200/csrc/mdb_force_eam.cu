@@ -3,11 +3,13 @@
 // (2) fp copied to the ghosts through the ghost map (the mid-step halo),
 // (3) pair forces from rho', phi' and fp_i + fp_j.
 //
-// Spline tables are re-laid out as rows of 8 coefficients (one 64-byte row
-// per grid point instead of 56 bytes) so a row is two aligned sectors.
+// Thread t handles atom order[t]. Spline tables are re-laid out as rows of 8
+// coefficients (one 64-byte row per grid point instead of 56 bytes) so a row
+// is two aligned sectors.
 // FP64 path: -fmad=false, bit-identical to the reference's strict build.
-// Mixed path: pair terms and spline rows in FP32 on exact fixed-point pair
-// differences; the density (embedding) sum, F'(rho) and all energy sums FP64.
+// Mixed path: pair terms and spline rows in FP32 on cell-relative FP32
+// positions (see mdb_force_lj.cu); the density (embedding) sum, F'(rho) and
+// all energy sums in FP64.
 #include "mdb_internal.cuh"
 
 namespace mdb {
@@ -17,16 +19,17 @@ static constexpr int EUNROLL     = 4;
 
 template <bool ENERGY>
 __global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_fp64(int nlocal,
-    const double4* __restrict__ x, const int* __restrict__ numneigh,
-    const int* __restrict__ neighbors, int ld, double cutforcesq, EamDev e,
-    double* __restrict__ fp, double* __restrict__ epart)
+    const int* __restrict__ order, const double4* __restrict__ x,
+    const int* __restrict__ numneigh, const int* __restrict__ neighbors, int ld,
+    double cutforcesq, EamDev e, double* __restrict__ fp, double* __restrict__ epart)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double eng  = 0.0;
-    if (i < nlocal) {
+    if (t < nlocal) {
+        const int i      = order[t];
         const double4 xi = x[i];
-        const int n      = numneigh[i];
-        const int* nb    = neighbors + i;
+        const int n      = numneigh[t];
+        const int* nb    = neighbors + t;
         double rhoi      = 0.0;
         auto pair        = [&](const double4& xj) {
             double delx = xi.x - xj.x;
@@ -38,7 +41,7 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_fp64(int nlocal,
                 int m    = (int)(p);
                 m        = m < e.nr - 1 ? m : e.nr - 1;
                 p -= m;
-                p              = p < 1.0 ? p : 1.0;
+                p               = p < 1.0 ? p : 1.0;
                 const double* c = e.rhor + 8 * m;
                 rhoi += ((__ldg(c + 3) * p + __ldg(c + 4)) * p + __ldg(c + 5)) * p + __ldg(c + 6);
             }
@@ -85,17 +88,18 @@ __global__ void k_eam_fp_ghost(int nlocal, double* __restrict__ fp,
 
 template <bool ENERGY>
 __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_fp64(int nlocal,
-    const double4* __restrict__ x, const int* __restrict__ numneigh,
-    const int* __restrict__ neighbors, int ld, double cutforcesq, EamDev e,
-    const double* __restrict__ fp, double* __restrict__ fx, double* __restrict__ fy,
-    double* __restrict__ fz, double* __restrict__ epart)
+    const int* __restrict__ order, const double4* __restrict__ x,
+    const int* __restrict__ numneigh, const int* __restrict__ neighbors, int ld,
+    double cutforcesq, EamDev e, const double* __restrict__ fp, double* __restrict__ fx,
+    double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ epart)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double eng  = 0.0;
-    if (i < nlocal) {
+    if (t < nlocal) {
+        const int i      = order[t];
         const double4 xi = x[i];
-        const int n      = numneigh[i];
-        const int* nb    = neighbors + i;
+        const int n      = numneigh[t];
+        const int* nb    = neighbors + t;
         const double fpi = fp[i];
         double fix = 0.0, fiy = 0.0, fiz = 0.0;
         auto pair = [&](int j, const double4& xj) {
@@ -156,32 +160,31 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_fp64(int nlocal,
 }
 
 // ---- mixed ------------------------------------------------------------------
-__device__ __forceinline__ void qdelta(const int4& a, const int4& b, const QScale& qs,
-    float& dx, float& dy, float& dz)
-{
-    dx = (float)(int)((unsigned)a.x - (unsigned)b.x) * qs.ix;
-    dy = (float)(int)((unsigned)a.y - (unsigned)b.y) * qs.iy;
-    dz = (float)(int)((unsigned)a.z - (unsigned)b.z) * qs.iz;
-}
-
 template <bool ENERGY>
 __global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_mixed(int nlocal,
-    const int4* __restrict__ xq, QScale qs, const int* __restrict__ numneigh,
-    const int* __restrict__ neighbors, int ld, float cutforcesq, EamDev e,
-    double* __restrict__ fp, double* __restrict__ epart)
+    const int* __restrict__ order, const float4* __restrict__ xr, ShiftTable sh,
+    const int* __restrict__ numneigh, const int* __restrict__ neighbors, int ld,
+    float cutforcesq, EamDev e, double* __restrict__ fp, double* __restrict__ epart)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ float4 s_shift[MDB_NCODES];
+    for (int k = threadIdx.x; k < MDB_NCODES; k += blockDim.x)
+        s_shift[k] = sh.s[k];
+    __syncthreads();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double eng  = 0.0;
-    if (i < nlocal) {
-        const int4 qi = xq[i];
-        const int n   = numneigh[i];
-        const int* nb = neighbors + i;
+    if (t < nlocal) {
+        const int i     = order[t];
+        const float4 pi = xr[i];
+        const int n     = numneigh[t];
+        const int* nb   = neighbors + t;
         const float rdr = (float)e.rdr;
-        double rhoi   = 0.0; // FP64 embedding (density) sum
-        auto pair     = [&](const int4& qj) {
-            float dx, dy, dz;
-            qdelta(qi, qj, qs, dx, dy, dz);
-            float rsq = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
+        double rhoi     = 0.0; // FP64 embedding (density) sum
+        auto pair       = [&](int en, const float4& pj) {
+            const float4 off = s_shift[(unsigned)en >> MDB_IDX_BITS];
+            float dx         = (pi.x - pj.x) - off.x;
+            float dy         = (pi.y - pj.y) - off.y;
+            float dz         = (pi.z - pj.z) - off.z;
+            float rsq        = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
             if (rsq < cutforcesq) {
                 float p = __fmaf_rn(sqrtf(rsq), rdr, 1.0f);
                 int m   = (int)p;
@@ -196,20 +199,22 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_mixed(int nlocal,
         };
         int k = 0;
         for (; k + EUNROLL <= n; k += EUNROLL) {
-            int j[EUNROLL];
-            int4 qj[EUNROLL];
+            int en[EUNROLL];
+            float4 pj[EUNROLL];
 #pragma unroll
             for (int u = 0; u < EUNROLL; u++)
-                j[u] = __ldcs(nb + (size_t)(k + u) * ld);
+                en[u] = __ldcs(nb + (size_t)(k + u) * ld);
 #pragma unroll
             for (int u = 0; u < EUNROLL; u++)
-                qj[u] = __ldg(xq + j[u]);
+                pj[u] = __ldg(xr + (en[u] & MDB_IDX_MASK));
 #pragma unroll
             for (int u = 0; u < EUNROLL; u++)
-                pair(qj[u]);
+                pair(en[u], pj[u]);
         }
-        for (; k < n; k++)
-            pair(__ldg(xq + __ldcs(nb + (size_t)k * ld)));
+        for (; k < n; k++) {
+            int en = __ldcs(nb + (size_t)k * ld);
+            pair(en, __ldg(xr + (en & MDB_IDX_MASK)));
+        }
         double p = 1.0 * rhoi * e.rdrho + 1.0;
         int m    = (int)(p);
         m        = m < e.nrho - 1 ? m : e.nrho - 1;
@@ -228,24 +233,32 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_mixed(int nlocal,
 
 template <bool ENERGY>
 __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_mixed(int nlocal,
-    const int4* __restrict__ xq, QScale qs, const int* __restrict__ numneigh,
-    const int* __restrict__ neighbors, int ld, float cutforcesq, EamDev e,
-    const double* __restrict__ fp, double* __restrict__ fx, double* __restrict__ fy,
-    double* __restrict__ fz, double* __restrict__ epart)
+    const int* __restrict__ order, const float4* __restrict__ xr, ShiftTable sh,
+    const int* __restrict__ numneigh, const int* __restrict__ neighbors, int ld,
+    float cutforcesq, EamDev e, const double* __restrict__ fp, double* __restrict__ fx,
+    double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ epart)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ float4 s_shift[MDB_NCODES];
+    for (int k = threadIdx.x; k < MDB_NCODES; k += blockDim.x)
+        s_shift[k] = sh.s[k];
+    __syncthreads();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double eng  = 0.0;
-    if (i < nlocal) {
-        const int4 qi   = xq[i];
-        const int n     = numneigh[i];
-        const int* nb   = neighbors + i;
+    if (t < nlocal) {
+        const int i     = order[t];
+        const float4 pi = xr[i];
+        const int n     = numneigh[t];
+        const int* nb   = neighbors + t;
         const float fpi = (float)fp[i];
         const float rdr = (float)e.rdr;
         float fix = 0.f, fiy = 0.f, fiz = 0.f;
-        auto pair = [&](int j, const int4& qj) {
-            float dx, dy, dz;
-            qdelta(qi, qj, qs, dx, dy, dz);
-            float rsq = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
+        auto pair = [&](int en, const float4& pj) {
+            const int j      = en & MDB_IDX_MASK;
+            const float4 off = s_shift[(unsigned)en >> MDB_IDX_BITS];
+            float dx         = (pi.x - pj.x) - off.x;
+            float dy         = (pi.y - pj.y) - off.y;
+            float dz         = (pi.z - pj.z) - off.z;
+            float rsq        = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
             if (rsq < cutforcesq) {
                 float r = sqrtf(rsq);
                 float p = __fmaf_rn(r, rdr, 1.0f);
@@ -259,7 +272,7 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_mixed(int nlocal,
                 float rhoip = __fmaf_rn(__fmaf_rn(r0.x, p, r0.y), p, r0.z);
                 float z2p   = __fmaf_rn(__fmaf_rn(z0.x, p, z0.y), p, z0.z);
                 float z2 = __fmaf_rn(__fmaf_rn(__fmaf_rn(z0.w, p, z1.x), p, z1.y), p, z1.z);
-                float recip = __frcp_rn(r);
+                float recip = __fdividef(1.0f, r);
                 float phi   = z2 * recip;
                 float phip  = __fmaf_rn(z2p, recip, -phi * recip);
                 float fpj   = (float)__ldg(fp + j);
@@ -273,21 +286,21 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_mixed(int nlocal,
         };
         int k = 0;
         for (; k + EUNROLL <= n; k += EUNROLL) {
-            int j[EUNROLL];
-            int4 qj[EUNROLL];
+            int en[EUNROLL];
+            float4 pj[EUNROLL];
 #pragma unroll
             for (int u = 0; u < EUNROLL; u++)
-                j[u] = __ldcs(nb + (size_t)(k + u) * ld);
+                en[u] = __ldcs(nb + (size_t)(k + u) * ld);
 #pragma unroll
             for (int u = 0; u < EUNROLL; u++)
-                qj[u] = __ldg(xq + j[u]);
+                pj[u] = __ldg(xr + (en[u] & MDB_IDX_MASK));
 #pragma unroll
             for (int u = 0; u < EUNROLL; u++)
-                pair(j[u], qj[u]);
+                pair(en[u], pj[u]);
         }
         for (; k < n; k++) {
-            int j = __ldcs(nb + (size_t)k * ld);
-            pair(j, __ldg(xq + j));
+            int en = __ldcs(nb + (size_t)k * ld);
+            pair(en, __ldg(xr + (en & MDB_IDX_MASK)));
         }
         fx[i] = (double)fix;
         fy[i] = (double)fiy;
@@ -308,50 +321,50 @@ static void fp_ghost(cudaStream_t s, int nlocal, int ghost_cap, double* fp,
     g_launches++;
 }
 
-void launch_eam_fp64(cudaStream_t s, int energy, int nlocal, int ghost_cap, const double4* x,
-    const int* numneigh, const int* neighbors, int ld, double cutforcesq, EamDev eam,
-    const int* border_map, const int* counters, double* fp, double* fx, double* fy,
-    double* fz, double* epart_rho, double* epart_pair)
-{
-    if (nlocal <= 0) return;
-    int nb = mdb_blocks(nlocal, EAM_THREADS);
-    if (energy)
-        k_eam_rho_fp64<true><<<nb, EAM_THREADS, 0, s>>>(nlocal, x, numneigh, neighbors, ld,
-            cutforcesq, eam, fp, epart_rho);
-    else
-        k_eam_rho_fp64<false><<<nb, EAM_THREADS, 0, s>>>(nlocal, x, numneigh, neighbors, ld,
-            cutforcesq, eam, fp, epart_rho);
-    g_launches++;
-    fp_ghost(s, nlocal, ghost_cap, fp, border_map, counters);
-    if (energy)
-        k_eam_force_fp64<true><<<nb, EAM_THREADS, 0, s>>>(nlocal, x, numneigh, neighbors, ld,
-            cutforcesq, eam, fp, fx, fy, fz, epart_pair);
-    else
-        k_eam_force_fp64<false><<<nb, EAM_THREADS, 0, s>>>(nlocal, x, numneigh, neighbors, ld,
-            cutforcesq, eam, fp, fx, fy, fz, epart_pair);
-    g_launches++;
-}
-
-void launch_eam_mixed(cudaStream_t s, int energy, int nlocal, int ghost_cap, const int4* xq,
-    QScale qs, const int* numneigh, const int* neighbors, int ld, float cutforcesq,
+void launch_eam_fp64(cudaStream_t s, int energy, int nlocal, int ghost_cap, const int* order,
+    const double4* x, const int* numneigh, const int* neighbors, int ld, double cutforcesq,
     EamDev eam, const int* border_map, const int* counters, double* fp, double* fx,
     double* fy, double* fz, double* epart_rho, double* epart_pair)
 {
     if (nlocal <= 0) return;
     int nb = mdb_blocks(nlocal, EAM_THREADS);
     if (energy)
-        k_eam_rho_mixed<true><<<nb, EAM_THREADS, 0, s>>>(nlocal, xq, qs, numneigh, neighbors,
+        k_eam_rho_fp64<true><<<nb, EAM_THREADS, 0, s>>>(nlocal, order, x, numneigh, neighbors,
             ld, cutforcesq, eam, fp, epart_rho);
     else
-        k_eam_rho_mixed<false><<<nb, EAM_THREADS, 0, s>>>(nlocal, xq, qs, numneigh, neighbors,
+        k_eam_rho_fp64<false><<<nb, EAM_THREADS, 0, s>>>(nlocal, order, x, numneigh, neighbors,
             ld, cutforcesq, eam, fp, epart_rho);
     g_launches++;
     fp_ghost(s, nlocal, ghost_cap, fp, border_map, counters);
     if (energy)
-        k_eam_force_mixed<true><<<nb, EAM_THREADS, 0, s>>>(nlocal, xq, qs, numneigh,
+        k_eam_force_fp64<true><<<nb, EAM_THREADS, 0, s>>>(nlocal, order, x, numneigh,
             neighbors, ld, cutforcesq, eam, fp, fx, fy, fz, epart_pair);
     else
-        k_eam_force_mixed<false><<<nb, EAM_THREADS, 0, s>>>(nlocal, xq, qs, numneigh,
+        k_eam_force_fp64<false><<<nb, EAM_THREADS, 0, s>>>(nlocal, order, x, numneigh,
+            neighbors, ld, cutforcesq, eam, fp, fx, fy, fz, epart_pair);
+    g_launches++;
+}
+
+void launch_eam_mixed(cudaStream_t s, int energy, int nlocal, int ghost_cap, const int* order,
+    const float4* xr, const ShiftTable& sh, const int* numneigh, const int* neighbors, int ld,
+    float cutforcesq, EamDev eam, const int* border_map, const int* counters, double* fp,
+    double* fx, double* fy, double* fz, double* epart_rho, double* epart_pair)
+{
+    if (nlocal <= 0) return;
+    int nb = mdb_blocks(nlocal, EAM_THREADS);
+    if (energy)
+        k_eam_rho_mixed<true><<<nb, EAM_THREADS, 0, s>>>(nlocal, order, xr, sh, numneigh,
+            neighbors, ld, cutforcesq, eam, fp, epart_rho);
+    else
+        k_eam_rho_mixed<false><<<nb, EAM_THREADS, 0, s>>>(nlocal, order, xr, sh, numneigh,
+            neighbors, ld, cutforcesq, eam, fp, epart_rho);
+    g_launches++;
+    fp_ghost(s, nlocal, ghost_cap, fp, border_map, counters);
+    if (energy)
+        k_eam_force_mixed<true><<<nb, EAM_THREADS, 0, s>>>(nlocal, order, xr, sh, numneigh,
+            neighbors, ld, cutforcesq, eam, fp, fx, fy, fz, epart_pair);
+    else
+        k_eam_force_mixed<false><<<nb, EAM_THREADS, 0, s>>>(nlocal, order, xr, sh, numneigh,
             neighbors, ld, cutforcesq, eam, fp, fx, fy, fz, epart_pair);
     g_launches++;
 }

@@ -1,20 +1,22 @@
 // Lennard-Jones forces over Verlet lists (computeForceLJFullNeigh /
 // computeForceLJHalfNeigh, verletlist/force_lj.c:17-206).
 //
-// One thread per local atom i; the list is k-major, so each step of the k
-// loop is one 128-byte coalesced read per warp, and neighbour positions are
-// 32-byte (FP64) or 16-byte (fixed point) gathers that mostly hit L2. The k
-// loop is unrolled by UNROLL with all list reads and gathers of a batch issued
-// before any arithmetic, which keeps enough bytes in flight to approach the
-// HBM bound on the list stream. Pairs are summed in list order.
+// Thread t handles atom i = order[t] (rows of one bin are adjacent threads).
+// The list is k-major, so each step of the k loop is one 128-byte coalesced
+// read per warp; neighbour positions are 32-byte (FP64) or 16-byte (mixed)
+// gathers that mostly hit L1/L2. The k loop is unrolled by UNROLL with all
+// list reads and gathers of a batch issued before any arithmetic, which keeps
+// enough bytes in flight for the HBM-bound list stream. Pairs are summed in
+// list order.
 //
 // FP64 path: -fmad=false keeps every product and sum rounded as the
 // reference's strict build rounds them, so full-list forces are bit-identical.
-// Mixed path: positions are 32-bit fixed point over the box, so the pair
-// difference qi - qj is exact in integer arithmetic (and wraps to the minimum
-// image); it is converted to FP32 once and the pair force is FP32 (explicit
-// FMAs). Force sums are FP32, or FP32 with a compensation term (two-sum) in
-// the compensated variant; the potential-energy sum is always FP64.
+// Mixed path: FP32 positions relative to the centre of each atom's cell (edge
+// G, a power of two) plus the cell offset of the pair, taken from the list
+// entry's code and a table of exact offsets in shared memory:
+// dx = (p_i - p_j) - shift[code]. No integer->float conversions and one
+// approximate reciprocal per pair; FP32 force sums (or two-sum compensated
+// sums), FP64 energy sums.
 #include "mdb_internal.cuh"
 
 namespace mdb {
@@ -26,10 +28,10 @@ int force_partial_blocks(int n) { return mdb_blocks(n > 0 ? n : 1, LJ_THREADS); 
 
 template <bool HALF, bool UNIFORM, bool ENERGY>
 __global__ void __launch_bounds__(LJ_THREADS) k_lj_fp64(int nlocal,
-    const double4* __restrict__ x, const int* __restrict__ numneigh,
-    const int* __restrict__ neighbors, int ld, double cutforcesq, LJTable tab,
-    double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
-    double* __restrict__ epart)
+    const int* __restrict__ order, const double4* __restrict__ x,
+    const int* __restrict__ numneigh, const int* __restrict__ neighbors, int ld,
+    double cutforcesq, LJTable tab, double* __restrict__ fx, double* __restrict__ fy,
+    double* __restrict__ fz, double* __restrict__ epart)
 {
     __shared__ double s_eps[MDB_MAX_TYPES * MDB_MAX_TYPES];
     __shared__ double s_sig6[MDB_MAX_TYPES * MDB_MAX_TYPES];
@@ -41,13 +43,14 @@ __global__ void __launch_bounds__(LJ_THREADS) k_lj_fp64(int nlocal,
         }
         __syncthreads();
     }
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double epot = 0.0;
-    if (i < nlocal) {
+    if (t < nlocal) {
+        const int i      = order[t];
         const double4 xi = x[i];
         const int ti     = type_of(xi);
-        const int n      = numneigh[i];
-        const int* nb    = neighbors + i;
+        const int n      = numneigh[t];
+        const int* nb    = neighbors + t;
         double fix = 0.0, fiy = 0.0, fiz = 0.0;
         const double eps0 = tab.eps[0], sig0 = tab.sig6[0];
 
@@ -117,91 +120,98 @@ __global__ void __launch_bounds__(LJ_THREADS) k_lj_fp64(int nlocal,
 
 template <bool HALF, bool UNIFORM, bool ENERGY, bool COMP>
 __global__ void __launch_bounds__(LJ_THREADS) k_lj_mixed(int nlocal,
-    const int4* __restrict__ xq, QScale qs, const int* __restrict__ numneigh,
-    const int* __restrict__ neighbors, int ld, float cutforcesq, LJTableF tab,
-    double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
-    double* __restrict__ epart)
+    const int* __restrict__ order, const float4* __restrict__ xr, ShiftTable sh,
+    const int* __restrict__ numneigh, const int* __restrict__ neighbors, int ld,
+    float cutforcesq, LJTableF tab, double* __restrict__ fx, double* __restrict__ fy,
+    double* __restrict__ fz, double* __restrict__ epart)
 {
+    __shared__ float4 s_shift[MDB_NCODES];
     __shared__ float s_eps[MDB_MAX_TYPES * MDB_MAX_TYPES];
     __shared__ float s_sig6[MDB_MAX_TYPES * MDB_MAX_TYPES];
     const int nt = tab.ntypes;
+    for (int k = threadIdx.x; k < MDB_NCODES; k += blockDim.x)
+        s_shift[k] = sh.s[k];
     if (!UNIFORM) {
         for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) {
             s_eps[k]  = tab.eps[k];
             s_sig6[k] = tab.sig6[k];
         }
-        __syncthreads();
     }
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    __syncthreads();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double epot = 0.0;
-    if (i < nlocal) {
-        const int4 qi = xq[i];
-        const int n   = numneigh[i];
-        const int* nb = neighbors + i;
+    if (t < nlocal) {
+        const int i     = order[t];
+        const float4 pi = xr[i];
+        const int ti    = __float_as_int(pi.w);
+        const int n     = numneigh[t];
+        const int* nb   = neighbors + t;
         float fix = 0.f, fiy = 0.f, fiz = 0.f;
         float cx = 0.f, cy = 0.f, cz = 0.f; // compensation terms
         const float eps0 = tab.eps[0], sig0 = tab.sig6[0];
 
-        auto acc = [&](float& s, float& c, float v) {
-            if (COMP) { // Knuth two-sum: s + c carries the exact running sum
-                float t  = s + v;
-                float bp = t - s;
-                float e  = (s - (t - bp)) + (v - bp);
-                s        = t;
+        auto acc = [&](float& s, float& c, float d, float f) {
+            if (COMP) { // Knuth two-sum: s + c carries the running sum exactly
+                float v  = d * f;
+                float u  = s + v;
+                float bp = u - s;
+                float e  = (s - (u - bp)) + (v - bp);
+                s        = u;
                 c += e;
             } else {
-                s += v;
+                s = __fmaf_rn(d, f, s);
             }
         };
 
-        auto pair = [&](int j, const int4& qj) {
-            float delx = (float)(int)((unsigned)qi.x - (unsigned)qj.x) * qs.ix;
-            float dely = (float)(int)((unsigned)qi.y - (unsigned)qj.y) * qs.iy;
-            float delz = (float)(int)((unsigned)qi.z - (unsigned)qj.z) * qs.iz;
-            float rsq  = __fmaf_rn(delx, delx, __fmaf_rn(dely, dely, delz * delz));
+        auto pair = [&](int e, const float4& pj) {
+            const int j      = e & MDB_IDX_MASK;
+            const float4 off = s_shift[(unsigned)e >> MDB_IDX_BITS];
+            float delx       = (pi.x - pj.x) - off.x;
+            float dely       = (pi.y - pj.y) - off.y;
+            float delz       = (pi.z - pj.z) - off.z;
+            float rsq        = __fmaf_rn(delx, delx, __fmaf_rn(dely, dely, delz * delz));
             float sigma6 = sig0, epsilon = eps0;
             if (!UNIFORM) {
-                int tij = qi.w * nt + qj.w;
+                int tij = ti * nt + __float_as_int(pj.w);
                 sigma6  = s_sig6[tij];
                 epsilon = s_eps[tij];
             }
             if (rsq < cutforcesq) {
-                float sr2   = __frcp_rn(rsq);
+                float sr2   = __fdividef(1.0f, rsq);
                 float sr6   = sr2 * sr2 * sr2 * sigma6;
                 float force = 48.0f * sr6 * (sr6 - 0.5f) * sr2 * epsilon;
-                float gx = delx * force, gy = dely * force, gz = delz * force;
-                acc(fix, cx, gx);
-                acc(fiy, cy, gy);
-                acc(fiz, cz, gz);
+                acc(fix, cx, delx, force);
+                acc(fiy, cy, dely, force);
+                acc(fiz, cz, delz, force);
                 if (HALF && j < nlocal) {
-                    atomicAdd(&fx[j], -(double)gx);
-                    atomicAdd(&fy[j], -(double)gy);
-                    atomicAdd(&fz[j], -(double)gz);
+                    atomicAdd(&fx[j], -(double)(delx * force));
+                    atomicAdd(&fy[j], -(double)(dely * force));
+                    atomicAdd(&fz[j], -(double)(delz * force));
                 }
                 if (ENERGY) {
-                    double e = (double)(4.0f * epsilon * sr6 * (sr6 - 1.0f));
-                    epot += (HALF && j < nlocal) ? e : 0.5 * e;
+                    double en = (double)(4.0f * epsilon * sr6 * (sr6 - 1.0f));
+                    epot += (HALF && j < nlocal) ? en : 0.5 * en;
                 }
             }
         };
 
         int k = 0;
         for (; k + UNROLL <= n; k += UNROLL) {
-            int j[UNROLL];
-            int4 qj[UNROLL];
+            int e[UNROLL];
+            float4 pj[UNROLL];
 #pragma unroll
             for (int u = 0; u < UNROLL; u++)
-                j[u] = __ldcs(nb + (size_t)(k + u) * ld);
+                e[u] = __ldcs(nb + (size_t)(k + u) * ld);
 #pragma unroll
             for (int u = 0; u < UNROLL; u++)
-                qj[u] = __ldg(xq + j[u]);
+                pj[u] = __ldg(xr + (e[u] & MDB_IDX_MASK));
 #pragma unroll
             for (int u = 0; u < UNROLL; u++)
-                pair(j[u], qj[u]);
+                pair(e[u], pj[u]);
         }
         for (; k < n; k++) {
-            int j = __ldcs(nb + (size_t)k * ld);
-            pair(j, __ldg(xq + j));
+            int e = __ldcs(nb + (size_t)k * ld);
+            pair(e, __ldg(xr + (e & MDB_IDX_MASK)));
         }
         double rx = (double)fix + (double)cx;
         double ry = (double)fiy + (double)cy;
@@ -223,87 +233,88 @@ __global__ void __launch_bounds__(LJ_THREADS) k_lj_mixed(int nlocal,
 }
 
 template <bool HALF, bool UNIFORM>
-static void lj64(cudaStream_t s, int energy, int nb, int nlocal, const double4* x,
-    const int* numneigh, const int* neighbors, int ld, double cut, const LJTable& tab,
-    double* fx, double* fy, double* fz, double* epart)
+static void lj64(cudaStream_t s, int energy, int nb, int nlocal, const int* order,
+    const double4* x, const int* numneigh, const int* neighbors, int ld, double cut,
+    const LJTable& tab, double* fx, double* fy, double* fz, double* epart)
 {
     if (energy)
-        k_lj_fp64<HALF, UNIFORM, true><<<nb, LJ_THREADS, 0, s>>>(nlocal, x, numneigh, neighbors,
-            ld, cut, tab, fx, fy, fz, epart);
+        k_lj_fp64<HALF, UNIFORM, true><<<nb, LJ_THREADS, 0, s>>>(nlocal, order, x, numneigh,
+            neighbors, ld, cut, tab, fx, fy, fz, epart);
     else
-        k_lj_fp64<HALF, UNIFORM, false><<<nb, LJ_THREADS, 0, s>>>(nlocal, x, numneigh,
+        k_lj_fp64<HALF, UNIFORM, false><<<nb, LJ_THREADS, 0, s>>>(nlocal, order, x, numneigh,
             neighbors, ld, cut, tab, fx, fy, fz, epart);
 }
 
-void launch_lj_fp64(cudaStream_t s, int half, int energy, int nlocal, const double4* x,
-    const int* numneigh, const int* neighbors, int ld, double cutforcesq, const LJTable& tab,
-    double* fx, double* fy, double* fz, double* epart)
+void launch_lj_fp64(cudaStream_t s, int half, int energy, int nlocal, const int* order,
+    const double4* x, const int* numneigh, const int* neighbors, int ld, double cutforcesq,
+    const LJTable& tab, double* fx, double* fy, double* fz, double* epart)
 {
     if (nlocal <= 0) return;
     int nb = force_partial_blocks(nlocal);
     if (half) {
         if (tab.uniform)
-            lj64<true, true>(s, energy, nb, nlocal, x, numneigh, neighbors, ld, cutforcesq, tab,
-                fx, fy, fz, epart);
+            lj64<true, true>(s, energy, nb, nlocal, order, x, numneigh, neighbors, ld,
+                cutforcesq, tab, fx, fy, fz, epart);
         else
-            lj64<true, false>(s, energy, nb, nlocal, x, numneigh, neighbors, ld, cutforcesq,
-                tab, fx, fy, fz, epart);
+            lj64<true, false>(s, energy, nb, nlocal, order, x, numneigh, neighbors, ld,
+                cutforcesq, tab, fx, fy, fz, epart);
     } else {
         if (tab.uniform)
-            lj64<false, true>(s, energy, nb, nlocal, x, numneigh, neighbors, ld, cutforcesq,
-                tab, fx, fy, fz, epart);
+            lj64<false, true>(s, energy, nb, nlocal, order, x, numneigh, neighbors, ld,
+                cutforcesq, tab, fx, fy, fz, epart);
         else
-            lj64<false, false>(s, energy, nb, nlocal, x, numneigh, neighbors, ld, cutforcesq,
-                tab, fx, fy, fz, epart);
+            lj64<false, false>(s, energy, nb, nlocal, order, x, numneigh, neighbors, ld,
+                cutforcesq, tab, fx, fy, fz, epart);
     }
     g_launches++;
 }
 
 template <bool HALF, bool UNIFORM, bool COMP>
-static void ljmx(cudaStream_t s, int energy, int nb, int nlocal, const int4* xq, QScale qs,
-    const int* numneigh, const int* neighbors, int ld, float cut, const LJTableF& tab,
-    double* fx, double* fy, double* fz, double* epart)
+static void ljmx(cudaStream_t s, int energy, int nb, int nlocal, const int* order,
+    const float4* xr, const ShiftTable& sh, const int* numneigh, const int* neighbors, int ld,
+    float cut, const LJTableF& tab, double* fx, double* fy, double* fz, double* epart)
 {
     if (energy)
-        k_lj_mixed<HALF, UNIFORM, true, COMP><<<nb, LJ_THREADS, 0, s>>>(nlocal, xq, qs,
+        k_lj_mixed<HALF, UNIFORM, true, COMP><<<nb, LJ_THREADS, 0, s>>>(nlocal, order, xr, sh,
             numneigh, neighbors, ld, cut, tab, fx, fy, fz, epart);
     else
-        k_lj_mixed<HALF, UNIFORM, false, COMP><<<nb, LJ_THREADS, 0, s>>>(nlocal, xq, qs,
+        k_lj_mixed<HALF, UNIFORM, false, COMP><<<nb, LJ_THREADS, 0, s>>>(nlocal, order, xr, sh,
             numneigh, neighbors, ld, cut, tab, fx, fy, fz, epart);
 }
 
 template <bool HALF, bool COMP>
-static void ljmx_u(cudaStream_t s, int energy, int nb, int nlocal, const int4* xq, QScale qs,
-    const int* numneigh, const int* neighbors, int ld, float cut, const LJTableF& tab,
-    double* fx, double* fy, double* fz, double* epart)
+static void ljmx_u(cudaStream_t s, int energy, int nb, int nlocal, const int* order,
+    const float4* xr, const ShiftTable& sh, const int* numneigh, const int* neighbors, int ld,
+    float cut, const LJTableF& tab, double* fx, double* fy, double* fz, double* epart)
 {
     if (tab.uniform)
-        ljmx<HALF, true, COMP>(s, energy, nb, nlocal, xq, qs, numneigh, neighbors, ld, cut, tab,
-            fx, fy, fz, epart);
+        ljmx<HALF, true, COMP>(s, energy, nb, nlocal, order, xr, sh, numneigh, neighbors, ld,
+            cut, tab, fx, fy, fz, epart);
     else
-        ljmx<HALF, false, COMP>(s, energy, nb, nlocal, xq, qs, numneigh, neighbors, ld, cut,
-            tab, fx, fy, fz, epart);
+        ljmx<HALF, false, COMP>(s, energy, nb, nlocal, order, xr, sh, numneigh, neighbors, ld,
+            cut, tab, fx, fy, fz, epart);
 }
 
 void launch_lj_mixed(cudaStream_t s, int comp, int half, int energy, int nlocal,
-    const int4* xq, QScale qs, const int* numneigh, const int* neighbors, int ld,
-    float cutforcesq, const LJTableF& tab, double* fx, double* fy, double* fz, double* epart)
+    const int* order, const float4* xr, const ShiftTable& sh, const int* numneigh,
+    const int* neighbors, int ld, float cutforcesq, const LJTableF& tab, double* fx,
+    double* fy, double* fz, double* epart)
 {
     if (nlocal <= 0) return;
     int nb = force_partial_blocks(nlocal);
     if (half) {
         if (comp)
-            ljmx_u<true, true>(s, energy, nb, nlocal, xq, qs, numneigh, neighbors, ld,
+            ljmx_u<true, true>(s, energy, nb, nlocal, order, xr, sh, numneigh, neighbors, ld,
                 cutforcesq, tab, fx, fy, fz, epart);
         else
-            ljmx_u<true, false>(s, energy, nb, nlocal, xq, qs, numneigh, neighbors, ld,
+            ljmx_u<true, false>(s, energy, nb, nlocal, order, xr, sh, numneigh, neighbors, ld,
                 cutforcesq, tab, fx, fy, fz, epart);
     } else {
         if (comp)
-            ljmx_u<false, true>(s, energy, nb, nlocal, xq, qs, numneigh, neighbors, ld,
+            ljmx_u<false, true>(s, energy, nb, nlocal, order, xr, sh, numneigh, neighbors, ld,
                 cutforcesq, tab, fx, fy, fz, epart);
         else
-            ljmx_u<false, false>(s, energy, nb, nlocal, xq, qs, numneigh, neighbors, ld,
+            ljmx_u<false, false>(s, energy, nb, nlocal, order, xr, sh, numneigh, neighbors, ld,
                 cutforcesq, tab, fx, fy, fz, epart);
     }
     g_launches++;

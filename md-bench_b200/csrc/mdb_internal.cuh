@@ -1,12 +1,16 @@
 // Internal declarations shared by the libmdb translation units.
 // Device data layout (HBM), per context:
-//   x       double4[nall_cap]  positions of locals then ghosts; .w holds the type
-//                              id as raw int bits (never used arithmetically)
-//   xq      int4[nall_cap]     mixed path: positions in 32-bit fixed point
-//                              (fraction of the box, wraps modulo the box), .w type
-//   vx,vy,vz / fx,fy,fz        SoA doubles over locals
-//   neighbors int32 [maxneighs][ld]  SoA (k-major) so a warp reads 128 B per k
-//   numneigh  int32 [nlocal]
+//   x        double4[nall_cap]  positions of locals then ghosts; .w holds the type
+//                               id as raw int bits (never used arithmetically)
+//   xr       float4[nall_cap]   mixed path: position relative to the centre of the
+//                               atom's cell (cells of edge G, a power of two, fixed at
+//                               each rebuild), .w type bits
+//   qcell    int[nall_cap]      mixed path: the cell of each atom, 10 bits per axis
+//   vx,vy,vz / fx,fy,fz         SoA doubles over locals
+//   neighbors int32 [maxneighs][ld]  SoA (k-major), row t belongs to atom
+//                               local_order[t] (atoms of one bin are adjacent rows);
+//                               mixed path: bits 0-24 index, bits 25-31 cell-offset code
+//   numneigh  int32 [nlocal]    indexed by row t
 //   bins: CSR (bin_start[mbins+1], bin_atoms[nall]) with atoms of a bin in
 //         ascending index order, so lists come out in the reference order
 #pragma once
@@ -18,6 +22,9 @@
 
 #define MDB_MAX_TYPES   8
 #define MDB_MAX_STENCIL 1331 /* (2*5+1)^3 */
+#define MDB_IDX_BITS    25   /* mixed-path list entries: index bits */
+#define MDB_IDX_MASK    ((1 << MDB_IDX_BITS) - 1)
+#define MDB_NCODES      125  /* cell offsets -2..2 per axis */
 
 // device counters (int slots)
 enum {
@@ -25,6 +32,7 @@ enum {
     CNT_NGHOST_TOTAL = 1, // ghosts requested by the last setupPbc
     CNT_MAXNEED      = 2, // largest numneigh seen when a row overflowed
     CNT_BADBIN       = 3, // atoms found outside the bin grid
+    CNT_BADCELL      = 4, // mixed path: neighbour farther than two cells
     CNT_SLOTS        = 8
 };
 
@@ -52,9 +60,15 @@ struct LJTableF {
     float sig6[MDB_MAX_TYPES * MDB_MAX_TYPES];
 };
 
-struct QScale { // fixed-point position scale: q = x * s (mod 2^32), dx = dq * inv
-    double sx, sy, sz;
-    float ix, iy, iz;
+// Mixed-path cells: edge G (a power of two, so cell offsets times G are exact
+// in FP32); shift[code] = (dqx, dqy, dqz) * G for code = (dqx+2)+5(dqy+2)+25(dqz+2).
+struct CellFrame {
+    double g;
+    double ginv;
+};
+
+struct ShiftTable {
+    float4 s[MDB_NCODES];
 };
 
 struct EamDev {
@@ -68,50 +82,36 @@ struct EamDev {
     const float* z2r32;
 };
 
-// ---- launch helpers (implemented in the .cu files) --------------------------
 namespace mdb {
 
-// scan: out[0..n] exclusive prefix sums of in[0..n-1]; out[n] = total.
-// scratch must hold scan_scratch_ints(n) ints.
-int scan_scratch_ints(int n);
-void scan_exclusive(const int* in, int* out, int n, int* scratch, cudaStream_t s);
+// ---- small device helpers ---------------------------------------------------
+__device__ __forceinline__ int type_of(const double4& p) { return (int)__double_as_longlong(p.w); }
 
-// integrator / pbc / thermo (mdb_vl.cu)
-void launch_initial_integrate(cudaStream_t s, int n, double dtf, double dt, double4* x,
-    double* vx, double* vy, double* vz, const double* fx, const double* fy, const double* fz,
-    int4* xq, QScale qs);
-void launch_final_integrate(cudaStream_t s, int n, double dtf, double* vx, double* vy,
-    double* vz, const double* fx, const double* fy, const double* fz);
-void launch_pack_atoms(cudaStream_t s, int n, const double* xa, const double* va,
-    const int* ta, double4* x, double* vx, double* vy, double* vz);
-void launch_unpack_atoms(cudaStream_t s, int n, const double4* x, const double* vx,
-    const double* vy, const double* vz, const double* fx, const double* fy, const double* fz,
-    double* xa, double* va, double* fa, int* ta);
-void launch_wrap(cudaStream_t s, int n, double4* x, double xprd, double yprd, double zprd);
-void launch_ghost_count(cudaStream_t s, int n, const double4* x, double cut, double xprd,
-    double yprd, double zprd, int px, int py, int pz, int* cnt);
-void launch_ghost_write(cudaStream_t s, int n, int ghost_cap, double4* x, int4* xq,
-    double cut, double xprd, double yprd, double zprd, int px, int py, int pz, const int* off,
-    int* border_map, int* pbc_code, int* counters);
-void launch_ghost_update(cudaStream_t s, int nlocal, int ghost_cap, double4* x,
-    const int* border_map, const int* pbc_code, double xprd, double yprd, double zprd,
-    const int* counters);
-void launch_ghost_update_q(cudaStream_t s, int nlocal, int ghost_cap, int4* xq,
-    const int* border_map, const int* counters);
-void launch_quantize(cudaStream_t s, int n, const double4* x, int4* xq, QScale qs);
-void launch_bin_count(cudaStream_t s, int nlocal, int nall_cap, const double4* x, BinGeom g,
-    int* atom_bin, int* atom_slot, int* bin_count, int* counters);
-void launch_bin_scatter(cudaStream_t s, int nlocal, int nall_cap, const int* atom_bin,
-    const int* atom_slot, const int* bin_start, int* bin_atoms, const int* counters);
-void launch_bin_sort(cudaStream_t s, int mbins, const int* bin_start, int* bin_atoms);
-void launch_build_list(cudaStream_t s, int nlocal, const double4* x, BinGeom g,
-    const int* stencil, const int* atom_bin, const int* bin_start, const int* bin_atoms,
-    double cutneighsq, int half, int maxneighs, int ld, int* neighbors, int* numneigh,
-    int* counters);
-int ke_partial_blocks(int n);
-void launch_ke_partial(cudaStream_t s, int n, const double* vx, const double* vy,
-    const double* vz, double mass, double* partials);
-void launch_reduce_partials(cudaStream_t s, int nparts, const double* partials, double* out);
+// read-only 32-byte position load as two 16-byte non-coherent loads of one sector
+__device__ __forceinline__ double4 ldg4(const double4* p)
+{
+    const double2* q = reinterpret_cast<const double2*>(p);
+    double2 a = __ldg(q), b = __ldg(q + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
+__device__ __forceinline__ int pack_cell(int cx, int cy, int cz)
+{
+    return (cx + 512) | ((cy + 512) << 10) | ((cz + 512) << 20);
+}
+
+__device__ __forceinline__ int cell_axis(int q, int a) { return ((q >> (10 * a)) & 1023) - 512; }
+
+// position relative to the centre of cell q, FP32
+__device__ __forceinline__ float4 rel_position(const double4& p, int q, const CellFrame& cf)
+{
+    float4 r;
+    r.x = (float)(p.x - ((double)cell_axis(q, 0) + 0.5) * cf.g);
+    r.y = (float)(p.y - ((double)cell_axis(q, 1) + 0.5) * cf.g);
+    r.z = (float)(p.z - ((double)cell_axis(q, 2) + 0.5) * cf.g);
+    r.w = __int_as_float(type_of(p));
+    return r;
+}
 
 // block-wide sum; the result is valid in thread 0 (all threads must call)
 __device__ __forceinline__ double block_sum(double v)
@@ -132,32 +132,76 @@ __device__ __forceinline__ double block_sum(double v)
     return t;
 }
 
-__device__ __forceinline__ int type_of(const double4& p) { return (int)__double_as_longlong(p.w); }
+// ---- launch helpers (implemented in the .cu files) --------------------------
 
-// read-only 32-byte position load as two 16-byte non-coherent loads of one sector
-__device__ __forceinline__ double4 ldg4(const double4* p)
-{
-    const double2* q = reinterpret_cast<const double2*>(p);
-    double2 a = __ldg(q), b = __ldg(q + 1);
-    return make_double4(a.x, a.y, b.x, b.y);
-}
+// scan: out[0..n] exclusive prefix sums of in[0..n-1]; out[n] = total.
+// scratch must hold scan_scratch_ints(n) ints.
+int scan_scratch_ints(int n);
+void scan_exclusive(const int* in, int* out, int n, int* scratch, cudaStream_t s);
 
-// forces (mdb_force_lj.cu, mdb_force_eam.cu)
+// integrator / pbc / thermo (mdb_vl.cu). xr/qcell are null on the FP64 path.
+void launch_initial_integrate(cudaStream_t s, int n, double dtf, double dt, double4* x,
+    double* vx, double* vy, double* vz, const double* fx, const double* fy, const double* fz,
+    float4* xr, const int* qcell, CellFrame cf);
+void launch_final_integrate(cudaStream_t s, int n, double dtf, double* vx, double* vy,
+    double* vz, const double* fx, const double* fy, const double* fz);
+// finalIntegrate of step n followed by initialIntegrate of step n+1 in one pass
+void launch_final_initial_integrate(cudaStream_t s, int n, double dtf, double dt, double4* x,
+    double* vx, double* vy, double* vz, const double* fx, const double* fy, const double* fz,
+    float4* xr, const int* qcell, CellFrame cf);
+void launch_pack_atoms(cudaStream_t s, int n, const double* xa, const double* va,
+    const int* ta, double4* x, double* vx, double* vy, double* vz);
+void launch_unpack_atoms(cudaStream_t s, int n, const double4* x, const double* vx,
+    const double* vy, const double* vz, const double* fx, const double* fy, const double* fz,
+    double* xa, double* va, double* fa, int* ta);
+void launch_wrap(cudaStream_t s, int n, double4* x, double xprd, double yprd, double zprd);
+void launch_ghost_count(cudaStream_t s, int n, const double4* x, double cut, double xprd,
+    double yprd, double zprd, int px, int py, int pz, int* cnt);
+void launch_ghost_write(cudaStream_t s, int n, int ghost_cap, double4* x, double cut,
+    double xprd, double yprd, double zprd, int px, int py, int pz, const int* off,
+    int* border_map, int* pbc_code, int* counters);
+// ghost positions from their owners; with xr/qcell also the mixed-path copies
+// (then x of the ghosts is not written: only the rebuild needs it)
+void launch_ghost_update(cudaStream_t s, int nlocal, int ghost_cap, double4* x,
+    const int* border_map, const int* pbc_code, double xprd, double yprd, double zprd,
+    const int* counters, float4* xr, const int* qcell, CellFrame cf);
+// cells and relative positions of atoms [first, first + count) (count may be
+// read from counters: pass count < 0 to use nlocal + counters[CNT_NGHOST])
+void launch_cells(cudaStream_t s, int nlocal, int nall_cap, const double4* x, float4* xr,
+    int* qcell, CellFrame cf, const int* counters, int locals_only);
+void launch_bin_count(cudaStream_t s, int nlocal, int nall_cap, const double4* x, BinGeom g,
+    int* atom_bin, int* atom_slot, int* bin_count, int* bin_lcount, int* counters);
+void launch_bin_scatter(cudaStream_t s, int nlocal, int nall_cap, const int* atom_bin,
+    const int* atom_slot, const int* bin_start, int* bin_atoms, const int* counters);
+void launch_bin_sort(cudaStream_t s, int mbins, const int* bin_start, int* bin_atoms,
+    const int* loc_start, int* local_order);
+// stencil entries: {flat bin offset, dx, dy, dz}; qcell non-null packs cell codes
+void launch_build_list(cudaStream_t s, int nlocal, const double4* x, BinGeom g,
+    const int4* stencil, const int* local_order, const int* atom_bin, const int* bin_start,
+    const int* bin_atoms, double cutneighsq, int half, int maxneighs, int ld, int* neighbors,
+    int* numneigh, int* counters, const int* qcell);
+int ke_partial_blocks(int n);
+void launch_ke_partial(cudaStream_t s, int n, const double* vx, const double* vy,
+    const double* vz, double mass, double* partials);
+void launch_reduce_partials(cudaStream_t s, int nparts, const double* partials, double* out);
+
+// forces (mdb_force_lj.cu, mdb_force_eam.cu); thread t handles atom order[t]
 int force_partial_blocks(int n);
-void launch_lj_fp64(cudaStream_t s, int half, int energy, int nlocal, const double4* x,
-    const int* numneigh, const int* neighbors, int ld, double cutforcesq, const LJTable& tab,
-    double* fx, double* fy, double* fz, double* epart);
+void launch_lj_fp64(cudaStream_t s, int half, int energy, int nlocal, const int* order,
+    const double4* x, const int* numneigh, const int* neighbors, int ld, double cutforcesq,
+    const LJTable& tab, double* fx, double* fy, double* fz, double* epart);
 void launch_lj_mixed(cudaStream_t s, int comp, int half, int energy, int nlocal,
-    const int4* xq, QScale qs, const int* numneigh, const int* neighbors, int ld,
-    float cutforcesq, const LJTableF& tab, double* fx, double* fy, double* fz, double* epart);
-void launch_eam_fp64(cudaStream_t s, int energy, int nlocal, int ghost_cap, const double4* x,
-    const int* numneigh, const int* neighbors, int ld, double cutforcesq, EamDev eam,
-    const int* border_map, const int* counters, double* fp, double* fx, double* fy,
-    double* fz, double* epart_rho, double* epart_pair);
-void launch_eam_mixed(cudaStream_t s, int energy, int nlocal, int ghost_cap, const int4* xq,
-    QScale qs, const int* numneigh, const int* neighbors, int ld, float cutforcesq,
+    const int* order, const float4* xr, const ShiftTable& sh, const int* numneigh,
+    const int* neighbors, int ld, float cutforcesq, const LJTableF& tab, double* fx,
+    double* fy, double* fz, double* epart);
+void launch_eam_fp64(cudaStream_t s, int energy, int nlocal, int ghost_cap, const int* order,
+    const double4* x, const int* numneigh, const int* neighbors, int ld, double cutforcesq,
     EamDev eam, const int* border_map, const int* counters, double* fp, double* fx,
     double* fy, double* fz, double* epart_rho, double* epart_pair);
+void launch_eam_mixed(cudaStream_t s, int energy, int nlocal, int ghost_cap, const int* order,
+    const float4* xr, const ShiftTable& sh, const int* numneigh, const int* neighbors, int ld,
+    float cutforcesq, EamDev eam, const int* border_map, const int* counters, double* fp,
+    double* fx, double* fy, double* fz, double* epart_rho, double* epart_pair);
 
 extern long long g_launches; // launches issued through these helpers (all contexts)
 

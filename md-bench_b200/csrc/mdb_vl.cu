@@ -9,36 +9,35 @@ namespace mdb {
 
 long long g_launches = 0;
 
-__device__ __forceinline__ int4 quantize(const double4& p, const QScale& qs)
-{
-    int4 q;
-    q.x = (int)(unsigned int)(unsigned long long)__double2ll_rn(p.x * qs.sx);
-    q.y = (int)(unsigned int)(unsigned long long)__double2ll_rn(p.y * qs.sy);
-    q.z = (int)(unsigned int)(unsigned long long)__double2ll_rn(p.z * qs.sz);
-    q.w = type_of(p);
-    return q;
-}
-
 // ---- integrator: verletlist/integrate.c:21-42 -------------------------------
-__global__ void k_initial_integrate(int n, double dtf, double dt, double4* __restrict__ x,
-    double* __restrict__ vx, double* __restrict__ vy, double* __restrict__ vz,
-    const double* __restrict__ fx, const double* __restrict__ fy,
-    const double* __restrict__ fz, int4* __restrict__ xq, QScale qs)
+__device__ __forceinline__ void initial_step(int i, double dtf, double dt, double4* x,
+    double& a, double& b, double& c, const double* fx, const double* fy, const double* fz,
+    float4* xr, const int* qcell, const CellFrame& cf)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double a = vx[i] + dtf * fx[i];
-    double b = vy[i] + dtf * fy[i];
-    double c = vz[i] + dtf * fz[i];
-    vx[i]     = a;
-    vy[i]     = b;
-    vz[i]     = c;
+    a = a + dtf * fx[i];
+    b = b + dtf * fy[i];
+    c = c + dtf * fz[i];
     double4 p = x[i];
     p.x       = p.x + dt * a;
     p.y       = p.y + dt * b;
     p.z       = p.z + dt * c;
     x[i]      = p;
-    if (xq) xq[i] = quantize(p, qs);
+    if (xr) xr[i] = rel_position(p, qcell[i], cf);
+}
+
+__global__ void k_initial_integrate(int n, double dtf, double dt, double4* __restrict__ x,
+    double* __restrict__ vx, double* __restrict__ vy, double* __restrict__ vz,
+    const double* __restrict__ fx, const double* __restrict__ fy,
+    const double* __restrict__ fz, float4* __restrict__ xr, const int* __restrict__ qcell,
+    CellFrame cf)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double a = vx[i], b = vy[i], c = vz[i];
+    initial_step(i, dtf, dt, x, a, b, c, fx, fy, fz, xr, qcell, cf);
+    vx[i] = a;
+    vy[i] = b;
+    vz[i] = c;
 }
 
 __global__ void k_final_integrate(int n, double dtf, double* __restrict__ vx,
@@ -52,13 +51,32 @@ __global__ void k_final_integrate(int n, double dtf, double* __restrict__ vx,
     vz[i] = vz[i] + dtf * fz[i];
 }
 
+// finalIntegrate(n) then initialIntegrate(n+1): two separately rounded
+// velocity updates, exactly as the two reference calls, in one pass
+__global__ void k_final_initial_integrate(int n, double dtf, double dt,
+    double4* __restrict__ x, double* __restrict__ vx, double* __restrict__ vy,
+    double* __restrict__ vz, const double* __restrict__ fx, const double* __restrict__ fy,
+    const double* __restrict__ fz, float4* __restrict__ xr, const int* __restrict__ qcell,
+    CellFrame cf)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double a = vx[i] + dtf * fx[i];
+    double b = vy[i] + dtf * fy[i];
+    double c = vz[i] + dtf * fz[i];
+    initial_step(i, dtf, dt, x, a, b, c, fx, fy, fz, xr, qcell, cf);
+    vx[i] = a;
+    vy[i] = b;
+    vz[i] = c;
+}
+
 void launch_initial_integrate(cudaStream_t s, int n, double dtf, double dt, double4* x,
     double* vx, double* vy, double* vz, const double* fx, const double* fy, const double* fz,
-    int4* xq, QScale qs)
+    float4* xr, const int* qcell, CellFrame cf)
 {
     if (n <= 0) return;
     k_initial_integrate<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(n, dtf, dt, x,
-        vx, vy, vz, fx, fy, fz, xq, qs);
+        vx, vy, vz, fx, fy, fz, xr, qcell, cf);
     g_launches++;
 }
 
@@ -68,6 +86,16 @@ void launch_final_integrate(cudaStream_t s, int n, double dtf, double* vx, doubl
     if (n <= 0) return;
     k_final_integrate<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(n, dtf, vx, vy, vz,
         fx, fy, fz);
+    g_launches++;
+}
+
+void launch_final_initial_integrate(cudaStream_t s, int n, double dtf, double dt, double4* x,
+    double* vx, double* vy, double* vz, const double* fx, const double* fy, const double* fz,
+    float4* xr, const int* qcell, CellFrame cf)
+{
+    if (n <= 0) return;
+    k_final_initial_integrate<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(n, dtf, dt,
+        x, vx, vy, vz, fx, fy, fz, xr, qcell, cf);
     g_launches++;
 }
 
@@ -216,26 +244,24 @@ __device__ __forceinline__ int pack_shift(int sx, int sy, int sz)
     return (sx + 1) | ((sy + 1) << 2) | ((sz + 1) << 4);
 }
 
-__global__ void k_ghost_write(int n, int ghost_cap, double4* __restrict__ x,
-    int4* __restrict__ xq, double c, double xp, double yp, double zp, int px, int py, int pz,
-    const int* __restrict__ off, int* __restrict__ border_map, int* __restrict__ pbc_code)
+__global__ void k_ghost_write(int n, int ghost_cap, double4* __restrict__ x, double c,
+    double xp, double yp, double zp, int px, int py, int pz, const int* __restrict__ off,
+    int* __restrict__ border_map, int* __restrict__ pbc_code)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double4 p = x[i];
     int g     = off[i];
-    int4 q    = xq ? xq[i] : make_int4(0, 0, 0, 0);
     for_each_image(p.x, p.y, p.z, c, xp, yp, zp, px, py, pz, [&](int sx, int sy, int sz) {
         if (g < ghost_cap) {
             border_map[g] = i;
             pbc_code[g]   = pack_shift(sx, sy, sz);
             double4 gp;
-            gp.x         = p.x + sx * xp;
-            gp.y         = p.y + sy * yp;
-            gp.z         = p.z + sz * zp;
-            gp.w         = p.w;
-            x[n + g]     = gp;
-            if (xq) xq[n + g] = q;
+            gp.x     = p.x + sx * xp;
+            gp.y     = p.y + sy * yp;
+            gp.z     = p.z + sz * zp;
+            gp.w     = p.w;
+            x[n + g] = gp;
         }
         g++;
     });
@@ -258,22 +284,23 @@ void launch_ghost_count(cudaStream_t s, int n, const double4* x, double cut, dou
     g_launches++;
 }
 
-void launch_ghost_write(cudaStream_t s, int n, int ghost_cap, double4* x, int4* xq,
-    double cut, double xprd, double yprd, double zprd, int px, int py, int pz, const int* off,
+void launch_ghost_write(cudaStream_t s, int n, int ghost_cap, double4* x, double cut,
+    double xprd, double yprd, double zprd, int px, int py, int pz, const int* off,
     int* border_map, int* pbc_code, int* counters)
 {
     k_ghost_finalize<<<1, 1, 0, s>>>(n, ghost_cap, off, counters);
     g_launches++;
     if (n <= 0) return;
-    k_ghost_write<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(n, ghost_cap, x, xq,
-        cut, xprd, yprd, zprd, px, py, pz, off, border_map, pbc_code);
+    k_ghost_write<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(n, ghost_cap, x, cut,
+        xprd, yprd, zprd, px, py, pz, off, border_map, pbc_code);
     g_launches++;
 }
 
 // ---- ghost update: updatePbcCPU, verletlist/pbc.c:42-58 ----------------------
-__global__ void k_ghost_update(int nlocal, int ghost_cap, double4* __restrict__ x,
+__global__ void k_ghost_update(int nlocal, double4* __restrict__ x,
     const int* __restrict__ border_map, const int* __restrict__ pbc_code, double xp,
-    double yp, double zp, const int* __restrict__ counters)
+    double yp, double zp, const int* __restrict__ counters, float4* __restrict__ xr,
+    const int* __restrict__ qcell, CellFrame cf)
 {
     int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= counters[CNT_NGHOST]) return;
@@ -282,52 +309,45 @@ __global__ void k_ghost_update(int nlocal, int ghost_cap, double4* __restrict__ 
     int sx    = (code & 3) - 1, sy = ((code >> 2) & 3) - 1, sz = ((code >> 4) & 3) - 1;
     double4 p = x[b];
     double4 q;
-    q.x           = p.x + sx * xp;
-    q.y           = p.y + sy * yp;
-    q.z           = p.z + sz * zp;
-    q.w           = p.w;
-    x[nlocal + g] = q;
-}
-
-__global__ void k_ghost_update_q(int nlocal, int4* __restrict__ xq,
-    const int* __restrict__ border_map, const int* __restrict__ counters)
-{
-    int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= counters[CNT_NGHOST]) return;
-    xq[nlocal + g] = xq[border_map[g]];
+    q.x = p.x + sx * xp;
+    q.y = p.y + sy * yp;
+    q.z = p.z + sz * zp;
+    q.w = p.w;
+    if (xr) xr[nlocal + g] = rel_position(q, qcell[nlocal + g], cf);
+    else x[nlocal + g] = q;
 }
 
 void launch_ghost_update(cudaStream_t s, int nlocal, int ghost_cap, double4* x,
     const int* border_map, const int* pbc_code, double xprd, double yprd, double zprd,
-    const int* counters)
+    const int* counters, float4* xr, const int* qcell, CellFrame cf)
 {
     if (ghost_cap <= 0) return;
-    k_ghost_update<<<mdb_blocks(ghost_cap, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(nlocal,
-        ghost_cap, x, border_map, pbc_code, xprd, yprd, zprd, counters);
+    k_ghost_update<<<mdb_blocks(ghost_cap, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(nlocal, x,
+        border_map, pbc_code, xprd, yprd, zprd, counters, xr, qcell, cf);
     g_launches++;
 }
 
-void launch_ghost_update_q(cudaStream_t s, int nlocal, int ghost_cap, int4* xq,
-    const int* border_map, const int* counters)
-{
-    if (ghost_cap <= 0) return;
-    k_ghost_update_q<<<mdb_blocks(ghost_cap, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(nlocal, xq,
-        border_map, counters);
-    g_launches++;
-}
-
-__global__ void k_quantize(int n, const double4* __restrict__ x, int4* __restrict__ xq,
-    QScale qs)
+// ---- mixed-path cells: qcell = floor(x / G) per axis, xr relative to its centre
+__global__ void k_cells(int nlocal, const double4* __restrict__ x, float4* __restrict__ xr,
+    int* __restrict__ qcell, CellFrame cf, const int* __restrict__ counters, int locals_only)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = locals_only ? nlocal : nlocal + counters[CNT_NGHOST];
     if (i >= n) return;
-    xq[i] = quantize(x[i], qs);
+    double4 p = x[i];
+    int q     = pack_cell((int)floor(p.x * cf.ginv), (int)floor(p.y * cf.ginv),
+            (int)floor(p.z * cf.ginv));
+    qcell[i]  = q;
+    xr[i]     = rel_position(p, q, cf);
 }
 
-void launch_quantize(cudaStream_t s, int n, const double4* x, int4* xq, QScale qs)
+void launch_cells(cudaStream_t s, int nlocal, int nall_cap, const double4* x, float4* xr,
+    int* qcell, CellFrame cf, const int* counters, int locals_only)
 {
+    int n = locals_only ? nlocal : nall_cap;
     if (n <= 0) return;
-    k_quantize<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(n, x, xq, qs);
+    k_cells<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(nlocal, x, xr, qcell, cf,
+        counters, locals_only);
     g_launches++;
 }
 
@@ -342,9 +362,10 @@ __device__ __forceinline__ int coord2bin(const double4& p, const BinGeom& g)
     return iz * g.mbiny * g.mbinx + iy * g.mbinx + ix;
 }
 
-__global__ void k_bin_count(int nlocal, int nall_cap, const double4* __restrict__ x,
-    BinGeom g, int* __restrict__ atom_bin, int* __restrict__ atom_slot,
-    int* __restrict__ bin_count, int* __restrict__ counters)
+// bin_count[b]: atoms in bin b; bin_lcount[b]: local atoms in bin b
+__global__ void k_bin_count(int nlocal, const double4* __restrict__ x, BinGeom g,
+    int* __restrict__ atom_bin, int* __restrict__ atom_slot, int* __restrict__ bin_count,
+    int* __restrict__ bin_lcount, int* __restrict__ counters)
 {
     int i    = blockIdx.x * blockDim.x + threadIdx.x;
     int nall = nlocal + counters[CNT_NGHOST];
@@ -357,6 +378,7 @@ __global__ void k_bin_count(int nlocal, int nall_cap, const double4* __restrict_
     }
     atom_bin[i]  = b;
     atom_slot[i] = atomicAdd(&bin_count[b], 1);
+    if (i < nlocal) atomicAdd(&bin_lcount[b], 1);
 }
 
 __global__ void k_bin_scatter(int nlocal, const int* __restrict__ atom_bin,
@@ -372,8 +394,13 @@ __global__ void k_bin_scatter(int nlocal, const int* __restrict__ atom_bin,
 }
 
 // Atoms of a bin in ascending index order: the order binatoms produces when it
-// fills bins in one serial pass (verletlist/neighbor.c:443-454).
-__global__ void k_bin_sort(int mbins, const int* __restrict__ bin_start, int* __restrict__ bin_atoms)
+// fills bins in one serial pass (verletlist/neighbor.c:443-454). Locals have
+// the smaller indices, so they form the head of each sorted bin; the heads of
+// all bins, concatenated in bin order, give local_order (the row order of the
+// neighbour list: atoms of one bin are adjacent rows).
+__global__ void k_bin_sort(int mbins, const int* __restrict__ bin_start,
+    int* __restrict__ bin_atoms, const int* __restrict__ loc_start,
+    int* __restrict__ local_order)
 {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= mbins) return;
@@ -387,13 +414,16 @@ __global__ void k_bin_sort(int mbins, const int* __restrict__ bin_start, int* __
         }
         bin_atoms[m + 1] = v;
     }
+    int o = loc_start[b], nl = loc_start[b + 1] - o;
+    for (int k = 0; k < nl; k++)
+        local_order[o + k] = bin_atoms[s + k];
 }
 
 void launch_bin_count(cudaStream_t s, int nlocal, int nall_cap, const double4* x, BinGeom g,
-    int* atom_bin, int* atom_slot, int* bin_count, int* counters)
+    int* atom_bin, int* atom_slot, int* bin_count, int* bin_lcount, int* counters)
 {
-    k_bin_count<<<mdb_blocks(nall_cap, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(nlocal, nall_cap,
-        x, g, atom_bin, atom_slot, bin_count, counters);
+    k_bin_count<<<mdb_blocks(nall_cap, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(nlocal, x, g,
+        atom_bin, atom_slot, bin_count, bin_lcount, counters);
     g_launches++;
 }
 
@@ -405,36 +435,64 @@ void launch_bin_scatter(cudaStream_t s, int nlocal, int nall_cap, const int* ato
     g_launches++;
 }
 
-void launch_bin_sort(cudaStream_t s, int mbins, const int* bin_start, int* bin_atoms)
+void launch_bin_sort(cudaStream_t s, int mbins, const int* bin_start, int* bin_atoms,
+    const int* loc_start, int* local_order)
 {
     k_bin_sort<<<mdb_blocks(mbins, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(mbins, bin_start,
-        bin_atoms);
+        bin_atoms, loc_start, local_order);
     g_launches++;
 }
 
 // ---- list build: buildNeighborCPU, verletlist/neighbor.c:260-352 -------------
-// One thread per local atom walks the stencil in the reference order and the
-// atoms of each bin in index order, so row i holds exactly the reference's
-// neighbours in the reference's order. Rows are stored k-major (SoA).
+// Thread t builds the row of atom i = local_order[t] (atoms of one bin are
+// adjacent threads, so a warp walks nearly the same stencil bins and the
+// row writes are coalesced: rows are stored k-major and indexed by t). The
+// stencil is walked in the reference order and each bin's atoms in index
+// order, so row t holds exactly the reference's neighbours of i in the
+// reference's order. A stencil bin is skipped when its box lies farther than
+// cutneigh from the atom (a lower bound on every distance to its atoms, with
+// a relative margin): this only removes candidates that would fail the test.
+// On the mixed path each entry also carries the offset between the cells of
+// i and j (code in bits 25-31).
 __global__ void __launch_bounds__(128) k_build_list(int nlocal, const double4* __restrict__ x,
-    BinGeom g, const int* __restrict__ stencil, const int* __restrict__ atom_bin,
-    const int* __restrict__ bin_start, const int* __restrict__ bin_atoms, double cutneighsq,
-    int half, int maxneighs, int ld, int* __restrict__ neighbors, int* __restrict__ numneigh,
-    int* __restrict__ counters)
+    BinGeom g, const int4* __restrict__ stencil, const int* __restrict__ local_order,
+    const int* __restrict__ atom_bin, const int* __restrict__ bin_start,
+    const int* __restrict__ bin_atoms, double cutneighsq, int half, int maxneighs, int ld,
+    int* __restrict__ neighbors, int* __restrict__ numneigh, int* __restrict__ counters,
+    const int* __restrict__ qcell)
 {
-    __shared__ int st[MDB_MAX_STENCIL];
+    __shared__ int4 st[MDB_MAX_STENCIL];
     for (int k = threadIdx.x; k < g.nstencil; k += blockDim.x)
         st[k] = stencil[k];
     __syncthreads();
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nlocal) return;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nlocal) return;
+    const int i      = local_order[t];
     const double4 xi = x[i];
     const int ibin   = atom_bin[i];
-    int n            = 0;
+    const int qi     = qcell ? qcell[i] : 0;
+    // position inside the home bin, in bin units: f in [0, 1)
+    const double ux  = (xi.x + g.xlo) * g.bininvx;
+    const double uy  = (xi.y + g.ylo) * g.bininvy;
+    const double uz  = (xi.z + g.zlo) * g.bininvz;
+    const float fx   = (float)(ux - (double)(int)ux);
+    const float fy   = (float)(uy - (double)(int)uy);
+    const float fz   = (float)(uz - (double)(int)uz);
+    const float bx = (float)g.binsizex, by = (float)g.binsizey, bz = (float)g.binsizez;
+    const float skip2 = (float)cutneighsq * 1.0001f + 1e-4f;
+    int n = 0, bad = 0;
     if (ibin >= 0) {
         for (int k = 0; k < g.nstencil; k++) {
-            int jbin = ibin + st[k];
+            const int4 sk = st[k];
+            int jbin      = ibin + sk.x;
             if (jbin < 0 || jbin >= g.mbins) continue;
+            float gx = sk.y > 0 ? (sk.y - fx) : (sk.y < 0 ? (fx - (sk.y + 1)) : 0.f);
+            float gy = sk.z > 0 ? (sk.z - fy) : (sk.z < 0 ? (fy - (sk.z + 1)) : 0.f);
+            float gz = sk.w > 0 ? (sk.w - fz) : (sk.w < 0 ? (fz - (sk.w + 1)) : 0.f);
+            gx *= bx;
+            gy *= by;
+            gz *= bz;
+            if (gx * gx + gy * gy + gz * gz > skip2) continue;
             int beg = __ldg(&bin_start[jbin]);
             int end = __ldg(&bin_start[jbin + 1]);
             for (int m = beg; m < end; m++) {
@@ -447,7 +505,17 @@ __global__ void __launch_bounds__(128) k_build_list(int nlocal, const double4* _
                 double delz = xi.z - xj.z;
                 double rsq  = delx * delx + dely * dely + delz * delz;
                 if (rsq <= cutneighsq) {
-                    if (n < maxneighs) neighbors[(size_t)n * ld + i] = j;
+                    int e = j;
+                    if (qcell) {
+                        int qj = __ldg(&qcell[j]);
+                        int cx = cell_axis(qj, 0) - cell_axis(qi, 0);
+                        int cy = cell_axis(qj, 1) - cell_axis(qi, 1);
+                        int cz = cell_axis(qj, 2) - cell_axis(qi, 2);
+                        if (cx < -2 || cx > 2 || cy < -2 || cy > 2 || cz < -2 || cz > 2) bad = 1;
+                        int code = (cx + 2) + 5 * (cy + 2) + 25 * (cz + 2);
+                        e        = j | ((code & 127) << MDB_IDX_BITS);
+                    }
+                    if (n < maxneighs) neighbors[(size_t)n * ld + t] = e;
                     n++;
                 }
             }
@@ -456,23 +524,25 @@ __global__ void __launch_bounds__(128) k_build_list(int nlocal, const double4* _
     // the stored count never exceeds the row capacity, so no consumer can read
     // past the list; the true count of an overflowing row goes to the host,
     // which grows the list and rebuilds before any force is computed
-    numneigh[i] = n < maxneighs ? n : maxneighs;
+    numneigh[t] = n < maxneighs ? n : maxneighs;
     if (n > maxneighs) atomicMax(&counters[CNT_MAXNEED], n);
+    if (bad) atomicAdd(&counters[CNT_BADCELL], 1);
 }
 
 void launch_build_list(cudaStream_t s, int nlocal, const double4* x, BinGeom g,
-    const int* stencil, const int* atom_bin, const int* bin_start, const int* bin_atoms,
-    double cutneighsq, int half, int maxneighs, int ld, int* neighbors, int* numneigh,
-    int* counters)
+    const int4* stencil, const int* local_order, const int* atom_bin, const int* bin_start,
+    const int* bin_atoms, double cutneighsq, int half, int maxneighs, int ld, int* neighbors,
+    int* numneigh, int* counters, const int* qcell)
 {
     if (nlocal <= 0) return;
-    k_build_list<<<mdb_blocks(nlocal, 128), 128, 0, s>>>(nlocal, x, g, stencil, atom_bin,
-        bin_start, bin_atoms, cutneighsq, half, maxneighs, ld, neighbors, numneigh, counters);
+    k_build_list<<<mdb_blocks(nlocal, 128), 128, 0, s>>>(nlocal, x, g, stencil, local_order,
+        atom_bin, bin_start, bin_atoms, cutneighsq, half, maxneighs, ld, neighbors, numneigh,
+        counters, qcell);
     g_launches++;
 }
 
-// ---- thermo: sum of v.v per block, then one fixed-order reduction ------------
-static constexpr int KE_THREADS = 256;
+// ---- thermo: sum of m v.v per block, then one fixed-order reduction ----------
+static constexpr int KE_THREADS    = 256;
 static constexpr int KE_MAX_BLOCKS = 1184; // 8 x 148 SMs
 
 int ke_partial_blocks(int n)

@@ -85,9 +85,10 @@ def test_bin_geometry_and_ghosts(cells):
     assert np.array_equal(s.positions_all(), o.positions_all())
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 @pytest.mark.parametrize("half", [0, 1])
-def test_lists_bit_exact_in_reference_order(half):
-    s, _ = lj_system(nx=8, ny=7, nz=9, half_neigh=half)
+def test_lists_bit_exact_in_reference_order(half, precision):
+    s, _ = lj_system(precision=precision, nx=8, ny=7, nz=9, half_neigh=half)
     o = lj_oracle(nx=8, ny=7, nz=9, half_neigh=half)
     ns, ls = s.neighbor_list()
     no, lo = o.neighbor_list()
@@ -192,13 +193,21 @@ def test_list_capacity_grows_on_overflow():
 
 
 def test_small_box_and_multiple_images():
-    """Box shorter than twice the cutoff: the FP64 path keeps every image like
-    the reference; the mixed path refuses it (minimum image would be wrong)."""
+    """Box shorter than twice the cutoff: an atom meets several images of the
+    same neighbour. Both paths keep every image like the reference (ghosts
+    carry their own positions)."""
     s, _ = lj_system(nx=3, ny=3, nz=3)
     o = lj_oracle(nx=3, ny=3, nz=3)
     assert np.array_equal(s.atoms()[2], o.atoms()[2])
-    with pytest.raises(mdb.MdbError):
-        lj_system(precision="mixed", nx=3, ny=3, nz=3)
+    o.run(60)
+    x, v, _, t = o.atoms()
+    o.set_state(x, v)
+    o.setup()
+    o.force()
+    m, _ = lj_system(precision="mixed", nx=3, ny=3, nz=3)
+    m.set_atoms(x, v, t)
+    m.setup()
+    assert rel_err(m.atoms()[2], o.atoms()[2])[1] <= MIXED_RMS
 
 
 def test_eam_fp64_bit_exact_against_reference_fixture():
