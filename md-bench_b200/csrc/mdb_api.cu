@@ -39,7 +39,7 @@ struct MdbCtx {
     LJTable tab;
     LJTableF tabf;
     CellFrame cf;
-    ShiftTable shift;
+    CellShift shift;
     double cutforcesq = 0, cutneighsq = 0;
     double mvv2e = 1, dof_boltz = 1, t_scale = 1, p_scale = 1;
 
@@ -326,17 +326,14 @@ extern "C" int mdb_create(const MdbParams* params, MdbCtx** out)
     ctx->cutforcesq = p.cutforce * p.cutforce;
     ctx->cutneighsq = p.cutneigh * p.cutneigh;
     {
-        // mixed-path cells: the smallest power of two G with 2 G >= cutneigh, so
-        // any listed pair lies within two cells per axis (code range -2..2)
+        // mixed-path cells: the smallest power of two G >= cutneigh, so the
+        // cells of any listed pair differ by at most one per axis
         double g = 1.0 / 1024;
-        while (2 * g < p.cutneigh)
+        while (g < p.cutneigh)
             g *= 2;
         ctx->cf.g    = g;
         ctx->cf.ginv = 1.0 / g;
-        for (int c = 0; c < MDB_NCODES; c++) {
-            int dx = c % 5 - 2, dy = (c / 5) % 5 - 2, dz = c / 25 - 2;
-            ctx->shift.s[c] = make_float4((float)(dx * g), (float)(dy * g), (float)(dz * g), 0.f);
-        }
+        ctx->shift.g = (float)g;
         double lmax = std::max(p.xprd, std::max(p.yprd, p.zprd)) + 2 * p.cutneigh;
         if (ctx->mixed && lmax * ctx->cf.ginv > 1000) {
             rc = fail(ctx, MDB_ERR_ARG, "box too large for the mixed path's cell index");
@@ -642,12 +639,12 @@ static void enq_force(MdbCtx* ctx, bool energy)
     double* ep1    = ctx->partials + ctx->npart;
     if (ctx->p.force_field == MDB_FF_EAM) {
         if (ctx->mixed)
-            launch_eam_mixed(s, energy, n, ctx->ghost_cap, ctx->local_order, ctx->xr,
+            launch_eam_mixed(s, energy, n, ctx->ghost_cap, nullptr,ctx->xr,
                 ctx->shift, ctx->numneigh, ctx->neighbors, ctx->ld, (float)ctx->cutforcesq,
                 ctx->eam, ctx->border_map, ctx->counters, ctx->fp, ctx->fx, ctx->fy, ctx->fz,
                 ep0, ep1);
         else
-            launch_eam_fp64(s, energy, n, ctx->ghost_cap, ctx->local_order, ctx->x,
+            launch_eam_fp64(s, energy, n, ctx->ghost_cap, nullptr,ctx->x,
                 ctx->numneigh, ctx->neighbors, ctx->ld, ctx->cutforcesq, ctx->eam,
                 ctx->border_map, ctx->counters, ctx->fp, ctx->fx, ctx->fy, ctx->fz, ep0, ep1);
         return;
@@ -659,10 +656,10 @@ static void enq_force(MdbCtx* ctx, bool energy)
     }
     if (ctx->mixed)
         launch_lj_mixed(s, ctx->p.precision == MDB_PREC_MIXED_COMP, ctx->p.half_neigh, energy, n,
-            ctx->local_order, ctx->xr, ctx->shift, ctx->numneigh, ctx->neighbors, ctx->ld,
+            nullptr, ctx->xr, ctx->shift, ctx->numneigh, ctx->neighbors, ctx->ld,
             (float)ctx->cutforcesq, ctx->tabf, ctx->fx, ctx->fy, ctx->fz, ep0);
     else
-        launch_lj_fp64(s, ctx->p.half_neigh, energy, n, ctx->local_order, ctx->x, ctx->numneigh,
+        launch_lj_fp64(s, ctx->p.half_neigh, energy, n, nullptr, ctx->x, ctx->numneigh,
             ctx->neighbors, ctx->ld, ctx->cutforcesq, ctx->tab, ctx->fx, ctx->fy, ctx->fz, ep0);
 }
 
@@ -690,6 +687,7 @@ static void enq_list(MdbCtx* ctx)
     cudaStream_t s = ctx->s;
     cudaMemsetAsync(ctx->bin_count, 0, sizeof(int) * ctx->g.mbins, s);
     cudaMemsetAsync(ctx->bin_lcount, 0, sizeof(int) * ctx->g.mbins, s);
+    cudaMemsetAsync(ctx->local_order, 0xff, sizeof(int) * std::max(ctx->nlocal, 1), s);
     launch_bin_count(s, ctx->nlocal, ctx->nall_cap, ctx->x, ctx->g, ctx->atom_bin,
         ctx->atom_slot, ctx->bin_count, ctx->bin_lcount, ctx->counters);
     scan_exclusive(ctx->bin_count, ctx->bin_start, ctx->g.mbins, ctx->scan_scratch, s);
@@ -1164,13 +1162,14 @@ extern "C" int mdb_get_neighbor_list(MdbCtx* ctx, int* numneigh, int* neighbors,
 {
     NEED_ATOMS();
     if (!ctx->have_list) return fail(ctx, MDB_ERR_STATE, "no neighbour list");
-    // rows are stored per list row t; atom local_order[t] owns row t. Mixed-path
+    // row i (column i of the k-major list) belongs to atom i. Mixed-path
     // entries carry a cell-offset code above the index bits, masked off here.
     int n = ctx->nlocal;
     std::vector<int> nn(n), order(n);
     CK(cudaStreamSynchronize(ctx->s));
     CK(cudaMemcpy(nn.data(), ctx->numneigh, sizeof(int) * n, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(order.data(), ctx->local_order, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    for (int t = 0; t < n; t++)
+        order[t] = t;
     if (numneigh)
         for (int t = 0; t < n; t++)
             numneigh[order[t]] = nn[t];

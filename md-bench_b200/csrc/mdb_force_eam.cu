@@ -3,7 +3,7 @@
 // (2) fp copied to the ghosts through the ghost map (the mid-step halo),
 // (3) pair forces from rho', phi' and fp_i + fp_j.
 //
-// Thread t handles atom order[t]. Spline tables are re-laid out as rows of 8
+// Thread t handles atom t (or order[t]). Spline tables are re-laid out as rows of 8
 // coefficients (one 64-byte row per grid point instead of 56 bytes) so a row
 // is two aligned sectors.
 // FP64 path: -fmad=false, bit-identical to the reference's strict build.
@@ -26,7 +26,7 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_fp64(int nlocal,
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double eng  = 0.0;
     if (t < nlocal) {
-        const int i      = order[t];
+        const int i      = order ? order[t] : t;
         const double4 xi = x[i];
         const int n      = numneigh[t];
         const int* nb    = neighbors + t;
@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_fp64(int nlocal,
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double eng  = 0.0;
     if (t < nlocal) {
-        const int i      = order[t];
+        const int i      = order ? order[t] : t;
         const double4 xi = x[i];
         const int n      = numneigh[t];
         const int* nb    = neighbors + t;
@@ -162,28 +162,23 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_fp64(int nlocal,
 // ---- mixed ------------------------------------------------------------------
 template <bool ENERGY>
 __global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_mixed(int nlocal,
-    const int* __restrict__ order, const float4* __restrict__ xr, ShiftTable sh,
+    const int* __restrict__ order, const float4* __restrict__ xr, CellShift sh,
     const int* __restrict__ numneigh, const int* __restrict__ neighbors, int ld,
     float cutforcesq, EamDev e, double* __restrict__ fp, double* __restrict__ epart)
 {
-    __shared__ float4 s_shift[MDB_NCODES];
-    for (int k = threadIdx.x; k < MDB_NCODES; k += blockDim.x)
-        s_shift[k] = sh.s[k];
-    __syncthreads();
+    const float cg = sh.g;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double eng  = 0.0;
     if (t < nlocal) {
-        const int i     = order[t];
+        const int i     = order ? order[t] : t;
         const float4 pi = xr[i];
         const int n     = numneigh[t];
         const int* nb   = neighbors + t;
         const float rdr = (float)e.rdr;
         double rhoi     = 0.0; // FP64 embedding (density) sum
         auto pair       = [&](int en, const float4& pj) {
-            const float4 off = s_shift[(unsigned)en >> MDB_IDX_BITS];
-            float dx         = (pi.x - pj.x) - off.x;
-            float dy         = (pi.y - pj.y) - off.y;
-            float dz         = (pi.z - pj.z) - off.z;
+            float dx, dy, dz;
+            cell_delta(pi, pj, (unsigned)en >> MDB_IDX_BITS, cg, dx, dy, dz);
             float rsq        = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
             if (rsq < cutforcesq) {
                 float p = __fmaf_rn(sqrtf(rsq), rdr, 1.0f);
@@ -233,19 +228,16 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_mixed(int nlocal,
 
 template <bool ENERGY>
 __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_mixed(int nlocal,
-    const int* __restrict__ order, const float4* __restrict__ xr, ShiftTable sh,
+    const int* __restrict__ order, const float4* __restrict__ xr, CellShift sh,
     const int* __restrict__ numneigh, const int* __restrict__ neighbors, int ld,
     float cutforcesq, EamDev e, const double* __restrict__ fp, double* __restrict__ fx,
     double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ epart)
 {
-    __shared__ float4 s_shift[MDB_NCODES];
-    for (int k = threadIdx.x; k < MDB_NCODES; k += blockDim.x)
-        s_shift[k] = sh.s[k];
-    __syncthreads();
+    const float cg = sh.g;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double eng  = 0.0;
     if (t < nlocal) {
-        const int i     = order[t];
+        const int i     = order ? order[t] : t;
         const float4 pi = xr[i];
         const int n     = numneigh[t];
         const int* nb   = neighbors + t;
@@ -254,10 +246,8 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_mixed(int nlocal,
         float fix = 0.f, fiy = 0.f, fiz = 0.f;
         auto pair = [&](int en, const float4& pj) {
             const int j      = en & MDB_IDX_MASK;
-            const float4 off = s_shift[(unsigned)en >> MDB_IDX_BITS];
-            float dx         = (pi.x - pj.x) - off.x;
-            float dy         = (pi.y - pj.y) - off.y;
-            float dz         = (pi.z - pj.z) - off.z;
+            float dx, dy, dz;
+            cell_delta(pi, pj, (unsigned)en >> MDB_IDX_BITS, cg, dx, dy, dz);
             float rsq        = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
             if (rsq < cutforcesq) {
                 float r = sqrtf(rsq);
@@ -346,7 +336,7 @@ void launch_eam_fp64(cudaStream_t s, int energy, int nlocal, int ghost_cap, cons
 }
 
 void launch_eam_mixed(cudaStream_t s, int energy, int nlocal, int ghost_cap, const int* order,
-    const float4* xr, const ShiftTable& sh, const int* numneigh, const int* neighbors, int ld,
+    const float4* xr, const CellShift& sh, const int* numneigh, const int* neighbors, int ld,
     float cutforcesq, EamDev eam, const int* border_map, const int* counters, double* fp,
     double* fx, double* fy, double* fz, double* epart_rho, double* epart_pair)
 {

@@ -1,8 +1,8 @@
 // Lennard-Jones forces over Verlet lists (computeForceLJFullNeigh /
 // computeForceLJHalfNeigh, verletlist/force_lj.c:17-206).
 //
-// Thread t handles atom i = order[t] (rows of one bin are adjacent threads).
-// The list is k-major, so each step of the k loop is one 128-byte coalesced
+// Thread t handles atom i = t (or order[t] when an order is given) and reads
+// row t of the list. The list is k-major, so each step of the k loop is one 128-byte coalesced
 // read per warp; neighbour positions are 32-byte (FP64) or 16-byte (mixed)
 // gathers that mostly hit L1/L2. The k loop is unrolled by UNROLL with all
 // list reads and gathers of a batch issued before any arithmetic, which keeps
@@ -12,11 +12,11 @@
 // FP64 path: -fmad=false keeps every product and sum rounded as the
 // reference's strict build rounds them, so full-list forces are bit-identical.
 // Mixed path: FP32 positions relative to the centre of each atom's cell (edge
-// G, a power of two) plus the cell offset of the pair, taken from the list
-// entry's code and a table of exact offsets in shared memory:
-// dx = (p_i - p_j) - shift[code]. No integer->float conversions and one
-// approximate reciprocal per pair; FP32 force sums (or two-sum compensated
-// sums), FP64 energy sums.
+// G, a power of two) plus the cell offset of the pair (-1, 0, +1 per axis,
+// 2-bit fields of the list entry): dx = (p_i - p_j) - offset * G, the offset
+// decoded into an exact float with integer bit operations. No int->float
+// conversions, no shared-memory table, one approximate reciprocal per pair;
+// FP32 force sums (or two-sum compensated sums), FP64 energy sums.
 #include "mdb_internal.cuh"
 
 namespace mdb {
@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(LJ_THREADS) k_lj_fp64(int nlocal,
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double epot = 0.0;
     if (t < nlocal) {
-        const int i      = order[t];
+        const int i      = order ? order[t] : t;
         const double4 xi = x[i];
         const int ti     = type_of(xi);
         const int n      = numneigh[t];
@@ -120,28 +120,26 @@ __global__ void __launch_bounds__(LJ_THREADS) k_lj_fp64(int nlocal,
 
 template <bool HALF, bool UNIFORM, bool ENERGY, bool COMP>
 __global__ void __launch_bounds__(LJ_THREADS) k_lj_mixed(int nlocal,
-    const int* __restrict__ order, const float4* __restrict__ xr, ShiftTable sh,
+    const int* __restrict__ order, const float4* __restrict__ xr, CellShift sh,
     const int* __restrict__ numneigh, const int* __restrict__ neighbors, int ld,
     float cutforcesq, LJTableF tab, double* __restrict__ fx, double* __restrict__ fy,
     double* __restrict__ fz, double* __restrict__ epart)
 {
-    __shared__ float4 s_shift[MDB_NCODES];
     __shared__ float s_eps[MDB_MAX_TYPES * MDB_MAX_TYPES];
     __shared__ float s_sig6[MDB_MAX_TYPES * MDB_MAX_TYPES];
     const int nt = tab.ntypes;
-    for (int k = threadIdx.x; k < MDB_NCODES; k += blockDim.x)
-        s_shift[k] = sh.s[k];
     if (!UNIFORM) {
         for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) {
             s_eps[k]  = tab.eps[k];
             s_sig6[k] = tab.sig6[k];
         }
+        __syncthreads();
     }
-    __syncthreads();
+    const float cg = sh.g;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double epot = 0.0;
     if (t < nlocal) {
-        const int i     = order[t];
+        const int i     = order ? order[t] : t;
         const float4 pi = xr[i];
         const int ti    = __float_as_int(pi.w);
         const int n     = numneigh[t];
@@ -164,12 +162,10 @@ __global__ void __launch_bounds__(LJ_THREADS) k_lj_mixed(int nlocal,
         };
 
         auto pair = [&](int e, const float4& pj) {
-            const int j      = e & MDB_IDX_MASK;
-            const float4 off = s_shift[(unsigned)e >> MDB_IDX_BITS];
-            float delx       = (pi.x - pj.x) - off.x;
-            float dely       = (pi.y - pj.y) - off.y;
-            float delz       = (pi.z - pj.z) - off.z;
-            float rsq        = __fmaf_rn(delx, delx, __fmaf_rn(dely, dely, delz * delz));
+            const int j = e & MDB_IDX_MASK;
+            float delx, dely, delz;
+            cell_delta(pi, pj, (unsigned)e >> MDB_IDX_BITS, cg, delx, dely, delz);
+            float rsq = __fmaf_rn(delx, delx, __fmaf_rn(dely, dely, delz * delz));
             float sigma6 = sig0, epsilon = eps0;
             if (!UNIFORM) {
                 int tij = ti * nt + __float_as_int(pj.w);
@@ -271,7 +267,7 @@ void launch_lj_fp64(cudaStream_t s, int half, int energy, int nlocal, const int*
 
 template <bool HALF, bool UNIFORM, bool COMP>
 static void ljmx(cudaStream_t s, int energy, int nb, int nlocal, const int* order,
-    const float4* xr, const ShiftTable& sh, const int* numneigh, const int* neighbors, int ld,
+    const float4* xr, const CellShift& sh, const int* numneigh, const int* neighbors, int ld,
     float cut, const LJTableF& tab, double* fx, double* fy, double* fz, double* epart)
 {
     if (energy)
@@ -284,7 +280,7 @@ static void ljmx(cudaStream_t s, int energy, int nb, int nlocal, const int* orde
 
 template <bool HALF, bool COMP>
 static void ljmx_u(cudaStream_t s, int energy, int nb, int nlocal, const int* order,
-    const float4* xr, const ShiftTable& sh, const int* numneigh, const int* neighbors, int ld,
+    const float4* xr, const CellShift& sh, const int* numneigh, const int* neighbors, int ld,
     float cut, const LJTableF& tab, double* fx, double* fy, double* fz, double* epart)
 {
     if (tab.uniform)
@@ -296,7 +292,7 @@ static void ljmx_u(cudaStream_t s, int energy, int nb, int nlocal, const int* or
 }
 
 void launch_lj_mixed(cudaStream_t s, int comp, int half, int energy, int nlocal,
-    const int* order, const float4* xr, const ShiftTable& sh, const int* numneigh,
+    const int* order, const float4* xr, const CellShift& sh, const int* numneigh,
     const int* neighbors, int ld, float cutforcesq, const LJTableF& tab, double* fx,
     double* fy, double* fz, double* epart)
 {

@@ -22,9 +22,8 @@
 
 #define MDB_MAX_TYPES   8
 #define MDB_MAX_STENCIL 1331 /* (2*5+1)^3 */
-#define MDB_IDX_BITS    25   /* mixed-path list entries: index bits */
+#define MDB_IDX_BITS    26   /* mixed-path list entries: index bits (6 code bits above) */
 #define MDB_IDX_MASK    ((1 << MDB_IDX_BITS) - 1)
-#define MDB_NCODES      125  /* cell offsets -2..2 per axis */
 
 // device counters (int slots)
 enum {
@@ -60,16 +59,36 @@ struct LJTableF {
     float sig6[MDB_MAX_TYPES * MDB_MAX_TYPES];
 };
 
-// Mixed-path cells: edge G (a power of two, so cell offsets times G are exact
-// in FP32); shift[code] = (dqx, dqy, dqz) * G for code = (dqx+2)+5(dqy+2)+25(dqz+2).
+// Mixed-path cells: edge G, the smallest power of two >= cutneigh, so the
+// cells of a listed pair differ by -1, 0 or +1 per axis and offset * G is
+// exact in FP32. A list entry stores the three offsets + 1 as 2-bit fields
+// above the index bits.
 struct CellFrame {
     double g;
     double ginv;
 };
 
-struct ShiftTable {
-    float4 s[MDB_NCODES];
+struct CellShift {
+    float g;
 };
+
+// cell offset (-1, 0 or +1) of 2-bit field f, as an exact float without an
+// int->float conversion: 0x4B400000 is 1.5 * 2^23, so OR-ing f into the
+// mantissa gives 12582912 + f exactly
+__device__ __forceinline__ float cell_offset(unsigned f)
+{
+    return __int_as_float(0x4B400000 | (int)f) - 12582913.0f;
+}
+
+// pair difference p_i - p_j - offset * G on the mixed path; a fused multiply-add
+// with the exact product offset * G rounds once
+__device__ __forceinline__ void cell_delta(const float4& pi, const float4& pj, unsigned code,
+    float g, float& dx, float& dy, float& dz)
+{
+    dx = __fmaf_rn(-cell_offset(code & 3u), g, pi.x - pj.x);
+    dy = __fmaf_rn(-cell_offset((code >> 2) & 3u), g, pi.y - pj.y);
+    dz = __fmaf_rn(-cell_offset((code >> 4) & 3u), g, pi.z - pj.z);
+}
 
 struct EamDev {
     int nrho, nr;
@@ -191,7 +210,7 @@ void launch_lj_fp64(cudaStream_t s, int half, int energy, int nlocal, const int*
     const double4* x, const int* numneigh, const int* neighbors, int ld, double cutforcesq,
     const LJTable& tab, double* fx, double* fy, double* fz, double* epart);
 void launch_lj_mixed(cudaStream_t s, int comp, int half, int energy, int nlocal,
-    const int* order, const float4* xr, const ShiftTable& sh, const int* numneigh,
+    const int* order, const float4* xr, const CellShift& sh, const int* numneigh,
     const int* neighbors, int ld, float cutforcesq, const LJTableF& tab, double* fx,
     double* fy, double* fz, double* epart);
 void launch_eam_fp64(cudaStream_t s, int energy, int nlocal, int ghost_cap, const int* order,
@@ -199,7 +218,7 @@ void launch_eam_fp64(cudaStream_t s, int energy, int nlocal, int ghost_cap, cons
     EamDev eam, const int* border_map, const int* counters, double* fp, double* fx,
     double* fy, double* fz, double* epart_rho, double* epart_pair);
 void launch_eam_mixed(cudaStream_t s, int energy, int nlocal, int ghost_cap, const int* order,
-    const float4* xr, const ShiftTable& sh, const int* numneigh, const int* neighbors, int ld,
+    const float4* xr, const CellShift& sh, const int* numneigh, const int* neighbors, int ld,
     float cutforcesq, EamDev eam, const int* border_map, const int* counters, double* fp,
     double* fx, double* fy, double* fz, double* epart_rho, double* epart_pair);
 

@@ -444,34 +444,30 @@ void launch_bin_sort(cudaStream_t s, int mbins, const int* bin_start, int* bin_a
 }
 
 // ---- list build: buildNeighborCPU, verletlist/neighbor.c:260-352 -------------
-// Thread t builds the row of atom i = local_order[t] (atoms of one bin are
-// adjacent threads, so a warp walks nearly the same stencil bins and the
-// row writes are coalesced: rows are stored k-major and indexed by t). The
-// stencil is walked in the reference order and each bin's atoms in index
-// order, so row t holds exactly the reference's neighbours of i in the
-// reference's order. A stencil bin is skipped when its box lies farther than
-// cutneigh from the atom (a lower bound on every distance to its atoms, with
-// a relative margin): this only removes candidates that would fail the test.
-// On the mixed path each entry also carries the offset between the cells of
-// i and j (code in bits 25-31).
+// One thread per local atom i (atom order, so the k-major row writes of a warp
+// are coalesced). The stencil is walked in the reference order and each bin's
+// atoms in index order, so row i holds exactly the reference's neighbours of i
+// in the reference's order. A stencil bin is skipped when its box lies farther
+// than cutneigh from the atom (a lower bound on every distance to its atoms,
+// with a relative margin: skipping only removes candidates that would fail the
+// test). The candidate loop handles two candidates per iteration so their
+// loads overlap. On the mixed path each entry also carries the cell offset of
+// the pair (2 bits per axis, bits 26-31).
 __global__ void __launch_bounds__(128) k_build_list(int nlocal, const double4* __restrict__ x,
-    BinGeom g, const int4* __restrict__ stencil, const int* __restrict__ local_order,
-    const int* __restrict__ atom_bin, const int* __restrict__ bin_start,
-    const int* __restrict__ bin_atoms, double cutneighsq, int half, int maxneighs, int ld,
-    int* __restrict__ neighbors, int* __restrict__ numneigh, int* __restrict__ counters,
-    const int* __restrict__ qcell)
+    BinGeom g, const int4* __restrict__ stencil, const int* __restrict__ atom_bin,
+    const int* __restrict__ bin_start, const int* __restrict__ bin_atoms, double cutneighsq,
+    int half, int maxneighs, int ld, int* __restrict__ neighbors, int* __restrict__ numneigh,
+    int* __restrict__ counters, const int* __restrict__ qcell)
 {
-    __shared__ int4 st[MDB_MAX_STENCIL];
+    extern __shared__ int4 st[];
     for (int k = threadIdx.x; k < g.nstencil; k += blockDim.x)
         st[k] = stencil[k];
     __syncthreads();
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nlocal) return;
-    const int i      = local_order[t];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nlocal) return;
     const double4 xi = x[i];
     const int ibin   = atom_bin[i];
     const int qi     = qcell ? qcell[i] : 0;
-    // position inside the home bin, in bin units: f in [0, 1)
     const double ux  = (xi.x + g.xlo) * g.bininvx;
     const double uy  = (xi.y + g.ylo) * g.bininvy;
     const double uz  = (xi.z + g.zlo) * g.bininvz;
@@ -481,10 +477,33 @@ __global__ void __launch_bounds__(128) k_build_list(int nlocal, const double4* _
     const float bx = (float)g.binsizex, by = (float)g.binsizey, bz = (float)g.binsizez;
     const float skip2 = (float)cutneighsq * 1.0001f + 1e-4f;
     int n = 0, bad = 0;
+
+    auto consider = [&](int j, const double4& xj) {
+        if (j == i || (half && j < i)) return;
+        double delx = xi.x - xj.x;
+        double dely = xi.y - xj.y;
+        double delz = xi.z - xj.z;
+        double rsq  = delx * delx + dely * dely + delz * delz;
+        if (rsq <= cutneighsq) {
+            int e = j;
+            if (qcell) {
+                int qj = __ldg(&qcell[j]);
+                int cx = cell_axis(qj, 0) - cell_axis(qi, 0);
+                int cy = cell_axis(qj, 1) - cell_axis(qi, 1);
+                int cz = cell_axis(qj, 2) - cell_axis(qi, 2);
+                if (cx < -1 || cx > 1 || cy < -1 || cy > 1 || cz < -1 || cz > 1) bad = 1;
+                int code = ((cx + 1) & 3) | (((cy + 1) & 3) << 2) | (((cz + 1) & 3) << 4);
+                e        = j | (code << MDB_IDX_BITS);
+            }
+            if (n < maxneighs) neighbors[(size_t)n * ld + i] = e;
+            n++;
+        }
+    };
+
     if (ibin >= 0) {
         for (int k = 0; k < g.nstencil; k++) {
             const int4 sk = st[k];
-            int jbin      = ibin + sk.x;
+            const int jbin = ibin + sk.x;
             if (jbin < 0 || jbin >= g.mbins) continue;
             float gx = sk.y > 0 ? (sk.y - fx) : (sk.y < 0 ? (fx - (sk.y + 1)) : 0.f);
             float gy = sk.z > 0 ? (sk.z - fy) : (sk.z < 0 ? (fy - (sk.z + 1)) : 0.f);
@@ -493,38 +512,27 @@ __global__ void __launch_bounds__(128) k_build_list(int nlocal, const double4* _
             gy *= by;
             gz *= bz;
             if (gx * gx + gy * gy + gz * gz > skip2) continue;
-            int beg = __ldg(&bin_start[jbin]);
-            int end = __ldg(&bin_start[jbin + 1]);
-            for (int m = beg; m < end; m++) {
-                int j = __ldg(&bin_atoms[m]);
-                if (j == i) continue;
-                if (half && j < i) continue;
-                double4 xj  = ldg4(&x[j]);
-                double delx = xi.x - xj.x;
-                double dely = xi.y - xj.y;
-                double delz = xi.z - xj.z;
-                double rsq  = delx * delx + dely * dely + delz * delz;
-                if (rsq <= cutneighsq) {
-                    int e = j;
-                    if (qcell) {
-                        int qj = __ldg(&qcell[j]);
-                        int cx = cell_axis(qj, 0) - cell_axis(qi, 0);
-                        int cy = cell_axis(qj, 1) - cell_axis(qi, 1);
-                        int cz = cell_axis(qj, 2) - cell_axis(qi, 2);
-                        if (cx < -2 || cx > 2 || cy < -2 || cy > 2 || cz < -2 || cz > 2) bad = 1;
-                        int code = (cx + 2) + 5 * (cy + 2) + 25 * (cz + 2);
-                        e        = j | ((code & 127) << MDB_IDX_BITS);
-                    }
-                    if (n < maxneighs) neighbors[(size_t)n * ld + t] = e;
-                    n++;
-                }
+            const int beg = __ldg(&bin_start[jbin]);
+            const int end = __ldg(&bin_start[jbin + 1]);
+            int m         = beg;
+            for (; m + 1 < end; m += 2) {
+                const int ja = __ldg(&bin_atoms[m]);
+                const int jb = __ldg(&bin_atoms[m + 1]);
+                const double4 xa = ldg4(&x[ja]);
+                const double4 xb = ldg4(&x[jb]);
+                consider(ja, xa);
+                consider(jb, xb);
+            }
+            if (m < end) {
+                const int ja = __ldg(&bin_atoms[m]);
+                consider(ja, ldg4(&x[ja]));
             }
         }
     }
     // the stored count never exceeds the row capacity, so no consumer can read
     // past the list; the true count of an overflowing row goes to the host,
     // which grows the list and rebuilds before any force is computed
-    numneigh[t] = n < maxneighs ? n : maxneighs;
+    numneigh[i] = n < maxneighs ? n : maxneighs;
     if (n > maxneighs) atomicMax(&counters[CNT_MAXNEED], n);
     if (bad) atomicAdd(&counters[CNT_BADCELL], 1);
 }
@@ -534,10 +542,12 @@ void launch_build_list(cudaStream_t s, int nlocal, const double4* x, BinGeom g,
     const int* bin_atoms, double cutneighsq, int half, int maxneighs, int ld, int* neighbors,
     int* numneigh, int* counters, const int* qcell)
 {
+    (void)local_order;
     if (nlocal <= 0) return;
-    k_build_list<<<mdb_blocks(nlocal, 128), 128, 0, s>>>(nlocal, x, g, stencil, local_order,
-        atom_bin, bin_start, bin_atoms, cutneighsq, half, maxneighs, ld, neighbors, numneigh,
-        counters, qcell);
+    size_t smem = sizeof(int4) * g.nstencil;
+    k_build_list<<<mdb_blocks(nlocal, 128), 128, smem, s>>>(nlocal, x, g, stencil, atom_bin,
+        bin_start, bin_atoms, cutneighsq, half, maxneighs, ld, neighbors, numneigh, counters,
+        qcell);
     g_launches++;
 }
 
