@@ -45,8 +45,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-variants", action="store_true", help="headline only")
-    ap.add_argument("--profile", choices=["lj_mixed", "lj_fp64", "eam_mixed", "eam_fp64",
-                                          "lj_mixed_half", "lj_fp64_half"],
+    ap.add_argument("--profile", choices=[f"{k}_{p}{h}" for k in ("lj", "eam", "cp44", "cp48")
+                                          for p in ("mixed", "fp64") for h in ("", "_half")],
                     help="run one variant only (W+K bench steps + force timing), for ncu")
     ap.add_argument("--cells", type=int, default=None, help="fcc cells per side (profiling)")
     return ap.parse_args()
@@ -99,6 +99,20 @@ def lj_workload(mdb, precision, device, cells=None, half=0):
     hp = mdb.host_params(nx=c, ny=c, nz=c, half_neigh=half)
     x, v, t = mdb.create_fcc(hp)
     s = mdb.system_from_host(hp, len(t), precision=precision, device=device)
+    return s, (x, v, t)
+
+
+def cp_workload(mdb, precision, device, cells=None, half=0, cluster_n=4):
+    """The cluster-pair scheme (GROMACS-style 4xN clusters) on the LJ workload."""
+    c = cells or LJ_CELLS
+    hp = mdb.host_params(nx=c, ny=c, nz=c, half_neigh=half)
+    x, v, t = mdb.create_fcc(hp)
+    s = mdb.ClusterSystem(natoms=len(t), cluster_n=cluster_n, half_neigh=half,
+                          precision=precision, device=device, xprd=hp.xprd, yprd=hp.yprd,
+                          zprd=hp.zprd, cutforce=hp.cutforce, cutneigh=hp.cutneigh, dt=hp.dt,
+                          dtforce=hp.dtforce, mass=hp.mass, epsilon=hp.epsilon,
+                          sigma=hp.sigma, ntypes=hp.ntypes, reneigh_every=hp.reneigh_every,
+                          nstat=hp.nstat)
     return s, (x, v, t)
 
 
@@ -169,8 +183,12 @@ def rel_force_err(a, b):
 
 
 def measure(torch, mdb, kind, precision, args, device, half=0):
-    make = lj_workload if kind == "lj" else eam_workload
-    s, (x, v, t) = make(mdb, precision, device, args.cells, half)
+    if kind.startswith("cp"):
+        s, (x, v, t) = cp_workload(mdb, precision, device, args.cells, half,
+                                   cluster_n=int(kind[3]))
+    else:
+        make = lj_workload if kind == "lj" else eam_workload
+        s, (x, v, t) = make(mdb, precision, device, args.cells, half)
     s.set_atoms(x, v, t)
     s.setup()
     th0 = s.thermo()

@@ -1,0 +1,118 @@
+/*
+ * mdb_cp.h - C ABI of libmdb's cluster-pair scheme: MD-Bench's GROMACS-style
+ * 4xN cluster-pair path (clusterpair/ in the reference) on B200 (sm_100a).
+ *
+ * The reference builds this scheme as a separate executable with its own
+ * Atom (clusterpair/atom.h:39-90) and binds its kernels through global function
+ * pointers: BuildClustersFunction, BuildNeighborFunction, PruneNeighborFunction
+ * (clusterpair/neighbor.h:56-61), UpdatePbcFunction (clusterpair/pbc.h),
+ * IntegrationFunction (clusterpair/integrate.h:14-16) and
+ * ComputeForceFunction (clusterpair/force.h:16-17). Each hook below names the
+ * function it replaces. As in mdb.h, all state lives in an opaque context that
+ * owns its device memory and one CUDA stream, every call is stream-ordered and
+ * returns an int status (MDB_OK = 0), and a context is not thread-safe.
+ *
+ * Cluster shapes: M x N = 4 x 4 (the reference's AVX2 build) or 4 x 8 (its
+ * AVX-512 build). LJ only (the reference's cluster-pair EAM is a stub).
+ *
+ * Layout of arrays crossing this boundary: atoms as AoS triples in atom order;
+ * "slots" in the reference's cluster order, slot cj*N + cjj = atom cjj of
+ * j-cluster cj (locals, then ghost clusters, then the dummy cluster), which is
+ * slot ci*M + cii of atom cii of i-cluster ci; bounding boxes as
+ * (minx maxx miny maxy minz maxz).
+ */
+#ifndef MDB_CP_H
+#define MDB_CP_H
+
+#include "mdb.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct MdbCp MdbCp;
+
+/* Context for the parameters of mdb.h (force_field must be MDB_FF_LJ;
+ * precision MDB_PREC_FP64 or MDB_PREC_MIXED; maxneighs 0 -> 200 as
+ * initNeighbor, clusterpair/neighbor.c:73-77) and cluster width
+ * cluster_n = 4 or 8; prune_every <= 0 keeps the reference's 1000. The column
+ * grid of setupNeighbor (clusterpair/neighbor.c:108-215) is fixed here from
+ * params->natoms and the box. Replaces initDevice + initNeighbor. */
+int mdb_cp_create(const MdbParams* params, int cluster_n, int prune_every, MdbCp** out);
+int mdb_cp_destroy(MdbCp* ctx);
+const char* mdb_cp_last_error(const MdbCp* ctx);
+void* mdb_cp_stream(MdbCp* ctx);
+int mdb_cp_synchronize(MdbCp* ctx);
+long long mdb_cp_launch_count(const MdbCp* ctx);
+
+/* Atom arrays (createAtom / readAtom output, or any state). */
+int mdb_cp_set_atoms(MdbCp* ctx, int nlocal, const double* x, const double* v, const int* type);
+/* Atom arrays as updateSingleAtoms last wrote them (cluster order after a rebuild). */
+int mdb_cp_get_atoms(MdbCp* ctx, double* x, double* v, int* type);
+
+/* ---- hooks ---------------------------------------------------------------- */
+/* buildClusters (clusterpair/neighbor.c:1513-1611): binAtoms, sortAtomsByZCoord,
+ * clusters and boxes; the GPU builds the j-cluster boxes in the same pass. */
+int mdb_cp_build_clusters(MdbCp* ctx);
+/* defineJClusters (clusterpair/neighbor.c:1807-1915): done by
+ * mdb_cp_build_clusters; kept so callers can keep the reference's sequence. */
+int mdb_cp_define_jclusters(MdbCp* ctx);
+/* setupPbc + updatePbc(first) (clusterpair/pbc.c:184-331). */
+int mdb_cp_setup_pbc(MdbCp* ctx);
+/* updatePbc (clusterpair/pbc.c:43-113): ghost positions from their owners. */
+int mdb_cp_update_pbc(MdbCp* ctx);
+/* binJClusters (clusterpair/neighbor.c:1917-2094). */
+int mdb_cp_bin_jclusters(MdbCp* ctx);
+/* buildNeighbor (clusterpair/neighbor.c:282-529), growing maxneighs by 1.2x
+ * the longest row when a row reaches it, as the reference does. */
+int mdb_cp_build_neighbor(MdbCp* ctx);
+/* pruneNeighbor (clusterpair/neighbor.c:1098-1264). */
+int mdb_cp_prune_neighbor(MdbCp* ctx);
+/* updateSingleAtoms (clusterpair/neighbor.c:2096-2149). */
+int mdb_cp_update_single_atoms(MdbCp* ctx);
+/* updateAtomsPbc (clusterpair/pbc.c:116-143). */
+int mdb_cp_update_atoms_pbc(MdbCp* ctx);
+/* computeForce: computeForceLJRef semantics (clusterpair/force_lj.c:23-189) in
+ * FP64, or FP32 pair forces on cluster-relative coordinates (MIXED). */
+int mdb_cp_compute_force(MdbCp* ctx);
+/* The same plus the potential energy (not computed by the reference). */
+int mdb_cp_compute_force_energy(MdbCp* ctx);
+/* initialIntegrate / finalIntegrate (clusterpair/integrate.c:29-86). */
+int mdb_cp_initial_integrate(MdbCp* ctx);
+int mdb_cp_final_integrate(MdbCp* ctx);
+/* computeThermo (common/thermo.c:60-100): T and P from the atom arrays, as
+ * the reference prints them (velocities as of the last updateSingleAtoms); ke,
+ * pe and etotal from the cluster state (pe of the last energy evaluation). */
+int mdb_cp_thermo(MdbCp* ctx, MdbThermo* out);
+
+/* setup() of clusterpair/main.c:44-97 for atoms already set: buildClusters,
+ * defineJClusters, setupPbc, binJClusters, buildNeighbor, then computeForce. */
+int mdb_cp_setup(MdbCp* ctx);
+/* The timestep loop of clusterpair/main.c:326-362 for steps first_step ..
+ * first_step+nsteps-1 (prune every prune_every steps, rebuild every
+ * reneigh_every), plain steps as CUDA graphs. Thermo samples after every step
+ * n with (n+1) % nstat == 0, up to max_samples (at most 64 per call). */
+int mdb_cp_run(MdbCp* ctx, int first_step, int nsteps, MdbThermo* samples, int max_samples,
+    int* nsamples);
+
+/* ---- introspection (tests, tools) ----------------------------------------- */
+/* counts: Nlocal Natoms Nclusters_local ncj Nclusters_ghost Nghost dummy_cj
+ * maxneighs */
+int mdb_cp_get_counts(MdbCp* ctx, int* counts);
+/* nslots slots of x, type; v and f for the local slots (others untouched). */
+int mdb_cp_get_slots(MdbCp* ctx, double* x, double* v, double* f, int* type, int nslots);
+int mdb_cp_get_iclusters(MdbCp* ctx, int* natoms, int* bin, double* bb);
+int mdb_cp_get_jclusters(MdbCp* ctx, int* natoms, double* bb, int count);
+int mdb_cp_get_ghosts(MdbCp* ctx, int* border_map, int* pbc_xyz);
+/* Row-major copy: neighbors[ci*ld + k], k < numneigh[ci], in list order. */
+int mdb_cp_get_neighbor_list(MdbCp* ctx, int* numneigh, int* nmasked, int* neighbors, int ld);
+/* j-cluster columns: start[mbins + 1], list[start[mbins]]; returns the count. */
+int mdb_cp_get_columns(MdbCp* ctx, int* start, int* list, int cap);
+/* ints: nbinx nbiny mbinx mbiny mbinxlo mbinylo nstencil; dbls: binsizex
+ * binsizey rbb_sq; stencil: nstencil flat offsets */
+int mdb_cp_get_geometry(MdbCp* ctx, int* ints, double* dbls, int* stencil, int max_stencil);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MDB_CP_H */

@@ -1,0 +1,1193 @@
+// libmdb cluster-pair C ABI (include/mdb_cp.h): context, buffers, the
+// reference hooks and the graph-captured timestep loop of clusterpair/main.c.
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "mdb_cp.h"
+#include "mdb_cp_internal.cuh"
+
+using namespace mdb;
+using namespace mdb::cp;
+
+struct CpGraph {
+    cudaGraphExec_t exec = nullptr;
+    long long kernels    = 0;
+};
+
+struct MdbCp {
+    MdbParams p;
+    std::vector<double> eps_t, sig_t;
+    int M = CP_M, N = 4, jfac = 1, prune_every = 1000;
+    bool mixed = false;
+    int dev        = 0;
+    cudaStream_t s = nullptr;
+    std::string err;
+    long long launches = 0;
+
+    int nlocal = 0, maxneighs = 200;
+    Geom g;
+    std::vector<int> stencil;
+    Types ty;
+    double cutforcesq = 0;
+    double t_scale = 1, dof_boltz = 1, p_scale = 1;
+
+    // capacities
+    int atom_cap = 0, ncl_cap = 0, ncj_cap = 0, ngc_cap = 0, slot_cap = 0, ld = 0;
+
+    // atom arrays and columns
+    double4 *ax = nullptr, *av = nullptr;
+    int *atom_col = nullptr, *col_count = nullptr, *col_start = nullptr, *col_fill = nullptr;
+    int *col_atoms = nullptr, *col_sorted = nullptr, *gidx = nullptr;
+    double* gz    = nullptr;
+    int *ncl_col = nullptr, *cl_start = nullptr;
+    // slots
+    double4 *cx = nullptr, *cv = nullptr, *cf = nullptr;
+    float4 *xr = nullptr, *cf32 = nullptr, *anchor = nullptr;
+    // clusters
+    int *inat = nullptr, *cbin = nullptr, *cl_first = nullptr, *jnat = nullptr;
+    double4 *ibbmin = nullptr, *ibbmax = nullptr, *jbbmin = nullptr, *jbbmax = nullptr;
+    // ghosts and j columns
+    int *gcount = nullptr, *gstart = nullptr, *border = nullptr, *pbc = nullptr;
+    int *gcolumn = nullptr, *gcol_count = nullptr, *gfill = nullptr, *jcol_n = nullptr;
+    int *jcol_start = nullptr, *gtmp = nullptr, *jcol = nullptr;
+    double4 *jcbbmin = nullptr, *jcbbmax = nullptr;
+    int* stencil_d = nullptr;
+    // list
+    int *list = nullptr, *numneigh = nullptr, *nmasked = nullptr;
+    // counters, scratch, reductions
+    int* cnt                 = nullptr;
+    unsigned long long* zext = nullptr;
+    int* scan_scratch        = nullptr;
+    int scan_scratch_n       = 0;
+    double* partials         = nullptr; // npart for energy + npart for ke
+    int npart                = 0;
+    double* red              = nullptr; // 64 slots x {ke_atoms, pe, ke_slots, pad}
+    double* stage            = nullptr;
+    int* stage_i             = nullptr;
+    size_t stage_n           = 0;
+    int* h_cnt               = nullptr;
+    double* h_red            = nullptr;
+
+    bool have_atoms = false, have_clusters = false, have_ghosts = false, have_list = false;
+    bool energy_valid = false;
+    int energy_blocks = 0; // partial-energy blocks of the last energy evaluation
+    CpGraph g_plain;
+};
+
+#define RED_SLOTS 64
+
+#define CK(call)                                                                         \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) return fail(ctx, MDB_ERR_CUDA, #call, e_);                \
+    } while (0)
+
+static int fail(MdbCp* ctx, int code, const char* what, cudaError_t e = cudaSuccess)
+{
+    if (ctx) {
+        char buf[512];
+        if (e != cudaSuccess) snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+        else snprintf(buf, sizeof buf, "%s", what);
+        ctx->err = buf;
+    }
+    return code;
+}
+
+template <typename T> static cudaError_t dalloc(T** p, size_t n)
+{
+    *p = nullptr;
+    if (n == 0) n = 1;
+    return cudaMalloc((void**)p, n * sizeof(T));
+}
+
+template <typename T> static void dfree(T*& p)
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+static void drop_graph(MdbCp* ctx)
+{
+    if (ctx->g_plain.exec) cudaGraphExecDestroy(ctx->g_plain.exec);
+    ctx->g_plain.exec    = nullptr;
+    ctx->g_plain.kernels = 0;
+}
+
+static long long mark() { return mdb::g_launches; }
+static void account(MdbCp* ctx, long long m) { ctx->launches += mdb::g_launches - m; }
+
+// ---------------------------------------------------------------------------
+// setupNeighbor, clusterpair/neighbor.c:108-215 (box at the origin)
+static double bindist2(const Geom& g, int i, int j)
+{
+    double dx, dy;
+    if (i > 0) dx = (i - 1) * g.binsizex;
+    else if (i == 0) dx = 0.0;
+    else dx = (i + 1) * g.binsizex;
+    if (j > 0) dy = (j - 1) * g.binsizey;
+    else if (j == 0) dy = 0.0;
+    else dy = (j + 1) * g.binsizey;
+    return dx * dx + dy * dy;
+}
+
+static void setup_columns(MdbCp* ctx)
+{
+    const MdbParams& p = ctx->p;
+    Geom& g            = ctx->g;
+    const double xprd = p.xprd, yprd = p.yprd, zprd = p.zprd, cut = p.cutneigh;
+    double density  = ((double)p.natoms) / ((xprd - 0.0) * (yprd - 0.0) * (zprd - 0.0));
+    double in_cell  = (double)std::max(ctx->M, ctx->N);
+    double tx       = cbrt(in_cell / density);
+    double ty       = cbrt(in_cell / density);
+    g.nbinx         = std::max(1, (int)ceil((xprd - 0.0) / tx));
+    g.nbiny         = std::max(1, (int)ceil((yprd - 0.0) / ty));
+    g.binsizex      = (xprd - 0.0) / g.nbinx;
+    g.binsizey      = (yprd - 0.0) / g.nbiny;
+    g.bininvx       = 1.0 / g.binsizex;
+    g.bininvy       = 1.0 / g.binsizey;
+    g.xprd          = xprd;
+    g.yprd          = yprd;
+    g.zprd          = zprd;
+    g.cutneigh      = cut;
+    g.cutneighsq    = cut * cut;
+    double coord    = 0.0 - cut - 1.0e-6 * xprd;
+    g.mbinxlo       = (int)(coord * g.bininvx);
+    if (coord < 0.0) g.mbinxlo = g.mbinxlo - 1;
+    coord       = xprd + cut + 1.0e-6 * xprd;
+    int mbinxhi = (int)(coord * g.bininvx);
+    coord       = 0.0 - cut - 1.0e-6 * yprd;
+    g.mbinylo   = (int)(coord * g.bininvy);
+    if (coord < 0.0) g.mbinylo = g.mbinylo - 1;
+    coord       = yprd + cut + 1.0e-6 * yprd;
+    int mbinyhi = (int)(coord * g.bininvy);
+    g.mbinxlo   = g.mbinxlo - 1;
+    mbinxhi     = mbinxhi + 1;
+    g.mbinx     = mbinxhi - g.mbinxlo + 1;
+    g.mbinylo   = g.mbinylo - 1;
+    mbinyhi     = mbinyhi + 1;
+    g.mbiny     = mbinyhi - g.mbinylo + 1;
+    int nextx   = (int)(cut * g.bininvx);
+    int nexty   = (int)(cut * g.bininvy);
+    if (nextx * g.binsizex < 0.999 * cut) nextx++;
+    if (nexty * g.binsizey < 0.999 * cut) nexty++;
+    ctx->stencil.clear();
+    for (int j = -nexty; j <= nexty; j++)
+        for (int i = -nextx; i <= nextx; i++)
+            if (bindist2(g, i, j) < g.cutneighsq) ctx->stencil.push_back(j * g.mbinx + i);
+    g.nstencil = (int)ctx->stencil.size();
+    g.mbins    = g.mbinx * g.mbiny;
+    // buildNeighborCPU, clusterpair/neighbor.c:300-303
+    double bbx = 0.5 * (g.binsizex + g.binsizex);
+    double bby = 0.5 * (g.binsizey + g.binsizey);
+    double rbb = std::max(0.0, cut - 0.5 * sqrt(bbx * bbx + bby * bby));
+    g.rbb_sq   = rbb * rbb;
+}
+
+// computePerTypeLJParameters (common/parameter.c:31-45): per-type sqrt(eps)
+// and sigma^3; pairs mix geometrically (clusterpair/force_lj.c:130-132)
+static int setup_types(MdbCp* ctx)
+{
+    int nt = std::max(1, ctx->p.ntypes);
+    if (nt > MDB_MAX_TYPES) return fail(ctx, MDB_ERR_ARG, "more than 8 atom types");
+    Types& t = ctx->ty;
+    memset(&t, 0, sizeof t);
+    t.ntypes     = nt;
+    bool uniform = true;
+    for (int k = 0; k < nt; k++) {
+        double e = k < (int)ctx->eps_t.size() ? ctx->eps_t[k] : ctx->p.epsilon;
+        double s = k < (int)ctx->sig_t.size() ? ctx->sig_t[k] : ctx->p.sigma;
+        t.sqrt_eps[k]   = sqrt(e);
+        t.sigma3[k]     = s * s * s;
+        t.sqrt_eps_f[k] = (float)t.sqrt_eps[k];
+        t.sigma3_f[k]   = (float)t.sigma3[k];
+        if (t.sqrt_eps[k] != t.sqrt_eps[0] || t.sigma3[k] != t.sigma3[0]) uniform = false;
+    }
+    t.uniform  = uniform ? 1 : 0;
+    t.eps0     = t.sqrt_eps[0] * t.sqrt_eps[0];
+    t.sigma6_0 = t.sigma3[0] * t.sigma3[0];
+    return MDB_OK;
+}
+
+extern "C" const char* mdb_cp_last_error(const MdbCp* ctx) { return ctx ? ctx->err.c_str() : ""; }
+extern "C" void* mdb_cp_stream(MdbCp* ctx) { return ctx ? (void*)ctx->s : nullptr; }
+extern "C" long long mdb_cp_launch_count(const MdbCp* ctx) { return ctx ? ctx->launches : 0; }
+
+extern "C" int mdb_cp_synchronize(MdbCp* ctx)
+{
+    if (!ctx) return MDB_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->s));
+    return MDB_OK;
+}
+
+static void free_all(MdbCp* ctx)
+{
+    dfree(ctx->ax), dfree(ctx->av), dfree(ctx->atom_col), dfree(ctx->col_count);
+    dfree(ctx->col_start), dfree(ctx->col_fill), dfree(ctx->col_atoms), dfree(ctx->col_sorted);
+    dfree(ctx->gidx), dfree(ctx->gz), dfree(ctx->ncl_col), dfree(ctx->cl_start);
+    dfree(ctx->cx), dfree(ctx->cv), dfree(ctx->cf), dfree(ctx->xr), dfree(ctx->cf32);
+    dfree(ctx->anchor), dfree(ctx->inat), dfree(ctx->cbin), dfree(ctx->cl_first);
+    dfree(ctx->jnat), dfree(ctx->ibbmin), dfree(ctx->ibbmax), dfree(ctx->jbbmin);
+    dfree(ctx->jbbmax), dfree(ctx->gcount), dfree(ctx->gstart), dfree(ctx->border);
+    dfree(ctx->pbc), dfree(ctx->gcolumn), dfree(ctx->gcol_count), dfree(ctx->gfill);
+    dfree(ctx->jcol_n), dfree(ctx->jcol_start), dfree(ctx->gtmp), dfree(ctx->jcol);
+    dfree(ctx->jcbbmin), dfree(ctx->jcbbmax);
+    dfree(ctx->stencil_d), dfree(ctx->list), dfree(ctx->numneigh), dfree(ctx->nmasked);
+    dfree(ctx->cnt), dfree(ctx->zext), dfree(ctx->scan_scratch), dfree(ctx->partials);
+    dfree(ctx->red), dfree(ctx->stage), dfree(ctx->stage_i);
+    if (ctx->h_cnt) cudaFreeHost(ctx->h_cnt);
+    if (ctx->h_red) cudaFreeHost(ctx->h_red);
+    ctx->h_cnt = nullptr;
+    ctx->h_red = nullptr;
+}
+
+extern "C" int mdb_cp_destroy(MdbCp* ctx)
+{
+    if (!ctx) return MDB_ERR_ARG;
+    cudaSetDevice(ctx->dev);
+    if (ctx->s) cudaStreamSynchronize(ctx->s);
+    drop_graph(ctx);
+    free_all(ctx);
+    if (ctx->s) cudaStreamDestroy(ctx->s);
+    delete ctx;
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_create(const MdbParams* params, int cluster_n, int prune_every, MdbCp** out)
+{
+    if (!params || !out) return MDB_ERR_ARG;
+    *out        = nullptr;
+    MdbCp* ctx  = new MdbCp();
+    ctx->p      = *params;
+    MdbParams& p = ctx->p;
+    int rc       = MDB_OK;
+    if (p.ntypes < 1) p.ntypes = 1;
+    if (p.epsilon_per_type) ctx->eps_t.assign(p.epsilon_per_type, p.epsilon_per_type + p.ntypes);
+    if (p.sigma_per_type) ctx->sig_t.assign(p.sigma_per_type, p.sigma_per_type + p.ntypes);
+    p.epsilon_per_type = nullptr;
+    p.sigma_per_type   = nullptr;
+    if (p.reneigh_every < 1) p.reneigh_every = 20;
+    if (p.nstat < 1) p.nstat = 100;
+    ctx->maxneighs   = p.maxneighs > 0 ? p.maxneighs : 200;
+    ctx->prune_every = prune_every > 0 ? prune_every : 1000;
+    ctx->N           = cluster_n;
+    ctx->jfac        = cluster_n / CP_M;
+    ctx->mixed       = p.precision == MDB_PREC_MIXED;
+    ctx->cutforcesq  = p.cutforce * p.cutforce;
+    if ((cluster_n != 4 && cluster_n != 8) || p.force_field != MDB_FF_LJ ||
+        !(p.precision == MDB_PREC_FP64 || p.precision == MDB_PREC_MIXED) ||
+        !(p.xprd > 0 && p.yprd > 0 && p.zprd > 0) || !(p.cutforce > 0) ||
+        !(p.cutneigh >= p.cutforce) || p.natoms < 1 || ctx->maxneighs > 12288) {
+        rc = fail(ctx, MDB_ERR_ARG, "invalid parameters for the cluster-pair scheme");
+        goto bad;
+    }
+    // the mixed path's anchors are multiples of 1/8 held in FP32
+    if (ctx->mixed && std::max(p.xprd, std::max(p.yprd, p.zprd)) > 1.0e5) {
+        rc = fail(ctx, MDB_ERR_ARG, "box too large for FP32 cluster anchors");
+        goto bad;
+    }
+    setup_columns(ctx);
+    if ((rc = setup_types(ctx)) != MDB_OK) goto bad;
+    // setupThermo, common/thermo.c:35-58 (LJ units)
+    ctx->dof_boltz = (p.natoms * 3 - 3);
+    ctx->t_scale   = 1.0 / ctx->dof_boltz;
+    ctx->p_scale   = 1.0 / 3 / p.xprd / p.yprd / p.zprd;
+    {
+        cudaError_t e;
+        if ((e = cudaSetDevice(p.device)) != cudaSuccess) {
+            rc = fail(ctx, MDB_ERR_CUDA, "cudaSetDevice", e);
+            goto bad;
+        }
+        ctx->dev = p.device;
+        if ((e = cudaStreamCreateWithFlags(&ctx->s, cudaStreamNonBlocking)) != cudaSuccess) {
+            rc = fail(ctx, MDB_ERR_CUDA, "cudaStreamCreate", e);
+            goto bad;
+        }
+        const int mb1 = ctx->g.mbins + 1;
+        if ((e = dalloc(&ctx->cnt, CP_SLOTS)) != cudaSuccess ||
+            (e = dalloc(&ctx->zext, 1)) != cudaSuccess ||
+            (e = dalloc(&ctx->stencil_d, ctx->g.nstencil)) != cudaSuccess ||
+            (e = dalloc(&ctx->col_count, mb1)) != cudaSuccess ||
+            (e = dalloc(&ctx->col_start, mb1 + 1)) != cudaSuccess ||
+            (e = dalloc(&ctx->col_fill, mb1)) != cudaSuccess ||
+            (e = dalloc(&ctx->ncl_col, mb1)) != cudaSuccess ||
+            (e = dalloc(&ctx->cl_start, mb1 + 1)) != cudaSuccess ||
+            (e = dalloc(&ctx->gcol_count, mb1)) != cudaSuccess ||
+            (e = dalloc(&ctx->gfill, mb1)) != cudaSuccess ||
+            (e = dalloc(&ctx->jcol_n, mb1)) != cudaSuccess ||
+            (e = dalloc(&ctx->jcol_start, mb1 + 1)) != cudaSuccess ||
+            (e = dalloc(&ctx->red, 4 * RED_SLOTS)) != cudaSuccess ||
+            (e = cudaMallocHost((void**)&ctx->h_cnt, CP_SLOTS * sizeof(int))) != cudaSuccess ||
+            (e = cudaMallocHost((void**)&ctx->h_red, 4 * RED_SLOTS * sizeof(double))) !=
+                cudaSuccess) {
+            rc = fail(ctx, MDB_ERR_NOMEM, "device allocation", e);
+            goto bad;
+        }
+        cudaMemset(ctx->cnt, 0, CP_SLOTS * sizeof(int));
+        cudaMemcpy(ctx->stencil_d, ctx->stencil.data(), sizeof(int) * ctx->g.nstencil,
+            cudaMemcpyHostToDevice);
+        if ((e = cudaGetLastError()) != cudaSuccess) {
+            rc = fail(ctx, MDB_ERR_CUDA, "setup copy", e);
+            goto bad;
+        }
+    }
+    *out = ctx;
+    return MDB_OK;
+bad:
+    fprintf(stderr, "mdb_cp_create: %s\n", ctx->err.c_str());
+    mdb_cp_destroy(ctx);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// buffers sized by the atom count (clusters) and by the ghost capacity
+static int alloc_atoms(MdbCp* ctx, int n)
+{
+    cudaError_t e;
+    const int mb = ctx->g.mbins;
+    // clusters: ceil(c / M) per column, +1 per column for even pairs (M < N)
+    ctx->ncl_cap  = n / ctx->M + 2 * mb + 8;
+    ctx->ncj_cap  = ctx->ncl_cap / ctx->jfac + 1;
+    ctx->ld       = ctx->ncl_cap;
+    ctx->atom_cap = n;
+    dfree(ctx->ax), dfree(ctx->av), dfree(ctx->atom_col), dfree(ctx->col_atoms);
+    dfree(ctx->col_sorted), dfree(ctx->gidx), dfree(ctx->gz), dfree(ctx->inat), dfree(ctx->cbin);
+    dfree(ctx->cl_first), dfree(ctx->ibbmin), dfree(ctx->ibbmax), dfree(ctx->gcount);
+    dfree(ctx->gstart), dfree(ctx->numneigh), dfree(ctx->nmasked), dfree(ctx->list);
+    dfree(ctx->scan_scratch), dfree(ctx->partials), dfree(ctx->stage), dfree(ctx->stage_i);
+    int scan_n          = std::max(std::max(mb + 2, ctx->ncj_cap + 1), 1);
+    ctx->scan_scratch_n = scan_scratch_ints(scan_n);
+    ctx->npart = std::max(force_blocks(ctx->ncl_cap), ke_blocks(ctx->ncl_cap * ctx->M));
+    ctx->stage_n = (size_t)3 * std::max(n, 1) * 3;
+    if ((e = dalloc(&ctx->ax, n)) != cudaSuccess || (e = dalloc(&ctx->av, n)) != cudaSuccess ||
+        (e = dalloc(&ctx->atom_col, n)) != cudaSuccess ||
+        (e = dalloc(&ctx->col_atoms, n)) != cudaSuccess ||
+        (e = dalloc(&ctx->col_sorted, n)) != cudaSuccess ||
+        (e = dalloc(&ctx->gidx, 2 * (size_t)n + 2)) != cudaSuccess ||
+        (e = dalloc(&ctx->gz, 2 * (size_t)n + 2)) != cudaSuccess ||
+        (e = dalloc(&ctx->inat, ctx->ncl_cap)) != cudaSuccess ||
+        (e = dalloc(&ctx->cbin, ctx->ncl_cap)) != cudaSuccess ||
+        (e = dalloc(&ctx->cl_first, ctx->ncl_cap)) != cudaSuccess ||
+        (e = dalloc(&ctx->ibbmin, ctx->ncl_cap)) != cudaSuccess ||
+        (e = dalloc(&ctx->ibbmax, ctx->ncl_cap)) != cudaSuccess ||
+        (e = dalloc(&ctx->gcount, ctx->ncj_cap)) != cudaSuccess ||
+        (e = dalloc(&ctx->gstart, ctx->ncj_cap + 1)) != cudaSuccess ||
+        (e = dalloc(&ctx->numneigh, ctx->ncl_cap)) != cudaSuccess ||
+        (e = dalloc(&ctx->nmasked, ctx->ncl_cap)) != cudaSuccess ||
+        (e = dalloc(&ctx->list, (size_t)ctx->maxneighs * ctx->ld)) != cudaSuccess ||
+        (e = dalloc(&ctx->scan_scratch, ctx->scan_scratch_n)) != cudaSuccess ||
+        (e = dalloc(&ctx->partials, 2 * (size_t)ctx->npart)) != cudaSuccess ||
+        (e = dalloc(&ctx->stage, ctx->stage_n)) != cudaSuccess ||
+        (e = dalloc(&ctx->stage_i, std::max(n, 1))) != cudaSuccess)
+        return fail(ctx, MDB_ERR_NOMEM, "device allocation (atoms)", e);
+    cudaMemsetAsync(ctx->numneigh, 0, sizeof(int) * ctx->ncl_cap, ctx->s);
+    return MDB_OK;
+}
+
+static int alloc_ghosts(MdbCp* ctx, int ngc_cap)
+{
+    cudaError_t e;
+    drop_graph(ctx);
+    ctx->ngc_cap  = ngc_cap;
+    const int nj  = ctx->ncj_cap + ngc_cap + 1;
+    ctx->slot_cap = nj * ctx->N;
+    dfree(ctx->cx), dfree(ctx->cv), dfree(ctx->cf), dfree(ctx->xr), dfree(ctx->cf32);
+    dfree(ctx->anchor), dfree(ctx->jnat), dfree(ctx->jbbmin), dfree(ctx->jbbmax);
+    dfree(ctx->border), dfree(ctx->pbc), dfree(ctx->gcolumn), dfree(ctx->gtmp), dfree(ctx->jcol);
+    dfree(ctx->jcbbmin), dfree(ctx->jcbbmax);
+    if ((e = dalloc(&ctx->cx, ctx->slot_cap)) != cudaSuccess ||
+        (e = dalloc(&ctx->jcbbmin, nj)) != cudaSuccess ||
+        (e = dalloc(&ctx->jcbbmax, nj)) != cudaSuccess ||
+        (e = dalloc(&ctx->cv, ctx->slot_cap)) != cudaSuccess ||
+        (e = dalloc(&ctx->cf, ctx->slot_cap)) != cudaSuccess ||
+        (e = dalloc(&ctx->jnat, nj)) != cudaSuccess ||
+        (e = dalloc(&ctx->jbbmin, nj)) != cudaSuccess ||
+        (e = dalloc(&ctx->jbbmax, nj)) != cudaSuccess ||
+        (e = dalloc(&ctx->border, ngc_cap)) != cudaSuccess ||
+        (e = dalloc(&ctx->pbc, ngc_cap)) != cudaSuccess ||
+        (e = dalloc(&ctx->gcolumn, ngc_cap)) != cudaSuccess ||
+        (e = dalloc(&ctx->gtmp, nj)) != cudaSuccess || (e = dalloc(&ctx->jcol, nj)) != cudaSuccess)
+        return fail(ctx, MDB_ERR_NOMEM, "device allocation (ghosts)", e);
+    if (ctx->mixed) {
+        if ((e = dalloc(&ctx->xr, ctx->slot_cap)) != cudaSuccess ||
+            (e = dalloc(&ctx->cf32, ctx->slot_cap)) != cudaSuccess ||
+            (e = dalloc(&ctx->anchor, nj)) != cudaSuccess)
+            return fail(ctx, MDB_ERR_NOMEM, "device allocation (ghosts)", e);
+    }
+    cudaMemsetAsync(ctx->cf, 0, sizeof(double4) * ctx->slot_cap, ctx->s);
+    if (ctx->cf32) cudaMemsetAsync(ctx->cf32, 0, sizeof(float4) * ctx->slot_cap, ctx->s);
+    ctx->have_clusters = ctx->have_ghosts = ctx->have_list = false;
+    return MDB_OK;
+}
+
+static int alloc_list(MdbCp* ctx, int maxneighs)
+{
+    if (maxneighs > 12288) return fail(ctx, MDB_ERR_OVERFLOW, "cluster list longer than 12288");
+    drop_graph(ctx);
+    dfree(ctx->list);
+    ctx->maxneighs = maxneighs;
+    CK(dalloc(&ctx->list, (size_t)maxneighs * ctx->ld));
+    return MDB_OK;
+}
+
+#define NEED_ATOMS()                                                                     \
+    do {                                                                                 \
+        if (!ctx) return MDB_ERR_ARG;                                                    \
+        if (!ctx->have_atoms) return fail(ctx, MDB_ERR_STATE, "no atoms set");           \
+    } while (0)
+
+extern "C" int mdb_cp_set_atoms(MdbCp* ctx, int nlocal, const double* x, const double* v,
+    const int* type)
+{
+    if (!ctx || nlocal < 1 || !x || !v) return MDB_ERR_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    CK(cudaStreamSynchronize(ctx->s));
+    if (nlocal != ctx->atom_cap) {
+        drop_graph(ctx);
+        int rc = alloc_atoms(ctx, nlocal);
+        if (rc) return rc;
+        // ghost j-clusters: start from the surface layer estimate (grown on
+        // overflow); the slot arrays depend on the local cluster capacity too
+        const MdbParams& p = ctx->p;
+        double vol   = p.xprd * p.yprd * p.zprd;
+        double shell = (p.xprd + 2 * p.cutneigh + 4) * (p.yprd + 2 * p.cutneigh + 4) *
+                           (p.zprd + 2 * p.cutneigh + 4) -
+                       vol;
+        double est = 1.5 * shell / vol * nlocal / ctx->N + 1024;
+        est        = std::max(est, (double)ctx->ngc_cap);
+        rc         = alloc_ghosts(ctx, (int)std::min(est, 2.0e9 / ctx->N));
+        if (rc) return rc;
+    }
+    ctx->nlocal = nlocal;
+    std::vector<double4> hx(nlocal), hv(nlocal);
+    for (int i = 0; i < nlocal; i++) {
+        long long t = type ? type[i] : 0;
+        if (t < 0 || t >= ctx->ty.ntypes) return fail(ctx, MDB_ERR_ARG, "atom type out of range");
+        double w;
+        memcpy(&w, &t, sizeof w);
+        hx[i] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], w);
+        hv[i] = make_double4(v[3 * i], v[3 * i + 1], v[3 * i + 2], 0.0);
+    }
+    CK(cudaMemcpy(ctx->ax, hx.data(), sizeof(double4) * nlocal, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->av, hv.data(), sizeof(double4) * nlocal, cudaMemcpyHostToDevice));
+    ctx->have_atoms    = true;
+    ctx->have_clusters = ctx->have_ghosts = ctx->have_list = false;
+    ctx->energy_valid  = false;
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_get_atoms(MdbCp* ctx, double* x, double* v, int* type)
+{
+    NEED_ATOMS();
+    int n = ctx->nlocal;
+    std::vector<double4> hx(n), hv(n);
+    CK(cudaMemcpyAsync(hx.data(), ctx->ax, sizeof(double4) * n, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaMemcpyAsync(hv.data(), ctx->av, sizeof(double4) * n, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    for (int i = 0; i < n; i++) {
+        if (x) {
+            x[3 * i] = hx[i].x, x[3 * i + 1] = hx[i].y, x[3 * i + 2] = hx[i].z;
+        }
+        if (v) {
+            v[3 * i] = hv[i].x, v[3 * i + 1] = hv[i].y, v[3 * i + 2] = hv[i].z;
+        }
+        if (type) {
+            long long t;
+            memcpy(&t, &hx[i].w, sizeof t);
+            type[i] = (int)t;
+        }
+    }
+    return MDB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// enqueue helpers (stream-ordered, graph-capturable)
+static void enq_clusters(MdbCp* ctx)
+{
+    cudaStream_t s = ctx->s;
+    const Geom& g  = ctx->g;
+    const int mb1  = g.mbins + 1;
+    cudaMemsetAsync(ctx->col_count, 0, sizeof(int) * mb1, s);
+    cudaMemsetAsync(ctx->col_fill, 0, sizeof(int) * mb1, s);
+    cudaMemsetAsync(ctx->ncl_col, 0, sizeof(int) * mb1, s);
+    cudaMemsetAsync(ctx->zext, 0, sizeof(unsigned long long), s);
+    launch_bin_atoms(s, ctx->nlocal, ctx->ax, g, ctx->atom_col, ctx->col_count, ctx->cnt);
+    scan_exclusive(ctx->col_count, ctx->col_start, g.mbins, ctx->scan_scratch, s);
+    launch_scatter_atoms(s, ctx->nlocal, ctx->atom_col, ctx->col_start, ctx->col_fill,
+        ctx->col_atoms);
+    launch_sort_columns(s, g, ctx->M, ctx->N, ctx->col_start, ctx->col_atoms, ctx->ax,
+        ctx->col_sorted, ctx->gidx, ctx->gz, ctx->ncl_col);
+    scan_exclusive(ctx->ncl_col, ctx->cl_start, mb1, ctx->scan_scratch, s);
+    launch_build_clusters(s, g, ctx->M, ctx->N, ctx->mixed, ctx->col_start, ctx->col_sorted,
+        ctx->cl_start, ctx->ax, ctx->av, ctx->cx, ctx->cv, ctx->inat, ctx->cbin, ctx->cl_first,
+        ctx->ibbmin, ctx->ibbmax, ctx->jnat, ctx->jbbmin, ctx->jbbmax, ctx->anchor, ctx->xr,
+        ctx->cnt, ctx->zext);
+}
+
+static void enq_setup_pbc(MdbCp* ctx)
+{
+    cudaStream_t s = ctx->s;
+    cudaMemsetAsync(ctx->cnt + CP_NGHOST_ATOMS, 0, sizeof(int), s);
+    launch_ghost_count(s, ctx->ncj_cap, ctx->cnt, ctx->jnat, ctx->jbbmin, ctx->jbbmax, ctx->g,
+        ctx->gcount);
+    scan_exclusive(ctx->gcount, ctx->gstart, ctx->ncj_cap, ctx->scan_scratch, s);
+    launch_ghost_write(s, ctx->ncj_cap, ctx->ngc_cap, ctx->cnt, ctx->jnat, ctx->jbbmin,
+        ctx->jbbmax, ctx->g, ctx->gstart, ctx->border, ctx->pbc);
+    launch_ghost_first(s, ctx->N, ctx->ngc_cap, ctx->mixed, ctx->cnt, ctx->border, ctx->pbc,
+        ctx->g, ctx->cx, ctx->jnat, ctx->jbbmin, ctx->jbbmax, ctx->anchor, ctx->xr, ctx->zext);
+}
+
+static void enq_bin_j(MdbCp* ctx)
+{
+    cudaStream_t s = ctx->s;
+    const int mb1  = ctx->g.mbins + 1;
+    cudaMemsetAsync(ctx->gcol_count, 0, sizeof(int) * mb1, s);
+    cudaMemsetAsync(ctx->gfill, 0, sizeof(int) * mb1, s);
+    launch_ghost_columns(s, ctx->N, ctx->ngc_cap, ctx->cnt, ctx->pbc, ctx->jnat, ctx->cx, ctx->g,
+        ctx->gcolumn, ctx->gcol_count);
+    launch_column_sizes(s, mb1, ctx->jfac, ctx->ncl_col, ctx->gcol_count, ctx->jcol_n);
+    scan_exclusive(ctx->jcol_n, ctx->jcol_start, mb1, ctx->scan_scratch, s);
+    launch_ghost_scatter(s, ctx->ngc_cap, ctx->cnt, ctx->gcolumn, ctx->jcol_start, ctx->ncl_col,
+        ctx->jfac, ctx->gfill, ctx->gtmp);
+    launch_merge_columns(s, mb1, ctx->jfac, ctx->ncl_col, ctx->cl_start, ctx->gcol_count,
+        ctx->jcol_start, ctx->gtmp, ctx->jbbmin, ctx->jbbmax, ctx->jcol, ctx->jcbbmin,
+        ctx->jcbbmax);
+}
+
+// list layout: row-major for the mixed kernel, k-major for the FP64 one
+static int lks(const MdbCp* ctx) { return ctx->mixed ? 1 : ctx->ld; }
+static int lcs(const MdbCp* ctx) { return ctx->mixed ? ctx->maxneighs : 1; }
+
+static void enq_list(MdbCp* ctx)
+{
+    launch_build_list(ctx->s, ctx->M, ctx->N, ctx->p.half_neigh, ctx->ncl_cap, ctx->cnt, ctx->g,
+        ctx->stencil_d, ctx->cbin, ctx->ibbmin, ctx->ibbmax, ctx->jcbbmin, ctx->jcbbmax, ctx->cx,
+        ctx->jcol_start, ctx->jcol, ctx->zext, ctx->maxneighs, lks(ctx), lcs(ctx), ctx->list,
+        ctx->numneigh, ctx->nmasked, ctx->cnt);
+}
+
+static void clear_build_counters(MdbCp* ctx)
+{
+    // CP_MAXNEED, CP_BADBIN, CP_WINDOW
+    cudaMemsetAsync(ctx->cnt + CP_MAXNEED, 0, 3 * sizeof(int), ctx->s);
+}
+
+// buildClusters .. buildNeighbor from the atom arrays (idempotent)
+static void enq_build(MdbCp* ctx)
+{
+    clear_build_counters(ctx);
+    enq_clusters(ctx);
+    enq_setup_pbc(ctx);
+    enq_bin_j(ctx);
+    enq_list(ctx);
+}
+
+static void enq_gather(MdbCp* ctx, int wrap)
+{
+    launch_gather(ctx->s, ctx->M, ctx->ncl_cap, ctx->cnt, ctx->cx, ctx->cv, ctx->cl_first,
+        ctx->ax, ctx->av, wrap, ctx->p.xprd, ctx->p.yprd, ctx->p.zprd);
+}
+
+// Reads the counters; grows what overflowed. 1: replay the build, 0: done,
+// <0: error (negated status). what: the stages that ran.
+enum { CHK_CLUSTERS = 1, CHK_GHOSTS = 2, CHK_LIST = 4, CHK_ALL = 7 };
+
+static int check_build(MdbCp* ctx, int what)
+{
+    cudaError_t e = cudaMemcpyAsync(ctx->h_cnt, ctx->cnt, CP_SLOTS * sizeof(int),
+        cudaMemcpyDeviceToHost, ctx->s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->s);
+    if (e != cudaSuccess) return -fail(ctx, MDB_ERR_CUDA, "rebuild check", e);
+    const int* h = ctx->h_cnt;
+    if (h[CP_BADBIN] > 0) return -fail(ctx, MDB_ERR_OVERFLOW, "atom outside the column grid");
+    if ((what & CHK_LIST) && h[CP_WINDOW] > 0)
+        return -fail(ctx, MDB_ERR_OVERFLOW, "more than 128 j-cluster candidates in one column");
+    if ((what & CHK_GHOSTS) && h[CP_NGC_TOTAL] > ctx->ngc_cap) {
+        int rc = alloc_ghosts(ctx, (int)(h[CP_NGC_TOTAL] * 1.2) + 1024);
+        if (rc) return -rc;
+        return 1;
+    }
+    if ((what & CHK_LIST) && h[CP_MAXNEED] >= ctx->maxneighs) {
+        // buildNeighborCPU: maxneighs = 1.2 x the longest row, then rebuild
+        int rc = alloc_list(ctx, (int)(h[CP_MAXNEED] * 1.2));
+        if (rc) return -rc;
+        return 1;
+    }
+    return 0;
+}
+
+static int do_build(MdbCp* ctx)
+{
+    for (int attempt = 0; attempt < 8; attempt++) {
+        long long m = mark();
+        enq_build(ctx);
+        account(ctx, m);
+        int r = check_build(ctx, CHK_ALL);
+        if (r < 0) return -r;
+        if (r == 0) {
+            ctx->have_clusters = ctx->have_ghosts = ctx->have_list = true;
+            return MDB_OK;
+        }
+    }
+    return fail(ctx, MDB_ERR_OVERFLOW, "rebuild did not converge");
+}
+
+static void enq_force(MdbCp* ctx, bool energy)
+{
+    cudaStream_t s = ctx->s;
+    const int nloc_slots = ctx->ncl_cap * ctx->M;
+    if (ctx->mixed) {
+        if (ctx->p.half_neigh)
+            cudaMemsetAsync(ctx->cf32, 0, sizeof(float4) * (size_t)nloc_slots, s);
+        launch_force_mixed(s, ctx->N, ctx->p.half_neigh, energy, ctx->ncl_cap, ctx->cnt, ctx->xr,
+            ctx->anchor, ctx->ty, (float)ctx->cutforcesq, ctx->list, lks(ctx), lcs(ctx),
+            ctx->numneigh, ctx->cf32, ctx->partials);
+        if (energy) ctx->energy_blocks = force_blocks(ctx->ncl_cap);
+    } else {
+        if (ctx->p.half_neigh)
+            cudaMemsetAsync(ctx->cf, 0, sizeof(double4) * (size_t)nloc_slots, s);
+        launch_force_fp64(s, ctx->M, ctx->N, ctx->p.half_neigh, energy, ctx->ncl_cap, ctx->cnt,
+            ctx->cx, ctx->ty, ctx->cutforcesq, ctx->list, lks(ctx), lcs(ctx), ctx->numneigh,
+            ctx->cf, ctx->partials);
+        if (energy) ctx->energy_blocks = mdb_blocks((long long)ctx->ncl_cap * 4, 128);
+    }
+}
+
+static void enq_initial(MdbCp* ctx)
+{
+    launch_cp_initial(ctx->s, ctx->M, ctx->N, ctx->ncl_cap, ctx->cnt, ctx->p.dtforce, ctx->p.dt,
+        ctx->cx, ctx->cv, ctx->cf, ctx->mixed ? ctx->cf32 : nullptr, ctx->anchor,
+        ctx->mixed ? ctx->xr : nullptr);
+}
+
+static void enq_final(MdbCp* ctx)
+{
+    launch_cp_final(ctx->s, ctx->M, ctx->ncl_cap, ctx->cnt, ctx->p.dtforce, ctx->cx, ctx->cv,
+        ctx->cf, ctx->mixed ? ctx->cf32 : nullptr);
+}
+
+static void enq_final_initial(MdbCp* ctx)
+{
+    launch_cp_final_initial(ctx->s, ctx->M, ctx->N, ctx->ncl_cap, ctx->cnt, ctx->p.dtforce,
+        ctx->p.dt, ctx->cx, ctx->cv, ctx->cf, ctx->mixed ? ctx->cf32 : nullptr, ctx->anchor,
+        ctx->mixed ? ctx->xr : nullptr);
+}
+
+static void enq_ghost_update(MdbCp* ctx)
+{
+    launch_ghost_update(ctx->s, ctx->N, ctx->ngc_cap, ctx->mixed, ctx->cnt, ctx->border,
+        ctx->pbc, ctx->jnat, ctx->g, ctx->cx, ctx->anchor, ctx->xr);
+}
+
+static void enq_prune(MdbCp* ctx)
+{
+    launch_prune(ctx->s, ctx->M, ctx->N, ctx->ncl_cap, ctx->cnt, ctx->cx, ctx->g.cutneighsq,
+        ctx->maxneighs, lks(ctx), lcs(ctx), ctx->list, ctx->numneigh, ctx->nmasked);
+}
+
+// T and P from the atom arrays (as computeThermo reads them), KE of the
+// cluster state, PE from the last energy evaluation
+static void enq_thermo(MdbCp* ctx, int slot, bool with_pe)
+{
+    cudaStream_t s = ctx->s;
+    double* r      = ctx->red + 4 * slot;
+    double* pk     = ctx->partials + ctx->npart;
+    launch_ke_atoms(s, ctx->nlocal, ctx->av, ctx->p.mass, pk);
+    launch_reduce_partials(s, ke_blocks(ctx->nlocal), pk, r + 0);
+    launch_ke_slots(s, ctx->M, ctx->ncl_cap, ctx->cnt, ctx->cx, ctx->cv, ctx->p.mass, pk);
+    launch_reduce_partials(s, ke_blocks(ctx->ncl_cap * ctx->M), pk, r + 2);
+    if (with_pe) launch_reduce_partials(s, ctx->energy_blocks, ctx->partials, r + 1);
+    else cudaMemsetAsync(r + 1, 0, sizeof(double), s);
+}
+
+static void finish_thermo(MdbCp* ctx, const double* r, int step, MdbThermo* out)
+{
+    out->step        = step;
+    double T         = r[0] * ctx->t_scale;
+    out->temperature = T;
+    out->pressure    = (T * ctx->dof_boltz) * ctx->p_scale;
+    out->ke          = 0.5 * r[2];
+    out->pe          = r[1];
+    out->etotal      = out->ke + out->pe;
+}
+
+// ---------------------------------------------------------------------------
+// hooks
+extern "C" int mdb_cp_build_clusters(MdbCp* ctx)
+{
+    NEED_ATOMS();
+    long long m = mark();
+    clear_build_counters(ctx);
+    enq_clusters(ctx);
+    account(ctx, m);
+    int r = check_build(ctx, CHK_CLUSTERS);
+    if (r < 0) return -r;
+    ctx->have_clusters = true;
+    ctx->have_ghosts = ctx->have_list = false;
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_define_jclusters(MdbCp* ctx)
+{
+    NEED_ATOMS();
+    if (!ctx->have_clusters) return fail(ctx, MDB_ERR_STATE, "buildClusters not run");
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_setup_pbc(MdbCp* ctx)
+{
+    NEED_ATOMS();
+    if (!ctx->have_clusters) return fail(ctx, MDB_ERR_STATE, "buildClusters not run");
+    for (int attempt = 0; attempt < 4; attempt++) {
+        long long m = mark();
+        enq_setup_pbc(ctx);
+        account(ctx, m);
+        int r = check_build(ctx, CHK_GHOSTS);
+        if (r < 0) return -r;
+        if (r == 0) {
+            ctx->have_ghosts = true;
+            return MDB_OK;
+        }
+        // ghost capacity grew: the slot arrays are new, rebuild the clusters
+        m = mark();
+        enq_clusters(ctx);
+        account(ctx, m);
+    }
+    return fail(ctx, MDB_ERR_OVERFLOW, "setupPbc did not converge");
+}
+
+extern "C" int mdb_cp_update_pbc(MdbCp* ctx)
+{
+    NEED_ATOMS();
+    if (!ctx->have_ghosts) return fail(ctx, MDB_ERR_STATE, "setupPbc not run");
+    long long m = mark();
+    enq_ghost_update(ctx);
+    account(ctx, m);
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_bin_jclusters(MdbCp* ctx)
+{
+    NEED_ATOMS();
+    if (!ctx->have_ghosts) return fail(ctx, MDB_ERR_STATE, "setupPbc not run");
+    long long m = mark();
+    enq_bin_j(ctx);
+    account(ctx, m);
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_build_neighbor(MdbCp* ctx)
+{
+    NEED_ATOMS();
+    if (!ctx->have_ghosts) return fail(ctx, MDB_ERR_STATE, "setupPbc not run");
+    for (int attempt = 0; attempt < 8; attempt++) {
+        long long m = mark();
+        clear_build_counters(ctx);
+        enq_list(ctx);
+        account(ctx, m);
+        int r = check_build(ctx, CHK_LIST);
+        if (r < 0) return -r;
+        if (r == 0) {
+            ctx->have_list = true;
+            return MDB_OK;
+        }
+        if (!ctx->have_ghosts) return do_build(ctx); // capacity change dropped the clusters
+    }
+    return fail(ctx, MDB_ERR_OVERFLOW, "buildNeighbor did not converge");
+}
+
+extern "C" int mdb_cp_prune_neighbor(MdbCp* ctx)
+{
+    NEED_ATOMS();
+    if (!ctx->have_list) return fail(ctx, MDB_ERR_STATE, "buildNeighbor not run");
+    long long m = mark();
+    enq_prune(ctx);
+    account(ctx, m);
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_update_single_atoms(MdbCp* ctx)
+{
+    NEED_ATOMS();
+    if (!ctx->have_clusters) return fail(ctx, MDB_ERR_STATE, "buildClusters not run");
+    long long m = mark();
+    enq_gather(ctx, 0);
+    account(ctx, m);
+    return MDB_OK;
+}
+
+__global__ void k_wrap_atoms(int n, double4* ax, double xprd, double yprd, double zprd)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double4 p = ax[i];
+    if (p.x < 0.0) p.x += xprd;
+    else if (p.x >= xprd) p.x -= xprd;
+    if (p.y < 0.0) p.y += yprd;
+    else if (p.y >= yprd) p.y -= yprd;
+    if (p.z < 0.0) p.z += zprd;
+    else if (p.z >= zprd) p.z -= zprd;
+    ax[i] = p;
+}
+
+extern "C" int mdb_cp_update_atoms_pbc(MdbCp* ctx)
+{
+    NEED_ATOMS();
+    k_wrap_atoms<<<mdb_blocks(ctx->nlocal, MDB_NTHREADS), MDB_NTHREADS, 0, ctx->s>>>(ctx->nlocal,
+        ctx->ax, ctx->p.xprd, ctx->p.yprd, ctx->p.zprd);
+    ctx->launches++;
+    CK(cudaGetLastError());
+    return MDB_OK;
+}
+
+static int compute_force(MdbCp* ctx, bool energy)
+{
+    NEED_ATOMS();
+    if (!ctx->have_list) return fail(ctx, MDB_ERR_STATE, "buildNeighbor not run");
+    long long m = mark();
+    enq_force(ctx, energy);
+    account(ctx, m);
+    CK(cudaGetLastError());
+    ctx->energy_valid = energy;
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_compute_force(MdbCp* ctx) { return compute_force(ctx, false); }
+extern "C" int mdb_cp_compute_force_energy(MdbCp* ctx) { return compute_force(ctx, true); }
+
+extern "C" int mdb_cp_initial_integrate(MdbCp* ctx)
+{
+    NEED_ATOMS();
+    if (!ctx->have_clusters) return fail(ctx, MDB_ERR_STATE, "buildClusters not run");
+    long long m = mark();
+    enq_initial(ctx);
+    account(ctx, m);
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_final_integrate(MdbCp* ctx)
+{
+    NEED_ATOMS();
+    if (!ctx->have_clusters) return fail(ctx, MDB_ERR_STATE, "buildClusters not run");
+    long long m = mark();
+    enq_final(ctx);
+    account(ctx, m);
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_thermo(MdbCp* ctx, MdbThermo* out)
+{
+    NEED_ATOMS();
+    if (!out) return MDB_ERR_ARG;
+    long long m = mark();
+    bool pe     = ctx->energy_valid && ctx->have_clusters;
+    if (ctx->have_clusters) {
+        enq_thermo(ctx, 0, pe);
+    } else {
+        double* pk = ctx->partials + ctx->npart;
+        launch_ke_atoms(ctx->s, ctx->nlocal, ctx->av, ctx->p.mass, pk);
+        launch_reduce_partials(ctx->s, ke_blocks(ctx->nlocal), pk, ctx->red);
+        cudaMemsetAsync(ctx->red + 1, 0, 3 * sizeof(double), ctx->s);
+    }
+    account(ctx, m);
+    CK(cudaMemcpyAsync(ctx->h_red, ctx->red, 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    finish_thermo(ctx, ctx->h_red, -1, out);
+    if (!pe) out->pe = out->etotal = NAN;
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_setup(MdbCp* ctx)
+{
+    NEED_ATOMS();
+    CK(cudaSetDevice(ctx->dev));
+    int rc = do_build(ctx);
+    if (rc) return rc;
+    return compute_force(ctx, true);
+}
+
+// A plain step whose predecessor left its final integration pending:
+// finalIntegrate(n-1) + initialIntegrate(n), updatePbc, force.
+static void enq_plain_step(MdbCp* ctx)
+{
+    enq_final_initial(ctx);
+    enq_ghost_update(ctx);
+    enq_force(ctx, false);
+}
+
+static int capture_plain(MdbCp* ctx)
+{
+    cudaGraph_t graph;
+    long long m0 = mark();
+    CK(cudaStreamBeginCapture(ctx->s, cudaStreamCaptureModeThreadLocal));
+    enq_plain_step(ctx);
+    cudaError_t e = cudaStreamEndCapture(ctx->s, &graph);
+    ctx->g_plain.kernels = mdb::g_launches - m0;
+    mdb::g_launches      = m0;
+    if (e != cudaSuccess) return fail(ctx, MDB_ERR_CUDA, "stream capture", e);
+    e = cudaGraphInstantiate(&ctx->g_plain.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(ctx, MDB_ERR_CUDA, "graph instantiate", e);
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_run(MdbCp* ctx, int first_step, int nsteps, MdbThermo* samples,
+    int max_samples, int* nsamples)
+{
+    NEED_ATOMS();
+    if (!ctx->have_list) return fail(ctx, MDB_ERR_STATE, "mdb_cp_setup not run");
+    if (nsteps < 0 || (max_samples > 0 && !samples)) return MDB_ERR_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    if (nsamples) *nsamples = 0;
+    int nslot = 0;
+    std::vector<int> slot_step;
+    const int last     = first_step + nsteps - 1;
+    bool pending_final = false;
+    for (int n = first_step; n <= last; n++) {
+        const bool reneigh = (n + 1) % ctx->p.reneigh_every == 0;
+        const bool prune   = !reneigh && (n + 1) % ctx->prune_every == 0;
+        const bool sample  = max_samples > 0 && (n + 1) % ctx->p.nstat == 0;
+        if (!reneigh && !prune && !sample && pending_final && n != last) {
+            if (!ctx->g_plain.exec) {
+                int rc = capture_plain(ctx);
+                if (rc) return rc;
+            }
+            CK(cudaGraphLaunch(ctx->g_plain.exec, ctx->s));
+            ctx->launches += ctx->g_plain.kernels;
+            continue;
+        }
+        long long m = mark();
+        if (pending_final) enq_final_initial(ctx);
+        else enq_initial(ctx);
+        pending_final = false;
+        account(ctx, m);
+        if (reneigh) {
+            // updateAtoms (updateSingleAtoms + updateAtomsPbc), then reneighbour
+            m = mark();
+            enq_gather(ctx, 1);
+            account(ctx, m);
+            int rc = do_build(ctx);
+            if (rc) return rc;
+        } else {
+            m = mark();
+            if (prune) enq_prune(ctx);
+            enq_ghost_update(ctx);
+            account(ctx, m);
+        }
+        m = mark();
+        enq_force(ctx, sample);
+        if (sample || n == last) enq_final(ctx);
+        else pending_final = true;
+        if (sample && nslot < RED_SLOTS && nslot < max_samples) {
+            enq_thermo(ctx, nslot, true);
+            slot_step.push_back(n + 1);
+            nslot++;
+        }
+        account(ctx, m);
+    }
+    if (pending_final) {
+        long long m = mark();
+        enq_final(ctx);
+        account(ctx, m);
+    }
+    ctx->energy_valid = nsteps > 0 && max_samples > 0 && ((last + 1) % ctx->p.nstat == 0);
+    CK(cudaGetLastError());
+    if (nslot > 0)
+        CK(cudaMemcpyAsync(ctx->h_red, ctx->red, 4 * sizeof(double) * nslot,
+            cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    for (int k = 0; k < nslot; k++)
+        finish_thermo(ctx, ctx->h_red + 4 * k, slot_step[k], &samples[k]);
+    if (nsamples) *nsamples = nslot;
+    return MDB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// introspection
+extern "C" int mdb_cp_get_counts(MdbCp* ctx, int* c)
+{
+    NEED_ATOMS();
+    if (!c) return MDB_ERR_ARG;
+    CK(cudaMemcpyAsync(ctx->h_cnt, ctx->cnt, CP_SLOTS * sizeof(int), cudaMemcpyDeviceToHost,
+        ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    const int* h = ctx->h_cnt;
+    c[0]         = ctx->nlocal;
+    c[1]         = ctx->p.natoms;
+    c[2]         = h[CP_NCL];
+    c[3]         = h[CP_NCJ];
+    c[4]         = h[CP_NGC];
+    c[5]         = h[CP_NGHOST_ATOMS];
+    c[6]         = h[CP_NCJ] + h[CP_NGC];
+    c[7]         = ctx->maxneighs;
+    return MDB_OK;
+}
+
+template <typename T>
+static int copy_back(MdbCp* ctx, std::vector<T>& h, const T* d, size_t n)
+{
+    h.resize(n);
+    if (n == 0) return MDB_OK;
+    CK(cudaMemcpyAsync(h.data(), d, sizeof(T) * n, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_get_slots(MdbCp* ctx, double* x, double* v, double* f, int* type, int nslots)
+{
+    NEED_ATOMS();
+    if (nslots < 0 || nslots > ctx->slot_cap) return MDB_ERR_ARG;
+    int c[8];
+    int rc = mdb_cp_get_counts(ctx, c);
+    if (rc) return rc;
+    const int nloc = c[2] * ctx->M;
+    std::vector<double4> hx, hv, hf;
+    std::vector<float4> hf32;
+    if ((rc = copy_back(ctx, hx, ctx->cx, nslots))) return rc;
+    if (v && (rc = copy_back(ctx, hv, ctx->cv, std::min(nslots, nloc)))) return rc;
+    if (f) {
+        if (ctx->mixed) rc = copy_back(ctx, hf32, ctx->cf32, std::min(nslots, nloc));
+        else rc = copy_back(ctx, hf, ctx->cf, std::min(nslots, nloc));
+        if (rc) return rc;
+    }
+    for (int s = 0; s < nslots; s++) {
+        if (x) {
+            x[3 * s] = hx[s].x, x[3 * s + 1] = hx[s].y, x[3 * s + 2] = hx[s].z;
+        }
+        if (type) {
+            long long t;
+            memcpy(&t, &hx[s].w, sizeof t);
+            type[s] = (int)t;
+        }
+        if (s < nloc) {
+            if (v) v[3 * s] = hv[s].x, v[3 * s + 1] = hv[s].y, v[3 * s + 2] = hv[s].z;
+            if (f && ctx->mixed)
+                f[3 * s] = hf32[s].x, f[3 * s + 1] = hf32[s].y, f[3 * s + 2] = hf32[s].z;
+            else if (f)
+                f[3 * s] = hf[s].x, f[3 * s + 1] = hf[s].y, f[3 * s + 2] = hf[s].z;
+        }
+    }
+    return MDB_OK;
+}
+
+static void bb_out(const double4& mn, const double4& mx, double* b)
+{
+    b[0] = mn.x, b[1] = mx.x, b[2] = mn.y, b[3] = mx.y, b[4] = mn.z, b[5] = mx.z;
+}
+
+extern "C" int mdb_cp_get_iclusters(MdbCp* ctx, int* natoms, int* bin, double* bb)
+{
+    NEED_ATOMS();
+    int c[8], rc = mdb_cp_get_counts(ctx, c);
+    if (rc) return rc;
+    const int n = c[2];
+    std::vector<int> hn, hb;
+    std::vector<double4> h0, h1;
+    if ((rc = copy_back(ctx, hn, ctx->inat, n)) || (rc = copy_back(ctx, hb, ctx->cbin, n)) ||
+        (rc = copy_back(ctx, h0, ctx->ibbmin, n)) || (rc = copy_back(ctx, h1, ctx->ibbmax, n)))
+        return rc;
+    for (int i = 0; i < n; i++) {
+        if (natoms) natoms[i] = hn[i];
+        if (bin) bin[i] = hb[i];
+        if (bb) bb_out(h0[i], h1[i], bb + 6 * i);
+    }
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_get_jclusters(MdbCp* ctx, int* natoms, double* bb, int count)
+{
+    NEED_ATOMS();
+    if (count < 0 || count > ctx->ncj_cap + ctx->ngc_cap) return MDB_ERR_ARG;
+    std::vector<int> hn;
+    std::vector<double4> h0, h1;
+    int rc;
+    if ((rc = copy_back(ctx, hn, ctx->jnat, count)) ||
+        (rc = copy_back(ctx, h0, ctx->jbbmin, count)) ||
+        (rc = copy_back(ctx, h1, ctx->jbbmax, count)))
+        return rc;
+    for (int i = 0; i < count; i++) {
+        if (natoms) natoms[i] = hn[i];
+        if (bb) bb_out(h0[i], h1[i], bb + 6 * i);
+    }
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_get_ghosts(MdbCp* ctx, int* border_map, int* pbc_xyz)
+{
+    NEED_ATOMS();
+    int c[8], rc = mdb_cp_get_counts(ctx, c);
+    if (rc) return rc;
+    std::vector<int> hb, hp;
+    if ((rc = copy_back(ctx, hb, ctx->border, c[4])) || (rc = copy_back(ctx, hp, ctx->pbc, c[4])))
+        return rc;
+    for (int g = 0; g < c[4]; g++) {
+        if (border_map) border_map[g] = hb[g];
+        if (pbc_xyz) {
+            pbc_xyz[3 * g]     = (hp[g] & 3) - 1;
+            pbc_xyz[3 * g + 1] = ((hp[g] >> 2) & 3) - 1;
+            pbc_xyz[3 * g + 2] = ((hp[g] >> 4) & 3) - 1;
+        }
+    }
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_get_neighbor_list(MdbCp* ctx, int* numneigh, int* nmasked, int* neighbors,
+    int ld)
+{
+    NEED_ATOMS();
+    if (!ctx->have_list) return fail(ctx, MDB_ERR_STATE, "buildNeighbor not run");
+    int c[8], rc = mdb_cp_get_counts(ctx, c);
+    if (rc) return rc;
+    const int n = c[2];
+    std::vector<int> hn, hm, hl;
+    if ((rc = copy_back(ctx, hn, ctx->numneigh, n)) || (rc = copy_back(ctx, hm, ctx->nmasked, n)))
+        return rc;
+    if (neighbors && (rc = copy_back(ctx, hl, ctx->list, (size_t)ctx->maxneighs * ctx->ld)))
+        return rc;
+    for (int i = 0; i < n; i++) {
+        if (numneigh) numneigh[i] = hn[i];
+        if (nmasked) nmasked[i] = hm[i];
+        if (neighbors)
+            for (int k = 0; k < hn[i] && k < ld; k++)
+                neighbors[(size_t)i * ld + k] =
+                    hl[(size_t)k * lks(ctx) + (size_t)i * lcs(ctx)];
+    }
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_get_columns(MdbCp* ctx, int* start, int* list, int cap)
+{
+    NEED_ATOMS();
+    const int mb = ctx->g.mbins;
+    std::vector<int> hs, hl;
+    int rc;
+    if ((rc = copy_back(ctx, hs, ctx->jcol_start, mb + 1))) return rc;
+    const int n = hs[mb];
+    if ((rc = copy_back(ctx, hl, ctx->jcol, n))) return rc;
+    if (start) memcpy(start, hs.data(), sizeof(int) * (mb + 1));
+    if (list)
+        for (int i = 0; i < n && i < cap; i++)
+            list[i] = hl[i];
+    return n;
+}
+
+extern "C" int mdb_cp_get_geometry(MdbCp* ctx, int* ints, double* dbls, int* stencil,
+    int max_stencil)
+{
+    if (!ctx) return MDB_ERR_ARG;
+    const Geom& g = ctx->g;
+    if (ints) {
+        ints[0] = g.nbinx, ints[1] = g.nbiny, ints[2] = g.mbinx, ints[3] = g.mbiny;
+        ints[4] = g.mbinxlo, ints[5] = g.mbinylo, ints[6] = g.nstencil;
+    }
+    if (dbls) dbls[0] = g.binsizex, dbls[1] = g.binsizey, dbls[2] = g.rbb_sq;
+    if (stencil)
+        for (int k = 0; k < g.nstencil && k < max_stencil; k++)
+            stencil[k] = ctx->stencil[k];
+    return MDB_OK;
+}

@@ -1,0 +1,909 @@
+// Cluster-pair scheme, the rebuild path: updateSingleAtoms/updateAtomsPbc,
+// binAtoms + sortAtomsByZCoord + buildClusters + defineJClusters, setupPbc +
+// updatePbc, binJClusters and buildNeighbor (4xN, bounding-box pruned), plus
+// pruneNeighbor. Every result is the reference's, bit for bit: the same FP64
+// expressions in the same order, and the same orders of atoms in columns, of
+// j-clusters in columns and of entries in the lists.
+#include <math.h>
+
+#include "mdb_cp_internal.cuh"
+
+namespace mdb {
+namespace cp {
+
+static __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+// ---- updateSingleAtoms + updateAtomsPbc --------------------------------------
+// clusterpair/neighbor.c:2096-2149 (slot -> atom index = atoms of the clusters
+// before it) and clusterpair/pbc.c:116-143 (wrap into the box)
+__global__ void k_gather(int M, const int* __restrict__ cnt, const double4* __restrict__ cx,
+    const double4* __restrict__ cv, const int* __restrict__ cl_first, double4* __restrict__ ax,
+    double4* __restrict__ av, int wrap, double xprd, double yprd, double zprd)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= cnt[CP_NCL] * M) return;
+    double4 p = cx[s];
+    if (slot_type(p) < 0) return;
+    const int a = cl_first[s / M] + s % M;
+    if (wrap) {
+        if (p.x < 0.0) p.x += xprd;
+        else if (p.x >= xprd) p.x -= xprd;
+        if (p.y < 0.0) p.y += yprd;
+        else if (p.y >= yprd) p.y -= yprd;
+        if (p.z < 0.0) p.z += zprd;
+        else if (p.z >= zprd) p.z -= zprd;
+    }
+    ax[a] = p;
+    av[a] = cv[s];
+}
+
+void launch_gather(cudaStream_t s, int M, int ncl_cap, const int* cnt, const double4* cx,
+    const double4* cv, const int* cl_first, double4* ax, double4* av, int wrap, double xprd,
+    double yprd, double zprd)
+{
+    long long n = (long long)ncl_cap * M;
+    k_gather<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(M, cnt, cx, cv, cl_first, ax,
+        av, wrap, xprd, yprd, zprd);
+    g_launches++;
+}
+
+// ---- binAtoms (clusterpair/neighbor.c:1409-1449) -----------------------------
+__global__ void k_bin_atoms(int n, const double4* __restrict__ ax, Geom g, int* atom_col,
+    int* col_count, int* cnt)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double4 p = ax[i];
+    int ix, iy;
+    coord2bin2d(g, p.x, p.y, ix, iy);
+    int b = iy * g.mbinx + ix + 1;
+    if (b < 0 || b >= g.mbins) {
+        atomicAdd(&cnt[CP_BADBIN], 1);
+        atom_col[i] = -1;
+        return;
+    }
+    atom_col[i] = b;
+    atomicAdd(&col_count[b], 1);
+}
+
+void launch_bin_atoms(cudaStream_t s, int n, const double4* ax, const Geom& g, int* atom_col,
+    int* col_count, int* cnt)
+{
+    if (n <= 0) return;
+    k_bin_atoms<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(n, ax, g, atom_col,
+        col_count, cnt);
+    g_launches++;
+}
+
+__global__ void k_scatter_atoms(int n, const int* __restrict__ atom_col,
+    const int* __restrict__ col_start, int* col_fill, int* col_atoms)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int b = atom_col[i];
+    if (b < 0) return;
+    col_atoms[col_start[b] + atomicAdd(&col_fill[b], 1)] = i;
+}
+
+void launch_scatter_atoms(cudaStream_t s, int n, const int* atom_col, const int* col_start,
+    int* col_fill, int* col_atoms)
+{
+    if (n <= 0) return;
+    k_scatter_atoms<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(n, atom_col, col_start,
+        col_fill, col_atoms);
+    g_launches++;
+}
+
+// ---- sortAtomsByZCoord (clusterpair/neighbor.c:1452-1481) ----------------------
+// One warp per column. The column's atoms arrive in arbitrary order from the
+// atomic scatter; a bitonic sort by atom index restores binAtoms' order (atoms
+// appended in index order). The reference then runs a selection sort that, for
+// each position a, swaps in the first minimum of z among positions a..c-1.
+// Without equal z values the result is the unique ascending order, which a
+// bitonic sort by z gives directly. Equal z values (a perfect lattice) make the
+// result depend on the swaps: such columns go back to index order and the warp
+// replays the selection sort exactly, each step a warp-wide (z, position)
+// minimum and one swap.
+template <bool BY_Z>
+__device__ void bitonic(int* idx, double* z, int P)
+{
+    const int lane = lane_id();
+    for (int size = 2; size <= P; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int t = lane; t < (P >> 1); t += 32) {
+                int i   = 2 * t - (t & (stride - 1));
+                int j   = i + stride;
+                bool up = (i & size) == 0;
+                int a = idx[i], b = idx[j];
+                double za = z[i], zb = z[j];
+                bool gt = BY_Z ? (za > zb || (za == zb && a > b)) : (a > b);
+                if (gt == up) {
+                    idx[i] = b;
+                    idx[j] = a;
+                    z[i]   = zb;
+                    z[j]   = za;
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+__device__ void sort_column(int* idx, double* z, int c, int P, const double4* __restrict__ ax)
+{
+    const int lane = lane_id();
+    for (int k = lane; k < P; k += 32) {
+        if (k >= c) idx[k] = 0x7fffffff;
+        z[k] = k < c ? ax[idx[k]].z : INFINITY;
+    }
+    __syncwarp();
+    bitonic<true>(idx, z, P);
+    bool tie = false;
+    for (int k = lane; k + 1 < c; k += 32)
+        tie |= z[k] == z[k + 1];
+    if (!__any_sync(0xffffffffu, tie)) return;
+    // equal z: back to binAtoms' order, then replay the selection sort
+    bitonic<false>(idx, z, P);
+    for (int a = 0; a < c; a++) {
+        double bz = INFINITY;
+        int bp    = 0x7fffffff;
+        for (int p = a + lane; p < c; p += 32) {
+            double zp = z[p];
+            if (zp < bz || bp == 0x7fffffff) {
+                bz = zp;
+                bp = p;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            double oz = __shfl_xor_sync(0xffffffffu, bz, o);
+            int op    = __shfl_xor_sync(0xffffffffu, bp, o);
+            if (op != 0x7fffffff && (bp == 0x7fffffff || oz < bz || (oz == bz && op < bp))) {
+                bz = oz;
+                bp = op;
+            }
+        }
+        if (lane == 0 && bp != a) {
+            int ta = idx[a];
+            idx[a] = idx[bp];
+            idx[bp] = ta;
+            double tz = z[a];
+            z[a]      = z[bp];
+            z[bp]     = tz;
+        }
+        __syncwarp();
+    }
+}
+
+#define CP_SORT_WARPS 4
+
+__global__ void __launch_bounds__(32 * CP_SORT_WARPS) k_sort_columns(int mbins, int M, int N,
+    const int* __restrict__ col_start, int* col_atoms, const double4* __restrict__ ax,
+    int* col_sorted, int* gidx, double* gz, int* ncl_col)
+{
+    __shared__ int s_idx[CP_SORT_WARPS][CP_COL_SMEM];
+    __shared__ double s_z[CP_SORT_WARPS][CP_COL_SMEM];
+    const int w    = threadIdx.x >> 5;
+    const int b    = blockIdx.x * CP_SORT_WARPS + w;
+    const int lane = lane_id();
+    if (b >= mbins) return;
+    const int start = col_start[b];
+    const int c     = col_start[b + 1] - start;
+    int P           = 1;
+    while (P < c) P <<= 1;
+    int* idx;
+    double* z;
+    if (P <= CP_COL_SMEM) {
+        idx = s_idx[w];
+        z   = s_z[w];
+    } else {
+        // 2 * start leaves room for the power-of-two padding of every column
+        idx = gidx + 2 * (size_t)start;
+        z   = gz + 2 * (size_t)start;
+    }
+    for (int k = lane; k < c; k += 32)
+        idx[k] = col_atoms[start + k];
+    __syncwarp();
+    if (c > 0) sort_column(idx, z, c, P, ax);
+    for (int k = lane; k < c; k += 32)
+        col_sorted[start + k] = idx[k];
+    if (lane == 0) {
+        int nc = (c + M - 1) / M;
+        if (N > M && (nc & 1)) nc++;
+        ncl_col[b] = nc;
+    }
+}
+
+void launch_sort_columns(cudaStream_t s, const Geom& g, int M, int N, const int* col_start,
+    int* col_atoms, const double4* ax, int* col_sorted, int* gidx, double* gz, int* ncl_col)
+{
+    // gidx / gz: 2 * nlocal entries each, used by columns longer than CP_COL_SMEM
+    int blocks = (g.mbins + CP_SORT_WARPS - 1) / CP_SORT_WARPS;
+    k_sort_columns<<<blocks, 32 * CP_SORT_WARPS, 0, s>>>(g.mbins, M, N, col_start, col_atoms, ax,
+        col_sorted, gidx, gz, ncl_col);
+    g_launches++;
+}
+
+// ---- buildClustersCPU + defineJClusters (clusterpair/neighbor.c:1513-1611, :1807-1915)
+// One warp per column: slots filled from the z-sorted column in chunks of M
+// (padding +INF, type -1), then per cluster its atom count, column and bounding
+// box with the reference's compare-and-replace order, then the j-cluster boxes
+// (M < N: the union of the two i-clusters of a pair). Mixed path: anchors and
+// anchor-relative FP32 positions.
+__device__ __forceinline__ float4 anchor_of(const double4& mn, const double4& mx)
+{
+    const double st = CP_ANCHOR_STEP;
+    float4 a;
+    a.x = (float)(rint(0.5 * (mn.x + mx.x) / st) * st);
+    a.y = (float)(rint(0.5 * (mn.y + mx.y) / st) * st);
+    a.z = (float)(rint(0.5 * (mn.z + mx.z) / st) * st);
+    a.w = 0.0f;
+    return a;
+}
+
+__device__ __forceinline__ float4 rel_slot(const double4& p, const float4& a)
+{
+    if (slot_type(p) < 0) return make_float4(CP_PAD_F, CP_PAD_F, CP_PAD_F, __int_as_float(-1));
+    return make_float4((float)(p.x - (double)a.x), (float)(p.y - (double)a.y),
+        (float)(p.z - (double)a.z), __int_as_float(slot_type(p)));
+}
+
+__device__ __forceinline__ void zext_max(unsigned long long* zext, double e)
+{
+    // non-negative doubles order like their bit patterns
+    unsigned long long v = (unsigned long long)__double_as_longlong(e > 0.0 ? e : 0.0);
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long u = __shfl_xor_sync(0xffffffffu, v, o);
+        v                    = u > v ? u : v;
+    }
+    if (lane_id() == 0) atomicMax(zext, v);
+}
+
+template <int M, int N>
+__global__ void k_build_clusters(int mbins, int mixed, const int* __restrict__ col_start,
+    const int* __restrict__ col_sorted, const int* __restrict__ cl_start,
+    const double4* __restrict__ ax, const double4* __restrict__ av, double4* cx, double4* cv,
+    int* inat, int* cbin, int* cl_first, double4* ibbmin, double4* ibbmax, int* jnat,
+    double4* jbbmin, double4* jbbmax, float4* anchor, float4* xr, int* cnt,
+    unsigned long long* zext)
+{
+    const int b    = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = lane_id();
+    if (b == 0 && lane == 0) {
+        cnt[CP_NCL] = cl_start[mbins];
+        cnt[CP_NCJ] = cl_start[mbins] / (N / M);
+    }
+    if (b >= mbins) return;
+    const int start = col_start[b];
+    const int c     = col_start[b + 1] - start;
+    const int k0    = cl_start[b];
+    const int nclu  = cl_start[b + 1] - k0;
+    for (int j = lane; j < nclu * M; j += 32) {
+        const int slot = k0 * M + j;
+        if (j < c) {
+            int i     = col_sorted[start + j];
+            cx[slot]  = ax[i];
+            cv[slot]  = av[i];
+        } else {
+            cx[slot] = make_double4(INFINITY, INFINITY, INFINITY, type_bits(-1));
+            cv[slot] = make_double4(0.0, 0.0, 0.0, 0.0);
+        }
+    }
+    __syncwarp();
+    double ext = 0.0;
+    for (int k = lane; k < nclu; k += 32) {
+        const int ci = k0 + k;
+        int nat      = c - k * M;
+        nat          = nat < 0 ? 0 : (nat > M ? M : nat);
+        double4 mn   = make_double4(INFINITY, INFINITY, INFINITY, 0.0);
+        double4 mx   = make_double4(-INFINITY, -INFINITY, -INFINITY, 0.0);
+        for (int a = 0; a < nat; a++) {
+            double4 p = cx[ci * M + a];
+            if (mn.x > p.x) mn.x = p.x;
+            if (mx.x < p.x) mx.x = p.x;
+            if (mn.y > p.y) mn.y = p.y;
+            if (mx.y < p.y) mx.y = p.y;
+            if (mn.z > p.z) mn.z = p.z;
+            if (mx.z < p.z) mx.z = p.z;
+        }
+        inat[ci]     = nat;
+        cbin[ci]     = b;
+        cl_first[ci] = start + k * M;
+        ibbmin[ci]   = mn;
+        ibbmax[ci]   = mx;
+        if (N == M) {
+            jnat[ci]   = nat;
+            jbbmin[ci] = mn;
+            jbbmax[ci] = mx;
+            if (nat > 0 && mx.z - mn.z > ext) ext = mx.z - mn.z;
+        }
+    }
+    __syncwarp();
+    if (N == 2 * M) {
+        for (int kk = lane; kk < (nclu >> 1); kk += 32) {
+            const int ci = k0 + 2 * kk, cj = ci >> 1;
+            double4 a0 = ibbmin[ci], a1 = ibbmax[ci], b0 = ibbmin[ci + 1], b1 = ibbmax[ci + 1];
+            double4 mn, mx;
+            mn.x = a0.x < b0.x ? a0.x : b0.x;
+            mx.x = a1.x > b1.x ? a1.x : b1.x;
+            mn.y = a0.y < b0.y ? a0.y : b0.y;
+            mx.y = a1.y > b1.y ? a1.y : b1.y;
+            mn.z = a0.z < b0.z ? a0.z : b0.z;
+            mx.z = a1.z > b1.z ? a1.z : b1.z;
+            mn.w = mx.w = 0.0;
+            jbbmin[cj] = mn;
+            jbbmax[cj] = mx;
+            jnat[cj]   = inat[ci] + inat[ci + 1];
+            if (mx.z - mn.z > ext) ext = mx.z - mn.z;
+        }
+        __syncwarp();
+    }
+    zext_max(zext, ext);
+    if (mixed) {
+        const int jfac = N / M;
+        const int j0 = k0 / jfac, nj = nclu / jfac;
+        for (int k = lane; k < nj; k += 32)
+            anchor[j0 + k] = anchor_of(jbbmin[j0 + k], jbbmax[j0 + k]);
+        __syncwarp();
+        for (int j = lane; j < nclu * M; j += 32) {
+            const int slot = k0 * M + j;
+            xr[slot]       = rel_slot(cx[slot], anchor[slot / N]);
+        }
+    }
+}
+
+void launch_build_clusters(cudaStream_t s, const Geom& g, int M, int N, int mixed,
+    const int* col_start, const int* col_sorted, const int* cl_start, const double4* ax,
+    const double4* av, double4* cx, double4* cv, int* inat, int* cbin, int* cl_first,
+    double4* ibbmin, double4* ibbmax, int* jnat, double4* jbbmin, double4* jbbmax,
+    float4* anchor, float4* xr, int* cnt, unsigned long long* zext)
+{
+    long long threads = (long long)g.mbins * 32;
+    int blocks        = mdb_blocks(threads, 128);
+    if (N == 4)
+        k_build_clusters<4, 4><<<blocks, 128, 0, s>>>(g.mbins, mixed, col_start, col_sorted,
+            cl_start, ax, av, cx, cv, inat, cbin, cl_first, ibbmin, ibbmax, jnat, jbbmin, jbbmax,
+            anchor, xr, cnt, zext);
+    else
+        k_build_clusters<4, 8><<<blocks, 128, 0, s>>>(g.mbins, mixed, col_start, col_sorted,
+            cl_start, ax, av, cx, cv, inat, cbin, cl_first, ibbmin, ibbmax, jnat, jbbmin, jbbmax,
+            anchor, xr, cnt, zext);
+    g_launches++;
+}
+
+// ---- setupPbc (clusterpair/pbc.c:184-331) -------------------------------------
+// The 26 images of a j-cluster in the reference's order: 6 faces, 8 corners,
+// 12 edges, each present when the box is within cutneigh of that side.
+__device__ __forceinline__ int ghost_images(const double4& mn, const double4& mx, const Geom& g,
+    int* codes)
+{
+    const double cut = g.cutneigh;
+    const bool lx = mn.x < cut, hx = mx.x >= (g.xprd - cut);
+    const bool ly = mn.y < cut, hy = mx.y >= (g.yprd - cut);
+    const bool lz = mn.z < cut, hz = mx.z >= (g.zprd - cut);
+    int n = 0;
+#define CP_IMG(c, dx, dy, dz)                                                            \
+    if (c) {                                                                             \
+        if (codes) codes[n] = ((dx) + 1) | (((dy) + 1) << 2) | (((dz) + 1) << 4);        \
+        n++;                                                                             \
+    }
+    CP_IMG(lx, +1, 0, 0)
+    CP_IMG(hx, -1, 0, 0)
+    CP_IMG(ly, 0, +1, 0)
+    CP_IMG(hy, 0, -1, 0)
+    CP_IMG(lz, 0, 0, +1)
+    CP_IMG(hz, 0, 0, -1)
+    CP_IMG(lx && ly && lz, +1, +1, +1)
+    CP_IMG(lx && hy && lz, +1, -1, +1)
+    CP_IMG(lx && ly && hz, +1, +1, -1)
+    CP_IMG(lx && hy && hz, +1, -1, -1)
+    CP_IMG(hx && ly && lz, -1, +1, +1)
+    CP_IMG(hx && hy && lz, -1, -1, +1)
+    CP_IMG(hx && ly && hz, -1, +1, -1)
+    CP_IMG(hx && hy && hz, -1, -1, -1)
+    CP_IMG(lx && lz, +1, 0, +1)
+    CP_IMG(lx && hz, +1, 0, -1)
+    CP_IMG(hx && lz, -1, 0, +1)
+    CP_IMG(hx && hz, -1, 0, -1)
+    CP_IMG(ly && lz, 0, +1, +1)
+    CP_IMG(ly && hz, 0, +1, -1)
+    CP_IMG(hy && lz, 0, -1, +1)
+    CP_IMG(hy && hz, 0, -1, -1)
+    CP_IMG(ly && lx, +1, +1, 0)
+    CP_IMG(ly && hx, -1, +1, 0)
+    CP_IMG(hy && lx, +1, -1, 0)
+    CP_IMG(hy && hx, -1, -1, 0)
+#undef CP_IMG
+    return n;
+}
+
+__global__ void k_ghost_count(int ncj_cap, const int* __restrict__ cnt,
+    const int* __restrict__ jnat, const double4* __restrict__ jbbmin,
+    const double4* __restrict__ jbbmax, Geom g, int* gcount)
+{
+    const int cj = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cj >= ncj_cap) return;
+    int n = 0;
+    if (cj < cnt[CP_NCJ] && jnat[cj] > 0) n = ghost_images(jbbmin[cj], jbbmax[cj], g, nullptr);
+    gcount[cj] = n;
+}
+
+void launch_ghost_count(cudaStream_t s, int ncj_cap, const int* cnt, const int* jnat,
+    const double4* jbbmin, const double4* jbbmax, const Geom& g, int* gcount)
+{
+    k_ghost_count<<<mdb_blocks(ncj_cap, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(ncj_cap, cnt, jnat,
+        jbbmin, jbbmax, g, gcount);
+    g_launches++;
+}
+
+__global__ void k_ghost_write(int ncj_cap, int ngc_cap, int* cnt, const int* __restrict__ jnat,
+    const double4* __restrict__ jbbmin, const double4* __restrict__ jbbmax, Geom g,
+    const int* __restrict__ gstart, int* border, int* pbc)
+{
+    const int cj = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cj == 0) {
+        int total          = gstart[ncj_cap];
+        cnt[CP_NGC_TOTAL]  = total;
+        cnt[CP_NGC]        = total < ngc_cap ? total : ngc_cap;
+    }
+    if (cj >= ncj_cap || cj >= cnt[CP_NCJ] || jnat[cj] <= 0) return;
+    int codes[26];
+    int n  = ghost_images(jbbmin[cj], jbbmax[cj], g, codes);
+    int g0 = gstart[cj];
+    for (int k = 0; k < n; k++) {
+        if (g0 + k >= ngc_cap) break;
+        border[g0 + k] = cj;
+        pbc[g0 + k]    = codes[k];
+    }
+}
+
+void launch_ghost_write(cudaStream_t s, int ncj_cap, int ngc_cap, int* cnt, const int* jnat,
+    const double4* jbbmin, const double4* jbbmax, const Geom& g, const int* gstart, int* border,
+    int* pbc)
+{
+    k_ghost_write<<<mdb_blocks(ncj_cap, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(ncj_cap, ngc_cap,
+        cnt, jnat, jbbmin, jbbmax, g, gstart, border, pbc);
+    g_launches++;
+}
+
+// updatePbcCPU(first = 1), clusterpair/pbc.c:43-113: ghost positions, padding,
+// boxes; one thread per ghost j-cluster, plus one for the dummy cluster
+__global__ void k_ghost_first(int N, int* cnt, const int* __restrict__ border,
+    const int* __restrict__ pbc, int mixed, Geom g, double4* cx, int* jnat, double4* jbbmin,
+    double4* jbbmax, float4* anchor, float4* xr, unsigned long long* zext)
+{
+    const int gi  = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ngc = cnt[CP_NGC], ncj = cnt[CP_NCJ];
+    double ext    = 0.0;
+    if (gi < ngc) {
+        const int cg = ncj + gi, o = border[gi], code = pbc[gi];
+        const double sx = (double)((code & 3) - 1) * g.xprd;
+        const double sy = (double)(((code >> 2) & 3) - 1) * g.yprd;
+        const double sz = (double)(((code >> 4) & 3) - 1) * g.zprd;
+        const int nat   = jnat[o];
+        jnat[cg]        = nat;
+        atomicAdd(&cnt[CP_NGHOST_ATOMS], nat);
+        double4 mn = make_double4(INFINITY, INFINITY, INFINITY, 0.0);
+        double4 mx = make_double4(-INFINITY, -INFINITY, -INFINITY, 0.0);
+        for (int k = 0; k < N; k++) {
+            double4 q;
+            if (k < nat) {
+                double4 p = cx[o * N + k];
+                q         = make_double4(p.x + sx, p.y + sy, p.z + sz, p.w);
+                if (mn.x > q.x) mn.x = q.x;
+                if (mx.x < q.x) mx.x = q.x;
+                if (mn.y > q.y) mn.y = q.y;
+                if (mx.y < q.y) mx.y = q.y;
+                if (mn.z > q.z) mn.z = q.z;
+                if (mx.z < q.z) mx.z = q.z;
+            } else {
+                q = make_double4(INFINITY, INFINITY, INFINITY, type_bits(-1));
+            }
+            cx[cg * N + k] = q;
+        }
+        jbbmin[cg] = mn;
+        jbbmax[cg] = mx;
+        if (nat > 0) ext = mx.z - mn.z;
+        if (mixed) {
+            float4 a   = anchor_of(mn, mx);
+            anchor[cg] = a;
+            for (int k = 0; k < N; k++)
+                xr[cg * N + k] = rel_slot(cx[cg * N + k], a);
+        }
+    } else if (gi == ngc) {
+        const int cd = ncj + ngc; // dummy cluster
+        for (int k = 0; k < N; k++) {
+            cx[cd * N + k] = make_double4(INFINITY, INFINITY, INFINITY, type_bits(-1));
+            if (mixed)
+                xr[cd * N + k] = make_float4(CP_PAD_F, CP_PAD_F, CP_PAD_F, __int_as_float(-1));
+        }
+        if (mixed) anchor[cd] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    zext_max(zext, ext);
+}
+
+void launch_ghost_first(cudaStream_t s, int N, int ngc_cap, int mixed, int* cnt,
+    const int* border, const int* pbc, const Geom& g, double4* cx, int* jnat, double4* jbbmin,
+    double4* jbbmax, float4* anchor, float4* xr, unsigned long long* zext)
+{
+    k_ghost_first<<<mdb_blocks(ngc_cap + 1, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(N, cnt, border,
+        pbc, mixed, g, cx, jnat, jbbmin, jbbmax, anchor, xr, zext);
+    g_launches++;
+}
+
+// updatePbcCPU(first = 0): ghost positions from their owners every step
+__global__ void k_ghost_update(int N, int mixed, const int* __restrict__ cnt,
+    const int* __restrict__ border, const int* __restrict__ pbc, const int* __restrict__ jnat,
+    Geom g, double4* cx, const float4* __restrict__ anchor, float4* xr)
+{
+    const int s  = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gi = s / N, k = s - gi * N;
+    if (gi >= cnt[CP_NGC]) return;
+    const int cg = cnt[CP_NCJ] + gi;
+    if (k >= jnat[cg]) return;
+    const int code = pbc[gi];
+    double4 p      = cx[border[gi] * N + k];
+    p.x += (double)((code & 3) - 1) * g.xprd;
+    p.y += (double)(((code >> 2) & 3) - 1) * g.yprd;
+    p.z += (double)(((code >> 4) & 3) - 1) * g.zprd;
+    cx[cg * N + k] = p;
+    if (mixed) xr[cg * N + k] = rel_slot(p, anchor[cg]);
+}
+
+void launch_ghost_update(cudaStream_t s, int N, int ngc_cap, int mixed, const int* cnt,
+    const int* border, const int* pbc, const int* jnat, const Geom& g, double4* cx,
+    const float4* anchor, float4* xr)
+{
+    long long n = (long long)ngc_cap * N;
+    k_ghost_update<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(N, mixed, cnt, border, pbc,
+        jnat, g, cx, anchor, xr);
+    g_launches++;
+}
+
+// ---- binJClusters (clusterpair/neighbor.c:1917-2094) ------------------------------
+// Ghost j-clusters go to the column of their innermost atom (per image
+// direction, indexes clamped to the grid) and are inserted before the first
+// entry with a larger bbminz. Local j-clusters come first in cluster order and
+// are already ordered by bbminz, so the final column is the stable merge of the
+// locals and of the ghosts sorted by (bbminz, index).
+__global__ void k_ghost_columns(int N, const int* __restrict__ cnt, const int* __restrict__ pbc,
+    const int* __restrict__ jnat, const double4* __restrict__ cx, Geom g, int* gcolumn,
+    int* gcol_count)
+{
+    const int gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= cnt[CP_NGC]) return;
+    const int cg = cnt[CP_NCJ] + gi, code = pbc[gi];
+    const int dx = (code & 3) - 1, dy = ((code >> 2) & 3) - 1;
+    int ix, iy;
+    double4 p = cx[cg * N];
+    coord2bin2d(g, p.x, p.y, ix, iy);
+    ix = max(min(ix, g.mbinx - 1), 0);
+    iy = max(min(iy, g.mbiny - 1), 0);
+    for (int k = 1; k < jnat[cg]; k++) {
+        int nix, niy;
+        p = cx[cg * N + k];
+        coord2bin2d(g, p.x, p.y, nix, niy);
+        nix = max(min(nix, g.mbinx - 1), 0);
+        niy = max(min(niy, g.mbiny - 1), 0);
+        if (dx > 0 && ix > nix) ix = nix;
+        if (dx < 0 && ix < nix) ix = nix;
+        if (dy > 0 && iy > niy) iy = niy;
+        if (dy < 0 && iy < niy) iy = niy;
+    }
+    int b       = iy * g.mbinx + ix + 1;
+    gcolumn[gi] = b;
+    atomicAdd(&gcol_count[b], 1);
+}
+
+void launch_ghost_columns(cudaStream_t s, int N, int ngc_cap, const int* cnt, const int* pbc,
+    const int* jnat, const double4* cx, const Geom& g, int* gcolumn, int* gcol_count)
+{
+    k_ghost_columns<<<mdb_blocks(ngc_cap, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(N, cnt, pbc, jnat,
+        cx, g, gcolumn, gcol_count);
+    g_launches++;
+}
+
+__global__ void k_column_sizes(int mbins1, int jfac, const int* __restrict__ ncl_col,
+    const int* __restrict__ gcol_count, int* jcol_n)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < mbins1) jcol_n[b] = ncl_col[b] / jfac + gcol_count[b];
+}
+
+void launch_column_sizes(cudaStream_t s, int mbins1, int jfac, const int* ncl_col,
+    const int* gcol_count, int* jcol_n)
+{
+    k_column_sizes<<<mdb_blocks(mbins1, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(mbins1, jfac, ncl_col,
+        gcol_count, jcol_n);
+    g_launches++;
+}
+
+__global__ void k_ghost_scatter(const int* __restrict__ cnt, const int* __restrict__ gcolumn,
+    const int* __restrict__ jcol_start, const int* __restrict__ ncl_col, int jfac, int* gfill,
+    int* gtmp)
+{
+    const int gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= cnt[CP_NGC]) return;
+    const int b = gcolumn[gi];
+    gtmp[jcol_start[b] + ncl_col[b] / jfac + atomicAdd(&gfill[b], 1)] = cnt[CP_NCJ] + gi;
+}
+
+void launch_ghost_scatter(cudaStream_t s, int ngc_cap, const int* cnt, const int* gcolumn,
+    const int* jcol_start, const int* ncl_col, int jfac, int* gfill, int* gtmp)
+{
+    k_ghost_scatter<<<mdb_blocks(ngc_cap, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(cnt, gcolumn,
+        jcol_start, ncl_col, jfac, gfill, gtmp);
+    g_launches++;
+}
+
+__global__ void k_merge_columns(int mbins1, int jfac, const int* __restrict__ ncl_col,
+    const int* __restrict__ cl_start, const int* __restrict__ gcol_count,
+    const int* __restrict__ jcol_start, const int* __restrict__ gtmp,
+    const double4* __restrict__ jbbmin, const double4* __restrict__ jbbmax, int* jcol,
+    double4* jcbbmin, double4* jcbbmax)
+{
+    const int b    = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = lane_id();
+    if (b >= mbins1) return;
+    const int start = jcol_start[b];
+    const int nl = ncl_col[b] / jfac, ng = gcol_count[b];
+    const int cj0 = b < mbins1 - 1 ? cl_start[b] / jfac : 0;
+    const int* gl = gtmp + start + nl;
+    for (int i = lane; i < nl; i += 32) {
+        const double key = jbbmin[cj0 + i].z;
+        int before       = 0;
+        for (int e = 0; e < ng; e++)
+            before += jbbmin[gl[e]].z < key;
+        const int m = start + i + before;
+        jcol[m]     = cj0 + i;
+        jcbbmin[m]  = jbbmin[cj0 + i];
+        jcbbmax[m]  = jbbmax[cj0 + i];
+    }
+    for (int e = lane; e < ng; e += 32) {
+        const int gj     = gl[e];
+        const double key = jbbmin[gj].z;
+        int pos          = 0;
+        for (int i = 0; i < nl; i++)
+            pos += jbbmin[cj0 + i].z <= key;
+        for (int f = 0; f < ng; f++) {
+            const int gf  = gl[f];
+            const double kf = jbbmin[gf].z;
+            pos += kf < key || (kf == key && gf < gj);
+        }
+        jcol[start + pos]    = gj;
+        jcbbmin[start + pos] = jbbmin[gj];
+        jcbbmax[start + pos] = jbbmax[gj];
+    }
+}
+
+void launch_merge_columns(cudaStream_t s, int mbins1, int jfac, const int* ncl_col,
+    const int* cl_start, const int* gcol_count, const int* jcol_start, const int* gtmp,
+    const double4* jbbmin, const double4* jbbmax, int* jcol, double4* jcbbmin, double4* jcbbmax)
+{
+    long long threads = (long long)mbins1 * 32;
+    k_merge_columns<<<mdb_blocks(threads, 128), 128, 0, s>>>(mbins1, jfac, ncl_col, cl_start,
+        gcol_count, jcol_start, gtmp, jbbmin, jbbmax, jcol, jcbbmin, jcbbmax);
+    g_launches++;
+}
+
+// ---- buildNeighborCPU (clusterpair/neighbor.c:282-529) ---------------------------
+// One warp per i-cluster; lane k takes stencil column k. Within a column the
+// j-clusters are sorted by bbminz, so the candidates are a window: a binary
+// search skips those whose box lies more than cutneigh below (using the
+// largest z extent of any j-cluster, with a margin), and the scan stops at the
+// first whose box starts more than cutneigh above; both skipped groups fail
+// the reference's test exactly. Each candidate gets the reference's test:
+// box distance squared (z, y, x) below cutneigh^2, accepted below rbb^2, else
+// if any atom pair has fma(dx,dx,fma(dy,dy,dz*dz)) below cutneigh^2. Accepted
+// candidates are kept as bits, counted, prefix-summed across lanes (so the row
+// is stencil order, then column order) and written; the diagonal entry is
+// then swapped to the front as the reference's masked entries are.
+template <int M, int N>
+__device__ __forceinline__ bool any_pair(const double3* xi, const double4* __restrict__ cj_x,
+    double cutsq)
+{
+    bool hit = false;
+#pragma unroll
+    for (int b = 0; b < N; b++) {
+        double4 xj = cj_x[b];
+#pragma unroll
+        for (int a = 0; a < M; a++) {
+            double dx = xi[a].x - xj.x, dy = xi[a].y - xj.y, dz = xi[a].z - xj.z;
+            double rsq = __fma_rn(dx, dx, __fma_rn(dy, dy, dz * dz));
+            hit |= rsq < cutsq;
+        }
+    }
+    return hit;
+}
+
+__device__ __forceinline__ double bb_axis(double imin, double imax, double jmin, double jmax)
+{
+    double dl = imin - jmax, dh = jmin - imax;
+    double dm = dl > dh ? dl : dh;
+    return dm > 0.0 ? dm : 0.0;
+}
+
+template <int M, int N>
+__global__ void __launch_bounds__(128) k_build_list(int half, const int* __restrict__ cnt,
+    Geom g, const int* __restrict__ stencil, const int* __restrict__ cbin,
+    const double4* __restrict__ ibbmin, const double4* __restrict__ ibbmax,
+    const double4* __restrict__ jcbbmin, const double4* __restrict__ jcbbmax,
+    const double4* __restrict__ cx, const int* __restrict__ jcol_start,
+    const int* __restrict__ jcol, const unsigned long long* __restrict__ zext, int maxneighs,
+    int ks, int cs, int* list, int* numneigh, int* nmasked, int* cnt_out)
+{
+    const int ci   = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = lane_id();
+    if (ci >= cnt[CP_NCL]) return;
+    const int ci_cj0 = ci / (N / M);
+    const double4 imn = ibbmin[ci], imx = ibbmax[ci];
+    double3 xi[M];
+#pragma unroll
+    for (int a = 0; a < M; a++) {
+        double4 p = cx[ci * M + a];
+        xi[a]     = make_double3(p.x, p.y, p.z);
+    }
+    const double zx  = __longlong_as_double((long long)*zext);
+    const double zlo = imn.z - g.cutneigh - zx - 1.0e-6;
+    const int ib     = cbin[ci];
+    int total = 0, diag_pos = -1;
+    for (int kb = 0; kb < g.nstencil; kb += 32) {
+        const int k = kb + lane;
+        unsigned long long acc0 = 0ull, acc1 = 0ull; // CP_WINDOW_BITS = 128
+        int lo = 0, nacc = 0, my_diag = -1;
+        if (k < g.nstencil) {
+            const int jb = ib + stencil[k];
+            int s0 = jcol_start[jb], s1 = jcol_start[jb + 1];
+            int L = s0, R = s1;
+            while (L < R) {
+                int mid = (L + R) >> 1;
+                if (jcbbmin[mid].z < zlo) L = mid + 1;
+                else R = mid;
+            }
+            lo = L;
+            for (int m = lo; m < s1; m++) {
+                const double4 jn = jcbbmin[m];
+                if (jn.z - imx.z > g.cutneigh) break;
+                const int cj = jcol[m];
+                if (half && ci_cj0 > cj) continue;
+                if (m - lo >= CP_WINDOW_BITS) {
+                    atomicAdd(&cnt_out[CP_WINDOW], 1);
+                    break;
+                }
+                const double4 jx = jcbbmax[m];
+                double d = bb_axis(imn.z, imx.z, jn.z, jx.z);
+                d        = d * d;
+                double e = bb_axis(imn.y, imx.y, jn.y, jx.y);
+                d += e * e;
+                e = bb_axis(imn.x, imx.x, jn.x, jx.x);
+                d += e * e;
+                if (d < g.cutneighsq) {
+                    bool ok = d < g.rbb_sq;
+                    if (!ok) ok = any_pair<M, N>(xi, cx + (size_t)cj * N, g.cutneighsq);
+                    if (ok) {
+                        const int bit = m - lo;
+                        if (bit < 64) acc0 |= 1ull << bit;
+                        else acc1 |= 1ull << (bit - 64);
+                        if (cj == ci_cj0) my_diag = nacc;
+                        nacc++;
+                    }
+                }
+            }
+        }
+        int incl = nacc;
+        for (int o = 1; o < 32; o <<= 1) {
+            int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        int p = total + incl - nacc;
+        if (my_diag >= 0) diag_pos = p + my_diag;
+        for (int w = 0; w < 2; w++) {
+            unsigned long long bits = w ? acc1 : acc0;
+            while (bits) {
+                int bit = __ffsll((long long)bits) - 1;
+                bits &= bits - 1;
+                if (p < maxneighs) list[(size_t)p * ks + (size_t)ci * cs] = jcol[lo + w * 64 + bit];
+                p++;
+            }
+        }
+        total += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    // the diagonal entry (mask != all) goes to the front, clusterpair/neighbor.c:599-649
+    diag_pos = __reduce_max_sync(0xffffffffu, diag_pos);
+    __syncwarp();
+    if (lane == 0) {
+        if (diag_pos > 0 && diag_pos < maxneighs) {
+            int* row                        = list + (size_t)ci * cs;
+            int first                       = row[0];
+            row[0]                          = row[(size_t)diag_pos * ks];
+            row[(size_t)diag_pos * ks]      = first;
+        }
+        numneigh[ci] = total < maxneighs ? total : maxneighs;
+        nmasked[ci]  = diag_pos >= 0 ? 1 : 0;
+        if (total >= maxneighs) atomicMax(&cnt_out[CP_MAXNEED], total);
+    }
+}
+
+void launch_build_list(cudaStream_t s, int M, int N, int half, int ncl_cap, const int* cnt,
+    const Geom& g, const int* stencil, const int* cbin, const double4* ibbmin,
+    const double4* ibbmax, const double4* jcbbmin, const double4* jcbbmax, const double4* cx,
+    const int* jcol_start, const int* jcol, const unsigned long long* zext, int maxneighs,
+    int ks, int cs, int* list, int* numneigh, int* nmasked, int* cnt_out)
+{
+    long long threads = (long long)ncl_cap * 32;
+    int blocks        = mdb_blocks(threads, 128);
+    (void)M;
+    if (N == 4)
+        k_build_list<4, 4><<<blocks, 128, 0, s>>>(half, cnt, g, stencil, cbin, ibbmin, ibbmax,
+            jcbbmin, jcbbmax, cx, jcol_start, jcol, zext, maxneighs, ks, cs, list, numneigh,
+            nmasked, cnt_out);
+    else
+        k_build_list<4, 8><<<blocks, 128, 0, s>>>(half, cnt, g, stencil, cbin, ibbmin, ibbmax,
+            jcbbmin, jcbbmax, cx, jcol_start, jcol, zext, maxneighs, ks, cs, list, numneigh,
+            nmasked, cnt_out);
+    g_launches++;
+}
+
+// ---- pruneNeighborCPU (clusterpair/neighbor.c:1098-1264) -------------------------
+// Entries are tested in parallel (any atom pair inside cutneigh, the SIMD
+// builds' fma form over all M x N slots); lane 0 then replays the reference's
+// compaction, which moves the last entry into each freed place.
+template <int M, int N>
+__global__ void k_prune(const int* __restrict__ cnt, const double4* __restrict__ cx,
+    double cutneighsq, int maxneighs, int ks, int cs, int* list, int* numneigh, int* nmasked)
+{
+    extern __shared__ unsigned char s_flags_raw[];
+    const int w    = threadIdx.x >> 5;
+    const int ci   = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = lane_id();
+    if (ci >= cnt[CP_NCL]) return;
+    const int nn = numneigh[ci];
+    unsigned char* flag = s_flags_raw + (size_t)w * maxneighs;
+    double3 xi[M];
+#pragma unroll
+    for (int a = 0; a < M; a++) {
+        double4 p = cx[ci * M + a];
+        xi[a]     = make_double3(p.x, p.y, p.z);
+    }
+    int* row = list + (size_t)ci * cs;
+    for (int k = lane; k < nn; k += 32) {
+        int cj  = row[(size_t)k * ks];
+        flag[k] = any_pair<M, N>(xi, cx + (size_t)cj * N, cutneighsq) ? 1 : 0;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        int n = nn, nm = nmasked[ci], k = 0;
+        while (k < n) {
+            if (flag[k]) {
+                k++;
+            } else {
+                n--;
+                if (k < nm) nm--;
+                row[(size_t)k * ks] = row[(size_t)n * ks];
+                flag[k]                   = flag[n];
+            }
+        }
+        numneigh[ci] = n;
+        nmasked[ci]  = nm;
+    }
+}
+
+void launch_prune(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt, const double4* cx,
+    double cutneighsq, int maxneighs, int ks, int cs, int* list, int* numneigh, int* nmasked)
+{
+    (void)M;
+    // one flag byte per list entry and warp (the caller keeps maxneighs
+    // below 12,288 so that 4 warps fit in 48 KB)
+    long long threads = (long long)ncl_cap * 32;
+    int blocks        = mdb_blocks(threads, 128);
+    size_t smem       = 4 * (size_t)maxneighs;
+    if (N == 4)
+        k_prune<4, 4><<<blocks, 128, smem, s>>>(cnt, cx, cutneighsq, maxneighs, ks, cs, list,
+            numneigh, nmasked);
+    else
+        k_prune<4, 8><<<blocks, 128, smem, s>>>(cnt, cx, cutneighsq, maxneighs, ks, cs, list,
+            numneigh, nmasked);
+    g_launches++;
+}
+
+} // namespace cp
+} // namespace mdb

@@ -1,0 +1,509 @@
+// Cluster-pair scheme: Lennard-Jones forces (FP64 reference-exact and FP32
+// mixed), the cluster-layout integrator and the thermo partial sums.
+#include <math.h>
+
+#include "mdb_cp_internal.cuh"
+
+namespace mdb {
+namespace cp {
+
+#define CP_FORCE_THREADS 128
+
+int force_blocks(int ncl_cap)
+{
+    // the FP64 kernel runs one thread per slot, the mixed one a warp per
+    // i-cluster; both size their partial-energy arrays by this count
+    long long t = (long long)ncl_cap * 32;
+    return mdb_blocks(t, CP_FORCE_THREADS);
+}
+
+// ---- FP64: computeForceLJRef (clusterpair/force_lj.c:23-189) -----------------
+// One thread per i slot. For each list entry the sum over the N j atoms is
+// formed first and then added to the atom's force, exactly the reference's
+// order, so full-list forces are bit-identical. Self pairs (and, for half
+// lists, the lower triangle) of the diagonal entry are excluded by cluster
+// index as the reference does; half lists subtract the reaction from local j
+// slots with atomics (the reference drops ghost reactions: without MPI its
+// reverse communication does nothing).
+template <int M, int N, bool HALF, bool ENERGY>
+__global__ void __launch_bounds__(CP_FORCE_THREADS) k_force_fp64(const int* __restrict__ cnt,
+    const double4* __restrict__ cx, Types ty, double cutforcesq, const int* __restrict__ list,
+    int ks, int cs, const int* __restrict__ numneigh, double4* cf, double* epart)
+{
+    __shared__ double s_se[MDB_MAX_TYPES], s_s3[MDB_MAX_TYPES];
+    if (threadIdx.x < MDB_MAX_TYPES) {
+        s_se[threadIdx.x] = ty.sqrt_eps[threadIdx.x];
+        s_s3[threadIdx.x] = ty.sigma3[threadIdx.x];
+    }
+    __syncthreads();
+    const int s    = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ncl  = cnt[CP_NCL];
+    const int nloc = ncl * M; // local slots (= ncj * N)
+    double epot    = 0.0;
+    if (s < nloc) {
+        const double4 pi = cx[s];
+        const int ti     = slot_type(pi);
+        if (ti >= 0) {
+            const int ci = s / M, a = s - ci * M;
+            const int ci_cj0 = ci / (N / M);
+            const int ai     = a + M * (ci % (N / M));
+            const double se_i = s_se[ti], s3_i = s_s3[ti];
+            double fx = 0.0, fy = 0.0, fz = 0.0;
+            const int nn = numneigh[ci];
+            for (int k = 0; k < nn; k++) {
+                const int cj = __ldg(&list[(size_t)k * ks + (size_t)ci * cs]);
+                double fix = 0.0, fiy = 0.0, fiz = 0.0;
+#pragma unroll
+                for (int b = 0; b < N; b++) {
+                    const bool cond = HALF ? (ci_cj0 != cj || ai < b) : (ci_cj0 != cj || ai != b);
+                    if (!cond) continue;
+                    const int sj     = cj * N + b;
+                    const double4 pj = cx[sj];
+                    const double delx = pi.x - pj.x;
+                    const double dely = pi.y - pj.y;
+                    const double delz = pi.z - pj.z;
+                    const double rsq  = delx * delx + dely * dely + delz * delz;
+                    if (rsq < cutforcesq) {
+                        int tj            = slot_type(pj);
+                        tj                = tj < 0 ? 0 : tj;
+                        const double sig6 = s3_i * s_s3[tj];
+                        const double eps  = se_i * s_se[tj];
+                        const double sr2  = 1.0 / rsq;
+                        const double sr6  = sr2 * sr2 * sr2 * sig6;
+                        const double force = 48.0 * sr6 * (sr6 - 0.5) * sr2 * eps;
+                        if (HALF && sj < nloc) {
+                            atomicAdd(&cf[sj].x, -(delx * force));
+                            atomicAdd(&cf[sj].y, -(dely * force));
+                            atomicAdd(&cf[sj].z, -(delz * force));
+                        }
+                        fix += delx * force;
+                        fiy += dely * force;
+                        fiz += delz * force;
+                        if (ENERGY) {
+                            double e = 4.0 * eps * sr6 * (sr6 - 1.0);
+                            epot += (HALF && sj < nloc) ? e : 0.5 * e;
+                        }
+                    }
+                }
+                fx += fix;
+                fy += fiy;
+                fz += fiz;
+            }
+            if (HALF) {
+                atomicAdd(&cf[s].x, fx);
+                atomicAdd(&cf[s].y, fy);
+                atomicAdd(&cf[s].z, fz);
+            } else {
+                cf[s] = make_double4(fx, fy, fz, 0.0);
+            }
+        }
+    }
+    if (ENERGY) {
+        double t = block_sum(epot);
+        if (threadIdx.x == 0) epart[blockIdx.x] = t;
+    }
+}
+
+template <int N, bool HALF, bool ENERGY>
+static void run_fp64(cudaStream_t s, int blocks, const int* cnt, const double4* cx,
+    const Types& ty, double cutforcesq, const int* list, int ks, int cs, const int* numneigh,
+    double4* cf, double* epart)
+{
+    k_force_fp64<4, N, HALF, ENERGY><<<blocks, CP_FORCE_THREADS, 0, s>>>(cnt, cx, ty, cutforcesq,
+        list, ks, cs, numneigh, cf, epart);
+}
+
+void launch_force_fp64(cudaStream_t s, int M, int N, int half, int energy, int ncl_cap,
+    const int* cnt, const double4* cx, const Types& ty, double cutforcesq, const int* list,
+    int ks, int cs, const int* numneigh, double4* cf, double* epart)
+{
+    (void)M;
+    // one thread per slot: ncl_cap * 4 threads; energy partials sized by
+    // force_blocks (ncl_cap * 32 threads) cover it
+    int blocks = mdb_blocks((long long)ncl_cap * 4, CP_FORCE_THREADS);
+    if (N == 4) {
+        if (half) energy ? run_fp64<4, true, true>(s, blocks, cnt, cx, ty, cutforcesq, list, ks, cs, numneigh, cf, epart)
+                         : run_fp64<4, true, false>(s, blocks, cnt, cx, ty, cutforcesq, list, ks, cs, numneigh, cf, epart);
+        else energy ? run_fp64<4, false, true>(s, blocks, cnt, cx, ty, cutforcesq, list, ks, cs, numneigh, cf, epart)
+                    : run_fp64<4, false, false>(s, blocks, cnt, cx, ty, cutforcesq, list, ks, cs, numneigh, cf, epart);
+    } else {
+        if (half) energy ? run_fp64<8, true, true>(s, blocks, cnt, cx, ty, cutforcesq, list, ks, cs, numneigh, cf, epart)
+                         : run_fp64<8, true, false>(s, blocks, cnt, cx, ty, cutforcesq, list, ks, cs, numneigh, cf, epart);
+        else energy ? run_fp64<8, false, true>(s, blocks, cnt, cx, ty, cutforcesq, list, ks, cs, numneigh, cf, epart)
+                    : run_fp64<8, false, false>(s, blocks, cnt, cx, ty, cutforcesq, list, ks, cs, numneigh, cf, epart);
+    }
+    g_launches++;
+}
+
+// ---- mixed: FP32 pair forces on anchor-relative coordinates ------------------------
+// One warp per i-cluster (M = 4 atoms, held by every lane). The warp takes
+// 32 / N list entries at a time; lane (e, b) owns atom b of entry e and
+// computes its pairs with the 4 i atoms. Positions are relative to per-cluster
+// anchors on a 1/8 grid: the anchor difference is exact in FP32 and is added
+// to the j position once per entry. Full lists reduce the i forces across the
+// warp once per i-cluster; half lists also accumulate each j atom's reaction
+// over the 4 i atoms in the lane and add it with one atomic per component.
+// Padding slots sit at +1e18 (j) and invalid i atoms are moved to -1e18, so
+// they fall outside the cutoff without INF arithmetic.
+__device__ __forceinline__ void warp_reduce_12(float (&v)[12], int lane)
+{
+    // transpose-reduce: after the xor-16 and xor-8 steps each lane holds 3
+    // partial sums of the i atom (lane >> 3); three more steps finish them
+    float h[6];
+    const bool up16 = lane & 16;
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        float send = up16 ? v[i] : v[i + 6];
+        float keep = up16 ? v[i + 6] : v[i];
+        h[i]       = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+    float q[3];
+    const bool up8 = lane & 8;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        float send = up8 ? h[i] : h[i + 3];
+        float keep = up8 ? h[i + 3] : h[i];
+        q[i]       = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1)
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+            q[i] += __shfl_xor_sync(0xffffffffu, q[i], o);
+    v[0] = q[0];
+    v[1] = q[1];
+    v[2] = q[2];
+}
+
+template <int N, bool HALF, bool ENERGY, bool UNIFORM, bool DIAG>
+__device__ __forceinline__ void mixed_entry(const float4 (&xi)[4], const float (&sei)[4],
+    const float (&s3i)[4], const float4& xj, float sej, float s3j, int ai0, int b,
+    float cutforcesq, float c48, float c24, float sig6u, double eps0, double ew, float (&f)[12],
+    float3& fj, double& e)
+{
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+        const float dx  = xi[a].x - xj.x;
+        const float dy  = xi[a].y - xj.y;
+        const float dz  = xi[a].z - xj.z;
+        const float rsq = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
+        const float sr2 = __fdividef(1.0f, rsq);
+        float sr6       = __fmul_rn(__fmul_rn(sr2, sr2), sr2);
+        float t;
+        if (UNIFORM) {
+            sr6 = __fmul_rn(sr6, sig6u);
+            t   = __fmaf_rn(c48, sr6, -c24);
+        } else {
+            sr6             = __fmul_rn(sr6, __fmul_rn(s3i[a], s3j));
+            const float eps = __fmul_rn(sei[a], sej);
+            t               = __fmul_rn(eps, __fmaf_rn(48.0f, sr6, -24.0f));
+        }
+        float force = __fmul_rn(__fmul_rn(sr2, sr6), t);
+        bool in     = rsq < cutforcesq;
+        if (DIAG) in = in && (HALF ? (ai0 + a < b) : (ai0 + a != b));
+        force = in ? force : 0.0f;
+        f[3 * a + 0] = __fmaf_rn(dx, force, f[3 * a + 0]);
+        f[3 * a + 1] = __fmaf_rn(dy, force, f[3 * a + 1]);
+        f[3 * a + 2] = __fmaf_rn(dz, force, f[3 * a + 2]);
+        if (HALF) {
+            fj.x = __fmaf_rn(-dx, force, fj.x);
+            fj.y = __fmaf_rn(-dy, force, fj.y);
+            fj.z = __fmaf_rn(-dz, force, fj.z);
+        }
+        if (ENERGY && in) {
+            const double eps = UNIFORM ? eps0 : (double)__fmul_rn(sei[a], sej);
+            e += ew * 4.0 * eps * (double)sr6 * ((double)sr6 - 1.0);
+        }
+    }
+}
+
+// j data of one list entry: position shifted into the i-cluster's anchor
+// frame (the anchor difference is exact), type parameters
+struct JEntry {
+    float4 x;
+    int cj;
+};
+
+template <int N>
+__device__ __forceinline__ JEntry load_entry(int cj, int b, const float4* __restrict__ xr,
+    const float4* __restrict__ anchor, const float4& ai)
+{
+    JEntry j;
+    j.cj = cj;
+    if (cj >= 0) {
+        j.x            = __ldg(&xr[cj * N + b]);
+        const float4 a = __ldg(&anchor[cj]);
+        // anchors are multiples of 1/8 of magnitude < 2^17: the difference is exact
+        j.x.x += a.x - ai.x;
+        j.x.y += a.y - ai.y;
+        j.x.z += a.z - ai.z;
+    } else {
+        j.x = make_float4(CP_PAD_F, CP_PAD_F, CP_PAD_F, __int_as_float(-1));
+    }
+    return j;
+}
+
+template <int N, bool HALF, bool ENERGY, bool UNIFORM>
+__global__ void __launch_bounds__(CP_FORCE_THREADS) k_force_mixed(const int* __restrict__ cnt,
+    const float4* __restrict__ xr, const float4* __restrict__ anchor, Types ty,
+    float cutforcesq, const int* __restrict__ list, int ks, int cs,
+    const int* __restrict__ numneigh, float4* cf32, double* epart)
+{
+    constexpr int JPW = 32 / N; // entries per warp iteration
+    __shared__ float s_se[MDB_MAX_TYPES], s_s3[MDB_MAX_TYPES];
+    if (threadIdx.x < MDB_MAX_TYPES) {
+        s_se[threadIdx.x] = ty.sqrt_eps_f[threadIdx.x];
+        s_s3[threadIdx.x] = ty.sigma3_f[threadIdx.x];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int ci   = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int ncl  = cnt[CP_NCL];
+    double e       = 0.0;
+    if (ci < ncl) {
+        const int jfac   = N / 4;
+        const int ci_cj0 = ci / jfac;
+        const int ai0    = 4 * (ci % jfac);
+        const int nloc   = ncl * 4;
+        // i atoms relative to their j-cluster's anchor; j positions are moved
+        // into that frame by adding (anchor_j - anchor_i), exact in FP32
+        const float4 ai = anchor[ci_cj0];
+        float4 xi[4];
+        float sei[4], s3i[4];
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+            xi[a] = xr[ci * 4 + a];
+            int t = __float_as_int(xi[a].w);
+            if (t < 0) {
+                xi[a].x = xi[a].y = xi[a].z = -CP_PAD_F;
+                t                           = 0;
+            }
+            sei[a] = UNIFORM ? 0.f : s_se[t];
+            s3i[a] = UNIFORM ? 0.f : s_s3[t];
+        }
+        const float c48   = (float)(48.0 * ty.eps0);
+        const float c24   = (float)(24.0 * ty.eps0);
+        const float sig6u = (float)ty.sigma6_0;
+        float f[12];
+#pragma unroll
+        for (int i = 0; i < 12; i++)
+            f[i] = 0.0f;
+        const int eidx = lane / N, b = lane - eidx * N;
+        const int nn   = numneigh[ci];
+        const int* row = list + (size_t)ci * cs;
+        // software pipeline: list entries in blocks of 32 (one coalesced load,
+        // the next block in flight), j data one iteration ahead
+        int lst_cur = lane < nn ? __ldg(&row[(size_t)lane * ks]) : -1;
+        int lst_nxt = 32 + lane < nn ? __ldg(&row[(size_t)(32 + lane) * ks]) : -1;
+        JEntry cur  = load_entry<N>(__shfl_sync(0xffffffffu, lst_cur, eidx), b, xr, anchor, ai);
+        for (int kb = 0; kb < nn; kb += JPW) {
+            const int kn = kb + JPW;
+            if ((kn & 31) == 0) {
+                lst_cur = lst_nxt;
+                lst_nxt = kn + 32 + lane < nn ? __ldg(&row[(size_t)(kn + 32 + lane) * ks]) : -1;
+            }
+            const int cjn  = __shfl_sync(0xffffffffu, lst_cur, (kn & 31) + eidx);
+            const JEntry nx = load_entry<N>(kn < nn ? cjn : -1, b, xr, anchor, ai);
+            const int cj    = cur.cj;
+            float sej = 0.f, s3j = 0.f;
+            if (!UNIFORM) {
+                int t = __float_as_int(cur.x.w);
+                t     = t < 0 ? 0 : t;
+                sej   = s_se[t];
+                s3j   = s_s3[t];
+            }
+            float3 fj = make_float3(0.f, 0.f, 0.f);
+            // energy weight: full lists see every pair twice; half lists once,
+            // except pairs with ghost atoms, which both owners list
+            const double ew = (!HALF || cj * N + b >= nloc) ? 0.5 : 1.0;
+            if (cj == ci_cj0)
+                mixed_entry<N, HALF, ENERGY, UNIFORM, true>(xi, sei, s3i, cur.x, sej, s3j, ai0,
+                    b, cutforcesq, c48, c24, sig6u, ty.eps0, ew, f, fj, e);
+            else
+                mixed_entry<N, HALF, ENERGY, UNIFORM, false>(xi, sei, s3i, cur.x, sej, s3j, ai0,
+                    b, cutforcesq, c48, c24, sig6u, ty.eps0, ew, f, fj, e);
+            if (HALF && cj >= 0 && cj * N + b < nloc && __float_as_int(cur.x.w) >= 0) {
+                float4* dst = &cf32[cj * N + b];
+                atomicAdd(&dst->x, fj.x);
+                atomicAdd(&dst->y, fj.y);
+                atomicAdd(&dst->z, fj.z);
+            }
+            cur = nx;
+        }
+        warp_reduce_12(f, lane);
+        if ((lane & 7) == 0) {
+            const int a = lane >> 3;
+            if (__float_as_int(xr[ci * 4 + a].w) >= 0) {
+                float4* dst = &cf32[ci * 4 + a];
+                if (HALF) {
+                    atomicAdd(&dst->x, f[0]);
+                    atomicAdd(&dst->y, f[1]);
+                    atomicAdd(&dst->z, f[2]);
+                } else {
+                    *dst = make_float4(f[0], f[1], f[2], 0.f);
+                }
+            }
+        }
+    }
+    if (ENERGY) {
+        double t = block_sum(e);
+        if (threadIdx.x == 0) epart[blockIdx.x] = t;
+    }
+}
+
+template <int N, bool HALF, bool ENERGY, bool UNIFORM>
+static void run_mixed(cudaStream_t s, int blocks, const int* cnt, const float4* xr,
+    const float4* anchor, const Types& ty, float cutforcesq, const int* list, int ks, int cs,
+    const int* numneigh, float4* cf32, double* epart)
+{
+    k_force_mixed<N, HALF, ENERGY, UNIFORM><<<blocks, CP_FORCE_THREADS, 0, s>>>(cnt, xr, anchor,
+        ty, cutforcesq, list, ks, cs, numneigh, cf32, epart);
+}
+
+template <int N, bool HALF>
+static void run_mixed_e(cudaStream_t s, int blocks, int energy, const int* cnt, const float4* xr,
+    const float4* anchor, const Types& ty, float cutforcesq, const int* list, int ks, int cs,
+    const int* numneigh, float4* cf32, double* epart)
+{
+    if (ty.uniform) {
+        if (energy) run_mixed<N, HALF, true, true>(s, blocks, cnt, xr, anchor, ty, cutforcesq, list, ks, cs, numneigh, cf32, epart);
+        else run_mixed<N, HALF, false, true>(s, blocks, cnt, xr, anchor, ty, cutforcesq, list, ks, cs, numneigh, cf32, epart);
+    } else {
+        if (energy) run_mixed<N, HALF, true, false>(s, blocks, cnt, xr, anchor, ty, cutforcesq, list, ks, cs, numneigh, cf32, epart);
+        else run_mixed<N, HALF, false, false>(s, blocks, cnt, xr, anchor, ty, cutforcesq, list, ks, cs, numneigh, cf32, epart);
+    }
+}
+
+void launch_force_mixed(cudaStream_t s, int N, int half, int energy, int ncl_cap,
+    const int* cnt, const float4* xr, const float4* anchor, const Types& ty, float cutforcesq,
+    const int* list, int ks, int cs, const int* numneigh, float4* cf32, double* epart)
+{
+    int blocks = force_blocks(ncl_cap);
+    if (N == 4) {
+        if (half) run_mixed_e<4, true>(s, blocks, energy, cnt, xr, anchor, ty, cutforcesq, list, ks, cs, numneigh, cf32, epart);
+        else run_mixed_e<4, false>(s, blocks, energy, cnt, xr, anchor, ty, cutforcesq, list, ks, cs, numneigh, cf32, epart);
+    } else {
+        if (half) run_mixed_e<8, true>(s, blocks, energy, cnt, xr, anchor, ty, cutforcesq, list, ks, cs, numneigh, cf32, epart);
+        else run_mixed_e<8, false>(s, blocks, energy, cnt, xr, anchor, ty, cutforcesq, list, ks, cs, numneigh, cf32, epart);
+    }
+    g_launches++;
+}
+
+// ---- integrator: initialIntegrateCPU / finalIntegrateCPU (clusterpair/integrate.c:29-86)
+__device__ __forceinline__ double3 slot_force(int s, const double4* cf, const float4* cf32)
+{
+    if (cf32) {
+        float4 f = cf32[s];
+        return make_double3((double)f.x, (double)f.y, (double)f.z);
+    }
+    double4 f = cf[s];
+    return make_double3(f.x, f.y, f.z);
+}
+
+template <bool FINAL, bool INITIAL>
+__global__ void k_cp_integrate(int M, int N, const int* __restrict__ cnt, double dtf, double dt,
+    double4* cx, double4* cv, const double4* __restrict__ cf, const float4* __restrict__ cf32,
+    const float4* __restrict__ anchor, float4* xr)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= cnt[CP_NCL] * M) return;
+    double4 p = cx[s];
+    if (slot_type(p) < 0) return;
+    double4 v       = cv[s];
+    const double3 f = slot_force(s, cf, cf32);
+    if (FINAL) {
+        v.x += dtf * f.x;
+        v.y += dtf * f.y;
+        v.z += dtf * f.z;
+    }
+    if (INITIAL) {
+        v.x += dtf * f.x;
+        v.y += dtf * f.y;
+        v.z += dtf * f.z;
+        p.x += dt * v.x;
+        p.y += dt * v.y;
+        p.z += dt * v.z;
+        cx[s] = p;
+        if (xr) {
+            const float4 a = anchor[s / N];
+            xr[s] = make_float4((float)(p.x - (double)a.x), (float)(p.y - (double)a.y),
+                (float)(p.z - (double)a.z), __int_as_float(slot_type(p)));
+        }
+    }
+    cv[s] = v;
+}
+
+void launch_cp_initial(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt, double dtf,
+    double dt, double4* cx, double4* cv, const double4* cf, const float4* cf32,
+    const float4* anchor, float4* xr)
+{
+    long long n = (long long)ncl_cap * M;
+    k_cp_integrate<false, true><<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(M, N, cnt,
+        dtf, dt, cx, cv, cf, cf32, anchor, xr);
+    g_launches++;
+}
+
+void launch_cp_final(cudaStream_t s, int M, int ncl_cap, const int* cnt, double dtf,
+    const double4* cx, double4* cv, const double4* cf, const float4* cf32)
+{
+    long long n = (long long)ncl_cap * M;
+    k_cp_integrate<true, false><<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(M, M, cnt,
+        dtf, 0.0, const_cast<double4*>(cx), cv, cf, cf32, nullptr, nullptr);
+    g_launches++;
+}
+
+void launch_cp_final_initial(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt,
+    double dtf, double dt, double4* cx, double4* cv, const double4* cf, const float4* cf32,
+    const float4* anchor, float4* xr)
+{
+    long long n = (long long)ncl_cap * M;
+    k_cp_integrate<true, true><<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(M, N, cnt,
+        dtf, dt, cx, cv, cf, cf32, anchor, xr);
+    g_launches++;
+}
+
+// ---- thermo: computeThermo (common/thermo.c:60-100) over the atom arrays ------------
+int ke_blocks(int n) { return mdb_blocks(n > 0 ? n : 1, MDB_NTHREADS); }
+
+__global__ void k_ke_atoms(int n, const double4* __restrict__ av, double mass, double* partials)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double t    = 0.0;
+    if (i < n) {
+        double4 v = av[i];
+        t         = (v.x * v.x + v.y * v.y + v.z * v.z) * mass;
+    }
+    t = block_sum(t);
+    if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+
+void launch_ke_atoms(cudaStream_t s, int n, const double4* av, double mass, double* partials)
+{
+    k_ke_atoms<<<ke_blocks(n), MDB_NTHREADS, 0, s>>>(n, av, mass, partials);
+    g_launches++;
+}
+
+// kinetic energy sum of the cluster state (locals): the same sum over slots
+__global__ void k_ke_slots(int M, const int* __restrict__ cnt, const double4* __restrict__ cx,
+    const double4* __restrict__ cv, double mass, double* partials)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    double t    = 0.0;
+    if (s < cnt[CP_NCL] * M && slot_type(cx[s]) >= 0) {
+        double4 v = cv[s];
+        t         = (v.x * v.x + v.y * v.y + v.z * v.z) * mass;
+    }
+    t = block_sum(t);
+    if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+
+void launch_ke_slots(cudaStream_t s, int M, int ncl_cap, const int* cnt, const double4* cx,
+    const double4* cv, double mass, double* partials)
+{
+    long long n = (long long)ncl_cap * M;
+    k_ke_slots<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(M, cnt, cx, cv, mass, partials);
+    g_launches++;
+}
+
+} // namespace cp
+} // namespace mdb

@@ -1,0 +1,155 @@
+// Cluster-pair (GROMACS-style) scheme: device layout and launch helpers shared
+// by mdb_cp_build.cu, mdb_cp_force.cu and mdb_cp_api.cu.
+//
+// Device data layout (HBM), per context, for cluster shape M x N (4x4 or 4x8):
+//   atom arrays (atom order, what updateSingleAtoms writes):
+//     ax double4[nlocal] (.w = type bits), av double4[nlocal]
+//   slots (cluster order): slot cj*N + cjj = atom cjj of j-cluster cj; locals
+//   first (slot ci*M + cii = atom cii of i-cluster ci), then ghost j-clusters,
+//   then one dummy cluster:
+//     cx  double4[slot_cap]  FP64 positions, .w = type bits, -1 for padding
+//                            (padding positions are +INF as in the reference)
+//     cv  double4 (locals), cf double4 (FP64 forces, locals + ghosts)
+//     xr  float4             mixed path: position relative to the anchor of the
+//                            slot's j-cluster, .w = type bits; padding holds a
+//                            large finite sentinel
+//     cf32 float4            mixed path forces
+//   per i-cluster: inat, cbin, cl_first (atom index of its first atom in the
+//     next updateSingleAtoms), ibbmin/ibbmax double4 (bbox)
+//   per j-cluster (locals + ghosts): jnat, jbbmin/jbbmax double4, anchor float4
+//     (mixed: a multiple of 1/8 near the box centre, so anchor differences are
+//     exact in FP32)
+//   ghosts: border (owner j-cluster), pbc code ((dx+1) | (dy+1)<<2 | (dz+1)<<4)
+//   columns: j-clusters per xy column as CSR (jcol_start, jcol), sorted by
+//     bbminz as binJClusters leaves them, with their boxes copied in column
+//     order (jcbbmin/jcbbmax) for the list build's window search
+//   list: entry k of i-cluster ci at list[k * ks + ci * cs]: k-major (ks =
+//     capacity of i-clusters, cs = 1) for the FP64 kernel's thread-per-atom
+//     reads, row-major (ks = 1, cs = maxneighs) for the mixed kernel's
+//     warp-per-cluster reads; numneigh[ci]; the diagonal (masked) entry first
+//     as the reference puts it
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "mdb_internal.cuh"
+
+#define CP_M            4    /* i-cluster size of the GPU shapes */
+#define CP_COL_SMEM     1024 /* column sort in shared memory up to this many atoms */
+#define CP_WINDOW_BITS  128  /* candidates per stencil column and i-cluster */
+#define CP_PAD_F        1.0e18f
+#define CP_ANCHOR_STEP  0.125
+
+// device counters of the cluster-pair scheme (int slots)
+enum {
+    CP_NCL          = 0,  // local i-clusters
+    CP_NCJ          = 1,  // local j-clusters
+    CP_NGC          = 2,  // ghost j-clusters in use (clamped to capacity)
+    CP_NGC_TOTAL    = 3,  // ghost j-clusters requested by setupPbc
+    CP_NGHOST_ATOMS = 4,
+    CP_MAXNEED      = 5,  // largest list length seen (>= maxneighs means regrow)
+    CP_BADBIN       = 6,  // atoms outside the column grid
+    CP_WINDOW       = 7,  // a column window wider than CP_WINDOW_BITS
+    CP_SLOTS        = 8
+};
+
+namespace mdb {
+namespace cp {
+
+struct Geom {
+    int nbinx, nbiny, mbinx, mbiny, mbinxlo, mbinylo, mbins, nstencil;
+    double binsizex, binsizey, bininvx, bininvy;
+    double xprd, yprd, zprd;
+    double cutneigh, cutneighsq, rbb_sq;
+};
+
+struct Types {
+    int ntypes, uniform;
+    double sqrt_eps[MDB_MAX_TYPES], sigma3[MDB_MAX_TYPES];
+    float sqrt_eps_f[MDB_MAX_TYPES], sigma3_f[MDB_MAX_TYPES];
+    double eps0, sigma6_0; // uniform case
+};
+
+__device__ __forceinline__ int slot_type(const double4& p) { return (int)__double_as_longlong(p.w); }
+
+__device__ __forceinline__ double type_bits(int t) { return __longlong_as_double((long long)t); }
+
+// coord2bin / coord2bin2D, clusterpair/neighbor.c:1366-1407
+__device__ __forceinline__ void coord2bin2d(const Geom& g, double x, double y, int& ix, int& iy)
+{
+    if (x >= g.xprd) ix = (int)((x - g.xprd) * g.bininvx) + g.nbinx - g.mbinxlo;
+    else if (x >= 0.0) ix = (int)(x * g.bininvx) - g.mbinxlo;
+    else ix = (int)(x * g.bininvx) - g.mbinxlo - 1;
+    if (y >= g.yprd) iy = (int)((y - g.yprd) * g.bininvy) + g.nbiny - g.mbinylo;
+    else if (y >= 0.0) iy = (int)(y * g.bininvy) - g.mbinylo;
+    else iy = (int)(y * g.bininvy) - g.mbinylo - 1;
+}
+
+// ---- launch helpers ---------------------------------------------------------
+// build (mdb_cp_build.cu)
+void launch_gather(cudaStream_t s, int M, int ncl_cap, const int* cnt, const double4* cx,
+    const double4* cv, const int* cl_first, double4* ax, double4* av, int wrap, double xprd,
+    double yprd, double zprd);
+void launch_bin_atoms(cudaStream_t s, int n, const double4* ax, const Geom& g, int* atom_col,
+    int* col_count, int* cnt);
+void launch_scatter_atoms(cudaStream_t s, int n, const int* atom_col, const int* col_start,
+    int* col_fill, int* col_atoms);
+void launch_sort_columns(cudaStream_t s, const Geom& g, int M, int N, const int* col_start,
+    int* col_atoms, const double4* ax, int* col_sorted, int* gidx, double* gz, int* ncl_col);
+void launch_build_clusters(cudaStream_t s, const Geom& g, int M, int N, int mixed,
+    const int* col_start, const int* col_sorted, const int* cl_start, const double4* ax,
+    const double4* av, double4* cx, double4* cv, int* inat, int* cbin, int* cl_first,
+    double4* ibbmin, double4* ibbmax, int* jnat, double4* jbbmin, double4* jbbmax,
+    float4* anchor, float4* xr, int* cnt, unsigned long long* zext);
+void launch_ghost_count(cudaStream_t s, int ncj_cap, const int* cnt, const int* jnat,
+    const double4* jbbmin, const double4* jbbmax, const Geom& g, int* gcount);
+void launch_ghost_write(cudaStream_t s, int ncj_cap, int ngc_cap, int* cnt, const int* jnat,
+    const double4* jbbmin, const double4* jbbmax, const Geom& g, const int* gstart,
+    int* border, int* pbc);
+void launch_ghost_first(cudaStream_t s, int N, int ngc_cap, int mixed, int* cnt,
+    const int* border, const int* pbc, const Geom& g, double4* cx, int* jnat, double4* jbbmin,
+    double4* jbbmax, float4* anchor, float4* xr, unsigned long long* zext);
+void launch_ghost_update(cudaStream_t s, int N, int ngc_cap, int mixed, const int* cnt,
+    const int* border, const int* pbc, const int* jnat, const Geom& g, double4* cx,
+    const float4* anchor, float4* xr);
+void launch_ghost_columns(cudaStream_t s, int N, int ngc_cap, const int* cnt, const int* pbc,
+    const int* jnat, const double4* cx, const Geom& g, int* gcolumn, int* gcol_count);
+void launch_column_sizes(cudaStream_t s, int mbins1, int jfac, const int* ncl_col,
+    const int* gcol_count, int* jcol_n);
+void launch_ghost_scatter(cudaStream_t s, int ngc_cap, const int* cnt, const int* gcolumn,
+    const int* jcol_start, const int* ncl_col, int jfac, int* gfill, int* gtmp);
+void launch_merge_columns(cudaStream_t s, int mbins1, int jfac, const int* ncl_col,
+    const int* cl_start, const int* gcol_count, const int* jcol_start, const int* gtmp,
+    const double4* jbbmin, const double4* jbbmax, int* jcol, double4* jcbbmin, double4* jcbbmax);
+void launch_build_list(cudaStream_t s, int M, int N, int half, int ncl_cap, const int* cnt,
+    const Geom& g, const int* stencil, const int* cbin, const double4* ibbmin,
+    const double4* ibbmax, const double4* jcbbmin, const double4* jcbbmax, const double4* cx,
+    const int* jcol_start, const int* jcol, const unsigned long long* zext, int maxneighs,
+    int ks, int cs, int* list, int* numneigh, int* nmasked, int* cnt_out);
+void launch_prune(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt, const double4* cx,
+    double cutneighsq, int maxneighs, int ks, int cs, int* list, int* numneigh, int* nmasked);
+
+// force / integrate / thermo (mdb_cp_force.cu)
+int force_blocks(int ncl_cap);
+void launch_force_fp64(cudaStream_t s, int M, int N, int half, int energy, int ncl_cap,
+    const int* cnt, const double4* cx, const Types& ty, double cutforcesq, const int* list,
+    int ks, int cs, const int* numneigh, double4* cf, double* epart);
+void launch_force_mixed(cudaStream_t s, int N, int half, int energy, int ncl_cap,
+    const int* cnt, const float4* xr, const float4* anchor, const Types& ty, float cutforcesq,
+    const int* list, int ks, int cs, const int* numneigh, float4* cf32, double* epart);
+void launch_cp_initial(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt, double dtf,
+    double dt, double4* cx, double4* cv, const double4* cf, const float4* cf32,
+    const float4* anchor, float4* xr);
+void launch_cp_final(cudaStream_t s, int M, int ncl_cap, const int* cnt, double dtf,
+    const double4* cx, double4* cv, const double4* cf, const float4* cf32);
+void launch_cp_final_initial(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt,
+    double dtf, double dt, double4* cx, double4* cv, const double4* cf, const float4* cf32,
+    const float4* anchor, float4* xr);
+int ke_blocks(int n);
+void launch_ke_atoms(cudaStream_t s, int n, const double4* av, double mass, double* partials);
+void launch_ke_slots(cudaStream_t s, int M, int ncl_cap, const int* cnt, const double4* cx,
+    const double4* cv, double mass, double* partials);
+
+} // namespace cp
+} // namespace mdb

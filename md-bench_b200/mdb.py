@@ -84,6 +84,18 @@ EXPORTS = [
     "mdb_get_positions_all", "mdb_get_ghosts", "mdb_get_neighbor_list",
     "mdb_get_bin_geometry", "mdb_get_eam_fp", "mdb_launch_count", "mdb_kinetic_sum_noalloc",
 ]
+# every symbol include/mdb_cp.h declares
+CP_EXPORTS = [
+    "mdb_cp_create", "mdb_cp_destroy", "mdb_cp_last_error", "mdb_cp_stream", "mdb_cp_synchronize",
+    "mdb_cp_launch_count", "mdb_cp_set_atoms", "mdb_cp_get_atoms", "mdb_cp_build_clusters",
+    "mdb_cp_define_jclusters", "mdb_cp_setup_pbc", "mdb_cp_update_pbc", "mdb_cp_bin_jclusters",
+    "mdb_cp_build_neighbor", "mdb_cp_prune_neighbor", "mdb_cp_update_single_atoms",
+    "mdb_cp_update_atoms_pbc", "mdb_cp_compute_force", "mdb_cp_compute_force_energy",
+    "mdb_cp_initial_integrate", "mdb_cp_final_integrate", "mdb_cp_thermo", "mdb_cp_setup",
+    "mdb_cp_run", "mdb_cp_get_counts", "mdb_cp_get_slots", "mdb_cp_get_iclusters",
+    "mdb_cp_get_jclusters", "mdb_cp_get_ghosts", "mdb_cp_get_neighbor_list",
+    "mdb_cp_get_columns", "mdb_cp_get_geometry",
+]
 # every symbol include/mdb_host.h declares
 HOST_EXPORTS = [
     "mdbh_defaults", "mdbh_read_params", "mdbh_read_types", "mdbh_apply_eam",
@@ -130,6 +142,33 @@ def load():
     for name in ("mdb_setup_pbc", "mdb_update_pbc", "mdb_update_atoms_pbc",
                  "mdb_build_neighbor", "mdb_compute_force", "mdb_compute_force_energy",
                  "mdb_initial_integrate", "mdb_final_integrate", "mdb_setup"):
+        sig[name] = ([vp], ip)
+    sig.update({
+        "mdb_cp_create": ([C.POINTER(MdbParams), ip, ip, C.POINTER(vp)], ip),
+        "mdb_cp_destroy": ([vp], ip),
+        "mdb_cp_last_error": ([vp], C.c_char_p),
+        "mdb_cp_stream": ([vp], vp),
+        "mdb_cp_launch_count": ([vp], C.c_longlong),
+        "mdb_cp_set_atoms": ([vp, ip, _dp, _dp, _ip], ip),
+        "mdb_cp_get_atoms": ([vp, vp, vp, vp], ip),
+        "mdb_cp_thermo": ([vp, C.POINTER(MdbThermo)], ip),
+        "mdb_cp_run": ([vp, ip, ip, C.POINTER(MdbThermo), ip, C.POINTER(ip)], ip),
+        "mdb_cp_get_counts": ([vp, _ip], ip),
+        "mdb_cp_get_slots": ([vp, vp, vp, vp, vp, ip], ip),
+        "mdb_cp_get_iclusters": ([vp, vp, vp, vp], ip),
+        "mdb_cp_get_jclusters": ([vp, vp, vp, ip], ip),
+        "mdb_cp_get_ghosts": ([vp, vp, vp], ip),
+        "mdb_cp_get_neighbor_list": ([vp, vp, vp, vp, ip], ip),
+        "mdb_cp_get_columns": ([vp, vp, vp, ip], ip),
+        "mdb_cp_get_geometry": ([vp, vp, vp, vp, ip], ip),
+    })
+    for name in ("mdb_cp_synchronize", "mdb_cp_build_clusters", "mdb_cp_define_jclusters",
+                 "mdb_cp_setup_pbc",
+                 "mdb_cp_update_pbc", "mdb_cp_bin_jclusters", "mdb_cp_build_neighbor",
+                 "mdb_cp_prune_neighbor", "mdb_cp_update_single_atoms",
+                 "mdb_cp_update_atoms_pbc", "mdb_cp_compute_force",
+                 "mdb_cp_compute_force_energy", "mdb_cp_initial_integrate",
+                 "mdb_cp_final_integrate", "mdb_cp_setup"):
         sig[name] = ([vp], ip)
     hp = C.POINTER(MdbHostParams)
     pd, pi = C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.POINTER(C.c_int))
@@ -461,3 +500,225 @@ class System:
     @property
     def launches(self):
         return self.lib.mdb_launch_count(self.h)
+
+
+def _vp(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class ClusterSystem:
+    """One device-resident system in the cluster-pair scheme (an ``MdbCp``):
+    GROMACS-style 4x4 (``cluster_n=4``) or 4x8 (``cluster_n=8``) clusters."""
+
+    def __init__(self, *, xprd, yprd, zprd, cutforce, cutneigh, dt, dtforce, natoms,
+                 cluster_n=4, prune_every=0, mass=1.0, half_neigh=0, precision=PREC_FP64,
+                 ntypes=1, epsilon=1.0, sigma=1.0, epsilon_per_type=None, sigma_per_type=None,
+                 reneigh_every=20, nstat=100, maxneighs=0, device=0, **_ignored):
+        self.lib = load()
+        if isinstance(precision, str):
+            precision = PRECISIONS[precision]
+        p = MdbParams(force_field=FF_LJ, half_neigh=half_neigh, precision=precision,
+                      ntypes=ntypes, reneigh_every=reneigh_every, nstat=nstat,
+                      maxneighs=maxneighs, natoms=natoms, device=device, xprd=xprd,
+                      yprd=yprd, zprd=zprd, dt=dt, dtforce=dtforce, mass=mass,
+                      cutforce=cutforce, cutneigh=cutneigh, epsilon=epsilon, sigma=sigma,
+                      pbc_x=1, pbc_y=1, pbc_z=1)
+        self._keep = []
+        if epsilon_per_type is not None:
+            e = np.ascontiguousarray(epsilon_per_type, dtype=np.float64)
+            s = np.ascontiguousarray(sigma_per_type, dtype=np.float64)
+            self._keep += [e, s]
+            p.epsilon_per_type = e.ctypes.data_as(C.POINTER(C.c_double))
+            p.sigma_per_type = s.ctypes.data_as(C.POINTER(C.c_double))
+        h = C.c_void_p()
+        rc = self.lib.mdb_cp_create(C.byref(p), cluster_n, prune_every, C.byref(h))
+        if rc:
+            raise MdbError(f"mdb_cp_create failed: {self.lib.mdb_status_string(rc).decode()}")
+        self.h = h
+        self.params = p
+        self.M, self.N = 4, cluster_n
+        self.nlocal = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mdb_cp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _ck(self, rc, what):
+        if rc:
+            msg = self.lib.mdb_cp_last_error(self.h)
+            raise MdbError(f"{what}: {self.lib.mdb_status_string(rc).decode()}"
+                           f" ({msg.decode() if msg else ''})")
+
+    def _call(self, name):
+        self._ck(getattr(self.lib, name)(self.h), name)
+
+    # -- data ---------------------------------------------------------------
+    def set_atoms(self, x, v, type_):
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+        v = np.ascontiguousarray(v, dtype=np.float64).reshape(-1)
+        t = np.ascontiguousarray(type_, dtype=np.int32)
+        self._ck(self.lib.mdb_cp_set_atoms(self.h, len(t), x, v, t), "mdb_cp_set_atoms")
+        self.nlocal = len(t)
+
+    def atoms(self):
+        n = self.nlocal
+        x = np.zeros((n, 3)); v = np.zeros((n, 3)); t = np.zeros(n, dtype=np.int32)
+        self._ck(self.lib.mdb_cp_get_atoms(self.h, _vp(x), _vp(v), _vp(t)), "mdb_cp_get_atoms")
+        return x, v, t
+
+    def counts(self):
+        c = np.zeros(8, dtype=np.int32)
+        self._ck(self.lib.mdb_cp_get_counts(self.h, c), "mdb_cp_get_counts")
+        return dict(zip(["nlocal", "natoms", "ncl", "ncj", "ngc", "nghost", "dummy",
+                         "maxneighs"], [int(v) for v in c]))
+
+    def nslots(self):
+        c = self.counts()
+        return (c["ncj"] + c["ngc"] + 1) * self.N
+
+    def slots(self):
+        ns = self.nslots()
+        x = np.zeros((ns, 3)); v = np.zeros((ns, 3)); f = np.zeros((ns, 3))
+        t = np.zeros(ns, dtype=np.int32)
+        self._ck(self.lib.mdb_cp_get_slots(self.h, _vp(x), _vp(v), _vp(f), _vp(t), ns),
+                 "mdb_cp_get_slots")
+        return x, v, f, t
+
+    def iclusters(self):
+        n = self.counts()["ncl"]
+        nat = np.zeros(max(n, 1), dtype=np.int32); b = np.zeros(max(n, 1), dtype=np.int32)
+        bb = np.zeros(max(6 * n, 6))
+        self._ck(self.lib.mdb_cp_get_iclusters(self.h, _vp(nat), _vp(b), _vp(bb)),
+                 "mdb_cp_get_iclusters")
+        return nat[:n], b[:n], bb[:6 * n].reshape(n, 6)
+
+    def jclusters(self):
+        c = self.counts()
+        n = c["ncj"] + c["ngc"]
+        nat = np.zeros(max(n, 1), dtype=np.int32); bb = np.zeros(max(6 * n, 6))
+        self._ck(self.lib.mdb_cp_get_jclusters(self.h, _vp(nat), _vp(bb), n),
+                 "mdb_cp_get_jclusters")
+        return nat[:n], bb[:6 * n].reshape(n, 6)
+
+    def ghosts(self):
+        ng = self.counts()["ngc"]
+        bm = np.zeros(max(ng, 1), dtype=np.int32); pb = np.zeros(max(3 * ng, 3), dtype=np.int32)
+        self._ck(self.lib.mdb_cp_get_ghosts(self.h, _vp(bm), _vp(pb)), "mdb_cp_get_ghosts")
+        return bm[:ng], pb[:3 * ng].reshape(ng, 3)
+
+    def neighbor_list(self):
+        c = self.counts()
+        n, ld = c["ncl"], c["maxneighs"]
+        nn = np.zeros(max(n, 1), dtype=np.int32); nm = np.zeros(max(n, 1), dtype=np.int32)
+        nb = np.zeros(max(n * ld, 1), dtype=np.int32)
+        self._ck(self.lib.mdb_cp_get_neighbor_list(self.h, _vp(nn), _vp(nm), _vp(nb), ld),
+                 "mdb_cp_get_neighbor_list")
+        return nn[:n], nm[:n], nb[:n * ld].reshape(n, ld)
+
+    def numneigh(self):
+        n = self.counts()["ncl"]
+        nn = np.zeros(max(n, 1), dtype=np.int32)
+        self._ck(self.lib.mdb_cp_get_neighbor_list(self.h, _vp(nn), None, None, 0),
+                 "mdb_cp_get_neighbor_list")
+        return nn[:n]
+
+    def columns(self):
+        g = self.geometry()
+        mb = g["mbinx"] * g["mbiny"]
+        start = np.zeros(mb + 1, dtype=np.int32)
+        n = self.lib.mdb_cp_get_columns(self.h, _vp(start), None, 0)
+        lst = np.zeros(max(n, 1), dtype=np.int32)
+        self.lib.mdb_cp_get_columns(self.h, _vp(start), _vp(lst), n)
+        return start, lst[:n]
+
+    def geometry(self):
+        ints = np.zeros(7, dtype=np.int32); d = np.zeros(3); st = np.zeros(4096, dtype=np.int32)
+        self._ck(self.lib.mdb_cp_get_geometry(self.h, _vp(ints), _vp(d), _vp(st), 4096),
+                 "mdb_cp_get_geometry")
+        keys = ["nbinx", "nbiny", "mbinx", "mbiny", "mbinxlo", "mbinylo", "nstencil"]
+        g = dict(zip(keys, [int(i) for i in ints]))
+        g.update(binsizex=d[0], binsizey=d[1], rbb_sq=d[2], stencil=st[:g["nstencil"]].copy())
+        return g
+
+    # -- hooks --------------------------------------------------------------
+    def setup(self):
+        self._call("mdb_cp_setup")
+
+    def build_clusters(self):
+        self._call("mdb_cp_build_clusters")
+        self._call("mdb_cp_define_jclusters")
+
+    def setup_pbc(self):
+        self._call("mdb_cp_setup_pbc")
+
+    def update_pbc(self):
+        self._call("mdb_cp_update_pbc")
+
+    def bin_jclusters(self):
+        self._call("mdb_cp_bin_jclusters")
+
+    def build_neighbor(self):
+        self._call("mdb_cp_build_neighbor")
+
+    def prune(self):
+        self._call("mdb_cp_prune_neighbor")
+
+    def update_single_atoms(self):
+        self._call("mdb_cp_update_single_atoms")
+
+    def update_atoms_pbc(self):
+        self._call("mdb_cp_update_atoms_pbc")
+
+    def compute_force(self, energy=False):
+        self._call("mdb_cp_compute_force_energy" if energy else "mdb_cp_compute_force")
+
+    def initial_integrate(self):
+        self._call("mdb_cp_initial_integrate")
+
+    def final_integrate(self):
+        self._call("mdb_cp_final_integrate")
+
+    def step_hooks(self, n, prune_every=1000):
+        """One timestep of clusterpair/main.c:326-362 through the single hooks."""
+        p = self.params
+        self.initial_integrate()
+        if (n + 1) % p.reneigh_every:
+            if not (n + 1) % prune_every:
+                self.prune()
+            self.update_pbc()
+        else:
+            self.update_single_atoms()
+            self.update_atoms_pbc()
+            self.build_clusters()
+            self.setup_pbc()
+            self.bin_jclusters()
+            self.build_neighbor()
+        self.compute_force()
+        self.final_integrate()
+
+    def run(self, nsteps, first_step=0, max_samples=64):
+        samples = (MdbThermo * max(max_samples, 1))()
+        ns = C.c_int()
+        self._ck(self.lib.mdb_cp_run(self.h, first_step, nsteps, samples, max_samples,
+                                     C.byref(ns)), "mdb_cp_run")
+        return [samples[i].as_dict() for i in range(ns.value)]
+
+    def thermo(self):
+        t = MdbThermo()
+        self._ck(self.lib.mdb_cp_thermo(self.h, C.byref(t)), "mdb_cp_thermo")
+        return t.as_dict()
+
+    def synchronize(self):
+        self._call("mdb_cp_synchronize")
+
+    @property
+    def stream(self):
+        return int(self.lib.mdb_cp_stream(self.h) or 0)
+
+    @property
+    def launches(self):
+        return int(self.lib.mdb_cp_launch_count(self.h))

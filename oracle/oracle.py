@@ -334,3 +334,324 @@ class RefVL:
         T = C.c_double(); P = C.c_double()
         self.lib.ref_vl_thermo(C.byref(T), C.byref(P))
         return dict(T=T.value, P=P.value)
+
+
+# ---------------------------------------------------------------------------
+# cluster-pair scheme
+REF_CP_SO = {shape: os.path.join(HERE, "_ref", f"libmdbref_cp_{shape}.so")
+             for shape in ("1x2", "4x4", "4x8")}
+REF_CP_BIN = {shape: os.path.join(HERE, "_ref", f"MDBench-CP-{shape}")
+              for shape in ("4x4", "4x8")}
+
+
+class OrcCpParams(C.Structure):
+    _fields_ = [
+        ("cluster_m", C.c_int), ("cluster_n", C.c_int), ("fma_rsq", C.c_int),
+        ("half_neigh", C.c_int), ("ntypes", C.c_int), ("natoms", C.c_int),
+        ("reneigh_every", C.c_int), ("prune_every", C.c_int), ("nstat", C.c_int),
+        ("xprd", C.c_double), ("yprd", C.c_double), ("zprd", C.c_double),
+        ("dt", C.c_double), ("dtforce", C.c_double), ("mass", C.c_double),
+        ("cutforce", C.c_double), ("cutneigh", C.c_double),
+        ("epsilon", C.c_double), ("sigma", C.c_double),
+        ("epsilon_per_type", C.POINTER(C.c_double)),
+        ("sigma_per_type", C.POINTER(C.c_double)),
+    ]
+
+
+_cp_lib = None
+
+
+def _load_cp():
+    global _cp_lib
+    if _cp_lib is None:
+        lib = _load()
+        lib.orccp_create.restype = C.c_void_p
+        lib.orccp_create.argtypes = [C.POINTER(OrcCpParams)]
+        lib.orccp_destroy.argtypes = [C.c_void_p]
+        lib.orccp_set_atoms.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _ip]
+        for n in ("orccp_setup", "orccp_build_clusters", "orccp_setup_pbc",
+                  "orccp_build_neighbor"):
+            getattr(lib, n).argtypes = [C.c_void_p]
+            getattr(lib, n).restype = C.c_int
+        for n in ("orccp_define_jclusters", "orccp_bin_jclusters", "orccp_prune_neighbor",
+                  "orccp_update_single_atoms", "orccp_update_atoms_pbc",
+                  "orccp_initial_integrate", "orccp_final_integrate"):
+            getattr(lib, n).argtypes = [C.c_void_p]
+            getattr(lib, n).restype = None
+        lib.orccp_update_pbc.argtypes = [C.c_void_p, C.c_int]
+        lib.orccp_compute_force.argtypes = [C.c_void_p]
+        lib.orccp_compute_force.restype = C.c_double
+        lib.orccp_step.argtypes = [C.c_void_p, C.c_int]
+        lib.orccp_thermo.argtypes = [C.c_void_p] + [C.POINTER(C.c_double)] * 2
+        lib.orccp_energy.argtypes = [C.c_void_p] + [C.POINTER(C.c_double)] * 2
+        lib.orccp_counts.argtypes = [C.c_void_p, _ip]
+        lib.orccp_get_atoms.argtypes = [C.c_void_p] + [C.c_void_p] * 3
+        lib.orccp_get_slots.argtypes = [C.c_void_p] + [C.c_void_p] * 4 + [C.c_int]
+        lib.orccp_set_slots.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.orccp_get_iclusters.argtypes = [C.c_void_p, _ip, C.c_void_p, C.c_void_p]
+        lib.orccp_get_jclusters.argtypes = [C.c_void_p, _ip, C.c_void_p, C.c_int]
+        lib.orccp_get_ghosts.argtypes = [C.c_void_p, _ip, _ip]
+        lib.orccp_get_list.argtypes = [C.c_void_p, _ip, C.c_void_p, _ip, C.c_void_p, C.c_int]
+        lib.orccp_bin_geometry.argtypes = [C.c_void_p, _ip, _dp, C.c_void_p]
+        lib.orccp_get_columns.argtypes = [C.c_void_p, _ip, _ip, C.c_int]
+        lib.orccp_get_columns.restype = C.c_int
+        _cp_lib = lib
+    return _cp_lib
+
+
+def _cp_counts(c):
+    return dict(zip(["nlocal", "natoms", "ncl", "ncj", "ngc", "nghost", "dummy",
+                     "maxneighs"], [int(v) for v in c]))
+
+
+class _CpViews:
+    """Shared getters of the cluster-pair oracle and the reference shim."""
+
+    def nslots(self):
+        c = self.counts()
+        return (c["ncj"] + c["ngc"] + 1) * self.N
+
+    def slots(self):
+        ns = self.nslots()
+        x = np.zeros((ns, 3)); v = np.zeros((ns, 3)); f = np.zeros((ns, 3))
+        t = np.zeros(ns, dtype=np.int32)
+        self._get_slots(_ptr(x), _ptr(v), _ptr(f), _ptr(t), ns)
+        return x, v, f, t
+
+    def neighbor_list(self):
+        c = self.counts()
+        n, ld = c["ncl"], c["maxneighs"]
+        nn = np.zeros(max(n, 1), dtype=np.int32)
+        nm = np.zeros(max(n, 1), dtype=np.int32)
+        nb = np.zeros(max(n * ld, 1), dtype=np.int32)
+        im = np.zeros(max(n * ld, 1), dtype=np.uint32)
+        self._get_list(nn, nm, nb, im, ld)
+        return nn[:n], nm[:n], nb[:n * ld].reshape(n, ld), im[:n * ld].reshape(n, ld)
+
+    def ghosts(self):
+        ng = self.counts()["ngc"]
+        bm = np.zeros(max(ng, 1), dtype=np.int32)
+        pb = np.zeros(max(3 * ng, 3), dtype=np.int32)
+        self._get_ghosts(bm, pb)
+        return bm[:ng], pb[:3 * ng].reshape(ng, 3)
+
+
+class OracleCP(_CpViews):
+    """One cluster-pair system held by the C restatement. Atoms come from the
+    caller (normally the Verlet-list oracle's lattice, pinned to the reference's
+    createAtom)."""
+
+    def __init__(self, x, v, type_, M=4, N=4, fma_rsq=None, half=0, ntypes=4, natoms=None,
+                 xprd=None, yprd=None, zprd=None, dt=0.005, dtforce=None, mass=1.0,
+                 cutforce=2.5, cutneigh=2.8, epsilon=1.0, sigma=1.0, reneigh_every=20,
+                 prune_every=1000, nstat=100, epsilon_per_type=None, sigma_per_type=None):
+        self.lib = _load_cp()
+        self.M, self.N = M, N
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 3)
+        v = np.ascontiguousarray(v, dtype=np.float64).reshape(-1, 3)
+        t = np.ascontiguousarray(type_, dtype=np.int32)
+        n = len(x)
+        p = OrcCpParams(cluster_m=M, cluster_n=N,
+                        fma_rsq=int(M > 1 if fma_rsq is None else fma_rsq), half_neigh=half,
+                        ntypes=ntypes, natoms=n if natoms is None else natoms,
+                        reneigh_every=reneigh_every, prune_every=prune_every, nstat=nstat,
+                        xprd=xprd, yprd=yprd, zprd=zprd, dt=dt,
+                        dtforce=0.5 * dt if dtforce is None else dtforce, mass=mass,
+                        cutforce=cutforce, cutneigh=cutneigh, epsilon=epsilon, sigma=sigma)
+        self._keep = []
+        if epsilon_per_type is not None:
+            e = np.ascontiguousarray(epsilon_per_type, dtype=np.float64)
+            s = np.ascontiguousarray(sigma_per_type, dtype=np.float64)
+            self._keep += [e, s]
+            p.epsilon_per_type = e.ctypes.data_as(C.POINTER(C.c_double))
+            p.sigma_per_type = s.ctypes.data_as(C.POINTER(C.c_double))
+        self.h = self.lib.orccp_create(C.byref(p))
+        if not self.h:
+            raise ValueError("oracle: unsupported cluster shape or types")
+        self.lib.orccp_set_atoms(self.h, n, x.reshape(-1), v.reshape(-1), t)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.orccp_destroy(self.h)
+            self.h = None
+
+    def setup(self):
+        rc = self.lib.orccp_setup(self.h)
+        if rc != 0:
+            raise RuntimeError("oracle: atom outside the column grid")
+
+    def counts(self):
+        c = np.zeros(8, dtype=np.int32)
+        self.lib.orccp_counts(self.h, c)
+        return _cp_counts(c)
+
+    def _get_slots(self, *a):
+        self.lib.orccp_get_slots(self.h, *a)
+
+    def _get_list(self, nn, nm, nb, im, ld):
+        self.lib.orccp_get_list(self.h, nn, _ptr(nm), nb, _ptr(im), ld)
+
+    def _get_ghosts(self, *a):
+        self.lib.orccp_get_ghosts(self.h, *a)
+
+    def set_slots(self, x=None, v=None):
+        xs = None if x is None else np.ascontiguousarray(x, dtype=np.float64)
+        vs = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+        self.lib.orccp_set_slots(self.h, _ptr(xs), _ptr(vs))
+
+    def iclusters(self):
+        n = self.counts()["ncl"]
+        nat = np.zeros(max(n, 1), dtype=np.int32); b = np.zeros(max(n, 1), dtype=np.int32)
+        bb = np.zeros(max(6 * n, 6))
+        self.lib.orccp_get_iclusters(self.h, nat, _ptr(b), _ptr(bb))
+        return nat[:n], b[:n], bb[:6 * n].reshape(n, 6)
+
+    def jclusters(self):
+        c = self.counts()
+        n = c["ncj"] + c["ngc"]
+        nat = np.zeros(max(n, 1), dtype=np.int32); bb = np.zeros(max(6 * n, 6))
+        self.lib.orccp_get_jclusters(self.h, nat, _ptr(bb), n)
+        return nat[:n], bb[:6 * n].reshape(n, 6)
+
+    def atoms(self):
+        n = self.counts()["nlocal"]
+        x = np.zeros((n, 3)); v = np.zeros((n, 3)); t = np.zeros(n, dtype=np.int32)
+        self.lib.orccp_get_atoms(self.h, _ptr(x), _ptr(v), _ptr(t))
+        return x, v, t
+
+    def bin_geometry(self):
+        ints = np.zeros(7, dtype=np.int32); d = np.zeros(3)
+        self.lib.orccp_bin_geometry(self.h, ints, d, None)
+        st = np.zeros(int(ints[6]), dtype=np.int32)
+        self.lib.orccp_bin_geometry(self.h, ints, d, _ptr(st))
+        keys = ["nbinx", "nbiny", "mbinx", "mbiny", "mbinxlo", "mbinylo", "nstencil"]
+        g = dict(zip(keys, [int(i) for i in ints]))
+        g.update(binsizex=d[0], binsizey=d[1], rbb_sq=d[2], stencil=st)
+        return g
+
+    def columns(self):
+        g = self.bin_geometry()
+        mb = g["mbinx"] * g["mbiny"]
+        start = np.zeros(mb + 1, dtype=np.int32)
+        n = self.lib.orccp_get_columns(self.h, start, np.zeros(1, dtype=np.int32), 0)
+        lst = np.zeros(max(n, 1), dtype=np.int32)
+        self.lib.orccp_get_columns(self.h, start, lst, n)
+        return start, lst[:n]
+
+    def force(self):
+        return self.lib.orccp_compute_force(self.h)
+
+    def prune(self):
+        self.lib.orccp_prune_neighbor(self.h)
+
+    def update_pbc(self, first=0):
+        self.lib.orccp_update_pbc(self.h, first)
+
+    def step(self, n):
+        self.lib.orccp_step(self.h, n)
+
+    def run(self, nsteps, start=0):
+        for n in range(start, start + nsteps):
+            self.step(n)
+
+    def thermo(self):
+        T = C.c_double(); P = C.c_double(); KE = C.c_double(); PE = C.c_double()
+        self.lib.orccp_thermo(self.h, C.byref(T), C.byref(P))
+        self.lib.orccp_energy(self.h, C.byref(KE), C.byref(PE))
+        return dict(T=T.value, P=P.value, KE=KE.value, PE=PE.value, E=KE.value + PE.value)
+
+
+_ref_cp = {}
+
+
+def ref_cp_available(shape="4x4"):
+    return os.path.exists(REF_CP_SO[shape])
+
+
+def _load_ref_cp(shape):
+    if shape not in _ref_cp:
+        lib = C.CDLL(REF_CP_SO[shape])
+        lib.ref_cp_shape.argtypes = [C.POINTER(C.c_int)] * 2
+        lib.ref_cp_shape.restype = C.c_int
+        lib.ref_cp_setup.argtypes = [C.c_int] * 4 + [C.c_char_p] * 2 + [C.c_int]
+        lib.ref_cp_setup.restype = C.c_int
+        lib.ref_cp_counts.argtypes = [_ip]
+        lib.ref_cp_params.argtypes = [_dp]
+        lib.ref_cp_get_atoms.argtypes = [C.c_void_p] * 3
+        lib.ref_cp_get_slots.argtypes = [C.c_void_p] * 4 + [C.c_int]
+        lib.ref_cp_get_iclusters.argtypes = [_ip, _ip, _dp]
+        lib.ref_cp_get_jclusters.argtypes = [_ip, _dp, C.c_int]
+        lib.ref_cp_get_ghosts.argtypes = [_ip, _ip]
+        lib.ref_cp_get_list.argtypes = [_ip, _ip, _ip, C.c_void_p, C.c_int]
+        lib.ref_cp_force.restype = C.c_double
+        lib.ref_cp_step.argtypes = [C.c_int]
+        lib.ref_cp_thermo.argtypes = [C.POINTER(C.c_double)] * 2
+        lib.ref_cp_set_threads.argtypes = [C.c_int]
+        _ref_cp[shape] = lib
+    return _ref_cp[shape]
+
+
+class RefCP(_CpViews):
+    """The reference cluster-pair scheme itself, one build per cluster shape
+    (one system per build and process: its state is global)."""
+
+    def __init__(self, shape="4x4", nx=8, ny=8, nz=8, half=0, param_file=None,
+                 input_file=None, prune_every=0, threads=1):
+        self.lib = _load_ref_cp(shape)
+        m = C.c_int(); n = C.c_int()
+        self.lib.ref_cp_shape(C.byref(m), C.byref(n))
+        self.M, self.N = m.value, n.value
+        self.lib.ref_cp_set_threads(threads)
+        enc = lambda s: None if s is None else s.encode()
+        self.lib.ref_cp_setup(nx, ny, nz, half, enc(param_file), enc(input_file), prune_every)
+
+    def counts(self):
+        c = np.zeros(8, dtype=np.int32)
+        self.lib.ref_cp_counts(c)
+        return _cp_counts(c)
+
+    def _get_slots(self, *a):
+        self.lib.ref_cp_get_slots(*a)
+
+    def _get_list(self, nn, nm, nb, im, ld):
+        self.lib.ref_cp_get_list(nn, nm, nb, _ptr(im), ld)
+
+    def _get_ghosts(self, *a):
+        self.lib.ref_cp_get_ghosts(*a)
+
+    def iclusters(self):
+        n = self.counts()["ncl"]
+        nat = np.zeros(max(n, 1), dtype=np.int32); b = np.zeros(max(n, 1), dtype=np.int32)
+        bb = np.zeros(max(6 * n, 6))
+        self.lib.ref_cp_get_iclusters(nat, b, bb)
+        return nat[:n], b[:n], bb[:6 * n].reshape(n, 6)
+
+    def jclusters(self):
+        c = self.counts()
+        n = c["ncj"] + c["ngc"]
+        nat = np.zeros(max(n, 1), dtype=np.int32); bb = np.zeros(max(6 * n, 6))
+        self.lib.ref_cp_get_jclusters(nat, bb, n)
+        return nat[:n], bb[:6 * n].reshape(n, 6)
+
+    def atoms(self):
+        n = self.counts()["nlocal"]
+        x = np.zeros((n, 3)); v = np.zeros((n, 3)); t = np.zeros(n, dtype=np.int32)
+        self.lib.ref_cp_get_atoms(_ptr(x), _ptr(v), _ptr(t))
+        return x, v, t
+
+    def params(self):
+        d = np.zeros(8)
+        self.lib.ref_cp_params(d)
+        return dict(zip(["xprd", "yprd", "zprd", "dt", "dtforce", "mass", "cutforce",
+                         "cutneigh"], d.tolist()))
+
+    def force(self):
+        return self.lib.ref_cp_force()
+
+    def step(self, n):
+        self.lib.ref_cp_step(n)
+
+    def thermo(self):
+        T = C.c_double(); P = C.c_double()
+        self.lib.ref_cp_thermo(C.byref(T), C.byref(P))
+        return dict(T=T.value, P=P.value)

@@ -19,6 +19,7 @@ def declared(header):
 
 
 @pytest.mark.parametrize("header,exports", [("mdb.h", mdb.EXPORTS),
+                                            ("mdb_cp.h", mdb.CP_EXPORTS),
                                             ("mdb_host.h", mdb.HOST_EXPORTS)])
 def test_library_exports_every_declared_symbol(header, exports):
     lib = mdb.load()
