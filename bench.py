@@ -49,6 +49,7 @@ def parse():
                                           for p in ("mixed", "fp64") for h in ("", "_half")],
                     help="run one variant only (W+K bench steps + force timing), for ncu")
     ap.add_argument("--cells", type=int, default=None, help="fcc cells per side (profiling)")
+    ap.add_argument("--tune", default=None, help="key=value[,key=value] cluster-pair tuning")
     return ap.parse_args()
 
 
@@ -186,6 +187,9 @@ def measure(torch, mdb, kind, precision, args, device, half=0):
     if kind.startswith("cp"):
         s, (x, v, t) = cp_workload(mdb, precision, device, args.cells, half,
                                    cluster_n=int(kind[3]))
+        for kv in (args.tune.split(",") if getattr(args, "tune", None) else []):
+            k, val = kv.split("=")
+            s.tune(k, int(val))
     else:
         make = lj_workload if kind == "lj" else eam_workload
         s, (x, v, t) = make(mdb, precision, device, args.cells, half)

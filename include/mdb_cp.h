@@ -43,6 +43,10 @@ int mdb_cp_destroy(MdbCp* ctx);
 const char* mdb_cp_last_error(const MdbCp* ctx);
 void* mdb_cp_stream(MdbCp* ctx);
 int mdb_cp_synchronize(MdbCp* ctx);
+/* Launch tuning (no counterpart in the reference; results are unchanged):
+ * "force_block" = threads per block of the mixed force kernel (32..512, a
+ * multiple of 32; default 128). */
+int mdb_cp_tune(MdbCp* ctx, const char* key, int value);
 long long mdb_cp_launch_count(const MdbCp* ctx);
 
 /* Atom arrays (createAtom / readAtom output, or any state). */

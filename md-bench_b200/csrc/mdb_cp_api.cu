@@ -208,8 +208,9 @@ static int setup_types(MdbCp* ctx)
         t.sigma3_f[k]   = (float)t.sigma3[k];
         if (t.sqrt_eps[k] != t.sqrt_eps[0] || t.sigma3[k] != t.sigma3[0]) uniform = false;
     }
-    t.uniform  = uniform ? 1 : 0;
-    t.eps0     = t.sqrt_eps[0] * t.sqrt_eps[0];
+    t.uniform     = uniform ? 1 : 0;
+    t.force_block = 128;
+    t.eps0        = t.sqrt_eps[0] * t.sqrt_eps[0];
     t.sigma6_0 = t.sigma3[0] * t.sigma3[0];
     return MDB_OK;
 }
@@ -217,6 +218,18 @@ static int setup_types(MdbCp* ctx)
 extern "C" const char* mdb_cp_last_error(const MdbCp* ctx) { return ctx ? ctx->err.c_str() : ""; }
 extern "C" void* mdb_cp_stream(MdbCp* ctx) { return ctx ? (void*)ctx->s : nullptr; }
 extern "C" long long mdb_cp_launch_count(const MdbCp* ctx) { return ctx ? ctx->launches : 0; }
+
+extern "C" int mdb_cp_tune(MdbCp* ctx, const char* key, int value)
+{
+    if (!ctx || !key) return MDB_ERR_ARG;
+    if (!strcmp(key, "force_block")) {
+        if (value < 32 || value > 512 || value % 32) return MDB_ERR_ARG;
+        drop_graph(ctx);
+        ctx->ty.force_block = value;
+        return MDB_OK;
+    }
+    return fail(ctx, MDB_ERR_ARG, "unknown tuning key");
+}
 
 extern "C" int mdb_cp_synchronize(MdbCp* ctx)
 {

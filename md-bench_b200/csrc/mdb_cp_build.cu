@@ -240,13 +240,6 @@ __device__ __forceinline__ float4 anchor_of(const double4& mn, const double4& mx
     return a;
 }
 
-__device__ __forceinline__ float4 rel_slot(const double4& p, const float4& a)
-{
-    if (slot_type(p) < 0) return make_float4(CP_PAD_F, CP_PAD_F, CP_PAD_F, __int_as_float(-1));
-    return make_float4((float)(p.x - (double)a.x), (float)(p.y - (double)a.y),
-        (float)(p.z - (double)a.z), __int_as_float(slot_type(p)));
-}
-
 __device__ __forceinline__ void zext_max(unsigned long long* zext, double e)
 {
     // non-negative doubles order like their bit patterns
@@ -346,7 +339,7 @@ __global__ void k_build_clusters(int mbins, int mixed, const int* __restrict__ c
         __syncwarp();
         for (int j = lane; j < nclu * M; j += 32) {
             const int slot = k0 * M + j;
-            xr[slot]       = rel_slot(cx[slot], anchor[slot / N]);
+            put_rel(xr, slot, cx[slot], anchor[slot / N]);
         }
     }
 }
@@ -507,14 +500,16 @@ __global__ void k_ghost_first(int N, int* cnt, const int* __restrict__ border,
             float4 a   = anchor_of(mn, mx);
             anchor[cg] = a;
             for (int k = 0; k < N; k++)
-                xr[cg * N + k] = rel_slot(cx[cg * N + k], a);
+                put_rel(xr, cg * N + k, cx[cg * N + k], a);
         }
     } else if (gi == ngc) {
         const int cd = ncj + ngc; // dummy cluster
         for (int k = 0; k < N; k++) {
             cx[cd * N + k] = make_double4(INFINITY, INFINITY, INFINITY, type_bits(-1));
             if (mixed)
-                xr[cd * N + k] = make_float4(CP_PAD_F, CP_PAD_F, CP_PAD_F, __int_as_float(-1));
+                put_rel(xr, cd * N + k,
+                    make_double4(INFINITY, INFINITY, INFINITY, type_bits(-1)),
+                    make_float4(0.f, 0.f, 0.f, 0.f));
         }
         if (mixed) anchor[cd] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
@@ -546,7 +541,7 @@ __global__ void k_ghost_update(int N, int mixed, const int* __restrict__ cnt,
     p.y += (double)(((code >> 2) & 3) - 1) * g.yprd;
     p.z += (double)(((code >> 4) & 3) - 1) * g.zprd;
     cx[cg * N + k] = p;
-    if (mixed) xr[cg * N + k] = rel_slot(p, anchor[cg]);
+    if (mixed) put_rel(xr, cg * N + k, p, anchor[cg]);
 }
 
 void launch_ghost_update(cudaStream_t s, int N, int ngc_cap, int mixed, const int* cnt,
@@ -686,17 +681,19 @@ void launch_merge_columns(cudaStream_t s, int mbins1, int jfac, const int* ncl_c
 }
 
 // ---- buildNeighborCPU (clusterpair/neighbor.c:282-529) ---------------------------
-// One warp per i-cluster; lane k takes stencil column k. Within a column the
-// j-clusters are sorted by bbminz, so the candidates are a window: a binary
-// search skips those whose box lies more than cutneigh below (using the
-// largest z extent of any j-cluster, with a margin), and the scan stops at the
-// first whose box starts more than cutneigh above; both skipped groups fail
-// the reference's test exactly. Each candidate gets the reference's test:
-// box distance squared (z, y, x) below cutneigh^2, accepted below rbb^2, else
-// if any atom pair has fma(dx,dx,fma(dy,dy,dz*dz)) below cutneigh^2. Accepted
-// candidates are kept as bits, counted, prefix-summed across lanes (so the row
-// is stencil order, then column order) and written; the diagonal entry is
-// then swapped to the front as the reference's masked entries are.
+// One warp per i-cluster. Within a column the j-clusters are sorted by bbminz,
+// so the candidates of each stencil column form a window [lo, hi): lane k
+// finds column k's window by two binary searches, skipping below the clusters
+// whose box lies more than cutneigh under the i box (with the largest z extent
+// of any j-cluster and a margin) and above those starting more than cutneigh
+// over it; both skipped groups fail the reference's test exactly. The windows
+// are then concatenated in stencil order and the warp tests 32 candidates at a
+// time, one per lane, with the reference's test: box distance squared (z, y,
+// x) below cutneigh^2, accepted below rbb^2, else if any atom pair has
+// fma(dx,dx,fma(dy,dy,dz*dz)) below cutneigh^2. A ballot keeps the accepted
+// ones in candidate order, so a row is stencil order, then column order; the
+// diagonal entry is then swapped to the front as the reference's masked
+// entries are.
 template <int M, int N>
 __device__ __forceinline__ bool any_pair(const double3* xi, const double4* __restrict__ cj_x,
     double cutsq)
@@ -722,15 +719,20 @@ __device__ __forceinline__ double bb_axis(double imin, double imax, double jmin,
     return dm > 0.0 ? dm : 0.0;
 }
 
+#define CP_LIST_WARPS 4
+
 template <int M, int N>
-__global__ void __launch_bounds__(128) k_build_list(int half, const int* __restrict__ cnt,
-    Geom g, const int* __restrict__ stencil, const int* __restrict__ cbin,
-    const double4* __restrict__ ibbmin, const double4* __restrict__ ibbmax,
-    const double4* __restrict__ jcbbmin, const double4* __restrict__ jcbbmax,
-    const double4* __restrict__ cx, const int* __restrict__ jcol_start,
-    const int* __restrict__ jcol, const unsigned long long* __restrict__ zext, int maxneighs,
-    int ks, int cs, int* list, int* numneigh, int* nmasked, int* cnt_out)
+__global__ void __launch_bounds__(32 * CP_LIST_WARPS) k_build_list(int half, int* cnt, Geom g, const int* __restrict__ stencil,
+    const int* __restrict__ cbin, const double4* __restrict__ ibbmin,
+    const double4* __restrict__ ibbmax, const double4* __restrict__ jcbbmin,
+    const double4* __restrict__ jcbbmax, const double4* __restrict__ cx,
+    const int* __restrict__ jcol_start, const int* __restrict__ jcol,
+    const unsigned long long* __restrict__ zext, int maxneighs, int ks, int cs, int* list,
+    int* numneigh, int* nmasked)
 {
+    __shared__ int s_lo[CP_LIST_WARPS][32];
+    __shared__ int s_ws[CP_LIST_WARPS][32];
+    const int w    = threadIdx.x >> 5;
     const int ci   = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = lane_id();
     if (ci >= cnt[CP_NCL]) return;
@@ -745,81 +747,85 @@ __global__ void __launch_bounds__(128) k_build_list(int half, const int* __restr
     const double zx  = __longlong_as_double((long long)*zext);
     const double zlo = imn.z - g.cutneigh - zx - 1.0e-6;
     const int ib     = cbin[ci];
+    int* row         = list + (size_t)ci * cs;
     int total = 0, diag_pos = -1;
     for (int kb = 0; kb < g.nstencil; kb += 32) {
         const int k = kb + lane;
-        unsigned long long acc0 = 0ull, acc1 = 0ull; // CP_WINDOW_BITS = 128
-        int lo = 0, nacc = 0, my_diag = -1;
+        int lo = 0, wn = 0;
         if (k < g.nstencil) {
             const int jb = ib + stencil[k];
-            int s0 = jcol_start[jb], s1 = jcol_start[jb + 1];
-            int L = s0, R = s1;
+            const int s1 = jcol_start[jb + 1];
+            int L = jcol_start[jb], R = s1;
             while (L < R) {
                 int mid = (L + R) >> 1;
                 if (jcbbmin[mid].z < zlo) L = mid + 1;
                 else R = mid;
             }
             lo = L;
-            for (int m = lo; m < s1; m++) {
-                const double4 jn = jcbbmin[m];
-                if (jn.z - imx.z > g.cutneigh) break;
-                const int cj = jcol[m];
-                if (half && ci_cj0 > cj) continue;
-                if (m - lo >= CP_WINDOW_BITS) {
-                    atomicAdd(&cnt_out[CP_WINDOW], 1);
-                    break;
-                }
-                const double4 jx = jcbbmax[m];
-                double d = bb_axis(imn.z, imx.z, jn.z, jx.z);
-                d        = d * d;
-                double e = bb_axis(imn.y, imx.y, jn.y, jx.y);
-                d += e * e;
-                e = bb_axis(imn.x, imx.x, jn.x, jx.x);
-                d += e * e;
-                if (d < g.cutneighsq) {
-                    bool ok = d < g.rbb_sq;
-                    if (!ok) ok = any_pair<M, N>(xi, cx + (size_t)cj * N, g.cutneighsq);
-                    if (ok) {
-                        const int bit = m - lo;
-                        if (bit < 64) acc0 |= 1ull << bit;
-                        else acc1 |= 1ull << (bit - 64);
-                        if (cj == ci_cj0) my_diag = nacc;
-                        nacc++;
-                    }
-                }
+            R  = s1;
+            while (L < R) {
+                int mid = (L + R) >> 1;
+                if (jcbbmin[mid].z - imx.z > g.cutneigh) R = mid;
+                else L = mid + 1;
             }
+            wn = L - lo;
         }
-        int incl = nacc;
+        int incl = wn;
         for (int o = 1; o < 32; o <<= 1) {
             int t = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += t;
         }
-        int p = total + incl - nacc;
-        if (my_diag >= 0) diag_pos = p + my_diag;
-        for (int w = 0; w < 2; w++) {
-            unsigned long long bits = w ? acc1 : acc0;
-            while (bits) {
-                int bit = __ffsll((long long)bits) - 1;
-                bits &= bits - 1;
-                if (p < maxneighs) list[(size_t)p * ks + (size_t)ci * cs] = jcol[lo + w * 64 + bit];
-                p++;
+        const int W     = __shfl_sync(0xffffffffu, incl, 31);
+        s_lo[w][lane]   = lo;
+        s_ws[w][lane]   = incl - wn;
+        __syncwarp();
+        for (int t0 = 0; t0 < W; t0 += 32) {
+            const int t = t0 + lane;
+            bool ok     = false;
+            int cj      = -1;
+            if (t < W) {
+                int a = 0, z = 31; // last column whose window starts at or before t
+                while (a < z) {
+                    int mid = (a + z + 1) >> 1;
+                    if (s_ws[w][mid] <= t) a = mid;
+                    else z = mid - 1;
+                }
+                const int m = s_lo[w][a] + (t - s_ws[w][a]);
+                cj          = jcol[m];
+                if (!(half && ci_cj0 > cj)) {
+                    const double4 jn = jcbbmin[m], jx = jcbbmax[m];
+                    double d = bb_axis(imn.z, imx.z, jn.z, jx.z);
+                    d        = d * d;
+                    double e = bb_axis(imn.y, imx.y, jn.y, jx.y);
+                    d += e * e;
+                    e = bb_axis(imn.x, imx.x, jn.x, jx.x);
+                    d += e * e;
+                    if (d < g.cutneighsq)
+                        ok = d < g.rbb_sq || any_pair<M, N>(xi, cx + (size_t)cj * N, g.cutneighsq);
+                }
             }
+            const unsigned bal = __ballot_sync(0xffffffffu, ok);
+            if (ok) {
+                const int p = total + __popc(bal & ((1u << lane) - 1u));
+                if (p < maxneighs) row[(size_t)p * ks] = cj;
+                if (cj == ci_cj0) diag_pos = p;
+            }
+            total += __popc(bal);
         }
-        total += __shfl_sync(0xffffffffu, incl, 31);
+        __syncwarp();
     }
     // the diagonal entry (mask != all) goes to the front, clusterpair/neighbor.c:599-649
     diag_pos = __reduce_max_sync(0xffffffffu, diag_pos);
     __syncwarp();
     if (lane == 0) {
         if (diag_pos > 0 && diag_pos < maxneighs) {
-            int* row                        = list + (size_t)ci * cs;
-            int first                       = row[0];
-            row[0]                          = row[(size_t)diag_pos * ks];
-            row[(size_t)diag_pos * ks]      = first;
+            int first                  = row[0];
+            row[0]                     = row[(size_t)diag_pos * ks];
+            row[(size_t)diag_pos * ks] = first;
         }
         numneigh[ci] = total < maxneighs ? total : maxneighs;
         nmasked[ci]  = diag_pos >= 0 ? 1 : 0;
-        if (total >= maxneighs) atomicMax(&cnt_out[CP_MAXNEED], total);
+        if (total >= maxneighs) atomicMax(&cnt[CP_MAXNEED], total);
     }
 }
 
@@ -830,16 +836,17 @@ void launch_build_list(cudaStream_t s, int M, int N, int half, int ncl_cap, cons
     int ks, int cs, int* list, int* numneigh, int* nmasked, int* cnt_out)
 {
     long long threads = (long long)ncl_cap * 32;
-    int blocks        = mdb_blocks(threads, 128);
+    int blocks        = mdb_blocks(threads, 32 * CP_LIST_WARPS);
     (void)M;
+    (void)cnt;
     if (N == 4)
-        k_build_list<4, 4><<<blocks, 128, 0, s>>>(half, cnt, g, stencil, cbin, ibbmin, ibbmax,
-            jcbbmin, jcbbmax, cx, jcol_start, jcol, zext, maxneighs, ks, cs, list, numneigh,
-            nmasked, cnt_out);
+        k_build_list<4, 4><<<blocks, 32 * CP_LIST_WARPS, 0, s>>>(half, cnt_out, g, stencil, cbin,
+            ibbmin, ibbmax, jcbbmin, jcbbmax, cx, jcol_start, jcol, zext, maxneighs, ks, cs, list,
+            numneigh, nmasked);
     else
-        k_build_list<4, 8><<<blocks, 128, 0, s>>>(half, cnt, g, stencil, cbin, ibbmin, ibbmax,
-            jcbbmin, jcbbmax, cx, jcol_start, jcol, zext, maxneighs, ks, cs, list, numneigh,
-            nmasked, cnt_out);
+        k_build_list<4, 8><<<blocks, 32 * CP_LIST_WARPS, 0, s>>>(half, cnt_out, g, stencil, cbin,
+            ibbmin, ibbmax, jcbbmin, jcbbmax, cx, jcol_start, jcol, zext, maxneighs, ks, cs, list,
+            numneigh, nmasked);
     g_launches++;
 }
 

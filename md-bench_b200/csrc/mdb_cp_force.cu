@@ -175,50 +175,119 @@ __device__ __forceinline__ void warp_reduce_12(float (&v)[12], int lane)
     v[2] = q[2];
 }
 
-template <int N, bool HALF, bool ENERGY, bool UNIFORM, bool DIAG>
-__device__ __forceinline__ void mixed_entry(const float4 (&xi)[4], const float (&sei)[4],
-    const float (&s3i)[4], const float4& xj, float sej, float s3j, int ai0, int b,
-    float cutforcesq, float c48, float c24, float sig6u, double eps0, double ew, float (&f)[12],
-    float3& fj, double& e)
+// PTX rcp.approx.ftz.f32: at most 1 ulp from 1/x, one MUFU operation
+__device__ __forceinline__ float rcp_approx(float x)
 {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// Packed FP32 pairs: sm_100 executes add/sub/mul/fma on two f32 lanes of a
+// 64-bit register in one instruction (PTX .f32x2), so each thread carries its
+// 4 i atoms as two packed pairs (atoms 0,1 and 2,3) and computes two pairs per
+// instruction.
+typedef unsigned long long f2;
+
+__device__ __forceinline__ f2 f2_pack(float lo, float hi)
+{
+    f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2_unpack(f2 v, float& lo, float& hi)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2 f2_sub(f2 a, f2 b)
+{
+    f2 r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f2 f2_mul(f2 a, f2 b)
+{
+    f2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f2 f2_fma(f2 a, f2 b, f2 c)
+{
+    f2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+
+// The i side of one i-cluster: coordinates and type parameters of atoms
+// (0,1) and (2,3) packed.
+struct IPack {
+    f2 x[2], y[2], z[2];
+    f2 se[2], s3[2];
+};
+
+// Pairs of one j atom with the 4 i atoms, two per packed instruction. With
+// u = 1/r^2 (0 outside the cutoff) and s = sigma^6, the LJ force over r is
+// 48 eps s u^4 (s u^3 - 1/2) = u^4 (A u^3 - B), A = 48 eps s^2, B = 24 eps s,
+// for uniform types. The i forces accumulate in fx/fy/fz (packed like the i
+// atoms); half lists also accumulate sum(d * force) for the j atom in g (its
+// reaction is minus the sum of both halves).
+template <bool HALF, bool ENERGY, bool UNIFORM, bool DIAG>
+__device__ __forceinline__ void mixed_entry(const IPack& ip, const float4& xj, float sej,
+    float s3j, int ai0, int b, float cutforcesq, f2 A2, f2 mB2, float sig6u, double eps0,
+    double ew, f2 (&fx)[2], f2 (&fy)[2], f2 (&fz)[2], f2& gx, f2& gy, f2& gz, double& e)
+{
+    const f2 XJ = f2_pack(xj.x, xj.x), YJ = f2_pack(xj.y, xj.y), ZJ = f2_pack(xj.z, xj.z);
 #pragma unroll
-    for (int a = 0; a < 4; a++) {
-        const float dx  = xi[a].x - xj.x;
-        const float dy  = xi[a].y - xj.y;
-        const float dz  = xi[a].z - xj.z;
-        const float rsq = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
-        const float sr2 = __fdividef(1.0f, rsq);
-        float sr6       = __fmul_rn(__fmul_rn(sr2, sr2), sr2);
-        float t;
+    for (int h = 0; h < 2; h++) {
+        const f2 DX  = f2_sub(ip.x[h], XJ);
+        const f2 DY  = f2_sub(ip.y[h], YJ);
+        const f2 DZ  = f2_sub(ip.z[h], ZJ);
+        const f2 RSQ = f2_fma(DX, DX, f2_fma(DY, DY, f2_mul(DZ, DZ)));
+        float r0, r1;
+        f2_unpack(RSQ, r0, r1);
+        bool in0 = r0 < cutforcesq, in1 = r1 < cutforcesq;
+        if (DIAG) {
+            const int a0 = ai0 + 2 * h, a1 = a0 + 1;
+            in0 = in0 && (HALF ? (a0 < b) : (a0 != b));
+            in1 = in1 && (HALF ? (a1 < b) : (a1 != b));
+        }
+        float u0 = rcp_approx(r0), u1 = rcp_approx(r1);
+        u0          = in0 ? u0 : 0.0f;
+        u1          = in1 ? u1 : 0.0f;
+        const f2 U  = f2_pack(u0, u1);
+        const f2 U2 = f2_mul(U, U);
+        const f2 U3 = f2_mul(U2, U);
+        f2 F, SR6 = 0, EP = 0;
         if (UNIFORM) {
-            sr6 = __fmul_rn(sr6, sig6u);
-            t   = __fmaf_rn(c48, sr6, -c24);
+            F = f2_mul(f2_mul(U2, U2), f2_fma(A2, U3, mB2));
+            if (ENERGY) SR6 = f2_mul(f2_pack(sig6u, sig6u), U3);
         } else {
-            sr6             = __fmul_rn(sr6, __fmul_rn(s3i[a], s3j));
-            const float eps = __fmul_rn(sei[a], sej);
-            t               = __fmul_rn(eps, __fmaf_rn(48.0f, sr6, -24.0f));
+            SR6 = f2_mul(f2_mul(ip.s3[h], f2_pack(s3j, s3j)), U3);
+            EP  = f2_mul(ip.se[h], f2_pack(sej, sej));
+            F   = f2_mul(f2_mul(U, SR6),
+                f2_mul(EP, f2_fma(f2_pack(48.0f, 48.0f), SR6, f2_pack(-24.0f, -24.0f))));
         }
-        float force = __fmul_rn(__fmul_rn(sr2, sr6), t);
-        bool in     = rsq < cutforcesq;
-        if (DIAG) in = in && (HALF ? (ai0 + a < b) : (ai0 + a != b));
-        force = in ? force : 0.0f;
-        f[3 * a + 0] = __fmaf_rn(dx, force, f[3 * a + 0]);
-        f[3 * a + 1] = __fmaf_rn(dy, force, f[3 * a + 1]);
-        f[3 * a + 2] = __fmaf_rn(dz, force, f[3 * a + 2]);
+        fx[h] = f2_fma(DX, F, fx[h]);
+        fy[h] = f2_fma(DY, F, fy[h]);
+        fz[h] = f2_fma(DZ, F, fz[h]);
         if (HALF) {
-            fj.x = __fmaf_rn(-dx, force, fj.x);
-            fj.y = __fmaf_rn(-dy, force, fj.y);
-            fj.z = __fmaf_rn(-dz, force, fj.z);
+            gx = f2_fma(DX, F, gx);
+            gy = f2_fma(DY, F, gy);
+            gz = f2_fma(DZ, F, gz);
         }
-        if (ENERGY && in) {
-            const double eps = UNIFORM ? eps0 : (double)__fmul_rn(sei[a], sej);
-            e += ew * 4.0 * eps * (double)sr6 * ((double)sr6 - 1.0);
+        if (ENERGY) {
+            float s0, s1, e0, e1;
+            f2_unpack(SR6, s0, s1);
+            f2_unpack(EP, e0, e1);
+            const double E0 = UNIFORM ? eps0 : (double)e0, E1 = UNIFORM ? eps0 : (double)e1;
+            if (in0) e += ew * 4.0 * E0 * (double)s0 * ((double)s0 - 1.0);
+            if (in1) e += ew * 4.0 * E1 * (double)s1 * ((double)s1 - 1.0);
         }
     }
 }
 
-// j data of one list entry: position shifted into the i-cluster's anchor
-// frame (the anchor difference is exact), type parameters
+// j data of one list entry: the atom's position moved into the i-cluster's
+// anchor frame (the anchor difference is exact), its type bits in .w
 struct JEntry {
     float4 x;
     int cj;
@@ -243,8 +312,18 @@ __device__ __forceinline__ JEntry load_entry(int cj, int b, const float4* __rest
     return j;
 }
 
+// One warp per i-cluster (M = 4 atoms, held by every lane as two packed
+// pairs). The warp takes 32 / N list entries at a time; lane (e, b) owns atom b
+// of entry e and computes its pairs with the 4 i atoms, two per packed
+// instruction. The list is read in coalesced blocks of 32 entries (the next
+// block in flight) and the j data of the next iteration is loaded while the
+// current one computes. Full lists reduce the i forces across the warp once
+// per i-cluster; half lists also accumulate each j atom's reaction over the 4
+// i atoms in the lane and add it with one atomic per component. Padding slots
+// sit at +1e18 (j) and invalid i atoms are moved to -1e18, so they fall outside
+// the cutoff without INF arithmetic.
 template <int N, bool HALF, bool ENERGY, bool UNIFORM>
-__global__ void __launch_bounds__(CP_FORCE_THREADS) k_force_mixed(const int* __restrict__ cnt,
+__global__ void __launch_bounds__(512) k_force_mixed(const int* __restrict__ cnt,
     const float4* __restrict__ xr, const float4* __restrict__ anchor, Types ty,
     float cutforcesq, const int* __restrict__ list, int ks, int cs,
     const int* __restrict__ numneigh, float4* cf32, double* epart)
@@ -281,18 +360,23 @@ __global__ void __launch_bounds__(CP_FORCE_THREADS) k_force_mixed(const int* __r
             sei[a] = UNIFORM ? 0.f : s_se[t];
             s3i[a] = UNIFORM ? 0.f : s_s3[t];
         }
-        const float c48   = (float)(48.0 * ty.eps0);
-        const float c24   = (float)(24.0 * ty.eps0);
-        const float sig6u = (float)ty.sigma6_0;
-        float f[12];
+        IPack ip;
 #pragma unroll
-        for (int i = 0; i < 12; i++)
-            f[i] = 0.0f;
+        for (int h = 0; h < 2; h++) {
+            ip.x[h]  = f2_pack(xi[2 * h].x, xi[2 * h + 1].x);
+            ip.y[h]  = f2_pack(xi[2 * h].y, xi[2 * h + 1].y);
+            ip.z[h]  = f2_pack(xi[2 * h].z, xi[2 * h + 1].z);
+            ip.se[h] = f2_pack(sei[2 * h], sei[2 * h + 1]);
+            ip.s3[h] = f2_pack(s3i[2 * h], s3i[2 * h + 1]);
+        }
+        const float cA    = (float)(48.0 * ty.eps0 * ty.sigma6_0 * ty.sigma6_0);
+        const float cB    = (float)(24.0 * ty.eps0 * ty.sigma6_0);
+        const float sig6u = (float)ty.sigma6_0;
+        const f2 A2 = f2_pack(cA, cA), mB2 = f2_pack(-cB, -cB);
+        f2 fx[2] = {0, 0}, fy[2] = {0, 0}, fz[2] = {0, 0};
         const int eidx = lane / N, b = lane - eidx * N;
         const int nn   = numneigh[ci];
         const int* row = list + (size_t)ci * cs;
-        // software pipeline: list entries in blocks of 32 (one coalesced load,
-        // the next block in flight), j data one iteration ahead
         int lst_cur = lane < nn ? __ldg(&row[(size_t)lane * ks]) : -1;
         int lst_nxt = 32 + lane < nn ? __ldg(&row[(size_t)(32 + lane) * ks]) : -1;
         JEntry cur  = load_entry<N>(__shfl_sync(0xffffffffu, lst_cur, eidx), b, xr, anchor, ai);
@@ -302,7 +386,7 @@ __global__ void __launch_bounds__(CP_FORCE_THREADS) k_force_mixed(const int* __r
                 lst_cur = lst_nxt;
                 lst_nxt = kn + 32 + lane < nn ? __ldg(&row[(size_t)(kn + 32 + lane) * ks]) : -1;
             }
-            const int cjn  = __shfl_sync(0xffffffffu, lst_cur, (kn & 31) + eidx);
+            const int cjn   = __shfl_sync(0xffffffffu, lst_cur, (kn & 31) + eidx);
             const JEntry nx = load_entry<N>(kn < nn ? cjn : -1, b, xr, anchor, ai);
             const int cj    = cur.cj;
             float sej = 0.f, s3j = 0.f;
@@ -312,23 +396,34 @@ __global__ void __launch_bounds__(CP_FORCE_THREADS) k_force_mixed(const int* __r
                 sej   = s_se[t];
                 s3j   = s_s3[t];
             }
-            float3 fj = make_float3(0.f, 0.f, 0.f);
+            f2 gx = 0, gy = 0, gz = 0;
             // energy weight: full lists see every pair twice; half lists once,
             // except pairs with ghost atoms, which both owners list
             const double ew = (!HALF || cj * N + b >= nloc) ? 0.5 : 1.0;
             if (cj == ci_cj0)
-                mixed_entry<N, HALF, ENERGY, UNIFORM, true>(xi, sei, s3i, cur.x, sej, s3j, ai0,
-                    b, cutforcesq, c48, c24, sig6u, ty.eps0, ew, f, fj, e);
+                mixed_entry<HALF, ENERGY, UNIFORM, true>(ip, cur.x, sej, s3j, ai0, b, cutforcesq,
+                    A2, mB2, sig6u, ty.eps0, ew, fx, fy, fz, gx, gy, gz, e);
             else
-                mixed_entry<N, HALF, ENERGY, UNIFORM, false>(xi, sei, s3i, cur.x, sej, s3j, ai0,
-                    b, cutforcesq, c48, c24, sig6u, ty.eps0, ew, f, fj, e);
+                mixed_entry<HALF, ENERGY, UNIFORM, false>(ip, cur.x, sej, s3j, ai0, b,
+                    cutforcesq, A2, mB2, sig6u, ty.eps0, ew, fx, fy, fz, gx, gy, gz, e);
             if (HALF && cj >= 0 && cj * N + b < nloc && __float_as_int(cur.x.w) >= 0) {
                 float4* dst = &cf32[cj * N + b];
-                atomicAdd(&dst->x, fj.x);
-                atomicAdd(&dst->y, fj.y);
-                atomicAdd(&dst->z, fj.z);
+                float lo, hi;
+                f2_unpack(gx, lo, hi);
+                atomicAdd(&dst->x, -(lo + hi));
+                f2_unpack(gy, lo, hi);
+                atomicAdd(&dst->y, -(lo + hi));
+                f2_unpack(gz, lo, hi);
+                atomicAdd(&dst->z, -(lo + hi));
             }
             cur = nx;
+        }
+        float f[12];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            f2_unpack(fx[h], f[6 * h + 0], f[6 * h + 3]);
+            f2_unpack(fy[h], f[6 * h + 1], f[6 * h + 4]);
+            f2_unpack(fz[h], f[6 * h + 2], f[6 * h + 5]);
         }
         warp_reduce_12(f, lane);
         if ((lane & 7) == 0) {
@@ -356,8 +451,13 @@ static void run_mixed(cudaStream_t s, int blocks, const int* cnt, const float4* 
     const float4* anchor, const Types& ty, float cutforcesq, const int* list, int ks, int cs,
     const int* numneigh, float4* cf32, double* epart)
 {
-    k_force_mixed<N, HALF, ENERGY, UNIFORM><<<blocks, CP_FORCE_THREADS, 0, s>>>(cnt, xr, anchor,
-        ty, cutforcesq, list, ks, cs, numneigh, cf32, epart);
+    // blocks of ty.force_block threads: consecutive i-clusters (z neighbours in
+    // one column) share most of their j-clusters, so larger blocks keep more of
+    // that reuse in one SM's L1
+    const int nt = ty.force_block;
+    const int nb = (int)(((long long)blocks * CP_FORCE_THREADS + nt - 1) / nt);
+    k_force_mixed<N, HALF, ENERGY, UNIFORM><<<nb, nt, 0, s>>>(cnt, xr, anchor, ty, cutforcesq,
+        list, ks, cs, numneigh, cf32, epart);
 }
 
 template <int N, bool HALF>
@@ -424,11 +524,7 @@ __global__ void k_cp_integrate(int M, int N, const int* __restrict__ cnt, double
         p.y += dt * v.y;
         p.z += dt * v.z;
         cx[s] = p;
-        if (xr) {
-            const float4 a = anchor[s / N];
-            xr[s] = make_float4((float)(p.x - (double)a.x), (float)(p.y - (double)a.y),
-                (float)(p.z - (double)a.z), __int_as_float(slot_type(p)));
-        }
+        if (xr) put_rel(xr, s, p, anchor[s / N]);
     }
     cv[s] = v;
 }

@@ -11,8 +11,8 @@
 //                            (padding positions are +INF as in the reference)
 //     cv  double4 (locals), cf double4 (FP64 forces, locals + ghosts)
 //     xr  float4             mixed path: position relative to the anchor of the
-//                            slot's j-cluster, .w = type bits; padding holds a
-//                            large finite sentinel
+//                            slot's j-cluster, .w = type bits (-1 for padding,
+//                            whose position holds a large finite sentinel)
 //     cf32 float4            mixed path forces
 //   per i-cluster: inat, cbin, cl_first (atom index of its first atom in the
 //     next updateSingleAtoms), ibbmin/ibbmax double4 (bbox)
@@ -69,11 +69,24 @@ struct Types {
     double sqrt_eps[MDB_MAX_TYPES], sigma3[MDB_MAX_TYPES];
     float sqrt_eps_f[MDB_MAX_TYPES], sigma3_f[MDB_MAX_TYPES];
     double eps0, sigma6_0; // uniform case
+    int force_block;       // threads per block of the mixed force kernel (tunable)
 };
 
 __device__ __forceinline__ int slot_type(const double4& p) { return (int)__double_as_longlong(p.w); }
 
 __device__ __forceinline__ double type_bits(int t) { return __longlong_as_double((long long)t); }
+
+// mixed-path position of one slot, relative to the anchor a of its j-cluster
+__device__ __forceinline__ void put_rel(float4* xr, int slot, const double4& p, const float4& a)
+{
+    const int t = slot_type(p);
+    if (t < 0) {
+        xr[slot] = make_float4(CP_PAD_F, CP_PAD_F, CP_PAD_F, __int_as_float(-1));
+    } else {
+        xr[slot] = make_float4((float)(p.x - (double)a.x), (float)(p.y - (double)a.y),
+            (float)(p.z - (double)a.z), __int_as_float(t));
+    }
+}
 
 // coord2bin / coord2bin2D, clusterpair/neighbor.c:1366-1407
 __device__ __forceinline__ void coord2bin2d(const Geom& g, double x, double y, int& ix, int& iy)

@@ -86,7 +86,7 @@ EXPORTS = [
 ]
 # every symbol include/mdb_cp.h declares
 CP_EXPORTS = [
-    "mdb_cp_create", "mdb_cp_destroy", "mdb_cp_last_error", "mdb_cp_stream", "mdb_cp_synchronize",
+    "mdb_cp_create", "mdb_cp_destroy", "mdb_cp_last_error", "mdb_cp_stream", "mdb_cp_synchronize", "mdb_cp_tune",
     "mdb_cp_launch_count", "mdb_cp_set_atoms", "mdb_cp_get_atoms", "mdb_cp_build_clusters",
     "mdb_cp_define_jclusters", "mdb_cp_setup_pbc", "mdb_cp_update_pbc", "mdb_cp_bin_jclusters",
     "mdb_cp_build_neighbor", "mdb_cp_prune_neighbor", "mdb_cp_update_single_atoms",
@@ -161,6 +161,7 @@ def load():
         "mdb_cp_get_neighbor_list": ([vp, vp, vp, vp, ip], ip),
         "mdb_cp_get_columns": ([vp, vp, vp, ip], ip),
         "mdb_cp_get_geometry": ([vp, vp, vp, vp, ip], ip),
+        "mdb_cp_tune": ([vp, C.c_char_p, ip], ip),
     })
     for name in ("mdb_cp_synchronize", "mdb_cp_build_clusters", "mdb_cp_define_jclusters",
                  "mdb_cp_setup_pbc",
@@ -714,6 +715,9 @@ class ClusterSystem:
 
     def synchronize(self):
         self._call("mdb_cp_synchronize")
+
+    def tune(self, key, value):
+        self._ck(self.lib.mdb_cp_tune(self.h, key.encode(), int(value)), "mdb_cp_tune")
 
     @property
     def stream(self):
