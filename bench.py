@@ -1,14 +1,16 @@
 """MD-Bench short-range timestep on B200: atom-steps/s, mixed FP32 vs FP64.
 
 One bench step = one rebuild period of the reference loop (reneigh_every = 20
-MD timesteps: 19 plain steps and one step with wrap, ghost map, binning and
-list build), thermo sampled every nstat = 100 steps as the reference does.
+MD timesteps: 19 plain steps and one step with the full rebuild), thermo
+sampled every nstat = 100 steps as the reference does.
 
-Headline (``value``): LJ, fcc 64^3 cells = 1,048,576 atoms, reduced density
-0.8442, T 1.44, cutoff 2.5 + skin 0.3, full Verlet lists, mixed precision.
-The same run reports the FP64 path on the same workload and both EAM paths on
-Cu fcc 32^3 cells (131,072 atoms, a = 3.615 A, 1600 K, funcfl Cu_u3), with
-the mixed path's force error and 1000-step energy drift against FP64.
+Headline (``value``): the cluster-pair scheme (GROMACS-style 4x4 clusters,
+bounding-box pruned lists) on LJ fcc 64^3 cells = 1,048,576 atoms, reduced
+density 0.8442, T 1.44, cutoff 2.5 + skin 0.3, half lists, mixed precision.
+The same run reports every other cluster-pair variant (4x4/4x8, full/half,
+mixed/FP64), the Verlet-list scheme on the same workload and both EAM paths on
+Cu fcc 32^3 cells (131,072 atoms, a = 3.615 A, 1600 K, funcfl Cu_u3), each
+mixed variant with its force error against FP64 and the energy drifts.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -34,8 +36,12 @@ EAM_CELLS = 32
 EAM_A = 3.615
 EAM_T = 1600.0
 EAM_FILE = os.path.join(ROOT, "tests", "golden", "data", "Cu_u3.eam")
-REF_BIN = os.path.join(ROOT, "oracle", "_ref", "MDBench-VL")
+REF_CP = {shape: os.path.join(ROOT, "oracle", "_ref", f"MDBench-CP-{shape}")
+          for shape in ("4x4", "4x8")}
 METRIC = "atom-steps/s, LJ+EAM mixed-FP32 vs FP64 on 1 B200 at stated force error"
+# headline workload: GROMACS-style 4x4 cluster pairs, half lists, mixed precision
+HEAD = {"kind": "cp44", "precision": "mixed", "half": 1}
+HEAD_WORKLOAD = f"lj-fcc-{LJ_CELLS}^3-clusterpair-4x4-half-mixed"
 
 
 def parse():
@@ -209,14 +215,14 @@ def measure(torch, mdb, kind, precision, args, device, half=0):
 def e2e(torch, s, init, steps, every):
     """Same metric through the public C ABI with host buffers: each step uploads
     the atoms from pinned host memory, runs setup + one rebuild period, and
-    reads positions, velocities and forces back."""
+    reads positions and velocities back."""
     x, v, t = init
     n = len(t)
     hx = torch.from_numpy(np.ascontiguousarray(x)).pin_memory().numpy()
     hv = torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy()
     ht = torch.from_numpy(np.ascontiguousarray(t)).pin_memory().numpy()
     bi = hx.nbytes + hv.nbytes + ht.nbytes
-    bo = 3 * 3 * 8 * n + 4 * n
+    bo = 2 * 3 * 8 * n + 4 * n
     s.synchronize()
     t0 = time.perf_counter()
     for k in range(steps):
@@ -230,22 +236,43 @@ def e2e(torch, s, init, steps, every):
                 d2h_bytes_per_step=bo)
 
 
-def cpu_baseline(kind_sample_steps=20):
-    """The reference CPU build on this host (all cores), bounded sample."""
+def host_has_avx512():
+    try:
+        with open("/proc/cpuinfo") as f:
+            return "avx512f" in f.read()
+    except OSError:
+        return False
+
+
+def ref_cp_binary():
+    """The fastest reference cluster-pair build this host can run."""
+    if host_has_avx512() and os.path.exists(REF_CP["4x8"]):
+        return REF_CP["4x8"], "4x8 AVX-512"
+    if os.path.exists(REF_CP["4x4"]):
+        return REF_CP["4x4"], "4x4 AVX2"
+    return None, None
+
+
+def cpu_baseline(md_steps=20, half=1):
+    """The reference CPU cluster-pair build on this host (all cores), a bounded
+    sample of the headline workload: LJ fcc 64^3, half lists when the headline
+    uses them, md_steps steps with one rebuild."""
     cores = os.cpu_count() or 1
-    if os.path.exists(REF_BIN):
+    binary, shape = ref_cp_binary()
+    if binary is not None:
         env = dict(os.environ, OMP_NUM_THREADS=str(cores), OMP_SCHEDULE="static",
                    OMP_PROC_BIND="close")
-        out = subprocess.run([REF_BIN, "-nx", str(LJ_CELLS), "-ny", str(LJ_CELLS), "-nz",
-                              str(LJ_CELLS), "-n", str(kind_sample_steps)], env=env,
-                             capture_output=True, text=True, timeout=900).stdout
+        out = subprocess.run([binary, "-nx", str(LJ_CELLS), "-ny", str(LJ_CELLS), "-nz",
+                              str(LJ_CELLS), "-n", str(md_steps), "-half", str(half)], env=env,
+                             capture_output=True, text=True, timeout=1200).stdout
         for line in out.splitlines():
             if "atom updates/us" in line:
                 val = float(line.split("|")[1].split()[0]) * 1e6
                 return dict(value=val, unit="atom-steps/s", cores=cores, kind="reference",
-                            sample=f"reference VL FP64 strict build, LJ {LJ_CELLS}^3 "
-                                   f"(1,048,576 atoms), {kind_sample_steps} steps incl. one "
-                                   "rebuild, OpenMP static")
+                            sample=f"reference cluster-pair {shape} build (-Ofast, OpenMP), "
+                                   f"LJ {LJ_CELLS}^3 (1,048,576 atoms), "
+                                   f"{'half' if half else 'full'} lists, {md_steps} steps "
+                                   "incl. one rebuild; its own Performance line")
         raise RuntimeError("reference run printed no performance line")
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle  # checker only: timed as the CPU baseline
@@ -254,27 +281,80 @@ def cpu_baseline(kind_sample_steps=20):
     o.setup()
     o.force()
     t0 = time.perf_counter()
-    o.run(kind_sample_steps)
+    o.run(md_steps)
     secs = time.perf_counter() - t0
-    return dict(value=32 ** 3 * 4 * kind_sample_steps / secs, unit="atom-steps/s", cores=1,
-                kind="port", sample=f"C restatement, LJ 32^3, {kind_sample_steps} steps")
+    return dict(value=32 ** 3 * 4 * md_steps / secs, unit="atom-steps/s", cores=1,
+                kind="port", sample=f"C restatement, LJ 32^3, {md_steps} steps")
 
 
 def reference_arm(args, rank):
     if rank != 0:
         return
     steps = 20 * max(args.steps // 5, 1)
-    cb = cpu_baseline(steps)
+    cb = cpu_baseline(steps, half=HEAD["half"])
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"],
             "unit": "atom-steps/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"lj-fcc-{LJ_CELLS}^3-verletlist-full", "natoms": 1048576,
-                       "md_steps": steps},
+            "config": {"workload": HEAD_WORKLOAD, "natoms": 1048576, "md_steps": steps},
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def fp32_peak():
+    """FP32 SIMT peak from the measured max SM clock: 148 SMs x 128 FP32 lanes x
+    2 flops per FMA (no FP32 figure is measured by the pool)."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            mhz = float(json.load(f)["sm_max_mhz"])
+        src = "derived from sm_max_mhz of MEASURED_PEAKS.json"
+    except Exception:
+        mhz, src = 1965.0, "derived from the nominal 1965 MHz"
+    return 148 * 128 * 2 * mhz * 1e6 / 1e12, src
+
+
+def pairs_in_cutoff(x, box, rc):
+    """P_c: ordered atom pairs inside the force cutoff per atom (periodic)."""
+    from scipy.spatial import cKDTree
+    xw = np.mod(x, box)
+    tree = cKDTree(xw, boxsize=box)
+    return (tree.count_neighbors(tree, rc) - len(x)) / len(x)
+
+
+def cp_flops_per_atom(pc, half):
+    """Algorithmic flops per atom-step of the cluster-pair LJ force: 24 per
+    in-cutoff pair (3 sub, 3 mul + 2 add, 1 cmp, 1 div, 3 mul, 5 force, 6 for the
+    accumulation), half lists P_c/2 pairs x (24 + 3 for the reaction)."""
+    return pc / 2 * 27 if half else pc * 24
+
+
+def drift(m):
+    e = [m["th0"]["E"]] + [q["E"] for q in m["samples"]]
+    return float((e[-1] - e[0]) / abs(e[0]))
+
+
+def force_compare(mix, f64, kind):
+    """Mixed force against FP64 on the FP64 run's final state (both systems get
+    the same atoms and rebuild)."""
+    sm, sf = mix["system"], f64["system"]
+    if kind.startswith("cp"):
+        x, v, t = sf.atoms()
+        for s in (sf, sm):
+            s.set_atoms(x, v, t)
+            s.setup()
+        nat = sm.iclusters()[0]
+        valid = np.concatenate([np.arange(4) < k for k in nat])
+        fm = sm.slots()[2][:len(valid)][valid]
+        ff = sf.slots()[2][:len(valid)][valid]
+    else:
+        x, v, _, t = sf.atoms()
+        for s in (sf, sm):
+            s.set_atoms(x, v, t)
+            s.setup()
+        fm, ff = sm.atoms()[2], sf.atoms()[2]
+    return rel_force_err(fm, ff)
 
 
 def main():
@@ -313,10 +393,10 @@ def main():
                           "launches": m["launches"]}), flush=True)
         return
 
-    # headline: LJ 1M atoms, mixed precision
+    # headline: the cluster-pair scheme on LJ 1M atoms, mixed precision
     barrier()
     clk = Clocks(local)
-    head = measure(torch, mdb, "lj", "mixed", args, local)
+    head = measure(torch, mdb, HEAD["kind"], HEAD["precision"], args, local, HEAD["half"])
     clocks = clk.stop()
     secs = head["secs"]
     if dist:
@@ -327,81 +407,87 @@ def main():
 
     s = head["system"]
     kt = force_kernel_time(torch, s)
-    alg, per_atom = algorithmic_bytes("lj", "mixed", head["natoms"], head["mean_list"])
-    hbm, src = peaks()
-    achieved = alg / kt / 1e9
+    xh, _, _ = s.atoms()
+    box = np.array([s.params.xprd, s.params.yprd, s.params.zprd])
+    pc = pairs_in_cutoff(xh, box, s.params.cutforce)
+    fpa = cp_flops_per_atom(pc, HEAD["half"])
+    peak, src = fp32_peak()
+    achieved = fpa * head["natoms"] / kt / 1e12
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
             tj = json.load(f)
-        if "lj_mixed_bytes_per_atom" in tj:
-            traffic = tj["lj_mixed_bytes_per_atom"] * head["natoms"]
-    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-            "frac": round(achieved / hbm, 4), "traffic": traffic,
-            "kernel": "k_lj_mixed (full list, uniform types)",
-            "kernel_ms": round(kt * 1e3, 4), "bytes_per_atom": round(per_atom, 1),
+        if "cp_head_bytes_per_atom" in tj:
+            traffic = tj["cp_head_bytes_per_atom"] * head["natoms"]
+    entries = float(s.numneigh().mean())
+    roof = {"bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak, 1),
+            "unit": "TFLOP/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+            "kernel": "k_force_mixed<4, %s> (cluster-pair, uniform types)"
+                      % ("half" if HEAD["half"] else "full"),
+            "kernel_ms": round(kt * 1e3, 4), "pairs_in_cutoff_per_atom": round(pc, 2),
+            "flops_per_atom": round(fpa, 1),
+            "computed_pairs_per_atom": round(entries * 4, 1),
             "peak_source": src}
 
     extra = {}
     if not args.no_variants and rank == 0:
-        fp = measure(torch, mdb, "lj", "fp64", args, local)
-        # mixed force error against FP64 on the same (melted) state
-        x, v, f64, t = fp["system"].atoms()
-        fp["system"].set_atoms(x, v, t)
-        fp["system"].setup()
-        _, _, f64, _ = fp["system"].atoms()
-        s.set_atoms(x, v, t)
-        s.setup()
-        rms, mx = rel_force_err(s.atoms()[2], f64)
+        runs = {}
+        for kind in ("cp44", "cp48"):
+            for half in (0, 1):
+                for prec in ("mixed", "fp64"):
+                    key = f"{kind}_{prec}{'_half' if half else ''}"
+                    if (kind, prec, half) == (HEAD["kind"], HEAD["precision"], HEAD["half"]):
+                        runs[key] = head
+                    else:
+                        runs[key] = measure(torch, mdb, kind, prec, args, local, half)
+        for kind in ("lj", "eam"):
+            for prec in ("mixed", "fp64"):
+                runs[f"{'vl' if kind == 'lj' else kind}_{prec}"] = measure(
+                    torch, mdb, kind, prec, args, local)
+        var = {}
+        for key, m in runs.items():
+            var[key] = {"value": m["value"], "ms_per_step": m["ms_per_step"],
+                        "natoms": m["natoms"], "energy_drift": drift(m),
+                        "md_steps": m["nsteps"], "mean_list": m["mean_list"]}
+        for key in list(runs):
+            if "_mixed" in key:
+                ref = key.replace("_mixed", "_fp64")
+                kind = key.split("_")[0]
+                rms, mx = force_compare(runs[key], runs[ref], kind)
+                var[key]["force_rms_rel_err"] = rms
+                var[key]["force_max_rel_err"] = mx
+                var[key]["excess_drift_vs_fp64"] = var[key]["energy_drift"] - var[ref]["energy_drift"]
+        extra = {"variants": var,
+                 "mixed_over_fp64": {k.replace("_mixed", ""): var[k]["value"] /
+                                     var[k.replace("_mixed", "_fp64")]["value"]
+                                     for k in var if "_mixed" in k}}
+        for m in runs.values():
+            if m is not head:
+                m["system"].close()
 
-        def drift(m):
-            e = [m["th0"]["E"]] + [q["E"] for q in m["samples"]]
-            return float((e[-1] - e[0]) / abs(e[0]))
-
-        em = measure(torch, mdb, "eam", "mixed", args, local)
-        ef = measure(torch, mdb, "eam", "fp64", args, local)
-        xe, ve, fe, te = ef["system"].atoms()
-        ef["system"].set_atoms(xe, ve, te)
-        ef["system"].setup()
-        em["system"].set_atoms(xe, ve, te)
-        em["system"].setup()
-        erms, emx = rel_force_err(em["system"].atoms()[2], ef["system"].atoms()[2])
-        extra = {
-            "variants": {
-                "lj_mixed": {"value": head["value"], "ms_per_step": head["ms_per_step"],
-                             "force_rms_rel_err": rms, "force_max_rel_err": mx,
-                             "energy_drift": drift(head), "md_steps": head["nsteps"]},
-                "lj_fp64": {"value": fp["value"], "ms_per_step": fp["ms_per_step"],
-                            "energy_drift": drift(fp), "md_steps": fp["nsteps"]},
-                "eam_mixed": {"value": em["value"], "ms_per_step": em["ms_per_step"],
-                              "natoms": em["natoms"], "force_rms_rel_err": erms,
-                              "force_max_rel_err": emx, "energy_drift": drift(em)},
-                "eam_fp64": {"value": ef["value"], "ms_per_step": ef["ms_per_step"],
-                             "natoms": ef["natoms"], "energy_drift": drift(ef)},
-            },
-            "mixed_over_fp64": {"lj": head["value"] / fp["value"],
-                                "eam": em["value"] / ef["value"]},
-        }
-
-    e2 = e2e(torch, s, head["init"], max(args.steps // 5, 3), 20)
+    # end to end from the state the timed run reached (a liquid, as in use)
+    e2 = e2e(torch, s, s.atoms(), max(args.steps // 5, 3), 20)
     if dist:
         tt = torch.tensor([e2["value"]], device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.SUM)
         e2["value"] = float(tt.item())
-    cb = cpu_baseline() if (rank == 0 and world == 1) else None
+    cb = cpu_baseline(half=HEAD["half"]) if (rank == 0 and world == 1) else None
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32-mixed",
                 "data": "synthetic",
-                "config": {"workload": f"lj-fcc-{LJ_CELLS}^3-verletlist-full-mixed",
+                "config": {"workload": HEAD_WORKLOAD,
                            "natoms_per_gpu": head["natoms"], "md_steps_per_bench_step": 20,
                            "rebuild_every": 20, "thermo_every": 100, "density": 0.8442,
-                           "cutoff": 2.5, "skin": 0.3,
-                           "l2": "inputs larger than L2 (Verlet list %.0f MB)"
-                                 % (head["mean_list"] * 4 * head["natoms"] / 1e6),
+                           "cutoff": 2.5, "skin": 0.3, "cluster": "4x4",
+                           "lists": "half" if HEAD["half"] else "full",
+                           "l2": "inputs larger than L2 (cluster list %.0f MB, "
+                                 "positions and velocities %.0f MB)"
+                                 % (head["mean_list"] * 4 * head["natoms"] / 4 / 1e6,
+                                    head["natoms"] * 96 / 1e6),
                            "parallelism": f"replicas{world}"},
                 "roofline": roof, "cpu_baseline": cb, "e2e": e2, "clocks": clocks,
                 "gpu_launches": head["launches"]}

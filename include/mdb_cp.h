@@ -45,7 +45,9 @@ void* mdb_cp_stream(MdbCp* ctx);
 int mdb_cp_synchronize(MdbCp* ctx);
 /* Launch tuning (no counterpart in the reference; results are unchanged):
  * "force_block" = threads per block of the mixed force kernel (32..512, a
- * multiple of 32; default 128). */
+ * multiple of 32; default 128); "force_variant" = 0..3, bit 0: j data
+ * prefetched two list blocks ahead instead of one, bit 1: a register budget
+ * for 8 resident blocks of 128 threads per SM (default 2). */
 int mdb_cp_tune(MdbCp* ctx, const char* key, int value);
 long long mdb_cp_launch_count(const MdbCp* ctx);
 

@@ -209,7 +209,8 @@ static int setup_types(MdbCp* ctx)
         if (t.sqrt_eps[k] != t.sqrt_eps[0] || t.sigma3[k] != t.sigma3[0]) uniform = false;
     }
     t.uniform     = uniform ? 1 : 0;
-    t.force_block = 128;
+    t.force_block   = 128;
+    t.force_variant = 2; // measured fastest on B200 at 1M atoms (4x4 and 4x8, full and half)
     t.eps0        = t.sqrt_eps[0] * t.sqrt_eps[0];
     t.sigma6_0 = t.sigma3[0] * t.sigma3[0];
     return MDB_OK;
@@ -226,6 +227,12 @@ extern "C" int mdb_cp_tune(MdbCp* ctx, const char* key, int value)
         if (value < 32 || value > 512 || value % 32) return MDB_ERR_ARG;
         drop_graph(ctx);
         ctx->ty.force_block = value;
+        return MDB_OK;
+    }
+    if (!strcmp(key, "force_variant")) {
+        if (value < 0 || value > 3) return MDB_ERR_ARG;
+        drop_graph(ctx);
+        ctx->ty.force_variant = value;
         return MDB_OK;
     }
     return fail(ctx, MDB_ERR_ARG, "unknown tuning key");
@@ -454,13 +461,38 @@ static int alloc_list(MdbCp* ctx, int maxneighs)
         if (!ctx->have_atoms) return fail(ctx, MDB_ERR_STATE, "no atoms set");           \
     } while (0)
 
+// AoS host triples <-> double4 atom arrays, converted on the device so that
+// pinned host buffers move by DMA at full speed
+__global__ void k_cp_pack_atoms(int n, const double* __restrict__ xa,
+    const double* __restrict__ va, const int* __restrict__ ta, int has_t, double4* ax,
+    double4* av, int ntypes, int* bad)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int t = has_t ? ta[i] : 0;
+    if (t < 0 || t >= ntypes) atomicAdd(bad, 1);
+    ax[i] = make_double4(xa[3 * i], xa[3 * i + 1], xa[3 * i + 2], type_bits(t));
+    av[i] = make_double4(va[3 * i], va[3 * i + 1], va[3 * i + 2], 0.0);
+}
+
+__global__ void k_cp_unpack_atoms(int n, const double4* __restrict__ ax,
+    const double4* __restrict__ av, double* xa, double* va, int* ta)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 p = ax[i], q = av[i];
+    xa[3 * i] = p.x, xa[3 * i + 1] = p.y, xa[3 * i + 2] = p.z;
+    va[3 * i] = q.x, va[3 * i + 1] = q.y, va[3 * i + 2] = q.z;
+    ta[i] = slot_type(p);
+}
+
 extern "C" int mdb_cp_set_atoms(MdbCp* ctx, int nlocal, const double* x, const double* v,
     const int* type)
 {
     if (!ctx || nlocal < 1 || !x || !v) return MDB_ERR_ARG;
     CK(cudaSetDevice(ctx->dev));
-    CK(cudaStreamSynchronize(ctx->s));
     if (nlocal != ctx->atom_cap) {
+        CK(cudaStreamSynchronize(ctx->s));
         drop_graph(ctx);
         int rc = alloc_atoms(ctx, nlocal);
         if (rc) return rc;
@@ -476,18 +508,24 @@ extern "C" int mdb_cp_set_atoms(MdbCp* ctx, int nlocal, const double* x, const d
         rc         = alloc_ghosts(ctx, (int)std::min(est, 2.0e9 / ctx->N));
         if (rc) return rc;
     }
-    ctx->nlocal = nlocal;
-    std::vector<double4> hx(nlocal), hv(nlocal);
-    for (int i = 0; i < nlocal; i++) {
-        long long t = type ? type[i] : 0;
-        if (t < 0 || t >= ctx->ty.ntypes) return fail(ctx, MDB_ERR_ARG, "atom type out of range");
-        double w;
-        memcpy(&w, &t, sizeof w);
-        hx[i] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], w);
-        hv[i] = make_double4(v[3 * i], v[3 * i + 1], v[3 * i + 2], 0.0);
-    }
-    CK(cudaMemcpy(ctx->ax, hx.data(), sizeof(double4) * nlocal, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->av, hv.data(), sizeof(double4) * nlocal, cudaMemcpyHostToDevice));
+    ctx->nlocal       = nlocal;
+    cudaStream_t s    = ctx->s;
+    const size_t n3   = 3 * (size_t)nlocal;
+    double* sx        = ctx->stage;
+    double* sv        = ctx->stage + n3;
+    int* bad          = ctx->cnt + CP_BADBIN; // reused as a scratch flag here
+    CK(cudaMemsetAsync(bad, 0, sizeof(int), s));
+    CK(cudaMemcpyAsync(sx, x, sizeof(double) * n3, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(sv, v, sizeof(double) * n3, cudaMemcpyHostToDevice, s));
+    if (type)
+        CK(cudaMemcpyAsync(ctx->stage_i, type, sizeof(int) * nlocal, cudaMemcpyHostToDevice, s));
+    k_cp_pack_atoms<<<mdb_blocks(nlocal, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(nlocal, sx, sv,
+        ctx->stage_i, type ? 1 : 0, ctx->ax, ctx->av, ctx->ty.ntypes, bad);
+    ctx->launches++;
+    int hbad = 0;
+    CK(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (hbad) return fail(ctx, MDB_ERR_ARG, "atom type out of range");
     ctx->have_atoms    = true;
     ctx->have_clusters = ctx->have_ghosts = ctx->have_list = false;
     ctx->energy_valid  = false;
@@ -497,24 +535,16 @@ extern "C" int mdb_cp_set_atoms(MdbCp* ctx, int nlocal, const double* x, const d
 extern "C" int mdb_cp_get_atoms(MdbCp* ctx, double* x, double* v, int* type)
 {
     NEED_ATOMS();
-    int n = ctx->nlocal;
-    std::vector<double4> hx(n), hv(n);
-    CK(cudaMemcpyAsync(hx.data(), ctx->ax, sizeof(double4) * n, cudaMemcpyDeviceToHost, ctx->s));
-    CK(cudaMemcpyAsync(hv.data(), ctx->av, sizeof(double4) * n, cudaMemcpyDeviceToHost, ctx->s));
-    CK(cudaStreamSynchronize(ctx->s));
-    for (int i = 0; i < n; i++) {
-        if (x) {
-            x[3 * i] = hx[i].x, x[3 * i + 1] = hx[i].y, x[3 * i + 2] = hx[i].z;
-        }
-        if (v) {
-            v[3 * i] = hv[i].x, v[3 * i + 1] = hv[i].y, v[3 * i + 2] = hv[i].z;
-        }
-        if (type) {
-            long long t;
-            memcpy(&t, &hx[i].w, sizeof t);
-            type[i] = (int)t;
-        }
-    }
+    const int n       = ctx->nlocal;
+    const size_t n3   = 3 * (size_t)n;
+    cudaStream_t s    = ctx->s;
+    k_cp_unpack_atoms<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(n, ctx->ax, ctx->av,
+        ctx->stage, ctx->stage + n3, ctx->stage_i);
+    ctx->launches++;
+    if (x) CK(cudaMemcpyAsync(x, ctx->stage, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
+    if (v) CK(cudaMemcpyAsync(v, ctx->stage + n3, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
+    if (type) CK(cudaMemcpyAsync(type, ctx->stage_i, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
     return MDB_OK;
 }
 

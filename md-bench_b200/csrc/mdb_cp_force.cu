@@ -322,8 +322,12 @@ __device__ __forceinline__ JEntry load_entry(int cj, int b, const float4* __rest
 // i atoms in the lane and add it with one atomic per component. Padding slots
 // sit at +1e18 (j) and invalid i atoms are moved to -1e18, so they fall outside
 // the cutoff without INF arithmetic.
-template <int N, bool HALF, bool ENERGY, bool UNIFORM>
-__global__ void __launch_bounds__(512) k_force_mixed(const int* __restrict__ cnt,
+// PF: j data prefetched 1 or 2 iterations ahead; MINB: minimum resident blocks
+// of 128 threads per SM asked of the register allocator (0: no request).
+// Both are launch-shape choices of the autotuner; results do not depend on them.
+template <int N, bool HALF, bool ENERGY, bool UNIFORM, int PF, int MINB>
+__global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_force_mixed(
+    const int* __restrict__ cnt,
     const float4* __restrict__ xr, const float4* __restrict__ anchor, Types ty,
     float cutforcesq, const int* __restrict__ list, int ks, int cs,
     const int* __restrict__ numneigh, float4* cf32, double* epart)
@@ -379,9 +383,15 @@ __global__ void __launch_bounds__(512) k_force_mixed(const int* __restrict__ cnt
         const int* row = list + (size_t)ci * cs;
         int lst_cur = lane < nn ? __ldg(&row[(size_t)lane * ks]) : -1;
         int lst_nxt = 32 + lane < nn ? __ldg(&row[(size_t)(32 + lane) * ks]) : -1;
-        JEntry cur  = load_entry<N>(__shfl_sync(0xffffffffu, lst_cur, eidx), b, xr, anchor, ai);
+        JEntry cur = load_entry<N>(__shfl_sync(0xffffffffu, lst_cur, eidx), b, xr, anchor, ai);
+        JEntry nx1;
+        if (PF == 2) {
+            const int c1 = __shfl_sync(0xffffffffu, lst_cur, JPW + eidx);
+            nx1          = load_entry<N>(JPW < nn ? c1 : -1, b, xr, anchor, ai);
+        }
         for (int kb = 0; kb < nn; kb += JPW) {
-            const int kn = kb + JPW;
+            // the entry block holding kn is rotated in when kn reaches it
+            const int kn = kb + PF * JPW;
             if ((kn & 31) == 0) {
                 lst_cur = lst_nxt;
                 lst_nxt = kn + 32 + lane < nn ? __ldg(&row[(size_t)(kn + 32 + lane) * ks]) : -1;
@@ -416,7 +426,12 @@ __global__ void __launch_bounds__(512) k_force_mixed(const int* __restrict__ cnt
                 f2_unpack(gz, lo, hi);
                 atomicAdd(&dst->z, -(lo + hi));
             }
-            cur = nx;
+            if (PF == 2) {
+                cur = nx1;
+                nx1 = nx;
+            } else {
+                cur = nx;
+            }
         }
         float f[12];
 #pragma unroll
@@ -451,13 +466,20 @@ static void run_mixed(cudaStream_t s, int blocks, const int* cnt, const float4* 
     const float4* anchor, const Types& ty, float cutforcesq, const int* list, int ks, int cs,
     const int* numneigh, float4* cf32, double* epart)
 {
-    // blocks of ty.force_block threads: consecutive i-clusters (z neighbours in
-    // one column) share most of their j-clusters, so larger blocks keep more of
-    // that reuse in one SM's L1
-    const int nt = ty.force_block;
+    // blocks of ty.force_block threads (128 when a register budget is asked)
+    const int v  = ty.force_variant;
+    const int nt = (v & 2) ? 128 : ty.force_block;
     const int nb = (int)(((long long)blocks * CP_FORCE_THREADS + nt - 1) / nt);
-    k_force_mixed<N, HALF, ENERGY, UNIFORM><<<nb, nt, 0, s>>>(cnt, xr, anchor, ty, cutforcesq,
-        list, ks, cs, numneigh, cf32, epart);
+#define CP_RUN(PF, MB)                                                                   \
+    k_force_mixed<N, HALF, ENERGY, UNIFORM, PF, MB><<<nb, nt, 0, s>>>(cnt, xr, anchor, ty,   \
+        cutforcesq, list, ks, cs, numneigh, cf32, epart)
+    switch (v) {
+    case 1: CP_RUN(2, 0); break;
+    case 2: CP_RUN(1, 8); break;
+    case 3: CP_RUN(2, 8); break;
+    default: CP_RUN(1, 0); break;
+    }
+#undef CP_RUN
 }
 
 template <int N, bool HALF>

@@ -70,6 +70,7 @@ struct Types {
     float sqrt_eps_f[MDB_MAX_TYPES], sigma3_f[MDB_MAX_TYPES];
     double eps0, sigma6_0; // uniform case
     int force_block;       // threads per block of the mixed force kernel (tunable)
+    int force_variant;     // mixed force kernel: bit 0 prefetch 2 ahead, bit 1 register budget
 };
 
 __device__ __forceinline__ int slot_type(const double4& p) { return (int)__double_as_longlong(p.w); }
