@@ -175,6 +175,15 @@ __device__ __forceinline__ void warp_reduce_12(float (&v)[12], int lane)
     v[2] = q[2];
 }
 
+// one vector reduction (red.global.add.v4.f32, sm_90+) instead of three
+// scalar atomics for a force update
+__device__ __forceinline__ void red_add4(float4* dst, float x, float y, float z)
+{
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(dst), "f"(x), "f"(y),
+                 "f"(z), "f"(0.0f)
+                 : "memory");
+}
+
 // PTX rcp.approx.ftz.f32: at most 1 ulp from 1/x, one MUFU operation
 __device__ __forceinline__ float rcp_approx(float x)
 {
@@ -231,9 +240,9 @@ struct IPack {
 // for uniform types. The i forces accumulate in fx/fy/fz (packed like the i
 // atoms); half lists also accumulate sum(d * force) for the j atom in g (its
 // reaction is minus the sum of both halves).
-template <bool HALF, bool ENERGY, bool UNIFORM, bool DIAG>
+template <bool HALF, bool ENERGY, bool UNIFORM>
 __device__ __forceinline__ void mixed_entry(const IPack& ip, const float4& xj, float sej,
-    float s3j, int ai0, int b, float cutforcesq, f2 A2, f2 mB2, float sig6u, double eps0,
+    float s3j, unsigned excl, float cutforcesq, f2 A2, f2 mB2, float sig6u, double eps0,
     double ew, f2 (&fx)[2], f2 (&fy)[2], f2 (&fz)[2], f2& gx, f2& gy, f2& gz, double& e)
 {
     const f2 XJ = f2_pack(xj.x, xj.x), YJ = f2_pack(xj.y, xj.y), ZJ = f2_pack(xj.z, xj.z);
@@ -245,12 +254,9 @@ __device__ __forceinline__ void mixed_entry(const IPack& ip, const float4& xj, f
         const f2 RSQ = f2_fma(DX, DX, f2_fma(DY, DY, f2_mul(DZ, DZ)));
         float r0, r1;
         f2_unpack(RSQ, r0, r1);
-        bool in0 = r0 < cutforcesq, in1 = r1 < cutforcesq;
-        if (DIAG) {
-            const int a0 = ai0 + 2 * h, a1 = a0 + 1;
-            in0 = in0 && (HALF ? (a0 < b) : (a0 != b));
-            in1 = in1 && (HALF ? (a1 < b) : (a1 != b));
-        }
+        // excl: bit a set when pair (i atom a, this j atom) is excluded
+        const bool in0 = r0 < cutforcesq && !((excl >> (2 * h)) & 1u);
+        const bool in1 = r1 < cutforcesq && !((excl >> (2 * h + 1)) & 1u);
         float u0 = rcp_approx(r0), u1 = rcp_approx(r1);
         u0          = in0 ? u0 : 0.0f;
         u1          = in1 ? u1 : 0.0f;
@@ -379,6 +385,13 @@ __global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_force_mix
         const f2 A2 = f2_pack(cA, cA), mB2 = f2_pack(-cB, -cB);
         f2 fx[2] = {0, 0}, fy[2] = {0, 0}, fz[2] = {0, 0};
         const int eidx = lane / N, b = lane - eidx * N;
+        // pairs of the diagonal entry (cj == ci_cj0) excluded as the
+        // reference's cond (clusterpair/force_lj.c:108-123): the self pair, and
+        // for half lists every pair with the i atom at or after the j atom
+        unsigned diag_excl = 0;
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+            if (HALF ? (ai0 + a >= b) : (ai0 + a == b)) diag_excl |= 1u << a;
         const int nn   = numneigh[ci];
         const int* row = list + (size_t)ci * cs;
         int lst_cur = lane < nn ? __ldg(&row[(size_t)lane * ks]) : -1;
@@ -410,21 +423,15 @@ __global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_force_mix
             // energy weight: full lists see every pair twice; half lists once,
             // except pairs with ghost atoms, which both owners list
             const double ew = (!HALF || cj * N + b >= nloc) ? 0.5 : 1.0;
-            if (cj == ci_cj0)
-                mixed_entry<HALF, ENERGY, UNIFORM, true>(ip, cur.x, sej, s3j, ai0, b, cutforcesq,
-                    A2, mB2, sig6u, ty.eps0, ew, fx, fy, fz, gx, gy, gz, e);
-            else
-                mixed_entry<HALF, ENERGY, UNIFORM, false>(ip, cur.x, sej, s3j, ai0, b,
-                    cutforcesq, A2, mB2, sig6u, ty.eps0, ew, fx, fy, fz, gx, gy, gz, e);
+            mixed_entry<HALF, ENERGY, UNIFORM>(ip, cur.x, sej, s3j,
+                cj == ci_cj0 ? diag_excl : 0u, cutforcesq, A2, mB2, sig6u, ty.eps0, ew, fx, fy,
+                fz, gx, gy, gz, e);
             if (HALF && cj >= 0 && cj * N + b < nloc && __float_as_int(cur.x.w) >= 0) {
-                float4* dst = &cf32[cj * N + b];
-                float lo, hi;
-                f2_unpack(gx, lo, hi);
-                atomicAdd(&dst->x, -(lo + hi));
-                f2_unpack(gy, lo, hi);
-                atomicAdd(&dst->y, -(lo + hi));
-                f2_unpack(gz, lo, hi);
-                atomicAdd(&dst->z, -(lo + hi));
+                float gx0, gx1, gy0, gy1, gz0, gz1;
+                f2_unpack(gx, gx0, gx1);
+                f2_unpack(gy, gy0, gy1);
+                f2_unpack(gz, gz0, gz1);
+                red_add4(&cf32[cj * N + b], -(gx0 + gx1), -(gy0 + gy1), -(gz0 + gz1));
             }
             if (PF == 2) {
                 cur = nx1;
@@ -445,13 +452,8 @@ __global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_force_mix
             const int a = lane >> 3;
             if (__float_as_int(xr[ci * 4 + a].w) >= 0) {
                 float4* dst = &cf32[ci * 4 + a];
-                if (HALF) {
-                    atomicAdd(&dst->x, f[0]);
-                    atomicAdd(&dst->y, f[1]);
-                    atomicAdd(&dst->z, f[2]);
-                } else {
-                    *dst = make_float4(f[0], f[1], f[2], 0.f);
-                }
+                if (HALF) red_add4(dst, f[0], f[1], f[2]);
+                else *dst = make_float4(f[0], f[1], f[2], 0.f);
             }
         }
     }
