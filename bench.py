@@ -32,6 +32,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "md-bench_b200"))
 
 LJ_CELLS = 64
+C5_CELLS = 128
+C4_REPLICAS = 256
 EAM_CELLS = 32
 EAM_A = 3.615
 EAM_T = 1600.0
@@ -52,10 +54,13 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-variants", action="store_true", help="headline only")
     ap.add_argument("--profile", choices=[f"{k}_{p}{h}" for k in ("lj", "eam", "cp44", "cp48")
-                                          for p in ("mixed", "fp64") for h in ("", "_half")],
+                                          for p in ("mixed", "fp64") for h in ("", "_half")]
+                    + ["c5_mixed", "c5_fp64", "c4_mixed"],
                     help="run one variant only (W+K bench steps + force timing), for ncu")
     ap.add_argument("--cells", type=int, default=None, help="fcc cells per side (profiling)")
     ap.add_argument("--tune", default=None, help="key=value[,key=value] cluster-pair tuning")
+    ap.add_argument("--replicas", type=int, default=C4_REPLICAS, help="ensemble size")
+    ap.add_argument("--no-autotune", action="store_true", help="ensemble with default choices")
     return ap.parse_args()
 
 
@@ -109,17 +114,26 @@ def lj_workload(mdb, precision, device, cells=None, half=0):
     return s, (x, v, t)
 
 
-def cp_workload(mdb, precision, device, cells=None, half=0, cluster_n=4):
-    """The cluster-pair scheme (GROMACS-style 4xN clusters) on the LJ workload."""
+def cp_workload(mdb, precision, device, cells=None, half=0, cluster_n=4, types=None):
+    """The cluster-pair scheme (GROMACS-style 4xN clusters) on the LJ workload;
+    ``types`` = (epsilon_per_type, sigma_per_type) gives the multi-type liquid
+    (types drawn by createAtom, cutoff 2.5 sigma_max)."""
     c = cells or LJ_CELLS
-    hp = mdb.host_params(nx=c, ny=c, nz=c, half_neigh=half)
+    kw = {}
+    if types is not None:
+        import workloads as W
+        kw = dict(types=types, cutforce=W.c5_cutoff(types[1]))
+    hp = mdb.host_params(nx=c, ny=c, nz=c, half_neigh=half, **kw)
     x, v, t = mdb.create_fcc(hp)
+    eps = sig = None
+    if types is not None:
+        eps, sig = list(types[0]), list(types[1])
     s = mdb.ClusterSystem(natoms=len(t), cluster_n=cluster_n, half_neigh=half,
                           precision=precision, device=device, xprd=hp.xprd, yprd=hp.yprd,
                           zprd=hp.zprd, cutforce=hp.cutforce, cutneigh=hp.cutneigh, dt=hp.dt,
                           dtforce=hp.dtforce, mass=hp.mass, epsilon=hp.epsilon,
                           sigma=hp.sigma, ntypes=hp.ntypes, reneigh_every=hp.reneigh_every,
-                          nstat=hp.nstat)
+                          nstat=hp.nstat, epsilon_per_type=eps, sigma_per_type=sig)
     return s, (x, v, t)
 
 
@@ -189,27 +203,136 @@ def rel_force_err(a, b):
     return float(np.sqrt(np.mean(d * d)) / rms), float(d.max() / rms)
 
 
-def measure(torch, mdb, kind, precision, args, device, half=0):
-    if kind.startswith("cp"):
+def measure(torch, mdb, kind, precision, args, device, half=0, steps=None):
+    steps = steps or args.steps
+    if kind == "c5":
+        import workloads as W
+        s, (x, v, t) = cp_workload(mdb, precision, device, args.cells or C5_CELLS, 1,
+                                   cluster_n=4, types=W.c5_types())
+    elif kind.startswith("cp"):
         s, (x, v, t) = cp_workload(mdb, precision, device, args.cells, half,
                                    cluster_n=int(kind[3]))
-        for kv in (args.tune.split(",") if getattr(args, "tune", None) else []):
-            k, val = kv.split("=")
-            s.tune(k, int(val))
     else:
         make = lj_workload if kind == "lj" else eam_workload
         s, (x, v, t) = make(mdb, precision, device, args.cells, half)
+    if kind.startswith("c"):
+        for kv in (args.tune.split(",") if getattr(args, "tune", None) else []):
+            k, val = kv.split("=")
+            s.tune(k, int(val))
     s.set_atoms(x, v, t)
     s.setup()
     th0 = s.thermo()
     nat = len(t)
     every = s.params.reneigh_every
-    secs, launches, samples, nsteps = time_run(torch, s, args.steps, args.warmup, every)
+    secs, launches, samples, nsteps = time_run(torch, s, steps, args.warmup, every)
     mean_list = float(s.numneigh().mean())
     return dict(system=s, natoms=nat, secs=secs, launches=launches, samples=samples,
                 nsteps=nsteps, th0=th0, mean_list=mean_list,
-                value=nat * every * args.steps / secs, ms_per_step=1e3 * secs / args.steps,
+                value=nat * every * steps / secs, ms_per_step=1e3 * secs / steps,
                 init=(x, v, t))
+
+
+def c4_specs(count):
+    import workloads as W
+    return [{"cells": n, "rho": rho, "temp": T, "natoms": 4 * n ** 3}
+            for n, rho, T in W.c4_replicas(count)]
+
+
+class Replicas:
+    """Initial states of ensemble replicas (createAtom at each replica's cells,
+    density and temperature) and set-up mixed-precision systems built from them."""
+
+    def __init__(self, mdb, device):
+        self.mdb, self.device, self.cache = mdb, device, {}
+
+    def state(self, sp):
+        key = (sp["cells"], sp["rho"], sp["temp"])
+        if key not in self.cache:
+            c = sp["cells"]
+            hp = self.mdb.host_params(nx=c, ny=c, nz=c, rho=sp["rho"], temp=sp["temp"])
+            x, v, t = self.mdb.create_fcc(hp)
+            self.cache[key] = (hp, x, v, t)
+        return self.cache[key]
+
+    def build(self, sp, cluster_n, half, choice=None):
+        import autotune as AT
+        hp, x, v, t = self.state(sp)
+        s = self.mdb.ClusterSystem(natoms=len(t), cluster_n=cluster_n, half_neigh=half,
+                                   precision="mixed", device=self.device, xprd=hp.xprd,
+                                   yprd=hp.yprd, zprd=hp.zprd, cutforce=hp.cutforce,
+                                   cutneigh=hp.cutneigh, dt=hp.dt, dtforce=hp.dtforce,
+                                   mass=hp.mass, reneigh_every=hp.reneigh_every,
+                                   nstat=hp.nstat, ntypes=hp.ntypes)
+        if choice is not None:
+            AT.apply_launch(s, choice)
+        s.set_atoms(x, v, t)
+        s.setup()
+        return s
+
+
+def c4_ensemble(torch, mdb, args, device):
+    """256 LJ replicas of uneven size, density and temperature advanced as one
+    ensemble (one graph launch per timestep), autotuned per size class."""
+    import autotune as AT
+    specs = c4_specs(args.replicas)
+    pool = Replicas(mdb, device)
+    t0 = time.perf_counter()
+    if args.no_autotune:
+        choice, trials = {}, []
+    else:
+        choice, trials = AT.tune_ensemble(specs, lambda sp, n, h: pool.build(sp, n, h))
+    tune_secs = time.perf_counter() - t0
+    members = []
+    for sp in specs:
+        c = choice.get(AT.size_class(sp["natoms"]), AT.DEFAULT)
+        members.append(pool.build(sp, c["cluster_n"], c["half"], c))
+    ens = mdb.Ensemble(members)
+    th0 = [m.thermo() for m in members]
+    every = 20
+    stream = torch.cuda.ExternalStream(ens.stream)
+    n = 0
+    for _ in range(args.warmup):
+        ens.run(every, first_step=n, max_samples=0)
+        n += every
+    torch.cuda.synchronize()
+    samples = [[] for _ in members]
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    l0 = ens.launches
+    e0.record(stream)
+    for _ in range(args.steps):
+        out = ens.run(every, first_step=n, max_samples=1)
+        for k, q in enumerate(out):
+            samples[k] += q
+        n += every
+    e1.record(stream)
+    e1.synchronize()
+    secs = e0.elapsed_time(e1) / 1e3
+    launches = ens.launches - l0
+    nat = sum(sp["natoms"] for sp in specs)
+    drifts = [abs((q[-1]["E"] - t["E"]) / t["E"]) for q, t in zip(samples, th0) if q]
+    # the same replicas advanced one after another (each its own graph loop)
+    t1 = time.perf_counter()
+    for m in members:
+        m.run(every, first_step=n, max_samples=0)
+    serial = time.perf_counter() - t1
+    ens.close()
+    for m in members:
+        m.close()
+    shapes = {}
+    for sp in specs:
+        c = choice.get(AT.size_class(sp["natoms"]), AT.DEFAULT)
+        key = f"{4}x{c['cluster_n']}-{'half' if c['half'] else 'full'}"
+        shapes[key] = shapes.get(key, 0) + 1
+    return {"value": nat * every * args.steps / secs, "ms_per_step": 1e3 * secs / args.steps,
+            "natoms": nat, "replicas": len(specs), "md_steps": every * args.steps,
+            "gpu_launches": launches, "graph_launches_per_md_step": 1,
+            "energy_drift_max_abs": max(drifts) if drifts else None,
+            "energy_drift_median_abs": float(np.median(drifts)) if drifts else None,
+            "serial_value": nat * every / serial,
+            "autotune": {"seconds": round(tune_secs, 2), "trials": len(trials),
+                         "choice_per_size_class": {str(k): v for k, v in choice.items()},
+                         "replicas_per_shape": shapes}}
 
 
 def e2e(torch, s, init, steps, every):
@@ -339,7 +462,7 @@ def force_compare(mix, f64, kind):
     """Mixed force against FP64 on the FP64 run's final state (both systems get
     the same atoms and rebuild)."""
     sm, sf = mix["system"], f64["system"]
-    if kind.startswith("cp"):
+    if kind.startswith("c"):
         x, v, t = sf.atoms()
         for s in (sf, sm):
             s.set_atoms(x, v, t)
@@ -382,6 +505,10 @@ def main():
         if dist:
             dist.barrier()
 
+    if args.profile == "c4_mixed":
+        print(json.dumps(dict(profile=args.profile, **c4_ensemble(torch, mdb, args, local))),
+              flush=True)
+        return
     if args.profile:
         kind, prec = args.profile.split("_")[:2]
         half = 1 if args.profile.endswith("_half") else 0
@@ -445,6 +572,10 @@ def main():
             for prec in ("mixed", "fp64"):
                 runs[f"{'vl' if kind == 'lj' else kind}_{prec}"] = measure(
                     torch, mdb, kind, prec, args, local)
+        # multi-type liquid at 128^3 cells, 500 MD steps
+        for prec in ("mixed", "fp64"):
+            runs[f"c5_{prec}"] = measure(torch, mdb, "c5", prec, args, local, 1,
+                                         steps=max(args.steps // 2, 1))
         var = {}
         for key, m in runs.items():
             var[key] = {"value": m["value"], "ms_per_step": m["ms_per_step"],
@@ -458,13 +589,14 @@ def main():
                 var[key]["force_rms_rel_err"] = rms
                 var[key]["force_max_rel_err"] = mx
                 var[key]["excess_drift_vs_fp64"] = var[key]["energy_drift"] - var[ref]["energy_drift"]
+        for m in runs.values():
+            if m is not head:
+                m["system"].close()
         extra = {"variants": var,
                  "mixed_over_fp64": {k.replace("_mixed", ""): var[k]["value"] /
                                      var[k.replace("_mixed", "_fp64")]["value"]
                                      for k in var if "_mixed" in k}}
-        for m in runs.values():
-            if m is not head:
-                m["system"].close()
+        var["c4_ensemble_mixed"] = c4_ensemble(torch, mdb, args, local)
 
     # end to end from the state the timed run reached (a liquid, as in use)
     e2 = e2e(torch, s, s.atoms(), max(args.steps // 5, 3), 20)

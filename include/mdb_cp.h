@@ -49,6 +49,11 @@ int mdb_cp_synchronize(MdbCp* ctx);
  * prefetched two list blocks ahead instead of one, bit 1: a register budget
  * for 8 resident blocks of 128 threads per SM (default 2). */
 int mdb_cp_tune(MdbCp* ctx, const char* key, int value);
+/* Device time of one force evaluation (no energy) on the context's stream:
+ * the mean over reps back-to-back launches after two untimed ones, from CUDA
+ * events. For launch tuning; the force array is overwritten with the same
+ * values. */
+int mdb_cp_time_force(MdbCp* ctx, int reps, double* seconds);
 long long mdb_cp_launch_count(const MdbCp* ctx);
 
 /* Atom arrays (createAtom / readAtom output, or any state). */
@@ -100,6 +105,25 @@ int mdb_cp_setup(MdbCp* ctx);
  * n with (n+1) % nstat == 0, up to max_samples (at most 64 per call). */
 int mdb_cp_run(MdbCp* ctx, int first_step, int nsteps, MdbThermo* samples, int max_samples,
     int* nsamples);
+
+/* ---- ensembles ----------------------------------------------------------------
+ * No counterpart in the reference (which runs one system per process). Many
+ * independent systems, each an MdbCp already set up with mdb_cp_setup, of any
+ * sizes and temperatures but the same reneigh_every, nstat and prune_every,
+ * advance together: every timestep of all members is one CUDA graph launch
+ * whose branches are the members' own kernel sequences, so small replicas run
+ * concurrently and fill the GPU. Rebuild steps synchronise once for all
+ * members. Thermo samples after every step n with (n+1) % nstat == 0, up to
+ * max_samples per member: samples[member * max_samples + k]. The members stay
+ * usable on their own between runs; do not use them while a run is active. */
+typedef struct MdbCpEnsemble MdbCpEnsemble;
+int mdb_cp_ensemble_create(MdbCp* const* members, int n, MdbCpEnsemble** out);
+int mdb_cp_ensemble_destroy(MdbCpEnsemble* ens);
+const char* mdb_cp_ensemble_last_error(const MdbCpEnsemble* ens);
+void* mdb_cp_ensemble_stream(MdbCpEnsemble* ens);
+long long mdb_cp_ensemble_launch_count(const MdbCpEnsemble* ens);
+int mdb_cp_ensemble_run(MdbCpEnsemble* ens, int first_step, int nsteps, MdbThermo* samples,
+    int max_samples, int* nsamples);
 
 /* ---- introspection (tests, tools) ----------------------------------------- */
 /* counts: Nlocal Natoms Nclusters_local ncj Nclusters_ghost Nghost dummy_cj

@@ -1,0 +1,123 @@
+"""Autotuner for the cluster-pair scheme's free choices.
+
+The reference fixes its cluster shape at compile time (CLUSTER_N = the SIMD
+width: 4x4 for AVX2, 4x8 for AVX-512; clusterpair/atom.h) and its list form on
+the command line (-half); the column grid then follows from the cluster shape
+(setupNeighbor, clusterpair/neighbor.c:108-215: columns of max(M, N) / rho
+atoms). Every choice below is therefore one of the reference's own valid
+configurations, and lists stay bit-exact against the reference build of the
+chosen shape. The tuner picks, per system size:
+
+* cluster shape N = 4 or 8 (which also fixes the column size),
+* list form: full or half (half-list reactions use atomics),
+* the mixed force kernel's launch: threads per block (``force_block``) and
+  ``force_variant`` (prefetch depth, register budget),
+
+by measurement on the device. A single large system is tuned on the force
+kernel's own time (``ClusterSystem.time_force``, CUDA events). Members of an
+ensemble run concurrently, so a size class is tuned on the throughput of an
+ensemble of its own members (atom-steps per second over whole rebuild periods),
+which includes the graph and rebuild costs a replica of that size pays.
+"""
+import math
+import time
+
+import mdb
+
+SHAPES = (4, 8)
+FORMS = (0, 1)
+BLOCKS = (64, 128, 256)
+VARIANTS = (0, 1, 2, 3)
+DEFAULT = {"cluster_n": 4, "half": 1, "force_block": 128, "force_variant": 2}
+
+
+def size_class(natoms):
+    """Octave of the atom count: replicas within a factor of two share a choice."""
+    return int(math.log2(max(int(natoms), 1)))
+
+
+def apply_launch(system, choice):
+    """Launch settings of a choice on a (mixed-precision) system."""
+    system.tune("force_block", choice["force_block"])
+    system.tune("force_variant", choice["force_variant"])
+
+
+def tune_system(build, precision="mixed", reps=20, shapes=SHAPES, forms=FORMS):
+    """Best choice for one system. ``build(cluster_n, half)`` returns a set-up
+    ClusterSystem; the choice minimises the force launch time (per step)."""
+    best, trials = None, []
+    for n in shapes:
+        for half in forms:
+            s = build(n, half)
+            t = s.time_force(reps)
+            trials.append(({"cluster_n": n, "half": half}, t))
+            if precision == "mixed":
+                for blk in BLOCKS:
+                    for var in VARIANTS:
+                        c = {"cluster_n": n, "half": half, "force_block": blk,
+                             "force_variant": var}
+                        apply_launch(s, c)
+                        t = s.time_force(reps)
+                        trials.append((c, t))
+                        if best is None or t < best[1]:
+                            best = (c, t)
+            elif best is None or t < best[1]:
+                best = ({"cluster_n": n, "half": half}, t)
+            s.close()
+    choice = dict(DEFAULT)
+    choice.update(best[0])
+    return choice, trials
+
+
+def _ensemble_rate(members, steps, rounds):
+    ens = mdb.Ensemble(members)
+    ens.run(steps, max_samples=0)  # graph capture, warm-up
+    nat = sum(m.nlocal for m in members)
+    t0 = time.perf_counter()
+    for r in range(rounds):
+        ens.run(steps, first_step=steps * (r + 1), max_samples=0)
+    secs = time.perf_counter() - t0
+    ens.close()
+    return nat * steps * rounds / secs
+
+
+def tune_ensemble(specs, build, steps=20, rounds=2, shapes=SHAPES, forms=FORMS):
+    """Choice per size class for an ensemble. ``specs`` is a list of replica
+    descriptions with an ``natoms`` entry; ``build(spec, cluster_n, half)``
+    returns a set-up mixed-precision ClusterSystem. Shape and list form are
+    picked first (default launch), then threads per block and the force kernel
+    variant, each on the throughput of an ensemble of the class's own members.
+    Returns ({size_class: choice}, trials)."""
+    classes = {}
+    for sp in specs:
+        classes.setdefault(size_class(sp["natoms"]), []).append(sp)
+    out, trials = {}, []
+    for cls, group in sorted(classes.items()):
+        best = None
+        for n in shapes:
+            for half in forms:
+                members = [build(sp, n, half) for sp in group]
+                c = dict(DEFAULT, cluster_n=n, half=half)
+                rate = _ensemble_rate(members, steps, rounds)
+                trials.append((cls, dict(c), rate))
+                if best is None or rate > best[1]:
+                    best = (c, rate)
+                for m in members:
+                    m.close()
+        c0 = best[0]
+        members = [build(sp, c0["cluster_n"], c0["half"]) for sp in group]
+        for key, values in (("force_block", BLOCKS), ("force_variant", VARIANTS)):
+            for val in values:
+                if val == best[0][key]:
+                    continue
+                c = dict(best[0], **{key: val})
+                for m in members:
+                    apply_launch(m, c)
+                rate = _ensemble_rate(members, steps, rounds)
+                trials.append((cls, dict(c), rate))
+                if rate > best[1]:
+                    best = (c, rate)
+        for m in members:
+            m.close()
+        out[cls] = best[0]
+    return out, trials

@@ -78,6 +78,7 @@ struct MdbCp {
     bool energy_valid = false;
     int energy_blocks = 0; // partial-energy blocks of the last energy evaluation
     CpGraph g_plain;
+    unsigned gen = 0; // bumped whenever buffers move (graphs that hold them are stale)
 };
 
 #define RED_SLOTS 64
@@ -114,6 +115,7 @@ template <typename T> static void dfree(T*& p)
 
 static void drop_graph(MdbCp* ctx)
 {
+    ctx->gen++;
     if (ctx->g_plain.exec) cudaGraphExecDestroy(ctx->g_plain.exec);
     ctx->g_plain.exec    = nullptr;
     ctx->g_plain.kernels = 0;
@@ -640,12 +642,9 @@ static void enq_gather(MdbCp* ctx, int wrap)
 // <0: error (negated status). what: the stages that ran.
 enum { CHK_CLUSTERS = 1, CHK_GHOSTS = 2, CHK_LIST = 4, CHK_ALL = 7 };
 
-static int check_build(MdbCp* ctx, int what)
+// evaluates counters already copied to ctx->h_cnt
+static int eval_build(MdbCp* ctx, int what)
 {
-    cudaError_t e = cudaMemcpyAsync(ctx->h_cnt, ctx->cnt, CP_SLOTS * sizeof(int),
-        cudaMemcpyDeviceToHost, ctx->s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->s);
-    if (e != cudaSuccess) return -fail(ctx, MDB_ERR_CUDA, "rebuild check", e);
     const int* h = ctx->h_cnt;
     if (h[CP_BADBIN] > 0) return -fail(ctx, MDB_ERR_OVERFLOW, "atom outside the column grid");
     if ((what & CHK_LIST) && h[CP_WINDOW] > 0)
@@ -662,6 +661,15 @@ static int check_build(MdbCp* ctx, int what)
         return 1;
     }
     return 0;
+}
+
+static int check_build(MdbCp* ctx, int what)
+{
+    cudaError_t e = cudaMemcpyAsync(ctx->h_cnt, ctx->cnt, CP_SLOTS * sizeof(int),
+        cudaMemcpyDeviceToHost, ctx->s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->s);
+    if (e != cudaSuccess) return -fail(ctx, MDB_ERR_CUDA, "rebuild check", e);
+    return eval_build(ctx, what);
 }
 
 static int do_build(MdbCp* ctx)
@@ -920,6 +928,35 @@ extern "C" int mdb_cp_final_integrate(MdbCp* ctx)
     long long m = mark();
     enq_final(ctx);
     account(ctx, m);
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_time_force(MdbCp* ctx, int reps, double* seconds)
+{
+    NEED_ATOMS();
+    if (!ctx->have_list) return fail(ctx, MDB_ERR_STATE, "mdb_cp_setup not run");
+    if (reps < 1 || !seconds) return MDB_ERR_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    cudaError_t e = cudaEventCreate(&e1);
+    if (e != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail(ctx, MDB_ERR_CUDA, "event", e);
+    }
+    long long m = mark();
+    for (int k = 0; k < 2; k++) enq_force(ctx, false);
+    cudaEventRecord(e0, ctx->s);
+    for (int k = 0; k < reps; k++) enq_force(ctx, false);
+    cudaEventRecord(e1, ctx->s);
+    account(ctx, m);
+    e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return fail(ctx, MDB_ERR_CUDA, "force timing", e);
+    *seconds = ms * 1e-3 / reps;
     return MDB_OK;
 }
 
@@ -1232,5 +1269,281 @@ extern "C" int mdb_cp_get_geometry(MdbCp* ctx, int* ints, double* dbls, int* ste
     if (stencil)
         for (int k = 0; k < g.nstencil && k < max_stencil; k++)
             stencil[k] = ctx->stencil[k];
+    return MDB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Ensemble of independent cluster-pair systems (replicas of uneven size and
+// temperature). Every timestep of all members is one CUDA graph launch: the
+// graph forks one branch per member (each branch is that member's own kernel
+// sequence on its own buffers) and joins them, so the replicas' kernels run
+// concurrently and fill the GPU even when single replicas are small. Rebuild
+// steps launch the members' rebuilds as one graph, read all their overflow
+// counters with one synchronisation, and redo only members that grew.
+struct MdbCpEnsemble {
+    std::vector<MdbCp*> m;
+    std::vector<cudaEvent_t> join;
+    cudaEvent_t fork = nullptr;
+    cudaStream_t s   = nullptr;
+    int dev          = 0;
+    std::string err;
+    long long launches = 0;
+    // graphs of the step parts (see the EG_ kinds), valid for the members'
+    // buffer generations in gen
+    CpGraph g[16];
+    std::vector<unsigned> gen;
+    double* h_red = nullptr; // 4 doubles per member
+};
+
+// step parts captured per ensemble: FI = final integration of the previous
+// step fused with the initial one of this step, I = initial only
+enum {
+    EG_PLAIN_FI, // FI, ghost update, force
+    EG_PLAIN_I,  // I, ghost update, force
+    EG_FRONT_FI, // FI, ghost update (a sample step follows with EG_SAMPLE)
+    EG_FRONT_I,  // I, ghost update
+    EG_REB_FI,   // FI, updateSingleAtoms + wrap, rebuild, counters to the host
+    EG_REB_I,    // I, the same
+    EG_FORCE,    // force
+    EG_SAMPLE,   // force with energy, final integration, thermo to the host
+    EG_FINAL,    // the final integration left pending by the last step
+    EG_COUNT
+};
+static_assert(EG_COUNT <= 16, "graph slots of MdbCpEnsemble");
+
+static void ens_drop(MdbCpEnsemble* e)
+{
+    for (size_t k = 0; k < e->m.size(); k++) e->gen[k] = e->m[k]->gen;
+    for (auto& g : e->g) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g.exec    = nullptr;
+        g.kernels = 0;
+    }
+}
+
+static int ens_fail(MdbCpEnsemble* e, int code, const char* what, cudaError_t ce = cudaSuccess)
+{
+    char buf[512];
+    if (ce != cudaSuccess) snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(ce));
+    else snprintf(buf, sizeof buf, "%s", what);
+    e->err = buf;
+    return code;
+}
+
+static void ens_body(MdbCp* c, int kind)
+{
+    switch (kind) {
+    case EG_PLAIN_FI: enq_plain_step(c); break;
+    case EG_PLAIN_I:
+        enq_initial(c);
+        enq_ghost_update(c);
+        enq_force(c, false);
+        break;
+    case EG_FRONT_FI:
+        enq_final_initial(c);
+        enq_ghost_update(c);
+        break;
+    case EG_FRONT_I:
+        enq_initial(c);
+        enq_ghost_update(c);
+        break;
+    case EG_REB_FI:
+    case EG_REB_I:
+        if (kind == EG_REB_FI) enq_final_initial(c);
+        else enq_initial(c);
+        enq_gather(c, 1);
+        enq_build(c);
+        cudaMemcpyAsync(c->h_cnt, c->cnt, CP_SLOTS * sizeof(int), cudaMemcpyDeviceToHost, c->s);
+        break;
+    case EG_FORCE: enq_force(c, false); break;
+    case EG_SAMPLE:
+        enq_force(c, true);
+        enq_final(c);
+        enq_thermo(c, 0, true);
+        cudaMemcpyAsync(c->h_red, c->red, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->s);
+        break;
+    case EG_FINAL: enq_final(c); break;
+    }
+}
+
+static int ens_capture(MdbCpEnsemble* e, int kind)
+{
+    CpGraph& g = e->g[kind];
+    if (g.exec) return MDB_OK;
+    cudaGraph_t graph;
+    long long m0 = mark();
+    cudaError_t ce = cudaStreamBeginCapture(e->s, cudaStreamCaptureModeThreadLocal);
+    if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "ensemble capture", ce);
+    cudaEventRecord(e->fork, e->s);
+    for (size_t k = 0; k < e->m.size(); k++) {
+        MdbCp* c = e->m[k];
+        cudaStreamWaitEvent(c->s, e->fork, 0);
+        ens_body(c, kind);
+        cudaEventRecord(e->join[k], c->s);
+        cudaStreamWaitEvent(e->s, e->join[k], 0);
+    }
+    ce        = cudaStreamEndCapture(e->s, &graph);
+    g.kernels = mdb::g_launches - m0;
+    mdb::g_launches = m0;
+    if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "ensemble capture", ce);
+    ce = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "ensemble graph instantiate", ce);
+    return MDB_OK;
+}
+
+static int ens_launch(MdbCpEnsemble* e, int kind)
+{
+    for (size_t k = 0; k < e->m.size(); k++)
+        if (e->gen[k] != e->m[k]->gen) {
+            ens_drop(e);
+            break;
+        }
+    int rc = ens_capture(e, kind);
+    if (rc) return rc;
+    cudaError_t ce = cudaGraphLaunch(e->g[kind].exec, e->s);
+    if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "ensemble graph launch", ce);
+    e->launches += e->g[kind].kernels;
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_ensemble_create(MdbCp* const* members, int n, MdbCpEnsemble** out)
+{
+    if (!members || n < 1 || !out) return MDB_ERR_ARG;
+    *out = nullptr;
+    for (int k = 0; k < n; k++) {
+        MdbCp* c = members[k];
+        if (!c || !c->have_list) return MDB_ERR_STATE;
+        if (c->dev != members[0]->dev || c->p.reneigh_every != members[0]->p.reneigh_every ||
+            c->p.nstat != members[0]->p.nstat || c->prune_every != members[0]->prune_every)
+            return MDB_ERR_ARG;
+    }
+    MdbCpEnsemble* e = new MdbCpEnsemble();
+    e->m.assign(members, members + n);
+    e->gen.assign(n, 0);
+    for (int k = 0; k < n; k++) e->gen[k] = members[k]->gen;
+    e->dev = members[0]->dev;
+    cudaError_t ce = cudaSetDevice(e->dev);
+    if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->s, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming);
+    e->join.assign(n, nullptr);
+    for (int k = 0; k < n && ce == cudaSuccess; k++)
+        ce = cudaEventCreateWithFlags(&e->join[k], cudaEventDisableTiming);
+    if (ce == cudaSuccess) ce = cudaMallocHost((void**)&e->h_red, 4 * sizeof(double) * n);
+    if (ce != cudaSuccess) {
+        mdb_cp_ensemble_destroy(e);
+        return MDB_ERR_CUDA;
+    }
+    *out = e;
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_ensemble_destroy(MdbCpEnsemble* e)
+{
+    if (!e) return MDB_ERR_ARG;
+    cudaSetDevice(e->dev);
+    if (e->s) cudaStreamSynchronize(e->s);
+    ens_drop(e);
+    for (auto ev : e->join)
+        if (ev) cudaEventDestroy(ev);
+    if (e->fork) cudaEventDestroy(e->fork);
+    if (e->h_red) cudaFreeHost(e->h_red);
+    if (e->s) cudaStreamDestroy(e->s);
+    delete e;
+    return MDB_OK;
+}
+
+extern "C" const char* mdb_cp_ensemble_last_error(const MdbCpEnsemble* e)
+{
+    return e ? e->err.c_str() : "";
+}
+extern "C" void* mdb_cp_ensemble_stream(MdbCpEnsemble* e) { return e ? (void*)e->s : nullptr; }
+extern "C" long long mdb_cp_ensemble_launch_count(const MdbCpEnsemble* e)
+{
+    return e ? e->launches : 0;
+}
+
+// rebuild: one graph for all members, one synchronisation, then members whose
+// buffers overflowed grow and rebuild on their own (their atom arrays already
+// hold the wrapped state, so the rebuild is idempotent)
+static int ens_rebuild(MdbCpEnsemble* e, bool pending_final)
+{
+    int rc = ens_launch(e, pending_final ? EG_REB_FI : EG_REB_I);
+    if (rc) return rc;
+    cudaError_t ce = cudaStreamSynchronize(e->s);
+    if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "ensemble rebuild", ce);
+    for (MdbCp* c : e->m) {
+        int r = eval_build(c, CHK_ALL);
+        if (r < 0) return ens_fail(e, -r, c->err.c_str());
+        if (r > 0) {
+            // grown buffers bump the member's generation: graphs are recaptured
+            rc = do_build(c);
+            if (rc) return ens_fail(e, rc, c->err.c_str());
+        }
+        c->have_clusters = c->have_ghosts = c->have_list = true;
+    }
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_ensemble_run(MdbCpEnsemble* e, int first_step, int nsteps,
+    MdbThermo* samples, int max_samples, int* nsamples)
+{
+    if (!e || nsteps < 0 || (max_samples > 0 && !samples)) return MDB_ERR_ARG;
+    cudaSetDevice(e->dev);
+    const int n = (int)e->m.size();
+    MdbCp* c0   = e->m[0];
+    if (nsamples) *nsamples = 0;
+    // members' own streams may still hold work: order the ensemble after it
+    for (MdbCp* c : e->m) cudaStreamSynchronize(c->s);
+    int nslot = 0, rc;
+    const int last     = first_step + nsteps - 1;
+    bool pending_final = false;
+    for (int step = first_step; step <= last; step++) {
+        const bool reneigh = (step + 1) % c0->p.reneigh_every == 0;
+        const bool prune   = !reneigh && (step + 1) % c0->prune_every == 0;
+        const bool sample  = max_samples > 0 && (step + 1) % c0->p.nstat == 0 && nslot < max_samples;
+        if (prune) {
+            // rare (default never): direct launches on the members' streams
+            cudaStreamSynchronize(e->s);
+            const long long m0 = mark();
+            for (MdbCp* c : e->m) {
+                if (pending_final) enq_final_initial(c);
+                else enq_initial(c);
+                enq_prune(c);
+                enq_ghost_update(c);
+                enq_force(c, false);
+                cudaStreamSynchronize(c->s);
+            }
+            e->launches += mark() - m0;
+            pending_final = true;
+        } else if (reneigh) {
+            if ((rc = ens_rebuild(e, pending_final))) return rc;
+            if ((rc = ens_launch(e, sample ? EG_SAMPLE : EG_FORCE))) return rc;
+            pending_final = !sample;
+        } else {
+            if (sample) {
+                if ((rc = ens_launch(e, pending_final ? EG_FRONT_FI : EG_FRONT_I))) return rc;
+                if ((rc = ens_launch(e, EG_SAMPLE))) return rc;
+                pending_final = false;
+            } else {
+                if ((rc = ens_launch(e, pending_final ? EG_PLAIN_FI : EG_PLAIN_I))) return rc;
+                pending_final = true;
+            }
+        }
+        if (sample) {
+            cudaError_t ce = cudaStreamSynchronize(e->s);
+            if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "ensemble sample", ce);
+            for (int k = 0; k < n; k++) {
+                MdbCp* c = e->m[k];
+                finish_thermo(c, c->h_red, step + 1, &samples[(size_t)k * max_samples + nslot]);
+                c->energy_valid = true;
+            }
+            nslot++;
+        }
+    }
+    if (pending_final && (rc = ens_launch(e, EG_FINAL))) return rc;
+    cudaError_t ce = cudaStreamSynchronize(e->s);
+    if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "ensemble run", ce);
+    if (nsamples) *nsamples = nslot;
     return MDB_OK;
 }

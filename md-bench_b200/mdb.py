@@ -94,7 +94,9 @@ CP_EXPORTS = [
     "mdb_cp_initial_integrate", "mdb_cp_final_integrate", "mdb_cp_thermo", "mdb_cp_setup",
     "mdb_cp_run", "mdb_cp_get_counts", "mdb_cp_get_slots", "mdb_cp_get_iclusters",
     "mdb_cp_get_jclusters", "mdb_cp_get_ghosts", "mdb_cp_get_neighbor_list",
-    "mdb_cp_get_columns", "mdb_cp_get_geometry",
+    "mdb_cp_get_columns", "mdb_cp_get_geometry", "mdb_cp_time_force", "mdb_cp_ensemble_create",
+    "mdb_cp_ensemble_destroy", "mdb_cp_ensemble_last_error", "mdb_cp_ensemble_stream",
+    "mdb_cp_ensemble_launch_count", "mdb_cp_ensemble_run",
 ]
 # every symbol include/mdb_host.h declares
 HOST_EXPORTS = [
@@ -162,6 +164,13 @@ def load():
         "mdb_cp_get_columns": ([vp, vp, vp, ip], ip),
         "mdb_cp_get_geometry": ([vp, vp, vp, vp, ip], ip),
         "mdb_cp_tune": ([vp, C.c_char_p, ip], ip),
+        "mdb_cp_time_force": ([vp, ip, C.POINTER(C.c_double)], ip),
+        "mdb_cp_ensemble_create": ([C.POINTER(vp), ip, C.POINTER(vp)], ip),
+        "mdb_cp_ensemble_destroy": ([vp], ip),
+        "mdb_cp_ensemble_last_error": ([vp], C.c_char_p),
+        "mdb_cp_ensemble_stream": ([vp], vp),
+        "mdb_cp_ensemble_launch_count": ([vp], C.c_longlong),
+        "mdb_cp_ensemble_run": ([vp, ip, ip, C.POINTER(MdbThermo), ip, C.POINTER(ip)], ip),
     })
     for name in ("mdb_cp_synchronize", "mdb_cp_build_clusters", "mdb_cp_define_jclusters",
                  "mdb_cp_setup_pbc",
@@ -719,6 +728,12 @@ class ClusterSystem:
     def tune(self, key, value):
         self._ck(self.lib.mdb_cp_tune(self.h, key.encode(), int(value)), "mdb_cp_tune")
 
+    def time_force(self, reps=20):
+        """Seconds per force launch (CUDA events on the context's stream)."""
+        t = C.c_double()
+        self._ck(self.lib.mdb_cp_time_force(self.h, int(reps), C.byref(t)), "mdb_cp_time_force")
+        return t.value
+
     @property
     def stream(self):
         return int(self.lib.mdb_cp_stream(self.h) or 0)
@@ -726,3 +741,49 @@ class ClusterSystem:
     @property
     def launches(self):
         return int(self.lib.mdb_cp_launch_count(self.h))
+
+
+class Ensemble:
+    """Independent cluster-pair systems advanced together, one CUDA graph launch
+    per timestep for all of them (an ``MdbCpEnsemble``). Members must be set up."""
+
+    def __init__(self, members):
+        self.lib = load()
+        self.members = list(members)
+        arr = (C.c_void_p * len(self.members))(*[m.h.value for m in self.members])
+        h = C.c_void_p()
+        rc = self.lib.mdb_cp_ensemble_create(arr, len(self.members), C.byref(h))
+        if rc:
+            raise MdbError(f"mdb_cp_ensemble_create failed: "
+                           f"{self.lib.mdb_status_string(rc).decode()}")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mdb_cp_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def run(self, nsteps, first_step=0, max_samples=16):
+        """Returns one list of thermo samples per member."""
+        n = len(self.members)
+        buf = (MdbThermo * max(n * max_samples, 1))()
+        ns = C.c_int()
+        rc = self.lib.mdb_cp_ensemble_run(self.h, first_step, nsteps, buf, max_samples,
+                                          C.byref(ns))
+        if rc:
+            msg = self.lib.mdb_cp_ensemble_last_error(self.h)
+            raise MdbError(f"mdb_cp_ensemble_run: {self.lib.mdb_status_string(rc).decode()}"
+                           f" ({msg.decode() if msg else ''})")
+        return [[buf[k * max_samples + j].as_dict() for j in range(ns.value)]
+                for k in range(n)]
+
+    @property
+    def stream(self):
+        return int(self.lib.mdb_cp_ensemble_stream(self.h) or 0)
+
+    @property
+    def launches(self):
+        return int(self.lib.mdb_cp_ensemble_launch_count(self.h))

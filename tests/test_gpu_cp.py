@@ -310,3 +310,119 @@ def test_launch_count_and_atoms_roundtrip():
     o.run(20)
     xo, vo, to = o.atoms()
     assert np.array_equal(xa, xo) and np.array_equal(va, vo) and np.array_equal(ta, to)
+
+
+# ---- multi-type liquid: 4 types, geometric mixing, cutoff 2.5 sigma_max, half lists
+
+def c5_params():
+    import workloads as W
+    eps, sig = W.c5_types()
+    return (eps, sig), W.c5_cutoff(sig)
+
+
+@pytest.mark.parametrize("N", SHAPES)
+def test_c5_types_bit_exact_small(N):
+    types, rc = c5_params()
+    hp, x, v, t = thermalised(6, types=types, cutforce=rc)
+    assert hp.ntypes == 4 and abs(hp.cutforce - rc) < 1e-15
+    s, o = pair(hp, x, v, t, N, half=1)
+    assert_same_build(s, o)
+    valid = valid_slots(o)
+    assert_forces_close(local_forces(s, valid), local_forces(o, valid))
+    sm, _ = pair(hp, x, v, t, N, half=1, precision="mixed")
+    f, fo = local_forces(sm, valid), local_forces(o, valid)
+    rms = np.sqrt(np.mean(np.sum(fo * fo, axis=1)))
+    assert np.sqrt(np.mean(np.sum((f - fo) ** 2, axis=1))) / rms <= MIXED_RMS
+
+
+@pytest.mark.slow
+def test_c5_full_scale_128():
+    """128^3 cells = 8,388,608 atoms, 4 types, half 4x4 lists: the mixed and FP64
+    contexts build identical clusters and lists, and after 20 steps from the
+    lattice the mixed forces on the FP64 state are within the error budget."""
+    types, rc = c5_params()
+    hp = mdb.host_params(nx=128, ny=128, nz=128, types=types, cutforce=rc)
+    x, v, t = mdb.create_fcc(hp)
+    assert len(t) == 8388608
+    kw = dict(xprd=hp.xprd, yprd=hp.yprd, zprd=hp.zprd, cutforce=hp.cutforce,
+              cutneigh=hp.cutneigh, dt=hp.dt, dtforce=hp.dtforce, mass=hp.mass, ntypes=4,
+              epsilon_per_type=types[0], sigma_per_type=types[1], natoms=len(t),
+              cluster_n=4, half_neigh=1)
+    s64 = mdb.ClusterSystem(precision="fp64", **kw)
+    s64.set_atoms(x, v, t)
+    s64.setup()
+    s64.run(20, max_samples=0)
+    xs, vs, ts = s64.atoms()
+    s32 = mdb.ClusterSystem(precision="mixed", **kw)
+    for s in (s64, s32):
+        s.set_atoms(xs, vs, ts)
+        s.setup()
+    assert s64.counts() == s32.counts()
+    assert np.array_equal(s64.numneigh(), s32.numneigh())
+    nat = s64.iclusters()[0]
+    valid = np.concatenate([np.arange(4) < k for k in nat])
+    f64 = s64.slots()[2][:len(valid)][valid]
+    f32 = s32.slots()[2][:len(valid)][valid]
+    rms = np.sqrt(np.mean(np.sum(f64 * f64, axis=1)))
+    err = np.sqrt(np.sum((f32 - f64) ** 2, axis=1))
+    assert np.sqrt(np.mean(err * err)) / rms <= MIXED_RMS
+    s64.close()
+    s32.close()
+
+
+# ---- ensembles of independent replicas (one graph launch per timestep)
+
+def replica(n, rho, temp, N, precision):
+    hp = mdb.host_params(nx=n, ny=n, nz=n, rho=rho, temp=temp, nstat=10)
+    x, v, t = mdb.create_fcc(hp)
+    kw = dict(xprd=hp.xprd, yprd=hp.yprd, zprd=hp.zprd, cutforce=hp.cutforce,
+              cutneigh=hp.cutneigh, dt=hp.dt, dtforce=hp.dtforce, mass=hp.mass,
+              reneigh_every=hp.reneigh_every, nstat=hp.nstat, natoms=len(t), cluster_n=N,
+              precision=precision, ntypes=hp.ntypes)
+    out = []
+    for _ in range(2):
+        s = mdb.ClusterSystem(**kw)
+        s.set_atoms(x, v, t)
+        s.setup()
+        out.append(s)
+    return out
+
+
+@pytest.mark.parametrize("N,precision", [(4, "fp64"), (8, "fp64"), (4, "mixed")])
+def test_ensemble_matches_members(N, precision):
+    """Replicas of uneven size, density and temperature advanced as one
+    ensemble follow, bit for bit, the trajectories and thermo samples of the
+    same replicas run one at a time (full lists: no atomics)."""
+    specs = [(4, 0.80, 0.9), (5, 0.9, 1.8), (7, 0.76, 1.2), (3, 0.94, 0.7)]
+    pairs = [replica(n, rho, T, N, precision) for n, rho, T in specs]
+    ens = mdb.Ensemble([p[0] for p in pairs])
+    got = ens.run(45, max_samples=8)
+    got2 = ens.run(17, first_step=45, max_samples=8)
+    assert ens.launches > 0
+    for k, (a, b) in enumerate(pairs):
+        want = b.run(45, max_samples=8)
+        want2 = b.run(17, first_step=45, max_samples=8)
+        assert [w["step"] for w in want] == [10, 20, 30, 40]
+        assert got[k] == want and got2[k] == want2, k
+        xa, va, ta = a.atoms()
+        xb, vb, tb = b.atoms()
+        assert np.array_equal(xa, xb) and np.array_equal(va, vb) and np.array_equal(ta, tb)
+        sa, sb = a.slots(), b.slots()
+        for u, w in zip(sa, sb):
+            assert np.array_equal(u, w)
+    ens.close()
+
+
+def test_ensemble_rejects_mismatched_members():
+    a = replica(3, 0.8442, 1.44, 4, "fp64")[0]
+    hp = mdb.host_params(nx=3, ny=3, nz=3, reneigh_every=10)
+    x, v, t = mdb.create_fcc(hp)
+    b = mdb.ClusterSystem(xprd=hp.xprd, yprd=hp.yprd, zprd=hp.zprd, cutforce=hp.cutforce,
+                          cutneigh=hp.cutneigh, dt=hp.dt, dtforce=hp.dtforce, natoms=len(t),
+                          reneigh_every=10, ntypes=hp.ntypes)
+    b.set_atoms(x, v, t)
+    with pytest.raises(mdb.MdbError):
+        mdb.Ensemble([a, b])  # b not set up
+    b.setup()
+    with pytest.raises(mdb.MdbError):
+        mdb.Ensemble([a, b])  # different rebuild period
