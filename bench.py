@@ -254,41 +254,27 @@ class Replicas:
             self.cache[key] = (hp, x, v, t)
         return self.cache[key]
 
-    def build(self, sp, cluster_n, half, choice=None):
+    def build(self, sp, cluster_n, half, choice=None, precision="mixed"):
         import autotune as AT
         hp, x, v, t = self.state(sp)
         s = self.mdb.ClusterSystem(natoms=len(t), cluster_n=cluster_n, half_neigh=half,
-                                   precision="mixed", device=self.device, xprd=hp.xprd,
+                                   precision=precision, device=self.device, xprd=hp.xprd,
                                    yprd=hp.yprd, zprd=hp.zprd, cutforce=hp.cutforce,
                                    cutneigh=hp.cutneigh, dt=hp.dt, dtforce=hp.dtforce,
                                    mass=hp.mass, reneigh_every=hp.reneigh_every,
                                    nstat=hp.nstat, ntypes=hp.ntypes)
-        if choice is not None:
+        if choice is not None and precision == "mixed":
             AT.apply_launch(s, choice)
         s.set_atoms(x, v, t)
         s.setup()
         return s
 
 
-def c4_ensemble(torch, mdb, args, device):
-    """256 LJ replicas of uneven size, density and temperature advanced as one
-    ensemble (one graph launch per timestep), autotuned per size class."""
-    import autotune as AT
-    specs = c4_specs(args.replicas)
-    pool = Replicas(mdb, device)
-    t0 = time.perf_counter()
-    if args.no_autotune:
-        choice, trials = {}, []
-    else:
-        choice, trials = AT.tune_ensemble(specs, lambda sp, n, h: pool.build(sp, n, h))
-    tune_secs = time.perf_counter() - t0
-    members = []
-    for sp in specs:
-        c = choice.get(AT.size_class(sp["natoms"]), AT.DEFAULT)
-        members.append(pool.build(sp, c["cluster_n"], c["half"], c))
+def run_ensemble(torch, mdb, members, args, every=20):
+    """Device time of args.steps rebuild periods of an ensemble (after
+    args.warmup untimed ones) and the energy drift of every member."""
     ens = mdb.Ensemble(members)
     th0 = [m.thermo() for m in members]
-    every = 20
     stream = torch.cuda.ExternalStream(ens.stream)
     n = 0
     for _ in range(args.warmup):
@@ -309,26 +295,55 @@ def c4_ensemble(torch, mdb, args, device):
     e1.synchronize()
     secs = e0.elapsed_time(e1) / 1e3
     launches = ens.launches - l0
-    nat = sum(sp["natoms"] for sp in specs)
-    drifts = [abs((q[-1]["E"] - t["E"]) / t["E"]) for q, t in zip(samples, th0) if q]
+    ens.close()
+    drifts = [(q[-1]["E"] - t["E"]) / abs(t["E"]) if q else 0.0
+              for q, t in zip(samples, th0)]
+    return secs, launches, np.array(drifts), n
+
+
+def c4_ensemble(torch, mdb, args, device):
+    """256 LJ replicas of uneven size, density and temperature advanced as one
+    ensemble (one graph launch per timestep, batched kernels over all
+    replicas), autotuned per size class; the same replicas in FP64 give the
+    energy drift the mixed path is compared with."""
+    import autotune as AT
+    specs = c4_specs(args.replicas)
+    pool = Replicas(mdb, device)
+    t0 = time.perf_counter()
+    if args.no_autotune:
+        choice, trials = {}, []
+    else:
+        choice, trials = AT.tune_ensemble(specs, lambda sp, n, h: pool.build(sp, n, h),
+                                          rounds=1)
+    tune_secs = time.perf_counter() - t0
+    pick = [choice.get(AT.size_class(sp["natoms"]), AT.DEFAULT) for sp in specs]
+    every = 20
+    members = [pool.build(sp, c["cluster_n"], c["half"], c) for sp, c in zip(specs, pick)]
+    secs, launches, d32, n = run_ensemble(torch, mdb, members, args, every)
     # the same replicas advanced one after another (each its own graph loop)
     t1 = time.perf_counter()
     for m in members:
         m.run(every, first_step=n, max_samples=0)
     serial = time.perf_counter() - t1
-    ens.close()
     for m in members:
         m.close()
+    members = [pool.build(sp, c["cluster_n"], c["half"], None, "fp64")
+               for sp, c in zip(specs, pick)]
+    secs64, _, d64, _ = run_ensemble(torch, mdb, members, args, every)
+    for m in members:
+        m.close()
+    nat = sum(sp["natoms"] for sp in specs)
     shapes = {}
-    for sp in specs:
-        c = choice.get(AT.size_class(sp["natoms"]), AT.DEFAULT)
-        key = f"{4}x{c['cluster_n']}-{'half' if c['half'] else 'full'}"
+    for c in pick:
+        key = f"4x{c['cluster_n']}-{'half' if c['half'] else 'full'}"
         shapes[key] = shapes.get(key, 0) + 1
     return {"value": nat * every * args.steps / secs, "ms_per_step": 1e3 * secs / args.steps,
             "natoms": nat, "replicas": len(specs), "md_steps": every * args.steps,
             "gpu_launches": launches, "graph_launches_per_md_step": 1,
-            "energy_drift_max_abs": max(drifts) if drifts else None,
-            "energy_drift_median_abs": float(np.median(drifts)) if drifts else None,
+            "energy_drift_max_abs": float(np.abs(d32).max()),
+            "energy_drift_fp64_max_abs": float(np.abs(d64).max()),
+            "excess_drift_vs_fp64_max_abs": float(np.abs(d32 - d64).max()),
+            "fp64_value": nat * every * args.steps / secs64,
             "serial_value": nat * every / serial,
             "autotune": {"seconds": round(tune_secs, 2), "trials": len(trials),
                          "choice_per_size_class": {str(k): v for k, v in choice.items()},

@@ -122,6 +122,12 @@ int mdb_cp_ensemble_destroy(MdbCpEnsemble* ens);
 const char* mdb_cp_ensemble_last_error(const MdbCpEnsemble* ens);
 void* mdb_cp_ensemble_stream(MdbCpEnsemble* ens);
 long long mdb_cp_ensemble_launch_count(const MdbCpEnsemble* ens);
+/* "batched" = 1 (the default when every member is MDB_PREC_MIXED): the
+ * integrator, the ghost update and the force kernel each run as one launch
+ * over all members (members grouped by cluster shape, list form, types and
+ * launch settings); 0: every member runs its own kernel sequence on its own
+ * graph branch. Results are the same either way. */
+int mdb_cp_ensemble_tune(MdbCpEnsemble* ens, const char* key, int value);
 int mdb_cp_ensemble_run(MdbCpEnsemble* ens, int first_step, int nsteps, MdbThermo* samples,
     int max_samples, int* nsamples);
 

@@ -384,7 +384,8 @@ static int alloc_atoms(MdbCp* ctx, int n)
     dfree(ctx->scan_scratch), dfree(ctx->partials), dfree(ctx->stage), dfree(ctx->stage_i);
     int scan_n          = std::max(std::max(mb + 2, ctx->ncj_cap + 1), 1);
     ctx->scan_scratch_n = scan_scratch_ints(scan_n);
-    ctx->npart = std::max(force_blocks(ctx->ncl_cap), ke_blocks(ctx->ncl_cap * ctx->M));
+    // energy partials: one per force block (mixed blocks of 32 threads at the least)
+    ctx->npart = std::max(4 * force_blocks(ctx->ncl_cap), ke_blocks(ctx->ncl_cap * ctx->M));
     ctx->stage_n = (size_t)3 * std::max(n, 1) * 3;
     if ((e = dalloc(&ctx->ax, n)) != cudaSuccess || (e = dalloc(&ctx->av, n)) != cudaSuccess ||
         (e = dalloc(&ctx->atom_col, n)) != cudaSuccess ||
@@ -695,10 +696,10 @@ static void enq_force(MdbCp* ctx, bool energy)
     if (ctx->mixed) {
         if (ctx->p.half_neigh)
             cudaMemsetAsync(ctx->cf32, 0, sizeof(float4) * (size_t)nloc_slots, s);
-        launch_force_mixed(s, ctx->N, ctx->p.half_neigh, energy, ctx->ncl_cap, ctx->cnt, ctx->xr,
-            ctx->anchor, ctx->ty, (float)ctx->cutforcesq, ctx->list, lks(ctx), lcs(ctx),
-            ctx->numneigh, ctx->cf32, ctx->partials);
-        if (energy) ctx->energy_blocks = force_blocks(ctx->ncl_cap);
+        const int nb = launch_force_mixed(s, ctx->N, ctx->p.half_neigh, energy, ctx->ncl_cap,
+            ctx->cnt, ctx->xr, ctx->anchor, ctx->ty, (float)ctx->cutforcesq, ctx->list, lks(ctx),
+            lcs(ctx), ctx->numneigh, ctx->cf32, ctx->partials);
+        if (energy) ctx->energy_blocks = nb;
     } else {
         if (ctx->p.half_neigh)
             cudaMemsetAsync(ctx->cf, 0, sizeof(double4) * (size_t)nloc_slots, s);
@@ -1293,6 +1294,25 @@ struct MdbCpEnsemble {
     CpGraph g[16];
     std::vector<unsigned> gen;
     double* h_red = nullptr; // 4 doubles per member
+    // batched launches (every member mixed): the integrator, the ghost update
+    // and each force group run as one launch over all members; the members'
+    // own streams only carry the rebuild and the thermo sums
+    bool batched   = false;
+    bool tables_ok = false;
+    CpStepMember* d_step   = nullptr;
+    CpForceMember* d_force = nullptr;
+    int2* d_bmap           = nullptr;
+    size_t bmap_cap        = 0;
+    int nb_integ = 0, nb_ghost = 0;
+    size_t off_integ = 0, off_ghost = 0;
+    struct Group { // members sharing cluster shape, list form, types and launch shape
+        int N, half;
+        Types ty;
+        float cutsq;
+        int nblocks;
+        size_t off;
+    };
+    std::vector<Group> groups;
 };
 
 // step parts captured per ensemble: FI = final integration of the previous
@@ -1313,6 +1333,7 @@ static_assert(EG_COUNT <= 16, "graph slots of MdbCpEnsemble");
 
 static void ens_drop(MdbCpEnsemble* e)
 {
+    e->tables_ok = false;
     for (size_t k = 0; k < e->m.size(); k++) e->gen[k] = e->m[k]->gen;
     for (auto& g : e->g) {
         if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -1366,22 +1387,182 @@ static void ens_body(MdbCp* c, int kind)
     }
 }
 
-static int ens_capture(MdbCpEnsemble* e, int kind)
+static bool same_types(const Types& a, const Types& b)
 {
-    CpGraph& g = e->g[kind];
-    if (g.exec) return MDB_OK;
-    cudaGraph_t graph;
-    long long m0 = mark();
-    cudaError_t ce = cudaStreamBeginCapture(e->s, cudaStreamCaptureModeThreadLocal);
-    if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "ensemble capture", ce);
+    if (a.ntypes != b.ntypes || a.uniform != b.uniform || a.eps0 != b.eps0 ||
+        a.sigma6_0 != b.sigma6_0 || a.force_block != b.force_block ||
+        a.force_variant != b.force_variant)
+        return false;
+    for (int t = 0; t < MDB_MAX_TYPES; t++)
+        if (a.sqrt_eps_f[t] != b.sqrt_eps_f[t] || a.sigma3_f[t] != b.sigma3_f[t]) return false;
+    return true;
+}
+
+// member tables and block maps of the batched launches, from the members'
+// current buffers and capacities
+static int ens_tables(MdbCpEnsemble* e)
+{
+    if (e->tables_ok) return MDB_OK;
+    // graphs launched earlier may still read the old tables
+    cudaError_t ce = cudaStreamSynchronize(e->s);
+    if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "ensemble tables", ce);
+    const int n = (int)e->m.size();
+    std::vector<CpStepMember> st(n);
+    std::vector<CpForceMember> fo(n);
+    std::vector<int2> maps;
+    auto add = [&](int k, int nb) {
+        for (int b = 0; b < nb; b++) maps.push_back(make_int2(k, b));
+    };
+    for (int k = 0; k < n; k++) {
+        const MdbCp* c = e->m[k];
+        CpStepMember& a = st[k];
+        a.cnt = c->cnt, a.cx = c->cx, a.cv = c->cv, a.cf = c->cf, a.cf32 = c->cf32;
+        a.anchor = c->anchor, a.xr = c->xr, a.border = c->border, a.pbc = c->pbc;
+        a.jnat = c->jnat, a.dtf = c->p.dtforce, a.dt = c->p.dt, a.xprd = c->g.xprd;
+        a.yprd = c->g.yprd, a.zprd = c->g.zprd, a.M = c->M, a.N = c->N, a.mixed = c->mixed;
+        a.zero_f = c->p.half_neigh;
+        CpForceMember& f = fo[k];
+        f.cnt = c->cnt, f.xr = c->xr, f.anchor = c->anchor, f.list = c->list;
+        f.numneigh = c->numneigh, f.cf32 = c->cf32, f.epart = c->partials, f.cs = lcs(c);
+        f.pad = 0;
+    }
+    e->off_integ = maps.size();
+    for (int k = 0; k < n; k++)
+        add(k, mdb_blocks((long long)e->m[k]->ncl_cap * e->m[k]->M, MDB_NTHREADS));
+    e->nb_integ  = (int)(maps.size() - e->off_integ);
+    e->off_ghost = maps.size();
+    for (int k = 0; k < n; k++)
+        add(k, mdb_blocks((long long)e->m[k]->ngc_cap * e->m[k]->N, MDB_NTHREADS));
+    e->nb_ghost = (int)(maps.size() - e->off_ghost);
+    e->groups.clear();
+    std::vector<int> gid(n, -1);
+    for (int k = 0; k < n; k++) {
+        const MdbCp* c    = e->m[k];
+        const float cutsq = (float)c->cutforcesq;
+        for (size_t q = 0; q < e->groups.size() && gid[k] < 0; q++) {
+            const auto& gr = e->groups[q];
+            if (gr.N == c->N && gr.half == c->p.half_neigh && gr.cutsq == cutsq &&
+                same_types(gr.ty, c->ty))
+                gid[k] = (int)q;
+        }
+        if (gid[k] < 0) {
+            gid[k] = (int)e->groups.size();
+            e->groups.push_back({c->N, c->p.half_neigh, c->ty, cutsq, 0, 0});
+        }
+    }
+    for (size_t q = 0; q < e->groups.size(); q++) {
+        auto& gr = e->groups[q];
+        gr.off   = maps.size();
+        for (int k = 0; k < n; k++)
+            if (gid[k] == (int)q) {
+                MdbCp* c         = e->m[k];
+                const int nb     = force_mixed_grid(c->ncl_cap, c->ty);
+                c->energy_blocks = nb; // the partials a batched energy launch writes
+                add(k, nb);
+            }
+        gr.nblocks = (int)(maps.size() - gr.off);
+    }
+    if (!e->d_step) {
+        ce = cudaMalloc((void**)&e->d_step, sizeof(CpStepMember) * n);
+        if (ce == cudaSuccess) ce = cudaMalloc((void**)&e->d_force, sizeof(CpForceMember) * n);
+        if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_NOMEM, "ensemble tables", ce);
+    }
+    if (maps.size() > e->bmap_cap) {
+        if (e->d_bmap) cudaFree(e->d_bmap);
+        e->d_bmap   = nullptr;
+        e->bmap_cap = maps.size() + maps.size() / 4;
+        ce          = cudaMalloc((void**)&e->d_bmap, sizeof(int2) * e->bmap_cap);
+        if (ce != cudaSuccess) {
+            e->bmap_cap = 0;
+            return ens_fail(e, MDB_ERR_NOMEM, "ensemble block maps", ce);
+        }
+    }
+    ce = cudaMemcpy(e->d_step, st.data(), sizeof(CpStepMember) * n, cudaMemcpyHostToDevice);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpy(e->d_force, fo.data(), sizeof(CpForceMember) * n, cudaMemcpyHostToDevice);
+    if (ce == cudaSuccess && !maps.empty())
+        ce = cudaMemcpy(e->d_bmap, maps.data(), sizeof(int2) * maps.size(),
+            cudaMemcpyHostToDevice);
+    if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "ensemble tables", ce);
+    e->tables_ok = true;
+    return MDB_OK;
+}
+
+static void ens_integ(MdbCpEnsemble* e, bool final_, bool initial)
+{
+    launch_cp_integrate_batch(e->s, final_, initial, e->nb_integ, e->d_step,
+        e->d_bmap + e->off_integ);
+}
+
+static void ens_forces(MdbCpEnsemble* e, bool energy)
+{
+    for (const auto& gr : e->groups)
+        launch_force_mixed_batch(e->s, gr.N, gr.half, energy, gr.ty, gr.cutsq, gr.nblocks,
+            e->d_force, e->d_bmap + gr.off);
+}
+
+// per-member work on the members' streams, forked from and joined to e->s
+template <class F> static void ens_fork(MdbCpEnsemble* e, F&& body)
+{
     cudaEventRecord(e->fork, e->s);
     for (size_t k = 0; k < e->m.size(); k++) {
         MdbCp* c = e->m[k];
         cudaStreamWaitEvent(c->s, e->fork, 0);
-        ens_body(c, kind);
+        body(c);
         cudaEventRecord(e->join[k], c->s);
         cudaStreamWaitEvent(e->s, e->join[k], 0);
     }
+}
+
+static void ens_body_batched(MdbCpEnsemble* e, int kind)
+{
+    const bool fi = kind == EG_PLAIN_FI || kind == EG_FRONT_FI || kind == EG_REB_FI;
+    switch (kind) {
+    case EG_PLAIN_FI:
+    case EG_PLAIN_I:
+    case EG_FRONT_FI:
+    case EG_FRONT_I:
+        ens_integ(e, fi, true);
+        launch_ghost_update_batch(e->s, e->nb_ghost, e->d_step, e->d_bmap + e->off_ghost);
+        if (kind == EG_PLAIN_FI || kind == EG_PLAIN_I) ens_forces(e, false);
+        break;
+    case EG_REB_FI:
+    case EG_REB_I:
+        ens_integ(e, fi, true);
+        ens_fork(e, [](MdbCp* c) {
+            enq_gather(c, 1);
+            enq_build(c);
+            cudaMemcpyAsync(c->h_cnt, c->cnt, CP_SLOTS * sizeof(int), cudaMemcpyDeviceToHost,
+                c->s);
+        });
+        break;
+    case EG_FORCE: ens_forces(e, false); break;
+    case EG_SAMPLE:
+        ens_forces(e, true);
+        ens_integ(e, true, false);
+        ens_fork(e, [](MdbCp* c) {
+            enq_thermo(c, 0, true);
+            cudaMemcpyAsync(c->h_red, c->red, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->s);
+        });
+        break;
+    case EG_FINAL: ens_integ(e, true, false); break;
+    }
+}
+
+static int ens_capture(MdbCpEnsemble* e, int kind)
+{
+    CpGraph& g = e->g[kind];
+    if (g.exec) return MDB_OK;
+    if (e->batched) {
+        int rc = ens_tables(e);
+        if (rc) return rc;
+    }
+    cudaGraph_t graph;
+    long long m0 = mark();
+    cudaError_t ce = cudaStreamBeginCapture(e->s, cudaStreamCaptureModeThreadLocal);
+    if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "ensemble capture", ce);
+    if (e->batched) ens_body_batched(e, kind);
+    else ens_fork(e, [kind](MdbCp* c) { ens_body(c, kind); });
     ce        = cudaStreamEndCapture(e->s, &graph);
     g.kernels = mdb::g_launches - m0;
     mdb::g_launches = m0;
@@ -1430,6 +1611,8 @@ extern "C" int mdb_cp_ensemble_create(MdbCp* const* members, int n, MdbCpEnsembl
     for (int k = 0; k < n && ce == cudaSuccess; k++)
         ce = cudaEventCreateWithFlags(&e->join[k], cudaEventDisableTiming);
     if (ce == cudaSuccess) ce = cudaMallocHost((void**)&e->h_red, 4 * sizeof(double) * n);
+    e->batched = true;
+    for (int k = 0; k < n; k++) e->batched = e->batched && members[k]->mixed;
     if (ce != cudaSuccess) {
         mdb_cp_ensemble_destroy(e);
         return MDB_ERR_CUDA;
@@ -1448,6 +1631,9 @@ extern "C" int mdb_cp_ensemble_destroy(MdbCpEnsemble* e)
         if (ev) cudaEventDestroy(ev);
     if (e->fork) cudaEventDestroy(e->fork);
     if (e->h_red) cudaFreeHost(e->h_red);
+    if (e->d_step) cudaFree(e->d_step);
+    if (e->d_force) cudaFree(e->d_force);
+    if (e->d_bmap) cudaFree(e->d_bmap);
     if (e->s) cudaStreamDestroy(e->s);
     delete e;
     return MDB_OK;
@@ -1458,6 +1644,21 @@ extern "C" const char* mdb_cp_ensemble_last_error(const MdbCpEnsemble* e)
     return e ? e->err.c_str() : "";
 }
 extern "C" void* mdb_cp_ensemble_stream(MdbCpEnsemble* e) { return e ? (void*)e->s : nullptr; }
+
+extern "C" int mdb_cp_ensemble_tune(MdbCpEnsemble* e, const char* key, int value)
+{
+    if (!e || !key) return MDB_ERR_ARG;
+    if (!strcmp(key, "batched")) {
+        bool all_mixed = true;
+        for (MdbCp* c : e->m) all_mixed = all_mixed && c->mixed;
+        if (value && !all_mixed) return ens_fail(e, MDB_ERR_ARG, "batched needs mixed members");
+        cudaStreamSynchronize(e->s);
+        e->batched = value != 0;
+        ens_drop(e);
+        return MDB_OK;
+    }
+    return ens_fail(e, MDB_ERR_ARG, "unknown tuning key");
+}
 extern "C" long long mdb_cp_ensemble_launch_count(const MdbCpEnsemble* e)
 {
     return e ? e->launches : 0;

@@ -526,22 +526,47 @@ void launch_ghost_first(cudaStream_t s, int N, int ngc_cap, int mixed, int* cnt,
 }
 
 // updatePbcCPU(first = 0): ghost positions from their owners every step
-__global__ void k_ghost_update(int N, int mixed, const int* __restrict__ cnt,
-    const int* __restrict__ border, const int* __restrict__ pbc, const int* __restrict__ jnat,
-    Geom g, double4* cx, const float4* __restrict__ anchor, float4* xr)
+__device__ __forceinline__ void ghost_update_slot(int s, int N, int mixed,
+    const int* __restrict__ cnt, const int* __restrict__ border, const int* __restrict__ pbc,
+    const int* __restrict__ jnat, double xprd, double yprd, double zprd, double4* cx,
+    const float4* __restrict__ anchor, float4* xr)
 {
-    const int s  = blockIdx.x * blockDim.x + threadIdx.x;
     const int gi = s / N, k = s - gi * N;
     if (gi >= cnt[CP_NGC]) return;
     const int cg = cnt[CP_NCJ] + gi;
     if (k >= jnat[cg]) return;
     const int code = pbc[gi];
     double4 p      = cx[border[gi] * N + k];
-    p.x += (double)((code & 3) - 1) * g.xprd;
-    p.y += (double)(((code >> 2) & 3) - 1) * g.yprd;
-    p.z += (double)(((code >> 4) & 3) - 1) * g.zprd;
+    p.x += (double)((code & 3) - 1) * xprd;
+    p.y += (double)(((code >> 2) & 3) - 1) * yprd;
+    p.z += (double)(((code >> 4) & 3) - 1) * zprd;
     cx[cg * N + k] = p;
     if (mixed) put_rel(xr, cg * N + k, p, anchor[cg]);
+}
+
+__global__ void k_ghost_update(int N, int mixed, const int* __restrict__ cnt,
+    const int* __restrict__ border, const int* __restrict__ pbc, const int* __restrict__ jnat,
+    Geom g, double4* cx, const float4* __restrict__ anchor, float4* xr)
+{
+    ghost_update_slot(blockIdx.x * blockDim.x + threadIdx.x, N, mixed, cnt, border, pbc, jnat,
+        g.xprd, g.yprd, g.zprd, cx, anchor, xr);
+}
+
+__global__ void k_ghost_update_batch(const CpStepMember* __restrict__ tab,
+    const int2* __restrict__ bmap)
+{
+    const int2 bm         = __ldg(&bmap[blockIdx.x]);
+    const CpStepMember& m = tab[bm.x];
+    ghost_update_slot(bm.y * blockDim.x + threadIdx.x, m.N, m.mixed, m.cnt, m.border, m.pbc,
+        m.jnat, m.xprd, m.yprd, m.zprd, m.cx, m.anchor, m.xr);
+}
+
+void launch_ghost_update_batch(cudaStream_t s, int nblocks, const CpStepMember* tab,
+    const int2* bmap)
+{
+    if (nblocks <= 0) return;
+    k_ghost_update_batch<<<nblocks, MDB_NTHREADS, 0, s>>>(tab, bmap);
+    g_launches++;
 }
 
 void launch_ghost_update(cudaStream_t s, int N, int ngc_cap, int mixed, const int* cnt,

@@ -331,22 +331,18 @@ __device__ __forceinline__ JEntry load_entry(int cj, int b, const float4* __rest
 // PF: j data prefetched 1 or 2 iterations ahead; MINB: minimum resident blocks
 // of 128 threads per SM asked of the register allocator (0: no request).
 // Both are launch-shape choices of the autotuner; results do not depend on them.
-template <int N, bool HALF, bool ENERGY, bool UNIFORM, int PF, int MINB>
-__global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_force_mixed(
-    const int* __restrict__ cnt,
-    const float4* __restrict__ xr, const float4* __restrict__ anchor, Types ty,
+// The work of block bid (warps = i-clusters); s_se / s_s3: the type tables in
+// shared memory.
+template <int N, bool HALF, bool ENERGY, bool UNIFORM, int PF>
+__device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict__ cnt,
+    const float4* __restrict__ xr, const float4* __restrict__ anchor, const Types& ty,
     float cutforcesq, const int* __restrict__ list, int ks, int cs,
-    const int* __restrict__ numneigh, float4* cf32, double* epart)
+    const int* __restrict__ numneigh, float4* cf32, double* epart, const float* s_se,
+    const float* s_s3)
 {
     constexpr int JPW = 32 / N; // entries per warp iteration
-    __shared__ float s_se[MDB_MAX_TYPES], s_s3[MDB_MAX_TYPES];
-    if (threadIdx.x < MDB_MAX_TYPES) {
-        s_se[threadIdx.x] = ty.sqrt_eps_f[threadIdx.x];
-        s_s3[threadIdx.x] = ty.sigma3_f[threadIdx.x];
-    }
-    __syncthreads();
     const int lane = threadIdx.x & 31;
-    const int ci   = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int ci   = (bid * blockDim.x + threadIdx.x) >> 5;
     const int ncl  = cnt[CP_NCL];
     double e       = 0.0;
     if (ci < ncl) {
@@ -459,8 +455,100 @@ __global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_force_mix
     }
     if (ENERGY) {
         double t = block_sum(e);
-        if (threadIdx.x == 0) epart[blockIdx.x] = t;
+        if (threadIdx.x == 0) epart[bid] = t;
     }
+}
+
+__device__ __forceinline__ void load_type_tables(const Types& ty, float* s_se, float* s_s3)
+{
+    if (threadIdx.x < MDB_MAX_TYPES) {
+        s_se[threadIdx.x] = ty.sqrt_eps_f[threadIdx.x];
+        s_s3[threadIdx.x] = ty.sigma3_f[threadIdx.x];
+    }
+    __syncthreads();
+}
+
+template <int N, bool HALF, bool ENERGY, bool UNIFORM, int PF, int MINB>
+__global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_force_mixed(
+    const int* __restrict__ cnt,
+    const float4* __restrict__ xr, const float4* __restrict__ anchor, Types ty,
+    float cutforcesq, const int* __restrict__ list, int ks, int cs,
+    const int* __restrict__ numneigh, float4* cf32, double* epart)
+{
+    __shared__ float s_se[MDB_MAX_TYPES], s_s3[MDB_MAX_TYPES];
+    load_type_tables(ty, s_se, s_s3);
+    force_mixed_block<N, HALF, ENERGY, UNIFORM, PF>(blockIdx.x, cnt, xr, anchor, ty, cutforcesq,
+        list, ks, cs, numneigh, cf32, epart, s_se, s_s3);
+}
+
+// all members of an ensemble group (same shape, list form, types and launch)
+template <int N, bool HALF, bool ENERGY, bool UNIFORM, int PF, int MINB>
+__global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_force_mixed_batch(
+    const CpForceMember* __restrict__ tab, const int2* __restrict__ bmap, Types ty,
+    float cutforcesq)
+{
+    __shared__ float s_se[MDB_MAX_TYPES], s_s3[MDB_MAX_TYPES];
+    load_type_tables(ty, s_se, s_s3);
+    const int2 bm          = __ldg(&bmap[blockIdx.x]);
+    const CpForceMember& m = tab[bm.x];
+    force_mixed_block<N, HALF, ENERGY, UNIFORM, PF>(bm.y, m.cnt, m.xr, m.anchor, ty, cutforcesq,
+        m.list, 1, m.cs, m.numneigh, m.cf32, m.epart, s_se, s_s3);
+}
+
+int force_mixed_threads(const Types& ty)
+{
+    // blocks of ty.force_block threads (128 when a register budget is asked)
+    return (ty.force_variant & 2) ? 128 : ty.force_block;
+}
+
+int force_mixed_grid(int ncl_cap, const Types& ty)
+{
+    const int nt = force_mixed_threads(ty);
+    return (int)(((long long)ncl_cap * 32 + nt - 1) / nt);
+}
+
+template <int N, bool HALF, bool ENERGY, bool UNIFORM>
+static void run_mixed_batch(cudaStream_t s, int nblocks, const CpForceMember* tab,
+    const int2* bmap, const Types& ty, float cutforcesq)
+{
+    const int nt = force_mixed_threads(ty);
+#define CP_RUN(PF, MB)                                                                   \
+    k_force_mixed_batch<N, HALF, ENERGY, UNIFORM, PF, MB><<<nblocks, nt, 0, s>>>(tab, bmap, ty, \
+        cutforcesq)
+    switch (ty.force_variant) {
+    case 1: CP_RUN(2, 0); break;
+    case 2: CP_RUN(1, 8); break;
+    case 3: CP_RUN(2, 8); break;
+    default: CP_RUN(1, 0); break;
+    }
+#undef CP_RUN
+}
+
+template <int N, bool HALF>
+static void run_mixed_batch_e(cudaStream_t s, int energy, int nblocks,
+    const CpForceMember* tab, const int2* bmap, const Types& ty, float cutforcesq)
+{
+    if (ty.uniform) {
+        if (energy) run_mixed_batch<N, HALF, true, true>(s, nblocks, tab, bmap, ty, cutforcesq);
+        else run_mixed_batch<N, HALF, false, true>(s, nblocks, tab, bmap, ty, cutforcesq);
+    } else {
+        if (energy) run_mixed_batch<N, HALF, true, false>(s, nblocks, tab, bmap, ty, cutforcesq);
+        else run_mixed_batch<N, HALF, false, false>(s, nblocks, tab, bmap, ty, cutforcesq);
+    }
+}
+
+void launch_force_mixed_batch(cudaStream_t s, int N, int half, int energy, const Types& ty,
+    float cutforcesq, int nblocks, const CpForceMember* tab, const int2* bmap)
+{
+    if (nblocks <= 0) return;
+    if (N == 4) {
+        if (half) run_mixed_batch_e<4, true>(s, energy, nblocks, tab, bmap, ty, cutforcesq);
+        else run_mixed_batch_e<4, false>(s, energy, nblocks, tab, bmap, ty, cutforcesq);
+    } else {
+        if (half) run_mixed_batch_e<8, true>(s, energy, nblocks, tab, bmap, ty, cutforcesq);
+        else run_mixed_batch_e<8, false>(s, energy, nblocks, tab, bmap, ty, cutforcesq);
+    }
+    g_launches++;
 }
 
 template <int N, bool HALF, bool ENERGY, bool UNIFORM>
@@ -468,10 +556,9 @@ static void run_mixed(cudaStream_t s, int blocks, const int* cnt, const float4* 
     const float4* anchor, const Types& ty, float cutforcesq, const int* list, int ks, int cs,
     const int* numneigh, float4* cf32, double* epart)
 {
-    // blocks of ty.force_block threads (128 when a register budget is asked)
     const int v  = ty.force_variant;
-    const int nt = (v & 2) ? 128 : ty.force_block;
-    const int nb = (int)(((long long)blocks * CP_FORCE_THREADS + nt - 1) / nt);
+    const int nt = force_mixed_threads(ty);
+    const int nb = blocks;
 #define CP_RUN(PF, MB)                                                                   \
     k_force_mixed<N, HALF, ENERGY, UNIFORM, PF, MB><<<nb, nt, 0, s>>>(cnt, xr, anchor, ty,   \
         cutforcesq, list, ks, cs, numneigh, cf32, epart)
@@ -498,11 +585,11 @@ static void run_mixed_e(cudaStream_t s, int blocks, int energy, const int* cnt, 
     }
 }
 
-void launch_force_mixed(cudaStream_t s, int N, int half, int energy, int ncl_cap,
+int launch_force_mixed(cudaStream_t s, int N, int half, int energy, int ncl_cap,
     const int* cnt, const float4* xr, const float4* anchor, const Types& ty, float cutforcesq,
     const int* list, int ks, int cs, const int* numneigh, float4* cf32, double* epart)
 {
-    int blocks = force_blocks(ncl_cap);
+    const int blocks = force_mixed_grid(ncl_cap, ty);
     if (N == 4) {
         if (half) run_mixed_e<4, true>(s, blocks, energy, cnt, xr, anchor, ty, cutforcesq, list, ks, cs, numneigh, cf32, epart);
         else run_mixed_e<4, false>(s, blocks, energy, cnt, xr, anchor, ty, cutforcesq, list, ks, cs, numneigh, cf32, epart);
@@ -511,6 +598,7 @@ void launch_force_mixed(cudaStream_t s, int N, int half, int energy, int ncl_cap
         else run_mixed_e<8, false>(s, blocks, energy, cnt, xr, anchor, ty, cutforcesq, list, ks, cs, numneigh, cf32, epart);
     }
     g_launches++;
+    return blocks;
 }
 
 // ---- integrator: initialIntegrateCPU / finalIntegrateCPU (clusterpair/integrate.c:29-86)
@@ -524,17 +612,23 @@ __device__ __forceinline__ double3 slot_force(int s, const double4* cf, const fl
     return make_double3(f.x, f.y, f.z);
 }
 
+// zero_f: clear the force slot after its use (half lists accumulate into it;
+// only when a force evaluation follows before anything reads the forces)
 template <bool FINAL, bool INITIAL>
-__global__ void k_cp_integrate(int M, int N, const int* __restrict__ cnt, double dtf, double dt,
-    double4* cx, double4* cv, const double4* __restrict__ cf, const float4* __restrict__ cf32,
-    const float4* __restrict__ anchor, float4* xr)
+__device__ __forceinline__ void cp_integrate_slot(int s, int M, int N,
+    const int* __restrict__ cnt, double dtf, double dt, double4* cx, double4* cv,
+    const double4* __restrict__ cf, float4* cf32, const float4* __restrict__ anchor, float4* xr,
+    bool zero_f)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= cnt[CP_NCL] * M) return;
     double4 p = cx[s];
     if (slot_type(p) < 0) return;
     double4 v       = cv[s];
     const double3 f = slot_force(s, cf, cf32);
+    if (INITIAL && zero_f) {
+        if (cf32) cf32[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+        else const_cast<double4*>(cf)[s] = make_double4(0.0, 0.0, 0.0, 0.0);
+    }
     if (FINAL) {
         v.x += dtf * f.x;
         v.y += dtf * f.y;
@@ -551,6 +645,36 @@ __global__ void k_cp_integrate(int M, int N, const int* __restrict__ cnt, double
         if (xr) put_rel(xr, s, p, anchor[s / N]);
     }
     cv[s] = v;
+}
+
+template <bool FINAL, bool INITIAL>
+__global__ void k_cp_integrate(int M, int N, const int* __restrict__ cnt, double dtf, double dt,
+    double4* cx, double4* cv, const double4* __restrict__ cf, const float4* __restrict__ cf32,
+    const float4* __restrict__ anchor, float4* xr)
+{
+    cp_integrate_slot<FINAL, INITIAL>(blockIdx.x * blockDim.x + threadIdx.x, M, N, cnt, dtf, dt,
+        cx, cv, cf, const_cast<float4*>(cf32), anchor, xr, false);
+}
+
+template <bool FINAL, bool INITIAL>
+__global__ void k_cp_integrate_batch(const CpStepMember* __restrict__ tab,
+    const int2* __restrict__ bmap)
+{
+    const int2 bm         = __ldg(&bmap[blockIdx.x]);
+    const CpStepMember& m = tab[bm.x];
+    cp_integrate_slot<FINAL, INITIAL>(bm.y * blockDim.x + threadIdx.x, m.M, m.N, m.cnt, m.dtf,
+        m.dt, m.cx, m.cv, m.cf, m.cf32, m.anchor, m.xr, m.zero_f != 0);
+}
+
+void launch_cp_integrate_batch(cudaStream_t s, bool final_, bool initial, int nblocks,
+    const CpStepMember* tab, const int2* bmap)
+{
+    if (nblocks <= 0) return;
+    if (final_ && initial)
+        k_cp_integrate_batch<true, true><<<nblocks, MDB_NTHREADS, 0, s>>>(tab, bmap);
+    else if (initial) k_cp_integrate_batch<false, true><<<nblocks, MDB_NTHREADS, 0, s>>>(tab, bmap);
+    else k_cp_integrate_batch<true, false><<<nblocks, MDB_NTHREADS, 0, s>>>(tab, bmap);
+    g_launches++;
 }
 
 void launch_cp_initial(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt, double dtf,

@@ -149,9 +149,13 @@ int force_blocks(int ncl_cap);
 void launch_force_fp64(cudaStream_t s, int M, int N, int half, int energy, int ncl_cap,
     const int* cnt, const double4* cx, const Types& ty, double cutforcesq, const int* list,
     int ks, int cs, const int* numneigh, double4* cf, double* epart);
-void launch_force_mixed(cudaStream_t s, int N, int half, int energy, int ncl_cap,
+// returns the number of blocks launched (= energy partials written)
+int launch_force_mixed(cudaStream_t s, int N, int half, int energy, int ncl_cap,
     const int* cnt, const float4* xr, const float4* anchor, const Types& ty, float cutforcesq,
     const int* list, int ks, int cs, const int* numneigh, float4* cf32, double* epart);
+// threads per block and block count of a mixed force launch
+int force_mixed_threads(const Types& ty);
+int force_mixed_grid(int ncl_cap, const Types& ty);
 void launch_cp_initial(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt, double dtf,
     double dt, double4* cx, double4* cv, const double4* cf, const float4* cf32,
     const float4* anchor, float4* xr);
@@ -161,6 +165,43 @@ void launch_cp_final_initial(cudaStream_t s, int M, int N, int ncl_cap, const in
     double dtf, double dt, double4* cx, double4* cv, const double4* cf, const float4* cf32,
     const float4* anchor, float4* xr);
 int ke_blocks(int n);
+
+// ---- batched launches over the members of an ensemble -----------------------
+// One launch covers every member: block b of the launch runs block bmap[b].y
+// of member bmap[b].x, whose buffers come from a device table. The block maps
+// are built on the host from the members' capacities, so a captured graph
+// stays valid until a member's buffers move.
+struct CpStepMember { // integrator and ghost update
+    const int* cnt;
+    double4* cx;
+    double4* cv;
+    const double4* cf;
+    float4* cf32;
+    const float4* anchor;
+    float4* xr;
+    const int* border;
+    const int* pbc;
+    const int* jnat;
+    double dtf, dt, xprd, yprd, zprd;
+    int M, N, mixed;
+    int zero_f; // half lists: the initial integration clears the forces it used
+};
+struct CpForceMember { // mixed force kernel (row-major lists)
+    const int* cnt;
+    const float4* xr;
+    const float4* anchor;
+    const int* list;
+    const int* numneigh;
+    float4* cf32;
+    double* epart;
+    int cs, pad;
+};
+void launch_cp_integrate_batch(cudaStream_t s, bool final_, bool initial, int nblocks,
+    const CpStepMember* tab, const int2* bmap);
+void launch_ghost_update_batch(cudaStream_t s, int nblocks, const CpStepMember* tab,
+    const int2* bmap);
+void launch_force_mixed_batch(cudaStream_t s, int N, int half, int energy, const Types& ty,
+    float cutforcesq, int nblocks, const CpForceMember* tab, const int2* bmap);
 void launch_ke_atoms(cudaStream_t s, int n, const double4* av, double mass, double* partials);
 void launch_ke_slots(cudaStream_t s, int M, int ncl_cap, const int* cnt, const double4* cx,
     const double4* cv, double mass, double* partials);

@@ -96,7 +96,7 @@ CP_EXPORTS = [
     "mdb_cp_get_jclusters", "mdb_cp_get_ghosts", "mdb_cp_get_neighbor_list",
     "mdb_cp_get_columns", "mdb_cp_get_geometry", "mdb_cp_time_force", "mdb_cp_ensemble_create",
     "mdb_cp_ensemble_destroy", "mdb_cp_ensemble_last_error", "mdb_cp_ensemble_stream",
-    "mdb_cp_ensemble_launch_count", "mdb_cp_ensemble_run",
+    "mdb_cp_ensemble_launch_count", "mdb_cp_ensemble_run", "mdb_cp_ensemble_tune",
 ]
 # every symbol include/mdb_host.h declares
 HOST_EXPORTS = [
@@ -171,6 +171,7 @@ def load():
         "mdb_cp_ensemble_stream": ([vp], vp),
         "mdb_cp_ensemble_launch_count": ([vp], C.c_longlong),
         "mdb_cp_ensemble_run": ([vp, ip, ip, C.POINTER(MdbThermo), ip, C.POINTER(ip)], ip),
+        "mdb_cp_ensemble_tune": ([vp, C.c_char_p, ip], ip),
     })
     for name in ("mdb_cp_synchronize", "mdb_cp_build_clusters", "mdb_cp_define_jclusters",
                  "mdb_cp_setup_pbc",
@@ -747,7 +748,7 @@ class Ensemble:
     """Independent cluster-pair systems advanced together, one CUDA graph launch
     per timestep for all of them (an ``MdbCpEnsemble``). Members must be set up."""
 
-    def __init__(self, members):
+    def __init__(self, members, batched=None):
         self.lib = load()
         self.members = list(members)
         arr = (C.c_void_p * len(self.members))(*[m.h.value for m in self.members])
@@ -757,6 +758,14 @@ class Ensemble:
             raise MdbError(f"mdb_cp_ensemble_create failed: "
                            f"{self.lib.mdb_status_string(rc).decode()}")
         self.h = h
+        if batched is not None:
+            self.tune("batched", int(batched))
+
+    def tune(self, key, value):
+        rc = self.lib.mdb_cp_ensemble_tune(self.h, key.encode(), int(value))
+        if rc:
+            msg = self.lib.mdb_cp_ensemble_last_error(self.h)
+            raise MdbError(f"mdb_cp_ensemble_tune: {msg.decode() if msg else rc}")
 
     def close(self):
         if getattr(self, "h", None):

@@ -372,13 +372,19 @@ def test_c5_full_scale_128():
 
 # ---- ensembles of independent replicas (one graph launch per timestep)
 
-def replica(n, rho, temp, N, precision):
-    hp = mdb.host_params(nx=n, ny=n, nz=n, rho=rho, temp=temp, nstat=10)
+def replica(n, rho, temp, N, precision, half=0, types=None):
+    extra = {}
+    if types is not None:
+        import workloads as W
+        extra = dict(types=types, cutforce=W.c5_cutoff(types[1]))
+    hp = mdb.host_params(nx=n, ny=n, nz=n, rho=rho, temp=temp, nstat=10, **extra)
     x, v, t = mdb.create_fcc(hp)
     kw = dict(xprd=hp.xprd, yprd=hp.yprd, zprd=hp.zprd, cutforce=hp.cutforce,
               cutneigh=hp.cutneigh, dt=hp.dt, dtforce=hp.dtforce, mass=hp.mass,
               reneigh_every=hp.reneigh_every, nstat=hp.nstat, natoms=len(t), cluster_n=N,
-              precision=precision, ntypes=hp.ntypes)
+              precision=precision, ntypes=hp.ntypes, half_neigh=half)
+    if types is not None:
+        kw.update(epsilon_per_type=list(types[0]), sigma_per_type=list(types[1]))
     out = []
     for _ in range(2):
         s = mdb.ClusterSystem(**kw)
@@ -388,14 +394,17 @@ def replica(n, rho, temp, N, precision):
     return out
 
 
-@pytest.mark.parametrize("N,precision", [(4, "fp64"), (8, "fp64"), (4, "mixed")])
-def test_ensemble_matches_members(N, precision):
+@pytest.mark.parametrize("N,precision,batched", [(4, "fp64", None), (8, "fp64", None),
+                                                 (4, "mixed", 1), (8, "mixed", 1),
+                                                 (4, "mixed", 0)])
+def test_ensemble_matches_members(N, precision, batched):
     """Replicas of uneven size, density and temperature advanced as one
     ensemble follow, bit for bit, the trajectories and thermo samples of the
-    same replicas run one at a time (full lists: no atomics)."""
+    same replicas run one at a time (full lists: no atomics), with batched
+    launches over all members and with one graph branch per member."""
     specs = [(4, 0.80, 0.9), (5, 0.9, 1.8), (7, 0.76, 1.2), (3, 0.94, 0.7)]
     pairs = [replica(n, rho, T, N, precision) for n, rho, T in specs]
-    ens = mdb.Ensemble([p[0] for p in pairs])
+    ens = mdb.Ensemble([p[0] for p in pairs], batched=batched)
     got = ens.run(45, max_samples=8)
     got2 = ens.run(17, first_step=45, max_samples=8)
     assert ens.launches > 0
@@ -426,3 +435,31 @@ def test_ensemble_rejects_mismatched_members():
     b.setup()
     with pytest.raises(mdb.MdbError):
         mdb.Ensemble([a, b])  # different rebuild period
+
+
+def test_ensemble_batched_groups_half_lists():
+    """One batched ensemble holding four force groups (4x4 / 4x8, full / half,
+    one type / four types): full-list members stay bit-identical to their solo
+    twins; half-list members (atomic reactions) agree to rounding."""
+    import workloads as W
+    types = W.c5_types()
+    cfg = [(4, 0.84, 1.44, 4, 0, None), (5, 0.80, 1.0, 8, 0, None),
+           (4, 0.90, 1.6, 4, 1, None), (5, 0.84, 1.2, 8, 1, types),
+           (6, 0.76, 0.8, 4, 1, types)]
+    pairs = [replica(n, rho, T, N, "mixed", half, ty) for n, rho, T, N, half, ty in cfg]
+    ens = mdb.Ensemble([p[0] for p in pairs])
+    got = ens.run(45, max_samples=8)
+    for k, ((a, b), c) in enumerate(zip(pairs, cfg)):
+        want = b.run(45, max_samples=8)
+        xa, va, _ = a.atoms()
+        xb, vb, _ = b.atoms()
+        if c[4] == 0:
+            assert got[k] == want, k
+            assert np.array_equal(xa, xb) and np.array_equal(va, vb), k
+        else:
+            assert len(got[k]) == len(want) == 4
+            for u, w in zip(got[k], want):
+                for key in ("T", "E", "P"):
+                    assert abs(u[key] - w[key]) <= 1e-4 * max(abs(w[key]), 1.0), (k, key)
+            assert np.abs(xa - xb).max() < 1e-3, k
+    ens.close()
