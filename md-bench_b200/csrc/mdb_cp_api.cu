@@ -1305,13 +1305,27 @@ struct MdbCpEnsemble {
     size_t bmap_cap        = 0;
     int nb_integ = 0, nb_ghost = 0;
     size_t off_integ = 0, off_ghost = 0;
+    // batched rebuild: member table, block map per stage, counters of all members
+    CpBuildMember* d_build = nullptr;
+    int nb_stage[CB_COUNT]     = {};
+    size_t off_stage[CB_COUNT] = {};
+    int* d_cnt_all = nullptr;
+    int* h_cnt_all = nullptr;
     struct Group { // members sharing cluster shape, list form, types and launch shape
         int N, half;
         Types ty;
         float cutsq;
         int nblocks;
-        size_t off;
+        size_t off, off_dyn;
     };
+    // block maps of the integrator, the ghost update and the force groups that
+    // cover only the members' current clusters (the rest of each region is
+    // unused entries); refreshed from the counters after every rebuild.
+    // Energy evaluations use the capacity maps, so that every energy partial
+    // of a member is written.
+    size_t off_integ_dyn = 0, off_ghost_dyn = 0, dyn_begin = 0, dyn_end = 0;
+    int2* h_dyn = nullptr;
+    std::vector<int> gid;
     std::vector<Group> groups;
 };
 
@@ -1398,6 +1412,44 @@ static bool same_types(const Types& a, const Types& b)
     return true;
 }
 
+// the dynamic block maps from the members' counters as the last build left
+// them (host copies in h_cnt); stream-ordered before the next graph launch
+static int ens_dyn_maps(MdbCpEnsemble* e)
+{
+    if (!e->batched || !e->tables_ok) return MDB_OK;
+    int2* h  = e->h_dyn;
+    size_t w = e->dyn_begin;
+    const int n = (int)e->m.size();
+    auto fill = [&](size_t cap, auto blocks_of) {
+        const size_t end = w + cap;
+        for (int k = 0; k < n; k++) {
+            const int nb = blocks_of(e->m[k]);
+            for (int b = 0; b < nb && w < end; b++) h[w++] = make_int2(k, b);
+        }
+        while (w < end) h[w++] = make_int2(-1, 0);
+    };
+    fill(e->nb_integ, [](const MdbCp* c) {
+        return mdb_blocks((long long)c->h_cnt[CP_NCL] * c->M, MDB_NTHREADS);
+    });
+    fill(e->nb_ghost, [](const MdbCp* c) {
+        return mdb_blocks((long long)c->h_cnt[CP_NGC] * c->N, MDB_NTHREADS);
+    });
+    for (size_t q = 0; q < e->groups.size(); q++) {
+        const size_t end = w + e->groups[q].nblocks;
+        for (int k = 0; k < n; k++) {
+            if (e->gid[k] != (int)q) continue;
+            const MdbCp* c = e->m[k];
+            const int nb   = force_mixed_grid(c->h_cnt[CP_NCL], c->ty);
+            for (int b = 0; b < nb && w < end; b++) h[w++] = make_int2(k, b);
+        }
+        while (w < end) h[w++] = make_int2(-1, 0);
+    }
+    cudaError_t ce = cudaMemcpyAsync(e->d_bmap + e->dyn_begin, h + e->dyn_begin,
+        sizeof(int2) * (e->dyn_end - e->dyn_begin), cudaMemcpyHostToDevice, e->s);
+    if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "ensemble block maps", ce);
+    return MDB_OK;
+}
+
 // member tables and block maps of the batched launches, from the members'
 // current buffers and capacities
 static int ens_tables(MdbCpEnsemble* e)
@@ -1405,7 +1457,7 @@ static int ens_tables(MdbCpEnsemble* e)
     if (e->tables_ok) return MDB_OK;
     // graphs launched earlier may still read the old tables
     cudaError_t ce = cudaStreamSynchronize(e->s);
-    if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "ensemble tables", ce);
+    if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "ensemble tables (sync)", ce);
     const int n = (int)e->m.size();
     std::vector<CpStepMember> st(n);
     std::vector<CpForceMember> fo(n);
@@ -1425,6 +1477,35 @@ static int ens_tables(MdbCpEnsemble* e)
         f.cnt = c->cnt, f.xr = c->xr, f.anchor = c->anchor, f.list = c->list;
         f.numneigh = c->numneigh, f.cf32 = c->cf32, f.epart = c->partials, f.cs = lcs(c);
         f.pad = 0;
+    }
+    std::vector<CpBuildMember> bt(n);
+    for (int k = 0; k < n; k++) {
+        const MdbCp* c   = e->m[k];
+        CpBuildMember& b = bt[k];
+        b.g = c->g, b.M = c->M, b.N = c->N, b.jfac = c->jfac, b.mixed = c->mixed;
+        b.half = c->p.half_neigh, b.nlocal = c->nlocal, b.ncl_cap = c->ncl_cap;
+        b.ncj_cap = c->ncj_cap, b.ngc_cap = c->ngc_cap, b.maxneighs = c->maxneighs;
+        b.ks = lks(c), b.cs = lcs(c), b.cnt = c->cnt, b.zext = c->zext;
+        b.ax = c->ax, b.av = c->av, b.cx = c->cx, b.cv = c->cv, b.cl_first = c->cl_first;
+        b.atom_col = c->atom_col, b.col_count = c->col_count, b.col_start = c->col_start;
+        b.col_fill = c->col_fill, b.col_atoms = c->col_atoms, b.col_sorted = c->col_sorted;
+        b.gidx = c->gidx, b.gz = c->gz, b.ncl_col = c->ncl_col, b.cl_start = c->cl_start;
+        b.inat = c->inat, b.cbin = c->cbin, b.ibbmin = c->ibbmin, b.ibbmax = c->ibbmax;
+        b.jnat = c->jnat, b.jbbmin = c->jbbmin, b.jbbmax = c->jbbmax, b.anchor = c->anchor;
+        b.xr = c->xr, b.gcount = c->gcount, b.gstart = c->gstart, b.border = c->border;
+        b.pbc = c->pbc, b.gcolumn = c->gcolumn, b.gcol_count = c->gcol_count;
+        b.jcol_n = c->jcol_n, b.jcol_start = c->jcol_start, b.gfill = c->gfill;
+        b.gtmp = c->gtmp, b.jcol = c->jcol, b.jcbbmin = c->jcbbmin, b.jcbbmax = c->jcbbmax;
+        b.stencil = c->stencil_d, b.list = c->list, b.numneigh = c->numneigh;
+        b.nmasked = c->nmasked;
+    }
+    for (int st = 0; st < CB_COUNT; st++) {
+        e->off_stage[st] = maps.size();
+        for (int k = 0; k < n; k++) {
+            int threads;
+            add(k, cp_build_stage_blocks(st, bt[k], &threads));
+        }
+        e->nb_stage[st] = (int)(maps.size() - e->off_stage[st]);
     }
     e->off_integ = maps.size();
     for (int k = 0; k < n; k++)
@@ -1462,43 +1543,69 @@ static int ens_tables(MdbCpEnsemble* e)
             }
         gr.nblocks = (int)(maps.size() - gr.off);
     }
+    e->gid = gid;
+    // dynamic regions, same sizes (contents written by ens_dyn_maps)
+    e->dyn_begin     = maps.size();
+    e->off_integ_dyn = maps.size();
+    maps.resize(maps.size() + e->nb_integ, make_int2(-1, 0));
+    e->off_ghost_dyn = maps.size();
+    maps.resize(maps.size() + e->nb_ghost, make_int2(-1, 0));
+    for (auto& gr : e->groups) {
+        gr.off_dyn = maps.size();
+        maps.resize(maps.size() + gr.nblocks, make_int2(-1, 0));
+    }
+    e->dyn_end = maps.size();
     if (!e->d_step) {
         ce = cudaMalloc((void**)&e->d_step, sizeof(CpStepMember) * n);
         if (ce == cudaSuccess) ce = cudaMalloc((void**)&e->d_force, sizeof(CpForceMember) * n);
+        if (ce == cudaSuccess) ce = cudaMalloc((void**)&e->d_build, sizeof(CpBuildMember) * n);
+        if (ce == cudaSuccess) ce = cudaMalloc((void**)&e->d_cnt_all, sizeof(int) * CP_SLOTS * n);
+        if (ce == cudaSuccess)
+            ce = cudaMallocHost((void**)&e->h_cnt_all, sizeof(int) * CP_SLOTS * n);
         if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_NOMEM, "ensemble tables", ce);
     }
     if (maps.size() > e->bmap_cap) {
         if (e->d_bmap) cudaFree(e->d_bmap);
+        if (e->h_dyn) cudaFreeHost(e->h_dyn);
         e->d_bmap   = nullptr;
+        e->h_dyn    = nullptr;
         e->bmap_cap = maps.size() + maps.size() / 4;
         ce          = cudaMalloc((void**)&e->d_bmap, sizeof(int2) * e->bmap_cap);
+        if (ce == cudaSuccess) ce = cudaMallocHost((void**)&e->h_dyn, sizeof(int2) * e->bmap_cap);
         if (ce != cudaSuccess) {
             e->bmap_cap = 0;
             return ens_fail(e, MDB_ERR_NOMEM, "ensemble block maps", ce);
         }
     }
+    const char* what = "member table";
     ce = cudaMemcpy(e->d_step, st.data(), sizeof(CpStepMember) * n, cudaMemcpyHostToDevice);
     if (ce == cudaSuccess)
         ce = cudaMemcpy(e->d_force, fo.data(), sizeof(CpForceMember) * n, cudaMemcpyHostToDevice);
-    if (ce == cudaSuccess && !maps.empty())
-        ce = cudaMemcpy(e->d_bmap, maps.data(), sizeof(int2) * maps.size(),
+    if (ce == cudaSuccess) {
+        what = "rebuild table";
+        ce = cudaMemcpy(e->d_build, bt.data(), sizeof(CpBuildMember) * n, cudaMemcpyHostToDevice);
+    }
+    if (ce == cudaSuccess && !maps.empty()) {
+        what = "block maps";
+        ce   = cudaMemcpy(e->d_bmap, maps.data(), sizeof(int2) * maps.size(),
             cudaMemcpyHostToDevice);
-    if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "ensemble tables", ce);
+    }
+    if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, what, ce);
     e->tables_ok = true;
-    return MDB_OK;
+    return ens_dyn_maps(e);
 }
 
 static void ens_integ(MdbCpEnsemble* e, bool final_, bool initial)
 {
     launch_cp_integrate_batch(e->s, final_, initial, e->nb_integ, e->d_step,
-        e->d_bmap + e->off_integ);
+        e->d_bmap + e->off_integ_dyn);
 }
 
 static void ens_forces(MdbCpEnsemble* e, bool energy)
 {
     for (const auto& gr : e->groups)
         launch_force_mixed_batch(e->s, gr.N, gr.half, energy, gr.ty, gr.cutsq, gr.nblocks,
-            e->d_force, e->d_bmap + gr.off);
+            e->d_force, e->d_bmap + (energy ? gr.off : gr.off_dyn));
 }
 
 // per-member work on the members' streams, forked from and joined to e->s
@@ -1523,19 +1630,41 @@ static void ens_body_batched(MdbCpEnsemble* e, int kind)
     case EG_FRONT_FI:
     case EG_FRONT_I:
         ens_integ(e, fi, true);
-        launch_ghost_update_batch(e->s, e->nb_ghost, e->d_step, e->d_bmap + e->off_ghost);
+        launch_ghost_update_batch(e->s, e->nb_ghost, e->d_step, e->d_bmap + e->off_ghost_dyn);
         if (kind == EG_PLAIN_FI || kind == EG_PLAIN_I) ens_forces(e, false);
         break;
     case EG_REB_FI:
-    case EG_REB_I:
+    case EG_REB_I: {
+        // updateAtoms + the whole rebuild of every member, stage by stage
         ens_integ(e, fi, true);
-        ens_fork(e, [](MdbCp* c) {
-            enq_gather(c, 1);
-            enq_build(c);
-            cudaMemcpyAsync(c->h_cnt, c->cnt, CP_SLOTS * sizeof(int), cudaMemcpyDeviceToHost,
-                c->s);
-        });
+        const int n = (int)e->m.size();
+        auto stage  = [e](int st) {
+            launch_build_stage_batch(e->s, st, e->nb_stage[st], e->d_build,
+                e->d_bmap + e->off_stage[st]);
+        };
+        stage(CB_RESET);
+        stage(CB_GATHER);
+        stage(CB_BIN);
+        launch_scan_batch(e->s, 0, n, e->d_build);
+        stage(CB_SCATTER);
+        stage(CB_SORT);
+        launch_scan_batch(e->s, 1, n, e->d_build);
+        stage(CB_CLUSTERS);
+        stage(CB_GCOUNT);
+        launch_scan_batch(e->s, 2, n, e->d_build);
+        stage(CB_GWRITE);
+        stage(CB_GFIRST);
+        stage(CB_GCOLS);
+        stage(CB_CSIZES);
+        launch_scan_batch(e->s, 3, n, e->d_build);
+        stage(CB_GSCATTER);
+        stage(CB_MERGE);
+        stage(CB_LIST);
+        launch_counters_batch(e->s, n, e->d_build, e->d_cnt_all);
+        cudaMemcpyAsync(e->h_cnt_all, e->d_cnt_all, sizeof(int) * CP_SLOTS * n,
+            cudaMemcpyDeviceToHost, e->s);
         break;
+    }
     case EG_FORCE: ens_forces(e, false); break;
     case EG_SAMPLE:
         ens_forces(e, true);
@@ -1634,6 +1763,10 @@ extern "C" int mdb_cp_ensemble_destroy(MdbCpEnsemble* e)
     if (e->d_step) cudaFree(e->d_step);
     if (e->d_force) cudaFree(e->d_force);
     if (e->d_bmap) cudaFree(e->d_bmap);
+    if (e->d_build) cudaFree(e->d_build);
+    if (e->d_cnt_all) cudaFree(e->d_cnt_all);
+    if (e->h_cnt_all) cudaFreeHost(e->h_cnt_all);
+    if (e->h_dyn) cudaFreeHost(e->h_dyn);
     if (e->s) cudaStreamDestroy(e->s);
     delete e;
     return MDB_OK;
@@ -1673,7 +1806,10 @@ static int ens_rebuild(MdbCpEnsemble* e, bool pending_final)
     if (rc) return rc;
     cudaError_t ce = cudaStreamSynchronize(e->s);
     if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "ensemble rebuild", ce);
-    for (MdbCp* c : e->m) {
+    for (size_t k = 0; k < e->m.size(); k++) {
+        MdbCp* c = e->m[k];
+        if (e->batched)
+            memcpy(c->h_cnt, e->h_cnt_all + k * CP_SLOTS, sizeof(int) * CP_SLOTS);
         int r = eval_build(c, CHK_ALL);
         if (r < 0) return ens_fail(e, -r, c->err.c_str());
         if (r > 0) {
@@ -1683,7 +1819,7 @@ static int ens_rebuild(MdbCpEnsemble* e, bool pending_final)
         }
         c->have_clusters = c->have_ghosts = c->have_list = true;
     }
-    return MDB_OK;
+    return ens_dyn_maps(e);
 }
 
 extern "C" int mdb_cp_ensemble_run(MdbCpEnsemble* e, int first_step, int nsteps,
@@ -1694,9 +1830,14 @@ extern "C" int mdb_cp_ensemble_run(MdbCpEnsemble* e, int first_step, int nsteps,
     const int n = (int)e->m.size();
     MdbCp* c0   = e->m[0];
     if (nsamples) *nsamples = 0;
+    for (MdbCp* c : e->m)
+        if (!c->have_list) return ens_fail(e, MDB_ERR_STATE, "a member is not set up");
     // members' own streams may still hold work: order the ensemble after it
     for (MdbCp* c : e->m) cudaStreamSynchronize(c->s);
+    cudaStreamSynchronize(e->s);
     int nslot = 0, rc;
+    // members may have been rebuilt on their own since the last run
+    if ((rc = ens_dyn_maps(e))) return rc;
     const int last     = first_step + nsteps - 1;
     bool pending_final = false;
     for (int step = first_step; step <= last; step++) {

@@ -16,11 +16,12 @@ static __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 // ---- updateSingleAtoms + updateAtomsPbc --------------------------------------
 // clusterpair/neighbor.c:2096-2149 (slot -> atom index = atoms of the clusters
 // before it) and clusterpair/pbc.c:116-143 (wrap into the box)
-__global__ void k_gather(int M, const int* __restrict__ cnt, const double4* __restrict__ cx,
+__device__ __forceinline__ void gather_blk(int bid, int M, const int* __restrict__ cnt,
+    const double4* __restrict__ cx,
     const double4* __restrict__ cv, const int* __restrict__ cl_first, double4* __restrict__ ax,
     double4* __restrict__ av, int wrap, double xprd, double yprd, double zprd)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = bid * blockDim.x + threadIdx.x;
     if (s >= cnt[CP_NCL] * M) return;
     double4 p = cx[s];
     if (slot_type(p) < 0) return;
@@ -37,6 +38,13 @@ __global__ void k_gather(int M, const int* __restrict__ cnt, const double4* __re
     av[a] = cv[s];
 }
 
+__global__ void k_gather(int M, const int* __restrict__ cnt, const double4* __restrict__ cx,
+    const double4* __restrict__ cv, const int* __restrict__ cl_first, double4* __restrict__ ax,
+    double4* __restrict__ av, int wrap, double xprd, double yprd, double zprd)
+{
+    gather_blk(blockIdx.x, M, cnt, cx, cv, cl_first, ax, av, wrap, xprd, yprd, zprd);
+}
+
 void launch_gather(cudaStream_t s, int M, int ncl_cap, const int* cnt, const double4* cx,
     const double4* cv, const int* cl_first, double4* ax, double4* av, int wrap, double xprd,
     double yprd, double zprd)
@@ -48,10 +56,11 @@ void launch_gather(cudaStream_t s, int M, int ncl_cap, const int* cnt, const dou
 }
 
 // ---- binAtoms (clusterpair/neighbor.c:1409-1449) -----------------------------
-__global__ void k_bin_atoms(int n, const double4* __restrict__ ax, Geom g, int* atom_col,
+__device__ __forceinline__ void bin_atoms_blk(int bid, int n, const double4* __restrict__ ax,
+    Geom g, int* atom_col,
     int* col_count, int* cnt)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = bid * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double4 p = ax[i];
     int ix, iy;
@@ -66,6 +75,12 @@ __global__ void k_bin_atoms(int n, const double4* __restrict__ ax, Geom g, int* 
     atomicAdd(&col_count[b], 1);
 }
 
+__global__ void k_bin_atoms(int n, const double4* __restrict__ ax, Geom g, int* atom_col,
+    int* col_count, int* cnt)
+{
+    bin_atoms_blk(blockIdx.x, n, ax, g, atom_col, col_count, cnt);
+}
+
 void launch_bin_atoms(cudaStream_t s, int n, const double4* ax, const Geom& g, int* atom_col,
     int* col_count, int* cnt)
 {
@@ -75,14 +90,20 @@ void launch_bin_atoms(cudaStream_t s, int n, const double4* ax, const Geom& g, i
     g_launches++;
 }
 
-__global__ void k_scatter_atoms(int n, const int* __restrict__ atom_col,
+__device__ __forceinline__ void scatter_atoms_blk(int bid, int n, const int* __restrict__ atom_col,
     const int* __restrict__ col_start, int* col_fill, int* col_atoms)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = bid * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int b = atom_col[i];
     if (b < 0) return;
     col_atoms[col_start[b] + atomicAdd(&col_fill[b], 1)] = i;
+}
+
+__global__ void k_scatter_atoms(int n, const int* __restrict__ atom_col,
+    const int* __restrict__ col_start, int* col_fill, int* col_atoms)
+{
+    scatter_atoms_blk(blockIdx.x, n, atom_col, col_start, col_fill, col_atoms);
 }
 
 void launch_scatter_atoms(cudaStream_t s, int n, const int* atom_col, const int* col_start,
@@ -176,14 +197,14 @@ __device__ void sort_column(int* idx, double* z, int c, int P, const double4* __
 
 #define CP_SORT_WARPS 4
 
-__global__ void __launch_bounds__(32 * CP_SORT_WARPS) k_sort_columns(int mbins, int M, int N,
+__device__ __forceinline__ void sort_columns_blk(int bid, int mbins, int M, int N,
     const int* __restrict__ col_start, int* col_atoms, const double4* __restrict__ ax,
     int* col_sorted, int* gidx, double* gz, int* ncl_col)
 {
     __shared__ int s_idx[CP_SORT_WARPS][CP_COL_SMEM];
     __shared__ double s_z[CP_SORT_WARPS][CP_COL_SMEM];
     const int w    = threadIdx.x >> 5;
-    const int b    = blockIdx.x * CP_SORT_WARPS + w;
+    const int b    = bid * CP_SORT_WARPS + w;
     const int lane = lane_id();
     if (b >= mbins) return;
     const int start = col_start[b];
@@ -211,6 +232,14 @@ __global__ void __launch_bounds__(32 * CP_SORT_WARPS) k_sort_columns(int mbins, 
         if (N > M && (nc & 1)) nc++;
         ncl_col[b] = nc;
     }
+}
+
+__global__ void __launch_bounds__(32 * CP_SORT_WARPS) k_sort_columns(int mbins, int M, int N,
+    const int* __restrict__ col_start, int* col_atoms, const double4* __restrict__ ax,
+    int* col_sorted, int* gidx, double* gz, int* ncl_col)
+{
+    sort_columns_blk(blockIdx.x, mbins, M, N, col_start, col_atoms, ax, col_sorted, gidx, gz,
+        ncl_col);
 }
 
 void launch_sort_columns(cudaStream_t s, const Geom& g, int M, int N, const int* col_start,
@@ -252,14 +281,15 @@ __device__ __forceinline__ void zext_max(unsigned long long* zext, double e)
 }
 
 template <int M, int N>
-__global__ void k_build_clusters(int mbins, int mixed, const int* __restrict__ col_start,
+__device__ __forceinline__ void build_clusters_blk(int bid, int mbins, int mixed,
+    const int* __restrict__ col_start,
     const int* __restrict__ col_sorted, const int* __restrict__ cl_start,
     const double4* __restrict__ ax, const double4* __restrict__ av, double4* cx, double4* cv,
     int* inat, int* cbin, int* cl_first, double4* ibbmin, double4* ibbmax, int* jnat,
     double4* jbbmin, double4* jbbmax, float4* anchor, float4* xr, int* cnt,
     unsigned long long* zext)
 {
-    const int b    = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int b    = (bid * blockDim.x + threadIdx.x) >> 5;
     const int lane = lane_id();
     if (b == 0 && lane == 0) {
         cnt[CP_NCL] = cl_start[mbins];
@@ -344,6 +374,18 @@ __global__ void k_build_clusters(int mbins, int mixed, const int* __restrict__ c
     }
 }
 
+template <int M, int N>
+__global__ void k_build_clusters(int mbins, int mixed, const int* __restrict__ col_start,
+    const int* __restrict__ col_sorted, const int* __restrict__ cl_start,
+    const double4* __restrict__ ax, const double4* __restrict__ av, double4* cx, double4* cv,
+    int* inat, int* cbin, int* cl_first, double4* ibbmin, double4* ibbmax, int* jnat,
+    double4* jbbmin, double4* jbbmax, float4* anchor, float4* xr, int* cnt,
+    unsigned long long* zext)
+{
+    build_clusters_blk<M, N>(blockIdx.x, mbins, mixed, col_start, col_sorted, cl_start, ax, av,
+        cx, cv, inat, cbin, cl_first, ibbmin, ibbmax, jnat, jbbmin, jbbmax, anchor, xr, cnt, zext);
+}
+
 void launch_build_clusters(cudaStream_t s, const Geom& g, int M, int N, int mixed,
     const int* col_start, const int* col_sorted, const int* cl_start, const double4* ax,
     const double4* av, double4* cx, double4* cv, int* inat, int* cbin, int* cl_first,
@@ -409,15 +451,22 @@ __device__ __forceinline__ int ghost_images(const double4& mn, const double4& mx
     return n;
 }
 
-__global__ void k_ghost_count(int ncj_cap, const int* __restrict__ cnt,
+__device__ __forceinline__ void ghost_count_blk(int bid, int ncj_cap, const int* __restrict__ cnt,
     const int* __restrict__ jnat, const double4* __restrict__ jbbmin,
     const double4* __restrict__ jbbmax, Geom g, int* gcount)
 {
-    const int cj = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cj = bid * blockDim.x + threadIdx.x;
     if (cj >= ncj_cap) return;
     int n = 0;
     if (cj < cnt[CP_NCJ] && jnat[cj] > 0) n = ghost_images(jbbmin[cj], jbbmax[cj], g, nullptr);
     gcount[cj] = n;
+}
+
+__global__ void k_ghost_count(int ncj_cap, const int* __restrict__ cnt,
+    const int* __restrict__ jnat, const double4* __restrict__ jbbmin,
+    const double4* __restrict__ jbbmax, Geom g, int* gcount)
+{
+    ghost_count_blk(blockIdx.x, ncj_cap, cnt, jnat, jbbmin, jbbmax, g, gcount);
 }
 
 void launch_ghost_count(cudaStream_t s, int ncj_cap, const int* cnt, const int* jnat,
@@ -428,11 +477,12 @@ void launch_ghost_count(cudaStream_t s, int ncj_cap, const int* cnt, const int* 
     g_launches++;
 }
 
-__global__ void k_ghost_write(int ncj_cap, int ngc_cap, int* cnt, const int* __restrict__ jnat,
+__device__ __forceinline__ void ghost_write_blk(int bid, int ncj_cap, int ngc_cap, int* cnt,
+    const int* __restrict__ jnat,
     const double4* __restrict__ jbbmin, const double4* __restrict__ jbbmax, Geom g,
     const int* __restrict__ gstart, int* border, int* pbc)
 {
-    const int cj = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cj = bid * blockDim.x + threadIdx.x;
     if (cj == 0) {
         int total          = gstart[ncj_cap];
         cnt[CP_NGC_TOTAL]  = total;
@@ -449,6 +499,14 @@ __global__ void k_ghost_write(int ncj_cap, int ngc_cap, int* cnt, const int* __r
     }
 }
 
+__global__ void k_ghost_write(int ncj_cap, int ngc_cap, int* cnt, const int* __restrict__ jnat,
+    const double4* __restrict__ jbbmin, const double4* __restrict__ jbbmax, Geom g,
+    const int* __restrict__ gstart, int* border, int* pbc)
+{
+    ghost_write_blk(blockIdx.x, ncj_cap, ngc_cap, cnt, jnat, jbbmin, jbbmax, g, gstart, border,
+        pbc);
+}
+
 void launch_ghost_write(cudaStream_t s, int ncj_cap, int ngc_cap, int* cnt, const int* jnat,
     const double4* jbbmin, const double4* jbbmax, const Geom& g, const int* gstart, int* border,
     int* pbc)
@@ -460,11 +518,12 @@ void launch_ghost_write(cudaStream_t s, int ncj_cap, int ngc_cap, int* cnt, cons
 
 // updatePbcCPU(first = 1), clusterpair/pbc.c:43-113: ghost positions, padding,
 // boxes; one thread per ghost j-cluster, plus one for the dummy cluster
-__global__ void k_ghost_first(int N, int* cnt, const int* __restrict__ border,
+__device__ __forceinline__ void ghost_first_blk(int bid, int N, int* cnt,
+    const int* __restrict__ border,
     const int* __restrict__ pbc, int mixed, Geom g, double4* cx, int* jnat, double4* jbbmin,
     double4* jbbmax, float4* anchor, float4* xr, unsigned long long* zext)
 {
-    const int gi  = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gi  = bid * blockDim.x + threadIdx.x;
     const int ngc = cnt[CP_NGC], ncj = cnt[CP_NCJ];
     double ext    = 0.0;
     if (gi < ngc) {
@@ -516,6 +575,14 @@ __global__ void k_ghost_first(int N, int* cnt, const int* __restrict__ border,
     zext_max(zext, ext);
 }
 
+__global__ void k_ghost_first(int N, int* cnt, const int* __restrict__ border,
+    const int* __restrict__ pbc, int mixed, Geom g, double4* cx, int* jnat, double4* jbbmin,
+    double4* jbbmax, float4* anchor, float4* xr, unsigned long long* zext)
+{
+    ghost_first_blk(blockIdx.x, N, cnt, border, pbc, mixed, g, cx, jnat, jbbmin, jbbmax, anchor,
+        xr, zext);
+}
+
 void launch_ghost_first(cudaStream_t s, int N, int ngc_cap, int mixed, int* cnt,
     const int* border, const int* pbc, const Geom& g, double4* cx, int* jnat, double4* jbbmin,
     double4* jbbmax, float4* anchor, float4* xr, unsigned long long* zext)
@@ -555,7 +622,8 @@ __global__ void k_ghost_update(int N, int mixed, const int* __restrict__ cnt,
 __global__ void k_ghost_update_batch(const CpStepMember* __restrict__ tab,
     const int2* __restrict__ bmap)
 {
-    const int2 bm         = __ldg(&bmap[blockIdx.x]);
+    const int2 bm = __ldg(&bmap[blockIdx.x]);
+    if (bm.x < 0) return;
     const CpStepMember& m = tab[bm.x];
     ghost_update_slot(bm.y * blockDim.x + threadIdx.x, m.N, m.mixed, m.cnt, m.border, m.pbc,
         m.jnat, m.xprd, m.yprd, m.zprd, m.cx, m.anchor, m.xr);
@@ -585,11 +653,12 @@ void launch_ghost_update(cudaStream_t s, int N, int ngc_cap, int mixed, const in
 // entry with a larger bbminz. Local j-clusters come first in cluster order and
 // are already ordered by bbminz, so the final column is the stable merge of the
 // locals and of the ghosts sorted by (bbminz, index).
-__global__ void k_ghost_columns(int N, const int* __restrict__ cnt, const int* __restrict__ pbc,
+__device__ __forceinline__ void ghost_columns_blk(int bid, int N, const int* __restrict__ cnt,
+    const int* __restrict__ pbc,
     const int* __restrict__ jnat, const double4* __restrict__ cx, Geom g, int* gcolumn,
     int* gcol_count)
 {
-    const int gi = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gi = bid * blockDim.x + threadIdx.x;
     if (gi >= cnt[CP_NGC]) return;
     const int cg = cnt[CP_NCJ] + gi, code = pbc[gi];
     const int dx = (code & 3) - 1, dy = ((code >> 2) & 3) - 1;
@@ -614,6 +683,13 @@ __global__ void k_ghost_columns(int N, const int* __restrict__ cnt, const int* _
     atomicAdd(&gcol_count[b], 1);
 }
 
+__global__ void k_ghost_columns(int N, const int* __restrict__ cnt, const int* __restrict__ pbc,
+    const int* __restrict__ jnat, const double4* __restrict__ cx, Geom g, int* gcolumn,
+    int* gcol_count)
+{
+    ghost_columns_blk(blockIdx.x, N, cnt, pbc, jnat, cx, g, gcolumn, gcol_count);
+}
+
 void launch_ghost_columns(cudaStream_t s, int N, int ngc_cap, const int* cnt, const int* pbc,
     const int* jnat, const double4* cx, const Geom& g, int* gcolumn, int* gcol_count)
 {
@@ -622,11 +698,18 @@ void launch_ghost_columns(cudaStream_t s, int N, int ngc_cap, const int* cnt, co
     g_launches++;
 }
 
+__device__ __forceinline__ void column_sizes_blk(int bid, int mbins1, int jfac,
+    const int* __restrict__ ncl_col,
+    const int* __restrict__ gcol_count, int* jcol_n)
+{
+    const int b = bid * blockDim.x + threadIdx.x;
+    if (b < mbins1) jcol_n[b] = ncl_col[b] / jfac + gcol_count[b];
+}
+
 __global__ void k_column_sizes(int mbins1, int jfac, const int* __restrict__ ncl_col,
     const int* __restrict__ gcol_count, int* jcol_n)
 {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b < mbins1) jcol_n[b] = ncl_col[b] / jfac + gcol_count[b];
+    column_sizes_blk(blockIdx.x, mbins1, jfac, ncl_col, gcol_count, jcol_n);
 }
 
 void launch_column_sizes(cudaStream_t s, int mbins1, int jfac, const int* ncl_col,
@@ -637,14 +720,22 @@ void launch_column_sizes(cudaStream_t s, int mbins1, int jfac, const int* ncl_co
     g_launches++;
 }
 
+__device__ __forceinline__ void ghost_scatter_blk(int bid, const int* __restrict__ cnt,
+    const int* __restrict__ gcolumn,
+    const int* __restrict__ jcol_start, const int* __restrict__ ncl_col, int jfac, int* gfill,
+    int* gtmp)
+{
+    const int gi = bid * blockDim.x + threadIdx.x;
+    if (gi >= cnt[CP_NGC]) return;
+    const int b = gcolumn[gi];
+    gtmp[jcol_start[b] + ncl_col[b] / jfac + atomicAdd(&gfill[b], 1)] = cnt[CP_NCJ] + gi;
+}
+
 __global__ void k_ghost_scatter(const int* __restrict__ cnt, const int* __restrict__ gcolumn,
     const int* __restrict__ jcol_start, const int* __restrict__ ncl_col, int jfac, int* gfill,
     int* gtmp)
 {
-    const int gi = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gi >= cnt[CP_NGC]) return;
-    const int b = gcolumn[gi];
-    gtmp[jcol_start[b] + ncl_col[b] / jfac + atomicAdd(&gfill[b], 1)] = cnt[CP_NCJ] + gi;
+    ghost_scatter_blk(blockIdx.x, cnt, gcolumn, jcol_start, ncl_col, jfac, gfill, gtmp);
 }
 
 void launch_ghost_scatter(cudaStream_t s, int ngc_cap, const int* cnt, const int* gcolumn,
@@ -655,13 +746,14 @@ void launch_ghost_scatter(cudaStream_t s, int ngc_cap, const int* cnt, const int
     g_launches++;
 }
 
-__global__ void k_merge_columns(int mbins1, int jfac, const int* __restrict__ ncl_col,
+__device__ __forceinline__ void merge_columns_blk(int bid, int mbins1, int jfac,
+    const int* __restrict__ ncl_col,
     const int* __restrict__ cl_start, const int* __restrict__ gcol_count,
     const int* __restrict__ jcol_start, const int* __restrict__ gtmp,
     const double4* __restrict__ jbbmin, const double4* __restrict__ jbbmax, int* jcol,
     double4* jcbbmin, double4* jcbbmax)
 {
-    const int b    = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int b    = (bid * blockDim.x + threadIdx.x) >> 5;
     const int lane = lane_id();
     if (b >= mbins1) return;
     const int start = jcol_start[b];
@@ -693,6 +785,16 @@ __global__ void k_merge_columns(int mbins1, int jfac, const int* __restrict__ nc
         jcbbmin[start + pos] = jbbmin[gj];
         jcbbmax[start + pos] = jbbmax[gj];
     }
+}
+
+__global__ void k_merge_columns(int mbins1, int jfac, const int* __restrict__ ncl_col,
+    const int* __restrict__ cl_start, const int* __restrict__ gcol_count,
+    const int* __restrict__ jcol_start, const int* __restrict__ gtmp,
+    const double4* __restrict__ jbbmin, const double4* __restrict__ jbbmax, int* jcol,
+    double4* jcbbmin, double4* jcbbmax)
+{
+    merge_columns_blk(blockIdx.x, mbins1, jfac, ncl_col, cl_start, gcol_count, jcol_start, gtmp,
+        jbbmin, jbbmax, jcol, jcbbmin, jcbbmax);
 }
 
 void launch_merge_columns(cudaStream_t s, int mbins1, int jfac, const int* ncl_col,
@@ -747,7 +849,8 @@ __device__ __forceinline__ double bb_axis(double imin, double imax, double jmin,
 #define CP_LIST_WARPS 4
 
 template <int M, int N>
-__global__ void __launch_bounds__(32 * CP_LIST_WARPS) k_build_list(int half, int* cnt, Geom g, const int* __restrict__ stencil,
+__device__ __forceinline__ void build_list_blk(int bid, int half, int* cnt, Geom g,
+    const int* __restrict__ stencil,
     const int* __restrict__ cbin, const double4* __restrict__ ibbmin,
     const double4* __restrict__ ibbmax, const double4* __restrict__ jcbbmin,
     const double4* __restrict__ jcbbmax, const double4* __restrict__ cx,
@@ -758,7 +861,7 @@ __global__ void __launch_bounds__(32 * CP_LIST_WARPS) k_build_list(int half, int
     __shared__ int s_lo[CP_LIST_WARPS][32];
     __shared__ int s_ws[CP_LIST_WARPS][32];
     const int w    = threadIdx.x >> 5;
-    const int ci   = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int ci   = (bid * blockDim.x + threadIdx.x) >> 5;
     const int lane = lane_id();
     if (ci >= cnt[CP_NCL]) return;
     const int ci_cj0 = ci / (N / M);
@@ -854,6 +957,20 @@ __global__ void __launch_bounds__(32 * CP_LIST_WARPS) k_build_list(int half, int
     }
 }
 
+template <int M, int N>
+__global__ void __launch_bounds__(32 * CP_LIST_WARPS) k_build_list(int half, int* cnt, Geom g,
+    const int* __restrict__ stencil,
+    const int* __restrict__ cbin, const double4* __restrict__ ibbmin,
+    const double4* __restrict__ ibbmax, const double4* __restrict__ jcbbmin,
+    const double4* __restrict__ jcbbmax, const double4* __restrict__ cx,
+    const int* __restrict__ jcol_start, const int* __restrict__ jcol,
+    const unsigned long long* __restrict__ zext, int maxneighs, int ks, int cs, int* list,
+    int* numneigh, int* nmasked)
+{
+    build_list_blk<M, N>(blockIdx.x, half, cnt, g, stencil, cbin, ibbmin, ibbmax, jcbbmin,
+        jcbbmax, cx, jcol_start, jcol, zext, maxneighs, ks, cs, list, numneigh, nmasked);
+}
+
 void launch_build_list(cudaStream_t s, int M, int N, int half, int ncl_cap, const int* cnt,
     const Geom& g, const int* stencil, const int* cbin, const double4* ibbmin,
     const double4* ibbmax, const double4* jcbbmin, const double4* jcbbmax, const double4* cx,
@@ -934,6 +1051,226 @@ void launch_prune(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt, con
     else
         k_prune<4, 8><<<blocks, 128, smem, s>>>(cnt, cx, cutneighsq, maxneighs, ks, cs, list,
             numneigh, nmasked);
+    g_launches++;
+}
+
+// ---- batched rebuild over the members of an ensemble ------------------------------
+// Each stage runs the single-member block bodies above; block b of a launch is
+// block bmap[b].y of member bmap[b].x.
+int cp_build_stage_blocks(int stage, const CpBuildMember& m, int* threads)
+{
+    const int T = MDB_NTHREADS, mb1 = m.g.mbins + 1;
+    *threads    = T;
+    switch (stage) {
+    case CB_RESET: return mdb_blocks(mb1, T);
+    case CB_GATHER: return mdb_blocks((long long)m.ncl_cap * m.M, T);
+    case CB_BIN:
+    case CB_SCATTER: return m.nlocal > 0 ? mdb_blocks(m.nlocal, T) : 0;
+    case CB_SORT: *threads = 32 * CP_SORT_WARPS; return mdb_blocks(m.g.mbins, CP_SORT_WARPS);
+    case CB_CLUSTERS: *threads = 128; return mdb_blocks((long long)m.g.mbins * 32, 128);
+    case CB_GCOUNT:
+    case CB_GWRITE: return mdb_blocks(m.ncj_cap, T);
+    case CB_GFIRST: return mdb_blocks(m.ngc_cap + 1, T);
+    case CB_GCOLS:
+    case CB_GSCATTER: return mdb_blocks(m.ngc_cap, T);
+    case CB_CSIZES: return mdb_blocks(mb1, T);
+    case CB_MERGE: *threads = 128; return mdb_blocks((long long)mb1 * 32, 128);
+    case CB_LIST:
+        *threads = 32 * CP_LIST_WARPS;
+        return mdb_blocks((long long)m.ncl_cap * 32, 32 * CP_LIST_WARPS);
+    }
+    return 0;
+}
+
+__device__ __forceinline__ void reset_blk(int bid, const CpBuildMember& m)
+{
+    const int t = bid * blockDim.x + threadIdx.x;
+    if (t <= m.g.mbins) {
+        m.col_count[t]  = 0;
+        m.col_fill[t]   = 0;
+        m.ncl_col[t]    = 0;
+        m.gcol_count[t] = 0;
+        m.gfill[t]      = 0;
+    }
+    if (t == 0) {
+        *m.zext                  = 0ull;
+        m.cnt[CP_MAXNEED]        = 0;
+        m.cnt[CP_BADBIN]         = 0;
+        m.cnt[CP_WINDOW]         = 0;
+        m.cnt[CP_NGHOST_ATOMS]   = 0;
+    }
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(256) k_build_stage_batch(const CpBuildMember* __restrict__ tab,
+    const int2* __restrict__ bmap)
+{
+    const int2 bm          = __ldg(&bmap[blockIdx.x]);
+    const CpBuildMember& m = tab[bm.x];
+    const int b            = bm.y;
+    switch (STAGE) {
+    case CB_RESET: reset_blk(b, m); break;
+    case CB_GATHER:
+        gather_blk(b, m.M, m.cnt, m.cx, m.cv, m.cl_first, m.ax, m.av, 1, m.g.xprd, m.g.yprd,
+            m.g.zprd);
+        break;
+    case CB_BIN: bin_atoms_blk(b, m.nlocal, m.ax, m.g, m.atom_col, m.col_count, m.cnt); break;
+    case CB_SCATTER:
+        scatter_atoms_blk(b, m.nlocal, m.atom_col, m.col_start, m.col_fill, m.col_atoms);
+        break;
+    case CB_SORT:
+        sort_columns_blk(b, m.g.mbins, m.M, m.N, m.col_start, m.col_atoms, m.ax, m.col_sorted,
+            m.gidx, m.gz, m.ncl_col);
+        break;
+    case CB_CLUSTERS:
+        if (m.N == 4)
+            build_clusters_blk<4, 4>(b, m.g.mbins, m.mixed, m.col_start, m.col_sorted,
+                m.cl_start, m.ax, m.av, m.cx, m.cv, m.inat, m.cbin, m.cl_first, m.ibbmin,
+                m.ibbmax, m.jnat, m.jbbmin, m.jbbmax, m.anchor, m.xr, m.cnt, m.zext);
+        else
+            build_clusters_blk<4, 8>(b, m.g.mbins, m.mixed, m.col_start, m.col_sorted,
+                m.cl_start, m.ax, m.av, m.cx, m.cv, m.inat, m.cbin, m.cl_first, m.ibbmin,
+                m.ibbmax, m.jnat, m.jbbmin, m.jbbmax, m.anchor, m.xr, m.cnt, m.zext);
+        break;
+    case CB_GCOUNT:
+        ghost_count_blk(b, m.ncj_cap, m.cnt, m.jnat, m.jbbmin, m.jbbmax, m.g, m.gcount);
+        break;
+    case CB_GWRITE:
+        ghost_write_blk(b, m.ncj_cap, m.ngc_cap, m.cnt, m.jnat, m.jbbmin, m.jbbmax, m.g, m.gstart,
+            m.border, m.pbc);
+        break;
+    case CB_GFIRST:
+        ghost_first_blk(b, m.N, m.cnt, m.border, m.pbc, m.mixed, m.g, m.cx, m.jnat, m.jbbmin,
+            m.jbbmax, m.anchor, m.xr, m.zext);
+        break;
+    case CB_GCOLS:
+        ghost_columns_blk(b, m.N, m.cnt, m.pbc, m.jnat, m.cx, m.g, m.gcolumn, m.gcol_count);
+        break;
+    case CB_CSIZES:
+        column_sizes_blk(b, m.g.mbins + 1, m.jfac, m.ncl_col, m.gcol_count, m.jcol_n);
+        break;
+    case CB_GSCATTER:
+        ghost_scatter_blk(b, m.cnt, m.gcolumn, m.jcol_start, m.ncl_col, m.jfac, m.gfill, m.gtmp);
+        break;
+    case CB_MERGE:
+        merge_columns_blk(b, m.g.mbins + 1, m.jfac, m.ncl_col, m.cl_start, m.gcol_count,
+            m.jcol_start, m.gtmp, m.jbbmin, m.jbbmax, m.jcol, m.jcbbmin, m.jcbbmax);
+        break;
+    case CB_LIST:
+        if (m.N == 4)
+            build_list_blk<4, 4>(b, m.half, m.cnt, m.g, m.stencil, m.cbin, m.ibbmin, m.ibbmax,
+                m.jcbbmin, m.jcbbmax, m.cx, m.jcol_start, m.jcol, m.zext, m.maxneighs, m.ks,
+                m.cs, m.list, m.numneigh, m.nmasked);
+        else
+            build_list_blk<4, 8>(b, m.half, m.cnt, m.g, m.stencil, m.cbin, m.ibbmin, m.ibbmax,
+                m.jcbbmin, m.jcbbmax, m.cx, m.jcol_start, m.jcol, m.zext, m.maxneighs, m.ks,
+                m.cs, m.list, m.numneigh, m.nmasked);
+        break;
+    }
+}
+
+void launch_build_stage_batch(cudaStream_t s, int stage, int nblocks, const CpBuildMember* tab,
+    const int2* bmap)
+{
+    if (nblocks <= 0) return;
+    CpBuildMember probe{};
+    probe.M = 4, probe.N = 4;
+    int T = 0;
+    cp_build_stage_blocks(stage, probe, &T);
+    switch (stage) {
+#define CP_STAGE(S)                                                                      \
+    case S: k_build_stage_batch<S><<<nblocks, T, 0, s>>>(tab, bmap); break;
+        CP_STAGE(CB_RESET)
+        CP_STAGE(CB_GATHER)
+        CP_STAGE(CB_BIN)
+        CP_STAGE(CB_SCATTER)
+        CP_STAGE(CB_SORT)
+        CP_STAGE(CB_CLUSTERS)
+        CP_STAGE(CB_GCOUNT)
+        CP_STAGE(CB_GWRITE)
+        CP_STAGE(CB_GFIRST)
+        CP_STAGE(CB_GCOLS)
+        CP_STAGE(CB_CSIZES)
+        CP_STAGE(CB_GSCATTER)
+        CP_STAGE(CB_MERGE)
+        CP_STAGE(CB_LIST)
+#undef CP_STAGE
+    default: return;
+    }
+    g_launches++;
+}
+
+// exclusive scan of one member's array by one block of 1024 threads (4 items
+// per thread per pass), out[n] = total
+#define CP_SCAN_T 1024
+__global__ void __launch_bounds__(CP_SCAN_T) k_scan_batch(const CpBuildMember* __restrict__ tab,
+    int which)
+{
+    __shared__ int s_w[CP_SCAN_T / 32];
+    const CpBuildMember& m = tab[blockIdx.x];
+    const int* in;
+    int* out;
+    int n;
+    switch (which) {
+    case 0: in = m.col_count, out = m.col_start, n = m.g.mbins; break;
+    case 1: in = m.ncl_col, out = m.cl_start, n = m.g.mbins + 1; break;
+    case 2: in = m.gcount, out = m.gstart, n = m.ncj_cap; break;
+    default: in = m.jcol_n, out = m.jcol_start, n = m.g.mbins + 1; break;
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int carry = 0;
+    for (int base = 0; base < n; base += 4 * CP_SCAN_T) {
+        const int i0 = base + 4 * threadIdx.x;
+        int v[4], t = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            v[k] = i0 + k < n ? in[i0 + k] : 0;
+            t += v[k];
+        }
+        int inc = t;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += u;
+        }
+        if (lane == 31) s_w[w] = inc;
+        __syncthreads();
+        if (w == 0) {
+            int x = s_w[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += u;
+            }
+            s_w[lane] = x;
+        }
+        __syncthreads();
+        int run = carry + (w > 0 ? s_w[w - 1] : 0) + inc - t;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (i0 + k < n) out[i0 + k] = run;
+            run += v[k];
+        }
+        carry += s_w[CP_SCAN_T / 32 - 1];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[n] = carry;
+}
+
+void launch_scan_batch(cudaStream_t s, int which, int nmem, const CpBuildMember* tab)
+{
+    if (nmem <= 0) return;
+    k_scan_batch<<<nmem, CP_SCAN_T, 0, s>>>(tab, which);
+    g_launches++;
+}
+
+__global__ void k_counters_batch(const CpBuildMember* __restrict__ tab, int* out)
+{
+    if (threadIdx.x < CP_SLOTS) out[blockIdx.x * CP_SLOTS + threadIdx.x] = tab[blockIdx.x].cnt[threadIdx.x];
+}
+
+void launch_counters_batch(cudaStream_t s, int nmem, const CpBuildMember* tab, int* out)
+{
+    if (nmem <= 0) return;
+    k_counters_batch<<<nmem, 32, 0, s>>>(tab, out);
     g_launches++;
 }
 

@@ -488,8 +488,9 @@ __global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_force_mix
     float cutforcesq)
 {
     __shared__ float s_se[MDB_MAX_TYPES], s_s3[MDB_MAX_TYPES];
+    const int2 bm = __ldg(&bmap[blockIdx.x]);
+    if (bm.x < 0) return; // an unused entry of a map sized for the capacities
     load_type_tables(ty, s_se, s_s3);
-    const int2 bm          = __ldg(&bmap[blockIdx.x]);
     const CpForceMember& m = tab[bm.x];
     force_mixed_block<N, HALF, ENERGY, UNIFORM, PF>(bm.y, m.cnt, m.xr, m.anchor, ty, cutforcesq,
         m.list, 1, m.cs, m.numneigh, m.cf32, m.epart, s_se, s_s3);
@@ -660,7 +661,8 @@ template <bool FINAL, bool INITIAL>
 __global__ void k_cp_integrate_batch(const CpStepMember* __restrict__ tab,
     const int2* __restrict__ bmap)
 {
-    const int2 bm         = __ldg(&bmap[blockIdx.x]);
+    const int2 bm = __ldg(&bmap[blockIdx.x]);
+    if (bm.x < 0) return;
     const CpStepMember& m = tab[bm.x];
     cp_integrate_slot<FINAL, INITIAL>(bm.y * blockDim.x + threadIdx.x, m.M, m.N, m.cnt, m.dtf,
         m.dt, m.cx, m.cv, m.cf, m.cf32, m.anchor, m.xr, m.zero_f != 0);

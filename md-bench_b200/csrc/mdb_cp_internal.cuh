@@ -196,6 +196,56 @@ struct CpForceMember { // mixed force kernel (row-major lists)
     double* epart;
     int cs, pad;
 };
+// Every buffer and size the rebuild kernels of one member use.
+struct CpBuildMember {
+    Geom g;
+    int M, N, jfac, mixed, half, nlocal, ncl_cap, ncj_cap, ngc_cap, maxneighs, ks, cs;
+    int* cnt;
+    unsigned long long* zext;
+    double4 *ax, *av, *cx, *cv;
+    int *cl_first, *atom_col, *col_count, *col_start, *col_fill, *col_atoms, *col_sorted, *gidx;
+    double* gz;
+    int *ncl_col, *cl_start, *inat, *cbin;
+    double4 *ibbmin, *ibbmax;
+    int* jnat;
+    double4 *jbbmin, *jbbmax;
+    float4 *anchor, *xr;
+    int *gcount, *gstart, *border, *pbc, *gcolumn, *gcol_count, *jcol_n, *jcol_start, *gfill;
+    int *gtmp, *jcol;
+    double4 *jcbbmin, *jcbbmax;
+    const int* stencil;
+    int *list, *numneigh, *nmasked;
+};
+// stages of a batched rebuild, in order; the block-map entry of each stage
+// covers every member's grid of the single-member launch
+enum CpBuildStage {
+    CB_RESET,    // counters and column counts to zero
+    CB_GATHER,   // updateSingleAtoms + updateAtomsPbc
+    CB_BIN,      // binAtoms
+    CB_SCATTER,  // column lists
+    CB_SORT,     // sortAtomsByZCoord
+    CB_CLUSTERS, // buildClusters + defineJClusters
+    CB_GCOUNT,   // setupPbc: images per j-cluster
+    CB_GWRITE,   // setupPbc: ghost table
+    CB_GFIRST,   // updatePbc(first)
+    CB_GCOLS,    // binJClusters: ghost columns
+    CB_CSIZES,   // binJClusters: column sizes
+    CB_GSCATTER, // binJClusters: ghosts into columns
+    CB_MERGE,    // binJClusters: merge by bbminz
+    CB_LIST,     // buildNeighbor
+    CB_COUNT
+};
+// blocks (and threads per block) of a stage for one member
+int cp_build_stage_blocks(int stage, const CpBuildMember& m, int* threads);
+// the stage over all members: nblocks entries of bmap
+void launch_build_stage_batch(cudaStream_t s, int stage, int nblocks,
+    const CpBuildMember* tab, const int2* bmap);
+// the column scans of the rebuild (which: 0 col_count, 1 ncl_col, 2 gcount,
+// 3 jcol_n), one block per member
+void launch_scan_batch(cudaStream_t s, int which, int nmem, const CpBuildMember* tab);
+// every member's CP_SLOTS counters into out[member * CP_SLOTS + k]
+void launch_counters_batch(cudaStream_t s, int nmem, const CpBuildMember* tab, int* out);
+
 void launch_cp_integrate_batch(cudaStream_t s, bool final_, bool initial, int nblocks,
     const CpStepMember* tab, const int2* bmap);
 void launch_ghost_update_batch(cudaStream_t s, int nblocks, const CpStepMember* tab,
