@@ -45,9 +45,10 @@ void* mdb_cp_stream(MdbCp* ctx);
 int mdb_cp_synchronize(MdbCp* ctx);
 /* Launch tuning (no counterpart in the reference; results are unchanged):
  * "force_block" = threads per block of the mixed force kernel (32..512, a
- * multiple of 32; default 128); "force_variant" = 0..3, bit 0: j data
- * prefetched two list blocks ahead instead of one, bit 1: a register budget
- * for 8 resident blocks of 128 threads per SM (default 2). */
+ * multiple of 32; default 128); "force_variant" = 0..3: 0 and 1 prefetch the
+ * j data one or two list blocks ahead with no register budget, 2 and 3 the same
+ * with a budget for 8 resident blocks of 128 threads per SM (these run blocks
+ * of 128 threads; default 2). */
 int mdb_cp_tune(MdbCp* ctx, const char* key, int value);
 /* Device time of one force evaluation (no energy) on the context's stream:
  * the mean over reps back-to-back launches after two untimed ones, from CUDA

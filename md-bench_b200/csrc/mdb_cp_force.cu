@@ -208,6 +208,12 @@ __device__ __forceinline__ void f2_unpack(f2 v, float& lo, float& hi)
 {
     asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
 }
+__device__ __forceinline__ f2 f2_add(f2 a, f2 b)
+{
+    f2 r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
 __device__ __forceinline__ f2 f2_sub(f2 a, f2 b)
 {
     f2 r;
@@ -308,9 +314,11 @@ __device__ __forceinline__ JEntry load_entry(int cj, int b, const float4* __rest
     if (cj >= 0) {
         j.x            = __ldg(&xr[cj * N + b]);
         const float4 a = __ldg(&anchor[cj]);
-        // anchors are multiples of 1/8 of magnitude < 2^17: the difference is exact
-        j.x.x += a.x - ai.x;
-        j.x.y += a.y - ai.y;
+        // anchors are multiples of 1/8 of magnitude < 2^17: the difference is
+        // exact (x and y as one packed pair)
+        const f2 dxy = f2_sub(f2_pack(a.x, a.y), f2_pack(ai.x, ai.y));
+        const f2 jxy = f2_add(f2_pack(j.x.x, j.x.y), dxy);
+        f2_unpack(jxy, j.x.x, j.x.y);
         j.x.z += a.z - ai.z;
     } else {
         j.x = make_float4(CP_PAD_F, CP_PAD_F, CP_PAD_F, __int_as_float(-1));
@@ -329,7 +337,8 @@ __device__ __forceinline__ JEntry load_entry(int cj, int b, const float4* __rest
 // sit at +1e18 (j) and invalid i atoms are moved to -1e18, so they fall outside
 // the cutoff without INF arithmetic.
 // PF: j data prefetched 1 or 2 iterations ahead; MINB: minimum resident blocks
-// of 128 threads per SM asked of the register allocator (0: no request).
+// of 128 threads per SM asked of the register allocator (0: no request; 8
+// caps a thread at 64 registers, measured best against 6, 7, 9 and 10).
 // Both are launch-shape choices of the autotuner; results do not depend on them.
 // The work of block bid (warps = i-clusters); s_se / s_s3: the type tables in
 // shared memory.
@@ -398,7 +407,9 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
             const int c1 = __shfl_sync(0xffffffffu, lst_cur, JPW + eidx);
             nx1          = load_entry<N>(JPW < nn ? c1 : -1, b, xr, anchor, ai);
         }
-        for (int kb = 0; kb < nn; kb += JPW) {
+        // one warp iteration: JPW entries, lane (eidx, b) on atom b of entry
+        // kb + eidx; masked: the iteration may hold the diagonal entry
+        auto step = [&](int kb, bool masked) {
             // the entry block holding kn is rotated in when kn reaches it
             const int kn = kb + PF * JPW;
             if ((kn & 31) == 0) {
@@ -420,9 +431,11 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
             // except pairs with ghost atoms, which both owners list
             const double ew = (!HALF || cj * N + b >= nloc) ? 0.5 : 1.0;
             mixed_entry<HALF, ENERGY, UNIFORM>(ip, cur.x, sej, s3j,
-                cj == ci_cj0 ? diag_excl : 0u, cutforcesq, A2, mB2, sig6u, ty.eps0, ew, fx, fy,
-                fz, gx, gy, gz, e);
-            if (HALF && cj >= 0 && cj * N + b < nloc && __float_as_int(cur.x.w) >= 0) {
+                (masked && cj == ci_cj0) ? diag_excl : 0u, cutforcesq, A2, mB2, sig6u, ty.eps0,
+                ew, fx, fy, fz, gx, gy, gz, e);
+            // reactions on local j atoms only (the reference drops ghost
+            // reactions); padding j slots get exact zeros
+            if (HALF && cj >= 0 && cj * N + b < nloc) {
                 float gx0, gx1, gy0, gy1, gz0, gz1;
                 f2_unpack(gx, gx0, gx1);
                 f2_unpack(gy, gy0, gy1);
@@ -435,6 +448,13 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
             } else {
                 cur = nx;
             }
+        };
+        // the diagonal entry is the first of its row (the list build swaps it
+        // to the front and pruning never removes it), so only the first
+        // iteration tests for it
+        if (nn > 0) {
+            step(0, true);
+            for (int kb = JPW; kb < nn; kb += JPW) step(kb, false);
         }
         float f[12];
 #pragma unroll
