@@ -141,6 +141,20 @@ int mdb_final_integrate(MdbCtx* ctx);
 /* computeThermo (common/thermo.c:60-100) of the current state. */
 int mdb_thermo(MdbCtx* ctx, MdbThermo* out);
 
+/* sortAtom (verletlist/neighbor.c:466-536): local atoms reordered bin by bin,
+ * each bin's atoms in index order, for locality of the list build and force
+ * gathers. Positions, types, velocities and forces move together (the
+ * reference moves positions and velocities only). Ghosts and lists are invalid
+ * afterwards, as in the reference (which clears Nghost first): run
+ * mdb_setup_pbc + mdb_update_pbc + mdb_build_neighbor, or mdb_setup, before
+ * the next force. */
+int mdb_sort_atoms(MdbCtx* ctx);
+/* SORT_ATOMS builds (verletlist/main.c:92-95, 372-381; Parameter.resort_every,
+ * reference default 400): mdb_run sorts before the initial integration of
+ * every step n with (n+1) % resort_every == 0 and rebuilds in that step.
+ * 0 (the default, as SORT_ATOMS ?= false) disables. */
+int mdb_set_resort(MdbCtx* ctx, int resort_every);
+
 /* setup tail of verletlist/main.c:96-111 for atoms already set:
  * setupPbc, updatePbc, buildNeighbor, computeForce. */
 int mdb_setup(MdbCtx* ctx);

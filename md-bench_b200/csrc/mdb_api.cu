@@ -78,6 +78,7 @@ struct MdbCtx {
 
     Graph g_plain, g_rebuild;
     bool energy_valid = false;
+    int resort_every  = 0; // SORT_ATOMS builds: sortAtom every resort_every steps
 };
 
 // ---------------------------------------------------------------------------
@@ -800,6 +801,55 @@ static int do_rebuild(MdbCtx* ctx, bool use_graph, bool wrap = true)
     return fail(ctx, MDB_ERR_OVERFLOW, "rebuild did not converge");
 }
 
+// sortAtom (verletlist/neighbor.c:466-536): the reference clears the ghosts,
+// bins the locals (binatoms: a bin's atoms in index order) and rewrites the
+// atom arrays bin by bin. Positions (with their type bits), velocities and
+// forces move together here; the reference moves only positions and
+// velocities. Ghosts and lists are left invalid, as in the reference.
+static int sort_atoms(MdbCtx* ctx)
+{
+    cudaStream_t s = ctx->s;
+    const int n    = ctx->nlocal;
+    long long m    = launch_mark();
+    cudaMemsetAsync(ctx->counters + CNT_NGHOST, 0, sizeof(int), s);
+    cudaMemsetAsync(ctx->counters + CNT_BADBIN, 0, sizeof(int), s);
+    cudaMemsetAsync(ctx->bin_count, 0, sizeof(int) * ctx->g.mbins, s);
+    cudaMemsetAsync(ctx->bin_lcount, 0, sizeof(int) * ctx->g.mbins, s);
+    cudaMemsetAsync(ctx->local_order, 0xff, sizeof(int) * std::max(n, 1), s);
+    launch_bin_count(s, n, ctx->nall_cap, ctx->x, ctx->g, ctx->atom_bin, ctx->atom_slot,
+        ctx->bin_count, ctx->bin_lcount, ctx->counters);
+    scan_exclusive(ctx->bin_count, ctx->bin_start, ctx->g.mbins, ctx->scan_scratch, s);
+    scan_exclusive(ctx->bin_lcount, ctx->loc_start, ctx->g.mbins, ctx->scan_scratch, s);
+    launch_bin_scatter(s, n, ctx->nall_cap, ctx->atom_bin, ctx->atom_slot, ctx->bin_start,
+        ctx->bin_atoms, ctx->counters);
+    launch_bin_sort(s, ctx->g.mbins, ctx->bin_start, ctx->bin_atoms, ctx->loc_start,
+        ctx->local_order);
+    // stage: 9 n doubles; positions as double4 [0, 4n), velocities [4n, 7n)
+    double4* sx = reinterpret_cast<double4*>(ctx->stage);
+    double* sv  = ctx->stage + 4 * (size_t)n;
+    launch_permute4(s, n, ctx->local_order, ctx->x, sx);
+    launch_permute3(s, n, ctx->local_order, ctx->vx, ctx->vy, ctx->vz, sv);
+    CK(cudaMemcpyAsync(ctx->x, sx, sizeof(double4) * n, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(ctx->vx, sv, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(ctx->vy, sv + n, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(ctx->vz, sv + 2 * (size_t)n, sizeof(double) * n,
+        cudaMemcpyDeviceToDevice, s));
+    launch_permute3(s, n, ctx->local_order, ctx->fx, ctx->fy, ctx->fz, ctx->stage);
+    CK(cudaMemcpyAsync(ctx->fx, ctx->stage, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(ctx->fy, ctx->stage + n, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+        s));
+    CK(cudaMemcpyAsync(ctx->fz, ctx->stage + 2 * (size_t)n, sizeof(double) * n,
+        cudaMemcpyDeviceToDevice, s));
+    launch_account(ctx, m);
+    CK(cudaMemcpyAsync(ctx->h_counters, ctx->counters, CNT_SLOTS * sizeof(int),
+        cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    ctx->have_ghosts = ctx->have_list = false;
+    if (ctx->h_counters[CNT_BADBIN] > 0)
+        return fail(ctx, MDB_ERR_OVERFLOW, "atom outside the bin grid");
+    return MDB_OK;
+}
+
 // ---------------------------------------------------------------------------
 // hooks
 #define NEED_ATOMS()                                                                     \
@@ -977,6 +1027,20 @@ static void enq_plain_step(MdbCtx* ctx)
     enq_force(ctx, false);
 }
 
+extern "C" int mdb_sort_atoms(MdbCtx* ctx)
+{
+    NEED_ATOMS();
+    CK(cudaSetDevice(ctx->dev));
+    return sort_atoms(ctx);
+}
+
+extern "C" int mdb_set_resort(MdbCtx* ctx, int resort_every)
+{
+    if (!ctx || resort_every < 0) return MDB_ERR_ARG;
+    ctx->resort_every = resort_every;
+    return MDB_OK;
+}
+
 extern "C" int mdb_run(MdbCtx* ctx, int first_step, int nsteps, MdbThermo* samples,
     int max_samples, int* nsamples)
 {
@@ -992,8 +1056,21 @@ extern "C" int mdb_run(MdbCtx* ctx, int first_step, int nsteps, MdbThermo* sampl
     // needs it on its own
     bool pending_final = false;
     for (int n = first_step; n <= last; n++) {
-        bool reneigh = (n + 1) % ctx->p.reneigh_every == 0;
-        bool sample  = max_samples > 0 && (n + 1) % ctx->p.nstat == 0;
+        // SORT_ATOMS builds resort before the step's initial integration
+        // (verletlist/main.c:372-381); the step then rebuilds ghosts and lists
+        const bool resort = ctx->resort_every > 0 && (n + 1) % ctx->resort_every == 0;
+        bool reneigh      = resort || (n + 1) % ctx->p.reneigh_every == 0;
+        bool sample       = max_samples > 0 && (n + 1) % ctx->p.nstat == 0;
+        if (resort) {
+            if (pending_final) {
+                long long m0 = launch_mark();
+                enq_final(ctx);
+                launch_account(ctx, m0);
+                pending_final = false;
+            }
+            int rc = sort_atoms(ctx);
+            if (rc) return rc;
+        }
         if (!reneigh && !sample && pending_final) {
             if (!ctx->g_plain.exec) {
                 int rc = capture(ctx, ctx->g_plain, enq_plain_step);

@@ -174,6 +174,10 @@ void launch_unpack_atoms(cudaStream_t s, int n, const double4* x, const double* 
     const double* vy, const double* vz, const double* fx, const double* fy, const double* fz,
     double* xa, double* va, double* fa, int* ta);
 void launch_wrap(cudaStream_t s, int n, double4* x, double xprd, double yprd, double zprd);
+// gathers of sortAtom: out[k] = in[order[k]] (three SoA arrays into out[0..3n))
+void launch_permute4(cudaStream_t s, int n, const int* order, const double4* in, double4* out);
+void launch_permute3(cudaStream_t s, int n, const int* order, const double* a, const double* b,
+    const double* c, double* out);
 void launch_ghost_count(cudaStream_t s, int n, const double4* x, double cut, double xprd,
     double yprd, double zprd, int px, int py, int pz, int* cnt);
 void launch_ghost_write(cudaStream_t s, int n, int ghost_cap, double4* x, double cut,

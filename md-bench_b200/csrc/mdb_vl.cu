@@ -175,6 +175,43 @@ void launch_wrap(cudaStream_t s, int n, double4* x, double xprd, double yprd, do
     g_launches++;
 }
 
+// ---- sortAtom, verletlist/neighbor.c:466-536 ----------------------------------
+// New atom k is old atom order[k] (the locals bin by bin, each bin's atoms in
+// index order); positions carry the type bits, so types move with them.
+__global__ void k_permute4(int n, const int* __restrict__ order, const double4* __restrict__ in,
+    double4* __restrict__ out)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) out[k] = in[order[k]];
+}
+
+// three SoA arrays a, b, c into out[0..n), out[n..2n), out[2n..3n)
+__global__ void k_permute3(int n, const int* __restrict__ order, const double* __restrict__ a,
+    const double* __restrict__ b, const double* __restrict__ c, double* __restrict__ out)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int o = order[k];
+    out[k]         = a[o];
+    out[n + k]     = b[o];
+    out[2 * n + k] = c[o];
+}
+
+void launch_permute4(cudaStream_t s, int n, const int* order, const double4* in, double4* out)
+{
+    if (n <= 0) return;
+    k_permute4<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(n, order, in, out);
+    g_launches++;
+}
+
+void launch_permute3(cudaStream_t s, int n, const int* order, const double* a, const double* b,
+    const double* c, double* out)
+{
+    if (n <= 0) return;
+    k_permute3<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(n, order, a, b, c, out);
+    g_launches++;
+}
+
 // ---- ghost map: setupPbc, verletlist/pbc.c:103-232 ---------------------------
 // The 26 image candidates of one atom, enumerated in the reference's order
 // (6 faces, 8 corners, 12 edges). For each candidate `visit(sx, sy, sz)` is

@@ -83,6 +83,7 @@ EXPORTS = [
     "mdb_initial_integrate", "mdb_final_integrate", "mdb_thermo", "mdb_setup", "mdb_run", "mdb_get_counts",
     "mdb_get_positions_all", "mdb_get_ghosts", "mdb_get_neighbor_list",
     "mdb_get_bin_geometry", "mdb_get_eam_fp", "mdb_launch_count", "mdb_kinetic_sum_noalloc",
+    "mdb_sort_atoms", "mdb_set_resort",
 ]
 # every symbol include/mdb_cp.h declares
 CP_EXPORTS = [
@@ -143,8 +144,10 @@ def load():
     }
     for name in ("mdb_setup_pbc", "mdb_update_pbc", "mdb_update_atoms_pbc",
                  "mdb_build_neighbor", "mdb_compute_force", "mdb_compute_force_energy",
-                 "mdb_initial_integrate", "mdb_final_integrate", "mdb_setup"):
+                 "mdb_initial_integrate", "mdb_final_integrate", "mdb_setup",
+                 "mdb_sort_atoms"):
         sig[name] = ([vp], ip)
+    sig["mdb_set_resort"] = ([vp, ip], ip)
     sig.update({
         "mdb_cp_create": ([C.POINTER(MdbParams), ip, ip, C.POINTER(vp)], ip),
         "mdb_cp_destroy": ([vp], ip),
@@ -458,6 +461,13 @@ class System:
 
     def update_atoms_pbc(self):
         self._ck(self.lib.mdb_update_atoms_pbc(self.h), "mdb_update_atoms_pbc")
+
+    def sort_atoms(self):
+        """sortAtom: locals bin by bin; ghosts and lists must be rebuilt."""
+        self._ck(self.lib.mdb_sort_atoms(self.h), "mdb_sort_atoms")
+
+    def set_resort(self, every):
+        self._ck(self.lib.mdb_set_resort(self.h, int(every)), "mdb_set_resort")
 
     def build_neighbor(self):
         self._ck(self.lib.mdb_build_neighbor(self.h), "mdb_build_neighbor")

@@ -61,6 +61,7 @@ struct OrcSys {
     double *frho, *rhor, *z2r;
     double *frho_spline, *rhor_spline, *z2r_spline;
     double *fp, *rho;
+    int resort_every; /* SORT_ATOMS builds: sortAtom period (0: never) */
 };
 
 /* ------------------------------------------------------------------------- */
@@ -988,10 +989,52 @@ int orc_setup(OrcSys* s)
     return orc_build_neighbor(s);
 }
 
+void orc_sort_atoms(OrcSys* s)
+{
+    /* sortAtom, verletlist/neighbor.c:466-536: no ghosts, binatoms, then the
+     * atoms bin by bin (each bin's atoms in index order). The reference
+     * rewrites positions and velocities only; types and forces move here too. */
+    s->nghost = 0;
+    orc_binatoms(s);
+    const int n = s->nlocal;
+    double* nx  = orc_alloc(sizeof(double) * 3 * (size_t)s->nmax);
+    double* nv  = orc_alloc(sizeof(double) * 3 * (size_t)s->nmax);
+    double* nf  = orc_alloc(sizeof(double) * 3 * (size_t)s->nmax);
+    int* nt     = orc_alloc(sizeof(int) * (size_t)s->nmax);
+    int k       = 0;
+    for (int b = 0; b < s->mbins; b++)
+        for (int c = 0; c < s->bincount[b]; c++, k++) {
+            const int o = s->bins[b * s->atoms_per_bin + c];
+            for (int d = 0; d < 3; d++) {
+                nx[3 * k + d] = s->x[3 * o + d];
+                nv[3 * k + d] = s->v[3 * o + d];
+                nf[3 * k + d] = s->f[3 * o + d];
+            }
+            nt[k] = s->type[o];
+        }
+    if (k != n) {
+        fprintf(stderr, "oracle: sort lost atoms (%d of %d)\n", k, n);
+        abort();
+    }
+    free(s->x);
+    free(s->v);
+    free(s->f);
+    free(s->type);
+    s->x    = nx;
+    s->v    = nv;
+    s->f    = nf;
+    s->type = nt;
+}
+
+void orc_set_resort(OrcSys* s, int every) { s->resort_every = every > 0 ? every : 0; }
+
 void orc_step(OrcSys* s, int n)
 {
-    /* verletlist/main.c:371-419 (no MPI: forward/reverse reduce to updatePbc) */
-    int reneigh = (n + 1) % s->p.reneigh_every == 0;
+    /* verletlist/main.c:371-419 (no MPI: forward/reverse reduce to updatePbc);
+     * SORT_ATOMS: sortAtom first (main.c:372-381), and the step rebuilds */
+    const int resort = s->resort_every > 0 && (n + 1) % s->resort_every == 0;
+    int reneigh      = resort || (n + 1) % s->p.reneigh_every == 0;
+    if (resort) orc_sort_atoms(s);
     orc_initial_integrate(s);
     if (reneigh) {
         orc_update_atoms_pbc(s);

@@ -67,6 +67,11 @@ void orc_initial_integrate(OrcSys* s);
 void orc_final_integrate(OrcSys* s);
 /* One timestep with index n (0-based), exactly as the main loop runs it. */
 void orc_step(OrcSys* s, int n);
+/* sortAtom (locals bin by bin; ghosts cleared: call orc_setup_pbc,
+ * orc_update_pbc, orc_build_neighbor before the next force) and the SORT_ATOMS
+ * resort period used by orc_step (0: never). */
+void orc_sort_atoms(OrcSys* s);
+void orc_set_resort(OrcSys* s, int every);
 
 /* Thermo of the current state: T and P as the reference prints them,
  * KE, PE (from the last force call) and E = KE + PE, all totals. */

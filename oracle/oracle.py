@@ -66,12 +66,13 @@ def _load():
             getattr(lib, name).argtypes = [C.c_void_p]
             getattr(lib, name).restype = C.c_int
         for name in ("orc_update_pbc", "orc_update_atoms_pbc", "orc_initial_integrate",
-                     "orc_final_integrate"):
+                     "orc_final_integrate", "orc_sort_atoms"):
             getattr(lib, name).argtypes = [C.c_void_p]
             getattr(lib, name).restype = None
         lib.orc_compute_force.argtypes = [C.c_void_p]
         lib.orc_compute_force.restype = C.c_double
         lib.orc_step.argtypes = [C.c_void_p, C.c_int]
+        lib.orc_set_resort.argtypes = [C.c_void_p, C.c_int]
         lib.orc_load_eam.argtypes = [C.c_void_p, C.c_char_p]
         lib.orc_load_eam.restype = C.c_int
         lib.orc_eam_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_int)] * 4 + \
@@ -148,6 +149,19 @@ class Oracle:
 
     def rebuild(self):
         self.lib.orc_update_atoms_pbc(self.h)
+        self.lib.orc_setup_pbc(self.h)
+        self.lib.orc_update_pbc(self.h)
+        self.lib.orc_build_neighbor(self.h)
+
+    def sort_atoms(self):
+        """sortAtom; ghosts and lists are cleared (rebuild before a force)."""
+        self.lib.orc_sort_atoms(self.h)
+
+    def set_resort(self, every):
+        self.lib.orc_set_resort(self.h, every)
+
+    def reghost(self):
+        """setupPbc + updatePbc + buildNeighbor without the wrap."""
         self.lib.orc_setup_pbc(self.h)
         self.lib.orc_update_pbc(self.h)
         self.lib.orc_build_neighbor(self.h)
@@ -266,6 +280,7 @@ def _load_ref():
         lib.ref_vl_get_list.argtypes = [_ip, _ip, C.c_int]
         lib.ref_vl_force.restype = C.c_double
         lib.ref_vl_step.argtypes = [C.c_int]
+        lib.ref_vl_sort.argtypes = []
         lib.ref_vl_thermo.argtypes = [C.POINTER(C.c_double)] * 2
         lib.ref_vl_set_threads.argtypes = [C.c_int]
         _ref = lib
@@ -323,6 +338,10 @@ class RefVL:
 
     def step(self, n):
         self.lib.ref_vl_step(n)
+
+    def sort_atoms(self):
+        """The reference's sortAtom (moves positions and velocities only)."""
+        self.lib.ref_vl_sort()
 
     def params(self):
         d = np.zeros(8)

@@ -153,6 +153,13 @@ void ref_vl_rebuild(void)
     buildNeighbor(&g_atom, &g_neighbor);
 }
 
+/* sortAtom as the SORT_ATOMS build calls it (verletlist/main.c:92-95) */
+void ref_vl_sort(void)
+{
+    g_atom.Nghost = 0;
+    sortAtom(&g_atom);
+}
+
 void ref_vl_step(int n)
 {
     /* verletlist/main.c:371-419 without MPI */

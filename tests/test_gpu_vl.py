@@ -147,6 +147,53 @@ def test_full_list_force_and_trajectory_bit_exact_hooks_and_graphs():
         assert last[k] == pytest.approx(th[k], rel=THERMO_REL)
 
 
+def test_sort_atoms_bit_exact():
+    """sortAtom on the GPU after 33 steps: the same permutation of positions,
+    velocities, types and forces as the oracle (itself pinned to the
+    reference's sortAtom), then a rebuild and the same forces."""
+    kw = dict(nx=7, ny=6, nz=5)
+    o = lj_oracle(**kw)
+    s, _ = lj_system(**kw)
+    for n in range(33):
+        o.step(n)
+        s.step(n)
+    o.sort_atoms()
+    s.sort_atoms()
+    xo, vo, fo, to = o.atoms()
+    x, v, f, t = s.atoms()
+    assert np.array_equal(x, xo) and np.array_equal(v, vo)
+    assert np.array_equal(t, to) and np.array_equal(f, fo)
+    o.reghost()
+    o.force()
+    s.setup_pbc()
+    s.update_pbc()
+    s.build_neighbor()
+    s.compute_force()
+    assert np.array_equal(s.atoms()[2], o.atoms()[2])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_resort_run(precision):
+    """mdb_run with a resort period follows the oracle's SORT_ATOMS loop bit for
+    bit in FP64 (full lists), and the mixed path stays within its budget."""
+    kw = dict(nx=8, ny=8, nz=8, nstat=50)
+    o = lj_oracle(**kw)
+    o.set_resort(40)
+    s, _ = lj_system(precision=precision, **kw)
+    s.set_resort(40)
+    samples = s.run(100)
+    o.run(100)
+    xo, vo, fo, to = o.atoms()
+    x, v, f, t = s.atoms()
+    assert np.array_equal(t, to)
+    if precision == "fp64":
+        assert np.array_equal(x, xo) and np.array_equal(v, vo) and np.array_equal(f, fo)
+    else:
+        assert np.abs(x - xo).max() < 1e-3
+    assert samples[-1]["step"] == 100
+    assert samples[-1]["T"] == pytest.approx(o.thermo()["T"], rel=THERMO_REL if precision == "fp64" else 1e-3)
+
+
 def test_half_list_forces_and_steps():
     kw = dict(nx=8, ny=8, nz=8, half_neigh=1)
     o = lj_oracle(**kw)
