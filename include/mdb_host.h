@@ -62,6 +62,25 @@ int mdbh_read_dmp(MdbHostParams* p, const char* path, double** x, double** v, in
 int mdbh_write_dmp(const char* path, int n, const double* x, const double* v, const int* type,
     double xprd, double yprd, double zprd);
 
+/* The other input formats of readAtom (verletlist/atom.c:260-760); each sets
+ * the box, ntypes (max type + 1) and from_file like mdbh_read_dmp and returns
+ * the atom count, or -MDB_ERR_ARG where the reference would exit. Arrays are
+ * malloc'd (free with free()).
+ * readAtom_pdb (:296-410): CRYST1 box, ATOM records, zero velocities. */
+int mdbh_read_pdb(MdbHostParams* p, const char* path, double** x, double** v, int** type);
+/* readAtom_gro (:412-527): title, count, atom lines with velocities, box. */
+int mdbh_read_gro(MdbHostParams* p, const char* path, double** x, double** v, int** type);
+/* readAtom_in (:658-760): "natoms xlo xhi ylo yhi zlo zhi", then
+ * "mass x y z vx vy vz" lines (sets p->mass). */
+int mdbh_read_in(MdbHostParams* p, const char* path, double** x, double** v, int** type);
+/* readAtom (:260-294): dispatch on .pdb / .gro / .dmp / .in. */
+int mdbh_read_atoms(MdbHostParams* p, const char* path, double** x, double** v, int** type);
+/* writeAtom (-w, :762-786): "type,1.0,x,y,z,vx,vy,vz,0" per atom. */
+int mdbh_write_atoms(const char* path, int n, const double* x, const double* v,
+    const int* type);
+/* write_atoms_to_vtk_file (verletlist/vtk.c:21-71): "<base>_<timestep>.vtk". */
+int mdbh_write_vtk(const char* base, int timestep, int n, const double* x);
+
 /* Fill MdbParams for an n-atom system described by p. */
 void mdbh_mdb_params(const MdbHostParams* p, int natoms, MdbParams* out);
 

@@ -35,7 +35,7 @@ static void usage(void)
     printf("MDBench-B200: MD-Bench's Verlet-list timestep on a B200\n"
            "-p / --params <file>   parameter file (key value)\n"
            "-f <lj|eam>            force field\n"
-           "-i <file.dmp>          input atoms (LAMMPS dump)\n"
+           "-i <file>              input atoms (.pdb, .gro, .dmp or .in, as readAtom)\n"
            "-e <file>              EAM funcfl file\n"
            "-n / --nsteps <int>    timesteps\n"
            "-nx/-ny/-nz <int>      unit cells\n"
@@ -44,7 +44,7 @@ static void usage(void)
            "-s / --skin <real>     Verlet skin\n"
            "--prec <fp64|mixed|mixed_comp>  precision of the force kernels\n"
            "--hooks                run the per-hook loop instead of CUDA graphs\n"
-           "-w <file.dmp>          write the initial atoms as a dump\n");
+           "-w <file>              write the initial atoms (writeAtom's format; .dmp: a dump)\n");
 }
 
 int main(int argc, char** argv)
@@ -131,7 +131,7 @@ int main(int argc, char** argv)
     int* type = NULL;
     int n;
     if (input) {
-        n = mdbh_read_dmp(&hp, input, &x, &v, &type);
+        n = mdbh_read_atoms(&hp, input, &x, &v, &type);
         if (n < 0) {
             fprintf(stderr, "Input error: atom data was not read from %s\n", input);
             return EXIT_FAILURE;
@@ -146,7 +146,13 @@ int main(int argc, char** argv)
             return EXIT_FAILURE;
         }
     }
-    if (write_file) mdbh_write_dmp(write_file, n, x, v, type, hp.xprd, hp.yprd, hp.zprd);
+    if (write_file) {
+        const size_t wl = strlen(write_file);
+        if (wl >= 4 && !strcmp(write_file + wl - 4, ".dmp"))
+            mdbh_write_dmp(write_file, n, x, v, type, hp.xprd, hp.yprd, hp.zprd);
+        else
+            mdbh_write_atoms(write_file, n, x, v, type);
+    }
 
     MdbParams mp;
     mdbh_mdb_params(&hp, n, &mp);

@@ -335,6 +335,271 @@ int mdbh_write_dmp(const char* path, int n, const double* x, const double* v, co
     return fclose(fp) == 0 ? MDB_OK : MDB_ERR_ARG;
 }
 
+/* ---- other input formats (readAtom, verletlist/atom.c:260-760) -------------- */
+
+/* growable atom arrays of the readers */
+typedef struct {
+    int n, cap;
+    double *x, *v;
+    int* type;
+} HostAtoms;
+
+static int ha_reserve(HostAtoms* a, int need)
+{
+    if (need <= a->cap) return 1;
+    int cap = a->cap ? a->cap : 1024;
+    while (cap < need) cap *= 2;
+    double* x = realloc(a->x, sizeof(double) * 3 * (size_t)cap);
+    if (x) a->x = x;
+    double* v = realloc(a->v, sizeof(double) * 3 * (size_t)cap);
+    if (v) a->v = v;
+    int* t = realloc(a->type, sizeof(int) * (size_t)cap);
+    if (t) a->type = t;
+    if (!x || !v || !t) return 0;
+    memset(a->x + 3 * (size_t)a->cap, 0, sizeof(double) * 3 * (size_t)(cap - a->cap));
+    memset(a->v + 3 * (size_t)a->cap, 0, sizeof(double) * 3 * (size_t)(cap - a->cap));
+    memset(a->type + a->cap, 0, sizeof(int) * (size_t)(cap - a->cap));
+    a->cap = cap;
+    return 1;
+}
+
+static void ha_free(HostAtoms* a)
+{
+    free(a->x);
+    free(a->v);
+    free(a->type);
+    memset(a, 0, sizeof *a);
+}
+
+static int ha_finish(HostAtoms* a, MdbHostParams* p, double** x, double** v, int** type)
+{
+    int tmax = 0;
+    for (int i = 0; i < a->n; i++) tmax = HMAX(tmax, a->type[i]);
+    p->ntypes    = tmax + 1; /* atom->ntypes = max type + 1 */
+    p->from_file = 1;
+    *x           = a->x;
+    *v           = a->v;
+    *type        = a->type;
+    return a->n;
+}
+
+/* the readers split lines at single spaces as strtok(line, " ") does */
+static char* next_tok(char** save) { return strtok_r(NULL, " ", save); }
+
+/* type names: only argon is known (type_str2int, verletlist/atom.c:248-258) */
+static int type_of_name(const char* name)
+{
+    return (name && strncmp(name, "Ar", 2) == 0) ? 0 : -1;
+}
+
+int mdbh_read_pdb(MdbHostParams* p, const char* path, double** x, double** v, int** type)
+{
+    /* readAtom_pdb, verletlist/atom.c:296-410: CRYST1 gives the box (lower
+     * corner at the origin); ATOM lines: serial, name, residue, residue id,
+     * x y z, occupancy, charge; velocities zero */
+    FILE* fp = fopen(path, "r");
+    if (!fp) return -MDB_ERR_ARG;
+    char line[4096];
+    HostAtoms a = { 0 };
+    int bad     = 0;
+    while (!bad && fgets(line, sizeof line, fp)) {
+        char* save = NULL;
+        char* item = strtok_r(line, " ", &save);
+        if (!item) continue;
+        if (!strncmp(item, "CRYST1", 6)) {
+            char *a1 = next_tok(&save), *a2 = next_tok(&save), *a3 = next_tok(&save);
+            if (!a1 || !a2 || !a3) {
+                bad = 1;
+                break;
+            }
+            p->xprd = atof(a1);
+            p->yprd = atof(a2);
+            p->zprd = atof(a3);
+        } else if (!strncmp(item, "ATOM", 4)) {
+            char* f[9];
+            for (int k = 0; k < 9; k++) f[k] = next_tok(&save);
+            if (!f[8]) {
+                bad = 1;
+                break;
+            }
+            const int id = atoi(f[0]) - 1;
+            const int t  = type_of_name(f[1]);
+            if (id < 0 || t < 0 || !ha_reserve(&a, id + 2)) {
+                bad = 1;
+                break;
+            }
+            a.type[id] = t;
+            for (int d = 0; d < 3; d++) {
+                a.x[3 * id + d] = atof(f[4 + d]);
+                a.v[3 * id + d] = 0.0;
+            }
+            a.n++;
+        } else if (strncmp(item, "HEADER", 6) && strncmp(item, "REMARK", 6) &&
+                   strncmp(item, "MODEL", 5) && strncmp(item, "TER", 3) &&
+                   strncmp(item, "ENDMDL", 6)) {
+            bad = 1; /* the reference stops on any other record */
+        }
+    }
+    fclose(fp);
+    if (bad || a.n == 0) {
+        ha_free(&a);
+        return -MDB_ERR_ARG;
+    }
+    return ha_finish(&a, p, x, v, type);
+}
+
+int mdbh_read_gro(MdbHostParams* p, const char* path, double** x, double** v, int** type)
+{
+    /* readAtom_gro, verletlist/atom.c:412-527: title, atom count, one line per
+     * atom (residue+name, atom name, number, x y z, vx vy vz; atoms stored in
+     * file order), then the box line */
+    FILE* fp = fopen(path, "r");
+    if (!fp) return -MDB_ERR_ARG;
+    char line[4096];
+    HostAtoms a = { 0 };
+    int bad = 0, want = 0;
+    if (!fgets(line, sizeof line, fp) || !fgets(line, sizeof line, fp)) bad = 1;
+    if (!bad) {
+        char* save = NULL;
+        char* c    = strtok_r(line, " ", &save);
+        want       = c ? atoi(c) : 0;
+        if (want <= 0 || !ha_reserve(&a, want + 1)) bad = 1;
+    }
+    while (!bad && a.n < want && fgets(line, sizeof line, fp)) {
+        char* save = NULL;
+        char* f[9];
+        f[0] = strtok_r(line, " ", &save);
+        for (int k = 1; k < 9; k++) f[k] = next_tok(&save);
+        const int t = type_of_name(f[1]);
+        if (!f[8] || t < 0) {
+            bad = 1;
+            break;
+        }
+        a.type[a.n] = t;
+        for (int d = 0; d < 3; d++) {
+            a.x[3 * a.n + d] = atof(f[3 + d]);
+            a.v[3 * a.n + d] = atof(f[6 + d]);
+        }
+        a.n++;
+    }
+    if (!bad && fgets(line, sizeof line, fp)) {
+        char* save = NULL;
+        char* b0   = strtok_r(line, " ", &save);
+        char* b1   = next_tok(&save);
+        char* b2   = next_tok(&save);
+        if (b0 && b1 && b2) {
+            p->xprd = atof(b0);
+            p->yprd = atof(b1);
+            p->zprd = atof(b2);
+        }
+    }
+    fclose(fp);
+    if (bad || a.n != want) {
+        ha_free(&a);
+        return -MDB_ERR_ARG;
+    }
+    return ha_finish(&a, p, x, v, type);
+}
+
+int mdbh_read_in(MdbHostParams* p, const char* path, double** x, double** v, int** type)
+{
+    /* readAtom_in, verletlist/atom.c:658-760: "natoms xlo xhi ylo yhi zlo zhi",
+     * then "mass x y z vx vy vz" per atom (the last finite mass becomes the
+     * mass; "inf" is skipped); one atom type */
+    FILE* fp = fopen(path, "r");
+    if (!fp) return -MDB_ERR_ARG;
+    char line[4096];
+    HostAtoms a = { 0 };
+    int bad = 0, natoms = 0;
+    double b[6] = { 0 };
+    if (!fgets(line, sizeof line, fp)) bad = 1;
+    if (!bad) {
+        char* save = NULL;
+        char* c    = strtok_r(line, " ", &save);
+        natoms     = c ? atoi(c) : 0;
+        for (int k = 0; k < 6 && !bad; k++) {
+            char* t = next_tok(&save);
+            if (!t) bad = 1;
+            else b[k] = atof(t);
+        }
+        if (natoms <= 0 || !ha_reserve(&a, natoms + 1)) bad = 1;
+    }
+    for (int i = 0; i < natoms && !bad; i++) {
+        char* save = NULL;
+        if (!fgets(line, sizeof line, fp)) {
+            bad = 1;
+            break;
+        }
+        char* f[7];
+        f[0] = strtok_r(line, " ", &save);
+        for (int k = 1; k < 7; k++) f[k] = next_tok(&save);
+        if (!f[6]) {
+            bad = 1;
+            break;
+        }
+        if (strncmp(f[0], "inf", 3) != 0) p->mass = atof(f[0]);
+        a.type[i] = 0;
+        for (int d = 0; d < 3; d++) {
+            a.x[3 * i + d] = atof(f[1 + d]);
+            a.v[3 * i + d] = atof(f[4 + d]);
+        }
+        a.n++;
+    }
+    fclose(fp);
+    if (bad) {
+        ha_free(&a);
+        return -MDB_ERR_ARG;
+    }
+    p->xprd = b[1] - b[0];
+    p->yprd = b[3] - b[2];
+    p->zprd = b[5] - b[4];
+    return ha_finish(&a, p, x, v, type);
+}
+
+int mdbh_read_atoms(MdbHostParams* p, const char* path, double** x, double** v, int** type)
+{
+    /* readAtom, verletlist/atom.c:260-294: by file extension */
+    const size_t n = strlen(path);
+    if (n >= 4 && !strcmp(path + n - 4, ".pdb")) return mdbh_read_pdb(p, path, x, v, type);
+    if (n >= 4 && !strcmp(path + n - 4, ".gro")) return mdbh_read_gro(p, path, x, v, type);
+    if (n >= 4 && !strcmp(path + n - 4, ".dmp")) return mdbh_read_dmp(p, path, x, v, type);
+    if (n >= 3 && !strcmp(path + n - 3, ".in")) return mdbh_read_in(p, path, x, v, type);
+    return -MDB_ERR_ARG;
+}
+
+int mdbh_write_atoms(const char* path, int n, const double* x, const double* v, const int* type)
+{
+    /* writeAtom (-w), verletlist/atom.c:762-786: "type,1.0,x,y,z,vx,vy,vz,0" */
+    FILE* fp = fopen(path, "w");
+    if (!fp) return MDB_ERR_ARG;
+    for (int i = 0; i < n; i++)
+        fprintf(fp, "%d,%f,%f,%f,%f,%f,%f,%f,0\n", type[i], 1.0, x[3 * i], x[3 * i + 1],
+            x[3 * i + 2], v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+    return fclose(fp) == 0 ? MDB_OK : MDB_ERR_ARG;
+}
+
+int mdbh_write_vtk(const char* base, int timestep, int n, const double* x)
+{
+    /* write_atoms_to_vtk_file, verletlist/vtk.c:21-71: "<base>_<step>.vtk",
+     * legacy ASCII unstructured grid of vertex cells, unit masses */
+    char path[4096];
+    snprintf(path, sizeof path, "%s_%d.vtk", base, timestep);
+    FILE* fp = fopen(path, "wb");
+    if (!fp) return MDB_ERR_ARG;
+    fprintf(fp, "# vtk DataFile Version 2.0\nParticle data\nASCII\nDATASET UNSTRUCTURED_GRID\n");
+    fprintf(fp, "POINTS %d double\n", n);
+    for (int i = 0; i < n; i++)
+        fprintf(fp, "%.4f %.4f %.4f\n", x[3 * i], x[3 * i + 1], x[3 * i + 2]);
+    fprintf(fp, "\n\nCELLS %d %d\n", n, 2 * n);
+    for (int i = 0; i < n; i++) fprintf(fp, "1 %d\n", i);
+    fprintf(fp, "\n\nCELL_TYPES %d\n", n);
+    for (int i = 0; i < n; i++) fprintf(fp, "1\n");
+    fprintf(fp, "\n\nPOINT_DATA %d\nSCALARS mass double\nLOOKUP_TABLE default\n", n);
+    for (int i = 0; i < n; i++) fprintf(fp, "1.0\n");
+    fprintf(fp, "\n\n");
+    return fclose(fp) == 0 ? MDB_OK : MDB_ERR_ARG;
+}
+
 void mdbh_mdb_params(const MdbHostParams* p, int natoms, MdbParams* o)
 {
     memset(o, 0, sizeof *o);

@@ -103,6 +103,8 @@ CP_EXPORTS = [
 HOST_EXPORTS = [
     "mdbh_defaults", "mdbh_read_params", "mdbh_read_types", "mdbh_apply_eam",
     "mdbh_finalize", "mdbh_create_fcc", "mdbh_read_dmp", "mdbh_write_dmp", "mdbh_mdb_params",
+    "mdbh_read_pdb", "mdbh_read_gro", "mdbh_read_in", "mdbh_read_atoms", "mdbh_write_atoms",
+    "mdbh_write_vtk",
 ]
 
 _lib = None
@@ -194,6 +196,12 @@ def load():
         "mdbh_finalize": ([hp], None),
         "mdbh_create_fcc": ([hp, pd, pd, pi], ip),
         "mdbh_read_dmp": ([hp, C.c_char_p, pd, pd, pi], ip),
+        "mdbh_read_pdb": ([hp, C.c_char_p, pd, pd, pi], ip),
+        "mdbh_read_gro": ([hp, C.c_char_p, pd, pd, pi], ip),
+        "mdbh_read_in": ([hp, C.c_char_p, pd, pd, pi], ip),
+        "mdbh_read_atoms": ([hp, C.c_char_p, pd, pd, pi], ip),
+        "mdbh_write_atoms": ([C.c_char_p, ip, _dp, _dp, _ip], ip),
+        "mdbh_write_vtk": ([C.c_char_p, ip, ip, _dp], ip),
         "mdbh_write_dmp": ([C.c_char_p, ip, _dp, _dp, _ip, C.c_double, C.c_double,
                             C.c_double], ip),
         "mdbh_mdb_params": ([hp, ip, C.POINTER(MdbParams)], None),
@@ -266,6 +274,37 @@ def read_dmp(hp, path):
     lib.mdbh_finalize(C.byref(hp))
     return (_take(xp, 3 * n, np.float64, (n, 3)), _take(vp, 3 * n, np.float64, (n, 3)),
             _take(tp, n, np.int32, (n,)))
+
+
+def read_atoms(hp, path):
+    """readAtom: .pdb / .gro / .dmp / .in by extension; sets hp's box, ntypes,
+    from_file (and mass for .in); returns (x, v, type)."""
+    lib = load()
+    xp, vp, tp = C.POINTER(C.c_double)(), C.POINTER(C.c_double)(), C.POINTER(C.c_int)()
+    n = lib.mdbh_read_atoms(C.byref(hp), path.encode(), C.byref(xp), C.byref(vp), C.byref(tp))
+    if n < 0:
+        raise MdbError(f"cannot read atoms from {path}")
+    lib.mdbh_finalize(C.byref(hp))
+    return (_take(xp, 3 * n, np.float64, (n, 3)), _take(vp, 3 * n, np.float64, (n, 3)),
+            _take(tp, n, np.int32, (n,)))
+
+
+def write_atoms(path, x, v, t):
+    """writeAtom (-w): one "type,1.0,x,y,z,vx,vy,vz,0" line per atom."""
+    rc = load().mdbh_write_atoms(path.encode(), len(t),
+                                 np.ascontiguousarray(x, np.float64).ravel(),
+                                 np.ascontiguousarray(v, np.float64).ravel(),
+                                 np.ascontiguousarray(t, np.int32))
+    if rc:
+        raise MdbError(f"cannot write {path}")
+
+
+def write_vtk(base, timestep, x):
+    """write_atoms_to_vtk_file: <base>_<timestep>.vtk."""
+    x = np.ascontiguousarray(x, np.float64).ravel()
+    rc = load().mdbh_write_vtk(base.encode(), int(timestep), len(x) // 3, x)
+    if rc:
+        raise MdbError(f"cannot write {base}_{timestep}.vtk")
 
 
 def write_dmp(path, x, v, t, box):

@@ -117,3 +117,110 @@ def test_param_and_types_files(tmp_path):
     assert hp.cutneigh == 2.0 + 0.2 and hp.dtforce == 0.5 * 0.001
     (tmp_path / "bad.conf").write_text(f"types_file {tmp_path / 'types.dat'}\nepsilon 2\n")
     assert mdb.load().mdbh_read_params(mdb.host_params(), str(tmp_path / "bad.conf").encode())
+
+
+# ---- the other input formats of readAtom, and the writers ----------------------
+
+def _argon_state(n=400, box=(16.0, 17.5, 15.25), seed=3):
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(0.0, 1.0, (n, 3)) * np.array(box)
+    v = rng.normal(0.0, 0.3, (n, 3))
+    return np.round(x, 3), np.round(v, 4), box
+
+
+def _write_gro(path, x, v, box):
+    with open(path, "w") as f:
+        f.write("Liquid argon test state\n")
+        f.write(f" {len(x)}\n")
+        for i, (p, q) in enumerate(zip(x, v)):
+            f.write(f"{i + 1:5d}Ar      Ar {i + 1:4d} {p[0]:7.3f} {p[1]:7.3f} {p[2]:7.3f}"
+                    f" {q[0]:7.4f} {q[1]:7.4f} {q[2]:7.4f}\n")
+        f.write(f" {box[0]:9.5f} {box[1]:9.5f} {box[2]:9.5f}\n")
+
+
+def _write_pdb(path, x, box):
+    with open(path, "w") as f:
+        f.write("HEADER    test\nREMARK    argon\n")
+        f.write(f"CRYST1 {box[0]:.3f} {box[1]:.3f} {box[2]:.3f} 90.00 90.00 90.00 P 1 1\n")
+        f.write("MODEL 1\n")
+        for i, p in enumerate(x):
+            f.write(f"ATOM {i + 1} Ar AR {i + 1} {p[0]:.3f} {p[1]:.3f} {p[2]:.3f} 1.00 0.00\n")
+        f.write("TER\nENDMDL\n")
+
+
+def _write_in(path, x, v, box, mass=39.94):
+    with open(path, "w") as f:
+        f.write(f"{len(x)} 0.0 {box[0]} 0.0 {box[1]} 0.0 {box[2]}\n")
+        for k, (p, q) in enumerate(zip(x, v)):
+            m = "inf" if k == 0 else f"{mass}"
+            f.write(f"{m} {p[0]} {p[1]} {p[2]} {q[0]} {q[1]} {q[2]}\n")
+
+
+@pytest.mark.parametrize("ext", ["gro", "pdb", "in"])
+def test_readers_parse_formats(tmp_path, ext):
+    x, v, box = _argon_state()
+    path = str(tmp_path / f"argon.{ext}")
+    {"gro": lambda: _write_gro(path, x, v, box), "pdb": lambda: _write_pdb(path, x, box),
+     "in": lambda: _write_in(path, x, v, box)}[ext]()
+    hp = mdb.host_params()
+    xr, vr, tr = mdb.read_atoms(hp, path)
+    assert xr.shape == x.shape and np.allclose(xr, x, atol=5e-4)
+    if ext == "pdb":
+        assert np.all(vr == 0.0)
+    else:
+        assert np.allclose(vr, v, atol=5e-5)
+    assert set(tr.tolist()) == {0} and hp.ntypes == 1 and hp.from_file == 1
+    assert (hp.xprd, hp.yprd, hp.zprd) == pytest.approx(box, abs=1e-3)
+    if ext == "in":
+        assert hp.mass == pytest.approx(39.94)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference not compiled here")
+@pytest.mark.parametrize("ext", ["gro", "pdb", "in"])
+def test_readers_match_reference_readers(tmp_path, ext):
+    """The same file read by the reference's readAtom (compiled from its
+    sources) and by mdbh_read_atoms: identical positions, velocities, types,
+    box (and mass)."""
+    x, v, box = _argon_state(n=300, box=(14.0, 14.5, 15.0))
+    path = str(tmp_path / f"argon.{ext}")
+    {"gro": lambda: _write_gro(path, x, v, box), "pdb": lambda: _write_pdb(path, x, box),
+     "in": lambda: _write_in(path, x, v, box)}[ext]()
+    hp = mdb.host_params()
+    xr, vr, tr = mdb.read_atoms(hp, path)
+    r = O.RefVL(input_file=path)
+    assert r.nlocal == len(tr)
+    xo, vo, _, to = r.atoms()
+    assert np.array_equal(xr, xo) and np.array_equal(vr, vo) and np.array_equal(tr, to)
+    d = r.params()
+    assert (hp.xprd, hp.yprd, hp.zprd) == (d["xprd"], d["yprd"], d["zprd"])
+    if ext == "in":
+        assert hp.mass == d["mass"]
+
+
+def test_readers_reject_bad_input(tmp_path):
+    bad = tmp_path / "bad.pdb"
+    bad.write_text("CRYST1 10 10 10\nATOM 1 Xe XE 1 1.0 1.0 1.0 1.00 0.00\n")
+    with pytest.raises(mdb.MdbError):
+        mdb.read_atoms(mdb.host_params(), str(bad))
+    short = tmp_path / "short.gro"
+    short.write_text("t\n 3\n    1Ar      Ar    1   1.0 1.0 1.0 0 0 0\n")
+    with pytest.raises(mdb.MdbError):
+        mdb.read_atoms(mdb.host_params(), str(short))
+    with pytest.raises(mdb.MdbError):
+        mdb.read_atoms(mdb.host_params(), str(tmp_path / "atoms.xyz"))
+
+
+def test_atom_and_vtk_writers(tmp_path):
+    x, v, box = _argon_state(n=5)
+    t = np.array([0, 1, 0, 2, 0], dtype=np.int32)
+    mdb.write_atoms(str(tmp_path / "w.csv"), x, v, t)
+    lines = (tmp_path / "w.csv").read_text().splitlines()
+    assert len(lines) == 5
+    f = lines[3].split(",")
+    assert f[0] == "2" and f[1] == "1.000000" and f[-1] == "0" and len(f) == 9
+    assert float(f[2]) == pytest.approx(x[3, 0], abs=1e-6)
+    mdb.write_vtk(str(tmp_path / "traj"), 7, x)
+    vtk = (tmp_path / "traj_7.vtk").read_text().splitlines()
+    assert vtk[0] == "# vtk DataFile Version 2.0" and vtk[4] == "POINTS 5 double"
+    assert "CELLS 5 10" in vtk and "CELL_TYPES 5" in vtk and "POINT_DATA 5" in vtk
+    assert vtk[5] == "%.4f %.4f %.4f" % tuple(x[0])
