@@ -34,6 +34,7 @@ sys.path.insert(0, os.path.join(ROOT, "md-bench_b200"))
 LJ_CELLS = 64
 C5_CELLS = 128
 C4_REPLICAS = 256
+STUB_ATOMS = 1 << 20
 EAM_CELLS = 32
 EAM_A = 3.615
 EAM_T = 1600.0
@@ -55,7 +56,7 @@ def parse():
     ap.add_argument("--no-variants", action="store_true", help="headline only")
     ap.add_argument("--profile", choices=[f"{k}_{p}{h}" for k in ("lj", "eam", "cp44", "cp48")
                                           for p in ("mixed", "fp64") for h in ("", "_half")]
-                    + ["c5_mixed", "c5_fp64", "c4_mixed"],
+                    + ["c5_mixed", "c5_fp64", "c4_mixed", "stub"],
                     help="run one variant only (W+K bench steps + force timing), for ncu")
     ap.add_argument("--cells", type=int, default=None, help="fcc cells per side (profiling)")
     ap.add_argument("--tune", default=None, help="key=value[,key=value] cluster-pair tuning")
@@ -230,6 +231,29 @@ def measure(torch, mdb, kind, precision, args, device, half=0, steps=None):
                 nsteps=nsteps, th0=th0, mean_list=mean_list,
                 value=nat * every * steps / secs, ms_per_step=1e3 * secs / steps,
                 init=(x, v, t))
+
+
+def stub_bench(torch, mdb, device, natoms=STUB_ATOMS, nneighs=76, reps=20):
+    """The stub gather benchmark (verletlist/main-stub.c) on the GPU: the FP64
+    full-list LJ force alone on synthetic lists (seq: the next 76 atoms, fix:
+    the same 76 atoms for all, rand: 76 random atoms), atoms on a diagonal,
+    every listed pair inside the cutoff. Reports the reference stub's figure,
+    atom updates per second, with ns per neighbour and the gather rate."""
+    out = {}
+    for pattern in ("seq", "fix", "rand"):
+        x, v, t, num, nb = mdb.stub_system(natoms, pattern, nneighs)
+        s, _, _ = mdb.stub_context(x, v, t, num, nb, device=device)
+        secs = force_kernel_time(torch, s, reps=reps)
+        s.close()
+        # list entry + the gathered double4 position per neighbour, plus per
+        # atom its own position, row length and force
+        bytes_per_atom = nneighs * (4 + 32) + 32 + 4 + 24
+        out[pattern] = {"atom_updates_per_s": natoms / secs,
+                        "ns_per_neighbor": secs / (natoms * nneighs) * 1e9,
+                        "force_us": secs * 1e6,
+                        "gather_gb_per_s": natoms * bytes_per_atom / secs / 1e9}
+    return {"natoms": natoms, "nneighs": nneighs, "precision": "fp64", "list": "full",
+            "patterns": out}
 
 
 def c4_specs(count):
@@ -520,6 +544,10 @@ def main():
         if dist:
             dist.barrier()
 
+    if args.profile == "stub":
+        print(json.dumps(dict(profile=args.profile, **stub_bench(torch, mdb, local))),
+              flush=True)
+        return
     if args.profile == "c4_mixed":
         print(json.dumps(dict(profile=args.profile, **c4_ensemble(torch, mdb, args, local))),
               flush=True)
@@ -612,6 +640,7 @@ def main():
                                      var[k.replace("_mixed", "_fp64")]["value"]
                                      for k in var if "_mixed" in k}}
         var["c4_ensemble_mixed"] = c4_ensemble(torch, mdb, args, local)
+        var["stub_gather_fp64"] = stub_bench(torch, mdb, local)
 
     # end to end from the state the timed run reached (a liquid, as in use)
     e2 = e2e(torch, s, s.atoms(), max(args.steps // 5, 3), 20)

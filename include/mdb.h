@@ -155,6 +155,13 @@ int mdb_sort_atoms(MdbCtx* ctx);
  * 0 (the default, as SORT_ATOMS ?= false) disables. */
 int mdb_set_resort(MdbCtx* ctx, int resort_every);
 
+/* A caller-made neighbour list (row-major, row i = numneigh[i] local atom
+ * indices, leading dimension ld) for the force kernels, with no ghosts, as the
+ * stub gather benchmark feeds computeForce (verletlist/main-stub.c:60-113,
+ * 250-262). Valid until the next list build. FP64 contexts only (the mixed
+ * kernels need the cell codes of a built list). */
+int mdb_set_neighbor_list(MdbCtx* ctx, const int* numneigh, const int* neighbors, int ld);
+
 /* setup tail of verletlist/main.c:96-111 for atoms already set:
  * setupPbc, updatePbc, buildNeighbor, computeForce. */
 int mdb_setup(MdbCtx* ctx);

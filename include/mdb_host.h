@@ -81,6 +81,21 @@ int mdbh_write_atoms(const char* path, int n, const double* x, const double* v,
 /* write_atoms_to_vtk_file (verletlist/vtk.c:21-71): "<base>_<timestep>.vtk". */
 int mdbh_write_vtk(const char* base, int timestep, int n, const double* x);
 
+/* The stub gather benchmark (verletlist/main-stub.c): synthetic atoms and
+ * neighbour patterns that feed the force kernels alone. Atoms: atom i at
+ * (i, i, i) * 1e-5, at rest, type rand() % ntypes after srand(seed) (1: a fresh
+ * process, as the reference). Patterns (createNeighbors, :60-113), row-major
+ * rows of nneighs * nreps entries: SEQ the atoms after i (cyclically; the
+ * reference's last atom points one past the end), FIX atoms 0..nneighs-1, RAND
+ * distinct random atoms other than i (rand(), continuing the atoms' stream),
+ * each row repeated nreps times. */
+#define MDBH_STUB_SEQ  0
+#define MDBH_STUB_FIX  1
+#define MDBH_STUB_RAND 2
+int mdbh_stub_atoms(int natoms, int ntypes, unsigned seed, double* x, double* v, int* type);
+int mdbh_stub_neighbors(int natoms, int pattern, int nneighs, int nreps, int* numneigh,
+    int* neighbors);
+
 /* Fill MdbParams for an n-atom system described by p. */
 void mdbh_mdb_params(const MdbHostParams* p, int natoms, MdbParams* out);
 

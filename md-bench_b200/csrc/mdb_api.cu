@@ -549,7 +549,8 @@ extern "C" int mdb_set_atoms(MdbCtx* ctx, int nlocal, const double* x, const dou
         double dens  = vol > 0 ? nlocal / vol : 0;
         double c     = ctx->p.cutneigh;
         double shell = (ctx->p.xprd + 2 * c) * (ctx->p.yprd + 2 * c) * (ctx->p.zprd + 2 * c) - vol;
-        int gcap     = (int)std::min(2.0e9, 1.25 * dens * shell + 1024);
+        // an atom has at most 7 images (3 faces, 3 edges, 1 corner)
+        int gcap = (int)std::min(7.0 * nlocal + 1024, 1.25 * dens * shell + 1024);
         ctx->x       = nullptr;
         if ((rc = alloc_ghost_sized(ctx, gcap)) != MDB_OK) return rc;
         if ((rc = alloc_list(ctx, ctx->maxneighs)) != MDB_OK) return rc;
@@ -1025,6 +1026,40 @@ static void enq_plain_step(MdbCtx* ctx)
     enq_final_initial(ctx);
     enq_ghost_update(ctx);
     enq_force(ctx, false);
+}
+
+extern "C" int mdb_set_neighbor_list(MdbCtx* ctx, const int* numneigh, const int* neighbors,
+    int ld)
+{
+    NEED_ATOMS();
+    if (!numneigh || !neighbors || ld < 1) return MDB_ERR_ARG;
+    if (ctx->mixed) return fail(ctx, MDB_ERR_ARG, "caller lists need an FP64 context");
+    const int n = ctx->nlocal;
+    int maxn    = 0;
+    for (int i = 0; i < n; i++) {
+        if (numneigh[i] < 0 || numneigh[i] > ld) return fail(ctx, MDB_ERR_ARG, "row length");
+        maxn = std::max(maxn, numneigh[i]);
+        for (int k = 0; k < numneigh[i]; k++) {
+            const int j = neighbors[(size_t)i * ld + k];
+            if (j < 0 || j >= n) return fail(ctx, MDB_ERR_ARG, "entry is not a local atom");
+        }
+    }
+    CK(cudaSetDevice(ctx->dev));
+    if (maxn > ctx->maxneighs) {
+        int rc = alloc_list(ctx, maxn);
+        if (rc) return rc;
+    }
+    // k-major on the device: entry k of atom i at k * ld + i
+    std::vector<int> all((size_t)ctx->maxneighs * ctx->ld, 0);
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < numneigh[i]; k++)
+            all[(size_t)k * ctx->ld + i] = neighbors[(size_t)i * ld + k];
+    CK(cudaStreamSynchronize(ctx->s));
+    CK(cudaMemcpy(ctx->neighbors, all.data(), sizeof(int) * all.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->numneigh, numneigh, sizeof(int) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemset(ctx->counters + CNT_NGHOST, 0, sizeof(int)));
+    ctx->have_ghosts = ctx->have_list = true;
+    return MDB_OK;
 }
 
 extern "C" int mdb_sort_atoms(MdbCtx* ctx)

@@ -600,6 +600,60 @@ int mdbh_write_vtk(const char* base, int timestep, int n, const double* x)
     return fclose(fp) == 0 ? MDB_OK : MDB_ERR_ARG;
 }
 
+/* ---- the stub gather benchmark (verletlist/main-stub.c) --------------------- */
+
+int mdbh_stub_atoms(int natoms, int ntypes, unsigned seed, double* x, double* v, int* type)
+{
+    /* main-stub.c:221-234: atom i at (i, i, i) * 1e-5 at rest, type rand() %
+     * ntypes from the process's rand() stream (a fresh process: seed 1) */
+    if (natoms < 1 || ntypes < 1 || !x || !v || !type) return MDB_ERR_ARG;
+    srand(seed);
+    for (int i = 0; i < natoms; i++) {
+        type[i] = rand() % ntypes;
+        for (int d = 0; d < 3; d++) {
+            x[3 * i + d] = (double)i * 0.00001;
+            v[3 * i + d] = 0.0;
+        }
+    }
+    return MDB_OK;
+}
+
+int mdbh_stub_neighbors(int natoms, int pattern, int nneighs, int nreps, int* numneigh,
+    int* neighbors)
+{
+    /* createNeighbors, main-stub.c:60-113, row-major rows of nneighs * nreps:
+     * seq: the nneighs atoms after i (cyclically), fix: atoms 0 .. nneighs-1,
+     * rand: distinct random atoms other than i, drawn from rand() (continuing
+     * the stream of mdbh_stub_atoms); the row is then repeated nreps times. */
+    if (natoms < 1 || nneighs < 1 || nreps < 1 || !numneigh || !neighbors) return MDB_ERR_ARG;
+    if (pattern < MDBH_STUB_SEQ || pattern > MDBH_STUB_RAND) return MDB_ERR_ARG;
+    if (pattern == MDBH_STUB_RAND && natoms <= nneighs) return MDB_ERR_ARG;
+    if (pattern == MDBH_STUB_FIX && natoms < nneighs) return MDB_ERR_ARG;
+    const size_t row = (size_t)nneighs * nreps;
+    for (int i = 0; i < natoms; i++) {
+        int* r = neighbors + (size_t)i * row;
+        for (int k = 0; k < nneighs; k++) {
+            int j;
+            if (pattern == MDBH_STUB_SEQ) {
+                j = (int)(((long long)i + 1 + k) % natoms);
+            } else if (pattern == MDBH_STUB_FIX) {
+                j = k;
+            } else {
+                int again;
+                do {
+                    j     = rand() % natoms;
+                    again = j == i;
+                    for (int l = 0; l < k && !again; l++) again = r[l] == j;
+                } while (again);
+            }
+            r[k] = j;
+        }
+        for (int q = 1; q < nreps; q++) memcpy(r + (size_t)q * nneighs, r, sizeof(int) * nneighs);
+        numneigh[i] = (int)row;
+    }
+    return MDB_OK;
+}
+
 void mdbh_mdb_params(const MdbHostParams* p, int natoms, MdbParams* o)
 {
     memset(o, 0, sizeof *o);

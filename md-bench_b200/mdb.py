@@ -83,7 +83,7 @@ EXPORTS = [
     "mdb_initial_integrate", "mdb_final_integrate", "mdb_thermo", "mdb_setup", "mdb_run", "mdb_get_counts",
     "mdb_get_positions_all", "mdb_get_ghosts", "mdb_get_neighbor_list",
     "mdb_get_bin_geometry", "mdb_get_eam_fp", "mdb_launch_count", "mdb_kinetic_sum_noalloc",
-    "mdb_sort_atoms", "mdb_set_resort",
+    "mdb_sort_atoms", "mdb_set_resort", "mdb_set_neighbor_list",
 ]
 # every symbol include/mdb_cp.h declares
 CP_EXPORTS = [
@@ -104,7 +104,7 @@ HOST_EXPORTS = [
     "mdbh_defaults", "mdbh_read_params", "mdbh_read_types", "mdbh_apply_eam",
     "mdbh_finalize", "mdbh_create_fcc", "mdbh_read_dmp", "mdbh_write_dmp", "mdbh_mdb_params",
     "mdbh_read_pdb", "mdbh_read_gro", "mdbh_read_in", "mdbh_read_atoms", "mdbh_write_atoms",
-    "mdbh_write_vtk",
+    "mdbh_write_vtk", "mdbh_stub_atoms", "mdbh_stub_neighbors",
 ]
 
 _lib = None
@@ -150,6 +150,7 @@ def load():
                  "mdb_sort_atoms"):
         sig[name] = ([vp], ip)
     sig["mdb_set_resort"] = ([vp, ip], ip)
+    sig["mdb_set_neighbor_list"] = ([vp, _ip, _ip, ip], ip)
     sig.update({
         "mdb_cp_create": ([C.POINTER(MdbParams), ip, ip, C.POINTER(vp)], ip),
         "mdb_cp_destroy": ([vp], ip),
@@ -202,6 +203,8 @@ def load():
         "mdbh_read_atoms": ([hp, C.c_char_p, pd, pd, pi], ip),
         "mdbh_write_atoms": ([C.c_char_p, ip, _dp, _dp, _ip], ip),
         "mdbh_write_vtk": ([C.c_char_p, ip, ip, _dp], ip),
+        "mdbh_stub_atoms": ([ip, ip, C.c_uint, _dp, _dp, _ip], ip),
+        "mdbh_stub_neighbors": ([ip, ip, ip, ip, _ip, _ip], ip),
         "mdbh_write_dmp": ([C.c_char_p, ip, _dp, _dp, _ip, C.c_double, C.c_double,
                             C.c_double], ip),
         "mdbh_mdb_params": ([hp, ip, C.POINTER(MdbParams)], None),
@@ -305,6 +308,42 @@ def write_vtk(base, timestep, x):
     rc = load().mdbh_write_vtk(base.encode(), int(timestep), len(x) // 3, x)
     if rc:
         raise MdbError(f"cannot write {base}_{timestep}.vtk")
+
+
+STUB_PATTERNS = {"seq": 0, "fix": 1, "rand": 2}
+
+
+def stub_system(natoms, pattern="seq", nneighs=76, nreps=1, ntypes=4, seed=1):
+    """The stub gather benchmark's input (verletlist/main-stub.c): atoms on a
+    diagonal at rest and a synthetic list. Returns (x, v, type, numneigh,
+    neighbors) with neighbors of shape (natoms, nneighs * nreps)."""
+    lib = load()
+    x = np.zeros((natoms, 3)); v = np.zeros((natoms, 3))
+    t = np.zeros(natoms, dtype=np.int32)
+    if lib.mdbh_stub_atoms(natoms, ntypes, seed, x.reshape(-1), v.reshape(-1), t):
+        raise MdbError("mdbh_stub_atoms: bad arguments")
+    nn = np.zeros(natoms, dtype=np.int32)
+    nb = np.zeros((natoms, nneighs * nreps), dtype=np.int32)
+    if lib.mdbh_stub_neighbors(natoms, STUB_PATTERNS[pattern], nneighs, nreps, nn,
+                               nb.reshape(-1)):
+        raise MdbError("mdbh_stub_neighbors: bad arguments")
+    return x, v, t, nn, nb
+
+
+def stub_context(x, v, t, numneigh, neighbors, half=0, ntypes=4, device=0):
+    """An FP64 LJ :class:`System` holding a stub list. The reference's stub sets
+    the cutoff to 1e6 so that every listed pair interacts; here the cutoff is
+    just above the diagonal's length (the same pairs interact) and the box its
+    length, which keeps the bin grid small."""
+    n = len(t)
+    box = max(n * 1e-5, 1.0)
+    cut = np.sqrt(3.0) * box * 1.001 + 1.0
+    s = System(xprd=box, yprd=box, zprd=box, cutforce=cut, cutneigh=cut, dt=0.005,
+               dtforce=0.0025, natoms=n, half_neigh=half, bin_rule=BINS_FILE, ntypes=ntypes,
+               maxneighs=neighbors.shape[1], device=device)
+    s.set_atoms(x, v, t)
+    s.set_neighbor_list(numneigh, neighbors)
+    return s, box, cut
 
 
 def write_dmp(path, x, v, t, box):
@@ -500,6 +539,12 @@ class System:
 
     def update_atoms_pbc(self):
         self._ck(self.lib.mdb_update_atoms_pbc(self.h), "mdb_update_atoms_pbc")
+
+    def set_neighbor_list(self, numneigh, neighbors):
+        """A caller's list of locals (FP64 contexts; the stub benchmark)."""
+        nb = np.ascontiguousarray(neighbors, dtype=np.int32)
+        self._ck(self.lib.mdb_set_neighbor_list(self.h, np.ascontiguousarray(
+            numneigh, dtype=np.int32), nb.reshape(-1), nb.shape[1]), "mdb_set_neighbor_list")
 
     def sort_atoms(self):
         """sortAtom: locals bin by bin; ghosts and lists must be rebuilt."""

@@ -1028,6 +1028,22 @@ void orc_sort_atoms(OrcSys* s)
 
 void orc_set_resort(OrcSys* s, int every) { s->resort_every = every > 0 ? every : 0; }
 
+void orc_set_list(OrcSys* s, const int* numneigh, const int* neighbors, int ld)
+{
+    /* the stub benchmark's createNeighbors (verletlist/main-stub.c:60-113)
+     * hands computeForce a list of locals with no ghosts */
+    const int n = s->nlocal;
+    s->nghost   = 0;
+    free(s->numneigh);
+    free(s->neighbors);
+    s->numneigh  = orc_alloc(sizeof(int) * (size_t)(n + 1));
+    s->neighbors = orc_alloc(sizeof(int) * (size_t)n * (size_t)ld + 1);
+    s->maxneighs = ld;
+    s->listcap   = n * ld;
+    memcpy(s->numneigh, numneigh, sizeof(int) * (size_t)n);
+    memcpy(s->neighbors, neighbors, sizeof(int) * (size_t)n * (size_t)ld);
+}
+
 void orc_step(OrcSys* s, int n)
 {
     /* verletlist/main.c:371-419 (no MPI: forward/reverse reduce to updatePbc);

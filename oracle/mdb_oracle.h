@@ -72,6 +72,9 @@ void orc_step(OrcSys* s, int n);
  * resort period used by orc_step (0: never). */
 void orc_sort_atoms(OrcSys* s);
 void orc_set_resort(OrcSys* s, int every);
+/* A caller's list (row-major, ld entries per row) of locals, no ghosts: the
+ * stub gather benchmark's input to computeForce. */
+void orc_set_list(OrcSys* s, const int* numneigh, const int* neighbors, int ld);
 
 /* Thermo of the current state: T and P as the reference prints them,
  * KE, PE (from the last force call) and E = KE + PE, all totals. */

@@ -73,6 +73,7 @@ def _load():
         lib.orc_compute_force.restype = C.c_double
         lib.orc_step.argtypes = [C.c_void_p, C.c_int]
         lib.orc_set_resort.argtypes = [C.c_void_p, C.c_int]
+        lib.orc_set_list.argtypes = [C.c_void_p, _ip, _ip, C.c_int]
         lib.orc_load_eam.argtypes = [C.c_void_p, C.c_char_p]
         lib.orc_load_eam.restype = C.c_int
         lib.orc_eam_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_int)] * 4 + \
@@ -159,6 +160,12 @@ class Oracle:
 
     def set_resort(self, every):
         self.lib.orc_set_resort(self.h, every)
+
+    def set_list(self, numneigh, neighbors):
+        """A caller's list of locals (rows of neighbors.shape[1] entries)."""
+        nb = np.ascontiguousarray(neighbors, dtype=np.int32)
+        self.lib.orc_set_list(self.h, np.ascontiguousarray(numneigh, dtype=np.int32), nb,
+                              nb.shape[1])
 
     def reghost(self):
         """setupPbc + updatePbc + buildNeighbor without the wrap."""

@@ -357,3 +357,41 @@ def test_launches_are_counted():
     n0 = s.launches
     s.run(20)
     assert s.launches - n0 >= 19 * 4
+
+
+# ---- the stub gather benchmark (verletlist/main-stub.c) -------------------------
+
+@pytest.mark.parametrize("pattern", ["seq", "fix", "rand"])
+@pytest.mark.parametrize("half", [0, 1])
+def test_stub_list_forces(pattern, half):
+    """Forces on the stub's synthetic lists: bit-identical to the oracle with
+    full lists, within the atomics tolerance with half lists."""
+    x, v, t, num, nb = mdb.stub_system(3000, pattern, 76, nreps=2)
+    s, box, cut = mdb.stub_context(x, v, t, num, nb, half=half)
+    s.compute_force()
+    o = O.Oracle(nx=1, ny=1, nz=1, from_file=1, xprd=box, yprd=box, zprd=box, cutforce=cut,
+                 skin=0.0, half_neigh=half)
+    o.set_atoms(x, v, t)
+    o.set_list(num, nb)
+    o.force()
+    f, fo = s.atoms()[2], o.atoms()[2]
+    # the fix pattern lists atom i itself for i < 76 (as the reference's
+    # does): those forces are NaN on both sides
+    if half:
+        ok = np.isfinite(fo).all(axis=1)
+        assert np.array_equal(np.isfinite(f).all(axis=1), ok)
+        scale = np.abs(fo[ok]).max()
+        assert np.abs(f[ok] - fo[ok]).max() <= 1e-12 * scale
+    else:
+        assert np.array_equal(f, fo, equal_nan=True)
+    s.close()
+
+
+def test_stub_list_rejected_for_mixed_and_bad_entries():
+    x, v, t, num, nb = mdb.stub_system(500, "seq", 8)
+    s, _, _ = mdb.stub_context(x, v, t, num, nb)
+    bad = nb.copy()
+    bad[3, 2] = 500
+    with pytest.raises(mdb.MdbError):
+        s.set_neighbor_list(num, bad)
+    s.close()

@@ -224,3 +224,48 @@ def test_atom_and_vtk_writers(tmp_path):
     assert vtk[0] == "# vtk DataFile Version 2.0" and vtk[4] == "POINTS 5 double"
     assert "CELLS 5 10" in vtk and "CELL_TYPES 5" in vtk and "POINT_DATA 5" in vtk
     assert vtk[5] == "%.4f %.4f %.4f" % tuple(x[0])
+
+
+# ---- the stub gather benchmark's inputs (verletlist/main-stub.c) ----------------
+
+def test_stub_patterns():
+    n, nn = 300, 16
+    x, v, t, num, nb = mdb.stub_system(n, "seq", nn, nreps=2)
+    assert np.all(num == 2 * nn) and nb.shape == (n, 2 * nn)
+    i = np.arange(n)[:, None]
+    assert np.array_equal(nb[:, :nn], (i + 1 + np.arange(nn)[None, :]) % n)
+    assert np.array_equal(nb[:, nn:], nb[:, :nn])
+    assert np.array_equal(x[:, 0], np.arange(n) * 0.00001) and np.all(v == 0)
+    assert t.min() >= 0 and t.max() < 4
+    _, _, _, _, fix = mdb.stub_system(n, "fix", nn)
+    assert np.all(fix == np.arange(nn)[None, :])
+    _, _, t1, _, rnd = mdb.stub_system(n, "rand", nn)
+    assert np.all((rnd >= 0) & (rnd < n)) and np.all(rnd != i)
+    assert all(len(set(r)) == nn for r in rnd.tolist())
+    _, _, t2, _, rnd2 = mdb.stub_system(n, "rand", nn)
+    assert np.array_equal(rnd, rnd2) and np.array_equal(t1, t2)  # seeded
+    with pytest.raises(mdb.MdbError):
+        mdb.stub_system(10, "rand", 16)  # the reference's own precondition
+
+
+def test_stub_force_oracle_matches_direct_sum():
+    """The oracle's computeForceLJFullNeigh on a stub list equals a direct
+    double-precision sum of the same pairs, to 1e-13 of the sum of the terms'
+    magnitudes (the pair terms span many orders and cancel)."""
+    n, nn = 200, 12
+    x, v, t, num, nb = mdb.stub_system(n, "rand", nn)
+    o = O.Oracle(nx=1, ny=1, nz=1, from_file=1, xprd=2.0, yprd=2.0, zprd=2.0, cutforce=10.0,
+                 skin=0.0)
+    o.set_atoms(x, v, t)
+    o.set_list(num, nb)
+    o.force()
+    f = o.atoms()[2]
+    d = x[:, None, :] - x[nb]
+    r2 = np.sum(d * d, axis=2)
+    sr2 = 1.0 / r2
+    sr6 = sr2 ** 3
+    fr = 48.0 * sr6 * (sr6 - 0.5) * sr2
+    terms = d * fr[:, :, None]
+    fd = np.sum(terms, axis=1)
+    scale = np.sum(np.abs(terms), axis=1)
+    assert np.all(np.abs(f - fd) <= 1e-13 * scale)
