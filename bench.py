@@ -325,13 +325,29 @@ def run_ensemble(torch, mdb, members, args, every=20):
     return secs, launches, np.array(drifts), n
 
 
-def c4_ensemble(torch, mdb, args, device):
+def reduce_scalar(torch, dist, x, op, device):
+    """x reduced over all ranks (op "max" or "sum"); x itself without a group."""
+    if dist is None:
+        return x
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def c4_ensemble(torch, mdb, args, device, rank=0, world=1, dist=None):
     """256 LJ replicas of uneven size, density and temperature advanced as one
     ensemble (one graph launch per timestep, batched kernels over all
     replicas), autotuned per size class; the same replicas in FP64 give the
-    energy drift the mixed path is compared with."""
+    energy drift the mixed path is compared with. With several ranks the
+    replicas are bin-packed by atom count over the GPUs (no exchange); the
+    time is the slowest rank's."""
     import autotune as AT
+    import workloads as W
     specs = c4_specs(args.replicas)
+    total_atoms = sum(sp["natoms"] for sp in specs)
+    if world > 1:
+        mine = W.assign_replicas([sp["natoms"] for sp in specs], world)[rank]
+        specs = [specs[i] for i in mine]
     pool = Replicas(mdb, device)
     t0 = time.perf_counter()
     if args.no_autotune:
@@ -344,6 +360,7 @@ def c4_ensemble(torch, mdb, args, device):
     every = 20
     members = [pool.build(sp, c["cluster_n"], c["half"], c) for sp, c in zip(specs, pick)]
     secs, launches, d32, n = run_ensemble(torch, mdb, members, args, every)
+    secs = reduce_scalar(torch, dist, secs, "max", "cuda")
     # the same replicas advanced one after another (each its own graph loop)
     t1 = time.perf_counter()
     for m in members:
@@ -354,9 +371,11 @@ def c4_ensemble(torch, mdb, args, device):
     members = [pool.build(sp, c["cluster_n"], c["half"], None, "fp64")
                for sp, c in zip(specs, pick)]
     secs64, _, d64, _ = run_ensemble(torch, mdb, members, args, every)
+    secs64 = reduce_scalar(torch, dist, secs64, "max", "cuda")
+    serial = reduce_scalar(torch, dist, serial, "max", "cuda")
     for m in members:
         m.close()
-    nat = sum(sp["natoms"] for sp in specs)
+    nat = total_atoms
     shapes = {}
     for c in pick:
         key = f"4x{c['cluster_n']}-{'half' if c['half'] else 'full'}"
@@ -364,9 +383,12 @@ def c4_ensemble(torch, mdb, args, device):
     return {"value": nat * every * args.steps / secs, "ms_per_step": 1e3 * secs / args.steps,
             "natoms": nat, "replicas": len(specs), "md_steps": every * args.steps,
             "gpu_launches": launches, "graph_launches_per_md_step": 1,
-            "energy_drift_max_abs": float(np.abs(d32).max()),
-            "energy_drift_fp64_max_abs": float(np.abs(d64).max()),
-            "excess_drift_vs_fp64_max_abs": float(np.abs(d32 - d64).max()),
+            "energy_drift_max_abs": reduce_scalar(torch, dist, np.abs(d32).max(), "max", "cuda"),
+            "energy_drift_fp64_max_abs": reduce_scalar(torch, dist, np.abs(d64).max(), "max",
+                                                       "cuda"),
+            "excess_drift_vs_fp64_max_abs": reduce_scalar(torch, dist, np.abs(d32 - d64).max(),
+                                                          "max", "cuda"),
+            "excess_drift_vs_fp64_median_abs": float(np.median(np.abs(d32 - d64))),
             "fp64_value": nat * every * args.steps / secs64,
             "serial_value": nat * every / serial,
             "autotune": {"seconds": round(tune_secs, 2), "trials": len(trials),
@@ -549,8 +571,12 @@ def main():
               flush=True)
         return
     if args.profile == "c4_mixed":
-        print(json.dumps(dict(profile=args.profile, **c4_ensemble(torch, mdb, args, local))),
-              flush=True)
+        res = c4_ensemble(torch, mdb, args, local, rank, world, dist)
+        if rank == 0:
+            print(json.dumps(dict(profile=args.profile, n_gpus=world, **res)), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
         return
     if args.profile:
         kind, prec = args.profile.split("_")[:2]
@@ -568,11 +594,7 @@ def main():
     clk = Clocks(local)
     head = measure(torch, mdb, HEAD["kind"], HEAD["precision"], args, local, HEAD["half"])
     clocks = clk.stop()
-    secs = head["secs"]
-    if dist:
-        tt = torch.tensor([secs], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        secs = float(tt.item())
+    secs = reduce_scalar(torch, dist, head["secs"], "max", "cuda")
     value = head["natoms"] * 20 * args.steps * world / secs
 
     s = head["system"]
@@ -601,7 +623,9 @@ def main():
             "peak_source": src}
 
     extra = {}
-    if not args.no_variants and rank == 0:
+    # the variants are one-GPU measurements: only in the one-rank run, so that
+    # no rank waits on them inside a collective
+    if not args.no_variants and world == 1:
         runs = {}
         for kind in ("cp44", "cp48"):
             for half in (0, 1):
@@ -644,10 +668,7 @@ def main():
 
     # end to end from the state the timed run reached (a liquid, as in use)
     e2 = e2e(torch, s, s.atoms(), max(args.steps // 5, 3), 20)
-    if dist:
-        tt = torch.tensor([e2["value"]], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.SUM)
-        e2["value"] = float(tt.item())
+    e2["value"] = reduce_scalar(torch, dist, e2["value"], "sum", "cuda")
     cb = cpu_baseline(half=HEAD["half"]) if (rank == 0 and world == 1) else None
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world,

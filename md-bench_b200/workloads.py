@@ -64,3 +64,17 @@ def c4_replicas(count=256):
         h3 = splitmix64(h2)
         out.append((int(n), 0.75 + 0.2 * uniform(h2), 0.7 + 1.3 * uniform(h3)))
     return out
+
+
+def assign_replicas(natoms, nranks):
+    """Replicas bin-packed by atom count over nranks GPUs (longest first, each
+    to the least-loaded rank, ties to the lower rank): the ensemble's
+    multi-GPU split, with no exchange between ranks. Returns one sorted index
+    list per rank."""
+    load = [0] * nranks
+    out = [[] for _ in range(nranks)]
+    for i in sorted(range(len(natoms)), key=lambda k: (-natoms[k], k)):
+        r = min(range(nranks), key=lambda q: (load[q], q))
+        out[r].append(i)
+        load[r] += natoms[i]
+    return [sorted(o) for o in out]
