@@ -299,7 +299,9 @@ __device__ __forceinline__ void mixed_entry(const IPack& ip, const float4& xj, f
 }
 
 // j data of one list entry: the atom's position moved into the i-cluster's
-// anchor frame (the anchor difference is exact), its type bits in .w
+// anchor frame (the anchor difference is exact), its type bits in .w. Lanes
+// past the end of a row read the dummy j-cluster (padding at +1e18, anchor 0),
+// so no lane branches.
 struct JEntry {
     float4 x;
     int cj;
@@ -310,19 +312,15 @@ __device__ __forceinline__ JEntry load_entry(int cj, int b, const float4* __rest
     const float4* __restrict__ anchor, const float4& ai)
 {
     JEntry j;
-    j.cj = cj;
-    if (cj >= 0) {
-        j.x            = __ldg(&xr[cj * N + b]);
-        const float4 a = __ldg(&anchor[cj]);
-        // anchors are multiples of 1/8 of magnitude < 2^17: the difference is
-        // exact (x and y as one packed pair)
-        const f2 dxy = f2_sub(f2_pack(a.x, a.y), f2_pack(ai.x, ai.y));
-        const f2 jxy = f2_add(f2_pack(j.x.x, j.x.y), dxy);
-        f2_unpack(jxy, j.x.x, j.x.y);
-        j.x.z += a.z - ai.z;
-    } else {
-        j.x = make_float4(CP_PAD_F, CP_PAD_F, CP_PAD_F, __int_as_float(-1));
-    }
+    j.cj           = cj;
+    j.x            = __ldg(&xr[cj * N + b]);
+    const float4 a = __ldg(&anchor[cj]);
+    // anchors are multiples of 1/8 of magnitude < 2^17: the difference is
+    // exact (x and y as one packed pair)
+    const f2 dxy = f2_sub(f2_pack(a.x, a.y), f2_pack(ai.x, ai.y));
+    const f2 jxy = f2_add(f2_pack(j.x.x, j.x.y), dxy);
+    f2_unpack(jxy, j.x.x, j.x.y);
+    j.x.z += a.z - ai.z;
     return j;
 }
 
@@ -397,15 +395,16 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
 #pragma unroll
         for (int a = 0; a < 4; a++)
             if (HALF ? (ai0 + a >= b) : (ai0 + a == b)) diag_excl |= 1u << a;
-        const int nn   = numneigh[ci];
-        const int* row = list + (size_t)ci * cs;
-        int lst_cur = lane < nn ? __ldg(&row[(size_t)lane * ks]) : -1;
-        int lst_nxt = 32 + lane < nn ? __ldg(&row[(size_t)(32 + lane) * ks]) : -1;
+        const int nn    = numneigh[ci];
+        const int dummy = cnt[CP_NCJ] + cnt[CP_NGC]; // the dummy j-cluster
+        const int* row  = list + (size_t)ci * cs;
+        int lst_cur = lane < nn ? __ldg(&row[(size_t)lane * ks]) : dummy;
+        int lst_nxt = 32 + lane < nn ? __ldg(&row[(size_t)(32 + lane) * ks]) : dummy;
         JEntry cur = load_entry<N>(__shfl_sync(0xffffffffu, lst_cur, eidx), b, xr, anchor, ai);
         JEntry nx1;
         if (PF == 2) {
             const int c1 = __shfl_sync(0xffffffffu, lst_cur, JPW + eidx);
-            nx1          = load_entry<N>(JPW < nn ? c1 : -1, b, xr, anchor, ai);
+            nx1          = load_entry<N>(JPW < nn ? c1 : dummy, b, xr, anchor, ai);
         }
         // one warp iteration: JPW entries, lane (eidx, b) on atom b of entry
         // kb + eidx; masked: the iteration may hold the diagonal entry
@@ -414,10 +413,11 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
             const int kn = kb + PF * JPW;
             if ((kn & 31) == 0) {
                 lst_cur = lst_nxt;
-                lst_nxt = kn + 32 + lane < nn ? __ldg(&row[(size_t)(kn + 32 + lane) * ks]) : -1;
+                lst_nxt = kn + 32 + lane < nn ? __ldg(&row[(size_t)(kn + 32 + lane) * ks])
+                                              : dummy;
             }
             const int cjn   = __shfl_sync(0xffffffffu, lst_cur, (kn & 31) + eidx);
-            const JEntry nx = load_entry<N>(kn < nn ? cjn : -1, b, xr, anchor, ai);
+            const JEntry nx = load_entry<N>(kn < nn ? cjn : dummy, b, xr, anchor, ai);
             const int cj    = cur.cj;
             float sej = 0.f, s3j = 0.f;
             if (!UNIFORM) {
@@ -434,8 +434,9 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
                 (masked && cj == ci_cj0) ? diag_excl : 0u, cutforcesq, A2, mB2, sig6u, ty.eps0,
                 ew, fx, fy, fz, gx, gy, gz, e);
             // reactions on local j atoms only (the reference drops ghost
-            // reactions); padding j slots get exact zeros
-            if (HALF && cj >= 0 && cj * N + b < nloc) {
+            // reactions; the dummy cluster lies past the ghosts); padding j
+            // slots get exact zeros
+            if (HALF && cj * N + b < nloc) {
                 float gx0, gx1, gy0, gy1, gz0, gz1;
                 f2_unpack(gx, gx0, gx1);
                 f2_unpack(gy, gy0, gy1);
@@ -454,6 +455,7 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
         // iteration tests for it
         if (nn > 0) {
             step(0, true);
+#pragma unroll 2
             for (int kb = JPW; kb < nn; kb += JPW) step(kb, false);
         }
         float f[12];
