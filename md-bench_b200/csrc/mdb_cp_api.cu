@@ -553,6 +553,10 @@ extern "C" int mdb_cp_get_atoms(MdbCp* ctx, double* x, double* v, int* type)
 
 // ---------------------------------------------------------------------------
 // enqueue helpers (stream-ordered, graph-capturable)
+// put_rel mode of xr: 0 FP64 (no xr), 1 mixed with type bits, 2 mixed with one
+// atom type (anchor components in .w, read by the UNIFORM force kernels)
+static int xr_mode(const MdbCp* ctx) { return ctx->mixed ? (ctx->ty.uniform ? 2 : 1) : 0; }
+
 static void enq_clusters(MdbCp* ctx)
 {
     cudaStream_t s = ctx->s;
@@ -569,7 +573,7 @@ static void enq_clusters(MdbCp* ctx)
     launch_sort_columns(s, g, ctx->M, ctx->N, ctx->col_start, ctx->col_atoms, ctx->ax,
         ctx->col_sorted, ctx->gidx, ctx->gz, ctx->ncl_col);
     scan_exclusive(ctx->ncl_col, ctx->cl_start, mb1, ctx->scan_scratch, s);
-    launch_build_clusters(s, g, ctx->M, ctx->N, ctx->mixed, ctx->col_start, ctx->col_sorted,
+    launch_build_clusters(s, g, ctx->M, ctx->N, xr_mode(ctx), ctx->col_start, ctx->col_sorted,
         ctx->cl_start, ctx->ax, ctx->av, ctx->cx, ctx->cv, ctx->inat, ctx->cbin, ctx->cl_first,
         ctx->ibbmin, ctx->ibbmax, ctx->jnat, ctx->jbbmin, ctx->jbbmax, ctx->anchor, ctx->xr,
         ctx->cnt, ctx->zext);
@@ -584,7 +588,7 @@ static void enq_setup_pbc(MdbCp* ctx)
     scan_exclusive(ctx->gcount, ctx->gstart, ctx->ncj_cap, ctx->scan_scratch, s);
     launch_ghost_write(s, ctx->ncj_cap, ctx->ngc_cap, ctx->cnt, ctx->jnat, ctx->jbbmin,
         ctx->jbbmax, ctx->g, ctx->gstart, ctx->border, ctx->pbc);
-    launch_ghost_first(s, ctx->N, ctx->ngc_cap, ctx->mixed, ctx->cnt, ctx->border, ctx->pbc,
+    launch_ghost_first(s, ctx->N, ctx->ngc_cap, xr_mode(ctx), ctx->cnt, ctx->border, ctx->pbc,
         ctx->g, ctx->cx, ctx->jnat, ctx->jbbmin, ctx->jbbmax, ctx->anchor, ctx->xr, ctx->zext);
 }
 
@@ -714,7 +718,7 @@ static void enq_initial(MdbCp* ctx)
 {
     launch_cp_initial(ctx->s, ctx->M, ctx->N, ctx->ncl_cap, ctx->cnt, ctx->p.dtforce, ctx->p.dt,
         ctx->cx, ctx->cv, ctx->cf, ctx->mixed ? ctx->cf32 : nullptr, ctx->anchor,
-        ctx->mixed ? ctx->xr : nullptr);
+        ctx->mixed ? ctx->xr : nullptr, xr_mode(ctx));
 }
 
 static void enq_final(MdbCp* ctx)
@@ -727,12 +731,12 @@ static void enq_final_initial(MdbCp* ctx)
 {
     launch_cp_final_initial(ctx->s, ctx->M, ctx->N, ctx->ncl_cap, ctx->cnt, ctx->p.dtforce,
         ctx->p.dt, ctx->cx, ctx->cv, ctx->cf, ctx->mixed ? ctx->cf32 : nullptr, ctx->anchor,
-        ctx->mixed ? ctx->xr : nullptr);
+        ctx->mixed ? ctx->xr : nullptr, xr_mode(ctx));
 }
 
 static void enq_ghost_update(MdbCp* ctx)
 {
-    launch_ghost_update(ctx->s, ctx->N, ctx->ngc_cap, ctx->mixed, ctx->cnt, ctx->border,
+    launch_ghost_update(ctx->s, ctx->N, ctx->ngc_cap, xr_mode(ctx), ctx->cnt, ctx->border,
         ctx->pbc, ctx->jnat, ctx->g, ctx->cx, ctx->anchor, ctx->xr);
 }
 
@@ -1471,7 +1475,7 @@ static int ens_tables(MdbCpEnsemble* e)
         a.cnt = c->cnt, a.cx = c->cx, a.cv = c->cv, a.cf = c->cf, a.cf32 = c->cf32;
         a.anchor = c->anchor, a.xr = c->xr, a.border = c->border, a.pbc = c->pbc;
         a.jnat = c->jnat, a.dtf = c->p.dtforce, a.dt = c->p.dt, a.xprd = c->g.xprd;
-        a.yprd = c->g.yprd, a.zprd = c->g.zprd, a.M = c->M, a.N = c->N, a.mixed = c->mixed;
+        a.yprd = c->g.yprd, a.zprd = c->g.zprd, a.M = c->M, a.N = c->N, a.mixed = xr_mode(c);
         a.zero_f = c->p.half_neigh;
         CpForceMember& f = fo[k];
         f.cnt = c->cnt, f.xr = c->xr, f.anchor = c->anchor, f.list = c->list;
@@ -1482,7 +1486,7 @@ static int ens_tables(MdbCpEnsemble* e)
     for (int k = 0; k < n; k++) {
         const MdbCp* c   = e->m[k];
         CpBuildMember& b = bt[k];
-        b.g = c->g, b.M = c->M, b.N = c->N, b.jfac = c->jfac, b.mixed = c->mixed;
+        b.g = c->g, b.M = c->M, b.N = c->N, b.jfac = c->jfac, b.mixed = xr_mode(c);
         b.half = c->p.half_neigh, b.nlocal = c->nlocal, b.ncl_cap = c->ncl_cap;
         b.ncj_cap = c->ncj_cap, b.ngc_cap = c->ngc_cap, b.maxneighs = c->maxneighs;
         b.ks = lks(c), b.cs = lcs(c), b.cnt = c->cnt, b.zext = c->zext;

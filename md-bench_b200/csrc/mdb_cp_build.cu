@@ -369,7 +369,7 @@ __device__ __forceinline__ void build_clusters_blk(int bid, int mbins, int mixed
         __syncwarp();
         for (int j = lane; j < nclu * M; j += 32) {
             const int slot = k0 * M + j;
-            put_rel(xr, slot, cx[slot], anchor[slot / N]);
+            put_rel(xr, slot, cx[slot], anchor[slot / N], mixed, slot % N);
         }
     }
 }
@@ -559,7 +559,7 @@ __device__ __forceinline__ void ghost_first_blk(int bid, int N, int* cnt,
             float4 a   = anchor_of(mn, mx);
             anchor[cg] = a;
             for (int k = 0; k < N; k++)
-                put_rel(xr, cg * N + k, cx[cg * N + k], a);
+                put_rel(xr, cg * N + k, cx[cg * N + k], a, mixed, k);
         }
     } else if (gi == ngc) {
         const int cd = ncj + ngc; // dummy cluster
@@ -568,7 +568,7 @@ __device__ __forceinline__ void ghost_first_blk(int bid, int N, int* cnt,
             if (mixed)
                 put_rel(xr, cd * N + k,
                     make_double4(INFINITY, INFINITY, INFINITY, type_bits(-1)),
-                    make_float4(0.f, 0.f, 0.f, 0.f));
+                    make_float4(0.f, 0.f, 0.f, 0.f), mixed, k);
         }
         if (mixed) anchor[cd] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
@@ -608,7 +608,7 @@ __device__ __forceinline__ void ghost_update_slot(int s, int N, int mixed,
     p.y += (double)(((code >> 2) & 3) - 1) * yprd;
     p.z += (double)(((code >> 4) & 3) - 1) * zprd;
     cx[cg * N + k] = p;
-    if (mixed) put_rel(xr, cg * N + k, p, anchor[cg]);
+    if (mixed) put_rel(xr, cg * N + k, p, anchor[cg], mixed, k);
 }
 
 __global__ void k_ghost_update(int N, int mixed, const int* __restrict__ cnt,

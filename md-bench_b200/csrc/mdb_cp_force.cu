@@ -307,20 +307,32 @@ struct JEntry {
     int cj;
 };
 
-template <int N>
+// the j position moved from its cluster's anchor a into the i frame (anchors
+// are multiples of 1/8 of magnitude < 2^17: a - ai is exact; x and y as one
+// packed pair)
+__device__ __forceinline__ void to_i_frame(float4& x, float ax, float ay, float az,
+    const float4& ai)
+{
+    const f2 dxy = f2_sub(f2_pack(ax, ay), f2_pack(ai.x, ai.y));
+    const f2 jxy = f2_add(f2_pack(x.x, x.y), dxy);
+    f2_unpack(jxy, x.x, x.y);
+    x.z += az - ai.z;
+}
+
+// AW (one atom type): the anchor travels in .w of the entry's slots 0..2 and
+// is applied when the entry is used (after its load has landed); otherwise
+// it is loaded here and applied at once.
+template <int N, bool AW>
 __device__ __forceinline__ JEntry load_entry(int cj, int b, const float4* __restrict__ xr,
     const float4* __restrict__ anchor, const float4& ai)
 {
     JEntry j;
-    j.cj           = cj;
-    j.x            = __ldg(&xr[cj * N + b]);
-    const float4 a = __ldg(&anchor[cj]);
-    // anchors are multiples of 1/8 of magnitude < 2^17: the difference is
-    // exact (x and y as one packed pair)
-    const f2 dxy = f2_sub(f2_pack(a.x, a.y), f2_pack(ai.x, ai.y));
-    const f2 jxy = f2_add(f2_pack(j.x.x, j.x.y), dxy);
-    f2_unpack(jxy, j.x.x, j.x.y);
-    j.x.z += a.z - ai.z;
+    j.cj = cj;
+    j.x  = __ldg(&xr[cj * N + b]);
+    if (!AW) {
+        const float4 a = __ldg(&anchor[cj]);
+        to_i_frame(j.x, a.x, a.y, a.z, ai);
+    }
     return j;
 }
 
@@ -365,8 +377,11 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
 #pragma unroll
         for (int a = 0; a < 4; a++) {
             xi[a] = xr[ci * 4 + a];
-            int t = __float_as_int(xi[a].w);
-            if (t < 0) {
+            // padding: type -1, or (one type: .w carries the anchor) the
+            // +1e18 position
+            int t          = UNIFORM ? 0 : __float_as_int(xi[a].w);
+            const bool pad = UNIFORM ? !(xi[a].x < 0.1f * CP_PAD_F) : t < 0;
+            if (pad) {
                 xi[a].x = xi[a].y = xi[a].z = -CP_PAD_F;
                 t                           = 0;
             }
@@ -400,11 +415,12 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
         const int* row  = list + (size_t)ci * cs;
         int lst_cur = lane < nn ? __ldg(&row[(size_t)lane * ks]) : dummy;
         int lst_nxt = 32 + lane < nn ? __ldg(&row[(size_t)(32 + lane) * ks]) : dummy;
-        JEntry cur = load_entry<N>(__shfl_sync(0xffffffffu, lst_cur, eidx), b, xr, anchor, ai);
+        JEntry cur =
+            load_entry<N, UNIFORM>(__shfl_sync(0xffffffffu, lst_cur, eidx), b, xr, anchor, ai);
         JEntry nx1;
         if (PF == 2) {
             const int c1 = __shfl_sync(0xffffffffu, lst_cur, JPW + eidx);
-            nx1          = load_entry<N>(JPW < nn ? c1 : dummy, b, xr, anchor, ai);
+            nx1          = load_entry<N, UNIFORM>(JPW < nn ? c1 : dummy, b, xr, anchor, ai);
         }
         // one warp iteration: JPW entries, lane (eidx, b) on atom b of entry
         // kb + eidx; masked: the iteration may hold the diagonal entry
@@ -417,8 +433,17 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
                                               : dummy;
             }
             const int cjn   = __shfl_sync(0xffffffffu, lst_cur, (kn & 31) + eidx);
-            const JEntry nx = load_entry<N>(kn < nn ? cjn : dummy, b, xr, anchor, ai);
+            const JEntry nx = load_entry<N, UNIFORM>(kn < nn ? cjn : dummy, b, xr, anchor, ai);
             const int cj    = cur.cj;
+            float4 xj       = cur.x;
+            if (UNIFORM) {
+                // the anchor of this entry's j-cluster from .w of its slots 0..2
+                const int base = lane - b;
+                const float ax = __shfl_sync(0xffffffffu, xj.w, base);
+                const float ay = __shfl_sync(0xffffffffu, xj.w, base + 1);
+                const float az = __shfl_sync(0xffffffffu, xj.w, base + 2);
+                to_i_frame(xj, ax, ay, az, ai);
+            }
             float sej = 0.f, s3j = 0.f;
             if (!UNIFORM) {
                 int t = __float_as_int(cur.x.w);
@@ -430,7 +455,7 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
             // energy weight: full lists see every pair twice; half lists once,
             // except pairs with ghost atoms, which both owners list
             const double ew = (!HALF || cj * N + b >= nloc) ? 0.5 : 1.0;
-            mixed_entry<HALF, ENERGY, UNIFORM>(ip, cur.x, sej, s3j,
+            mixed_entry<HALF, ENERGY, UNIFORM>(ip, xj, sej, s3j,
                 (masked && cj == ci_cj0) ? diag_excl : 0u, cutforcesq, A2, mB2, sig6u, ty.eps0,
                 ew, fx, fy, fz, gx, gy, gz, e);
             // reactions on local j atoms only (the reference drops ghost
@@ -455,7 +480,7 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
         // iteration tests for it
         if (nn > 0) {
             step(0, true);
-#pragma unroll 2
+#pragma unroll(HALF ? 1 : 2)
             for (int kb = JPW; kb < nn; kb += JPW) step(kb, false);
         }
         float f[12];
@@ -467,8 +492,9 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
         }
         warp_reduce_12(f, lane);
         if ((lane & 7) == 0) {
-            const int a = lane >> 3;
-            if (__float_as_int(xr[ci * 4 + a].w) >= 0) {
+            const int a     = lane >> 3;
+            const float4 xa = xr[ci * 4 + a];
+            if (UNIFORM ? xa.x < 0.1f * CP_PAD_F : __float_as_int(xa.w) >= 0) {
                 float4* dst = &cf32[ci * 4 + a];
                 if (HALF) red_add4(dst, f[0], f[1], f[2]);
                 else *dst = make_float4(f[0], f[1], f[2], 0.f);
@@ -641,7 +667,7 @@ template <bool FINAL, bool INITIAL>
 __device__ __forceinline__ void cp_integrate_slot(int s, int M, int N,
     const int* __restrict__ cnt, double dtf, double dt, double4* cx, double4* cv,
     const double4* __restrict__ cf, float4* cf32, const float4* __restrict__ anchor, float4* xr,
-    bool zero_f)
+    bool zero_f, int xmode)
 {
     if (s >= cnt[CP_NCL] * M) return;
     double4 p = cx[s];
@@ -665,7 +691,7 @@ __device__ __forceinline__ void cp_integrate_slot(int s, int M, int N,
         p.y += dt * v.y;
         p.z += dt * v.z;
         cx[s] = p;
-        if (xr) put_rel(xr, s, p, anchor[s / N]);
+        if (xr) put_rel(xr, s, p, anchor[s / N], xmode, s % N);
     }
     cv[s] = v;
 }
@@ -673,10 +699,10 @@ __device__ __forceinline__ void cp_integrate_slot(int s, int M, int N,
 template <bool FINAL, bool INITIAL>
 __global__ void k_cp_integrate(int M, int N, const int* __restrict__ cnt, double dtf, double dt,
     double4* cx, double4* cv, const double4* __restrict__ cf, const float4* __restrict__ cf32,
-    const float4* __restrict__ anchor, float4* xr)
+    const float4* __restrict__ anchor, float4* xr, int xmode)
 {
     cp_integrate_slot<FINAL, INITIAL>(blockIdx.x * blockDim.x + threadIdx.x, M, N, cnt, dtf, dt,
-        cx, cv, cf, const_cast<float4*>(cf32), anchor, xr, false);
+        cx, cv, cf, const_cast<float4*>(cf32), anchor, xr, false, xmode);
 }
 
 template <bool FINAL, bool INITIAL>
@@ -687,7 +713,7 @@ __global__ void k_cp_integrate_batch(const CpStepMember* __restrict__ tab,
     if (bm.x < 0) return;
     const CpStepMember& m = tab[bm.x];
     cp_integrate_slot<FINAL, INITIAL>(bm.y * blockDim.x + threadIdx.x, m.M, m.N, m.cnt, m.dtf,
-        m.dt, m.cx, m.cv, m.cf, m.cf32, m.anchor, m.xr, m.zero_f != 0);
+        m.dt, m.cx, m.cv, m.cf, m.cf32, m.anchor, m.xr, m.zero_f != 0, m.mixed);
 }
 
 void launch_cp_integrate_batch(cudaStream_t s, bool final_, bool initial, int nblocks,
@@ -703,11 +729,11 @@ void launch_cp_integrate_batch(cudaStream_t s, bool final_, bool initial, int nb
 
 void launch_cp_initial(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt, double dtf,
     double dt, double4* cx, double4* cv, const double4* cf, const float4* cf32,
-    const float4* anchor, float4* xr)
+    const float4* anchor, float4* xr, int xmode)
 {
     long long n = (long long)ncl_cap * M;
     k_cp_integrate<false, true><<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(M, N, cnt,
-        dtf, dt, cx, cv, cf, cf32, anchor, xr);
+        dtf, dt, cx, cv, cf, cf32, anchor, xr, xmode);
     g_launches++;
 }
 
@@ -716,17 +742,17 @@ void launch_cp_final(cudaStream_t s, int M, int ncl_cap, const int* cnt, double 
 {
     long long n = (long long)ncl_cap * M;
     k_cp_integrate<true, false><<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(M, M, cnt,
-        dtf, 0.0, const_cast<double4*>(cx), cv, cf, cf32, nullptr, nullptr);
+        dtf, 0.0, const_cast<double4*>(cx), cv, cf, cf32, nullptr, nullptr, 0);
     g_launches++;
 }
 
 void launch_cp_final_initial(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt,
     double dtf, double dt, double4* cx, double4* cv, const double4* cf, const float4* cf32,
-    const float4* anchor, float4* xr)
+    const float4* anchor, float4* xr, int xmode)
 {
     long long n = (long long)ncl_cap * M;
     k_cp_integrate<true, true><<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(M, N, cnt,
-        dtf, dt, cx, cv, cf, cf32, anchor, xr);
+        dtf, dt, cx, cv, cf, cf32, anchor, xr, xmode);
     g_launches++;
 }
 

@@ -77,15 +77,22 @@ __device__ __forceinline__ int slot_type(const double4& p) { return (int)__doubl
 
 __device__ __forceinline__ double type_bits(int t) { return __longlong_as_double((long long)t); }
 
-// mixed-path position of one slot, relative to the anchor a of its j-cluster
-__device__ __forceinline__ void put_rel(float4* xr, int slot, const double4& p, const float4& a)
+// mixed-path position of one slot, relative to the anchor a of its j-cluster;
+// b = the slot's index in its j-cluster. mode 1: .w holds the type bits;
+// mode 2 (one atom type, no type needed): slots 0, 1, 2 of a j-cluster carry
+// the anchor's x, y, z in .w instead, so the force kernel reads a j atom and
+// its cluster's anchor in one load (padding is told by its position).
+__device__ __forceinline__ void put_rel(float4* xr, int slot, const double4& p, const float4& a,
+    int mode, int b)
 {
     const int t = slot_type(p);
+    float w     = __int_as_float(t < 0 ? -1 : t);
+    if (mode == 2 && b < 3) w = b == 0 ? a.x : (b == 1 ? a.y : a.z);
     if (t < 0) {
-        xr[slot] = make_float4(CP_PAD_F, CP_PAD_F, CP_PAD_F, __int_as_float(-1));
+        xr[slot] = make_float4(CP_PAD_F, CP_PAD_F, CP_PAD_F, w);
     } else {
         xr[slot] = make_float4((float)(p.x - (double)a.x), (float)(p.y - (double)a.y),
-            (float)(p.z - (double)a.z), __int_as_float(t));
+            (float)(p.z - (double)a.z), w);
     }
 }
 
@@ -156,14 +163,15 @@ int launch_force_mixed(cudaStream_t s, int N, int half, int energy, int ncl_cap,
 // threads per block and block count of a mixed force launch
 int force_mixed_threads(const Types& ty);
 int force_mixed_grid(int ncl_cap, const Types& ty);
+// xmode: the put_rel mode of xr (ignored when xr is null)
 void launch_cp_initial(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt, double dtf,
     double dt, double4* cx, double4* cv, const double4* cf, const float4* cf32,
-    const float4* anchor, float4* xr);
+    const float4* anchor, float4* xr, int xmode);
 void launch_cp_final(cudaStream_t s, int M, int ncl_cap, const int* cnt, double dtf,
     const double4* cx, double4* cv, const double4* cf, const float4* cf32);
 void launch_cp_final_initial(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt,
     double dtf, double dt, double4* cx, double4* cv, const double4* cf, const float4* cf32,
-    const float4* anchor, float4* xr);
+    const float4* anchor, float4* xr, int xmode);
 int ke_blocks(int n);
 
 // ---- batched launches over the members of an ensemble -----------------------
@@ -183,7 +191,7 @@ struct CpStepMember { // integrator and ghost update
     const int* pbc;
     const int* jnat;
     double dtf, dt, xprd, yprd, zprd;
-    int M, N, mixed;
+    int M, N, mixed; // mixed: 0 FP64, else the xr mode of put_rel
     int zero_f; // half lists: the initial integration clears the forces it used
 };
 struct CpForceMember { // mixed force kernel (row-major lists)
