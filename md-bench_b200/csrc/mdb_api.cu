@@ -41,6 +41,8 @@ struct MdbCtx {
     CellFrame cf;
     CellShift shift;
     double cutforcesq = 0, cutneighsq = 0;
+    // |FP32 rsq - exact rsq| bound of the list build's prefilter (box size)
+    float list_margin = 0;
     double mvv2e = 1, dof_boltz = 1, t_scale = 1, p_scale = 1;
 
     // device buffers
@@ -53,6 +55,8 @@ struct MdbCtx {
     int *ghost_cnt = nullptr, *ghost_off = nullptr;
     int *atom_bin = nullptr, *atom_slot = nullptr;
     int *bin_count = nullptr, *bin_start = nullptr, *bin_atoms = nullptr;
+    double4* bin_x = nullptr; // positions in bin order, atom index bits in .w
+    float4* bin_xf = nullptr; // the same rounded to FP32 (list build prefilter)
     int *bin_lcount = nullptr, *loc_start = nullptr; // locals per bin, their offsets
     int* local_order = nullptr;                      // row t of the list -> atom
     int4* stencil_d  = nullptr;                      // {flat offset, dx, dy, dz}
@@ -327,6 +331,18 @@ extern "C" int mdb_create(const MdbParams* params, MdbCtx** out)
     ctx->cutforcesq = p.cutforce * p.cutforce;
     ctx->cutneighsq = p.cutneigh * p.cutneigh;
     {
+        // coordinates (ghosts included) lie within the box grown by cutneigh;
+        // rounding each to FP32 moves a difference by at most 2 e, e = |x|max
+        // 2^-24, and rsq by at most 2 e (|dx| + |dy| + |dz|) + 3 (2e)^2 with
+        // |d| <= cutneigh near the threshold, plus the FP32 rounding of the
+        // three products and two sums; a factor 4 covers the rest
+        const double xmax = std::max(p.xprd, std::max(p.yprd, p.zprd)) + 2.0 * p.cutneigh;
+        const double e    = xmax * 0x1p-24;
+        const double bnd  = 2.0 * e * 3.0 * p.cutneigh + 12.0 * e * e +
+                           8.0 * ctx->cutneighsq * 0x1p-24;
+        ctx->list_margin = (float)(4.0 * bnd);
+    }
+    {
         // mixed-path cells: the smallest power of two G >= cutneigh, so the
         // cells of any listed pair differ by at most one per axis
         double g = 1.0 / 1024;
@@ -404,6 +420,8 @@ static void free_atom_buffers(MdbCtx* ctx)
     dfree(ctx->atom_bin);
     dfree(ctx->atom_slot);
     dfree(ctx->bin_atoms);
+    dfree(ctx->bin_x);
+    dfree(ctx->bin_xf);
     dfree(ctx->numneigh);
     dfree(ctx->neighbors);
     dfree(ctx->scan_scratch);
@@ -476,12 +494,16 @@ static int alloc_ghost_sized(MdbCtx* ctx, int ghost_cap)
     dfree(ctx->atom_bin);
     dfree(ctx->atom_slot);
     dfree(ctx->bin_atoms);
+    dfree(ctx->bin_x);
+    dfree(ctx->bin_xf);
     dfree(ctx->fp);
     CK(dalloc(&ctx->border_map, ghost_cap));
     CK(dalloc(&ctx->pbc_code, ghost_cap));
     CK(dalloc(&ctx->atom_bin, nall));
     CK(dalloc(&ctx->atom_slot, nall));
     CK(dalloc(&ctx->bin_atoms, nall));
+    CK(dalloc(&ctx->bin_x, nall));
+    CK(dalloc(&ctx->bin_xf, nall));
     if (ctx->p.force_field == MDB_FF_EAM) CK(dalloc(&ctx->fp, nall));
     ctx->ghost_cap   = ghost_cap;
     ctx->nall_cap    = nall;
@@ -698,10 +720,12 @@ static void enq_list(MdbCtx* ctx)
         ctx->bin_start, ctx->bin_atoms, ctx->counters);
     launch_bin_sort(s, ctx->g.mbins, ctx->bin_start, ctx->bin_atoms, ctx->loc_start,
         ctx->local_order);
+    launch_bin_positions(s, ctx->nall_cap, ctx->g.mbins, ctx->x, ctx->bin_start, ctx->bin_atoms,
+        ctx->bin_x, ctx->bin_xf);
     launch_build_list(s, ctx->nlocal, ctx->x, ctx->g, ctx->stencil_d, ctx->local_order,
-        ctx->atom_bin, ctx->bin_start, ctx->bin_atoms, ctx->cutneighsq, ctx->p.half_neigh,
-        ctx->maxneighs, ctx->ld, ctx->neighbors, ctx->numneigh, ctx->counters,
-        ctx->mixed ? ctx->qcell : nullptr);
+        ctx->atom_bin, ctx->bin_start, ctx->bin_x, ctx->bin_xf, ctx->cutneighsq,
+        ctx->list_margin, ctx->p.half_neigh, ctx->maxneighs, ctx->ld, ctx->neighbors,
+        ctx->numneigh, ctx->counters, ctx->mixed ? ctx->qcell : nullptr);
 }
 
 static void clear_rebuild_counters(MdbCtx* ctx)

@@ -199,10 +199,16 @@ void launch_bin_scatter(cudaStream_t s, int nlocal, int nall_cap, const int* ato
 void launch_bin_sort(cudaStream_t s, int mbins, const int* bin_start, int* bin_atoms,
     const int* loc_start, int* local_order);
 // stencil entries: {flat bin offset, dx, dy, dz}; qcell non-null packs cell codes
+// positions of the binned atoms in bin order (atom index bits in .w), FP64
+// and rounded to FP32
+void launch_bin_positions(cudaStream_t s, int nall_cap, int mbins, const double4* x,
+    const int* bin_start, const int* bin_atoms, double4* bin_x, float4* bin_xf);
+// the Verlet list from the bin-ordered positions; margin bounds the FP32
+// prefilter's rsq error (only candidates within it take the exact FP64 test)
 void launch_build_list(cudaStream_t s, int nlocal, const double4* x, BinGeom g,
     const int4* stencil, const int* local_order, const int* atom_bin, const int* bin_start,
-    const int* bin_atoms, double cutneighsq, int half, int maxneighs, int ld, int* neighbors,
-    int* numneigh, int* counters, const int* qcell);
+    const double4* bin_x, const float4* bin_xf, double cutneighsq, float margin, int half,
+    int maxneighs, int ld, int* neighbors, int* numneigh, int* counters, const int* qcell);
 int ke_partial_blocks(int n);
 void launch_ke_partial(cudaStream_t s, int n, const double* vx, const double* vy,
     const double* vz, double mass, double* partials);

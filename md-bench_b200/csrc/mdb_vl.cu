@@ -490,10 +490,36 @@ void launch_bin_sort(cudaStream_t s, int mbins, const int* bin_start, int* bin_a
 // test). The candidate loop handles two candidates per iteration so their
 // loads overlap. On the mixed path each entry also carries the cell offset of
 // the pair (2 bits per axis, bits 26-31).
+__global__ void k_bin_positions(int mbins, const double4* __restrict__ x,
+    const int* __restrict__ bin_start, const int* __restrict__ bin_atoms,
+    double4* __restrict__ bin_x, float4* __restrict__ bin_xf)
+{
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= bin_start[mbins]) return;
+    const int j     = bin_atoms[m];
+    const double4 p = x[j];
+    bin_x[m]  = make_double4(p.x, p.y, p.z, __longlong_as_double((long long)j));
+    bin_xf[m] = make_float4((float)p.x, (float)p.y, (float)p.z, __int_as_float(j));
+}
+
+void launch_bin_positions(cudaStream_t s, int nall_cap, int mbins, const double4* x,
+    const int* bin_start, const int* bin_atoms, double4* bin_x, float4* bin_xf)
+{
+    k_bin_positions<<<mdb_blocks(nall_cap, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(mbins, x,
+        bin_start, bin_atoms, bin_x, bin_xf);
+    g_launches++;
+}
+
+// Candidates come from the bin-ordered copies (a bin's atoms contiguous, in
+// index order): the FP32 copy decides every candidate whose FP32 distance lies
+// more than `margin` (a bound on its rounding error) from cutneigh^2; the few
+// within it take the reference's exact FP64 test on the FP64 copy. Accepted
+// sets and their order are therefore exactly the reference's.
 __global__ void __launch_bounds__(128) k_build_list(int nlocal, const double4* __restrict__ x,
     BinGeom g, const int4* __restrict__ stencil, const int* __restrict__ atom_bin,
-    const int* __restrict__ bin_start, const int* __restrict__ bin_atoms, double cutneighsq,
-    int half, int maxneighs, int ld, int* __restrict__ neighbors, int* __restrict__ numneigh,
+    const int* __restrict__ bin_start, const double4* __restrict__ bin_x,
+    const float4* __restrict__ bin_xf, double cutneighsq, float margin, int half,
+    int maxneighs, int ld, int* __restrict__ neighbors, int* __restrict__ numneigh,
     int* __restrict__ counters, const int* __restrict__ qcell)
 {
     extern __shared__ int4 st[];
@@ -513,28 +539,37 @@ __global__ void __launch_bounds__(128) k_build_list(int nlocal, const double4* _
     const float fz   = (float)(uz - (double)(int)uz);
     const float bx = (float)g.binsizex, by = (float)g.binsizey, bz = (float)g.binsizez;
     const float skip2 = (float)cutneighsq * 1.0001f + 1e-4f;
+    const float xif = (float)xi.x, yif = (float)xi.y, zif = (float)xi.z;
+    const float lo = (float)cutneighsq - margin, hi = (float)cutneighsq + margin;
     int n = 0, bad = 0;
 
-    auto consider = [&](int j, const double4& xj) {
+    auto consider = [&](int m, const float4& c) {
+        const int j = __float_as_int(c.w);
         if (j == i || (half && j < i)) return;
-        double delx = xi.x - xj.x;
-        double dely = xi.y - xj.y;
-        double delz = xi.z - xj.z;
-        double rsq  = delx * delx + dely * dely + delz * delz;
-        if (rsq <= cutneighsq) {
-            int e = j;
-            if (qcell) {
-                int qj = __ldg(&qcell[j]);
-                int cx = cell_axis(qj, 0) - cell_axis(qi, 0);
-                int cy = cell_axis(qj, 1) - cell_axis(qi, 1);
-                int cz = cell_axis(qj, 2) - cell_axis(qi, 2);
-                if (cx < -1 || cx > 1 || cy < -1 || cy > 1 || cz < -1 || cz > 1) bad = 1;
-                int code = ((cx + 1) & 3) | (((cy + 1) & 3) << 2) | (((cz + 1) & 3) << 4);
-                e        = j | (code << MDB_IDX_BITS);
-            }
-            if (n < maxneighs) neighbors[(size_t)n * ld + i] = e;
-            n++;
+        const float dx = xif - c.x, dy = yif - c.y, dz = zif - c.z;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 > hi) return;
+        if (r2 >= lo) {
+            // the reference's test, verletlist/neighbor.c:320-330
+            const double4 xj = ldg4(&bin_x[m]);
+            double delx      = xi.x - xj.x;
+            double dely      = xi.y - xj.y;
+            double delz      = xi.z - xj.z;
+            double rsq       = delx * delx + dely * dely + delz * delz;
+            if (!(rsq <= cutneighsq)) return;
         }
+        int e = j;
+        if (qcell) {
+            int qj = __ldg(&qcell[j]);
+            int cx = cell_axis(qj, 0) - cell_axis(qi, 0);
+            int cy = cell_axis(qj, 1) - cell_axis(qi, 1);
+            int cz = cell_axis(qj, 2) - cell_axis(qi, 2);
+            if (cx < -1 || cx > 1 || cy < -1 || cy > 1 || cz < -1 || cz > 1) bad = 1;
+            int code = ((cx + 1) & 3) | (((cy + 1) & 3) << 2) | (((cz + 1) & 3) << 4);
+            e        = j | (code << MDB_IDX_BITS);
+        }
+        if (n < maxneighs) neighbors[(size_t)n * ld + i] = e;
+        n++;
     };
 
     if (ibin >= 0) {
@@ -553,17 +588,12 @@ __global__ void __launch_bounds__(128) k_build_list(int nlocal, const double4* _
             const int end = __ldg(&bin_start[jbin + 1]);
             int m         = beg;
             for (; m + 1 < end; m += 2) {
-                const int ja = __ldg(&bin_atoms[m]);
-                const int jb = __ldg(&bin_atoms[m + 1]);
-                const double4 xa = ldg4(&x[ja]);
-                const double4 xb = ldg4(&x[jb]);
-                consider(ja, xa);
-                consider(jb, xb);
+                const float4 ca = __ldg(&bin_xf[m]);
+                const float4 cb = __ldg(&bin_xf[m + 1]);
+                consider(m, ca);
+                consider(m + 1, cb);
             }
-            if (m < end) {
-                const int ja = __ldg(&bin_atoms[m]);
-                consider(ja, ldg4(&x[ja]));
-            }
+            if (m < end) consider(m, __ldg(&bin_xf[m]));
         }
     }
     // the stored count never exceeds the row capacity, so no consumer can read
@@ -576,15 +606,15 @@ __global__ void __launch_bounds__(128) k_build_list(int nlocal, const double4* _
 
 void launch_build_list(cudaStream_t s, int nlocal, const double4* x, BinGeom g,
     const int4* stencil, const int* local_order, const int* atom_bin, const int* bin_start,
-    const int* bin_atoms, double cutneighsq, int half, int maxneighs, int ld, int* neighbors,
-    int* numneigh, int* counters, const int* qcell)
+    const double4* bin_x, const float4* bin_xf, double cutneighsq, float margin, int half,
+    int maxneighs, int ld, int* neighbors, int* numneigh, int* counters, const int* qcell)
 {
     (void)local_order;
     if (nlocal <= 0) return;
     size_t smem = sizeof(int4) * g.nstencil;
     k_build_list<<<mdb_blocks(nlocal, 128), 128, smem, s>>>(nlocal, x, g, stencil, atom_bin,
-        bin_start, bin_atoms, cutneighsq, half, maxneighs, ld, neighbors, numneigh, counters,
-        qcell);
+        bin_start, bin_x, bin_xf, cutneighsq, margin, half, maxneighs, ld, neighbors, numneigh,
+        counters, qcell);
     g_launches++;
 }
 
