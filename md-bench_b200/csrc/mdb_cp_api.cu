@@ -57,6 +57,7 @@ struct MdbCp {
     int *gcolumn = nullptr, *gcol_count = nullptr, *gfill = nullptr, *jcol_n = nullptr;
     int *jcol_start = nullptr, *gtmp = nullptr, *jcol = nullptr;
     double4 *jcbbmin = nullptr, *jcbbmax = nullptr;
+    float4 *jcbbf = nullptr, *cxf = nullptr; // FP32 copies for the list build
     int* stencil_d = nullptr;
     // list
     int *list = nullptr, *numneigh = nullptr, *nmasked = nullptr;
@@ -189,6 +190,17 @@ static void setup_columns(MdbCp* ctx)
     double bby = 0.5 * (g.binsizey + g.binsizey);
     double rbb = std::max(0.0, cut - 0.5 * sqrt(bbx * bbx + bby * bby));
     g.rbb_sq   = rbb * rbb;
+    // coordinates (ghosts included) lie within the box grown by cutneigh;
+    // rounding each to FP32 moves a difference by at most 2e, e = |x|max
+    // 2^-24, and a squared distance (or box distance) by at most
+    // 4e (|dx| + |dy| + |dz|) + 12 e^2 with |d| <= cutneigh near a threshold,
+    // plus the FP32 rounding of three products and two sums; doubled
+    {
+        const double xmax = std::max(g.xprd, std::max(g.yprd, g.zprd)) + 2.0 * cut;
+        const double e    = xmax * 0x1p-24;
+        const double bnd  = 4.0 * e * 3.0 * cut + 12.0 * e * e + 8.0 * g.cutneighsq * 0x1p-24;
+        g.list_margin     = (float)(2.0 * bnd);
+    }
 }
 
 // computePerTypeLJParameters (common/parameter.c:31-45): per-type sqrt(eps)
@@ -258,7 +270,7 @@ static void free_all(MdbCp* ctx)
     dfree(ctx->jbbmax), dfree(ctx->gcount), dfree(ctx->gstart), dfree(ctx->border);
     dfree(ctx->pbc), dfree(ctx->gcolumn), dfree(ctx->gcol_count), dfree(ctx->gfill);
     dfree(ctx->jcol_n), dfree(ctx->jcol_start), dfree(ctx->gtmp), dfree(ctx->jcol);
-    dfree(ctx->jcbbmin), dfree(ctx->jcbbmax);
+    dfree(ctx->jcbbmin), dfree(ctx->jcbbmax), dfree(ctx->jcbbf), dfree(ctx->cxf);
     dfree(ctx->stencil_d), dfree(ctx->list), dfree(ctx->numneigh), dfree(ctx->nmasked);
     dfree(ctx->cnt), dfree(ctx->zext), dfree(ctx->scan_scratch), dfree(ctx->partials);
     dfree(ctx->red), dfree(ctx->stage), dfree(ctx->stage_i);
@@ -422,9 +434,11 @@ static int alloc_ghosts(MdbCp* ctx, int ngc_cap)
     dfree(ctx->cx), dfree(ctx->cv), dfree(ctx->cf), dfree(ctx->xr), dfree(ctx->cf32);
     dfree(ctx->anchor), dfree(ctx->jnat), dfree(ctx->jbbmin), dfree(ctx->jbbmax);
     dfree(ctx->border), dfree(ctx->pbc), dfree(ctx->gcolumn), dfree(ctx->gtmp), dfree(ctx->jcol);
-    dfree(ctx->jcbbmin), dfree(ctx->jcbbmax);
+    dfree(ctx->jcbbmin), dfree(ctx->jcbbmax), dfree(ctx->jcbbf), dfree(ctx->cxf);
     if ((e = dalloc(&ctx->cx, ctx->slot_cap)) != cudaSuccess ||
         (e = dalloc(&ctx->jcbbmin, nj)) != cudaSuccess ||
+        (e = dalloc(&ctx->jcbbf, 2 * (size_t)nj)) != cudaSuccess ||
+        (e = dalloc(&ctx->cxf, ctx->slot_cap)) != cudaSuccess ||
         (e = dalloc(&ctx->jcbbmax, nj)) != cudaSuccess ||
         (e = dalloc(&ctx->cv, ctx->slot_cap)) != cudaSuccess ||
         (e = dalloc(&ctx->cf, ctx->slot_cap)) != cudaSuccess ||
@@ -615,10 +629,12 @@ static int lcs(const MdbCp* ctx) { return ctx->mixed ? ctx->maxneighs : 1; }
 
 static void enq_list(MdbCp* ctx)
 {
+    launch_list_prep(ctx->s, ctx->N, ctx->slot_cap, ctx->g.mbins + 1, ctx->cnt,
+        ctx->jcol_start, ctx->jcbbmin, ctx->jcbbmax, ctx->cx, ctx->jcbbf, ctx->cxf);
     launch_build_list(ctx->s, ctx->M, ctx->N, ctx->p.half_neigh, ctx->ncl_cap, ctx->cnt, ctx->g,
         ctx->stencil_d, ctx->cbin, ctx->ibbmin, ctx->ibbmax, ctx->jcbbmin, ctx->jcbbmax, ctx->cx,
-        ctx->jcol_start, ctx->jcol, ctx->zext, ctx->maxneighs, lks(ctx), lcs(ctx), ctx->list,
-        ctx->numneigh, ctx->nmasked, ctx->cnt);
+        ctx->jcbbf, ctx->cxf, ctx->jcol_start, ctx->jcol, ctx->zext, ctx->maxneighs, lks(ctx),
+        lcs(ctx), ctx->list, ctx->numneigh, ctx->nmasked, ctx->cnt);
 }
 
 static void clear_build_counters(MdbCp* ctx)
@@ -1500,6 +1516,7 @@ static int ens_tables(MdbCpEnsemble* e)
         b.pbc = c->pbc, b.gcolumn = c->gcolumn, b.gcol_count = c->gcol_count;
         b.jcol_n = c->jcol_n, b.jcol_start = c->jcol_start, b.gfill = c->gfill;
         b.gtmp = c->gtmp, b.jcol = c->jcol, b.jcbbmin = c->jcbbmin, b.jcbbmax = c->jcbbmax;
+        b.jcbbf = c->jcbbf, b.cxf = c->cxf, b.slot_cap = c->slot_cap;
         b.stencil = c->stencil_d, b.list = c->list, b.numneigh = c->numneigh;
         b.nmasked = c->nmasked;
     }
@@ -1663,6 +1680,7 @@ static void ens_body_batched(MdbCpEnsemble* e, int kind)
         launch_scan_batch(e->s, 3, n, e->d_build);
         stage(CB_GSCATTER);
         stage(CB_MERGE);
+        stage(CB_PREP);
         stage(CB_LIST);
         launch_counters_batch(e->s, n, e->d_build, e->d_cnt_all);
         cudaMemcpyAsync(e->h_cnt_all, e->d_cnt_all, sizeof(int) * CP_SLOTS * n,

@@ -847,6 +847,110 @@ __device__ __forceinline__ double bb_axis(double imin, double imax, double jmin,
 }
 
 #define CP_LIST_WARPS 4
+// resident blocks of 4 warps asked of the register allocator for the list
+// build (latency-bound: occupancy pays more than registers for its rare
+// exact fallbacks)
+#define CP_LIST_MINB 7
+
+// FP32 copies for the prefilter: thread t rounds slot t's position and, if t
+// is a column entry, that entry's box
+__device__ __forceinline__ void list_prep_blk(int bid, int N, int slot_cap, int mbins1,
+    const int* __restrict__ cnt, const int* __restrict__ jcol_start,
+    const double4* __restrict__ jcbbmin, const double4* __restrict__ jcbbmax,
+    const double4* __restrict__ cx, float4* jcbbf, float4* cxf)
+{
+    const int t = bid * blockDim.x + threadIdx.x;
+    if (t < (cnt[CP_NCJ] + cnt[CP_NGC] + 1) * N && t < slot_cap) {
+        const double4 p = cx[t];
+        cxf[t]          = make_float4((float)p.x, (float)p.y, (float)p.z, 0.f);
+    }
+    if (t < jcol_start[mbins1]) {
+        const double4 a = jcbbmin[t], b = jcbbmax[t];
+        jcbbf[2 * t]     = make_float4((float)a.x, (float)a.y, (float)a.z, 0.f);
+        jcbbf[2 * t + 1] = make_float4((float)b.x, (float)b.y, (float)b.z, 0.f);
+    }
+}
+
+__global__ void k_list_prep(int N, int slot_cap, int mbins1, const int* __restrict__ cnt,
+    const int* __restrict__ jcol_start, const double4* __restrict__ jcbbmin,
+    const double4* __restrict__ jcbbmax, const double4* __restrict__ cx, float4* jcbbf,
+    float4* cxf)
+{
+    list_prep_blk(blockIdx.x, N, slot_cap, mbins1, cnt, jcol_start, jcbbmin, jcbbmax, cx, jcbbf,
+        cxf);
+}
+
+void launch_list_prep(cudaStream_t s, int N, int slot_cap, int mbins1, const int* cnt,
+    const int* jcol_start, const double4* jcbbmin, const double4* jcbbmax, const double4* cx,
+    float4* jcbbf, float4* cxf)
+{
+    k_list_prep<<<mdb_blocks(slot_cap, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(N, slot_cap, mbins1,
+        cnt, jcol_start, jcbbmin, jcbbmax, cx, jcbbf, cxf);
+    g_launches++;
+}
+
+__device__ __forceinline__ float bb_axis_f(float imin, float imax, float jmin, float jmax)
+{
+    float dl = imin - jmax, dh = jmin - imax;
+    float dm = dl > dh ? dl : dh;
+    return dm > 0.f ? dm : 0.f;
+}
+
+// The exact FP64 tests, taken only near a threshold: kept out of line so that
+// their registers do not weigh on the FP32 path.
+template <int M, int N>
+__device__ __noinline__ bool exact_any_pair(const double4* __restrict__ ci_x,
+    const double4* __restrict__ cj_x, double cutsq)
+{
+    double3 xi[M];
+#pragma unroll
+    for (int a = 0; a < M; a++) {
+        const double4 p = ci_x[a];
+        xi[a]           = make_double3(p.x, p.y, p.z);
+    }
+    return any_pair<M, N>(xi, cj_x, cutsq);
+}
+
+// the reference's box distance (z, y, x); returns d < cutsq, *in_rbb = d < rbbsq
+__device__ __noinline__ bool exact_box(const double4* __restrict__ imn_p,
+    const double4* __restrict__ imx_p, const double4* __restrict__ jn_p,
+    const double4* __restrict__ jx_p, double cutsq, double rbbsq, bool* in_rbb)
+{
+    const double4 imn = *imn_p, imx = *imx_p, jn = *jn_p, jx = *jx_p;
+    double d = bb_axis(imn.z, imx.z, jn.z, jx.z);
+    d        = d * d;
+    double e = bb_axis(imn.y, imx.y, jn.y, jx.y);
+    d += e * e;
+    e = bb_axis(imn.x, imx.x, jn.x, jx.x);
+    d += e * e;
+    *in_rbb = d < rbbsq;
+    return d < cutsq;
+}
+
+// The reference's pair test decided in FP32 where the rounding margin allows
+// (some pair surely inside cutneigh, or every pair surely outside), else by
+// the exact FP64 test on the i-cluster's slots ci*M.. and the j-cluster's.
+template <int M, int N>
+__device__ __forceinline__ bool any_pair_f(const float3* xif, const float4* __restrict__ cjf,
+    float lo, float hi, const double4* __restrict__ ci_x, const double4* __restrict__ cj_x,
+    double cutsq)
+{
+    bool sure = false, maybe = false;
+#pragma unroll
+    for (int b = 0; b < N; b++) {
+        const float4 xj = __ldg(&cjf[b]);
+#pragma unroll
+        for (int a = 0; a < M; a++) {
+            const float dx = xif[a].x - xj.x, dy = xif[a].y - xj.y, dz = xif[a].z - xj.z;
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            sure |= r2 < lo;
+            maybe |= r2 <= hi;
+        }
+    }
+    if (sure) return true;
+    if (!maybe) return false;
+    return exact_any_pair<M, N>(ci_x, cj_x, cutsq);
+}
 
 template <int M, int N>
 __device__ __forceinline__ void build_list_blk(int bid, int half, int* cnt, Geom g,
@@ -854,6 +958,7 @@ __device__ __forceinline__ void build_list_blk(int bid, int half, int* cnt, Geom
     const int* __restrict__ cbin, const double4* __restrict__ ibbmin,
     const double4* __restrict__ ibbmax, const double4* __restrict__ jcbbmin,
     const double4* __restrict__ jcbbmax, const double4* __restrict__ cx,
+    const float4* __restrict__ jcbbf, const float4* __restrict__ cxf,
     const int* __restrict__ jcol_start, const int* __restrict__ jcol,
     const unsigned long long* __restrict__ zext, int maxneighs, int ks, int cs, int* list,
     int* numneigh, int* nmasked)
@@ -865,15 +970,22 @@ __device__ __forceinline__ void build_list_blk(int bid, int half, int* cnt, Geom
     const int lane = lane_id();
     if (ci >= cnt[CP_NCL]) return;
     const int ci_cj0 = ci / (N / M);
-    const double4 imn = ibbmin[ci], imx = ibbmax[ci];
-    double3 xi[M];
+    const double imnz = ibbmin[ci].z, imxz = ibbmax[ci].z;
+    float3 xif[M];
 #pragma unroll
     for (int a = 0; a < M; a++) {
-        double4 p = cx[ci * M + a];
-        xi[a]     = make_double3(p.x, p.y, p.z);
+        const float4 p = cxf[ci * M + a];
+        xif[a]         = make_float3(p.x, p.y, p.z);
     }
+    // FP32 decisions are taken only outside +-margin of the thresholds
+    const float mg     = g.list_margin;
+    const float cut_lo = (float)g.cutneighsq - mg, cut_hi = (float)g.cutneighsq + mg;
+    const float rbb_lo = (float)g.rbb_sq - mg, rbb_hi = (float)g.rbb_sq + mg;
+    const float imnxf = (float)ibbmin[ci].x, imnyf = (float)ibbmin[ci].y;
+    const float imxxf = (float)ibbmax[ci].x, imxyf = (float)ibbmax[ci].y;
+    const float imnzf = (float)imnz, imxzf = (float)imxz;
     const double zx  = __longlong_as_double((long long)*zext);
-    const double zlo = imn.z - g.cutneigh - zx - 1.0e-6;
+    const double zlo = imnz - g.cutneigh - zx - 1.0e-6;
     const int ib     = cbin[ci];
     int* row         = list + (size_t)ci * cs;
     int total = 0, diag_pos = -1;
@@ -893,7 +1005,7 @@ __device__ __forceinline__ void build_list_blk(int bid, int half, int* cnt, Geom
             R  = s1;
             while (L < R) {
                 int mid = (L + R) >> 1;
-                if (jcbbmin[mid].z - imx.z > g.cutneigh) R = mid;
+                if (jcbbmin[mid].z - imxz > g.cutneigh) R = mid;
                 else L = mid + 1;
             }
             wn = L - lo;
@@ -921,15 +1033,23 @@ __device__ __forceinline__ void build_list_blk(int bid, int half, int* cnt, Geom
                 const int m = s_lo[w][a] + (t - s_ws[w][a]);
                 cj          = jcol[m];
                 if (!(half && ci_cj0 > cj)) {
-                    const double4 jn = jcbbmin[m], jx = jcbbmax[m];
-                    double d = bb_axis(imn.z, imx.z, jn.z, jx.z);
-                    d        = d * d;
-                    double e = bb_axis(imn.y, imx.y, jn.y, jx.y);
-                    d += e * e;
-                    e = bb_axis(imn.x, imx.x, jn.x, jx.x);
-                    d += e * e;
-                    if (d < g.cutneighsq)
-                        ok = d < g.rbb_sq || any_pair<M, N>(xi, cx + (size_t)cj * N, g.cutneighsq);
+                    const float4 fn = __ldg(&jcbbf[2 * m]), fx = __ldg(&jcbbf[2 * m + 1]);
+                    float df = bb_axis_f(imnzf, imxzf, fn.z, fx.z);
+                    df       = df * df;
+                    float ef = bb_axis_f(imnyf, imxyf, fn.y, fx.y);
+                    df += ef * ef;
+                    ef = bb_axis_f(imnxf, imxxf, fn.x, fx.x);
+                    df += ef * ef;
+                    if (df <= cut_hi) {
+                        bool in_cut = true, in_rbb = df < rbb_lo;
+                        if (df >= cut_lo || (df >= rbb_lo && df <= rbb_hi))
+                            in_cut = exact_box(&ibbmin[ci], &ibbmax[ci], &jcbbmin[m],
+                                &jcbbmax[m], g.cutneighsq, g.rbb_sq, &in_rbb);
+                        if (in_cut)
+                            ok = in_rbb || any_pair_f<M, N>(xif, cxf + (size_t)cj * N, cut_lo,
+                                               cut_hi, cx + (size_t)ci * M,
+                                               cx + (size_t)cj * N, g.cutneighsq);
+                    }
                 }
             }
             const unsigned bal = __ballot_sync(0xffffffffu, ok);
@@ -958,24 +1078,27 @@ __device__ __forceinline__ void build_list_blk(int bid, int half, int* cnt, Geom
 }
 
 template <int M, int N>
-__global__ void __launch_bounds__(32 * CP_LIST_WARPS) k_build_list(int half, int* cnt, Geom g,
+__global__ void __launch_bounds__(32 * CP_LIST_WARPS, CP_LIST_MINB) k_build_list(int half, int* cnt, Geom g,
     const int* __restrict__ stencil,
     const int* __restrict__ cbin, const double4* __restrict__ ibbmin,
     const double4* __restrict__ ibbmax, const double4* __restrict__ jcbbmin,
     const double4* __restrict__ jcbbmax, const double4* __restrict__ cx,
+    const float4* __restrict__ jcbbf, const float4* __restrict__ cxf,
     const int* __restrict__ jcol_start, const int* __restrict__ jcol,
     const unsigned long long* __restrict__ zext, int maxneighs, int ks, int cs, int* list,
     int* numneigh, int* nmasked)
 {
     build_list_blk<M, N>(blockIdx.x, half, cnt, g, stencil, cbin, ibbmin, ibbmax, jcbbmin,
-        jcbbmax, cx, jcol_start, jcol, zext, maxneighs, ks, cs, list, numneigh, nmasked);
+        jcbbmax, cx, jcbbf, cxf, jcol_start, jcol, zext, maxneighs, ks, cs, list, numneigh,
+        nmasked);
 }
 
 void launch_build_list(cudaStream_t s, int M, int N, int half, int ncl_cap, const int* cnt,
     const Geom& g, const int* stencil, const int* cbin, const double4* ibbmin,
     const double4* ibbmax, const double4* jcbbmin, const double4* jcbbmax, const double4* cx,
-    const int* jcol_start, const int* jcol, const unsigned long long* zext, int maxneighs,
-    int ks, int cs, int* list, int* numneigh, int* nmasked, int* cnt_out)
+    const float4* jcbbf, const float4* cxf, const int* jcol_start, const int* jcol,
+    const unsigned long long* zext, int maxneighs, int ks, int cs, int* list, int* numneigh,
+    int* nmasked, int* cnt_out)
 {
     long long threads = (long long)ncl_cap * 32;
     int blocks        = mdb_blocks(threads, 32 * CP_LIST_WARPS);
@@ -983,12 +1106,12 @@ void launch_build_list(cudaStream_t s, int M, int N, int half, int ncl_cap, cons
     (void)cnt;
     if (N == 4)
         k_build_list<4, 4><<<blocks, 32 * CP_LIST_WARPS, 0, s>>>(half, cnt_out, g, stencil, cbin,
-            ibbmin, ibbmax, jcbbmin, jcbbmax, cx, jcol_start, jcol, zext, maxneighs, ks, cs, list,
-            numneigh, nmasked);
+            ibbmin, ibbmax, jcbbmin, jcbbmax, cx, jcbbf, cxf, jcol_start, jcol, zext, maxneighs,
+            ks, cs, list, numneigh, nmasked);
     else
         k_build_list<4, 8><<<blocks, 32 * CP_LIST_WARPS, 0, s>>>(half, cnt_out, g, stencil, cbin,
-            ibbmin, ibbmax, jcbbmin, jcbbmax, cx, jcol_start, jcol, zext, maxneighs, ks, cs, list,
-            numneigh, nmasked);
+            ibbmin, ibbmax, jcbbmin, jcbbmax, cx, jcbbf, cxf, jcol_start, jcol, zext, maxneighs,
+            ks, cs, list, numneigh, nmasked);
     g_launches++;
 }
 
@@ -1075,6 +1198,7 @@ int cp_build_stage_blocks(int stage, const CpBuildMember& m, int* threads)
     case CB_GSCATTER: return mdb_blocks(m.ngc_cap, T);
     case CB_CSIZES: return mdb_blocks(mb1, T);
     case CB_MERGE: *threads = 128; return mdb_blocks((long long)mb1 * 32, 128);
+    case CB_PREP: return mdb_blocks(m.slot_cap, T);
     case CB_LIST:
         *threads = 32 * CP_LIST_WARPS;
         return mdb_blocks((long long)m.ncl_cap * 32, 32 * CP_LIST_WARPS);
@@ -1102,7 +1226,8 @@ __device__ __forceinline__ void reset_blk(int bid, const CpBuildMember& m)
 }
 
 template <int STAGE>
-__global__ void __launch_bounds__(256) k_build_stage_batch(const CpBuildMember* __restrict__ tab,
+__global__ void __launch_bounds__(256, STAGE == CB_LIST ? 3 : 1)
+    k_build_stage_batch(const CpBuildMember* __restrict__ tab,
     const int2* __restrict__ bmap)
 {
     const int2 bm          = __ldg(&bmap[blockIdx.x]);
@@ -1159,12 +1284,16 @@ __global__ void __launch_bounds__(256) k_build_stage_batch(const CpBuildMember* 
     case CB_LIST:
         if (m.N == 4)
             build_list_blk<4, 4>(b, m.half, m.cnt, m.g, m.stencil, m.cbin, m.ibbmin, m.ibbmax,
-                m.jcbbmin, m.jcbbmax, m.cx, m.jcol_start, m.jcol, m.zext, m.maxneighs, m.ks,
-                m.cs, m.list, m.numneigh, m.nmasked);
+                m.jcbbmin, m.jcbbmax, m.cx, m.jcbbf, m.cxf, m.jcol_start, m.jcol, m.zext,
+                m.maxneighs, m.ks, m.cs, m.list, m.numneigh, m.nmasked);
         else
             build_list_blk<4, 8>(b, m.half, m.cnt, m.g, m.stencil, m.cbin, m.ibbmin, m.ibbmax,
-                m.jcbbmin, m.jcbbmax, m.cx, m.jcol_start, m.jcol, m.zext, m.maxneighs, m.ks,
-                m.cs, m.list, m.numneigh, m.nmasked);
+                m.jcbbmin, m.jcbbmax, m.cx, m.jcbbf, m.cxf, m.jcol_start, m.jcol, m.zext,
+                m.maxneighs, m.ks, m.cs, m.list, m.numneigh, m.nmasked);
+        break;
+    case CB_PREP:
+        list_prep_blk(b, m.N, m.slot_cap, m.g.mbins + 1, m.cnt, m.jcol_start, m.jcbbmin,
+            m.jcbbmax, m.cx, m.jcbbf, m.cxf);
         break;
     }
 }
@@ -1193,6 +1322,7 @@ void launch_build_stage_batch(cudaStream_t s, int stage, int nblocks, const CpBu
         CP_STAGE(CB_CSIZES)
         CP_STAGE(CB_GSCATTER)
         CP_STAGE(CB_MERGE)
+        CP_STAGE(CB_PREP)
         CP_STAGE(CB_LIST)
 #undef CP_STAGE
     default: return;

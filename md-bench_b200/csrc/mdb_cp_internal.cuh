@@ -62,6 +62,9 @@ struct Geom {
     double binsizex, binsizey, bininvx, bininvy;
     double xprd, yprd, zprd;
     double cutneigh, cutneighsq, rbb_sq;
+    // bound on |FP32 - FP64| of a squared distance or box distance computed
+    // from coordinates rounded to FP32 (the list build's prefilter)
+    float list_margin;
 };
 
 struct Types {
@@ -143,11 +146,17 @@ void launch_ghost_scatter(cudaStream_t s, int ngc_cap, const int* cnt, const int
 void launch_merge_columns(cudaStream_t s, int mbins1, int jfac, const int* ncl_col,
     const int* cl_start, const int* gcol_count, const int* jcol_start, const int* gtmp,
     const double4* jbbmin, const double4* jbbmax, int* jcol, double4* jcbbmin, double4* jcbbmax);
+// FP32 copies for the list build's prefilter: the column-ordered j boxes
+// (jcbbf[2m] min, [2m+1] max) and the slot positions (all j-clusters)
+void launch_list_prep(cudaStream_t s, int N, int slot_cap, int mbins1, const int* cnt,
+    const int* jcol_start, const double4* jcbbmin, const double4* jcbbmax, const double4* cx,
+    float4* jcbbf, float4* cxf);
 void launch_build_list(cudaStream_t s, int M, int N, int half, int ncl_cap, const int* cnt,
     const Geom& g, const int* stencil, const int* cbin, const double4* ibbmin,
     const double4* ibbmax, const double4* jcbbmin, const double4* jcbbmax, const double4* cx,
-    const int* jcol_start, const int* jcol, const unsigned long long* zext, int maxneighs,
-    int ks, int cs, int* list, int* numneigh, int* nmasked, int* cnt_out);
+    const float4* jcbbf, const float4* cxf, const int* jcol_start, const int* jcol,
+    const unsigned long long* zext, int maxneighs, int ks, int cs, int* list, int* numneigh,
+    int* nmasked, int* cnt_out);
 void launch_prune(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt, const double4* cx,
     double cutneighsq, int maxneighs, int ks, int cs, int* list, int* numneigh, int* nmasked);
 
@@ -221,6 +230,8 @@ struct CpBuildMember {
     int *gcount, *gstart, *border, *pbc, *gcolumn, *gcol_count, *jcol_n, *jcol_start, *gfill;
     int *gtmp, *jcol;
     double4 *jcbbmin, *jcbbmax;
+    float4 *jcbbf, *cxf;
+    int slot_cap;
     const int* stencil;
     int *list, *numneigh, *nmasked;
 };
@@ -240,6 +251,7 @@ enum CpBuildStage {
     CB_CSIZES,   // binJClusters: column sizes
     CB_GSCATTER, // binJClusters: ghosts into columns
     CB_MERGE,    // binJClusters: merge by bbminz
+    CB_PREP,     // buildNeighbor: FP32 copies of boxes and positions
     CB_LIST,     // buildNeighbor
     CB_COUNT
 };
