@@ -850,7 +850,7 @@ __device__ __forceinline__ double bb_axis(double imin, double imax, double jmin,
 // resident blocks of 4 warps asked of the register allocator for the list
 // build (latency-bound: occupancy pays more than registers for its rare
 // exact fallbacks)
-#define CP_LIST_MINB 7
+#define CP_LIST_MINB 8
 
 // FP32 copies for the prefilter: thread t rounds slot t's position and, if t
 // is a column entry, that entry's box
