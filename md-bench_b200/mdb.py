@@ -669,9 +669,13 @@ class ClusterSystem:
         self._ck(self.lib.mdb_cp_set_atoms(self.h, len(t), x, v, t), "mdb_cp_set_atoms")
         self.nlocal = len(t)
 
-    def atoms(self):
+    def atoms(self, out=None):
+        """(x, v, type) as updateSingleAtoms last wrote them; out: arrays of those
+        shapes to fill (pinned host memory makes the copy a DMA at full speed)."""
         n = self.nlocal
-        x = np.zeros((n, 3)); v = np.zeros((n, 3)); t = np.zeros(n, dtype=np.int32)
+        if out is None:
+            out = (np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n, dtype=np.int32))
+        x, v, t = out
         self._ck(self.lib.mdb_cp_get_atoms(self.h, _vp(x), _vp(v), _vp(t)), "mdb_cp_get_atoms")
         return x, v, t
 
