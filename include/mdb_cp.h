@@ -107,6 +107,18 @@ int mdb_cp_setup(MdbCp* ctx);
 int mdb_cp_run(MdbCp* ctx, int first_step, int nsteps, MdbThermo* samples, int max_samples,
     int* nsamples);
 
+/* Displacement-checked rebuilds (no counterpart in the reference, which only
+ * rebuilds every reneigh_every steps). With max_displacement > 0, mdb_cp_run
+ * also rebuilds in any step in which some atom has moved farther than
+ * max_displacement since the last build (skin / 2 keeps every list complete
+ * whatever the motion); the integrator tests the displacement and the host
+ * reads one flag per step. 0 (the default) restores the fixed schedule alone.
+ * After a change the next step rebuilds first. */
+int mdb_cp_set_rebuild_check(MdbCp* ctx, double max_displacement);
+/* Rebuilds performed by mdb_cp_run with the check on: on the fixed schedule,
+ * and triggered by the displacement test. */
+int mdb_cp_get_rebuilds(MdbCp* ctx, long long* scheduled, long long* checked);
+
 /* ---- ensembles ----------------------------------------------------------------
  * No counterpart in the reference (which runs one system per process). Many
  * independent systems, each an MdbCp already set up with mdb_cp_setup, of any

@@ -80,6 +80,15 @@ struct MdbCp {
     int energy_blocks = 0; // partial-energy blocks of the last energy evaluation
     CpGraph g_plain;
     unsigned gen = 0; // bumped whenever buffers move (graphs that hold them are stale)
+    // displacement-checked rebuilds (0: the reference's fixed schedule only):
+    // slot positions at the last build, a device flag set by the integrator
+    double disp_max    = 0.0;
+    double4* xbuild    = nullptr;
+    int xbuild_n       = 0;
+    int* dflag         = nullptr;
+    int* h_dflag       = nullptr;
+    bool snap_valid    = false;
+    long long rebuilds_sched = 0, rebuilds_check = 0;
 };
 
 #define RED_SLOTS 64
@@ -272,6 +281,10 @@ static void free_all(MdbCp* ctx)
     dfree(ctx->jcol_n), dfree(ctx->jcol_start), dfree(ctx->gtmp), dfree(ctx->jcol);
     dfree(ctx->jcbbmin), dfree(ctx->jcbbmax), dfree(ctx->jcbbf), dfree(ctx->cxf);
     dfree(ctx->stencil_d), dfree(ctx->list), dfree(ctx->numneigh), dfree(ctx->nmasked);
+    dfree(ctx->xbuild), dfree(ctx->dflag);
+    if (ctx->h_dflag) cudaFreeHost(ctx->h_dflag);
+    ctx->h_dflag  = nullptr;
+    ctx->xbuild_n = 0;
     dfree(ctx->cnt), dfree(ctx->zext), dfree(ctx->scan_scratch), dfree(ctx->partials);
     dfree(ctx->red), dfree(ctx->stage), dfree(ctx->stage_i);
     if (ctx->h_cnt) cudaFreeHost(ctx->h_cnt);
@@ -693,6 +706,28 @@ static int check_build(MdbCp* ctx, int what)
     return eval_build(ctx, what);
 }
 
+// positions of the slots as built, for the displacement check
+static int snapshot(MdbCp* ctx)
+{
+    if (ctx->disp_max <= 0.0) return MDB_OK;
+    const int n = ctx->ncl_cap * ctx->M;
+    if (ctx->xbuild_n < n) {
+        dfree(ctx->xbuild);
+        CK(dalloc(&ctx->xbuild, n));
+        ctx->xbuild_n = n;
+        drop_graph(ctx);
+    }
+    if (!ctx->dflag) {
+        CK(dalloc(&ctx->dflag, 1));
+        CK(cudaMallocHost((void**)&ctx->h_dflag, sizeof(int)));
+    }
+    CK(cudaMemcpyAsync(ctx->xbuild, ctx->cx, sizeof(double4) * n, cudaMemcpyDeviceToDevice,
+        ctx->s));
+    CK(cudaMemsetAsync(ctx->dflag, 0, sizeof(int), ctx->s));
+    ctx->snap_valid = true;
+    return MDB_OK;
+}
+
 static int do_build(MdbCp* ctx)
 {
     for (int attempt = 0; attempt < 8; attempt++) {
@@ -703,7 +738,7 @@ static int do_build(MdbCp* ctx)
         if (r < 0) return -r;
         if (r == 0) {
             ctx->have_clusters = ctx->have_ghosts = ctx->have_list = true;
-            return MDB_OK;
+            return snapshot(ctx);
         }
     }
     return fail(ctx, MDB_ERR_OVERFLOW, "rebuild did not converge");
@@ -730,11 +765,18 @@ static void enq_force(MdbCp* ctx, bool energy)
     }
 }
 
+// the displacement check's arguments for the integrator (none when off)
+static const double4* check_xb(const MdbCp* ctx)
+{
+    return ctx->disp_max > 0.0 && ctx->snap_valid ? ctx->xbuild : nullptr;
+}
+
 static void enq_initial(MdbCp* ctx)
 {
     launch_cp_initial(ctx->s, ctx->M, ctx->N, ctx->ncl_cap, ctx->cnt, ctx->p.dtforce, ctx->p.dt,
         ctx->cx, ctx->cv, ctx->cf, ctx->mixed ? ctx->cf32 : nullptr, ctx->anchor,
-        ctx->mixed ? ctx->xr : nullptr, xr_mode(ctx));
+        ctx->mixed ? ctx->xr : nullptr, xr_mode(ctx), check_xb(ctx),
+        ctx->disp_max * ctx->disp_max, ctx->dflag);
 }
 
 static void enq_final(MdbCp* ctx)
@@ -747,7 +789,8 @@ static void enq_final_initial(MdbCp* ctx)
 {
     launch_cp_final_initial(ctx->s, ctx->M, ctx->N, ctx->ncl_cap, ctx->cnt, ctx->p.dtforce,
         ctx->p.dt, ctx->cx, ctx->cv, ctx->cf, ctx->mixed ? ctx->cf32 : nullptr, ctx->anchor,
-        ctx->mixed ? ctx->xr : nullptr, xr_mode(ctx));
+        ctx->mixed ? ctx->xr : nullptr, xr_mode(ctx), check_xb(ctx),
+        ctx->disp_max * ctx->disp_max, ctx->dflag);
 }
 
 static void enq_ghost_update(MdbCp* ctx)
@@ -1037,6 +1080,92 @@ static int capture_plain(MdbCp* ctx)
     return MDB_OK;
 }
 
+// The timestep loop with the displacement check: each step's initial
+// integration also tests every atom's displacement since the last build; the
+// host reads the flag (one synchronisation per step) and rebuilds in that
+// step when an atom moved farther than disp_max, besides the reference's
+// fixed schedule. Lists are then complete at every step for any motion.
+static int run_checked(MdbCp* ctx, int first_step, int nsteps, MdbThermo* samples,
+    int max_samples, int* nsamples)
+{
+    int nslot = 0;
+    std::vector<int> slot_step;
+    const int last     = first_step + nsteps - 1;
+    bool pending_final = false;
+    for (int n = first_step; n <= last; n++) {
+        const bool sched  = (n + 1) % ctx->p.reneigh_every == 0;
+        const bool prune  = !sched && (n + 1) % ctx->prune_every == 0;
+        const bool sample = max_samples > 0 && (n + 1) % ctx->p.nstat == 0;
+        const bool had    = ctx->snap_valid;
+        long long m       = mark();
+        if (pending_final) enq_final_initial(ctx);
+        else enq_initial(ctx);
+        pending_final = false;
+        account(ctx, m);
+        bool reneigh = sched || !had;
+        if (!reneigh) {
+            CK(cudaMemcpyAsync(ctx->h_dflag, ctx->dflag, sizeof(int), cudaMemcpyDeviceToHost,
+                ctx->s));
+            CK(cudaStreamSynchronize(ctx->s));
+            reneigh = *ctx->h_dflag != 0;
+            if (reneigh) ctx->rebuilds_check++;
+        } else if (sched) {
+            ctx->rebuilds_sched++;
+        }
+        if (reneigh) {
+            m = mark();
+            enq_gather(ctx, 1);
+            account(ctx, m);
+            int rc = do_build(ctx);
+            if (rc) return rc;
+        } else {
+            m = mark();
+            if (prune) enq_prune(ctx);
+            enq_ghost_update(ctx);
+            account(ctx, m);
+        }
+        m = mark();
+        enq_force(ctx, sample);
+        if (sample || n == last) enq_final(ctx);
+        else pending_final = true;
+        if (sample && nslot < RED_SLOTS && nslot < max_samples) {
+            enq_thermo(ctx, nslot, true);
+            slot_step.push_back(n + 1);
+            nslot++;
+        }
+        account(ctx, m);
+    }
+    ctx->energy_valid = nsteps > 0 && max_samples > 0 && ((last + 1) % ctx->p.nstat == 0);
+    CK(cudaGetLastError());
+    if (nslot > 0)
+        CK(cudaMemcpyAsync(ctx->h_red, ctx->red, 4 * sizeof(double) * nslot,
+            cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    for (int k = 0; k < nslot; k++)
+        finish_thermo(ctx, ctx->h_red + 4 * k, slot_step[k], &samples[k]);
+    if (nsamples) *nsamples = nslot;
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_set_rebuild_check(MdbCp* ctx, double max_displacement)
+{
+    if (!ctx || !(max_displacement >= 0.0)) return MDB_ERR_ARG;
+    CK(cudaSetDevice(ctx->dev));
+    CK(cudaStreamSynchronize(ctx->s));
+    drop_graph(ctx);
+    ctx->disp_max   = max_displacement;
+    ctx->snap_valid = false; // the next step rebuilds (and snapshots) first
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_get_rebuilds(MdbCp* ctx, long long* scheduled, long long* checked)
+{
+    if (!ctx) return MDB_ERR_ARG;
+    if (scheduled) *scheduled = ctx->rebuilds_sched;
+    if (checked) *checked = ctx->rebuilds_check;
+    return MDB_OK;
+}
+
 extern "C" int mdb_cp_run(MdbCp* ctx, int first_step, int nsteps, MdbThermo* samples,
     int max_samples, int* nsamples)
 {
@@ -1044,6 +1173,10 @@ extern "C" int mdb_cp_run(MdbCp* ctx, int first_step, int nsteps, MdbThermo* sam
     if (!ctx->have_list) return fail(ctx, MDB_ERR_STATE, "mdb_cp_setup not run");
     if (nsteps < 0 || (max_samples > 0 && !samples)) return MDB_ERR_ARG;
     CK(cudaSetDevice(ctx->dev));
+    if (ctx->disp_max > 0.0) {
+        if (nsamples) *nsamples = 0;
+        return run_checked(ctx, first_step, nsteps, samples, max_samples, nsamples);
+    }
     if (nsamples) *nsamples = 0;
     int nslot = 0;
     std::vector<int> slot_step;

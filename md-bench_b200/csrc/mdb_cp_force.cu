@@ -663,11 +663,14 @@ __device__ __forceinline__ double3 slot_force(int s, const double4* cf, const fl
 
 // zero_f: clear the force slot after its use (half lists accumulate into it;
 // only when a force evaluation follows before anything reads the forces)
+// xb (displacement check, null: off): positions at the last build; a slot
+// that moved farther than sqrt(lim2) since then sets *flag.
 template <bool FINAL, bool INITIAL>
 __device__ __forceinline__ void cp_integrate_slot(int s, int M, int N,
     const int* __restrict__ cnt, double dtf, double dt, double4* cx, double4* cv,
     const double4* __restrict__ cf, float4* cf32, const float4* __restrict__ anchor, float4* xr,
-    bool zero_f, int xmode)
+    bool zero_f, int xmode, const double4* __restrict__ xb = nullptr, double lim2 = 0.0,
+    int* flag = nullptr)
 {
     if (s >= cnt[CP_NCL] * M) return;
     double4 p = cx[s];
@@ -692,6 +695,11 @@ __device__ __forceinline__ void cp_integrate_slot(int s, int M, int N,
         p.z += dt * v.z;
         cx[s] = p;
         if (xr) put_rel(xr, s, p, anchor[s / N], xmode, s % N);
+        if (xb) {
+            const double4 q = xb[s];
+            const double dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+            if (dx * dx + dy * dy + dz * dz > lim2) *flag = 1;
+        }
     }
     cv[s] = v;
 }
@@ -699,10 +707,11 @@ __device__ __forceinline__ void cp_integrate_slot(int s, int M, int N,
 template <bool FINAL, bool INITIAL>
 __global__ void k_cp_integrate(int M, int N, const int* __restrict__ cnt, double dtf, double dt,
     double4* cx, double4* cv, const double4* __restrict__ cf, const float4* __restrict__ cf32,
-    const float4* __restrict__ anchor, float4* xr, int xmode)
+    const float4* __restrict__ anchor, float4* xr, int xmode, const double4* __restrict__ xb,
+    double lim2, int* flag)
 {
     cp_integrate_slot<FINAL, INITIAL>(blockIdx.x * blockDim.x + threadIdx.x, M, N, cnt, dtf, dt,
-        cx, cv, cf, const_cast<float4*>(cf32), anchor, xr, false, xmode);
+        cx, cv, cf, const_cast<float4*>(cf32), anchor, xr, false, xmode, xb, lim2, flag);
 }
 
 template <bool FINAL, bool INITIAL>
@@ -713,7 +722,8 @@ __global__ void k_cp_integrate_batch(const CpStepMember* __restrict__ tab,
     if (bm.x < 0) return;
     const CpStepMember& m = tab[bm.x];
     cp_integrate_slot<FINAL, INITIAL>(bm.y * blockDim.x + threadIdx.x, m.M, m.N, m.cnt, m.dtf,
-        m.dt, m.cx, m.cv, m.cf, m.cf32, m.anchor, m.xr, m.zero_f != 0, m.mixed);
+        m.dt, m.cx, m.cv, m.cf, m.cf32, m.anchor, m.xr, m.zero_f != 0, m.mixed, m.xb, m.lim2,
+        m.flag);
 }
 
 void launch_cp_integrate_batch(cudaStream_t s, bool final_, bool initial, int nblocks,
@@ -729,11 +739,11 @@ void launch_cp_integrate_batch(cudaStream_t s, bool final_, bool initial, int nb
 
 void launch_cp_initial(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt, double dtf,
     double dt, double4* cx, double4* cv, const double4* cf, const float4* cf32,
-    const float4* anchor, float4* xr, int xmode)
+    const float4* anchor, float4* xr, int xmode, const double4* xb, double lim2, int* flag)
 {
     long long n = (long long)ncl_cap * M;
     k_cp_integrate<false, true><<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(M, N, cnt,
-        dtf, dt, cx, cv, cf, cf32, anchor, xr, xmode);
+        dtf, dt, cx, cv, cf, cf32, anchor, xr, xmode, xb, lim2, flag);
     g_launches++;
 }
 
@@ -742,17 +752,18 @@ void launch_cp_final(cudaStream_t s, int M, int ncl_cap, const int* cnt, double 
 {
     long long n = (long long)ncl_cap * M;
     k_cp_integrate<true, false><<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(M, M, cnt,
-        dtf, 0.0, const_cast<double4*>(cx), cv, cf, cf32, nullptr, nullptr, 0);
+        dtf, 0.0, const_cast<double4*>(cx), cv, cf, cf32, nullptr, nullptr, 0, nullptr, 0.0,
+        nullptr);
     g_launches++;
 }
 
 void launch_cp_final_initial(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt,
     double dtf, double dt, double4* cx, double4* cv, const double4* cf, const float4* cf32,
-    const float4* anchor, float4* xr, int xmode)
+    const float4* anchor, float4* xr, int xmode, const double4* xb, double lim2, int* flag)
 {
     long long n = (long long)ncl_cap * M;
     k_cp_integrate<true, true><<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(M, N, cnt,
-        dtf, dt, cx, cv, cf, cf32, anchor, xr, xmode);
+        dtf, dt, cx, cv, cf, cf32, anchor, xr, xmode, xb, lim2, flag);
     g_launches++;
 }
 

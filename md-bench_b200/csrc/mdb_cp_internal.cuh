@@ -173,14 +173,16 @@ int launch_force_mixed(cudaStream_t s, int N, int half, int energy, int ncl_cap,
 int force_mixed_threads(const Types& ty);
 int force_mixed_grid(int ncl_cap, const Types& ty);
 // xmode: the put_rel mode of xr (ignored when xr is null)
+// xb (null: no check): slot positions at the last build; a slot farther than
+// sqrt(lim2) from it sets *flag (the displacement check of a rebuild policy)
 void launch_cp_initial(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt, double dtf,
     double dt, double4* cx, double4* cv, const double4* cf, const float4* cf32,
-    const float4* anchor, float4* xr, int xmode);
+    const float4* anchor, float4* xr, int xmode, const double4* xb, double lim2, int* flag);
 void launch_cp_final(cudaStream_t s, int M, int ncl_cap, const int* cnt, double dtf,
     const double4* cx, double4* cv, const double4* cf, const float4* cf32);
 void launch_cp_final_initial(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt,
     double dtf, double dt, double4* cx, double4* cv, const double4* cf, const float4* cf32,
-    const float4* anchor, float4* xr, int xmode);
+    const float4* anchor, float4* xr, int xmode, const double4* xb, double lim2, int* flag);
 int ke_blocks(int n);
 
 // ---- batched launches over the members of an ensemble -----------------------
@@ -202,6 +204,9 @@ struct CpStepMember { // integrator and ghost update
     double dtf, dt, xprd, yprd, zprd;
     int M, N, mixed; // mixed: 0 FP64, else the xr mode of put_rel
     int zero_f; // half lists: the initial integration clears the forces it used
+    const double4* xb; // displacement check (null: off), see launch_cp_initial
+    double lim2;
+    int* flag;
 };
 struct CpForceMember { // mixed force kernel (row-major lists)
     const int* cnt;

@@ -98,6 +98,7 @@ CP_EXPORTS = [
     "mdb_cp_get_columns", "mdb_cp_get_geometry", "mdb_cp_time_force", "mdb_cp_ensemble_create",
     "mdb_cp_ensemble_destroy", "mdb_cp_ensemble_last_error", "mdb_cp_ensemble_stream",
     "mdb_cp_ensemble_launch_count", "mdb_cp_ensemble_run", "mdb_cp_ensemble_tune",
+    "mdb_cp_set_rebuild_check", "mdb_cp_get_rebuilds",
 ]
 # every symbol include/mdb_host.h declares
 HOST_EXPORTS = [
@@ -171,6 +172,8 @@ def load():
         "mdb_cp_get_geometry": ([vp, vp, vp, vp, ip], ip),
         "mdb_cp_tune": ([vp, C.c_char_p, ip], ip),
         "mdb_cp_time_force": ([vp, ip, C.POINTER(C.c_double)], ip),
+        "mdb_cp_set_rebuild_check": ([vp, C.c_double], ip),
+        "mdb_cp_get_rebuilds": ([vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], ip),
         "mdb_cp_ensemble_create": ([C.POINTER(vp), ip, C.POINTER(vp)], ip),
         "mdb_cp_ensemble_destroy": ([vp], ip),
         "mdb_cp_ensemble_last_error": ([vp], C.c_char_p),
@@ -826,6 +829,19 @@ class ClusterSystem:
 
     def tune(self, key, value):
         self._ck(self.lib.mdb_cp_tune(self.h, key.encode(), int(value)), "mdb_cp_tune")
+
+    def set_rebuild_check(self, max_displacement):
+        """Also rebuild whenever an atom moved farther than max_displacement
+        since the last build (0: the fixed schedule alone)."""
+        self._ck(self.lib.mdb_cp_set_rebuild_check(self.h, float(max_displacement)),
+                 "mdb_cp_set_rebuild_check")
+
+    def rebuilds(self):
+        """(scheduled, displacement-triggered) rebuilds of checked runs."""
+        a, b = C.c_longlong(), C.c_longlong()
+        self._ck(self.lib.mdb_cp_get_rebuilds(self.h, C.byref(a), C.byref(b)),
+                 "mdb_cp_get_rebuilds")
+        return a.value, b.value
 
     def time_force(self, reps=20):
         """Seconds per force launch (CUDA events on the context's stream)."""

@@ -463,3 +463,70 @@ def test_ensemble_batched_groups_half_lists():
                     assert abs(u[key] - w[key]) <= 1e-4 * max(abs(w[key]), 1.0), (k, key)
             assert np.abs(xa - xb).max() < 1e-3, k
     ens.close()
+
+
+# ---- displacement-checked rebuilds -------------------------------------------
+
+def _hot_system(check, n=6, rho=0.95, temp=2.0, precision="fp64"):
+    hp = mdb.host_params(nx=n, ny=n, nz=n, rho=rho, temp=temp)
+    x, v, t = mdb.create_fcc(hp)
+    kw = dict(xprd=hp.xprd, yprd=hp.yprd, zprd=hp.zprd, cutforce=hp.cutforce,
+              cutneigh=hp.cutneigh, dt=hp.dt, dtforce=hp.dtforce, mass=hp.mass,
+              reneigh_every=hp.reneigh_every, nstat=hp.nstat, natoms=len(t), cluster_n=4,
+              precision=precision, ntypes=hp.ntypes)
+    s = mdb.ClusterSystem(**kw)
+    s.set_rebuild_check(check)
+    s.set_atoms(x, v, t)
+    s.setup()
+    return s, kw, (x, v, t)
+
+
+def _local_state(s):
+    x, v, f, t = s.slots()
+    nat = s.iclusters()[0]
+    valid = np.concatenate([np.arange(4) < k for k in nat])
+    return x[:len(valid)][valid], v[:len(valid)][valid], f[:len(valid)][valid], \
+        t[:len(valid)][valid]
+
+
+def _force_error_vs_fresh_build(s, kw):
+    x, v, f, t = _local_state(s)
+    ref = mdb.ClusterSystem(**kw)
+    ref.set_atoms(x, v, t)
+    ref.setup()
+    x2, _, f2, _ = _local_state(ref)
+    o1 = np.lexsort(x.T)
+    o2 = np.lexsort(x2.T)
+    assert np.array_equal(x[o1], x2[o2])
+    err = np.abs(f[o1] - f2[o2]).max() / np.abs(f2).max()
+    ref.close()
+    return err
+
+
+def test_rebuild_check_keeps_lists_complete():
+    """A hot dense liquid (rho 0.95, T 2.0) moves past half the skin within the
+    fixed 20-step period: with the displacement check on, the run rebuilds in
+    between (the scheduled rebuilds still happen), and the forces 17 steps
+    after the last scheduled rebuild equal those of a fresh build (1e-12).
+    (The cluster-pair lists carry enough slack that the fixed schedule missed
+    no pair either in this state; the check guarantees it for any motion.)"""
+    s, kw, _ = _hot_system(0.15)
+    s.run(57, max_samples=0)
+    sched, trig = s.rebuilds()
+    assert sched == 2 and trig > 0
+    assert _force_error_vs_fresh_build(s, kw) <= 1e-12
+    s.close()
+
+
+def test_rebuild_check_idle_when_atoms_barely_move():
+    """A cold lattice (T 0.01) never triggers the check: the trajectory is the
+    fixed schedule's, bit for bit."""
+    a, _, _ = _hot_system(0.15, n=5, rho=0.8442, temp=0.01)
+    b, _, _ = _hot_system(0.0, n=5, rho=0.8442, temp=0.01)
+    sa = a.run(45, max_samples=8)
+    sb = b.run(45, max_samples=8)
+    assert a.rebuilds()[1] == 0
+    assert sa == sb
+    xa, va, _, _ = _local_state(a)
+    xb, vb, _, _ = _local_state(b)
+    assert np.array_equal(xa, xb) and np.array_equal(va, vb)
