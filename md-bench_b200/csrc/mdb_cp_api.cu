@@ -1464,6 +1464,9 @@ struct MdbCpEnsemble {
     size_t off_stage[CB_COUNT] = {};
     int* d_cnt_all = nullptr;
     int* h_cnt_all = nullptr;
+    // displacement check: one flag per member (set by the batched integrator)
+    int* d_flags = nullptr;
+    int* h_flags = nullptr;
     struct Group { // members sharing cluster shape, list form, types and launch shape
         int N, half;
         Types ty;
@@ -1494,6 +1497,11 @@ enum {
     EG_FORCE,    // force
     EG_SAMPLE,   // force with energy, final integration, thermo to the host
     EG_FINAL,    // the final integration left pending by the last step
+    // displacement-checked steps (batched ensembles)
+    EG_CK_FI,     // FI with the check, flags to the host
+    EG_CK_I,      // I with the check, flags to the host
+    EG_REB_NOINT, // the rebuild of EG_REB_* without the integration
+    EG_GHOST,     // ghost update
     EG_COUNT
 };
 static_assert(EG_COUNT <= 16, "graph slots of MdbCpEnsemble");
@@ -1626,6 +1634,9 @@ static int ens_tables(MdbCpEnsemble* e)
         a.jnat = c->jnat, a.dtf = c->p.dtforce, a.dt = c->p.dt, a.xprd = c->g.xprd;
         a.yprd = c->g.yprd, a.zprd = c->g.zprd, a.M = c->M, a.N = c->N, a.mixed = xr_mode(c);
         a.zero_f = c->p.half_neigh;
+        a.xb     = c->disp_max > 0.0 ? c->xbuild : nullptr;
+        a.lim2   = c->disp_max * c->disp_max;
+        a.flag   = nullptr; // set once the flags exist, below
         CpForceMember& f = fo[k];
         f.cnt = c->cnt, f.xr = c->xr, f.anchor = c->anchor, f.list = c->list;
         f.numneigh = c->numneigh, f.cf32 = c->cf32, f.epart = c->partials, f.cs = lcs(c);
@@ -1716,6 +1727,9 @@ static int ens_tables(MdbCpEnsemble* e)
         if (ce == cudaSuccess) ce = cudaMalloc((void**)&e->d_cnt_all, sizeof(int) * CP_SLOTS * n);
         if (ce == cudaSuccess)
             ce = cudaMallocHost((void**)&e->h_cnt_all, sizeof(int) * CP_SLOTS * n);
+        if (ce == cudaSuccess) ce = cudaMalloc((void**)&e->d_flags, sizeof(int) * n);
+        if (ce == cudaSuccess) ce = cudaMallocHost((void**)&e->h_flags, sizeof(int) * n);
+        if (ce == cudaSuccess) ce = cudaMemset(e->d_flags, 0, sizeof(int) * n);
         if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_NOMEM, "ensemble tables", ce);
     }
     if (maps.size() > e->bmap_cap) {
@@ -1731,6 +1745,7 @@ static int ens_tables(MdbCpEnsemble* e)
             return ens_fail(e, MDB_ERR_NOMEM, "ensemble block maps", ce);
         }
     }
+    for (int k = 0; k < n; k++) st[k].flag = e->d_flags + k;
     const char* what = "member table";
     ce = cudaMemcpy(e->d_step, st.data(), sizeof(CpStepMember) * n, cudaMemcpyHostToDevice);
     if (ce == cudaSuccess)
@@ -1788,9 +1803,10 @@ static void ens_body_batched(MdbCpEnsemble* e, int kind)
         if (kind == EG_PLAIN_FI || kind == EG_PLAIN_I) ens_forces(e, false);
         break;
     case EG_REB_FI:
-    case EG_REB_I: {
+    case EG_REB_I:
+    case EG_REB_NOINT: {
         // updateAtoms + the whole rebuild of every member, stage by stage
-        ens_integ(e, fi, true);
+        if (kind != EG_REB_NOINT) ens_integ(e, fi, true);
         const int n = (int)e->m.size();
         auto stage  = [e](int st) {
             launch_build_stage_batch(e->s, st, e->nb_stage[st], e->d_build,
@@ -1818,8 +1834,23 @@ static void ens_body_batched(MdbCpEnsemble* e, int kind)
         launch_counters_batch(e->s, n, e->d_build, e->d_cnt_all);
         cudaMemcpyAsync(e->h_cnt_all, e->d_cnt_all, sizeof(int) * CP_SLOTS * n,
             cudaMemcpyDeviceToHost, e->s);
+        // positions as built, for the members' displacement checks (the
+        // flags are cleared by the host after the rebuild)
+        for (MdbCp* c : e->m)
+            if (c->disp_max > 0.0 && c->xbuild)
+                cudaMemcpyAsync(c->xbuild, c->cx, sizeof(double4) * c->ncl_cap * c->M,
+                    cudaMemcpyDeviceToDevice, e->s);
         break;
     }
+    case EG_CK_FI:
+    case EG_CK_I:
+        ens_integ(e, kind == EG_CK_FI, true);
+        cudaMemcpyAsync(e->h_flags, e->d_flags, sizeof(int) * e->m.size(),
+            cudaMemcpyDeviceToHost, e->s);
+        break;
+    case EG_GHOST:
+        launch_ghost_update_batch(e->s, e->nb_ghost, e->d_step, e->d_bmap + e->off_ghost_dyn);
+        break;
     case EG_FORCE: ens_forces(e, false); break;
     case EG_SAMPLE:
         ens_forces(e, true);
@@ -1922,6 +1953,8 @@ extern "C" int mdb_cp_ensemble_destroy(MdbCpEnsemble* e)
     if (e->d_cnt_all) cudaFree(e->d_cnt_all);
     if (e->h_cnt_all) cudaFreeHost(e->h_cnt_all);
     if (e->h_dyn) cudaFreeHost(e->h_dyn);
+    if (e->d_flags) cudaFree(e->d_flags);
+    if (e->h_flags) cudaFreeHost(e->h_flags);
     if (e->s) cudaStreamDestroy(e->s);
     delete e;
     return MDB_OK;
@@ -1955,11 +1988,13 @@ extern "C" long long mdb_cp_ensemble_launch_count(const MdbCpEnsemble* e)
 // rebuild: one graph for all members, one synchronisation, then members whose
 // buffers overflowed grow and rebuild on their own (their atom arrays already
 // hold the wrapped state, so the rebuild is idempotent)
-static int ens_rebuild(MdbCpEnsemble* e, bool pending_final)
+static int ens_rebuild(MdbCpEnsemble* e, int kind)
 {
-    int rc = ens_launch(e, pending_final ? EG_REB_FI : EG_REB_I);
+    int rc = ens_launch(e, kind);
     if (rc) return rc;
     cudaError_t ce = cudaStreamSynchronize(e->s);
+    if (ce == cudaSuccess && e->d_flags)
+        ce = cudaMemsetAsync(e->d_flags, 0, sizeof(int) * e->m.size(), e->s);
     if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "ensemble rebuild", ce);
     for (size_t k = 0; k < e->m.size(); k++) {
         MdbCp* c = e->m[k];
@@ -1973,6 +2008,7 @@ static int ens_rebuild(MdbCpEnsemble* e, bool pending_final)
             if (rc) return ens_fail(e, rc, c->err.c_str());
         }
         c->have_clusters = c->have_ghosts = c->have_list = true;
+        if (c->disp_max > 0.0 && c->xbuild) c->snap_valid = true;
     }
     return ens_dyn_maps(e);
 }
@@ -1991,6 +2027,20 @@ extern "C" int mdb_cp_ensemble_run(MdbCpEnsemble* e, int first_step, int nsteps,
     for (MdbCp* c : e->m) cudaStreamSynchronize(c->s);
     cudaStreamSynchronize(e->s);
     int nslot = 0, rc;
+    // displacement check (batched ensembles): a member that moved too far
+    // since the last build makes every member rebuild in that step
+    bool checked = false, force_reb = false;
+    for (MdbCp* c : e->m) {
+        if (c->disp_max <= 0.0) continue;
+        if (!e->batched) return ens_fail(e, MDB_ERR_ARG, "the check needs a batched ensemble");
+        checked = true;
+        if (!c->snap_valid) {
+            // no positions of the last build: rebuild first (this allocates)
+            if ((rc = snapshot(c))) return ens_fail(e, rc, c->err.c_str());
+            cudaStreamSynchronize(c->s);
+            force_reb = true;
+        }
+    }
     // members may have been rebuilt on their own since the last run
     if ((rc = ens_dyn_maps(e))) return rc;
     const int last     = first_step + nsteps - 1;
@@ -1999,7 +2049,29 @@ extern "C" int mdb_cp_ensemble_run(MdbCpEnsemble* e, int first_step, int nsteps,
         const bool reneigh = (step + 1) % c0->p.reneigh_every == 0;
         const bool prune   = !reneigh && (step + 1) % c0->prune_every == 0;
         const bool sample  = max_samples > 0 && (step + 1) % c0->p.nstat == 0 && nslot < max_samples;
-        if (prune) {
+        if (checked && !prune && !reneigh && !force_reb) {
+            if ((rc = ens_launch(e, pending_final ? EG_CK_FI : EG_CK_I))) return rc;
+            pending_final  = false;
+            cudaError_t ce = cudaStreamSynchronize(e->s);
+            if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "ensemble check", ce);
+            bool any = false;
+            for (int k = 0; k < n; k++) any = any || e->h_flags[k] != 0;
+            if (any) {
+                if ((rc = ens_rebuild(e, EG_REB_NOINT))) return rc;
+                for (MdbCp* c : e->m) c->rebuilds_check++;
+            } else if ((rc = ens_launch(e, EG_GHOST))) {
+                return rc;
+            }
+            if ((rc = ens_launch(e, sample ? EG_SAMPLE : EG_FORCE))) return rc;
+            pending_final = !sample;
+        } else if (checked && !prune) {
+            // scheduled (or first) rebuild
+            if ((rc = ens_rebuild(e, pending_final ? EG_REB_FI : EG_REB_I))) return rc;
+            for (MdbCp* c : e->m) (reneigh ? c->rebuilds_sched : c->rebuilds_check)++;
+            force_reb = false;
+            if ((rc = ens_launch(e, sample ? EG_SAMPLE : EG_FORCE))) return rc;
+            pending_final = !sample;
+        } else if (prune) {
             // rare (default never): direct launches on the members' streams
             cudaStreamSynchronize(e->s);
             const long long m0 = mark();
@@ -2014,7 +2086,7 @@ extern "C" int mdb_cp_ensemble_run(MdbCpEnsemble* e, int first_step, int nsteps,
             e->launches += mark() - m0;
             pending_final = true;
         } else if (reneigh) {
-            if ((rc = ens_rebuild(e, pending_final))) return rc;
+            if ((rc = ens_rebuild(e, pending_final ? EG_REB_FI : EG_REB_I))) return rc;
             if ((rc = ens_launch(e, sample ? EG_SAMPLE : EG_FORCE))) return rc;
             pending_final = !sample;
         } else {

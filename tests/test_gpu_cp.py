@@ -530,3 +530,43 @@ def test_rebuild_check_idle_when_atoms_barely_move():
     xa, va, _, _ = _local_state(a)
     xb, vb, _, _ = _local_state(b)
     assert np.array_equal(xa, xb) and np.array_equal(va, vb)
+
+
+def test_ensemble_rebuild_check():
+    """Batched ensemble with the displacement check: cold replicas never trip it
+    and follow the fixed schedule bit for bit; with a hot replica in the set
+    every member rebuilds when it trips, and each member's forces 17 steps
+    after the last scheduled rebuild agree with a fresh build (mixed
+    precision: RMS 1e-5 of the force scale)."""
+    cold = [(4, 0.8442, 0.02), (5, 0.8, 0.05)]
+    a = [_hot_system(0.15, n, rho, T, "mixed")[0] for n, rho, T in cold]
+    b = [_hot_system(0.0, n, rho, T, "mixed")[0] for n, rho, T in cold]
+    ea, eb = mdb.Ensemble(a), mdb.Ensemble(b)
+    assert ea.run(45, max_samples=8) == eb.run(45, max_samples=8)
+    assert a[0].rebuilds()[1] == 0
+    for u, w in zip(a, b):
+        xu, vu, _, _ = _local_state(u)
+        xw, vw, _, _ = _local_state(w)
+        assert np.array_equal(xu, xw) and np.array_equal(vu, vw)
+    ea.close()
+    eb.close()
+    hot = [(6, 0.95, 2.0), (4, 0.8, 0.5)]
+    sys_kw = [_hot_system(0.15, n, rho, T, "mixed")[:2] for n, rho, T in hot]
+    members = [s for s, _ in sys_kw]
+    ens = mdb.Ensemble(members)
+    ens.run(57, max_samples=0)
+    sched, trig = members[1].rebuilds()
+    assert sched == 2 and trig > 0
+    for s, kw in sys_kw:
+        x, v, f, t = _local_state(s)
+        ref = mdb.ClusterSystem(**kw)
+        ref.set_atoms(x, v, t)
+        ref.setup()
+        x2, _, f2, _ = _local_state(ref)
+        o1, o2 = np.lexsort(x.T), np.lexsort(x2.T)
+        assert np.array_equal(x[o1], x2[o2])
+        rms = np.sqrt(np.mean(np.sum(f2 * f2, axis=1)))
+        d = f[o1] - f2[o2]
+        assert np.sqrt(np.mean(np.sum(d * d, axis=1))) <= 1e-5 * rms
+        ref.close()
+    ens.close()
