@@ -48,7 +48,9 @@ int mdb_cp_synchronize(MdbCp* ctx);
  * multiple of 32; default 128); "force_variant" = 0..3: 0 and 1 prefetch the
  * j data one or two list blocks ahead with no register budget, 2 and 3 the same
  * with a budget for 8 resident blocks of 128 threads per SM (these run blocks
- * of 128 threads; default 2). */
+ * of 128 threads; default 2); "force_swizzle" = 1: the blocks one resident
+ * slot runs in turn take neighbouring i-clusters (L1 reuse of j data; default
+ * 0, measured within 2 % either way). */
 int mdb_cp_tune(MdbCp* ctx, const char* key, int value);
 /* Device time of one force evaluation (no energy) on the context's stream:
  * the mean over reps back-to-back launches after two untimed ones, from CUDA

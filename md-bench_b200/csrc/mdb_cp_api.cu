@@ -234,6 +234,7 @@ static int setup_types(MdbCp* ctx)
     t.uniform     = uniform ? 1 : 0;
     t.force_block   = 128;
     t.force_variant = 2; // measured fastest on B200 at 1M atoms (4x4 and 4x8, full and half)
+    t.force_swizzle = 0;
     t.eps0        = t.sqrt_eps[0] * t.sqrt_eps[0];
     t.sigma6_0 = t.sigma3[0] * t.sigma3[0];
     return MDB_OK;
@@ -250,6 +251,12 @@ extern "C" int mdb_cp_tune(MdbCp* ctx, const char* key, int value)
         if (value < 32 || value > 512 || value % 32) return MDB_ERR_ARG;
         drop_graph(ctx);
         ctx->ty.force_block = value;
+        return MDB_OK;
+    }
+    if (!strcmp(key, "force_swizzle")) {
+        if (value < 0 || value > 1) return MDB_ERR_ARG;
+        drop_graph(ctx);
+        ctx->ty.force_swizzle = value;
         return MDB_OK;
     }
     if (!strcmp(key, "force_variant")) {

@@ -2,6 +2,8 @@
 // mixed), the cluster-layout integrator and the thermo partial sums.
 #include <math.h>
 
+#include <algorithm>
+
 #include "mdb_cp_internal.cuh"
 
 namespace mdb {
@@ -516,16 +518,22 @@ __device__ __forceinline__ void load_type_tables(const Types& ty, float* s_se, f
     __syncthreads();
 }
 
+// slots > 0: the grid is slots x K blocks and block b works on block
+// (b % slots) * K + b / slots, so that the blocks one resident slot runs one
+// after another take neighbouring i-clusters, whose j data is then still in
+// that SM's L1 (blocks of a launch start in index order)
 template <int N, bool HALF, bool ENERGY, bool UNIFORM, int PF, int MINB>
 __global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_force_mixed(
     const int* __restrict__ cnt,
     const float4* __restrict__ xr, const float4* __restrict__ anchor, Types ty,
     float cutforcesq, const int* __restrict__ list, int ks, int cs,
-    const int* __restrict__ numneigh, float4* cf32, double* epart)
+    const int* __restrict__ numneigh, float4* cf32, double* epart, int slots)
 {
     __shared__ float s_se[MDB_MAX_TYPES], s_s3[MDB_MAX_TYPES];
     load_type_tables(ty, s_se, s_s3);
-    force_mixed_block<N, HALF, ENERGY, UNIFORM, PF>(blockIdx.x, cnt, xr, anchor, ty, cutforcesq,
+    int bid = blockIdx.x;
+    if (slots > 0) bid = (blockIdx.x % slots) * (gridDim.x / slots) + blockIdx.x / slots;
+    force_mixed_block<N, HALF, ENERGY, UNIFORM, PF>(bid, cnt, xr, anchor, ty, cutforcesq,
         list, ks, cs, numneigh, cf32, epart, s_se, s_s3);
 }
 
@@ -607,10 +615,24 @@ static void run_mixed(cudaStream_t s, int blocks, const int* cnt, const float4* 
 {
     const int v  = ty.force_variant;
     const int nt = force_mixed_threads(ty);
-    const int nb = blocks;
+    int nb = blocks, slots = 0;
+    if (!ENERGY && ty.force_swizzle) {
+        // resident blocks of the whole GPU: the SM count times the blocks of
+        // this shape one SM holds
+        static int nsm = 0;
+        if (!nsm) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        }
+        const int per_sm = (v & 2) ? 8 : std::max(1, 2048 / nt);
+        slots            = nsm * per_sm;
+        if (nb > slots) nb = (nb + slots - 1) / slots * slots;
+        else slots = 0;
+    }
 #define CP_RUN(PF, MB)                                                                   \
     k_force_mixed<N, HALF, ENERGY, UNIFORM, PF, MB><<<nb, nt, 0, s>>>(cnt, xr, anchor, ty,   \
-        cutforcesq, list, ks, cs, numneigh, cf32, epart)
+        cutforcesq, list, ks, cs, numneigh, cf32, epart, slots)
     switch (v) {
     case 1: CP_RUN(2, 0); break;
     case 2: CP_RUN(1, 8); break;

@@ -74,6 +74,7 @@ struct Types {
     double eps0, sigma6_0; // uniform case
     int force_block;       // threads per block of the mixed force kernel (tunable)
     int force_variant;     // mixed force kernel: bit 0 prefetch 2 ahead, bit 1 register budget
+    int force_swizzle;     // mixed force kernel: blocks walk contiguous cluster ranges (0/1)
 };
 
 __device__ __forceinline__ int slot_type(const double4& p) { return (int)__double_as_longlong(p.w); }
