@@ -176,9 +176,10 @@ int mdb_run(MdbCtx* ctx, int first_step, int nsteps, MdbThermo* samples, int max
 
 /* ---- allocation-free entry point -------------------------------------------
  * No counterpart in the reference. For callers that keep their own device
- * arrays and cannot allocate device memory (inside their own stream capture,
- * under an allocator that owns the device, in a loop that must not call
- * cudaMalloc): sum over n atoms of mass * (vx^2 + vy^2 + vz^2), the sum that
+ * arrays and cannot let a library allocate device memory (a framework whose
+ * allocator has reserved the device's memory, a timed loop in which
+ * cudaMalloc would synchronise the device, a plugin host that forbids it):
+ * sum over n atoms of mass * (vx^2 + vy^2 + vz^2), the sum that
  * computeThermo turns into T (common/thermo.c:74-77; T = sum * mvv2e / dof).
  * d_v: n AoS velocity triples in device memory; d_out: one double in device
  * memory; stream: a cudaStream_t (NULL = legacy default stream). Asynchronous.

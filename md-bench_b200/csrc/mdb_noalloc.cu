@@ -1,13 +1,14 @@
 // mdb_kinetic_sum_noalloc: the thermo velocity reduction for callers that own
 // their device buffers and cannot allocate device memory.
 //
-// Who needs it: code that drives its own MD state on the GPU and calls into
-// this library from a place where cudaMalloc is not allowed or not wanted -
-// while its stream is being captured into a CUDA graph, under a host
-// allocator that owns the whole device pool, or from a real-time loop that
-// must not touch the driver's allocator. mdb_thermo needs a context, and
-// creating a context allocates; this entry point only reads the caller's
-// velocities and writes the caller's output.
+// Who needs it: code that keeps its own MD state on the GPU and may not let a
+// library allocate device memory - a framework whose caching allocator or
+// memory pool has reserved the device's memory up front (a cudaMalloc from
+// here would fail or fragment that pool), a timed or latency-critical loop
+// in which cudaMalloc / cudaFree would synchronise the device, or a plugin
+// host that forbids its libraries to own device memory. mdb_thermo needs a
+// context, and creating a context allocates; this entry point only reads the
+// caller's velocities and writes the caller's output.
 //
 // Scratch: the per-block partial sums live in a file-scope __device__ array of
 // NOALLOC_MAX_PARTIALS doubles (32 KiB on every device that loads this
@@ -30,7 +31,7 @@ constexpr int NOALLOC_MAX_PARTIALS = 4096;
 constexpr int NOALLOC_THREADS      = 256;
 constexpr int NOALLOC_MAX_DEVICES  = 64;
 
-__device__ __align__(256) double g_noalloc_partials[NOALLOC_MAX_PARTIALS];
+static __device__ __align__(256) double g_noalloc_partials[NOALLOC_MAX_PARTIALS];
 
 std::mutex g_noalloc_lock;
 double* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
@@ -82,7 +83,8 @@ extern "C" int mdb_kinetic_sum_noalloc(const double* d_v, int n, double mass, do
     double* scratch = nullptr;
     {
         // once per device, with that device current: the device address of
-        // the static array (must happen outside any stream capture)
+        // the static array (the first call on a device does this look-up, so
+        // make that call before any stream capture)
         std::lock_guard<std::mutex> lock(g_noalloc_lock);
         if (!g_noalloc_addr[dev]) {
             void* p = nullptr;

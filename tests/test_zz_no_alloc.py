@@ -1,7 +1,8 @@
 """mdb_kinetic_sum_noalloc, the allocation-free thermo reduction.
 
-It serves callers that own their device arrays and may not allocate device
-memory (for example while their stream is being captured into a CUDA graph).
+It serves callers that own their device arrays and may not let a library
+allocate device memory (a framework whose allocator has reserved the device's
+memory, or a timed loop in which cudaMalloc would synchronise the device).
 This test feeds it velocities that the test itself placed on the device and
 checks, on two calls in a row with different states, that its sum gives the
 same temperature as mdb_thermo on the same state, to 1e-12 relative (the two
