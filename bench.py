@@ -396,31 +396,70 @@ def c4_ensemble(torch, mdb, args, device, rank=0, world=1, dist=None):
                          "replicas_per_shape": shapes}}
 
 
-def e2e(torch, s, init, steps, every):
-    """Same metric through the public C ABI with host buffers: each step uploads
-    the atoms from pinned host memory, runs setup + one rebuild period, and
-    reads positions and velocities back."""
+# systems in flight in the end-to-end measurement (each its own context,
+# device buffers, stream and host thread)
+E2E_INFLIGHT = 2
+
+
+def e2e(torch, systems, init, steps, every, device):
+    """Same metric through the public C ABI with host buffers: each step
+    uploads one system's atoms from pinned host memory, runs setup + one
+    rebuild period and reads positions and velocities back into pinned host
+    memory. ``systems`` are independent contexts, each driven by its own host
+    thread (the ABI calls release the GIL), so that one step's copies and
+    host-side waits overlap another step's kernels, as a caller feeding a
+    stream of systems would run them; every step's copies stay inside the
+    timed region."""
+    import threading
     x, v, t = init
     n = len(t)
-    hx = torch.from_numpy(np.ascontiguousarray(x)).pin_memory().numpy()
-    hv = torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy()
-    ht = torch.from_numpy(np.ascontiguousarray(t)).pin_memory().numpy()
+
+    def pinned(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+
+    hx, hv, ht = pinned(x), pinned(v), pinned(t)
     bi = hx.nbytes + hv.nbytes + ht.nbytes
     bo = 2 * 3 * 8 * n + 4 * n
-    # results land in pinned host buffers as well
-    out = tuple(torch.empty(a.shape, dtype=torch.float64 if a.dtype == np.float64
-                            else torch.int32).pin_memory().numpy() for a in (hx, hv, ht))
-    s.synchronize()
-    t0 = time.perf_counter()
-    for k in range(steps):
+    # results land in pinned host buffers as well, one set per system
+    outs = [tuple(pinned(np.empty_like(a)) for a in (hx, hv, ht)) for _ in systems]
+    share = [steps // len(systems) + (1 if k < steps % len(systems) else 0)
+             for k in range(len(systems))]
+    errors = []
+
+    def work(k):
+        try:
+            torch.cuda.set_device(device)
+            s, out = systems[k], outs[k]
+            for _ in range(share[k]):
+                s.set_atoms(hx, hv, ht)
+                s.setup()
+                s.run(every, first_step=0)
+                s.atoms(out=out)
+            s.synchronize()
+        except Exception as e:  # re-raised on the calling thread
+            errors.append(e)
+
+    # one untimed step per system: first-use allocations and graph captures
+    for s, out in zip(systems, outs):
         s.set_atoms(hx, hv, ht)
         s.setup()
         s.run(every, first_step=0)
         s.atoms(out=out)
-    s.synchronize()
+        s.synchronize()
+    workers = [threading.Thread(target=work, args=(k,)) for k in range(len(systems))]
+    t0 = time.perf_counter()
+    for w in workers:
+        w.start()
+    for w in workers:
+        w.join()
     secs = time.perf_counter() - t0
+    if errors:
+        raise errors[0]
+    for k, out in enumerate(outs):
+        if share[k] and not np.all(np.isfinite(out[0])):
+            raise RuntimeError("end-to-end run returned non-finite positions")
     return dict(value=n * every * steps / secs, unit="atom-steps/s", h2d_bytes_per_step=bi,
-                d2h_bytes_per_step=bo)
+                d2h_bytes_per_step=bo, systems_in_flight=len(systems))
 
 
 def host_has_avx512():
@@ -670,7 +709,16 @@ def main():
         var["stub_gather_fp64"] = stub_bench(torch, mdb, local)
 
     # end to end from the state the timed run reached (a liquid, as in use)
-    e2 = e2e(torch, s, s.atoms(), max(args.steps // 5, 3), 20)
+    extra_sys = [cp_workload(mdb, HEAD["precision"], local, half=HEAD["half"])[0]
+                 for _ in range(E2E_INFLIGHT - 1)]
+    for es in extra_sys:
+        for kv in (args.tune.split(",") if getattr(args, "tune", None) else []):
+            k, val = kv.split("=")
+            es.tune(k, int(val))
+    e2 = e2e(torch, [s] + extra_sys, s.atoms(), max(args.steps // 4, 4 * E2E_INFLIGHT), 20,
+             local)
+    for es in extra_sys:
+        es.close()
     e2["value"] = reduce_scalar(torch, dist, e2["value"], "sum", "cuda")
     cb = cpu_baseline(half=HEAD["half"]) if (rank == 0 and world == 1) else None
     if rank == 0:

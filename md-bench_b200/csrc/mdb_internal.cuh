@@ -232,7 +232,10 @@ void launch_eam_mixed(cudaStream_t s, int energy, int nlocal, int ghost_cap, con
     float cutforcesq, EamDev eam, const int* border_map, const int* counters, double* fp,
     double* fx, double* fy, double* fz, double* epart_rho, double* epart_pair);
 
-extern long long g_launches; // launches issued through these helpers (all contexts)
+// launches issued through these helpers by the calling host thread (per
+// thread, so that contexts driven from different threads count their own:
+// a context is used by one thread at a time)
+extern thread_local long long g_launches;
 
 } // namespace mdb
 

@@ -7,7 +7,7 @@
 
 namespace mdb {
 
-long long g_launches = 0;
+thread_local long long g_launches = 0;
 
 // ---- integrator: verletlist/integrate.c:21-42 -------------------------------
 __device__ __forceinline__ void initial_step(int i, double dtf, double dt, double4* x,
