@@ -56,6 +56,7 @@ struct MdbCp {
     int *gcount = nullptr, *gstart = nullptr, *border = nullptr, *pbc = nullptr;
     int *gcolumn = nullptr, *gcol_count = nullptr, *gfill = nullptr, *jcol_n = nullptr;
     int *jcol_start = nullptr, *gtmp = nullptr, *jcol = nullptr;
+    int* ztab = nullptr; // the list build's window table (Geom zq, z0, zinv)
     double4 *jcbbmin = nullptr, *jcbbmax = nullptr;
     float4 *jcbbf = nullptr, *cxf = nullptr; // FP32 copies for the list build
     int* stencil_d = nullptr;
@@ -210,6 +211,17 @@ static void setup_columns(MdbCp* ctx)
         const double bnd  = 4.0 * e * 3.0 * cut + 12.0 * e * e + 8.0 * g.cutneighsq * 0x1p-24;
         g.list_margin     = (float)(2.0 * bnd);
     }
+    // window table of the list build: buckets of about a quarter of a
+    // j-cluster's height over the z range of local and ghost j-clusters
+    {
+        const double per_col = (double)p.natoms / ((double)ctx->N * g.nbinx * g.nbiny);
+        const double span    = zprd + 2.0 * cut + 2.0;
+        double dz            = 0.25 * zprd / std::max(per_col, 1.0);
+        if (!(dz > span / 8192.0)) dz = span / 8192.0;
+        g.z0   = -cut - 1.0;
+        g.zinv = 1.0 / dz;
+        g.zq   = std::max(1, (int)ceil(span * g.zinv));
+    }
 }
 
 // computePerTypeLJParameters (common/parameter.c:31-45): per-type sqrt(eps)
@@ -286,6 +298,7 @@ static void free_all(MdbCp* ctx)
     dfree(ctx->jbbmax), dfree(ctx->gcount), dfree(ctx->gstart), dfree(ctx->border);
     dfree(ctx->pbc), dfree(ctx->gcolumn), dfree(ctx->gcol_count), dfree(ctx->gfill);
     dfree(ctx->jcol_n), dfree(ctx->jcol_start), dfree(ctx->gtmp), dfree(ctx->jcol);
+    dfree(ctx->ztab);
     dfree(ctx->jcbbmin), dfree(ctx->jcbbmax), dfree(ctx->jcbbf), dfree(ctx->cxf);
     dfree(ctx->stencil_d), dfree(ctx->list), dfree(ctx->numneigh), dfree(ctx->nmasked);
     dfree(ctx->xbuild), dfree(ctx->dflag);
@@ -375,6 +388,7 @@ extern "C" int mdb_cp_create(const MdbParams* params, int cluster_n, int prune_e
             (e = dalloc(&ctx->gfill, mb1)) != cudaSuccess ||
             (e = dalloc(&ctx->jcol_n, mb1)) != cudaSuccess ||
             (e = dalloc(&ctx->jcol_start, mb1 + 1)) != cudaSuccess ||
+            (e = dalloc(&ctx->ztab, (size_t)ctx->g.mbins * (ctx->g.zq + 2))) != cudaSuccess ||
             (e = dalloc(&ctx->red, 4 * RED_SLOTS)) != cudaSuccess ||
             (e = cudaMallocHost((void**)&ctx->h_cnt, CP_SLOTS * sizeof(int))) != cudaSuccess ||
             (e = cudaMallocHost((void**)&ctx->h_red, 4 * RED_SLOTS * sizeof(double))) !=
@@ -649,11 +663,11 @@ static int lcs(const MdbCp* ctx) { return ctx->mixed ? ctx->maxneighs : 1; }
 
 static void enq_list(MdbCp* ctx)
 {
-    launch_list_prep(ctx->s, ctx->N, ctx->slot_cap, ctx->g.mbins + 1, ctx->cnt,
-        ctx->jcol_start, ctx->jcbbmin, ctx->jcbbmax, ctx->cx, ctx->jcbbf, ctx->cxf);
+    launch_list_prep(ctx->s, ctx->N, ctx->slot_cap, ctx->g, ctx->cnt, ctx->jcol_start,
+        ctx->jcbbmin, ctx->jcbbmax, ctx->cx, ctx->jcbbf, ctx->cxf, ctx->ztab);
     launch_build_list(ctx->s, ctx->M, ctx->N, ctx->p.half_neigh, ctx->ncl_cap, ctx->cnt, ctx->g,
         ctx->stencil_d, ctx->cbin, ctx->ibbmin, ctx->ibbmax, ctx->jcbbmin, ctx->jcbbmax, ctx->cx,
-        ctx->jcbbf, ctx->cxf, ctx->jcol_start, ctx->jcol, ctx->zext, ctx->maxneighs, lks(ctx),
+        ctx->jcbbf, ctx->cxf, ctx->jcol, ctx->ztab, ctx->zext, ctx->maxneighs, lks(ctx),
         lcs(ctx), ctx->list, ctx->numneigh, ctx->nmasked, ctx->cnt);
 }
 
@@ -1667,7 +1681,7 @@ static int ens_tables(MdbCpEnsemble* e)
         b.pbc = c->pbc, b.gcolumn = c->gcolumn, b.gcol_count = c->gcol_count;
         b.jcol_n = c->jcol_n, b.jcol_start = c->jcol_start, b.gfill = c->gfill;
         b.gtmp = c->gtmp, b.jcol = c->jcol, b.jcbbmin = c->jcbbmin, b.jcbbmax = c->jcbbmax;
-        b.jcbbf = c->jcbbf, b.cxf = c->cxf, b.slot_cap = c->slot_cap;
+        b.jcbbf = c->jcbbf, b.cxf = c->cxf, b.slot_cap = c->slot_cap, b.ztab = c->ztab;
         b.stencil = c->stencil_d, b.list = c->list, b.numneigh = c->numneigh;
         b.nmasked = c->nmasked;
     }

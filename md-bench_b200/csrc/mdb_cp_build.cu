@@ -853,39 +853,60 @@ __device__ __forceinline__ double bb_axis(double imin, double imax, double jmin,
 #define CP_LIST_MINB 8
 
 // FP32 copies for the prefilter: thread t rounds slot t's position and, if t
-// is a column entry, that entry's box
-__device__ __forceinline__ void list_prep_blk(int bid, int N, int slot_cap, int mbins1,
+// is a column entry, that entry's box. Window table: entry q of column c
+// (t = c * (zq + 2) + q) is the first entry of the column whose bbminz lies
+// in bucket q or above (the column end for q = zq + 1), so that the entries
+// of buckets [qa, qb] are [ztab[qa], ztab[qb + 1]).
+__host__ __device__ __forceinline__ int list_prep_threads(const Geom& g, int slot_cap)
+{
+    const int zt = g.mbins * (g.zq + 2);
+    return slot_cap > zt ? slot_cap : zt;
+}
+
+__device__ __forceinline__ void list_prep_blk(int bid, int N, int slot_cap, const Geom& g,
     const int* __restrict__ cnt, const int* __restrict__ jcol_start,
     const double4* __restrict__ jcbbmin, const double4* __restrict__ jcbbmax,
-    const double4* __restrict__ cx, float4* jcbbf, float4* cxf)
+    const double4* __restrict__ cx, float4* jcbbf, float4* cxf, int* ztab)
 {
     const int t = bid * blockDim.x + threadIdx.x;
     if (t < (cnt[CP_NCJ] + cnt[CP_NGC] + 1) * N && t < slot_cap) {
         const double4 p = cx[t];
         cxf[t]          = make_float4((float)p.x, (float)p.y, (float)p.z, 0.f);
     }
-    if (t < jcol_start[mbins1]) {
+    if (t < jcol_start[g.mbins + 1]) {
         const double4 a = jcbbmin[t], b = jcbbmax[t];
         jcbbf[2 * t]     = make_float4((float)a.x, (float)a.y, (float)a.z, 0.f);
         jcbbf[2 * t + 1] = make_float4((float)b.x, (float)b.y, (float)b.z, 0.f);
     }
+    const int zn = g.zq + 2;
+    if (t < g.mbins * zn) {
+        const int c = t / zn, q = t - c * zn;
+        int L = jcol_start[c], R = jcol_start[c + 1];
+        while (L < R) {
+            const int mid = (L + R) >> 1;
+            if (zbucket(g, jcbbmin[mid].z) < q) L = mid + 1;
+            else R = mid;
+        }
+        ztab[t] = L;
+    }
 }
 
-__global__ void k_list_prep(int N, int slot_cap, int mbins1, const int* __restrict__ cnt,
+__global__ void k_list_prep(int N, int slot_cap, Geom g, const int* __restrict__ cnt,
     const int* __restrict__ jcol_start, const double4* __restrict__ jcbbmin,
     const double4* __restrict__ jcbbmax, const double4* __restrict__ cx, float4* jcbbf,
-    float4* cxf)
+    float4* cxf, int* ztab)
 {
-    list_prep_blk(blockIdx.x, N, slot_cap, mbins1, cnt, jcol_start, jcbbmin, jcbbmax, cx, jcbbf,
-        cxf);
+    list_prep_blk(blockIdx.x, N, slot_cap, g, cnt, jcol_start, jcbbmin, jcbbmax, cx, jcbbf, cxf,
+        ztab);
 }
 
-void launch_list_prep(cudaStream_t s, int N, int slot_cap, int mbins1, const int* cnt,
+void launch_list_prep(cudaStream_t s, int N, int slot_cap, const Geom& g, const int* cnt,
     const int* jcol_start, const double4* jcbbmin, const double4* jcbbmax, const double4* cx,
-    float4* jcbbf, float4* cxf)
+    float4* jcbbf, float4* cxf, int* ztab)
 {
-    k_list_prep<<<mdb_blocks(slot_cap, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(N, slot_cap, mbins1,
-        cnt, jcol_start, jcbbmin, jcbbmax, cx, jcbbf, cxf);
+    const long long zt = (long long)g.mbins * (g.zq + 2);
+    k_list_prep<<<mdb_blocks(slot_cap > zt ? slot_cap : zt, MDB_NTHREADS), MDB_NTHREADS, 0,
+        s>>>(N, slot_cap, g, cnt, jcol_start, jcbbmin, jcbbmax, cx, jcbbf, cxf, ztab);
     g_launches++;
 }
 
@@ -959,7 +980,7 @@ __device__ __forceinline__ void build_list_blk(int bid, int half, int* cnt, Geom
     const double4* __restrict__ ibbmax, const double4* __restrict__ jcbbmin,
     const double4* __restrict__ jcbbmax, const double4* __restrict__ cx,
     const float4* __restrict__ jcbbf, const float4* __restrict__ cxf,
-    const int* __restrict__ jcol_start, const int* __restrict__ jcol,
+    const int* __restrict__ jcol, const int* __restrict__ ztab,
     const unsigned long long* __restrict__ zext, int maxneighs, int ks, int cs, int* list,
     int* numneigh, int* nmasked)
 {
@@ -986,6 +1007,11 @@ __device__ __forceinline__ void build_list_blk(int bid, int half, int* cnt, Geom
     const float imnzf = (float)imnz, imxzf = (float)imxz;
     const double zx  = __longlong_as_double((long long)*zext);
     const double zlo = imnz - g.cutneigh - zx - 1.0e-6;
+    // window of a column: the entries of buckets [qa, qb], a superset of those
+    // with zlo <= bbminz <= imxz + cutneigh (zbucket is monotone); all others
+    // fail the box test
+    const int zn = g.zq + 2;
+    const int qa = zbucket(g, zlo), qb1 = zbucket(g, imxz + g.cutneigh + 1.0e-6) + 1;
     const int ib     = cbin[ci];
     int* row         = list + (size_t)ci * cs;
     int total = 0, diag_pos = -1;
@@ -993,22 +1019,10 @@ __device__ __forceinline__ void build_list_blk(int bid, int half, int* cnt, Geom
         const int k = kb + lane;
         int lo = 0, wn = 0;
         if (k < g.nstencil) {
-            const int jb = ib + stencil[k];
-            const int s1 = jcol_start[jb + 1];
-            int L = jcol_start[jb], R = s1;
-            while (L < R) {
-                int mid = (L + R) >> 1;
-                if (jcbbmin[mid].z < zlo) L = mid + 1;
-                else R = mid;
-            }
-            lo = L;
-            R  = s1;
-            while (L < R) {
-                int mid = (L + R) >> 1;
-                if (jcbbmin[mid].z - imxz > g.cutneigh) R = mid;
-                else L = mid + 1;
-            }
-            wn = L - lo;
+            const int* zt = ztab + (size_t)(ib + stencil[k]) * zn;
+            lo            = __ldg(&zt[qa]);
+            const int hi  = __ldg(&zt[qb1]);
+            wn            = hi > lo ? hi - lo : 0;
         }
         int incl = wn;
         for (int o = 1; o < 32; o <<= 1) {
@@ -1084,19 +1098,19 @@ __global__ void __launch_bounds__(32 * CP_LIST_WARPS, CP_LIST_MINB) k_build_list
     const double4* __restrict__ ibbmax, const double4* __restrict__ jcbbmin,
     const double4* __restrict__ jcbbmax, const double4* __restrict__ cx,
     const float4* __restrict__ jcbbf, const float4* __restrict__ cxf,
-    const int* __restrict__ jcol_start, const int* __restrict__ jcol,
+    const int* __restrict__ jcol, const int* __restrict__ ztab,
     const unsigned long long* __restrict__ zext, int maxneighs, int ks, int cs, int* list,
     int* numneigh, int* nmasked)
 {
     build_list_blk<M, N>(blockIdx.x, half, cnt, g, stencil, cbin, ibbmin, ibbmax, jcbbmin,
-        jcbbmax, cx, jcbbf, cxf, jcol_start, jcol, zext, maxneighs, ks, cs, list, numneigh,
+        jcbbmax, cx, jcbbf, cxf, jcol, ztab, zext, maxneighs, ks, cs, list, numneigh,
         nmasked);
 }
 
 void launch_build_list(cudaStream_t s, int M, int N, int half, int ncl_cap, const int* cnt,
     const Geom& g, const int* stencil, const int* cbin, const double4* ibbmin,
     const double4* ibbmax, const double4* jcbbmin, const double4* jcbbmax, const double4* cx,
-    const float4* jcbbf, const float4* cxf, const int* jcol_start, const int* jcol,
+    const float4* jcbbf, const float4* cxf, const int* jcol, const int* ztab,
     const unsigned long long* zext, int maxneighs, int ks, int cs, int* list, int* numneigh,
     int* nmasked, int* cnt_out)
 {
@@ -1106,11 +1120,11 @@ void launch_build_list(cudaStream_t s, int M, int N, int half, int ncl_cap, cons
     (void)cnt;
     if (N == 4)
         k_build_list<4, 4><<<blocks, 32 * CP_LIST_WARPS, 0, s>>>(half, cnt_out, g, stencil, cbin,
-            ibbmin, ibbmax, jcbbmin, jcbbmax, cx, jcbbf, cxf, jcol_start, jcol, zext, maxneighs,
+            ibbmin, ibbmax, jcbbmin, jcbbmax, cx, jcbbf, cxf, jcol, ztab, zext, maxneighs,
             ks, cs, list, numneigh, nmasked);
     else
         k_build_list<4, 8><<<blocks, 32 * CP_LIST_WARPS, 0, s>>>(half, cnt_out, g, stencil, cbin,
-            ibbmin, ibbmax, jcbbmin, jcbbmax, cx, jcbbf, cxf, jcol_start, jcol, zext, maxneighs,
+            ibbmin, ibbmax, jcbbmin, jcbbmax, cx, jcbbf, cxf, jcol, ztab, zext, maxneighs,
             ks, cs, list, numneigh, nmasked);
     g_launches++;
 }
@@ -1198,7 +1212,7 @@ int cp_build_stage_blocks(int stage, const CpBuildMember& m, int* threads)
     case CB_GSCATTER: return mdb_blocks(m.ngc_cap, T);
     case CB_CSIZES: return mdb_blocks(mb1, T);
     case CB_MERGE: *threads = 128; return mdb_blocks((long long)mb1 * 32, 128);
-    case CB_PREP: return mdb_blocks(m.slot_cap, T);
+    case CB_PREP: return mdb_blocks(list_prep_threads(m.g, m.slot_cap), T);
     case CB_LIST:
         *threads = 32 * CP_LIST_WARPS;
         return mdb_blocks((long long)m.ncl_cap * 32, 32 * CP_LIST_WARPS);
@@ -1284,16 +1298,16 @@ __global__ void __launch_bounds__(256, STAGE == CB_LIST ? 3 : 1)
     case CB_LIST:
         if (m.N == 4)
             build_list_blk<4, 4>(b, m.half, m.cnt, m.g, m.stencil, m.cbin, m.ibbmin, m.ibbmax,
-                m.jcbbmin, m.jcbbmax, m.cx, m.jcbbf, m.cxf, m.jcol_start, m.jcol, m.zext,
+                m.jcbbmin, m.jcbbmax, m.cx, m.jcbbf, m.cxf, m.jcol, m.ztab, m.zext,
                 m.maxneighs, m.ks, m.cs, m.list, m.numneigh, m.nmasked);
         else
             build_list_blk<4, 8>(b, m.half, m.cnt, m.g, m.stencil, m.cbin, m.ibbmin, m.ibbmax,
-                m.jcbbmin, m.jcbbmax, m.cx, m.jcbbf, m.cxf, m.jcol_start, m.jcol, m.zext,
+                m.jcbbmin, m.jcbbmax, m.cx, m.jcbbf, m.cxf, m.jcol, m.ztab, m.zext,
                 m.maxneighs, m.ks, m.cs, m.list, m.numneigh, m.nmasked);
         break;
     case CB_PREP:
-        list_prep_blk(b, m.N, m.slot_cap, m.g.mbins + 1, m.cnt, m.jcol_start, m.jcbbmin,
-            m.jcbbmax, m.cx, m.jcbbf, m.cxf);
+        list_prep_blk(b, m.N, m.slot_cap, m.g, m.cnt, m.jcol_start, m.jcbbmin, m.jcbbmax, m.cx,
+            m.jcbbf, m.cxf, m.ztab);
         break;
     }
 }

@@ -65,7 +65,19 @@ struct Geom {
     // bound on |FP32 - FP64| of a squared distance or box distance computed
     // from coordinates rounded to FP32 (the list build's prefilter)
     float list_margin;
+    // z buckets of the list build's window table: bucket of z =
+    // clamp(floor((z - z0) * zinv), 0, zq); per column zq + 2 entries
+    int zq;
+    double z0, zinv;
 };
+
+// the window table's bucket of a z coordinate (monotone in z; NaN -> 0)
+__host__ __device__ __forceinline__ int zbucket(const Geom& g, double z)
+{
+    double q = floor((z - g.z0) * g.zinv);
+    q        = fmin(fmax(q, 0.0), (double)g.zq);
+    return (int)q;
+}
 
 struct Types {
     int ntypes, uniform;
@@ -149,13 +161,13 @@ void launch_merge_columns(cudaStream_t s, int mbins1, int jfac, const int* ncl_c
     const double4* jbbmin, const double4* jbbmax, int* jcol, double4* jcbbmin, double4* jcbbmax);
 // FP32 copies for the list build's prefilter: the column-ordered j boxes
 // (jcbbf[2m] min, [2m+1] max) and the slot positions (all j-clusters)
-void launch_list_prep(cudaStream_t s, int N, int slot_cap, int mbins1, const int* cnt,
+void launch_list_prep(cudaStream_t s, int N, int slot_cap, const Geom& g, const int* cnt,
     const int* jcol_start, const double4* jcbbmin, const double4* jcbbmax, const double4* cx,
-    float4* jcbbf, float4* cxf);
+    float4* jcbbf, float4* cxf, int* ztab);
 void launch_build_list(cudaStream_t s, int M, int N, int half, int ncl_cap, const int* cnt,
     const Geom& g, const int* stencil, const int* cbin, const double4* ibbmin,
     const double4* ibbmax, const double4* jcbbmin, const double4* jcbbmax, const double4* cx,
-    const float4* jcbbf, const float4* cxf, const int* jcol_start, const int* jcol,
+    const float4* jcbbf, const float4* cxf, const int* jcol, const int* ztab,
     const unsigned long long* zext, int maxneighs, int ks, int cs, int* list, int* numneigh,
     int* nmasked, int* cnt_out);
 void launch_prune(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt, const double4* cx,
@@ -237,6 +249,7 @@ struct CpBuildMember {
     int *gtmp, *jcol;
     double4 *jcbbmin, *jcbbmax;
     float4 *jcbbf, *cxf;
+    int* ztab;
     int slot_cap;
     const int* stencil;
     int *list, *numneigh, *nmasked;
@@ -257,7 +270,7 @@ enum CpBuildStage {
     CB_CSIZES,   // binJClusters: column sizes
     CB_GSCATTER, // binJClusters: ghosts into columns
     CB_MERGE,    // binJClusters: merge by bbminz
-    CB_PREP,     // buildNeighbor: FP32 copies of boxes and positions
+    CB_PREP,     // buildNeighbor: FP32 copies of boxes and positions, window table
     CB_LIST,     // buildNeighbor
     CB_COUNT
 };
