@@ -354,7 +354,7 @@ def c4_ensemble(torch, mdb, args, device, rank=0, world=1, dist=None):
         choice, trials = {}, []
     else:
         choice, trials = AT.tune_ensemble(specs, lambda sp, n, h: pool.build(sp, n, h),
-                                          rounds=1)
+                                          rounds=2)
     tune_secs = time.perf_counter() - t0
     pick = [choice.get(AT.size_class(sp["natoms"]), AT.DEFAULT) for sp in specs]
     every = 20

@@ -15,9 +15,11 @@ chosen shape. The tuner picks, per system size:
 
 by measurement on the device. A single large system is tuned on the force
 kernel's own time (``ClusterSystem.time_force``, CUDA events). Members of an
-ensemble run concurrently, so a size class is tuned on the throughput of an
-ensemble of its own members (atom-steps per second over whole rebuild periods),
-which includes the graph and rebuild costs a replica of that size pays.
+ensemble run concurrently and share the GPU, so an ensemble is tuned on the
+throughput of the whole ensemble (atom-steps per second over whole rebuild
+periods, graph and rebuild costs included), one size class and one setting at
+a time: a size class tuned alone does not fill the GPU and favours choices
+(full lists, small blocks) that lose once every replica shares it.
 """
 import math
 import time
@@ -81,43 +83,71 @@ def _ensemble_rate(members, steps, rounds):
     return nat * steps * rounds / secs
 
 
-def tune_ensemble(specs, build, steps=20, rounds=2, shapes=SHAPES, forms=FORMS):
-    """Choice per size class for an ensemble. ``specs`` is a list of replica
-    descriptions with an ``natoms`` entry; ``build(spec, cluster_n, half)``
-    returns a set-up mixed-precision ClusterSystem. Shape and list form are
-    picked first (default launch), then threads per block and the force kernel
-    variant, each on the throughput of an ensemble of the class's own members.
-    Returns ({size_class: choice}, trials)."""
+def tune_ensemble(specs, build, steps=20, rounds=2, shapes=SHAPES, forms=FORMS, margin=0.02,
+                  rate=None):
+    """Choice per size class for an ensemble, by coordinate descent on the whole
+    ensemble's throughput. ``specs`` is a list of replica descriptions with an
+    ``natoms`` entry; ``build(spec, cluster_n, half)`` returns a set-up
+    mixed-precision ClusterSystem (with ``close()``). Every class starts at
+    DEFAULT; classes are visited largest (total atoms) first, each trying the
+    other shapes and list forms, then the other threads per block and kernel
+    variants, with every other class at its current choice. A change is kept
+    only if the ensemble gets faster by more than ``margin`` (timing noise).
+    ``rate(members)`` measures the throughput (default: an mdb.Ensemble run of
+    ``rounds`` rebuild periods of ``steps`` steps after one untimed period).
+    Returns ({size_class: choice}, trials), trials = (class, choice, rate)."""
+    if rate is None:
+        def rate(members):
+            return _ensemble_rate(members, steps, rounds)
     classes = {}
     for sp in specs:
         classes.setdefault(size_class(sp["natoms"]), []).append(sp)
-    out, trials = {}, []
-    for cls, group in sorted(classes.items()):
-        best = None
+    order = sorted(classes, key=lambda c: (-sum(sp["natoms"] for sp in classes[c]), c))
+    choice = {c: dict(DEFAULT) for c in classes}
+    members = {c: [build(sp, DEFAULT["cluster_n"], DEFAULT["half"]) for sp in classes[c]]
+               for c in classes}
+
+    def everyone():
+        return [m for c in sorted(members) for m in members[c]]
+
+    best = rate(everyone())
+    trials = [(None, dict(DEFAULT), best)]
+
+    def close(ms):
+        for m in ms:
+            m.close()
+
+    for c in order:
         for n in shapes:
             for half in forms:
-                members = [build(sp, n, half) for sp in group]
-                c = dict(DEFAULT, cluster_n=n, half=half)
-                rate = _ensemble_rate(members, steps, rounds)
-                trials.append((cls, dict(c), rate))
-                if best is None or rate > best[1]:
-                    best = (c, rate)
-                for m in members:
-                    m.close()
-        c0 = best[0]
-        members = [build(sp, c0["cluster_n"], c0["half"]) for sp in group]
+                if (n, half) == (choice[c]["cluster_n"], choice[c]["half"]):
+                    continue
+                trial = dict(choice[c], cluster_n=n, half=half)
+                old, members[c] = members[c], [build(sp, n, half) for sp in classes[c]]
+                for m in members[c]:
+                    apply_launch(m, trial)
+                r = rate(everyone())
+                trials.append((c, dict(trial), r))
+                if r > best * (1.0 + margin):
+                    best, choice[c] = r, trial
+                    close(old)
+                else:
+                    close(members[c])
+                    members[c] = old
+    for c in order:
         for key, values in (("force_block", BLOCKS), ("force_variant", VARIANTS)):
             for val in values:
-                if val == best[0][key]:
+                if val == choice[c][key]:
                     continue
-                c = dict(best[0], **{key: val})
-                for m in members:
-                    apply_launch(m, c)
-                rate = _ensemble_rate(members, steps, rounds)
-                trials.append((cls, dict(c), rate))
-                if rate > best[1]:
-                    best = (c, rate)
-        for m in members:
-            m.close()
-        out[cls] = best[0]
-    return out, trials
+                trial = dict(choice[c], **{key: val})
+                for m in members[c]:
+                    apply_launch(m, trial)
+                r = rate(everyone())
+                trials.append((c, dict(trial), r))
+                if r > best * (1.0 + margin):
+                    best, choice[c] = r, trial
+                else:
+                    for m in members[c]:
+                        apply_launch(m, choice[c])
+    close(everyone())
+    return choice, trials
