@@ -1793,6 +1793,7 @@ static void ens_integ(MdbCpEnsemble* e, bool final_, bool initial)
 
 static void ens_forces(MdbCpEnsemble* e, bool energy)
 {
+    launch_zero_forces_batch(e->s, e->nb_integ, e->d_step, e->d_bmap + e->off_integ_dyn);
     for (const auto& gr : e->groups)
         launch_force_mixed_batch(e->s, gr.N, gr.half, energy, gr.ty, gr.cutsq, gr.nblocks,
             e->d_force, e->d_bmap + (energy ? gr.off : gr.off_dyn));

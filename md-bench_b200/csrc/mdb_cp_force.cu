@@ -744,8 +744,30 @@ __global__ void k_cp_integrate_batch(const CpStepMember* __restrict__ tab,
     if (bm.x < 0) return;
     const CpStepMember& m = tab[bm.x];
     cp_integrate_slot<FINAL, INITIAL>(bm.y * blockDim.x + threadIdx.x, m.M, m.N, m.cnt, m.dtf,
-        m.dt, m.cx, m.cv, m.cf, m.cf32, m.anchor, m.xr, m.zero_f != 0, m.mixed, m.xb, m.lim2,
-        m.flag);
+        m.dt, m.cx, m.cv, m.cf, m.cf32, m.anchor, m.xr, false, m.mixed, m.xb, m.lim2, m.flag);
+}
+
+// Clearing the half-list force slots right before the force kernel (rather
+// than in the integrator, which streams positions and velocities through L2
+// after it) leaves the slots in L2 when the kernel's reduction atomics arrive.
+__global__ void k_zero_forces_batch(const CpStepMember* __restrict__ tab,
+    const int2* __restrict__ bmap)
+{
+    const int2 bm = __ldg(&bmap[blockIdx.x]);
+    if (bm.x < 0) return;
+    const CpStepMember& m = tab[bm.x];
+    const int s           = bm.y * blockDim.x + threadIdx.x;
+    if (!m.zero_f || s >= m.cnt[CP_NCL] * m.M) return;
+    if (m.cf32) m.cf32[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+    else const_cast<double4*>(m.cf)[s] = make_double4(0.0, 0.0, 0.0, 0.0);
+}
+
+void launch_zero_forces_batch(cudaStream_t s, int nblocks, const CpStepMember* tab,
+    const int2* bmap)
+{
+    if (nblocks <= 0) return;
+    k_zero_forces_batch<<<nblocks, MDB_NTHREADS, 0, s>>>(tab, bmap);
+    g_launches++;
 }
 
 void launch_cp_integrate_batch(cudaStream_t s, bool final_, bool initial, int nblocks,

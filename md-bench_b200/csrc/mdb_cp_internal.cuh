@@ -216,7 +216,7 @@ struct CpStepMember { // integrator and ghost update
     const int* jnat;
     double dtf, dt, xprd, yprd, zprd;
     int M, N, mixed; // mixed: 0 FP64, else the xr mode of put_rel
-    int zero_f; // half lists: the initial integration clears the forces it used
+    int zero_f; // half lists: the force slots are cleared before each force evaluation
     const double4* xb; // displacement check (null: off), see launch_cp_initial
     double lim2;
     int* flag;
@@ -287,6 +287,10 @@ void launch_counters_batch(cudaStream_t s, int nmem, const CpBuildMember* tab, i
 
 void launch_cp_integrate_batch(cudaStream_t s, bool final_, bool initial, int nblocks,
     const CpStepMember* tab, const int2* bmap);
+// half-list members (zero_f): force slots [0, ncl * M) to zero, over the
+// integrator's block map; launched right before the force evaluation
+void launch_zero_forces_batch(cudaStream_t s, int nblocks, const CpStepMember* tab,
+    const int2* bmap);
 void launch_ghost_update_batch(cudaStream_t s, int nblocks, const CpStepMember* tab,
     const int2* bmap);
 void launch_force_mixed_batch(cudaStream_t s, int N, int half, int energy, const Types& ty,
