@@ -87,7 +87,8 @@ class Clocks:
         if shutil.which("nvidia-smi"):
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "-i", str(device),
                                        "--format=csv,noheader,nounits", "-lms", "200"],
-                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True,
+                                      errors="replace")
 
     def stop(self):
         if self.p is None:
@@ -490,7 +491,8 @@ def cpu_baseline(md_steps=20, half=1):
                    OMP_PROC_BIND="close")
         out = subprocess.run([binary, "-nx", str(LJ_CELLS), "-ny", str(LJ_CELLS), "-nz",
                               str(LJ_CELLS), "-n", str(md_steps), "-half", str(half)], env=env,
-                             capture_output=True, text=True, timeout=1200).stdout
+                             capture_output=True, text=True, errors="replace",
+                             timeout=1200).stdout  # it may print stray bytes
         for line in out.splitlines():
             if "atom updates/us" in line:
                 val = float(line.split("|")[1].split()[0]) * 1e6
