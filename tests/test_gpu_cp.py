@@ -570,3 +570,32 @@ def test_ensemble_rebuild_check():
         assert np.sqrt(np.mean(np.sum(d * d, axis=1))) <= 1e-5 * rms
         ref.close()
     ens.close()
+
+
+def thermalised_box(nx, ny, nz, steps=150):
+    """A disordered state of an nx x ny x nz fcc box (Verlet-list oracle)."""
+    o = O.Oracle(nx=nx, ny=ny, nz=nz)
+    o.lattice()
+    o.setup()
+    o.run(steps)
+    x, v, _, t = o.atoms()
+    hp = mdb.host_params(nx=nx, ny=ny, nz=nz)
+    mdb.create_fcc(hp)
+    return hp, x, v, t
+
+
+@pytest.mark.parametrize("N", SHAPES)
+@pytest.mark.parametrize("half", [0, 1])
+def test_setup_elongated_box_bit_exact(N, half):
+    """A box 12 times taller than wide (4 x 4 x 48 cells, 3,072 atoms): few long
+    columns and some two hundred z buckets in the list build's window table;
+    clusters, columns and lists (in order) bit-identical, FP64 forces too."""
+    hp, x, v, t = thermalised_box(4, 4, 48)
+    s, o = pair(hp, x, v, t, N, half=half)
+    assert_same_build(s, o)
+    valid = valid_slots(o)
+    fs, fo = local_forces(s, valid), local_forces(o, valid)
+    if half:
+        assert_forces_close(fs, fo)
+    else:
+        assert np.array_equal(fs, fo)
