@@ -664,6 +664,12 @@ def main():
             "kernel_ms": round(kt * 1e3, 4), "pairs_in_cutoff_per_atom": round(pc, 2),
             "flops_per_atom": round(fpa, 1),
             "computed_pairs_per_atom": round(entries * 4, 1),
+            # pairs credited above over the pair slots the list makes the kernel
+            # evaluate, and the rate with every such slot credited (the FP32
+            # pipe's view; the roofline fraction counts only in-cutoff pairs)
+            "cluster_efficiency": round((pc / 2 if HEAD["half"] else pc) / (entries * 4), 3),
+            "achieved_all_listed_pairs": round(
+                achieved * (entries * 4) / (pc / 2 if HEAD["half"] else pc), 3),
             "peak_source": src}
 
     extra = {}
