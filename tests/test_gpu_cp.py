@@ -599,3 +599,42 @@ def test_setup_elongated_box_bit_exact(N, half):
         assert_forces_close(fs, fo)
     else:
         assert np.array_equal(fs, fo)
+
+
+def test_contexts_on_two_host_threads_match_serial_runs():
+    """Two contexts driven at the same time from two host threads (as the
+    end-to-end benchmark runs them) end bit-identical to the same runs made one
+    after another, and each counts only its own kernel launches: contexts share
+    no state, and the launch bookkeeping is per host thread."""
+    import threading
+    hp, x, v, t = thermalised(6)
+    runs = []
+    for k in range(2):
+        s, _ = pair(hp, x, v, t, 4)
+        n0 = s.launches
+        s.run(40 + 20 * k, max_samples=0)
+        runs.append((s.atoms(), s.launches - n0))
+        s.close()
+    systems = [pair(hp, x, v, t, 4)[0] for _ in range(2)]
+    base = [s.launches for s in systems]
+    errors = []
+
+    def work(k):
+        try:
+            systems[k].run(40 + 20 * k, max_samples=0)
+            systems[k].synchronize()
+        except Exception as e:
+            errors.append(e)
+
+    workers = [threading.Thread(target=work, args=(k,)) for k in range(2)]
+    for w in workers:
+        w.start()
+    for w in workers:
+        w.join()
+    assert not errors, errors
+    for k, s in enumerate(systems):
+        (xs, vs, ts), launches = runs[k]
+        xa, va, ta = s.atoms()
+        assert np.array_equal(xa, xs) and np.array_equal(va, vs) and np.array_equal(ta, ts)
+        assert s.launches - base[k] == launches
+        s.close()
