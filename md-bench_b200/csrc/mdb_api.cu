@@ -58,7 +58,7 @@ struct MdbCtx {
     double4* bin_x = nullptr; // positions in bin order, atom index bits in .w
     float4* bin_xf = nullptr; // the same rounded to FP32 (list build prefilter)
     int *bin_lcount = nullptr, *loc_start = nullptr; // locals per bin, their offsets
-    int* local_order = nullptr;                      // row t of the list -> atom
+    int* local_order = nullptr; // local atoms bin by bin (the order sortAtom gives)
     int4* stencil_d  = nullptr;                      // {flat offset, dx, dy, dz}
     int *numneigh = nullptr, *neighbors = nullptr;
     int* counters = nullptr;
@@ -722,10 +722,10 @@ static void enq_list(MdbCtx* ctx)
         ctx->local_order);
     launch_bin_positions(s, ctx->nall_cap, ctx->g.mbins, ctx->x, ctx->bin_start, ctx->bin_atoms,
         ctx->bin_x, ctx->bin_xf);
-    launch_build_list(s, ctx->nlocal, ctx->x, ctx->g, ctx->stencil_d, ctx->local_order,
-        ctx->atom_bin, ctx->bin_start, ctx->bin_x, ctx->bin_xf, ctx->cutneighsq,
-        ctx->list_margin, ctx->p.half_neigh, ctx->maxneighs, ctx->ld, ctx->neighbors,
-        ctx->numneigh, ctx->counters, ctx->mixed ? ctx->qcell : nullptr);
+    launch_build_list(s, ctx->nlocal, ctx->x, ctx->g, ctx->stencil_d, ctx->atom_bin,
+        ctx->bin_start, ctx->bin_x, ctx->bin_xf, ctx->cutneighsq, ctx->list_margin,
+        ctx->p.half_neigh, ctx->maxneighs, ctx->ld, ctx->neighbors, ctx->numneigh,
+        ctx->counters, ctx->mixed ? ctx->qcell : nullptr);
 }
 
 static void clear_rebuild_counters(MdbCtx* ctx)

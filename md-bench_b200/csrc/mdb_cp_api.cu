@@ -673,8 +673,8 @@ static void enq_list(MdbCp* ctx)
 
 static void clear_build_counters(MdbCp* ctx)
 {
-    // CP_MAXNEED, CP_BADBIN, CP_WINDOW
-    cudaMemsetAsync(ctx->cnt + CP_MAXNEED, 0, 3 * sizeof(int), ctx->s);
+    // CP_MAXNEED, CP_BADBIN
+    cudaMemsetAsync(ctx->cnt + CP_MAXNEED, 0, 2 * sizeof(int), ctx->s);
 }
 
 // buildClusters .. buildNeighbor from the atom arrays (idempotent)
@@ -702,8 +702,6 @@ static int eval_build(MdbCp* ctx, int what)
 {
     const int* h = ctx->h_cnt;
     if (h[CP_BADBIN] > 0) return -fail(ctx, MDB_ERR_OVERFLOW, "atom outside the column grid");
-    if ((what & CHK_LIST) && h[CP_WINDOW] > 0)
-        return -fail(ctx, MDB_ERR_OVERFLOW, "more than 128 j-cluster candidates in one column");
     if ((what & CHK_GHOSTS) && h[CP_NGC_TOTAL] > ctx->ngc_cap) {
         int rc = alloc_ghosts(ctx, (int)(h[CP_NGC_TOTAL] * 1.2) + 1024);
         if (rc) return -rc;

@@ -1234,7 +1234,6 @@ __device__ __forceinline__ void reset_blk(int bid, const CpBuildMember& m)
         *m.zext                  = 0ull;
         m.cnt[CP_MAXNEED]        = 0;
         m.cnt[CP_BADBIN]         = 0;
-        m.cnt[CP_WINDOW]         = 0;
         m.cnt[CP_NGHOST_ATOMS]   = 0;
     }
 }

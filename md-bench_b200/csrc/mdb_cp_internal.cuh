@@ -37,7 +37,6 @@
 
 #define CP_M            4    /* i-cluster size of the GPU shapes */
 #define CP_COL_SMEM     1024 /* column sort in shared memory up to this many atoms */
-#define CP_WINDOW_BITS  128  /* candidates per stencil column and i-cluster */
 #define CP_PAD_F        1.0e18f
 #define CP_ANCHOR_STEP  0.125
 
@@ -50,8 +49,7 @@ enum {
     CP_NGHOST_ATOMS = 4,
     CP_MAXNEED      = 5,  // largest list length seen (>= maxneighs means regrow)
     CP_BADBIN       = 6,  // atoms outside the column grid
-    CP_WINDOW       = 7,  // a column window wider than CP_WINDOW_BITS
-    CP_SLOTS        = 8
+    CP_SLOTS        = 7
 };
 
 namespace mdb {

@@ -433,8 +433,8 @@ __global__ void k_bin_scatter(int nlocal, const int* __restrict__ atom_bin,
 // Atoms of a bin in ascending index order: the order binatoms produces when it
 // fills bins in one serial pass (verletlist/neighbor.c:443-454). Locals have
 // the smaller indices, so they form the head of each sorted bin; the heads of
-// all bins, concatenated in bin order, give local_order (the row order of the
-// neighbour list: atoms of one bin are adjacent rows).
+// all bins, concatenated in bin order, give local_order (the order in which
+// sortAtom places the local atoms).
 __global__ void k_bin_sort(int mbins, const int* __restrict__ bin_start,
     int* __restrict__ bin_atoms, const int* __restrict__ loc_start,
     int* __restrict__ local_order)
@@ -605,11 +605,10 @@ __global__ void __launch_bounds__(128) k_build_list(int nlocal, const double4* _
 }
 
 void launch_build_list(cudaStream_t s, int nlocal, const double4* x, BinGeom g,
-    const int4* stencil, const int* local_order, const int* atom_bin, const int* bin_start,
+    const int4* stencil, const int* atom_bin, const int* bin_start,
     const double4* bin_x, const float4* bin_xf, double cutneighsq, float margin, int half,
     int maxneighs, int ld, int* neighbors, int* numneigh, int* counters, const int* qcell)
 {
-    (void)local_order;
     if (nlocal <= 0) return;
     size_t smem = sizeof(int4) * g.nstencil;
     k_build_list<<<mdb_blocks(nlocal, 128), 128, smem, s>>>(nlocal, x, g, stencil, atom_bin,
