@@ -38,7 +38,7 @@ STUB_ATOMS = 1 << 20
 EAM_CELLS = 32
 EAM_A = 3.615
 EAM_T = 1600.0
-EAM_FILE = os.path.join(ROOT, "tests", "golden", "data", "Cu_u3.eam")
+EAM_FILE = os.path.join(ROOT, "md-bench_b200", "data", "Cu_u3.eam")
 REF_CP = {shape: os.path.join(ROOT, "oracle", "_ref", f"MDBench-CP-{shape}")
           for shape in ("4x4", "4x8")}
 METRIC = "atom-steps/s, LJ+EAM mixed-FP32 vs FP64 on 1 B200 at stated force error"

@@ -187,7 +187,11 @@ int mdb_run(MdbCtx* ctx, int first_step, int nsteps, MdbThermo* samples, int max
  * every call on a device shares (overlapping calls on the GPU race; each call
  * rewrites every slot it reads, so no clearing is needed). At most 8,388,608
  * atoms per call (MDB_ERR_ARG beyond). The first call on a device looks up the
- * array's device address; make that first call before any stream capture. */
+ * array's device address; make that first call before any stream capture. The
+ * address is cached per device and CUDA context: the first call under another
+ * context of the device (a non-primary driver-API context, or the new primary
+ * context after cudaDeviceReset) looks it up again, so make that call before
+ * any capture too. */
 int mdb_kinetic_sum_noalloc(const double* d_v, int n, double mass, double* d_out, void* stream);
 
 /* ---- introspection (tests, tools) ----------------------------------------- */

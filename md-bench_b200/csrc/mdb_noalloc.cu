@@ -17,7 +17,14 @@
 // NOALLOC_MAX_PARTIALS * NOALLOC_CHUNK = 8,388,608 atoms and rejects more.
 // Host code must not pass the array's name to a kernel (in host code it is a
 // host-side shadow, not a device address): the device address is looked up
-// once per device with cudaGetSymbolAddress and cached.
+// with cudaGetSymbolAddress, with the device current, once per device and
+// CUDA context, and cached. The cache is keyed on the current context as well
+// as the device number, so a call made under another context of the same
+// device (a driver-API context that is not the primary one, or the new
+// primary context after cudaDeviceReset) looks the address up again instead
+// of using one that belongs to a module of a context that is gone. Such a
+// look-up is part of that call: make the first call under each context before
+// any stream capture.
 #include <stdio.h>
 
 #include <mutex>
@@ -34,7 +41,30 @@ constexpr int NOALLOC_MAX_DEVICES  = 64;
 static __device__ __align__(256) double g_noalloc_partials[NOALLOC_MAX_PARTIALS];
 
 std::mutex g_noalloc_lock;
-double* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+struct ScratchAddr {
+    void* ctx    = nullptr; // the CUDA context the address belongs to
+    double* addr = nullptr;
+};
+ScratchAddr g_noalloc_addr[NOALLOC_MAX_DEVICES];
+
+// cuCtxGetCurrent through the runtime's driver entry point (no link-time
+// dependency on the driver library)
+typedef int (*CtxGetCurrentFn)(void** pctx);
+
+static int current_context(void** ctx)
+{
+    static CtxGetCurrentFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !p)
+            return -1;
+        fn = reinterpret_cast<CtxGetCurrentFn>(p);
+    }
+    return fn(ctx) == 0 && *ctx ? 0 : -1;
+}
 
 // Each block sums (vx^2 + vy^2 + vz^2) * mass over its chunk of AoS velocities
 // (verletlist/atom.h:78-88 layout) and writes one partial; every partial slot
@@ -80,19 +110,26 @@ extern "C" int mdb_kinetic_sum_noalloc(const double* d_v, int n, double mass, do
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES)
         return MDB_ERR_CUDA;
+    // no current context yet (a caller whose first runtime call this is): the
+    // symbol look-up below makes the device's primary context current
+    void* ctx = nullptr;
+    if (current_context(&ctx) != 0) ctx = nullptr;
     double* scratch = nullptr;
     {
-        // once per device, with that device current: the device address of
-        // the static array (the first call on a device does this look-up, so
-        // make that call before any stream capture)
+        // once per device and context, with that device current: the device
+        // address of the static array (the first call under a context does
+        // this look-up, so make that call before any stream capture)
         std::lock_guard<std::mutex> lock(g_noalloc_lock);
-        if (!g_noalloc_addr[dev]) {
+        ScratchAddr& c = g_noalloc_addr[dev];
+        if (!ctx || !c.addr || c.ctx != ctx) {
             void* p = nullptr;
             if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p)
                 return MDB_ERR_CUDA;
-            g_noalloc_addr[dev] = static_cast<double*>(p);
+            if (!ctx && current_context(&ctx) != 0) return MDB_ERR_CUDA;
+            c.addr = static_cast<double*>(p);
+            c.ctx  = ctx;
         }
-        scratch = g_noalloc_addr[dev];
+        scratch = c.addr;
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     int nparts     = n > 0 ? (n + NOALLOC_CHUNK - 1) / NOALLOC_CHUNK : 1;

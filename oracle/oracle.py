@@ -18,6 +18,18 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmdbref_vl.so")
 REF_BIN = os.path.join(HERE, "_ref", "MDBench-VL")
+REF_TREE_FILE = os.path.join(HERE, "_ref", "reference_tree.txt")
+
+
+def reference_tree():
+    """The MD-Bench source tree the checkers were built from (recorded by
+    oracle/Makefile), or None where it is absent (e.g. on a GPU host)."""
+    try:
+        with open(REF_TREE_FILE) as f:
+            path = f.read().strip()
+    except OSError:
+        return None
+    return path if path and os.path.isdir(path) else None
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")

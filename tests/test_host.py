@@ -97,9 +97,11 @@ def test_dump_reader_rejects_truncated_file(tmp_path):
 
 def test_reference_dump_files_parse():
     """The reference's copper inputs use the same dump layout (1-based types)."""
-    ref = "/root/reference/data/copper_melting/input_eam_cu_one_atomtype_20x20x20.dmp"
-    if not os.path.exists(ref):
+    import oracle as O
+    tree = O.reference_tree()
+    if tree is None:
         pytest.skip("reference tree not present")
+    ref = os.path.join(tree, "data", "copper_melting", "input_eam_cu_one_atomtype_20x20x20.dmp")
     hp = mdb.host_params()
     x, v, t = mdb.read_dmp(hp, ref)
     assert len(t) == 32000 and hp.xprd == pytest.approx(72.3) and set(t.tolist()) == {1}

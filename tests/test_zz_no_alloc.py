@@ -65,3 +65,30 @@ def test_noalloc_rejects_more_atoms_than_its_scratch():
     rc = lib.mdb_kinetic_sum_noalloc(C.c_void_p(d_v.data_ptr()), 8388609, 1.0,
                                      C.c_void_p(d_out.data_ptr()), None)
     assert rc == 1  # MDB_ERR_ARG
+
+
+def test_noalloc_many_partials_and_empty():
+    """More than 1024 block partials (2.2M atoms: the final kernel's strided
+    loop runs) against a float64 numpy sum, then n = 0, which must give 0 even
+    though the shared scratch still holds the previous call's partials."""
+    torch = pytest.importorskip("torch")
+    lib = mdb.load()
+    n = 2_200_000                      # 1,075 partials of 2,048 atoms
+    rng = np.random.default_rng(7)
+    v = rng.standard_normal((n, 3))
+    mass = 1.5
+    d_v = torch.from_numpy(v.reshape(-1)).cuda()
+    d_out = torch.full((1,), -1.0, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):
+        rc = lib.mdb_kinetic_sum_noalloc(C.c_void_p(d_v.data_ptr()), n, mass,
+                                         C.c_void_p(d_out.data_ptr()), C.c_void_p(stream))
+        assert rc == 0, lib.mdb_status_string(rc)
+        torch.cuda.synchronize()
+        want = float(np.sum(v * v) * mass)
+        assert float(d_out.item()) == pytest.approx(want, rel=REL)
+    rc = lib.mdb_kinetic_sum_noalloc(None, 0, mass, C.c_void_p(d_out.data_ptr()),
+                                     C.c_void_p(stream))
+    assert rc == 0, lib.mdb_status_string(rc)
+    torch.cuda.synchronize()
+    assert float(d_out.item()) == 0.0
