@@ -269,6 +269,7 @@ def test_c3_eam_copper_against_oracle():
     xo, vo, fo, _ = o.atoms()
     assert np.array_equal(xs, xo) and np.array_equal(vs, vo) and np.array_equal(fs, fo)
     assert np.array_equal(s.eam_fp()[:n], o.eam_fp()[:n])
+    s.compute_force(energy=True)  # PE is reported after an energy evaluation
     ts, to = s.thermo(), o.thermo()
     for key in ("T", "P", "PE"):
         assert ts[key] == pytest.approx(to[key], rel=THERMO_REL), key
