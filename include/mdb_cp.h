@@ -50,8 +50,24 @@ int mdb_cp_synchronize(MdbCp* ctx);
  * with a budget for 8 resident blocks of 128 threads per SM (these run blocks
  * of 128 threads; default 2); "force_swizzle" = 1: the blocks one resident
  * slot runs in turn take neighbouring i-clusters (L1 reuse of j data; default
- * 0, measured within 2 % either way). */
+ * 0, measured within 2 % either way); "force_path" (mixed contexts) = 0: the
+ * cluster-pair kernel evaluates every pair slot of the listed cluster pairs,
+ * as the reference's computeForceLJ kernels do (clusterpair/force_lj.c);
+ * 1: the pair-list kernel evaluates only the listed cluster pairs' pairs
+ * within r_c + buffer of each other when last derived (see
+ * mdb_cp_set_pair_buffer), re-derived inside the timestep whenever an atom
+ * has moved more than buffer / 2 since: the same pairs inside r_c, so the
+ * same forces up to FP32 summation order. */
 int mdb_cp_tune(MdbCp* ctx, const char* key, int value);
+/* Buffer of the pair-list path (force_path 1; no counterpart in the
+ * reference): pairs are kept within r_c + buffer, and any atom moving more
+ * than buffer / 2 since the last derivation triggers a new one in the next
+ * force evaluation. Negative (the default): the list skin, cutneigh -
+ * cutforce. */
+int mdb_cp_set_pair_buffer(MdbCp* ctx, double buffer);
+/* Pair-list path statistics: derivations run so far, and the j atoms listed
+ * by the last derivation over all i pairs (each stands for two pair slots). */
+int mdb_cp_get_pair_stats(MdbCp* ctx, long long* derivations, long long* codes);
 /* Device time of one force evaluation (no energy) on the context's stream:
  * the mean over reps back-to-back launches after two untimed ones, from CUDA
  * events. For launch tuning; the force array is overwritten with the same
@@ -130,7 +146,9 @@ int mdb_cp_get_rebuilds(MdbCp* ctx, long long* scheduled, long long* checked);
  * concurrently and fill the GPU. Rebuild steps synchronise once for all
  * members. Thermo samples after every step n with (n+1) % nstat == 0, up to
  * max_samples per member: samples[member * max_samples + k]. The members stay
- * usable on their own between runs; do not use them while a run is active. */
+ * usable on their own between runs; do not use them while a run is active.
+ * Members must run the cluster-pair force kernel (force_path 0): MDB_ERR_ARG
+ * otherwise. */
 typedef struct MdbCpEnsemble MdbCpEnsemble;
 int mdb_cp_ensemble_create(MdbCp* const* members, int n, MdbCpEnsemble** out);
 int mdb_cp_ensemble_destroy(MdbCpEnsemble* ens);

@@ -90,6 +90,17 @@ struct MdbCp {
     int* h_dflag       = nullptr;
     bool snap_valid    = false;
     long long rebuilds_sched = 0, rebuilds_check = 0;
+    // pair-list force path of the mixed scheme (force_path 1, mdb_cp_pairs.cu):
+    // codes per (i pair, chunk), their counts, the positions they were
+    // derived from, and {derive flag, derivations run}
+    int force_path        = 0;
+    double pair_buffer    = -1.0; // r_in - r_c; < 0: the list's skin
+    PairTypes pt;
+    unsigned char* pcode  = nullptr;
+    unsigned short* pcnt  = nullptr;
+    float4* xq            = nullptr;
+    int* qflag            = nullptr;
+    int pair_ncl = 0, pair_chmax = 0;
 };
 
 #define RED_SLOTS 64
@@ -131,6 +142,9 @@ static void drop_graph(MdbCp* ctx)
     ctx->g_plain.exec    = nullptr;
     ctx->g_plain.kernels = 0;
 }
+
+static int ensure_pairs(MdbCp* ctx);
+static int mark_derive(MdbCp* ctx);
 
 static long long mark() { return mdb::g_launches; }
 static void account(MdbCp* ctx, long long m) { ctx->launches += mdb::g_launches - m; }
@@ -249,6 +263,21 @@ static int setup_types(MdbCp* ctx)
     t.force_swizzle = 0;
     t.eps0        = t.sqrt_eps[0] * t.sqrt_eps[0];
     t.sigma6_0 = t.sigma3[0] * t.sigma3[0];
+    // the pair-list path's constants (geometric mixing, in FP64 then rounded)
+    PairTypes& pt = ctx->pt;
+    memset(&pt, 0, sizeof pt);
+    for (int a = 0; a < MDB_MAX_TYPES; a++)
+        for (int b = 0; b < MDB_MAX_TYPES; b++) {
+            const int ta = a < nt ? a : 0, tb = b < nt ? b : 0;
+            const double e  = t.sqrt_eps[ta] * t.sqrt_eps[tb];
+            const double s6 = t.sigma3[ta] * t.sigma3[tb];
+            pt.tab[a * MDB_MAX_TYPES + b] =
+                make_float4((float)(48.0 * e * s6 * s6), (float)(24.0 * e * s6), (float)s6, (float)e);
+        }
+    pt.a0     = (float)(48.0 * t.eps0 * t.sigma6_0 * t.sigma6_0);
+    pt.b0     = (float)(24.0 * t.eps0 * t.sigma6_0);
+    pt.sig6_0 = (float)t.sigma6_0;
+    pt.eps0   = t.eps0;
     return MDB_OK;
 }
 
@@ -277,7 +306,49 @@ extern "C" int mdb_cp_tune(MdbCp* ctx, const char* key, int value)
         ctx->ty.force_variant = value;
         return MDB_OK;
     }
+    if (!strcmp(key, "force_path")) {
+        if (value < 0 || value > 1 || (value == 1 && !ctx->mixed)) return MDB_ERR_ARG;
+        drop_graph(ctx);
+        ctx->force_path = value;
+        return ensure_pairs(ctx);
+    }
     return fail(ctx, MDB_ERR_ARG, "unknown tuning key");
+}
+
+extern "C" int mdb_cp_set_pair_buffer(MdbCp* ctx, double buffer)
+{
+    if (!ctx || !(buffer == buffer)) return MDB_ERR_ARG;
+    drop_graph(ctx);
+    ctx->pair_buffer = buffer;
+    return mark_derive(ctx);
+}
+
+extern "C" int mdb_cp_get_pair_stats(MdbCp* ctx, long long* derivations, long long* codes)
+{
+    if (!ctx) return MDB_ERR_ARG;
+    if (derivations) *derivations = 0;
+    if (codes) *codes = 0;
+    if (!ctx->qflag) return MDB_OK;
+    CK(cudaSetDevice(ctx->dev));
+    int q[2] = {0, 0};
+    CK(cudaMemcpyAsync(q, ctx->qflag, sizeof q, cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    if (derivations) *derivations = q[1];
+    if (codes && ctx->pcnt) {
+        // codes of the current clusters (two i pairs per i-cluster)
+        CK(cudaMemcpyAsync(ctx->h_cnt, ctx->cnt, CP_SLOTS * sizeof(int), cudaMemcpyDeviceToHost,
+            ctx->s));
+        CK(cudaStreamSynchronize(ctx->s));
+        const size_t n = (size_t)ctx->h_cnt[CP_NCL] * 2 * ctx->pair_chmax;
+        std::vector<unsigned short> h(n);
+        if (n) {
+            CK(cudaMemcpy(h.data(), ctx->pcnt, n * sizeof(unsigned short), cudaMemcpyDeviceToHost));
+        }
+        long long t = 0;
+        for (unsigned short v : h) t += v;
+        *codes = t;
+    }
+    return MDB_OK;
 }
 
 extern "C" int mdb_cp_synchronize(MdbCp* ctx)
@@ -302,6 +373,8 @@ static void free_all(MdbCp* ctx)
     dfree(ctx->jcbbmin), dfree(ctx->jcbbmax), dfree(ctx->jcbbf), dfree(ctx->cxf);
     dfree(ctx->stencil_d), dfree(ctx->list), dfree(ctx->numneigh), dfree(ctx->nmasked);
     dfree(ctx->xbuild), dfree(ctx->dflag);
+    dfree(ctx->pcode), dfree(ctx->pcnt), dfree(ctx->xq), dfree(ctx->qflag);
+    ctx->pair_ncl = ctx->pair_chmax = 0;
     if (ctx->h_dflag) cudaFreeHost(ctx->h_dflag);
     ctx->h_dflag  = nullptr;
     ctx->xbuild_n = 0;
@@ -504,6 +577,45 @@ static int alloc_list(MdbCp* ctx, int maxneighs)
     ctx->maxneighs = maxneighs;
     CK(dalloc(&ctx->list, (size_t)maxneighs * ctx->ld));
     return MDB_OK;
+}
+
+// r_in - r_c of the pair-list path
+static double pair_buffer(const MdbCp* ctx)
+{
+    return ctx->pair_buffer >= 0.0 ? ctx->pair_buffer : ctx->p.cutneigh - ctx->p.cutforce;
+}
+
+// the next force evaluation derives the pair codes again
+static int mark_derive(MdbCp* ctx)
+{
+    if (!ctx->qflag) return MDB_OK;
+    CK(cudaMemsetAsync(ctx->qflag, 1, sizeof(int), ctx->s)); // any non-zero value
+    return MDB_OK;
+}
+
+// Buffers of the pair-list path for the current cluster and list capacities
+// (called after builds, never inside a capture: buffers that move drop the
+// captured graphs), then a derivation is due.
+static int ensure_pairs(MdbCp* ctx)
+{
+    if (!ctx->mixed || ctx->force_path != 1 || ctx->ncl_cap <= 0) return MDB_OK;
+    const int chmax = pair_chunks(ctx->maxneighs, ctx->N);
+    if (!ctx->qflag) {
+        CK(dalloc(&ctx->qflag, 2));
+        CK(cudaMemsetAsync(ctx->qflag, 0, 2 * sizeof(int), ctx->s));
+    }
+    if (ctx->pair_ncl < ctx->ncl_cap || ctx->pair_chmax != chmax) {
+        drop_graph(ctx);
+        dfree(ctx->pcode), dfree(ctx->pcnt), dfree(ctx->xq);
+        ctx->pair_ncl = ctx->pair_chmax = 0;
+        const size_t n2 = (size_t)ctx->ncl_cap * 2 * chmax;
+        CK(dalloc(&ctx->pcode, n2 * 256));
+        CK(dalloc(&ctx->pcnt, n2));
+        CK(dalloc(&ctx->xq, (size_t)ctx->ncl_cap * 4));
+        ctx->pair_ncl   = ctx->ncl_cap;
+        ctx->pair_chmax = chmax;
+    }
+    return mark_derive(ctx);
 }
 
 #define NEED_ATOMS()                                                                     \
@@ -757,17 +869,52 @@ static int do_build(MdbCp* ctx)
         if (r < 0) return -r;
         if (r == 0) {
             ctx->have_clusters = ctx->have_ghosts = ctx->have_list = true;
+            int rc = ensure_pairs(ctx);
+            if (rc) return rc;
             return snapshot(ctx);
         }
     }
     return fail(ctx, MDB_ERR_OVERFLOW, "rebuild did not converge");
 }
 
+static bool pair_path(const MdbCp* ctx) { return ctx->mixed && ctx->force_path == 1 && ctx->qflag; }
+
+// pair codes, when an atom moved past half the buffer or a build asked for it
+static void enq_derive(MdbCp* ctx, int force)
+{
+    const double rin = ctx->p.cutforce + pair_buffer(ctx);
+    launch_pair_derive(ctx->s, ctx->N, ctx->p.half_neigh, ctx->ty.uniform, ctx->ncl_cap, ctx->cnt,
+        ctx->xr, ctx->anchor, ctx->list, lcs(ctx), ctx->numneigh, (float)(rin * rin), ctx->qflag,
+        force, ctx->pcode, ctx->pcnt, ctx->pair_chmax, ctx->xq);
+}
+
+static int enq_force_pairs(MdbCp* ctx, bool energy)
+{
+    return launch_force_pairs(ctx->s, ctx->N, ctx->p.half_neigh, energy, ctx->ty.uniform,
+        ctx->ncl_cap, ctx->cnt, ctx->xr, ctx->anchor, ctx->pt, (float)ctx->cutforcesq, ctx->list,
+        lcs(ctx), ctx->numneigh, ctx->pcode, ctx->pcnt, ctx->pair_chmax, ctx->cf32,
+        ctx->partials, ctx->qflag);
+}
+
+// the integrator's test of the pair-list path: half the buffer, less a
+// margin for the FP32 rounding of the positions it compares
+static float pair_qlim2(const MdbCp* ctx)
+{
+    const double q = 0.5 * pair_buffer(ctx) * 0.999;
+    return (float)(q * q);
+}
+
 static void enq_force(MdbCp* ctx, bool energy)
 {
     cudaStream_t s = ctx->s;
     const int nloc_slots = ctx->ncl_cap * ctx->M;
-    if (ctx->mixed) {
+    if (pair_path(ctx)) {
+        if (ctx->p.half_neigh)
+            cudaMemsetAsync(ctx->cf32, 0, sizeof(float4) * (size_t)nloc_slots, s);
+        enq_derive(ctx, 0);
+        const int nb = enq_force_pairs(ctx, energy);
+        if (energy) ctx->energy_blocks = nb;
+    } else if (ctx->mixed) {
         if (ctx->p.half_neigh)
             cudaMemsetAsync(ctx->cf32, 0, sizeof(float4) * (size_t)nloc_slots, s);
         const int nb = launch_force_mixed(s, ctx->N, ctx->p.half_neigh, energy, ctx->ncl_cap,
@@ -792,10 +939,12 @@ static const double4* check_xb(const MdbCp* ctx)
 
 static void enq_initial(MdbCp* ctx)
 {
+    const bool pq = pair_path(ctx);
     launch_cp_initial(ctx->s, ctx->M, ctx->N, ctx->ncl_cap, ctx->cnt, ctx->p.dtforce, ctx->p.dt,
         ctx->cx, ctx->cv, ctx->cf, ctx->mixed ? ctx->cf32 : nullptr, ctx->anchor,
         ctx->mixed ? ctx->xr : nullptr, xr_mode(ctx), check_xb(ctx),
-        ctx->disp_max * ctx->disp_max, ctx->dflag);
+        ctx->disp_max * ctx->disp_max, ctx->dflag, pq ? ctx->xq : nullptr, pair_qlim2(ctx),
+        pq ? ctx->qflag : nullptr);
 }
 
 static void enq_final(MdbCp* ctx)
@@ -806,10 +955,12 @@ static void enq_final(MdbCp* ctx)
 
 static void enq_final_initial(MdbCp* ctx)
 {
+    const bool pq = pair_path(ctx);
     launch_cp_final_initial(ctx->s, ctx->M, ctx->N, ctx->ncl_cap, ctx->cnt, ctx->p.dtforce,
         ctx->p.dt, ctx->cx, ctx->cv, ctx->cf, ctx->mixed ? ctx->cf32 : nullptr, ctx->anchor,
         ctx->mixed ? ctx->xr : nullptr, xr_mode(ctx), check_xb(ctx),
-        ctx->disp_max * ctx->disp_max, ctx->dflag);
+        ctx->disp_max * ctx->disp_max, ctx->dflag, pq ? ctx->xq : nullptr, pair_qlim2(ctx),
+        pq ? ctx->qflag : nullptr);
 }
 
 static void enq_ghost_update(MdbCp* ctx)
@@ -822,6 +973,7 @@ static void enq_prune(MdbCp* ctx)
 {
     launch_prune(ctx->s, ctx->M, ctx->N, ctx->ncl_cap, ctx->cnt, ctx->cx, ctx->g.cutneighsq,
         ctx->maxneighs, lks(ctx), lcs(ctx), ctx->list, ctx->numneigh, ctx->nmasked);
+    if (pair_path(ctx)) mark_derive(ctx); // the rows moved: codes index list entries
 }
 
 // T and P from the atom arrays (as computeThermo reads them), KE of the
@@ -928,7 +1080,7 @@ extern "C" int mdb_cp_build_neighbor(MdbCp* ctx)
         if (r < 0) return -r;
         if (r == 0) {
             ctx->have_list = true;
-            return MDB_OK;
+            return ensure_pairs(ctx);
         }
         if (!ctx->have_ghosts) return do_build(ctx); // capacity change dropped the clusters
     }
@@ -1028,10 +1180,14 @@ extern "C" int mdb_cp_time_force(MdbCp* ctx, int reps, double* seconds)
         return fail(ctx, MDB_ERR_CUDA, "event", e);
     }
     long long m = mark();
-    for (int k = 0; k < 2; k++) enq_force(ctx, false);
+    // the pair-list path: the codes once, then the force kernel alone
+    const bool pq = pair_path(ctx);
+    if (pq) enq_derive(ctx, 1);
+    for (int k = 0; k < 2; k++) pq ? (void)enq_force_pairs(ctx, false) : enq_force(ctx, false);
     cudaEventRecord(e0, ctx->s);
-    for (int k = 0; k < reps; k++) enq_force(ctx, false);
+    for (int k = 0; k < reps; k++) pq ? (void)enq_force_pairs(ctx, false) : enq_force(ctx, false);
     cudaEventRecord(e1, ctx->s);
+    if (pq) enq_force(ctx, false); // the state's forces again (half lists accumulated)
     account(ctx, m);
     e = cudaEventSynchronize(e1);
     float ms = 0.f;
@@ -1933,6 +2089,9 @@ extern "C" int mdb_cp_ensemble_create(MdbCp* const* members, int n, MdbCpEnsembl
         if (c->dev != members[0]->dev || c->p.reneigh_every != members[0]->p.reneigh_every ||
             c->p.nstat != members[0]->p.nstat || c->prune_every != members[0]->prune_every)
             return MDB_ERR_ARG;
+        // the batched rebuild does not derive pair codes: members run the
+        // cluster-pair kernel
+        if (c->force_path != 0) return fail(c, MDB_ERR_ARG, "ensemble member on force_path 1");
     }
     MdbCpEnsemble* e = new MdbCpEnsemble();
     e->m.assign(members, members + n);

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 
+#include "mdb_cp_f2.cuh"
 #include "mdb_cp_internal.cuh"
 
 namespace mdb {
@@ -175,64 +176,6 @@ __device__ __forceinline__ void warp_reduce_12(float (&v)[12], int lane)
     v[0] = q[0];
     v[1] = q[1];
     v[2] = q[2];
-}
-
-// one vector reduction (red.global.add.v4.f32, sm_90+) instead of three
-// scalar atomics for a force update
-__device__ __forceinline__ void red_add4(float4* dst, float x, float y, float z)
-{
-    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(dst), "f"(x), "f"(y),
-                 "f"(z), "f"(0.0f)
-                 : "memory");
-}
-
-// PTX rcp.approx.ftz.f32: at most 1 ulp from 1/x, one MUFU operation
-__device__ __forceinline__ float rcp_approx(float x)
-{
-    float r;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
-}
-
-// Packed FP32 pairs: sm_100 executes add/sub/mul/fma on two f32 lanes of a
-// 64-bit register in one instruction (PTX .f32x2), so each thread carries its
-// 4 i atoms as two packed pairs (atoms 0,1 and 2,3) and computes two pairs per
-// instruction.
-typedef unsigned long long f2;
-
-__device__ __forceinline__ f2 f2_pack(float lo, float hi)
-{
-    f2 r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-    return r;
-}
-__device__ __forceinline__ void f2_unpack(f2 v, float& lo, float& hi)
-{
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
-}
-__device__ __forceinline__ f2 f2_add(f2 a, f2 b)
-{
-    f2 r;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-__device__ __forceinline__ f2 f2_sub(f2 a, f2 b)
-{
-    f2 r;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-__device__ __forceinline__ f2 f2_mul(f2 a, f2 b)
-{
-    f2 r;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-__device__ __forceinline__ f2 f2_fma(f2 a, f2 b, f2 c)
-{
-    f2 r;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
-    return r;
 }
 
 // The i side of one i-cluster: coordinates and type parameters of atoms
@@ -692,7 +635,8 @@ __device__ __forceinline__ void cp_integrate_slot(int s, int M, int N,
     const int* __restrict__ cnt, double dtf, double dt, double4* cx, double4* cv,
     const double4* __restrict__ cf, float4* cf32, const float4* __restrict__ anchor, float4* xr,
     bool zero_f, int xmode, const double4* __restrict__ xb = nullptr, double lim2 = 0.0,
-    int* flag = nullptr)
+    int* flag = nullptr, const float4* __restrict__ xq = nullptr, float qlim2 = 0.f,
+    int* qflag = nullptr)
 {
     if (s >= cnt[CP_NCL] * M) return;
     double4 p = cx[s];
@@ -717,6 +661,11 @@ __device__ __forceinline__ void cp_integrate_slot(int s, int M, int N,
         p.z += dt * v.z;
         cx[s] = p;
         if (xr) put_rel(xr, s, p, anchor[s / N], xmode, s % N);
+        if (xq) {
+            const float4 r = xr[s], q = xq[s];
+            const float dx = r.x - q.x, dy = r.y - q.y, dz = r.z - q.z;
+            if (dx * dx + dy * dy + dz * dz > qlim2) *qflag = 1;
+        }
         if (xb) {
             const double4 q = xb[s];
             const double dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
@@ -730,10 +679,11 @@ template <bool FINAL, bool INITIAL>
 __global__ void k_cp_integrate(int M, int N, const int* __restrict__ cnt, double dtf, double dt,
     double4* cx, double4* cv, const double4* __restrict__ cf, const float4* __restrict__ cf32,
     const float4* __restrict__ anchor, float4* xr, int xmode, const double4* __restrict__ xb,
-    double lim2, int* flag)
+    double lim2, int* flag, const float4* __restrict__ xq, float qlim2, int* qflag)
 {
     cp_integrate_slot<FINAL, INITIAL>(blockIdx.x * blockDim.x + threadIdx.x, M, N, cnt, dtf, dt,
-        cx, cv, cf, const_cast<float4*>(cf32), anchor, xr, false, xmode, xb, lim2, flag);
+        cx, cv, cf, const_cast<float4*>(cf32), anchor, xr, false, xmode, xb, lim2, flag, xq,
+        qlim2, qflag);
 }
 
 template <bool FINAL, bool INITIAL>
@@ -783,11 +733,12 @@ void launch_cp_integrate_batch(cudaStream_t s, bool final_, bool initial, int nb
 
 void launch_cp_initial(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt, double dtf,
     double dt, double4* cx, double4* cv, const double4* cf, const float4* cf32,
-    const float4* anchor, float4* xr, int xmode, const double4* xb, double lim2, int* flag)
+    const float4* anchor, float4* xr, int xmode, const double4* xb, double lim2, int* flag,
+    const float4* xq, float qlim2, int* qflag)
 {
     long long n = (long long)ncl_cap * M;
     k_cp_integrate<false, true><<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(M, N, cnt,
-        dtf, dt, cx, cv, cf, cf32, anchor, xr, xmode, xb, lim2, flag);
+        dtf, dt, cx, cv, cf, cf32, anchor, xr, xmode, xb, lim2, flag, xq, qlim2, qflag);
     g_launches++;
 }
 
@@ -797,17 +748,18 @@ void launch_cp_final(cudaStream_t s, int M, int ncl_cap, const int* cnt, double 
     long long n = (long long)ncl_cap * M;
     k_cp_integrate<true, false><<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(M, M, cnt,
         dtf, 0.0, const_cast<double4*>(cx), cv, cf, cf32, nullptr, nullptr, 0, nullptr, 0.0,
-        nullptr);
+        nullptr, nullptr, 0.f, nullptr);
     g_launches++;
 }
 
 void launch_cp_final_initial(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt,
     double dtf, double dt, double4* cx, double4* cv, const double4* cf, const float4* cf32,
-    const float4* anchor, float4* xr, int xmode, const double4* xb, double lim2, int* flag)
+    const float4* anchor, float4* xr, int xmode, const double4* xb, double lim2, int* flag,
+    const float4* xq, float qlim2, int* qflag)
 {
     long long n = (long long)ncl_cap * M;
     k_cp_integrate<true, true><<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(M, N, cnt,
-        dtf, dt, cx, cv, cf, cf32, anchor, xr, xmode, xb, lim2, flag);
+        dtf, dt, cx, cv, cf, cf32, anchor, xr, xmode, xb, lim2, flag, xq, qlim2, qflag);
     g_launches++;
 }
 

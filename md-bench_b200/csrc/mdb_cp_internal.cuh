@@ -186,15 +186,48 @@ int force_mixed_grid(int ncl_cap, const Types& ty);
 // xmode: the put_rel mode of xr (ignored when xr is null)
 // xb (null: no check): slot positions at the last build; a slot farther than
 // sqrt(lim2) from it sets *flag (the displacement check of a rebuild policy)
+// xq (null: no check): the mixed positions the pair codes were derived from;
+// a slot farther than sqrt(qlim2) from it sets *qflag (the pair-list path)
 void launch_cp_initial(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt, double dtf,
     double dt, double4* cx, double4* cv, const double4* cf, const float4* cf32,
-    const float4* anchor, float4* xr, int xmode, const double4* xb, double lim2, int* flag);
+    const float4* anchor, float4* xr, int xmode, const double4* xb, double lim2, int* flag,
+    const float4* xq = nullptr, float qlim2 = 0.f, int* qflag = nullptr);
 void launch_cp_final(cudaStream_t s, int M, int ncl_cap, const int* cnt, double dtf,
     const double4* cx, double4* cv, const double4* cf, const float4* cf32);
 void launch_cp_final_initial(cudaStream_t s, int M, int N, int ncl_cap, const int* cnt,
     double dtf, double dt, double4* cx, double4* cv, const double4* cf, const float4* cf32,
-    const float4* anchor, float4* xr, int xmode, const double4* xb, double lim2, int* flag);
+    const float4* anchor, float4* xr, int xmode, const double4* xb, double lim2, int* flag,
+    const float4* xq = nullptr, float qlim2 = 0.f, int* qflag = nullptr);
 int ke_blocks(int n);
+
+// ---- pair-list force path (mdb_cp_pairs.cu) ---------------------------------
+// LJ constants per (type i, type j): x = 48 eps s^2, y = 24 eps s, z = s, w = eps
+// with s = sigma_ij^6 = sigma_i^3 sigma_j^3 and eps = sqrt(eps_i eps_j) (the
+// reference's geometric rule, clusterpair/force_lj.c:130-132); one-type
+// systems use a0, b0, sig6_0, eps0
+struct PairTypes {
+    float4 tab[MDB_MAX_TYPES * MDB_MAX_TYPES];
+    float a0, b0, sig6_0;
+    double eps0;
+};
+// chunks of a list row of maxneighs entries (256 / N entries each)
+int pair_chunks(int maxneighs, int N);
+// blocks of the derivation and force launches (one warp per i-cluster)
+int pair_grid(int ncl_cap);
+// codes of every i pair (j atoms within sqrt(rin2)) and the positions they
+// were derived from (xq); returns at once unless qflag[0] or force is set;
+// qflag[1] counts the derivations that ran
+void launch_pair_derive(cudaStream_t s, int N, int half, int uniform, int ncl_cap,
+    const int* cnt, const float4* xr, const float4* anchor, const int* list, int cs,
+    const int* numneigh, float rin2, int* qflag, int force, unsigned char* pcode,
+    unsigned short* pcnt, int chmax, float4* xq);
+// forces from the codes; clears qflag[0]; returns the blocks launched
+// (= energy partials written)
+int launch_force_pairs(cudaStream_t s, int N, int half, int energy, int uniform, int ncl_cap,
+    const int* cnt, const float4* xr, const float4* anchor, const PairTypes& pt,
+    float cutforcesq, const int* list, int cs, const int* numneigh,
+    const unsigned char* pcode, const unsigned short* pcnt, int chmax, float4* cf32,
+    double* epart, int* qflag);
 
 // ---- batched launches over the members of an ensemble -----------------------
 // One launch covers every member: block b of the launch runs block bmap[b].y

@@ -1,0 +1,377 @@
+// Cluster-pair scheme, mixed precision: the pair-list force path.
+//
+// The cluster-pair list (built bit-exactly as the reference's
+// buildNeighborCPU, clusterpair/neighbor.c:282-765) lists whole 4 x N
+// cluster pairs: on the LJ liquid about a quarter of their pair slots lie
+// inside the cutoff, and the cluster-pair force kernel (mdb_cp_force.cu) pays
+// for all of them. This path derives from that list, per pair of i atoms
+// (atoms 0,1 and 2,3 of an i-cluster), the j atoms of its listed cluster
+// pairs that lie within r_in = r_c + buffer of either atom, and evaluates
+// only those: each lane holds one i pair packed in .f32x2 registers and
+// computes both pairs of a j atom per packed instruction.
+//
+// Exactness of the pair set: a pair left out had r > r_in when the codes
+// were derived; it can come inside r_c only after one of its atoms moved more
+// than buffer / 2. The integrator compares every atom's position with its
+// position at the last derivation and raises a device flag past that limit;
+// the derivation kernel runs at every force evaluation but returns at once
+// unless the flag is set (or a list build asked for it), so the pairs
+// evaluated are exactly the listed cluster pairs' pairs within r_c, as in the
+// cluster-pair kernels, with no host round trip inside the captured timestep.
+//
+// Codes: for i pair h of i-cluster ci and chunk c of its list row (chunks of
+// 256 / N entries), one byte per j atom, e * N + b (entry e of the chunk, atom
+// b of that j-cluster); pcnt holds the count. Storage is fixed at 256 bytes
+// per (i pair, chunk), so a derivation can never overflow it.
+#include "mdb_cp_f2.cuh"
+#include "mdb_cp_internal.cuh"
+
+namespace mdb {
+namespace cp {
+
+#define PAIR_THREADS 128
+#define PAIR_WARPS (PAIR_THREADS / 32)
+
+template <int N> struct PairChunk {
+    static constexpr int CH   = 256 / N; // list entries per chunk: codes e * N + b < 256
+    static constexpr int LOGN = N == 4 ? 2 : 3;
+};
+
+int pair_chunks(int maxneighs, int N) { return (maxneighs + 256 / N - 1) / (256 / N); }
+
+// i atom of an i-cluster in its cluster frame; padding (type -1, or with one
+// atom type the +1e18 position) reported invalid and moved to -1e18, where it
+// pairs with nothing
+template <bool UNIFORM>
+__device__ __forceinline__ float4 i_atom(const float4* __restrict__ xr, int slot, bool& valid,
+    int& type)
+{
+    float4 p = __ldg(&xr[slot]);
+    type     = UNIFORM ? 0 : __float_as_int(p.w);
+    valid    = UNIFORM ? p.x < 0.1f * CP_PAD_F : type >= 0;
+    if (!valid) {
+        p.x = p.y = p.z = -CP_PAD_F;
+        type            = 0;
+    }
+    return p;
+}
+
+// ---- derivation ---------------------------------------------------------------
+// One warp per i-cluster. Lane q of a pass takes atom q of the chunk's
+// flattened entries (entry q / N, atom q % N), tests it against the 4 i
+// atoms and is listed for each i pair with an atom within r_in (excluded
+// pairs of the diagonal entry, the reference's cond of
+// clusterpair/force_lj.c:108-123, do not count); ballots keep the list order.
+// Also records the i atoms' positions for the integrator's displacement test.
+// Returns at once unless *qflag or force is set.
+template <int N, bool HALF, bool UNIFORM>
+__global__ void __launch_bounds__(PAIR_THREADS) k_pair_derive(const int* __restrict__ cnt,
+    const float4* __restrict__ xr, const float4* __restrict__ anchor,
+    const int* __restrict__ list, int cs, const int* __restrict__ numneigh, float rin2,
+    int* qflag, int force, unsigned char* __restrict__ pcode,
+    unsigned short* __restrict__ pcnt, int chmax, float4* __restrict__ xq)
+{
+    if (!force && *(volatile int*)qflag == 0) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) qflag[1] += 1; // derivations run
+    constexpr int CH = PairChunk<N>::CH, LOGN = PairChunk<N>::LOGN;
+    const int lane = threadIdx.x & 31;
+    const int ci   = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int ncl  = cnt[CP_NCL];
+    if (ci >= ncl) return;
+    const int jfac = N / 4, ci_cj0 = ci / jfac, ai0 = 4 * (ci % jfac);
+    const float4 ai = __ldg(&anchor[ci_cj0]);
+    float xi[4], yi[4], zi[4];
+    bool vi[4];
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+        int t;
+        const float4 p = i_atom<UNIFORM>(xr, ci * 4 + a, vi[a], t);
+        xi[a] = p.x, yi[a] = p.y, zi[a] = p.z;
+    }
+    if (lane < 4) xq[ci * 4 + lane] = __ldg(&xr[ci * 4 + lane]);
+    const int nn      = numneigh[ci];
+    const int dummy   = cnt[CP_NCJ] + cnt[CP_NGC];
+    const int* row    = list + (size_t)ci * cs;
+    const int nch     = (nn + CH - 1) / CH;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int c = 0; c < nch; c++) {
+        const int ns       = min(CH, nn - c * CH) * N;
+        unsigned char* o0  = pcode + ((size_t)(2 * ci) * chmax + c) * 256;
+        unsigned char* o1  = o0 + (size_t)chmax * 256;
+        int n0 = 0, n1 = 0;
+        for (int q0 = 0; q0 < ns; q0 += 32) {
+            const int q    = q0 + lane;
+            const bool act = q < ns;
+            const int b    = q & (N - 1);
+            const int cj   = act ? __ldg(&row[c * CH + (q >> LOGN)]) : dummy;
+            const float4 x = __ldg(&xr[cj * N + b]);
+            const float4 a = __ldg(&anchor[cj]);
+            const float jx = x.x + (a.x - ai.x), jy = x.y + (a.y - ai.y),
+                        jz = x.z + (a.z - ai.z);
+            const bool diag = cj == ci_cj0;
+            bool in0 = false, in1 = false;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const float dx = xi[k] - jx, dy = yi[k] - jy, dz = zi[k] - jz;
+                const float r2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
+                const bool ex  = diag && (HALF ? (ai0 + k >= b) : (ai0 + k == b));
+                const bool ok  = act && vi[k] && !ex && r2 < rin2;
+                if (k < 2) in0 |= ok;
+                else in1 |= ok;
+            }
+            const unsigned m0 = __ballot_sync(0xffffffffu, in0);
+            const unsigned m1 = __ballot_sync(0xffffffffu, in1);
+            if (in0) o0[n0 + __popc(m0 & lt)] = (unsigned char)q;
+            if (in1) o1[n1 + __popc(m1 & lt)] = (unsigned char)q;
+            n0 += __popc(m0);
+            n1 += __popc(m1);
+        }
+        if (lane == 0) {
+            pcnt[(size_t)(2 * ci) * chmax + c]     = (unsigned short)n0;
+            pcnt[(size_t)(2 * ci + 1) * chmax + c] = (unsigned short)n1;
+        }
+    }
+}
+
+// ---- force --------------------------------------------------------------------
+// One warp per i-cluster; lanes 16h..16h+15 own i pair h (atoms 2h, 2h+1,
+// packed) and take its codes 16 at a time. Per chunk the warp first caches
+// the chunk's entries in shared memory (each j-cluster's slot base and its
+// anchor offset from the i-cluster's anchor: a difference of multiples of
+// 1/8, exact in FP32), so a code costs one shared load, one 16-byte j load
+// and the pair arithmetic. Half lists add each j atom's reaction (summed over
+// the pair) with one vector reduction; the i forces are reduced over the 16
+// lanes at the end. Thread 0 of block 0 clears the derivation flag (the
+// derivation of this evaluation has run before this kernel starts).
+template <int N, bool HALF, bool ENERGY, bool UNIFORM>
+__global__ void __launch_bounds__(PAIR_THREADS) k_force_pairs(const int* __restrict__ cnt,
+    const float4* __restrict__ xr, const float4* __restrict__ anchor, PairTypes pt,
+    float cutforcesq, const int* __restrict__ list, int cs, const int* __restrict__ numneigh,
+    const unsigned char* __restrict__ pcode, const unsigned short* __restrict__ pcnt,
+    int chmax, float4* cf32, double* epart, int* qflag)
+{
+    constexpr int CH = PairChunk<N>::CH, LOGN = PairChunk<N>::LOGN;
+    __shared__ float4 s_row[PAIR_WARPS][CH];
+    __shared__ float4 s_tab[UNIFORM ? 1 : MDB_MAX_TYPES * MDB_MAX_TYPES];
+    if (!UNIFORM) {
+        for (int k = threadIdx.x; k < MDB_MAX_TYPES * MDB_MAX_TYPES; k += blockDim.x)
+            s_tab[k] = pt.tab[k];
+        __syncthreads();
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) qflag[0] = 0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ci   = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int ncl  = cnt[CP_NCL];
+    double e       = 0.0;
+    if (ci < ncl) {
+        const int h = lane >> 4, s = lane & 15;
+        const int jfac = N / 4, ci_cj0 = ci / jfac, ai0 = 4 * (ci % jfac);
+        const int nloc = ncl * 4;
+        const float4 ai = __ldg(&anchor[ci_cj0]);
+        bool v0, v1;
+        int t0, t1;
+        const float4 p0 = i_atom<UNIFORM>(xr, ci * 4 + 2 * h, v0, t0);
+        const float4 p1 = i_atom<UNIFORM>(xr, ci * 4 + 2 * h + 1, v1, t1);
+        const f2 XI = f2_pack(p0.x, p1.x), YI = f2_pack(p0.y, p1.y), ZI = f2_pack(p0.z, p1.z);
+        // pairs of the diagonal entry excluded as the reference's cond
+        // (clusterpair/force_lj.c:108-123): bit 2b + k for i atom 2h + k and
+        // atom b of the i-cluster's own j-cluster
+        unsigned xtab = 0;
+#pragma unroll
+        for (int b = 0; b < N; b++)
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const int ia = ai0 + 2 * h + k;
+                if (HALF ? (ia >= b) : (ia == b)) xtab |= 1u << (2 * b + k);
+            }
+        const float cA    = pt.a0, cB = pt.b0, sig6u = pt.sig6_0;
+        const f2 A2 = f2_pack(cA, cA), mB2 = f2_pack(-cB, -cB);
+        f2 fx = 0, fy = 0, fz = 0;
+        const int nn     = numneigh[ci];
+        const int* row   = list + (size_t)ci * cs;
+        const int nch    = (nn + CH - 1) / CH;
+        const bool diag0 = nn > 0 && __ldg(&row[0]) == ci_cj0;
+        for (int c = 0; c < nch; c++) {
+            const int ne = min(CH, nn - c * CH);
+            for (int k = lane; k < ne; k += 32) {
+                const int cj   = __ldg(&row[c * CH + k]);
+                const float4 a = __ldg(&anchor[cj]);
+                s_row[warp][k] = make_float4(a.x - ai.x, a.y - ai.y, a.z - ai.z,
+                    __int_as_float(cj * N));
+            }
+            __syncwarp();
+            // codes and counts always come from a derivation on the current
+            // rows; the clamps keep every access inside this chunk regardless
+            const int ns               = ne * N;
+            const int ncode            = min((int)pcnt[(size_t)(2 * ci + h) * chmax + c], ns);
+            const unsigned char* codes = pcode + ((size_t)(2 * ci + h) * chmax + c) * 256;
+            for (int k = s; k < ncode; k += 16) {
+                const int q = codes[k];
+                if (q >= ns) continue;
+                const float4 d = s_row[warp][q >> LOGN];
+                const int sj   = __float_as_int(d.w) + (q & (N - 1));
+                float4 xj      = __ldg(&xr[sj]);
+                // into the i frame: the same roundings as the cluster-pair kernel
+                const f2 jxy = f2_add(f2_pack(xj.x, xj.y), f2_pack(d.x, d.y));
+                f2_unpack(jxy, xj.x, xj.y);
+                xj.z += d.z;
+                unsigned ex = 0;
+                if (c == 0 && diag0 && q < N) ex = (xtab >> (2 * q)) & 3u;
+                const f2 DX  = f2_sub(XI, f2_pack(xj.x, xj.x));
+                const f2 DY  = f2_sub(YI, f2_pack(xj.y, xj.y));
+                const f2 DZ  = f2_sub(ZI, f2_pack(xj.z, xj.z));
+                const f2 RSQ = f2_fma(DX, DX, f2_fma(DY, DY, f2_mul(DZ, DZ)));
+                float r0, r1;
+                f2_unpack(RSQ, r0, r1);
+                const bool in0 = r0 < cutforcesq && !(ex & 1u);
+                const bool in1 = r1 < cutforcesq && !(ex & 2u);
+                float u0 = rcp_approx(r0), u1 = rcp_approx(r1);
+                u0          = in0 ? u0 : 0.0f;
+                u1          = in1 ? u1 : 0.0f;
+                const f2 U  = f2_pack(u0, u1);
+                const f2 U2 = f2_mul(U, U);
+                const f2 U3 = f2_mul(U2, U);
+                f2 F;
+                float4 ta = make_float4(0.f, 0.f, 0.f, 0.f), tb = ta;
+                if (UNIFORM) {
+                    F = f2_mul(f2_mul(U2, U2), f2_fma(A2, U3, mB2));
+                } else {
+                    int tj = __float_as_int(xj.w);
+                    tj     = tj < 0 ? 0 : tj;
+                    ta     = s_tab[t0 * MDB_MAX_TYPES + tj];
+                    tb     = s_tab[t1 * MDB_MAX_TYPES + tj];
+                    F = f2_mul(f2_mul(U2, U2),
+                        f2_fma(f2_pack(ta.x, tb.x), U3, f2_pack(-ta.y, -tb.y)));
+                }
+                fx = f2_fma(DX, F, fx);
+                fy = f2_fma(DY, F, fy);
+                fz = f2_fma(DZ, F, fz);
+                if (HALF && sj < nloc) {
+                    float gx0, gx1, gy0, gy1, gz0, gz1;
+                    f2_unpack(f2_mul(DX, F), gx0, gx1);
+                    f2_unpack(f2_mul(DY, F), gy0, gy1);
+                    f2_unpack(f2_mul(DZ, F), gz0, gz1);
+                    red_add4(&cf32[sj], -(gx0 + gx1), -(gy0 + gy1), -(gz0 + gz1));
+                }
+                if (ENERGY) {
+                    // full lists see every pair twice; half lists once,
+                    // except pairs with ghost atoms, which both owners list
+                    const double ew = (!HALF || sj >= nloc) ? 0.5 : 1.0;
+                    float s0, s1;
+                    f2_unpack(f2_mul(UNIFORM ? f2_pack(sig6u, sig6u) : f2_pack(ta.z, tb.z), U3),
+                        s0, s1);
+                    const double E0 = UNIFORM ? pt.eps0 : (double)ta.w;
+                    const double E1 = UNIFORM ? pt.eps0 : (double)tb.w;
+                    if (in0) e += ew * 4.0 * E0 * (double)s0 * ((double)s0 - 1.0);
+                    if (in1) e += ew * 4.0 * E1 * (double)s1 * ((double)s1 - 1.0);
+                }
+            }
+            __syncwarp();
+        }
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) {
+            fx = f2_add(fx, __shfl_xor_sync(0xffffffffu, fx, o));
+            fy = f2_add(fy, __shfl_xor_sync(0xffffffffu, fy, o));
+            fz = f2_add(fz, __shfl_xor_sync(0xffffffffu, fz, o));
+        }
+        if (s == 0) {
+            float ax, bx, ay, by, az, bz;
+            f2_unpack(fx, ax, bx);
+            f2_unpack(fy, ay, by);
+            f2_unpack(fz, az, bz);
+            float4* dst = &cf32[ci * 4 + 2 * h];
+            if (HALF) {
+                if (v0) red_add4(dst, ax, ay, az);
+                if (v1) red_add4(dst + 1, bx, by, bz);
+            } else {
+                if (v0) dst[0] = make_float4(ax, ay, az, 0.f);
+                if (v1) dst[1] = make_float4(bx, by, bz, 0.f);
+            }
+        }
+    }
+    if (ENERGY) {
+        const double t = block_sum(e);
+        if (threadIdx.x == 0) epart[blockIdx.x] = t;
+    }
+}
+
+int pair_grid(int ncl_cap) { return (int)(((long long)ncl_cap * 32 + PAIR_THREADS - 1) / PAIR_THREADS); }
+
+template <int N, bool HALF>
+static void derive_n(cudaStream_t s, int uniform, int grid, const int* cnt, const float4* xr,
+    const float4* anchor, const int* list, int cs, const int* numneigh, float rin2, int* qflag,
+    int force, unsigned char* pcode, unsigned short* pcnt, int chmax, float4* xq)
+{
+    if (uniform)
+        k_pair_derive<N, HALF, true><<<grid, PAIR_THREADS, 0, s>>>(cnt, xr, anchor, list, cs,
+            numneigh, rin2, qflag, force, pcode, pcnt, chmax, xq);
+    else
+        k_pair_derive<N, HALF, false><<<grid, PAIR_THREADS, 0, s>>>(cnt, xr, anchor, list, cs,
+            numneigh, rin2, qflag, force, pcode, pcnt, chmax, xq);
+}
+
+void launch_pair_derive(cudaStream_t s, int N, int half, int uniform, int ncl_cap,
+    const int* cnt, const float4* xr, const float4* anchor, const int* list, int cs,
+    const int* numneigh, float rin2, int* qflag, int force, unsigned char* pcode,
+    unsigned short* pcnt, int chmax, float4* xq)
+{
+    const int grid = pair_grid(ncl_cap);
+    if (N == 4) {
+        if (half) derive_n<4, true>(s, uniform, grid, cnt, xr, anchor, list, cs, numneigh, rin2, qflag, force, pcode, pcnt, chmax, xq);
+        else derive_n<4, false>(s, uniform, grid, cnt, xr, anchor, list, cs, numneigh, rin2, qflag, force, pcode, pcnt, chmax, xq);
+    } else {
+        if (half) derive_n<8, true>(s, uniform, grid, cnt, xr, anchor, list, cs, numneigh, rin2, qflag, force, pcode, pcnt, chmax, xq);
+        else derive_n<8, false>(s, uniform, grid, cnt, xr, anchor, list, cs, numneigh, rin2, qflag, force, pcode, pcnt, chmax, xq);
+    }
+    g_launches++;
+}
+
+template <int N, bool HALF, bool ENERGY>
+static void pairs_e(cudaStream_t s, int uniform, int grid, const int* cnt, const float4* xr,
+    const float4* anchor, const PairTypes& pt, float cutforcesq, const int* list, int cs,
+    const int* numneigh, const unsigned char* pcode, const unsigned short* pcnt, int chmax,
+    float4* cf32, double* epart, int* qflag)
+{
+    if (uniform)
+        k_force_pairs<N, HALF, ENERGY, true><<<grid, PAIR_THREADS, 0, s>>>(cnt, xr, anchor, pt,
+            cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+    else
+        k_force_pairs<N, HALF, ENERGY, false><<<grid, PAIR_THREADS, 0, s>>>(cnt, xr, anchor, pt,
+            cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+}
+
+template <int N>
+static void pairs_n(cudaStream_t s, int half, int energy, int uniform, int grid,
+    const int* cnt, const float4* xr, const float4* anchor, const PairTypes& pt,
+    float cutforcesq, const int* list, int cs, const int* numneigh,
+    const unsigned char* pcode, const unsigned short* pcnt, int chmax, float4* cf32,
+    double* epart, int* qflag)
+{
+    if (half) {
+        if (energy) pairs_e<N, true, true>(s, uniform, grid, cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+        else pairs_e<N, true, false>(s, uniform, grid, cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+    } else {
+        if (energy) pairs_e<N, false, true>(s, uniform, grid, cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+        else pairs_e<N, false, false>(s, uniform, grid, cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+    }
+}
+
+int launch_force_pairs(cudaStream_t s, int N, int half, int energy, int uniform, int ncl_cap,
+    const int* cnt, const float4* xr, const float4* anchor, const PairTypes& pt,
+    float cutforcesq, const int* list, int cs, const int* numneigh,
+    const unsigned char* pcode, const unsigned short* pcnt, int chmax, float4* cf32,
+    double* epart, int* qflag)
+{
+    const int grid = pair_grid(ncl_cap);
+    if (N == 4)
+        pairs_n<4>(s, half, energy, uniform, grid, cnt, xr, anchor, pt, cutforcesq, list, cs,
+            numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+    else
+        pairs_n<8>(s, half, energy, uniform, grid, cnt, xr, anchor, pt, cutforcesq, list, cs,
+            numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+    g_launches++;
+    return grid;
+}
+
+} // namespace cp
+} // namespace mdb

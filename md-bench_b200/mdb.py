@@ -98,7 +98,8 @@ CP_EXPORTS = [
     "mdb_cp_get_columns", "mdb_cp_get_geometry", "mdb_cp_time_force", "mdb_cp_ensemble_create",
     "mdb_cp_ensemble_destroy", "mdb_cp_ensemble_last_error", "mdb_cp_ensemble_stream",
     "mdb_cp_ensemble_launch_count", "mdb_cp_ensemble_run", "mdb_cp_ensemble_tune",
-    "mdb_cp_set_rebuild_check", "mdb_cp_get_rebuilds",
+    "mdb_cp_set_rebuild_check", "mdb_cp_get_rebuilds", "mdb_cp_set_pair_buffer",
+    "mdb_cp_get_pair_stats",
 ]
 # every symbol include/mdb_host.h declares
 HOST_EXPORTS = [
@@ -173,6 +174,8 @@ def load():
         "mdb_cp_tune": ([vp, C.c_char_p, ip], ip),
         "mdb_cp_time_force": ([vp, ip, C.POINTER(C.c_double)], ip),
         "mdb_cp_set_rebuild_check": ([vp, C.c_double], ip),
+        "mdb_cp_set_pair_buffer": ([vp, C.c_double], ip),
+        "mdb_cp_get_pair_stats": ([vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], ip),
         "mdb_cp_get_rebuilds": ([vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], ip),
         "mdb_cp_ensemble_create": ([C.POINTER(vp), ip, C.POINTER(vp)], ip),
         "mdb_cp_ensemble_destroy": ([vp], ip),
@@ -835,6 +838,18 @@ class ClusterSystem:
         since the last build (0: the fixed schedule alone)."""
         self._ck(self.lib.mdb_cp_set_rebuild_check(self.h, float(max_displacement)),
                  "mdb_cp_set_rebuild_check")
+
+    def set_pair_buffer(self, buffer):
+        """r_in - r_c of the pair-list path (force_path 1); negative: the skin."""
+        self._ck(self.lib.mdb_cp_set_pair_buffer(self.h, float(buffer)),
+                 "mdb_cp_set_pair_buffer")
+
+    def pair_stats(self):
+        """(derivations run, j atoms listed over all i pairs) of the pair-list path."""
+        a, b = C.c_longlong(), C.c_longlong()
+        self._ck(self.lib.mdb_cp_get_pair_stats(self.h, C.byref(a), C.byref(b)),
+                 "mdb_cp_get_pair_stats")
+        return a.value, b.value
 
     def rebuilds(self):
         """(scheduled, displacement-triggered) rebuilds of checked runs."""
