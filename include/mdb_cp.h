@@ -57,7 +57,10 @@ int mdb_cp_synchronize(MdbCp* ctx);
  * within r_c + buffer of each other when last derived (see
  * mdb_cp_set_pair_buffer), re-derived inside the timestep whenever an atom
  * has moved more than buffer / 2 since: the same pairs inside r_c, so the
- * same forces up to FP32 summation order. */
+ * same forces up to FP32 summation order; "pair_variant" = 0..3: launch
+ * shape of the pair-list kernel (j loads in flight per lane and register
+ * budget: 0 = 4 loads, 1 = 2, 2 = 3 with a budget for 6 blocks of 128
+ * threads per SM, 3 = 2 with a budget for 8; default 0). */
 int mdb_cp_tune(MdbCp* ctx, const char* key, int value);
 /* Buffer of the pair-list path (force_path 1; no counterpart in the
  * reference): pairs are kept within r_c + buffer, and any atom moving more

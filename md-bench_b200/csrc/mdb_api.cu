@@ -69,6 +69,7 @@ struct MdbCtx {
     double* red = nullptr; // reductions: [slot*4 + {ke, pe_a, pe_b}]
     int nred_slots = 0;
     double* fp = nullptr;
+    float4* xe = nullptr; // mixed EAM: (cell-relative position, F'(rho)) of every atom
     double* stage  = nullptr; // 9 * nlocal doubles: AoS x, v, f for host transfers
     int* stage_t   = nullptr; // nlocal types
     double *eam_frho = nullptr, *eam_rhor = nullptr, *eam_z2r = nullptr;
@@ -428,6 +429,7 @@ static void free_atom_buffers(MdbCtx* ctx)
     dfree(ctx->partials);
     dfree(ctx->red);
     dfree(ctx->fp);
+    dfree(ctx->xe);
     dfree(ctx->stage);
     dfree(ctx->stage_t);
     if (ctx->h_red) cudaFreeHost(ctx->h_red);
@@ -497,6 +499,7 @@ static int alloc_ghost_sized(MdbCtx* ctx, int ghost_cap)
     dfree(ctx->bin_x);
     dfree(ctx->bin_xf);
     dfree(ctx->fp);
+    dfree(ctx->xe);
     CK(dalloc(&ctx->border_map, ghost_cap));
     CK(dalloc(&ctx->pbc_code, ghost_cap));
     CK(dalloc(&ctx->atom_bin, nall));
@@ -505,6 +508,7 @@ static int alloc_ghost_sized(MdbCtx* ctx, int ghost_cap)
     CK(dalloc(&ctx->bin_x, nall));
     CK(dalloc(&ctx->bin_xf, nall));
     if (ctx->p.force_field == MDB_FF_EAM) CK(dalloc(&ctx->fp, nall));
+    if (ctx->p.force_field == MDB_FF_EAM && ctx->mixed) CK(dalloc(&ctx->xe, nall));
     ctx->ghost_cap   = ghost_cap;
     ctx->nall_cap    = nall;
     ctx->have_ghosts = false;
@@ -561,7 +565,8 @@ extern "C" int mdb_set_atoms(MdbCtx* ctx, int nlocal, const double* x, const dou
         int nscan         = std::max(scan_scratch_ints(nlocal), scan_scratch_ints(ctx->g.mbins));
         ctx->scan_scratch_n = nscan;
         CK(dalloc(&ctx->scan_scratch, nscan));
-        ctx->npart = std::max(force_partial_blocks(nlocal), ke_partial_blocks(nlocal));
+        ctx->npart = std::max(std::max(force_partial_blocks(nlocal), ke_partial_blocks(nlocal)),
+            eam_mixed_blocks(nlocal));
         CK(dalloc(&ctx->partials, 3 * (size_t)ctx->npart));
         ctx->nred_slots = 64;
         CK(dalloc(&ctx->red, 4 * (size_t)ctx->nred_slots));
@@ -662,15 +667,16 @@ static void enq_force(MdbCtx* ctx, bool energy)
     double* ep0    = ctx->partials;
     double* ep1    = ctx->partials + ctx->npart;
     if (ctx->p.force_field == MDB_FF_EAM) {
-        if (ctx->mixed)
-            launch_eam_mixed(s, energy, n, ctx->ghost_cap, nullptr,ctx->xr,
-                ctx->shift, ctx->numneigh, ctx->neighbors, ctx->ld, (float)ctx->cutforcesq,
-                ctx->eam, ctx->border_map, ctx->counters, ctx->fp, ctx->fx, ctx->fy, ctx->fz,
-                ep0, ep1);
-        else
+        if (ctx->mixed) {
+            launch_eam_mixed(s, energy, ctx->p.precision == MDB_PREC_MIXED_COMP,
+                n, ctx->ghost_cap, ctx->xr, ctx->shift, ctx->numneigh, ctx->neighbors, ctx->ld,
+                (float)ctx->cutforcesq, ctx->eam, ctx->border_map, ctx->counters, ctx->fp,
+                ctx->xe, ctx->fx, ctx->fy, ctx->fz, ep0, ep1);
+        } else {
             launch_eam_fp64(s, energy, n, ctx->ghost_cap, nullptr,ctx->x,
                 ctx->numneigh, ctx->neighbors, ctx->ld, ctx->cutforcesq, ctx->eam,
                 ctx->border_map, ctx->counters, ctx->fp, ctx->fx, ctx->fy, ctx->fz, ep0, ep1);
+        }
         return;
     }
     if (ctx->p.half_neigh) {
@@ -995,7 +1001,10 @@ static void enq_thermo(MdbCtx* ctx, int slot, bool with_pe)
         ctx->partials + 2 * (size_t)ctx->npart);
     launch_reduce_partials(s, nke, ctx->partials + 2 * (size_t)ctx->npart, r + 0);
     if (with_pe) {
-        int nf = force_partial_blocks(ctx->nlocal);
+        // the mixed EAM passes write eam_mixed_blocks partials, the rest one
+        // per block of the force kernels
+        int nf = ctx->p.force_field == MDB_FF_EAM && ctx->mixed ? eam_mixed_blocks(ctx->nlocal)
+                                                               : force_partial_blocks(ctx->nlocal);
         launch_reduce_partials(s, nf, ctx->partials, r + 1);
         if (ctx->p.force_field == MDB_FF_EAM)
             launch_reduce_partials(s, nf, ctx->partials + ctx->npart, r + 2);

@@ -306,6 +306,12 @@ extern "C" int mdb_cp_tune(MdbCp* ctx, const char* key, int value)
         ctx->ty.force_variant = value;
         return MDB_OK;
     }
+    if (!strcmp(key, "pair_variant")) {
+        if (value < 0 || value > 3) return MDB_ERR_ARG;
+        drop_graph(ctx);
+        ctx->ty.pair_variant = value;
+        return MDB_OK;
+    }
     if (!strcmp(key, "force_path")) {
         if (value < 0 || value > 1 || (value == 1 && !ctx->mixed)) return MDB_ERR_ARG;
         drop_graph(ctx);
@@ -601,8 +607,8 @@ static int ensure_pairs(MdbCp* ctx)
     if (!ctx->mixed || ctx->force_path != 1 || ctx->ncl_cap <= 0) return MDB_OK;
     const int chmax = pair_chunks(ctx->maxneighs, ctx->N);
     if (!ctx->qflag) {
-        CK(dalloc(&ctx->qflag, 2));
-        CK(cudaMemsetAsync(ctx->qflag, 0, 2 * sizeof(int), ctx->s));
+        CK(dalloc(&ctx->qflag, 3));
+        CK(cudaMemsetAsync(ctx->qflag, 0, 3 * sizeof(int), ctx->s));
     }
     if (ctx->pair_ncl < ctx->ncl_cap || ctx->pair_chmax != chmax) {
         drop_graph(ctx);
@@ -879,7 +885,8 @@ static int do_build(MdbCp* ctx)
 
 static bool pair_path(const MdbCp* ctx) { return ctx->mixed && ctx->force_path == 1 && ctx->qflag; }
 
-// pair codes, when an atom moved past half the buffer or a build asked for it
+// pair codes, when an atom moved past half the buffer, a build asked for it,
+// or force
 static void enq_derive(MdbCp* ctx, int force)
 {
     const double rin = ctx->p.cutforce + pair_buffer(ctx);
@@ -891,7 +898,7 @@ static void enq_derive(MdbCp* ctx, int force)
 static int enq_force_pairs(MdbCp* ctx, bool energy)
 {
     return launch_force_pairs(ctx->s, ctx->N, ctx->p.half_neigh, energy, ctx->ty.uniform,
-        ctx->ncl_cap, ctx->cnt, ctx->xr, ctx->anchor, ctx->pt, (float)ctx->cutforcesq, ctx->list,
+        ctx->ty.pair_variant, ctx->ncl_cap, ctx->cnt, ctx->xr, ctx->anchor, ctx->pt, (float)ctx->cutforcesq, ctx->list,
         lcs(ctx), ctx->numneigh, ctx->pcode, ctx->pcnt, ctx->pair_chmax, ctx->cf32,
         ctx->partials, ctx->qflag);
 }
@@ -1180,7 +1187,8 @@ extern "C" int mdb_cp_time_force(MdbCp* ctx, int reps, double* seconds)
         return fail(ctx, MDB_ERR_CUDA, "event", e);
     }
     long long m = mark();
-    // the pair-list path: the codes once, then the force kernel alone
+    // the pair-list path: the codes once, then the force kernel on them
+    // alone (half lists accumulate: the forces are restored below)
     const bool pq = pair_path(ctx);
     if (pq) enq_derive(ctx, 1);
     for (int k = 0; k < 2; k++) pq ? (void)enq_force_pairs(ctx, false) : enq_force(ctx, false);

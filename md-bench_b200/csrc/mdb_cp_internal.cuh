@@ -85,6 +85,7 @@ struct Types {
     int force_block;       // threads per block of the mixed force kernel (tunable)
     int force_variant;     // mixed force kernel: bit 0 prefetch 2 ahead, bit 1 register budget
     int force_swizzle;     // mixed force kernel: blocks walk contiguous cluster ranges (0/1)
+    int pair_variant;      // pair-list force kernel: launch shape (0..3)
 };
 
 __device__ __forceinline__ int slot_type(const double4& p) { return (int)__double_as_longlong(p.w); }
@@ -221,9 +222,10 @@ void launch_pair_derive(cudaStream_t s, int N, int half, int uniform, int ncl_ca
     const int* cnt, const float4* xr, const float4* anchor, const int* list, int cs,
     const int* numneigh, float rin2, int* qflag, int force, unsigned char* pcode,
     unsigned short* pcnt, int chmax, float4* xq);
-// forces from the codes; clears qflag[0]; returns the blocks launched
-// (= energy partials written)
-int launch_force_pairs(cudaStream_t s, int N, int half, int energy, int uniform, int ncl_cap,
+// forces from the codes; clears qflag[0]; variant: launch shape (0..3);
+// returns the blocks launched (= energy partials written)
+int launch_force_pairs(cudaStream_t s, int N, int half, int energy, int uniform, int variant,
+    int ncl_cap,
     const int* cnt, const float4* xr, const float4* anchor, const PairTypes& pt,
     float cutforcesq, const int* list, int cs, const int* numneigh,
     const unsigned char* pcode, const unsigned short* pcnt, int chmax, float4* cf32,

@@ -23,6 +23,8 @@
 // 256 / N entries), one byte per j atom, e * N + b (entry e of the chunk, atom
 // b of that j-cluster); pcnt holds the count. Storage is fixed at 256 bytes
 // per (i pair, chunk), so a derivation can never overflow it.
+#include <algorithm>
+
 #include "mdb_cp_f2.cuh"
 #include "mdb_cp_internal.cuh"
 
@@ -31,6 +33,10 @@ namespace cp {
 
 #define PAIR_THREADS 128
 #define PAIR_WARPS (PAIR_THREADS / 32)
+// launch shapes of the force kernel (tuning key pair_variant; results do not
+// depend on them): codes a lane has in flight, and the minimum resident blocks
+// of 128 threads per SM asked of the register allocator (0: no request)
+static constexpr int PAIR_VARIANTS[4][2] = {{4, 0}, {2, 0}, {3, 6}, {2, 8}};
 
 template <int N> struct PairChunk {
     static constexpr int CH   = 256 / N; // list entries per chunk: codes e * N + b < 256
@@ -56,14 +62,78 @@ __device__ __forceinline__ float4 i_atom(const float4* __restrict__ xr, int slot
     return p;
 }
 
-// ---- derivation ---------------------------------------------------------------
-// One warp per i-cluster. Lane q of a pass takes atom q of the chunk's
-// flattened entries (entry q / N, atom q % N), tests it against the 4 i
-// atoms and is listed for each i pair with an atom within r_in (excluded
-// pairs of the diagonal entry, the reference's cond of
-// clusterpair/force_lj.c:108-123, do not count); ballots keep the list order.
-// Also records the i atoms' positions for the integrator's displacement test.
-// Returns at once unless *qflag or force is set.
+// ---- one code: a j atom against the lane's i pair ------------------------------
+// Packed FP32: both pairs per instruction, the cutoff and the exclusion bits
+// ex (bit k: pair with i atom 2h + k excluded) as select masks. The j
+// position is already in the i frame. Half lists add the reaction on local j
+// atoms (summed over the pair) with one vector reduction.
+template <bool HALF, bool ENERGY, bool UNIFORM>
+__device__ __forceinline__ void pair2(const f2& XI, const f2& YI, const f2& ZI,
+    const float4& xj, int sj, unsigned ex, int t0, int t1, const float4* s_tab,
+    const PairTypes& pt, float cutforcesq, const f2& A2, const f2& mB2, int nloc, f2& fx,
+    f2& fy, f2& fz, float4* cf32, double& e)
+{
+    const f2 DX  = f2_sub(XI, f2_pack(xj.x, xj.x));
+    const f2 DY  = f2_sub(YI, f2_pack(xj.y, xj.y));
+    const f2 DZ  = f2_sub(ZI, f2_pack(xj.z, xj.z));
+    const f2 RSQ = f2_fma(DX, DX, f2_fma(DY, DY, f2_mul(DZ, DZ)));
+    float r0, r1;
+    f2_unpack(RSQ, r0, r1);
+    const bool in0 = r0 < cutforcesq && !(ex & 1u);
+    const bool in1 = r1 < cutforcesq && !(ex & 2u);
+    float u0 = rcp_approx(r0), u1 = rcp_approx(r1);
+    u0          = in0 ? u0 : 0.0f;
+    u1          = in1 ? u1 : 0.0f;
+    const f2 U  = f2_pack(u0, u1);
+    const f2 U2 = f2_mul(U, U);
+    const f2 U3 = f2_mul(U2, U);
+    f2 F;
+    float4 ta = make_float4(0.f, 0.f, 0.f, 0.f), tb = ta;
+    if (UNIFORM) {
+        F = f2_mul(f2_mul(U2, U2), f2_fma(A2, U3, mB2));
+    } else {
+        int tj = __float_as_int(xj.w);
+        tj     = tj < 0 ? 0 : tj;
+        ta     = s_tab[t0 * MDB_MAX_TYPES + tj];
+        tb     = s_tab[t1 * MDB_MAX_TYPES + tj];
+        F = f2_mul(f2_mul(U2, U2), f2_fma(f2_pack(ta.x, tb.x), U3, f2_pack(-ta.y, -tb.y)));
+    }
+    fx = f2_fma(DX, F, fx);
+    fy = f2_fma(DY, F, fy);
+    fz = f2_fma(DZ, F, fz);
+    if (HALF && sj < nloc) {
+        float gx0, gx1, gy0, gy1, gz0, gz1;
+        f2_unpack(f2_mul(DX, F), gx0, gx1);
+        f2_unpack(f2_mul(DY, F), gy0, gy1);
+        f2_unpack(f2_mul(DZ, F), gz0, gz1);
+        red_add4(&cf32[sj], -(gx0 + gx1), -(gy0 + gy1), -(gz0 + gz1));
+    }
+    if (ENERGY) {
+        // full lists see every pair twice; half lists once, except pairs
+        // with ghost atoms, which both owners list
+        const double ew = (!HALF || sj >= nloc) ? 0.5 : 1.0;
+        float s0, s1;
+        f2_unpack(f2_mul(UNIFORM ? f2_pack(pt.sig6_0, pt.sig6_0) : f2_pack(ta.z, tb.z), U3), s0,
+            s1);
+        const double E0 = UNIFORM ? pt.eps0 : (double)ta.w;
+        const double E1 = UNIFORM ? pt.eps0 : (double)tb.w;
+        if (in0) e += ew * 4.0 * E0 * (double)s0 * ((double)s0 - 1.0);
+        if (in1) e += ew * 4.0 * E1 * (double)s1 * ((double)s1 - 1.0);
+    }
+}
+
+// ---- derivation ----------------------------------------------------------------
+// Runs before every force evaluation and returns at once unless the flag is
+// set (an atom moved past half the buffer since the last derivation, or a
+// build asked for it) or force is given; its grid is one wave of resident
+// blocks that loops over the clusters, so the common case costs one wave of
+// early exits. One warp per i-cluster at a time: the warp caches the chunk's
+// entries (slot base, anchor offset) in shared memory, then tests every atom
+// of them against the cluster's 4 i atoms, two candidate passes in flight,
+// with the reference's exclusions on the diagonal entry
+// (clusterpair/force_lj.c:108-123); ballots keep the list order; the codes of
+// both i pairs, their counts and the i atoms' positions (for the
+// integrator's test) are written.
 template <int N, bool HALF, bool UNIFORM>
 __global__ void __launch_bounds__(PAIR_THREADS) k_pair_derive(const int* __restrict__ cnt,
     const float4* __restrict__ xr, const float4* __restrict__ anchor,
@@ -74,81 +144,102 @@ __global__ void __launch_bounds__(PAIR_THREADS) k_pair_derive(const int* __restr
     if (!force && *(volatile int*)qflag == 0) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) qflag[1] += 1; // derivations run
     constexpr int CH = PairChunk<N>::CH, LOGN = PairChunk<N>::LOGN;
-    const int lane = threadIdx.x & 31;
-    const int ci   = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    __shared__ float4 s_row[PAIR_WARPS][CH];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ncl  = cnt[CP_NCL];
-    if (ci >= ncl) return;
-    const int jfac = N / 4, ci_cj0 = ci / jfac, ai0 = 4 * (ci % jfac);
-    const float4 ai = __ldg(&anchor[ci_cj0]);
-    float xi[4], yi[4], zi[4];
-    bool vi[4];
-#pragma unroll
-    for (int a = 0; a < 4; a++) {
-        int t;
-        const float4 p = i_atom<UNIFORM>(xr, ci * 4 + a, vi[a], t);
-        xi[a] = p.x, yi[a] = p.y, zi[a] = p.z;
-    }
-    if (lane < 4) xq[ci * 4 + lane] = __ldg(&xr[ci * 4 + lane]);
-    const int nn      = numneigh[ci];
-    const int dummy   = cnt[CP_NCJ] + cnt[CP_NGC];
-    const int* row    = list + (size_t)ci * cs;
-    const int nch     = (nn + CH - 1) / CH;
+    const int jfac = N / 4;
     const unsigned lt = (1u << lane) - 1u;
-    for (int c = 0; c < nch; c++) {
-        const int ns       = min(CH, nn - c * CH) * N;
-        unsigned char* o0  = pcode + ((size_t)(2 * ci) * chmax + c) * 256;
-        unsigned char* o1  = o0 + (size_t)chmax * 256;
-        int n0 = 0, n1 = 0;
-        for (int q0 = 0; q0 < ns; q0 += 32) {
-            const int q    = q0 + lane;
-            const bool act = q < ns;
-            const int b    = q & (N - 1);
-            const int cj   = act ? __ldg(&row[c * CH + (q >> LOGN)]) : dummy;
-            const float4 x = __ldg(&xr[cj * N + b]);
-            const float4 a = __ldg(&anchor[cj]);
-            const float jx = x.x + (a.x - ai.x), jy = x.y + (a.y - ai.y),
-                        jz = x.z + (a.z - ai.z);
-            const bool diag = cj == ci_cj0;
-            bool in0 = false, in1 = false;
+    for (int ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ci < ncl;
+         ci += (gridDim.x * blockDim.x) >> 5) {
+        const int ci_cj0 = ci / jfac, ai0 = 4 * (ci % jfac);
+        const int nn     = __ldg(&numneigh[ci]);
+        const int* row   = list + (size_t)ci * cs;
+        const float4 ai  = __ldg(&anchor[ci_cj0]);
+        float xi[4], yi[4], zi[4];
+        unsigned vmask = 0;
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const float dx = xi[k] - jx, dy = yi[k] - jy, dz = zi[k] - jz;
-                const float r2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
-                const bool ex  = diag && (HALF ? (ai0 + k >= b) : (ai0 + k == b));
-                const bool ok  = act && vi[k] && !ex && r2 < rin2;
-                if (k < 2) in0 |= ok;
-                else in1 |= ok;
-            }
-            const unsigned m0 = __ballot_sync(0xffffffffu, in0);
-            const unsigned m1 = __ballot_sync(0xffffffffu, in1);
-            if (in0) o0[n0 + __popc(m0 & lt)] = (unsigned char)q;
-            if (in1) o1[n1 + __popc(m1 & lt)] = (unsigned char)q;
-            n0 += __popc(m0);
-            n1 += __popc(m1);
+        for (int a = 0; a < 4; a++) {
+            bool v;
+            int t;
+            const float4 p = i_atom<UNIFORM>(xr, ci * 4 + a, v, t);
+            xi[a] = p.x, yi[a] = p.y, zi[a] = p.z;
+            vmask |= (v ? 1u : 0u) << a;
         }
-        if (lane == 0) {
-            pcnt[(size_t)(2 * ci) * chmax + c]     = (unsigned short)n0;
-            pcnt[(size_t)(2 * ci + 1) * chmax + c] = (unsigned short)n1;
+        if (lane < 4) xq[ci * 4 + lane] = __ldg(&xr[ci * 4 + lane]);
+        const int nch = (nn + CH - 1) / CH;
+        for (int c = 0; c < nch; c++) {
+            const int ne = min(CH, nn - c * CH);
+            const int ns = ne * N;
+            for (int k = lane; k < ne; k += 32) {
+                const int cj   = __ldg(&row[c * CH + k]);
+                const float4 a = __ldg(&anchor[cj]);
+                s_row[warp][k] = make_float4(a.x - ai.x, a.y - ai.y, a.z - ai.z,
+                    __int_as_float(cj * N));
+            }
+            __syncwarp();
+            unsigned char* o0 = pcode + ((size_t)(2 * ci) * chmax + c) * 256;
+            unsigned char* o1 = o0 + (size_t)chmax * 256;
+            int n0 = 0, n1 = 0;
+            for (int q0 = 0; q0 < ns; q0 += 64) {
+                float4 xa[2], da[2];
+                int qa[2];
+#pragma unroll
+                for (int u = 0; u < 2; u++) {
+                    qa[u]          = q0 + 32 * u + lane;
+                    const bool act = qa[u] < ns;
+                    da[u]          = s_row[warp][act ? qa[u] >> LOGN : 0];
+                    xa[u] = act ? __ldg(&xr[__float_as_int(da[u].w) + (qa[u] & (N - 1))])
+                                : make_float4(CP_PAD_F, CP_PAD_F, CP_PAD_F, 0.f);
+                }
+#pragma unroll
+                for (int u = 0; u < 2; u++) {
+                    const int b    = qa[u] & (N - 1);
+                    const float jx = xa[u].x + da[u].x, jy = xa[u].y + da[u].y,
+                                jz = xa[u].z + da[u].z;
+                    const bool dg  = __float_as_int(da[u].w) == ci_cj0 * N;
+                    bool in0 = false, in1 = false;
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        const float dx = xi[k] - jx, dy = yi[k] - jy, dz = zi[k] - jz;
+                        const float r2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
+                        const bool ex  = dg && (HALF ? (ai0 + k >= b) : (ai0 + k == b));
+                        const bool ok  = ((vmask >> k) & 1u) && !ex && r2 < rin2;
+                        if (k < 2) in0 |= ok;
+                        else in1 |= ok;
+                    }
+                    const unsigned m0 = __ballot_sync(0xffffffffu, in0);
+                    const unsigned m1 = __ballot_sync(0xffffffffu, in1);
+                    if (in0) o0[n0 + __popc(m0 & lt)] = (unsigned char)qa[u];
+                    if (in1) o1[n1 + __popc(m1 & lt)] = (unsigned char)qa[u];
+                    n0 += __popc(m0);
+                    n1 += __popc(m1);
+                }
+            }
+            if (lane == 0) {
+                pcnt[(size_t)(2 * ci) * chmax + c]     = (unsigned short)n0;
+                pcnt[(size_t)(2 * ci + 1) * chmax + c] = (unsigned short)n1;
+            }
+            __syncwarp(); // the cached row is rewritten for the next chunk
         }
     }
 }
 
-// ---- force --------------------------------------------------------------------
+// ---- force -------------------------------------------------------------------
 // One warp per i-cluster; lanes 16h..16h+15 own i pair h (atoms 2h, 2h+1,
-// packed) and take its codes 16 at a time. Per chunk the warp first caches
-// the chunk's entries in shared memory (each j-cluster's slot base and its
-// anchor offset from the i-cluster's anchor: a difference of multiples of
-// 1/8, exact in FP32), so a code costs one shared load, one 16-byte j load
-// and the pair arithmetic. Half lists add each j atom's reaction (summed over
-// the pair) with one vector reduction; the i forces are reduced over the 16
-// lanes at the end. Thread 0 of block 0 clears the derivation flag (the
-// derivation of this evaluation has run before this kernel starts).
-template <int N, bool HALF, bool ENERGY, bool UNIFORM>
-__global__ void __launch_bounds__(PAIR_THREADS) k_force_pairs(const int* __restrict__ cnt,
+// packed). Every load that depends on no other is issued first (row length,
+// first list entries, first codes and their count, i atoms, anchor); per
+// chunk the warp then caches the entries in shared memory (each j-cluster's
+// slot base and its anchor offset from the i-cluster's anchor, a difference
+// of multiples of 1/8 and so exact in FP32), and each lane takes its codes
+// PAIR_BATCH at a time with all their j loads in flight together. Thread 0
+// of block 0 clears the derivation flag (the derivation kernel of this
+// evaluation has completed before this kernel starts).
+template <int N, bool HALF, bool ENERGY, bool UNIFORM, int PAIR_BATCH, int MINB>
+__global__ void __launch_bounds__(PAIR_THREADS, MINB ? MINB : 1) k_force_pairs(const int* __restrict__ cnt,
     const float4* __restrict__ xr, const float4* __restrict__ anchor, PairTypes pt,
     float cutforcesq, const int* __restrict__ list, int cs, const int* __restrict__ numneigh,
-    const unsigned char* __restrict__ pcode, const unsigned short* __restrict__ pcnt,
-    int chmax, float4* cf32, double* epart, int* qflag)
+    const unsigned char* __restrict__ pcode, const unsigned short* __restrict__ pcnt, int chmax,
+    float4* cf32, double* epart, int* qflag)
 {
     constexpr int CH = PairChunk<N>::CH, LOGN = PairChunk<N>::LOGN;
     __shared__ float4 s_row[PAIR_WARPS][CH];
@@ -167,15 +258,25 @@ __global__ void __launch_bounds__(PAIR_THREADS) k_force_pairs(const int* __restr
         const int h = lane >> 4, s = lane & 15;
         const int jfac = N / 4, ci_cj0 = ci / jfac, ai0 = 4 * (ci % jfac);
         const int nloc = ncl * 4;
+        // loads that depend on nothing else
+        const int nn          = __ldg(&numneigh[ci]);
+        const int* row        = list + (size_t)ci * cs;
+        int rw0               = lane < cs ? __ldg(&row[lane]) : 0;
+        int rw1               = (CH > 32 && lane + 32 < cs) ? __ldg(&row[lane + 32]) : 0;
+        const unsigned char* mycode = pcode + (size_t)(2 * ci + h) * chmax * 256;
+        int ncode             = pcnt[(size_t)(2 * ci + h) * chmax];
+        int cw[PAIR_BATCH];
+#pragma unroll
+        for (int m = 0; m < PAIR_BATCH; m++)
+            cw[m] = mycode[s + 16 * m];
         const float4 ai = __ldg(&anchor[ci_cj0]);
         bool v0, v1;
         int t0, t1;
         const float4 p0 = i_atom<UNIFORM>(xr, ci * 4 + 2 * h, v0, t0);
         const float4 p1 = i_atom<UNIFORM>(xr, ci * 4 + 2 * h + 1, v1, t1);
         const f2 XI = f2_pack(p0.x, p1.x), YI = f2_pack(p0.y, p1.y), ZI = f2_pack(p0.z, p1.z);
-        // pairs of the diagonal entry excluded as the reference's cond
-        // (clusterpair/force_lj.c:108-123): bit 2b + k for i atom 2h + k and
-        // atom b of the i-cluster's own j-cluster
+        // exclusion bits of the diagonal entry for the lane's pair: bit 2b + k
+        // for i atom 2h + k and atom b of the i-cluster's own j-cluster
         unsigned xtab = 0;
 #pragma unroll
         for (int b = 0; b < N; b++)
@@ -184,86 +285,66 @@ __global__ void __launch_bounds__(PAIR_THREADS) k_force_pairs(const int* __restr
                 const int ia = ai0 + 2 * h + k;
                 if (HALF ? (ia >= b) : (ia == b)) xtab |= 1u << (2 * b + k);
             }
-        const float cA    = pt.a0, cB = pt.b0, sig6u = pt.sig6_0;
-        const f2 A2 = f2_pack(cA, cA), mB2 = f2_pack(-cB, -cB);
+        const f2 A2 = f2_pack(pt.a0, pt.a0), mB2 = f2_pack(-pt.b0, -pt.b0);
         f2 fx = 0, fy = 0, fz = 0;
-        const int nn     = numneigh[ci];
-        const int* row   = list + (size_t)ci * cs;
         const int nch    = (nn + CH - 1) / CH;
-        const bool diag0 = nn > 0 && __ldg(&row[0]) == ci_cj0;
+        const bool diag0 = nn > 0 && __shfl_sync(0xffffffffu, rw0, 0) == ci_cj0;
         for (int c = 0; c < nch; c++) {
             const int ne = min(CH, nn - c * CH);
-            for (int k = lane; k < ne; k += 32) {
-                const int cj   = __ldg(&row[c * CH + k]);
-                const float4 a = __ldg(&anchor[cj]);
-                s_row[warp][k] = make_float4(a.x - ai.x, a.y - ai.y, a.z - ai.z,
-                    __int_as_float(cj * N));
+            const int ns = ne * N;
+            if (c > 0) {
+                rw0 = lane < ne ? __ldg(&row[c * CH + lane]) : 0;
+                rw1 = (CH > 32 && lane + 32 < ne) ? __ldg(&row[c * CH + lane + 32]) : 0;
+                ncode = pcnt[(size_t)(2 * ci + h) * chmax + c];
+#pragma unroll
+                for (int m = 0; m < PAIR_BATCH; m++)
+                    cw[m] = mycode[c * 256 + s + 16 * m];
+            }
+            if (lane < ne) {
+                const float4 a = __ldg(&anchor[rw0]);
+                s_row[warp][lane] = make_float4(a.x - ai.x, a.y - ai.y, a.z - ai.z,
+                    __int_as_float(rw0 * N));
+            }
+            if (CH > 32 && lane + 32 < ne) {
+                const float4 a = __ldg(&anchor[rw1]);
+                s_row[warp][lane + 32] = make_float4(a.x - ai.x, a.y - ai.y, a.z - ai.z,
+                    __int_as_float(rw1 * N));
             }
             __syncwarp();
-            // codes and counts always come from a derivation on the current
-            // rows; the clamps keep every access inside this chunk regardless
-            const int ns               = ne * N;
-            const int ncode            = min((int)pcnt[(size_t)(2 * ci + h) * chmax + c], ns);
-            const unsigned char* codes = pcode + ((size_t)(2 * ci + h) * chmax + c) * 256;
-            for (int k = s; k < ncode; k += 16) {
-                const int q = codes[k];
-                if (q >= ns) continue;
-                const float4 d = s_row[warp][q >> LOGN];
-                const int sj   = __float_as_int(d.w) + (q & (N - 1));
-                float4 xj      = __ldg(&xr[sj]);
-                // into the i frame: the same roundings as the cluster-pair kernel
-                const f2 jxy = f2_add(f2_pack(xj.x, xj.y), f2_pack(d.x, d.y));
-                f2_unpack(jxy, xj.x, xj.y);
-                xj.z += d.z;
-                unsigned ex = 0;
-                if (c == 0 && diag0 && q < N) ex = (xtab >> (2 * q)) & 3u;
-                const f2 DX  = f2_sub(XI, f2_pack(xj.x, xj.x));
-                const f2 DY  = f2_sub(YI, f2_pack(xj.y, xj.y));
-                const f2 DZ  = f2_sub(ZI, f2_pack(xj.z, xj.z));
-                const f2 RSQ = f2_fma(DX, DX, f2_fma(DY, DY, f2_mul(DZ, DZ)));
-                float r0, r1;
-                f2_unpack(RSQ, r0, r1);
-                const bool in0 = r0 < cutforcesq && !(ex & 1u);
-                const bool in1 = r1 < cutforcesq && !(ex & 2u);
-                float u0 = rcp_approx(r0), u1 = rcp_approx(r1);
-                u0          = in0 ? u0 : 0.0f;
-                u1          = in1 ? u1 : 0.0f;
-                const f2 U  = f2_pack(u0, u1);
-                const f2 U2 = f2_mul(U, U);
-                const f2 U3 = f2_mul(U2, U);
-                f2 F;
-                float4 ta = make_float4(0.f, 0.f, 0.f, 0.f), tb = ta;
-                if (UNIFORM) {
-                    F = f2_mul(f2_mul(U2, U2), f2_fma(A2, U3, mB2));
-                } else {
-                    int tj = __float_as_int(xj.w);
-                    tj     = tj < 0 ? 0 : tj;
-                    ta     = s_tab[t0 * MDB_MAX_TYPES + tj];
-                    tb     = s_tab[t1 * MDB_MAX_TYPES + tj];
-                    F = f2_mul(f2_mul(U2, U2),
-                        f2_fma(f2_pack(ta.x, tb.x), U3, f2_pack(-ta.y, -tb.y)));
+            // codes and counts come from a derivation on the current rows;
+            // the clamps keep every access inside this chunk regardless
+            ncode = min(ncode, ns);
+            for (int base = 0; base < ncode; base += 16 * PAIR_BATCH) {
+                if (base > 0) {
+#pragma unroll
+                    for (int m = 0; m < PAIR_BATCH; m++) {
+                        const int k = base + s + 16 * m;
+                        cw[m]       = k < ncode ? mycode[c * 256 + k] : 0;
+                    }
                 }
-                fx = f2_fma(DX, F, fx);
-                fy = f2_fma(DY, F, fy);
-                fz = f2_fma(DZ, F, fz);
-                if (HALF && sj < nloc) {
-                    float gx0, gx1, gy0, gy1, gz0, gz1;
-                    f2_unpack(f2_mul(DX, F), gx0, gx1);
-                    f2_unpack(f2_mul(DY, F), gy0, gy1);
-                    f2_unpack(f2_mul(DZ, F), gz0, gz1);
-                    red_add4(&cf32[sj], -(gx0 + gx1), -(gy0 + gy1), -(gz0 + gz1));
+                float4 xj[PAIR_BATCH], dj[PAIR_BATCH];
+                bool ok[PAIR_BATCH];
+#pragma unroll
+                for (int m = 0; m < PAIR_BATCH; m++) {
+                    ok[m] = base + s + 16 * m < ncode && cw[m] < ns;
+                    dj[m] = s_row[warp][ok[m] ? cw[m] >> LOGN : 0];
                 }
-                if (ENERGY) {
-                    // full lists see every pair twice; half lists once,
-                    // except pairs with ghost atoms, which both owners list
-                    const double ew = (!HALF || sj >= nloc) ? 0.5 : 1.0;
-                    float s0, s1;
-                    f2_unpack(f2_mul(UNIFORM ? f2_pack(sig6u, sig6u) : f2_pack(ta.z, tb.z), U3),
-                        s0, s1);
-                    const double E0 = UNIFORM ? pt.eps0 : (double)ta.w;
-                    const double E1 = UNIFORM ? pt.eps0 : (double)tb.w;
-                    if (in0) e += ew * 4.0 * E0 * (double)s0 * ((double)s0 - 1.0);
-                    if (in1) e += ew * 4.0 * E1 * (double)s1 * ((double)s1 - 1.0);
+#pragma unroll
+                for (int m = 0; m < PAIR_BATCH; m++)
+                    if (ok[m]) xj[m] = __ldg(&xr[__float_as_int(dj[m].w) + (cw[m] & (N - 1))]);
+#pragma unroll
+                for (int m = 0; m < PAIR_BATCH; m++) {
+                    if (!ok[m]) continue;
+                    const int q  = cw[m];
+                    const int sj = __float_as_int(dj[m].w) + (q & (N - 1));
+                    // into the i frame: the same roundings as the cluster-pair kernel
+                    float4 x     = xj[m];
+                    const f2 jxy = f2_add(f2_pack(x.x, x.y), f2_pack(dj[m].x, dj[m].y));
+                    f2_unpack(jxy, x.x, x.y);
+                    x.z += dj[m].z;
+                    const unsigned ex = (c == 0 && diag0 && q < N) ? (xtab >> (2 * q)) & 3u : 0u;
+                    pair2<HALF, ENERGY, UNIFORM>(XI, YI, ZI, x, sj, ex, t0, t1, s_tab, pt,
+                        cutforcesq, A2, mB2, nloc, fx, fy, fz, cf32, e);
                 }
             }
             __syncwarp();
@@ -297,6 +378,19 @@ __global__ void __launch_bounds__(PAIR_THREADS) k_force_pairs(const int* __restr
 
 int pair_grid(int ncl_cap) { return (int)(((long long)ncl_cap * 32 + PAIR_THREADS - 1) / PAIR_THREADS); }
 
+// one wave of resident derivation blocks (at most the clusters' own grid)
+static int derive_grid(int ncl_cap)
+{
+    static int nsm = 0;
+    if (!nsm) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (nsm < 1) nsm = 1;
+    }
+    return std::max(1, std::min(pair_grid(ncl_cap), nsm * (2048 / PAIR_THREADS)));
+}
+
 template <int N, bool HALF>
 static void derive_n(cudaStream_t s, int uniform, int grid, const int* cnt, const float4* xr,
     const float4* anchor, const int* list, int cs, const int* numneigh, float rin2, int* qflag,
@@ -315,7 +409,7 @@ void launch_pair_derive(cudaStream_t s, int N, int half, int uniform, int ncl_ca
     const int* numneigh, float rin2, int* qflag, int force, unsigned char* pcode,
     unsigned short* pcnt, int chmax, float4* xq)
 {
-    const int grid = pair_grid(ncl_cap);
+    const int grid = derive_grid(ncl_cap);
     if (N == 4) {
         if (half) derive_n<4, true>(s, uniform, grid, cnt, xr, anchor, list, cs, numneigh, rin2, qflag, force, pcode, pcnt, chmax, xq);
         else derive_n<4, false>(s, uniform, grid, cnt, xr, anchor, list, cs, numneigh, rin2, qflag, force, pcode, pcnt, chmax, xq);
@@ -326,49 +420,69 @@ void launch_pair_derive(cudaStream_t s, int N, int half, int uniform, int ncl_ca
     g_launches++;
 }
 
-template <int N, bool HALF, bool ENERGY>
-static void pairs_e(cudaStream_t s, int uniform, int grid, const int* cnt, const float4* xr,
+template <int N, bool HALF, bool ENERGY, bool UNIFORM>
+static void pairs_v(cudaStream_t s, int variant, int grid, const int* cnt, const float4* xr,
     const float4* anchor, const PairTypes& pt, float cutforcesq, const int* list, int cs,
     const int* numneigh, const unsigned char* pcode, const unsigned short* pcnt, int chmax,
     float4* cf32, double* epart, int* qflag)
 {
+#define PAIR_RUN(V)                                                                      \
+    k_force_pairs<N, HALF, ENERGY, UNIFORM, PAIR_VARIANTS[V][0], PAIR_VARIANTS[V][1]>      \
+        <<<grid, PAIR_THREADS, 0, s>>>(cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, \
+            pcode, pcnt, chmax, cf32, epart, qflag)
+    // energy evaluations (every nstat steps) use the default shape
+    switch (ENERGY ? 0 : variant) {
+    case 1: PAIR_RUN(1); break;
+    case 2: PAIR_RUN(2); break;
+    case 3: PAIR_RUN(3); break;
+    default: PAIR_RUN(0); break;
+    }
+#undef PAIR_RUN
+}
+
+template <int N, bool HALF, bool ENERGY>
+static void pairs_e(cudaStream_t s, int uniform, int variant, int grid, const int* cnt,
+    const float4* xr, const float4* anchor, const PairTypes& pt, float cutforcesq,
+    const int* list, int cs, const int* numneigh, const unsigned char* pcode,
+    const unsigned short* pcnt, int chmax, float4* cf32, double* epart, int* qflag)
+{
     if (uniform)
-        k_force_pairs<N, HALF, ENERGY, true><<<grid, PAIR_THREADS, 0, s>>>(cnt, xr, anchor, pt,
-            cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+        pairs_v<N, HALF, ENERGY, true>(s, variant, grid, cnt, xr, anchor, pt, cutforcesq, list,
+            cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
     else
-        k_force_pairs<N, HALF, ENERGY, false><<<grid, PAIR_THREADS, 0, s>>>(cnt, xr, anchor, pt,
-            cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+        pairs_v<N, HALF, ENERGY, false>(s, variant, grid, cnt, xr, anchor, pt, cutforcesq, list,
+            cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
 }
 
 template <int N>
-static void pairs_n(cudaStream_t s, int half, int energy, int uniform, int grid,
+static void pairs_n(cudaStream_t s, int half, int energy, int uniform, int variant, int grid,
     const int* cnt, const float4* xr, const float4* anchor, const PairTypes& pt,
     float cutforcesq, const int* list, int cs, const int* numneigh,
     const unsigned char* pcode, const unsigned short* pcnt, int chmax, float4* cf32,
     double* epart, int* qflag)
 {
     if (half) {
-        if (energy) pairs_e<N, true, true>(s, uniform, grid, cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
-        else pairs_e<N, true, false>(s, uniform, grid, cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+        if (energy) pairs_e<N, true, true>(s, uniform, variant, grid, cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+        else pairs_e<N, true, false>(s, uniform, variant, grid, cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
     } else {
-        if (energy) pairs_e<N, false, true>(s, uniform, grid, cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
-        else pairs_e<N, false, false>(s, uniform, grid, cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+        if (energy) pairs_e<N, false, true>(s, uniform, variant, grid, cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+        else pairs_e<N, false, false>(s, uniform, variant, grid, cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
     }
 }
 
-int launch_force_pairs(cudaStream_t s, int N, int half, int energy, int uniform, int ncl_cap,
-    const int* cnt, const float4* xr, const float4* anchor, const PairTypes& pt,
+int launch_force_pairs(cudaStream_t s, int N, int half, int energy, int uniform, int variant,
+    int ncl_cap, const int* cnt, const float4* xr, const float4* anchor, const PairTypes& pt,
     float cutforcesq, const int* list, int cs, const int* numneigh,
     const unsigned char* pcode, const unsigned short* pcnt, int chmax, float4* cf32,
     double* epart, int* qflag)
 {
     const int grid = pair_grid(ncl_cap);
     if (N == 4)
-        pairs_n<4>(s, half, energy, uniform, grid, cnt, xr, anchor, pt, cutforcesq, list, cs,
-            numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+        pairs_n<4>(s, half, energy, uniform, variant, grid, cnt, xr, anchor, pt, cutforcesq,
+            list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
     else
-        pairs_n<8>(s, half, energy, uniform, grid, cnt, xr, anchor, pt, cutforcesq, list, cs,
-            numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+        pairs_n<8>(s, half, energy, uniform, variant, grid, cnt, xr, anchor, pt, cutforcesq,
+            list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
     g_launches++;
     return grid;
 }

@@ -160,26 +160,56 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_fp64(int nlocal,
 }
 
 // ---- mixed ------------------------------------------------------------------
+// Four threads per atom: lane u * 8 + a of a warp takes atom a of the warp's 8
+// atoms and its list entries k = u, u + 4, u + 8, ... (one warp load of a
+// list row then reads 8 consecutive atoms: one full 32-byte sector), and two
+// shuffles combine the four partial sums. At 131k atoms a thread per atom
+// fills under half of the GPU's warp slots and leaves each SM few gathers in
+// flight; four per atom give 4x both.
+// The density pass also writes xe = (position, F'(rho)) of every local atom
+// and k_eam_xe_ghost that of every ghost, so the force pass gathers position
+// and F'(rho_j) of a neighbour in one 16-byte load.
+static constexpr int EAM_TPA = 4;
+
+__device__ __forceinline__ int eam_atom(int& u)
+{
+    const int lane = threadIdx.x & 31;
+    u              = lane >> 3;
+    return ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 8 + (lane & 7);
+}
+
+// the four partial sums of an atom (lanes a, a + 8, a + 16, a + 24)
+__device__ __forceinline__ double eam_combine(double v)
+{
+    v += __shfl_xor_sync(0xffffffffu, v, 8);
+    v += __shfl_xor_sync(0xffffffffu, v, 16);
+    return v;
+}
+
+int eam_mixed_blocks(int nlocal) { return mdb_blocks((long long)nlocal * EAM_TPA, EAM_THREADS); }
+
 template <bool ENERGY>
 __global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_mixed(int nlocal,
-    const int* __restrict__ order, const float4* __restrict__ xr, CellShift sh,
-    const int* __restrict__ numneigh, const int* __restrict__ neighbors, int ld,
-    float cutforcesq, EamDev e, double* __restrict__ fp, double* __restrict__ epart)
+    const float4* __restrict__ xr, CellShift sh, const int* __restrict__ numneigh,
+    const int* __restrict__ neighbors, int ld, float cutforcesq, EamDev e,
+    double* __restrict__ fp, float4* __restrict__ xe, double* __restrict__ epart)
 {
     const float cg = sh.g;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    double eng  = 0.0;
-    if (t < nlocal) {
-        const int i     = order ? order[t] : t;
-        const float4 pi = xr[i];
-        const int n     = numneigh[t];
-        const int* nb   = neighbors + t;
+    int u;
+    const int i    = eam_atom(u);
+    const bool act = i < nlocal;
+    double rhoi    = 0.0; // FP64 embedding (density) sum
+    double eng     = 0.0;
+    float4 pi      = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (act) {
+        pi              = xr[i];
+        const int n     = numneigh[i];
+        const int* nb   = neighbors + i;
         const float rdr = (float)e.rdr;
-        double rhoi     = 0.0; // FP64 embedding (density) sum
         auto pair       = [&](int en, const float4& pj) {
             float dx, dy, dz;
             cell_delta(pi, pj, (unsigned)en >> MDB_IDX_BITS, cg, dx, dy, dz);
-            float rsq        = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
+            float rsq = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
             if (rsq < cutforcesq) {
                 float p = __fmaf_rn(sqrtf(rsq), rdr, 1.0f);
                 int m   = (int)p;
@@ -192,32 +222,37 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_mixed(int nlocal,
                 rhoi += (double)__fmaf_rn(__fmaf_rn(__fmaf_rn(c.w, p, d.x), p, d.y), p, d.z);
             }
         };
-        int k = 0;
-        for (; k + EUNROLL <= n; k += EUNROLL) {
+        int k = u;
+        for (; k + EAM_TPA * (EUNROLL - 1) < n; k += EAM_TPA * EUNROLL) {
             int en[EUNROLL];
             float4 pj[EUNROLL];
 #pragma unroll
-            for (int u = 0; u < EUNROLL; u++)
-                en[u] = __ldcs(nb + (size_t)(k + u) * ld);
+            for (int v = 0; v < EUNROLL; v++)
+                en[v] = __ldcs(nb + (size_t)(k + EAM_TPA * v) * ld);
 #pragma unroll
-            for (int u = 0; u < EUNROLL; u++)
-                pj[u] = __ldg(xr + (en[u] & MDB_IDX_MASK));
+            for (int v = 0; v < EUNROLL; v++)
+                pj[v] = __ldg(xr + (en[v] & MDB_IDX_MASK));
 #pragma unroll
-            for (int u = 0; u < EUNROLL; u++)
-                pair(en[u], pj[u]);
+            for (int v = 0; v < EUNROLL; v++)
+                pair(en[v], pj[v]);
         }
-        for (; k < n; k++) {
+        for (; k < n; k += EAM_TPA) {
             int en = __ldcs(nb + (size_t)k * ld);
             pair(en, __ldg(xr + (en & MDB_IDX_MASK)));
         }
+    }
+    rhoi = eam_combine(rhoi);
+    if (act && u == 0) {
         double p = 1.0 * rhoi * e.rdrho + 1.0;
         int m    = (int)(p);
         m        = m < e.nrho - 1 ? m : e.nrho - 1;
         m        = m > 1 ? m : 1;
         p -= m;
-        p               = p < 1.0 ? p : 1.0;
-        const double* c = e.frho + 8 * m;
-        fp[i]           = (__ldg(c + 0) * p + __ldg(c + 1)) * p + __ldg(c + 2);
+        p                = p < 1.0 ? p : 1.0;
+        const double* c  = e.frho + 8 * m;
+        const double fpi = (__ldg(c + 0) * p + __ldg(c + 1)) * p + __ldg(c + 2);
+        fp[i]            = fpi;
+        xe[i]            = make_float4(pi.x, pi.y, pi.z, (float)fpi);
         if (ENERGY) eng = ((__ldg(c + 3) * p + __ldg(c + 4)) * p + __ldg(c + 5)) * p + __ldg(c + 6);
     }
     if (ENERGY) {
@@ -226,29 +261,57 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_mixed(int nlocal,
     }
 }
 
-template <bool ENERGY>
+// F'(rho) of the ghosts from their owners (the mid-step halo of
+// computeForceEam, verletlist/force_eam.c:120-130), with their positions
+__global__ void k_eam_xe_ghost(int nlocal, const float4* __restrict__ xr,
+    double* __restrict__ fp, float4* __restrict__ xe, const int* __restrict__ border_map,
+    const int* __restrict__ counters)
+{
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= counters[CNT_NGHOST]) return;
+    const double f   = fp[border_map[g]];
+    const float4 p   = xr[nlocal + g];
+    fp[nlocal + g]   = f;
+    xe[nlocal + g]   = make_float4(p.x, p.y, p.z, (float)f);
+}
+
+// COMP: Knuth two-sum compensated force sums (MDB_PREC_MIXED_COMP)
+template <bool ENERGY, bool COMP>
 __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_mixed(int nlocal,
-    const int* __restrict__ order, const float4* __restrict__ xr, CellShift sh,
-    const int* __restrict__ numneigh, const int* __restrict__ neighbors, int ld,
-    float cutforcesq, EamDev e, const double* __restrict__ fp, double* __restrict__ fx,
-    double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ epart)
+    const float4* __restrict__ xe, CellShift sh, const int* __restrict__ numneigh,
+    const int* __restrict__ neighbors, int ld, float cutforcesq, EamDev e,
+    double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
+    double* __restrict__ epart)
 {
     const float cg = sh.g;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    double eng  = 0.0;
-    if (t < nlocal) {
-        const int i     = order ? order[t] : t;
-        const float4 pi = xr[i];
-        const int n     = numneigh[t];
-        const int* nb   = neighbors + t;
-        const float fpi = (float)fp[i];
+    int u;
+    const int i    = eam_atom(u);
+    const bool act = i < nlocal;
+    double eng     = 0.0;
+    float fix = 0.f, fiy = 0.f, fiz = 0.f;
+    float cx = 0.f, cy = 0.f, cz = 0.f; // compensation terms
+    if (act) {
+        const float4 pi = xe[i];
+        const int n     = numneigh[i];
+        const int* nb   = neighbors + i;
+        const float fpi = pi.w;
         const float rdr = (float)e.rdr;
-        float fix = 0.f, fiy = 0.f, fiz = 0.f;
+        auto acc = [&](float& s, float& c, float d, float f) {
+            if (COMP) { // s + c carries the running sum exactly
+                float v  = d * f;
+                float w  = s + v;
+                float bp = w - s;
+                float r  = (s - (w - bp)) + (v - bp);
+                s        = w;
+                c += r;
+            } else {
+                s = __fmaf_rn(d, f, s);
+            }
+        };
         auto pair = [&](int en, const float4& pj) {
-            const int j      = en & MDB_IDX_MASK;
             float dx, dy, dz;
             cell_delta(pi, pj, (unsigned)en >> MDB_IDX_BITS, cg, dx, dy, dz);
-            float rsq        = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
+            float rsq = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
             if (rsq < cutforcesq) {
                 float r = sqrtf(rsq);
                 float p = __fmaf_rn(r, rdr, 1.0f);
@@ -265,36 +328,41 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_mixed(int nlocal,
                 float recip = __fdividef(1.0f, r);
                 float phi   = z2 * recip;
                 float phip  = __fmaf_rn(z2p, recip, -phi * recip);
-                float fpj   = (float)__ldg(fp + j);
-                float psip  = __fmaf_rn(fpi + fpj, rhoip, phip);
+                float psip  = __fmaf_rn(fpi + pj.w, rhoip, phip);
                 float fpair = -psip * recip;
-                fix         = __fmaf_rn(dx, fpair, fix);
-                fiy         = __fmaf_rn(dy, fpair, fiy);
-                fiz         = __fmaf_rn(dz, fpair, fiz);
+                acc(fix, cx, dx, fpair);
+                acc(fiy, cy, dy, fpair);
+                acc(fiz, cz, dz, fpair);
                 if (ENERGY) eng += 0.5 * (double)phi;
             }
         };
-        int k = 0;
-        for (; k + EUNROLL <= n; k += EUNROLL) {
+        int k = u;
+        for (; k + EAM_TPA * (EUNROLL - 1) < n; k += EAM_TPA * EUNROLL) {
             int en[EUNROLL];
             float4 pj[EUNROLL];
 #pragma unroll
-            for (int u = 0; u < EUNROLL; u++)
-                en[u] = __ldcs(nb + (size_t)(k + u) * ld);
+            for (int v = 0; v < EUNROLL; v++)
+                en[v] = __ldcs(nb + (size_t)(k + EAM_TPA * v) * ld);
 #pragma unroll
-            for (int u = 0; u < EUNROLL; u++)
-                pj[u] = __ldg(xr + (en[u] & MDB_IDX_MASK));
+            for (int v = 0; v < EUNROLL; v++)
+                pj[v] = __ldg(xe + (en[v] & MDB_IDX_MASK));
 #pragma unroll
-            for (int u = 0; u < EUNROLL; u++)
-                pair(en[u], pj[u]);
+            for (int v = 0; v < EUNROLL; v++)
+                pair(en[v], pj[v]);
         }
-        for (; k < n; k++) {
+        for (; k < n; k += EAM_TPA) {
             int en = __ldcs(nb + (size_t)k * ld);
-            pair(en, __ldg(xr + (en & MDB_IDX_MASK)));
+            pair(en, __ldg(xe + (en & MDB_IDX_MASK)));
         }
-        fx[i] = (double)fix;
-        fy[i] = (double)fiy;
-        fz[i] = (double)fiz;
+    }
+    // the four partial sums combined in FP64
+    const double sx = eam_combine((double)fix + (double)cx);
+    const double sy = eam_combine((double)fiy + (double)cy);
+    const double sz = eam_combine((double)fiz + (double)cz);
+    if (act && u == 0) {
+        fx[i] = sx;
+        fy[i] = sy;
+        fz[i] = sz;
     }
     if (ENERGY) {
         double s = block_sum(eng);
@@ -335,28 +403,38 @@ void launch_eam_fp64(cudaStream_t s, int energy, int nlocal, int ghost_cap, cons
     g_launches++;
 }
 
-void launch_eam_mixed(cudaStream_t s, int energy, int nlocal, int ghost_cap, const int* order,
+int launch_eam_mixed(cudaStream_t s, int energy, int comp, int nlocal, int ghost_cap,
     const float4* xr, const CellShift& sh, const int* numneigh, const int* neighbors, int ld,
     float cutforcesq, EamDev eam, const int* border_map, const int* counters, double* fp,
-    double* fx, double* fy, double* fz, double* epart_rho, double* epart_pair)
+    float4* xe, double* fx, double* fy, double* fz, double* epart_rho, double* epart_pair)
 {
-    if (nlocal <= 0) return;
-    int nb = mdb_blocks(nlocal, EAM_THREADS);
+    if (nlocal <= 0) return 0;
+    const int nb = eam_mixed_blocks(nlocal);
     if (energy)
-        k_eam_rho_mixed<true><<<nb, EAM_THREADS, 0, s>>>(nlocal, order, xr, sh, numneigh,
-            neighbors, ld, cutforcesq, eam, fp, epart_rho);
+        k_eam_rho_mixed<true><<<nb, EAM_THREADS, 0, s>>>(nlocal, xr, sh, numneigh, neighbors,
+            ld, cutforcesq, eam, fp, xe, epart_rho);
     else
-        k_eam_rho_mixed<false><<<nb, EAM_THREADS, 0, s>>>(nlocal, order, xr, sh, numneigh,
-            neighbors, ld, cutforcesq, eam, fp, epart_rho);
+        k_eam_rho_mixed<false><<<nb, EAM_THREADS, 0, s>>>(nlocal, xr, sh, numneigh, neighbors,
+            ld, cutforcesq, eam, fp, xe, epart_rho);
     g_launches++;
-    fp_ghost(s, nlocal, ghost_cap, fp, border_map, counters);
-    if (energy)
-        k_eam_force_mixed<true><<<nb, EAM_THREADS, 0, s>>>(nlocal, order, xr, sh, numneigh,
-            neighbors, ld, cutforcesq, eam, fp, fx, fy, fz, epart_pair);
-    else
-        k_eam_force_mixed<false><<<nb, EAM_THREADS, 0, s>>>(nlocal, order, xr, sh, numneigh,
-            neighbors, ld, cutforcesq, eam, fp, fx, fy, fz, epart_pair);
+    if (ghost_cap > 0) {
+        k_eam_xe_ghost<<<mdb_blocks(ghost_cap, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(nlocal, xr,
+            fp, xe, border_map, counters);
+        g_launches++;
+    }
+#define EAM_FM(E, C)                                                                     \
+    k_eam_force_mixed<E, C><<<nb, EAM_THREADS, 0, s>>>(nlocal, xe, sh, numneigh, neighbors, ld, \
+        cutforcesq, eam, fx, fy, fz, epart_pair)
+    if (energy) {
+        if (comp) EAM_FM(true, true);
+        else EAM_FM(true, false);
+    } else {
+        if (comp) EAM_FM(false, true);
+        else EAM_FM(false, false);
+    }
+#undef EAM_FM
     g_launches++;
+    return nb;
 }
 
 } // namespace mdb

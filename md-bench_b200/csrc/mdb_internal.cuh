@@ -227,10 +227,14 @@ void launch_eam_fp64(cudaStream_t s, int energy, int nlocal, int ghost_cap, cons
     const double4* x, const int* numneigh, const int* neighbors, int ld, double cutforcesq,
     EamDev eam, const int* border_map, const int* counters, double* fp, double* fx,
     double* fy, double* fz, double* epart_rho, double* epart_pair);
-void launch_eam_mixed(cudaStream_t s, int energy, int nlocal, int ghost_cap, const int* order,
+// mixed EAM: four threads per atom; xe (nlocal + ghost_cap) receives
+// (position, F'(rho)) of every atom for the force pass; comp: two-sum
+// compensated force sums; returns the energy partials written per pass
+int launch_eam_mixed(cudaStream_t s, int energy, int comp, int nlocal, int ghost_cap,
     const float4* xr, const CellShift& sh, const int* numneigh, const int* neighbors, int ld,
     float cutforcesq, EamDev eam, const int* border_map, const int* counters, double* fp,
-    double* fx, double* fy, double* fz, double* epart_rho, double* epart_pair);
+    float4* xe, double* fx, double* fy, double* fz, double* epart_rho, double* epart_pair);
+int eam_mixed_blocks(int nlocal);
 
 // launches issued through these helpers by the calling host thread (per
 // thread, so that contexts driven from different threads count their own:

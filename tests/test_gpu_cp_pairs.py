@@ -115,9 +115,20 @@ def test_pair_path_no_pair_missed_over_a_hot_run(N, half):
         r, m = rel(fp, fc)
         assert r <= SUM_ORDER and m <= 20 * SUM_ORDER, (k, r, m)
     d1, codes = s.pair_stats()
-    # more derivations than the two rebuilds and the switches back would give
-    assert d1 - d0 > 10, (d0, d1)
-    assert codes > 0
+    assert d1 > d0 and codes > 0
+    # with a small buffer (limit 0.05 per atom) the integrator's test triggers
+    # derivations inside the rebuild period, and forces stay the same
+    s.set_pair_buffer(0.1)
+    s.run(1, first_step=done, max_samples=0)
+    d2, _ = s.pair_stats()
+    s.run(15, first_step=done + 1, max_samples=0)
+    d3, _ = s.pair_stats()
+    assert d3 - d2 >= 5, (d2, d3)
+    fp = valid_forces(s)
+    s.tune("force_path", 0)
+    s.compute_force()
+    r, m = rel(fp, valid_forces(s))
+    assert r <= SUM_ORDER and m <= 20 * SUM_ORDER, (r, m)
 
 
 @pytest.mark.parametrize("half", [0, 1])

@@ -276,6 +276,32 @@ def test_c3_eam_copper_against_oracle():
     s.close()
 
 
+@pytest.mark.parametrize("precision", ["mixed", "mixed_comp"])
+def test_c3_eam_copper_mixed_against_oracle(precision):
+    """The mixed EAM passes (four threads per atom, F'(rho) gathered with the
+    position) on the copper state after 100 FP64 steps, against the oracle's
+    FP64 forces on the same state: within the mixed path's budget."""
+    tab, hp, x, v, t = copper()
+    s = mdb.system_from_host(hp, len(t), eam=tab)
+    s.set_atoms(x, v, t)
+    s.setup()
+    s.run(100, max_samples=0)
+    xa, va, _, ta = s.atoms()
+    s.close()
+    o = O.Oracle(eam_file=EAM_FILE, force_field=1, from_file=1, xprd=hp.xprd, yprd=hp.yprd,
+                 zprd=hp.zprd)
+    o.set_atoms(xa, va, ta)
+    o.setup()
+    o.force()
+    m = mdb.system_from_host(hp, len(t), eam=tab, precision=precision)
+    m.set_atoms(xa, va, ta)
+    m.setup()
+    assert rel_rms(m.atoms()[2], o.atoms()[2]) <= MIXED_RMS
+    m.compute_force(energy=True)
+    assert m.thermo()["PE"] == pytest.approx(o.thermo()["PE"], rel=1e-6)
+    m.close()
+
+
 @pytest.mark.skipif(not O.ref_available(), reason="reference build absent")
 def test_c3_eam_copper_against_reference(tmp_path):
     """The reference itself (its own sources, strict FP64 build) reads the
