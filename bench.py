@@ -43,7 +43,7 @@ REF_CP = {shape: os.path.join(ROOT, "oracle", "_ref", f"MDBench-CP-{shape}")
           for shape in ("4x4", "4x8")}
 METRIC = "atom-steps/s, LJ+EAM mixed-FP32 vs FP64 on 1 B200 at stated force error"
 # headline workload: GROMACS-style 4x4 cluster pairs, half lists, mixed precision
-HEAD = {"kind": "cp44", "precision": "mixed", "half": 1}
+HEAD = {"kind": "cp44", "precision": "mixed", "half": 1, "path": 1}
 HEAD_WORKLOAD = f"lj-fcc-{LJ_CELLS}^3-clusterpair-4x4-half-mixed"
 
 
@@ -56,7 +56,8 @@ def parse():
     ap.add_argument("--no-variants", action="store_true", help="headline only")
     ap.add_argument("--profile", choices=[f"{k}_{p}{h}" for k in ("lj", "eam", "cp44", "cp48")
                                           for p in ("mixed", "fp64") for h in ("", "_half")]
-                    + ["c5_mixed", "c5_fp64", "c4_mixed", "stub"],
+                    + [f"{k}_mixed{h}_pairs" for k in ("cp44", "cp48") for h in ("", "_half")]
+                    + ["c5_mixed", "c5_mixed_pairs", "c5_fp64", "c4_mixed", "stub"],
                     help="run one variant only (W+K bench steps + force timing), for ncu")
     ap.add_argument("--cells", type=int, default=None, help="fcc cells per side (profiling)")
     ap.add_argument("--tune", default=None, help="key=value[,key=value] cluster-pair tuning")
@@ -205,33 +206,50 @@ def rel_force_err(a, b):
     return float(np.sqrt(np.mean(d * d)) / rms), float(d.max() / rms)
 
 
-def measure(torch, mdb, kind, precision, args, device, half=0, steps=None):
-    steps = steps or args.steps
+def make_system(mdb, kind, precision, args, device, half=0, path=0):
+    """A workload's context and initial state; path 1: the pair-list force path
+    of the mixed cluster-pair scheme."""
     if kind == "c5":
         import workloads as W
-        s, (x, v, t) = cp_workload(mdb, precision, device, args.cells or C5_CELLS, 1,
-                                   cluster_n=4, types=W.c5_types())
+        s, init = cp_workload(mdb, precision, device, args.cells or C5_CELLS, 1, cluster_n=4,
+                              types=W.c5_types())
     elif kind.startswith("cp"):
-        s, (x, v, t) = cp_workload(mdb, precision, device, args.cells, half,
-                                   cluster_n=int(kind[3]))
+        s, init = cp_workload(mdb, precision, device, args.cells, half, cluster_n=int(kind[3]))
     else:
         make = lj_workload if kind == "lj" else eam_workload
-        s, (x, v, t) = make(mdb, precision, device, args.cells, half)
+        s, init = make(mdb, precision, device, args.cells, half)
     if kind.startswith("c"):
+        if path:
+            s.tune("force_path", 1)
         for kv in (args.tune.split(",") if getattr(args, "tune", None) else []):
             k, val = kv.split("=")
             s.tune(k, int(val))
+    return s, init
+
+
+def measure(torch, mdb, kind, precision, args, device, half=0, steps=None, path=0):
+    steps = steps or args.steps
+    s, (x, v, t) = make_system(mdb, kind, precision, args, device, half, path)
     s.set_atoms(x, v, t)
     s.setup()
     th0 = s.thermo()
     nat = len(t)
     every = s.params.reneigh_every
+    d0 = s.pair_stats()[0] if path else 0
     secs, launches, samples, nsteps = time_run(torch, s, steps, args.warmup, every)
     mean_list = float(s.numneigh().mean())
-    return dict(system=s, natoms=nat, secs=secs, launches=launches, samples=samples,
-                nsteps=nsteps, th0=th0, mean_list=mean_list,
-                value=nat * every * steps / secs, ms_per_step=1e3 * secs / steps,
-                init=(x, v, t))
+    out = dict(system=s, natoms=nat, secs=secs, launches=launches, samples=samples,
+               nsteps=nsteps, th0=th0, mean_list=mean_list,
+               value=nat * every * steps / secs, ms_per_step=1e3 * secs / steps,
+               init=(x, v, t))
+    if path:
+        d1, codes = s.pair_stats()
+        # derivations of the pair codes during the warm-up and timed periods,
+        # and the pair slots the force kernel evaluates per atom
+        out["pair_stats"] = {"pair_derivations": d1 - d0,
+                             "pair_md_steps": (args.warmup + steps) * every,
+                             "pair_slots_per_atom": round(2.0 * codes / nat, 2)}
+    return out
 
 
 def stub_bench(torch, mdb, device, natoms=STUB_ATOMS, nneighs=76, reps=20):
@@ -252,7 +270,10 @@ def stub_bench(torch, mdb, device, natoms=STUB_ATOMS, nneighs=76, reps=20):
         out[pattern] = {"atom_updates_per_s": natoms / secs,
                         "ns_per_neighbor": secs / (natoms * nneighs) * 1e9,
                         "force_us": secs * 1e6,
-                        "gather_gb_per_s": natoms * bytes_per_atom / secs / 1e9}
+                        # list entries plus gathered positions per second: the
+                        # positions (32 MB) are served from L2/L1, not HBM, so
+                        # this is no HBM roofline figure
+                        "cache_served_gather_gb_per_s": natoms * bytes_per_atom / secs / 1e9}
     return {"natoms": natoms, "nneighs": nneighs, "precision": "fp64", "list": "full",
             "patterns": out}
 
@@ -558,15 +579,50 @@ def cp_flops_per_atom(pc, half):
     return pc / 2 * 27 if half else pc * 24
 
 
-def drift(m):
-    e = [m["th0"]["E"]] + [q["E"] for q in m["samples"]]
-    return float((e[-1] - e[0]) / abs(e[0]))
+# the fixed window of the energy-drift comparison (MD steps; the multi-type
+# liquid runs its configuration's 500)
+DRIFT_STEPS = 1000
 
 
-def force_compare(mix, f64, kind):
-    """Mixed force against FP64 on the FP64 run's final state (both systems get
-    the same atoms and rebuild)."""
-    sm, sf = mix["system"], f64["system"]
+def _variant_spec():
+    """key -> (kind, precision, half lists, force path) of every variant in the
+    line; force path 1 is the pair-list kernel of the mixed cluster-pair scheme."""
+    spec = {}
+    for kind in ("cp44", "cp48"):
+        for half in (0, 1):
+            h = "_half" if half else ""
+            spec[f"{kind}_mixed{h}"] = (kind, "mixed", half, 0)
+            spec[f"{kind}_mixed{h}_pairs"] = (kind, "mixed", half, 1)
+            spec[f"{kind}_fp64{h}"] = (kind, "fp64", half, 0)
+    for prec in ("mixed", "fp64"):
+        spec[f"vl_{prec}"] = ("lj", prec, 0, 0)
+        spec[f"eam_{prec}"] = ("eam", prec, 0, 0)
+        spec[f"c5_{prec}"] = ("c5", prec, 1, 0)
+    spec["c5_mixed_pairs"] = ("c5", "mixed", 1, 1)
+    return spec
+
+
+VARIANT_SPEC = _variant_spec()
+# the FP64 variant each mixed one is compared with
+FP64_TWIN = {k: k.replace("_mixed", "_fp64").replace("_pairs", "")
+             for k in VARIANT_SPEC if "_mixed" in k}
+
+
+def drift_window(mdb, kind, precision, args, device, half=0, path=0, md_steps=DRIFT_STEPS):
+    """Total-energy drift (E_end - E_0) / |E_0| over md_steps MD steps from the
+    workload's initial state, whatever --steps is; returns the system at the
+    window's end with it."""
+    s, (x, v, t) = make_system(mdb, kind, precision, args, device, half, path)
+    s.set_atoms(x, v, t)
+    s.setup()
+    e0 = s.thermo()["E"]
+    e1 = s.run(md_steps)[-1]["E"]
+    return s, float((e1 - e0) / abs(e0))
+
+
+def force_compare(sm, sf, kind):
+    """Mixed force against FP64 on the FP64 system's current state (both systems
+    get the same atoms and rebuild)."""
     if kind.startswith("c"):
         x, v, t = sf.atoms()
         for s in (sf, sm):
@@ -624,8 +680,9 @@ def main():
         return
     if args.profile:
         kind, prec = args.profile.split("_")[:2]
-        half = 1 if args.profile.endswith("_half") else 0
-        m = measure(torch, mdb, kind, prec, args, local, half)
+        half = 1 if "_half" in args.profile or kind == "c5" else 0
+        path = 1 if args.profile.endswith("_pairs") else 0
+        m = measure(torch, mdb, kind, prec, args, local, half, path=path)
         kt = force_kernel_time(torch, m["system"], reps=3)
         print(json.dumps({"profile": args.profile, "natoms": m["natoms"],
                           "value": m["value"], "ms_per_step": m["ms_per_step"],
@@ -636,7 +693,8 @@ def main():
     # headline: the cluster-pair scheme on LJ 1M atoms, mixed precision
     barrier()
     clk = Clocks(local)
-    head = measure(torch, mdb, HEAD["kind"], HEAD["precision"], args, local, HEAD["half"])
+    head = measure(torch, mdb, HEAD["kind"], HEAD["precision"], args, local, HEAD["half"],
+                   path=HEAD["path"])
     clocks = clk.stop()
     secs = reduce_scalar(torch, dist, head["secs"], "max", "cuda")
     value = head["natoms"] * 20 * args.steps * world / secs
@@ -649,27 +707,37 @@ def main():
     fpa = cp_flops_per_atom(pc, HEAD["half"])
     peak, src = fp32_peak()
     achieved = fpa * head["natoms"] / kt / 1e12
-    traffic = None
+    # DRAM bytes of one launch from the ncu capture recorded in profiles/ (not
+    # a counter of this run)
+    traffic, tsrc = None, None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    tkey = "cp_pairs_bytes_per_atom" if HEAD["path"] else "cp_head_bytes_per_atom"
     if os.path.exists(tpath):
         with open(tpath) as f:
             tj = json.load(f)
-        if "cp_head_bytes_per_atom" in tj:
-            traffic = tj["cp_head_bytes_per_atom"] * head["natoms"]
-    entries = float(s.numneigh().mean())
+        if tkey in tj:
+            traffic = tj[tkey] * head["natoms"]
+            tsrc = "profiles/traffic.json (ncu dram__bytes of one launch; not measured in this run)"
+    if HEAD["path"]:
+        # pair slots the pair-list kernel evaluates: two per listed j atom code
+        computed = head["pair_stats"]["pair_slots_per_atom"]
+        kname = "k_force_pairs<4, %s> (cluster-pair pair list, uniform types)"
+    else:
+        computed = float(s.numneigh().mean()) * 4
+        kname = "k_force_mixed<4, %s> (cluster-pair, uniform types)"
+    credited = pc / 2 if HEAD["half"] else pc
     roof = {"bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak, 1),
             "unit": "TFLOP/s", "frac": round(achieved / peak, 4), "traffic": traffic,
-            "kernel": "k_force_mixed<4, %s> (cluster-pair, uniform types)"
-                      % ("half" if HEAD["half"] else "full"),
+            "traffic_source": tsrc,
+            "kernel": kname % ("half" if HEAD["half"] else "full"),
             "kernel_ms": round(kt * 1e3, 4), "pairs_in_cutoff_per_atom": round(pc, 2),
             "flops_per_atom": round(fpa, 1),
-            "computed_pairs_per_atom": round(entries * 4, 1),
-            # pairs credited above over the pair slots the list makes the kernel
-            # evaluate, and the rate with every such slot credited (the FP32
-            # pipe's view; the roofline fraction counts only in-cutoff pairs)
-            "cluster_efficiency": round((pc / 2 if HEAD["half"] else pc) / (entries * 4), 3),
-            "achieved_all_listed_pairs": round(
-                achieved * (entries * 4) / (pc / 2 if HEAD["half"] else pc), 3),
+            "computed_pairs_per_atom": round(computed, 1),
+            # pairs credited above over the pair slots the kernel evaluates,
+            # and the rate with every such slot credited (the FP32 pipe's view;
+            # the roofline fraction counts only in-cutoff pairs)
+            "cluster_efficiency": round(credited / computed, 3),
+            "achieved_all_computed_pairs": round(achieved * computed / credited, 3),
             "peak_source": src}
 
     extra = {}
@@ -677,52 +745,68 @@ def main():
     # no rank waits on them inside a collective
     if not args.no_variants and world == 1:
         runs = {}
-        for kind in ("cp44", "cp48"):
-            for half in (0, 1):
-                for prec in ("mixed", "fp64"):
-                    key = f"{kind}_{prec}{'_half' if half else ''}"
-                    if (kind, prec, half) == (HEAD["kind"], HEAD["precision"], HEAD["half"]):
-                        runs[key] = head
-                    else:
-                        runs[key] = measure(torch, mdb, kind, prec, args, local, half)
-        for kind in ("lj", "eam"):
-            for prec in ("mixed", "fp64"):
-                runs[f"{'vl' if kind == 'lj' else kind}_{prec}"] = measure(
-                    torch, mdb, kind, prec, args, local)
-        # multi-type liquid at 128^3 cells, 500 MD steps
-        for prec in ("mixed", "fp64"):
-            runs[f"c5_{prec}"] = measure(torch, mdb, "c5", prec, args, local, 1,
-                                         steps=max(args.steps // 2, 1))
+        for key, (kind, prec, half, path) in VARIANT_SPEC.items():
+            if (kind, prec, half, path) == (HEAD["kind"], HEAD["precision"], HEAD["half"],
+                                            HEAD["path"]):
+                runs[key] = head
+            else:
+                # the multi-type liquid (128^3 cells) times half as many periods
+                steps = max(args.steps // 2, 1) if kind == "c5" else None
+                runs[key] = measure(torch, mdb, kind, prec, args, local, half, steps, path)
         var = {}
         for key, m in runs.items():
             var[key] = {"value": m["value"], "ms_per_step": m["ms_per_step"],
-                        "natoms": m["natoms"], "energy_drift": drift(m),
-                        "md_steps": m["nsteps"], "mean_list": m["mean_list"]}
-        for key in list(runs):
-            if "_mixed" in key:
-                ref = key.replace("_mixed", "_fp64")
-                kind = key.split("_")[0]
-                rms, mx = force_compare(runs[key], runs[ref], kind)
-                var[key]["force_rms_rel_err"] = rms
-                var[key]["force_max_rel_err"] = mx
-                var[key]["excess_drift_vs_fp64"] = var[key]["energy_drift"] - var[ref]["energy_drift"]
+                        "natoms": m["natoms"], "md_steps_timed": m["nsteps"],
+                        "mean_list": m["mean_list"]}
+            if "pair_stats" in m:
+                var[key].update(m["pair_stats"])
         for m in runs.values():
             if m is not head:
                 m["system"].close()
+        # energy drift over a fixed window from the initial state, mixed and
+        # FP64 twins, and the mixed force error on the FP64 window's final state
+        spec = {k: v for k, v in VARIANT_SPEC.items() if k in runs}
+        f64_end = {}
+        for key, (kind, prec, half, path) in spec.items():
+            if prec != "fp64":
+                continue
+            n = 500 if kind == "c5" else DRIFT_STEPS
+            sf, d = drift_window(mdb, kind, prec, args, local, half, 0, n)
+            f64_end[key] = sf
+            var[key]["drift_window_md_steps"] = n
+            var[key]["energy_drift"] = d
+        for key, (kind, prec, half, path) in spec.items():
+            if prec == "fp64":
+                continue
+            ref = FP64_TWIN[key]
+            n = var[ref]["drift_window_md_steps"]
+            sm, d = drift_window(mdb, kind, prec, args, local, half, path, n)
+            var[key]["drift_window_md_steps"] = n
+            var[key]["energy_drift"] = d
+            var[key]["energy_drift_fp64"] = var[ref]["energy_drift"]
+            var[key]["excess_drift_vs_fp64"] = d - var[ref]["energy_drift"]
+            rms, mx = force_compare(sm, f64_end[ref], kind)
+            var[key]["force_rms_rel_err"] = rms
+            var[key]["force_max_rel_err"] = mx
+            var[key]["force_err_state"] = f"FP64 state after {n} MD steps"
+            sm.close()
+        for sf in f64_end.values():
+            sf.close()
         extra = {"variants": var,
                  "mixed_over_fp64": {k.replace("_mixed", ""): var[k]["value"] /
-                                     var[k.replace("_mixed", "_fp64")]["value"]
-                                     for k in var if "_mixed" in k}}
+                                     var[FP64_TWIN[k]]["value"] for k in var if k in FP64_TWIN},
+                 "drift_note": "energy_drift: (E - E0)/|E0| over the fixed window "
+                               "drift_window_md_steps from each workload's initial state; the "
+                               "reference's LJ and EAM potentials are not shifted at the "
+                               "cutoff, so the FP64 path itself drifts past 1e-4 per 1000 "
+                               "steps on these workloads; excess_drift_vs_fp64 is the mixed "
+                               "path's part"}
         var["c4_ensemble_mixed"] = c4_ensemble(torch, mdb, args, local)
         var["stub_gather_fp64"] = stub_bench(torch, mdb, local)
 
     # end to end from the state the timed run reached (a liquid, as in use)
-    extra_sys = [cp_workload(mdb, HEAD["precision"], local, half=HEAD["half"])[0]
-                 for _ in range(E2E_INFLIGHT - 1)]
-    for es in extra_sys:
-        for kv in (args.tune.split(",") if getattr(args, "tune", None) else []):
-            k, val = kv.split("=")
-            es.tune(k, int(val))
+    extra_sys = [make_system(mdb, HEAD["kind"], HEAD["precision"], args, local, HEAD["half"],
+                             HEAD["path"])[0] for _ in range(E2E_INFLIGHT - 1)]
     e2 = e2e(torch, [s] + extra_sys, s.atoms(), max(args.steps // 4, 4 * E2E_INFLIGHT), 20,
              local)
     for es in extra_sys:
@@ -739,6 +823,9 @@ def main():
                            "natoms_per_gpu": head["natoms"], "md_steps_per_bench_step": 20,
                            "rebuild_every": 20, "thermo_every": 100, "density": 0.8442,
                            "cutoff": 2.5, "skin": 0.3, "cluster": "4x4",
+                           "force_path": "pair list (listed cluster pairs' pairs within "
+                                         "r_c + skin, re-derived when an atom moves past "
+                                         "skin / 2)" if HEAD["path"] else "cluster pair",
                            "lists": "half" if HEAD["half"] else "full",
                            "l2": "inputs larger than L2 (cluster list %.0f MB, "
                                  "positions and velocities %.0f MB)"

@@ -174,6 +174,31 @@ int mdb_setup(MdbCtx* ctx);
 int mdb_run(MdbCtx* ctx, int first_step, int nsteps, MdbThermo* samples, int max_samples,
     int* nsamples);
 
+/* ---- domain decomposition ----------------------------------------------------
+ * The reference's MPI halo (forward(), common/shell_methods.h:28-54, with
+ * ghostNeighbor/exchangeComm of common/comm.c:233-631) as building blocks for
+ * a caller that splits the box into slabs over GPUs and moves the halo with
+ * its own transport (NCCL, gloo, device copies): the context holds the
+ * domain's own atoms first and then the halo atoms received from the
+ * neighbouring domains, already shifted into this domain's periodic frame.
+ * Halo atoms are binned, listed and imaged by the periodic directions like
+ * owned atoms but get no force row, no integration and no thermo; the caller
+ * refreshes their positions before every force evaluation and runs the
+ * per-step hooks (mdb_run refuses a context with halo atoms). Full lists and
+ * LJ only: half lists would need the reverse force exchange and EAM the
+ * mid-step F'(rho) exchange. */
+/* Atoms [nown, nlocal) of the last mdb_set_atoms are halo atoms (nown =
+ * nlocal: none); mdb_set_atoms resets it. */
+int mdb_set_owned(MdbCtx* ctx, int nown);
+/* Device AoS triples d_out[3k..3k+2] = position of atom d_idx[k] + shift,
+ * k < n (the positions another domain receives as its halo). Asynchronous on
+ * the context's stream. */
+int mdb_gather_positions(MdbCtx* ctx, const int* d_idx, int n, double shift_x,
+    double shift_y, double shift_z, double* d_out);
+/* The halo atoms' positions from device AoS triples (n = nlocal - nown).
+ * Asynchronous on the context's stream; follow with mdb_update_pbc. */
+int mdb_set_halo_positions(MdbCtx* ctx, const double* d_x, int n);
+
 /* ---- allocation-free entry point -------------------------------------------
  * No counterpart in the reference. For callers that keep their own device
  * arrays and cannot let a library allocate device memory (a framework whose

@@ -26,8 +26,10 @@ struct MdbCtx {
     std::string err;
     long long launches = 0;
 
-    // sizes
-    int nlocal = 0, ntypes = 1;
+    // sizes; atoms [nown, nlocal) are halo copies from neighbouring domains
+    // (binned, imaged and listed, but without force row, integration or
+    // thermo); nown = 0: every atom is owned
+    int nlocal = 0, ntypes = 1, nown = 0;
     int ghost_cap = 0, nall_cap = 0;
     int maxneighs = 100, ld = 0;
     bool have_atoms = false, have_list = false, have_ghosts = false, mixed = false;
@@ -118,6 +120,9 @@ template <typename T> static void dfree(T*& p)
     if (p) cudaFree(p);
     p = nullptr;
 }
+
+// atoms this context integrates and computes forces for
+static int owned(const MdbCtx* ctx) { return ctx->nown > 0 ? ctx->nown : ctx->nlocal; }
 
 static void destroy_graph(Graph& g)
 {
@@ -532,7 +537,8 @@ extern "C" int mdb_set_atoms(MdbCtx* ctx, int nlocal, const double* x, const dou
 {
     if (!ctx || nlocal < 0 || (nlocal > 0 && (!x || !v || !type))) return MDB_ERR_ARG;
     CK(cudaSetDevice(ctx->dev));
-    int maxt = 0;
+    ctx->nown = 0; // new atoms: all owned until mdb_set_owned
+    int maxt  = 0;
     for (int i = 0; i < nlocal; i++) {
         if (type[i] < 0) return fail(ctx, MDB_ERR_ARG, "negative atom type");
         maxt = std::max(maxt, type[i] + 1);
@@ -632,21 +638,21 @@ extern "C" int mdb_get_atoms(MdbCtx* ctx, double* x, double* v, double* f, int* 
 // enqueue helpers (no host synchronisation; safe inside stream capture)
 static void enq_initial(MdbCtx* ctx)
 {
-    launch_initial_integrate(ctx->s, ctx->nlocal, ctx->p.dtforce, ctx->p.dt, ctx->x, ctx->vx,
+    launch_initial_integrate(ctx->s, owned(ctx), ctx->p.dtforce, ctx->p.dt, ctx->x, ctx->vx,
         ctx->vy, ctx->vz, ctx->fx, ctx->fy, ctx->fz, ctx->mixed ? ctx->xr : nullptr,
         ctx->qcell, ctx->cf);
 }
 
 static void enq_final(MdbCtx* ctx)
 {
-    launch_final_integrate(ctx->s, ctx->nlocal, ctx->p.dtforce, ctx->vx, ctx->vy, ctx->vz,
+    launch_final_integrate(ctx->s, owned(ctx), ctx->p.dtforce, ctx->vx, ctx->vy, ctx->vz,
         ctx->fx, ctx->fy, ctx->fz);
 }
 
 // finalIntegrate of the previous step fused with initialIntegrate of this one
 static void enq_final_initial(MdbCtx* ctx)
 {
-    launch_final_initial_integrate(ctx->s, ctx->nlocal, ctx->p.dtforce, ctx->p.dt, ctx->x,
+    launch_final_initial_integrate(ctx->s, owned(ctx), ctx->p.dtforce, ctx->p.dt, ctx->x,
         ctx->vx, ctx->vy, ctx->vz, ctx->fx, ctx->fy, ctx->fz, ctx->mixed ? ctx->xr : nullptr,
         ctx->qcell, ctx->cf);
 }
@@ -663,7 +669,7 @@ static void enq_ghost_update(MdbCtx* ctx)
 static void enq_force(MdbCtx* ctx, bool energy)
 {
     cudaStream_t s = ctx->s;
-    int n          = ctx->nlocal;
+    int n          = owned(ctx); // rows of the owned atoms (full lists with halos)
     double* ep0    = ctx->partials;
     double* ep1    = ctx->partials + ctx->npart;
     if (ctx->p.force_field == MDB_FF_EAM) {
@@ -996,15 +1002,15 @@ static void enq_thermo(MdbCtx* ctx, int slot, bool with_pe)
 {
     cudaStream_t s = ctx->s;
     double* r      = ctx->red + 4 * slot;
-    int nke        = ke_partial_blocks(ctx->nlocal);
-    launch_ke_partial(s, ctx->nlocal, ctx->vx, ctx->vy, ctx->vz, ctx->p.mass,
+    int nke        = ke_partial_blocks(owned(ctx));
+    launch_ke_partial(s, owned(ctx), ctx->vx, ctx->vy, ctx->vz, ctx->p.mass,
         ctx->partials + 2 * (size_t)ctx->npart);
     launch_reduce_partials(s, nke, ctx->partials + 2 * (size_t)ctx->npart, r + 0);
     if (with_pe) {
         // the mixed EAM passes write eam_mixed_blocks partials, the rest one
         // per block of the force kernels
-        int nf = ctx->p.force_field == MDB_FF_EAM && ctx->mixed ? eam_mixed_blocks(ctx->nlocal)
-                                                               : force_partial_blocks(ctx->nlocal);
+        int nf = ctx->p.force_field == MDB_FF_EAM && ctx->mixed ? eam_mixed_blocks(owned(ctx))
+                                                               : force_partial_blocks(owned(ctx));
         launch_reduce_partials(s, nf, ctx->partials, r + 1);
         if (ctx->p.force_field == MDB_FF_EAM)
             launch_reduce_partials(s, nf, ctx->partials + ctx->npart, r + 2);
@@ -1109,11 +1115,51 @@ extern "C" int mdb_set_resort(MdbCtx* ctx, int resort_every)
     return MDB_OK;
 }
 
+// ---- domain decomposition -------------------------------------------------------
+extern "C" int mdb_set_owned(MdbCtx* ctx, int nown)
+{
+    NEED_ATOMS();
+    if (nown < 1 || nown > ctx->nlocal) return fail(ctx, MDB_ERR_ARG, "owned count out of range");
+    if (nown < ctx->nlocal && (ctx->p.half_neigh || ctx->p.force_field != MDB_FF_LJ))
+        return fail(ctx, MDB_ERR_ARG, "halo atoms need full lists and LJ forces");
+    ctx->nown = nown == ctx->nlocal ? 0 : nown;
+    drop_graphs(ctx);
+    return MDB_OK;
+}
+
+extern "C" int mdb_gather_positions(MdbCtx* ctx, const int* d_idx, int n, double shift_x,
+    double shift_y, double shift_z, double* d_out)
+{
+    NEED_ATOMS();
+    if (n < 0 || (n > 0 && (!d_idx || !d_out))) return MDB_ERR_ARG;
+    long long m = launch_mark();
+    launch_gather_positions(ctx->s, n, d_idx, ctx->x, shift_x, shift_y, shift_z, d_out);
+    launch_account(ctx, m);
+    CK(cudaGetLastError());
+    return MDB_OK;
+}
+
+extern "C" int mdb_set_halo_positions(MdbCtx* ctx, const double* d_x, int n)
+{
+    NEED_ATOMS();
+    const int first = owned(ctx), nhalo = ctx->nown > 0 ? ctx->nlocal - ctx->nown : 0;
+    if (n != nhalo || (n > 0 && !d_x)) return fail(ctx, MDB_ERR_ARG, "halo size mismatch");
+    long long m = launch_mark();
+    launch_set_halo(ctx->s, first, n, d_x, ctx->x, ctx->mixed ? ctx->xr : nullptr, ctx->qcell,
+        ctx->cf);
+    launch_account(ctx, m);
+    CK(cudaGetLastError());
+    return MDB_OK;
+}
+
 extern "C" int mdb_run(MdbCtx* ctx, int first_step, int nsteps, MdbThermo* samples,
     int max_samples, int* nsamples)
 {
     NEED_ATOMS();
     if (!ctx->have_list) return fail(ctx, MDB_ERR_STATE, "mdb_setup not run");
+    if (ctx->nown > 0)
+        return fail(ctx, MDB_ERR_STATE,
+            "halo atoms are refreshed between steps by the caller: drive the steps by the hooks");
     if (nsteps < 0 || (max_samples > 0 && !samples)) return MDB_ERR_ARG;
     if (nsamples) *nsamples = 0;
     int nslot = 0;

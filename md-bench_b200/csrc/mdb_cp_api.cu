@@ -25,6 +25,9 @@ struct MdbCp {
     std::vector<double> eps_t, sig_t;
     int M = CP_M, N = 4, jfac = 1, prune_every = 1000;
     bool mixed = false;
+    // MDB_PREC_MIXED_COMP: the pair-list kernel with compensated sums and
+    // exact cutoff decisions, forces in the FP64 slots cf
+    bool comp = false;
     int dev        = 0;
     cudaStream_t s = nullptr;
     std::string err;
@@ -313,7 +316,9 @@ extern "C" int mdb_cp_tune(MdbCp* ctx, const char* key, int value)
         return MDB_OK;
     }
     if (!strcmp(key, "force_path")) {
-        if (value < 0 || value > 1 || (value == 1 && !ctx->mixed)) return MDB_ERR_ARG;
+        // compensated contexts run the pair-list kernel only
+        if (value < 0 || value > 1 || (value == 1 && !ctx->mixed) || (value == 0 && ctx->comp))
+            return MDB_ERR_ARG;
         drop_graph(ctx);
         ctx->force_path = value;
         return ensure_pairs(ctx);
@@ -423,10 +428,13 @@ extern "C" int mdb_cp_create(const MdbParams* params, int cluster_n, int prune_e
     ctx->prune_every = prune_every > 0 ? prune_every : 1000;
     ctx->N           = cluster_n;
     ctx->jfac        = cluster_n / CP_M;
-    ctx->mixed       = p.precision == MDB_PREC_MIXED;
+    ctx->mixed       = p.precision == MDB_PREC_MIXED || p.precision == MDB_PREC_MIXED_COMP;
+    ctx->comp        = p.precision == MDB_PREC_MIXED_COMP;
+    ctx->force_path  = ctx->comp ? 1 : 0;
     ctx->cutforcesq  = p.cutforce * p.cutforce;
     if ((cluster_n != 4 && cluster_n != 8) || p.force_field != MDB_FF_LJ ||
-        !(p.precision == MDB_PREC_FP64 || p.precision == MDB_PREC_MIXED) ||
+        !(p.precision == MDB_PREC_FP64 || p.precision == MDB_PREC_MIXED ||
+            p.precision == MDB_PREC_MIXED_COMP) ||
         !(p.xprd > 0 && p.yprd > 0 && p.zprd > 0) || !(p.cutforce > 0) ||
         !(p.cutneigh >= p.cutforce) || p.natoms < 1 || ctx->maxneighs > 12288) {
         rc = fail(ctx, MDB_ERR_ARG, "invalid parameters for the cluster-pair scheme");
@@ -897,11 +905,17 @@ static void enq_derive(MdbCp* ctx, int force)
 
 static int enq_force_pairs(MdbCp* ctx, bool energy)
 {
+    CompArgs ca;
+    if (ctx->comp) ca.cx = ctx->cx, ca.cf64 = ctx->cf, ca.cutsq = ctx->cutforcesq;
     return launch_force_pairs(ctx->s, ctx->N, ctx->p.half_neigh, energy, ctx->ty.uniform,
-        ctx->ty.pair_variant, ctx->ncl_cap, ctx->cnt, ctx->xr, ctx->anchor, ctx->pt, (float)ctx->cutforcesq, ctx->list,
-        lcs(ctx), ctx->numneigh, ctx->pcode, ctx->pcnt, ctx->pair_chmax, ctx->cf32,
-        ctx->partials, ctx->qflag);
+        ctx->ty.pair_variant, ctx->ncl_cap, ctx->cnt, ctx->xr, ctx->anchor, ctx->pt,
+        (float)ctx->cutforcesq, ctx->list, lcs(ctx), ctx->numneigh, ctx->pcode, ctx->pcnt,
+        ctx->pair_chmax, ctx->cf32, ctx->partials, ctx->qflag, ca);
 }
+
+// the FP32 force slots the integrator reads (null: it reads the FP64 slots,
+// as FP64 and compensated contexts keep their forces there)
+static float4* f32_slots(const MdbCp* ctx) { return ctx->mixed && !ctx->comp ? ctx->cf32 : nullptr; }
 
 // the integrator's test of the pair-list path: half the buffer, less a
 // margin for the FP32 rounding of the positions it compares
@@ -916,7 +930,9 @@ static void enq_force(MdbCp* ctx, bool energy)
     cudaStream_t s = ctx->s;
     const int nloc_slots = ctx->ncl_cap * ctx->M;
     if (pair_path(ctx)) {
-        if (ctx->p.half_neigh)
+        if (ctx->p.half_neigh && ctx->comp)
+            cudaMemsetAsync(ctx->cf, 0, sizeof(double4) * (size_t)nloc_slots, s);
+        else if (ctx->p.half_neigh)
             cudaMemsetAsync(ctx->cf32, 0, sizeof(float4) * (size_t)nloc_slots, s);
         enq_derive(ctx, 0);
         const int nb = enq_force_pairs(ctx, energy);
@@ -948,7 +964,7 @@ static void enq_initial(MdbCp* ctx)
 {
     const bool pq = pair_path(ctx);
     launch_cp_initial(ctx->s, ctx->M, ctx->N, ctx->ncl_cap, ctx->cnt, ctx->p.dtforce, ctx->p.dt,
-        ctx->cx, ctx->cv, ctx->cf, ctx->mixed ? ctx->cf32 : nullptr, ctx->anchor,
+        ctx->cx, ctx->cv, ctx->cf, f32_slots(ctx), ctx->anchor,
         ctx->mixed ? ctx->xr : nullptr, xr_mode(ctx), check_xb(ctx),
         ctx->disp_max * ctx->disp_max, ctx->dflag, pq ? ctx->xq : nullptr, pair_qlim2(ctx),
         pq ? ctx->qflag : nullptr);
@@ -957,14 +973,14 @@ static void enq_initial(MdbCp* ctx)
 static void enq_final(MdbCp* ctx)
 {
     launch_cp_final(ctx->s, ctx->M, ctx->ncl_cap, ctx->cnt, ctx->p.dtforce, ctx->cx, ctx->cv,
-        ctx->cf, ctx->mixed ? ctx->cf32 : nullptr);
+        ctx->cf, f32_slots(ctx));
 }
 
 static void enq_final_initial(MdbCp* ctx)
 {
     const bool pq = pair_path(ctx);
     launch_cp_final_initial(ctx->s, ctx->M, ctx->N, ctx->ncl_cap, ctx->cnt, ctx->p.dtforce,
-        ctx->p.dt, ctx->cx, ctx->cv, ctx->cf, ctx->mixed ? ctx->cf32 : nullptr, ctx->anchor,
+        ctx->p.dt, ctx->cx, ctx->cv, ctx->cf, f32_slots(ctx), ctx->anchor,
         ctx->mixed ? ctx->xr : nullptr, xr_mode(ctx), check_xb(ctx),
         ctx->disp_max * ctx->disp_max, ctx->dflag, pq ? ctx->xq : nullptr, pair_qlim2(ctx),
         pq ? ctx->qflag : nullptr);
@@ -1468,7 +1484,7 @@ extern "C" int mdb_cp_get_slots(MdbCp* ctx, double* x, double* v, double* f, int
     if ((rc = copy_back(ctx, hx, ctx->cx, nslots))) return rc;
     if (v && (rc = copy_back(ctx, hv, ctx->cv, std::min(nslots, nloc)))) return rc;
     if (f) {
-        if (ctx->mixed) rc = copy_back(ctx, hf32, ctx->cf32, std::min(nslots, nloc));
+        if (f32_slots(ctx)) rc = copy_back(ctx, hf32, ctx->cf32, std::min(nslots, nloc));
         else rc = copy_back(ctx, hf, ctx->cf, std::min(nslots, nloc));
         if (rc) return rc;
     }
@@ -1483,7 +1499,7 @@ extern "C" int mdb_cp_get_slots(MdbCp* ctx, double* x, double* v, double* f, int
         }
         if (s < nloc) {
             if (v) v[3 * s] = hv[s].x, v[3 * s + 1] = hv[s].y, v[3 * s + 2] = hv[s].z;
-            if (f && ctx->mixed)
+            if (f && f32_slots(ctx))
                 f[3 * s] = hf32[s].x, f[3 * s + 1] = hf32[s].y, f[3 * s + 2] = hf32[s].z;
             else if (f)
                 f[3 * s] = hf[s].x, f[3 * s + 1] = hf[s].y, f[3 * s + 2] = hf[s].z;

@@ -222,6 +222,13 @@ void launch_pair_derive(cudaStream_t s, int N, int half, int uniform, int ncl_ca
     const int* cnt, const float4* xr, const float4* anchor, const int* list, int cs,
     const int* numneigh, float rin2, int* qflag, int force, unsigned char* pcode,
     unsigned short* pcnt, int chmax, float4* xq);
+// MDB_PREC_MIXED_COMP: FP64 slot positions for the exact cutoff decision, the
+// FP64 force slots that receive the forces, FP64 r_c^2 (cf64 null: plain mixed)
+struct CompArgs {
+    const double4* cx = nullptr;
+    double4* cf64     = nullptr;
+    double cutsq      = 0.0;
+};
 // forces from the codes; clears qflag[0]; variant: launch shape (0..3);
 // returns the blocks launched (= energy partials written)
 int launch_force_pairs(cudaStream_t s, int N, int half, int energy, int uniform, int variant,
@@ -229,7 +236,7 @@ int launch_force_pairs(cudaStream_t s, int N, int half, int energy, int uniform,
     const int* cnt, const float4* xr, const float4* anchor, const PairTypes& pt,
     float cutforcesq, const int* list, int cs, const int* numneigh,
     const unsigned char* pcode, const unsigned short* pcnt, int chmax, float4* cf32,
-    double* epart, int* qflag);
+    double* epart, int* qflag, const CompArgs& ca = CompArgs());
 
 // ---- batched launches over the members of an ensemble -----------------------
 // One launch covers every member: block b of the launch runs block bmap[b].y

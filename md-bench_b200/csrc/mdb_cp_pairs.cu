@@ -67,11 +67,31 @@ __device__ __forceinline__ float4 i_atom(const float4* __restrict__ xr, int slot
 // ex (bit k: pair with i atom 2h + k excluded) as select masks. The j
 // position is already in the i frame. Half lists add the reaction on local j
 // atoms (summed over the pair) with one vector reduction.
-template <bool HALF, bool ENERGY, bool UNIFORM>
+// COMP (MDB_PREC_MIXED_COMP): a pair whose FP32 distance lies within an FP32
+// rounding margin of r_c is tested again in FP64 on the positions the FP64
+// path uses (cx, the same expression), so both paths take the same pairs; the
+// i sums carry two-sum compensation terms (c*) and half-list reactions go to
+// the FP64 force slots by FP64 atomics.
+struct CompState {
+    const double4* cx;
+    double cutsq;
+    int si0;  // slot of i atom 2h
+    f2 cx_, cy_, cz_;
+};
+
+__device__ __forceinline__ void two_sum2(f2& s, f2& c, const f2& v)
+{
+    const f2 t  = f2_add(s, v);
+    const f2 bp = f2_sub(t, s);
+    c           = f2_add(c, f2_add(f2_sub(s, f2_sub(t, bp)), f2_sub(v, bp)));
+    s           = t;
+}
+
+template <bool HALF, bool ENERGY, bool UNIFORM, bool COMP>
 __device__ __forceinline__ void pair2(const f2& XI, const f2& YI, const f2& ZI,
     const float4& xj, int sj, unsigned ex, int t0, int t1, const float4* s_tab,
     const PairTypes& pt, float cutforcesq, const f2& A2, const f2& mB2, int nloc, f2& fx,
-    f2& fy, f2& fz, float4* cf32, double& e)
+    f2& fy, f2& fz, float4* cf32, double4* cf64, CompState& cs, double& e)
 {
     const f2 DX  = f2_sub(XI, f2_pack(xj.x, xj.x));
     const f2 DY  = f2_sub(YI, f2_pack(xj.y, xj.y));
@@ -79,8 +99,26 @@ __device__ __forceinline__ void pair2(const f2& XI, const f2& YI, const f2& ZI,
     const f2 RSQ = f2_fma(DX, DX, f2_fma(DY, DY, f2_mul(DZ, DZ)));
     float r0, r1;
     f2_unpack(RSQ, r0, r1);
-    const bool in0 = r0 < cutforcesq && !(ex & 1u);
-    const bool in1 = r1 < cutforcesq && !(ex & 2u);
+    bool in0 = r0 < cutforcesq && !(ex & 1u);
+    bool in1 = r1 < cutforcesq && !(ex & 2u);
+    if (COMP) {
+        // FP32 distances are within ~1e-6 relative of the exact ones here
+        const float band = 1e-5f * cutforcesq;
+        const bool b0 = fabsf(r0 - cutforcesq) < band, b1 = fabsf(r1 - cutforcesq) < band;
+        if (b0 || b1) {
+            const double4 pj = cs.cx[sj];
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                if (!(k ? b1 : b0)) continue;
+                const double4 pi  = cs.cx[cs.si0 + k];
+                const double delx = pi.x - pj.x, dely = pi.y - pj.y, delz = pi.z - pj.z;
+                const double rsq  = delx * delx + dely * dely + delz * delz;
+                const bool in     = rsq < cs.cutsq && !((ex >> k) & 1u);
+                if (k) in1 = in;
+                else in0 = in;
+            }
+        }
+    }
     float u0 = rcp_approx(r0), u1 = rcp_approx(r1);
     u0          = in0 ? u0 : 0.0f;
     u1          = in1 ? u1 : 0.0f;
@@ -98,15 +136,31 @@ __device__ __forceinline__ void pair2(const f2& XI, const f2& YI, const f2& ZI,
         tb     = s_tab[t1 * MDB_MAX_TYPES + tj];
         F = f2_mul(f2_mul(U2, U2), f2_fma(f2_pack(ta.x, tb.x), U3, f2_pack(-ta.y, -tb.y)));
     }
-    fx = f2_fma(DX, F, fx);
-    fy = f2_fma(DY, F, fy);
-    fz = f2_fma(DZ, F, fz);
-    if (HALF && sj < nloc) {
-        float gx0, gx1, gy0, gy1, gz0, gz1;
-        f2_unpack(f2_mul(DX, F), gx0, gx1);
-        f2_unpack(f2_mul(DY, F), gy0, gy1);
-        f2_unpack(f2_mul(DZ, F), gz0, gz1);
-        red_add4(&cf32[sj], -(gx0 + gx1), -(gy0 + gy1), -(gz0 + gz1));
+    if (COMP) {
+        const f2 GX = f2_mul(DX, F), GY = f2_mul(DY, F), GZ = f2_mul(DZ, F);
+        two_sum2(fx, cs.cx_, GX);
+        two_sum2(fy, cs.cy_, GY);
+        two_sum2(fz, cs.cz_, GZ);
+        if (HALF && sj < nloc) {
+            float gx0, gx1, gy0, gy1, gz0, gz1;
+            f2_unpack(GX, gx0, gx1);
+            f2_unpack(GY, gy0, gy1);
+            f2_unpack(GZ, gz0, gz1);
+            atomicAdd(&cf64[sj].x, -((double)gx0 + (double)gx1));
+            atomicAdd(&cf64[sj].y, -((double)gy0 + (double)gy1));
+            atomicAdd(&cf64[sj].z, -((double)gz0 + (double)gz1));
+        }
+    } else {
+        fx = f2_fma(DX, F, fx);
+        fy = f2_fma(DY, F, fy);
+        fz = f2_fma(DZ, F, fz);
+        if (HALF && sj < nloc) {
+            float gx0, gx1, gy0, gy1, gz0, gz1;
+            f2_unpack(f2_mul(DX, F), gx0, gx1);
+            f2_unpack(f2_mul(DY, F), gy0, gy1);
+            f2_unpack(f2_mul(DZ, F), gz0, gz1);
+            red_add4(&cf32[sj], -(gx0 + gx1), -(gy0 + gy1), -(gz0 + gz1));
+        }
     }
     if (ENERGY) {
         // full lists see every pair twice; half lists once, except pairs
@@ -234,12 +288,13 @@ __global__ void __launch_bounds__(PAIR_THREADS) k_pair_derive(const int* __restr
 // PAIR_BATCH at a time with all their j loads in flight together. Thread 0
 // of block 0 clears the derivation flag (the derivation kernel of this
 // evaluation has completed before this kernel starts).
-template <int N, bool HALF, bool ENERGY, bool UNIFORM, int PAIR_BATCH, int MINB>
+template <int N, bool HALF, bool ENERGY, bool UNIFORM, int PAIR_BATCH, int MINB, bool COMP>
 __global__ void __launch_bounds__(PAIR_THREADS, MINB ? MINB : 1) k_force_pairs(const int* __restrict__ cnt,
     const float4* __restrict__ xr, const float4* __restrict__ anchor, PairTypes pt,
     float cutforcesq, const int* __restrict__ list, int cs, const int* __restrict__ numneigh,
     const unsigned char* __restrict__ pcode, const unsigned short* __restrict__ pcnt, int chmax,
-    float4* cf32, double* epart, int* qflag)
+    float4* cf32, double* epart, int* qflag, const double4* __restrict__ cx, double4* cf64,
+    double cutsq64)
 {
     constexpr int CH = PairChunk<N>::CH, LOGN = PairChunk<N>::LOGN;
     __shared__ float4 s_row[PAIR_WARPS][CH];
@@ -287,6 +342,9 @@ __global__ void __launch_bounds__(PAIR_THREADS, MINB ? MINB : 1) k_force_pairs(c
             }
         const f2 A2 = f2_pack(pt.a0, pt.a0), mB2 = f2_pack(-pt.b0, -pt.b0);
         f2 fx = 0, fy = 0, fz = 0;
+        CompState cst;
+        cst.cx = cx, cst.cutsq = cutsq64, cst.si0 = ci * 4 + 2 * h;
+        cst.cx_ = cst.cy_ = cst.cz_ = 0;
         const int nch    = (nn + CH - 1) / CH;
         const bool diag0 = nn > 0 && __shfl_sync(0xffffffffu, rw0, 0) == ci_cj0;
         for (int c = 0; c < nch; c++) {
@@ -343,11 +401,43 @@ __global__ void __launch_bounds__(PAIR_THREADS, MINB ? MINB : 1) k_force_pairs(c
                     f2_unpack(jxy, x.x, x.y);
                     x.z += dj[m].z;
                     const unsigned ex = (c == 0 && diag0 && q < N) ? (xtab >> (2 * q)) & 3u : 0u;
-                    pair2<HALF, ENERGY, UNIFORM>(XI, YI, ZI, x, sj, ex, t0, t1, s_tab, pt,
-                        cutforcesq, A2, mB2, nloc, fx, fy, fz, cf32, e);
+                    pair2<HALF, ENERGY, UNIFORM, COMP>(XI, YI, ZI, x, sj, ex, t0, t1, s_tab, pt,
+                        cutforcesq, A2, mB2, nloc, fx, fy, fz, cf32, cf64, cst, e);
                 }
             }
             __syncwarp();
+        }
+        if (COMP) {
+            // each lane's sum and compensation in FP64, reduced over the 16
+            // lanes of the pair in FP64
+            float a0, a1, b0, b1;
+            double d[6];
+            f2_unpack(fx, a0, a1);
+            f2_unpack(cst.cx_, b0, b1);
+            d[0] = (double)a0 + (double)b0, d[3] = (double)a1 + (double)b1;
+            f2_unpack(fy, a0, a1);
+            f2_unpack(cst.cy_, b0, b1);
+            d[1] = (double)a0 + (double)b0, d[4] = (double)a1 + (double)b1;
+            f2_unpack(fz, a0, a1);
+            f2_unpack(cst.cz_, b0, b1);
+            d[2] = (double)a0 + (double)b0, d[5] = (double)a1 + (double)b1;
+#pragma unroll
+            for (int o = 8; o > 0; o >>= 1)
+#pragma unroll
+                for (int k = 0; k < 6; k++)
+                    d[k] += __shfl_xor_sync(0xffffffffu, d[k], o);
+            if (s == 0) {
+                double4* dst = &cf64[ci * 4 + 2 * h];
+                if (HALF) {
+                    if (v0) atomicAdd(&dst[0].x, d[0]), atomicAdd(&dst[0].y, d[1]),
+                        atomicAdd(&dst[0].z, d[2]);
+                    if (v1) atomicAdd(&dst[1].x, d[3]), atomicAdd(&dst[1].y, d[4]),
+                        atomicAdd(&dst[1].z, d[5]);
+                } else {
+                    if (v0) dst[0] = make_double4(d[0], d[1], d[2], 0.0);
+                    if (v1) dst[1] = make_double4(d[3], d[4], d[5], 0.0);
+                }
+            }
         }
 #pragma unroll
         for (int o = 8; o > 0; o >>= 1) {
@@ -355,7 +445,7 @@ __global__ void __launch_bounds__(PAIR_THREADS, MINB ? MINB : 1) k_force_pairs(c
             fy = f2_add(fy, __shfl_xor_sync(0xffffffffu, fy, o));
             fz = f2_add(fz, __shfl_xor_sync(0xffffffffu, fz, o));
         }
-        if (s == 0) {
+        if (!COMP && s == 0) {
             float ax, bx, ay, by, az, bz;
             f2_unpack(fx, ax, bx);
             f2_unpack(fy, ay, by);
@@ -424,12 +514,18 @@ template <int N, bool HALF, bool ENERGY, bool UNIFORM>
 static void pairs_v(cudaStream_t s, int variant, int grid, const int* cnt, const float4* xr,
     const float4* anchor, const PairTypes& pt, float cutforcesq, const int* list, int cs,
     const int* numneigh, const unsigned char* pcode, const unsigned short* pcnt, int chmax,
-    float4* cf32, double* epart, int* qflag)
+    float4* cf32, double* epart, int* qflag, const CompArgs& ca)
 {
+    if (ca.cf64) { // compensated: the default shape
+        k_force_pairs<N, HALF, ENERGY, UNIFORM, PAIR_VARIANTS[0][0], PAIR_VARIANTS[0][1], true>
+            <<<grid, PAIR_THREADS, 0, s>>>(cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh,
+                pcode, pcnt, chmax, cf32, epart, qflag, ca.cx, ca.cf64, ca.cutsq);
+        return;
+    }
 #define PAIR_RUN(V)                                                                      \
-    k_force_pairs<N, HALF, ENERGY, UNIFORM, PAIR_VARIANTS[V][0], PAIR_VARIANTS[V][1]>      \
+    k_force_pairs<N, HALF, ENERGY, UNIFORM, PAIR_VARIANTS[V][0], PAIR_VARIANTS[V][1], false> \
         <<<grid, PAIR_THREADS, 0, s>>>(cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, \
-            pcode, pcnt, chmax, cf32, epart, qflag)
+            pcode, pcnt, chmax, cf32, epart, qflag, nullptr, nullptr, 0.0)
     // energy evaluations (every nstat steps) use the default shape
     switch (ENERGY ? 0 : variant) {
     case 1: PAIR_RUN(1); break;
@@ -444,14 +540,15 @@ template <int N, bool HALF, bool ENERGY>
 static void pairs_e(cudaStream_t s, int uniform, int variant, int grid, const int* cnt,
     const float4* xr, const float4* anchor, const PairTypes& pt, float cutforcesq,
     const int* list, int cs, const int* numneigh, const unsigned char* pcode,
-    const unsigned short* pcnt, int chmax, float4* cf32, double* epart, int* qflag)
+    const unsigned short* pcnt, int chmax, float4* cf32, double* epart, int* qflag,
+    const CompArgs& ca)
 {
     if (uniform)
         pairs_v<N, HALF, ENERGY, true>(s, variant, grid, cnt, xr, anchor, pt, cutforcesq, list,
-            cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+            cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag, ca);
     else
         pairs_v<N, HALF, ENERGY, false>(s, variant, grid, cnt, xr, anchor, pt, cutforcesq, list,
-            cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+            cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag, ca);
 }
 
 template <int N>
@@ -459,14 +556,14 @@ static void pairs_n(cudaStream_t s, int half, int energy, int uniform, int varia
     const int* cnt, const float4* xr, const float4* anchor, const PairTypes& pt,
     float cutforcesq, const int* list, int cs, const int* numneigh,
     const unsigned char* pcode, const unsigned short* pcnt, int chmax, float4* cf32,
-    double* epart, int* qflag)
+    double* epart, int* qflag, const CompArgs& ca)
 {
     if (half) {
-        if (energy) pairs_e<N, true, true>(s, uniform, variant, grid, cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
-        else pairs_e<N, true, false>(s, uniform, variant, grid, cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+        if (energy) pairs_e<N, true, true>(s, uniform, variant, grid, cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag, ca);
+        else pairs_e<N, true, false>(s, uniform, variant, grid, cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag, ca);
     } else {
-        if (energy) pairs_e<N, false, true>(s, uniform, variant, grid, cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
-        else pairs_e<N, false, false>(s, uniform, variant, grid, cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+        if (energy) pairs_e<N, false, true>(s, uniform, variant, grid, cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag, ca);
+        else pairs_e<N, false, false>(s, uniform, variant, grid, cnt, xr, anchor, pt, cutforcesq, list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag, ca);
     }
 }
 
@@ -474,15 +571,15 @@ int launch_force_pairs(cudaStream_t s, int N, int half, int energy, int uniform,
     int ncl_cap, const int* cnt, const float4* xr, const float4* anchor, const PairTypes& pt,
     float cutforcesq, const int* list, int cs, const int* numneigh,
     const unsigned char* pcode, const unsigned short* pcnt, int chmax, float4* cf32,
-    double* epart, int* qflag)
+    double* epart, int* qflag, const CompArgs& ca)
 {
     const int grid = pair_grid(ncl_cap);
     if (N == 4)
         pairs_n<4>(s, half, energy, uniform, variant, grid, cnt, xr, anchor, pt, cutforcesq,
-            list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+            list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag, ca);
     else
         pairs_n<8>(s, half, energy, uniform, variant, grid, cnt, xr, anchor, pt, cutforcesq,
-            list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag);
+            list, cs, numneigh, pcode, pcnt, chmax, cf32, epart, qflag, ca);
     g_launches++;
     return grid;
 }

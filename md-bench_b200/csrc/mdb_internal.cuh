@@ -236,6 +236,14 @@ int launch_eam_mixed(cudaStream_t s, int energy, int comp, int nlocal, int ghost
     float4* xe, double* fx, double* fy, double* fz, double* epart_rho, double* epart_pair);
 int eam_mixed_blocks(int nlocal);
 
+// domain-decomposed runs: positions of atoms idx[0..n) plus a shift, AoS
+// triples (the halo another domain receives); and the positions of halo
+// atoms [first, first + n) from AoS triples (mixed: relative copies too)
+void launch_gather_positions(cudaStream_t s, int n, const int* idx, const double4* x, double sx,
+    double sy, double sz, double* out);
+void launch_set_halo(cudaStream_t s, int first, int n, const double* in, double4* x, float4* xr,
+    const int* qcell, const CellFrame& cf);
+
 // launches issued through these helpers by the calling host thread (per
 // thread, so that contexts driven from different threads count their own:
 // a context is used by one thread at a time)

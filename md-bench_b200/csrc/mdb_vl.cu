@@ -664,4 +664,52 @@ void launch_reduce_partials(cudaStream_t s, int nparts, const double* partials, 
     g_launches++;
 }
 
+// ---- halo atoms of a domain-decomposed run ------------------------------------
+// out[3k..3k+2] = position of atom idx[k] plus shift (the periodic image a
+// neighbouring domain sees across the global box boundary; one FP64 addition
+// per coordinate, as a ghost image is made)
+__global__ void k_gather_positions(int n, const int* __restrict__ idx,
+    const double4* __restrict__ x, double sx, double sy, double sz, double* __restrict__ out)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const double4 p = x[idx[k]];
+    out[3 * k]      = p.x + sx;
+    out[3 * k + 1]  = p.y + sy;
+    out[3 * k + 2]  = p.z + sz;
+}
+
+void launch_gather_positions(cudaStream_t s, int n, const int* idx, const double4* x, double sx,
+    double sy, double sz, double* out)
+{
+    if (n <= 0) return;
+    k_gather_positions<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(n, idx, x, sx, sy,
+        sz, out);
+    g_launches++;
+}
+
+// halo atoms [first, first + n) take positions from in (AoS triples); their
+// type bits stay; the mixed path's relative copy follows (cells fixed at the
+// last build, as for the atoms the integrator moves)
+__global__ void k_set_halo(int first, int n, const double* __restrict__ in, double4* x,
+    float4* xr, const int* __restrict__ qcell, CellFrame cf)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int i = first + k;
+    double4 p   = x[i];
+    p.x = in[3 * k], p.y = in[3 * k + 1], p.z = in[3 * k + 2];
+    x[i] = p;
+    if (xr) xr[i] = rel_position(p, qcell[i], cf);
+}
+
+void launch_set_halo(cudaStream_t s, int first, int n, const double* in, double4* x, float4* xr,
+    const int* qcell, const CellFrame& cf)
+{
+    if (n <= 0) return;
+    k_set_halo<<<mdb_blocks(n, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(first, n, in, x, xr, qcell,
+        cf);
+    g_launches++;
+}
+
 } // namespace mdb

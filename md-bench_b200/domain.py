@@ -1,0 +1,264 @@
+"""z-slab domain decomposition of the Verlet-list timestep over ranks.
+
+The reference runs one MPI rank per subdomain and moves atoms between them
+with a 6-swap halo (common/comm.c:233-631, driven by forward() and
+updateAtoms()/reneighbour() in verletlist/main.c:150-161, 115-135 and
+common/shell_methods.h:28-54). Here the box is cut into slabs along z, one per
+rank (one GPU each), periodic in x and y inside every rank. Per rebuild
+period:
+
+* at a rebuild step each rank wraps its atoms into the box, sends the atoms
+  that left its slab to the rank that now owns them (atoms move less than
+  the skin in a period, but any rank is reachable), and sends every owned
+  atom within cutneigh of a slab face to the neighbouring rank across it,
+  shifted by the box length where that face is the box boundary; the rank
+  then holds its owned atoms followed by that halo (``mdb_set_owned``) and
+  builds its ghosts (x, y images) and lists;
+* at every other step the same halo atoms' positions are sent again, after
+  the initial integration and before the force (``mdb_gather_positions`` /
+  ``mdb_set_halo_positions``).
+
+Full lists, so no reverse exchange: each rank computes the forces of its own
+atoms from owned and halo neighbours. Thermo sums are reduced over ranks.
+
+The exchange goes through a ``Transport``: ``DistTransport`` uses
+torch.distributed point-to-point calls (NCCL with device tensors between
+GPUs, gloo with host tensors on CPU); the driver itself (``SlabRun``) is the
+same for any engine with the small interface of ``MdbEngine``.
+"""
+import numpy as np
+
+
+class Slabs:
+    """Slab geometry: rank r owns z in [r * Lz / P, (r + 1) * Lz / P)."""
+
+    def __init__(self, box, cutneigh, world, rank):
+        self.box = np.asarray(box, dtype=np.float64)
+        self.cut = float(cutneigh)
+        self.world, self.rank = int(world), int(rank)
+        self.lz = self.box[2] / self.world
+        if self.world > 1 and self.lz < self.cut:
+            raise ValueError("slabs thinner than the neighbour cutoff")
+        self.zlo = self.rank * self.lz
+        self.zhi = self.box[2] if self.rank == self.world - 1 else (self.rank + 1) * self.lz
+
+    def owner(self, z):
+        """The rank owning each z (wrapped positions)."""
+        r = np.floor(np.asarray(z) / self.lz).astype(np.int64)
+        return np.clip(r, 0, self.world - 1)
+
+    def wrap(self, x):
+        """updateAtomsPbcCPU (verletlist/pbc.c:62-87): one box length back
+        into [0, L) per coordinate."""
+        x = np.array(x, dtype=np.float64, copy=True)
+        for d in range(3):
+            lo, hi = x[:, d] < 0.0, x[:, d] >= self.box[d]
+            x[lo, d] += self.box[d]
+            x[hi, d] -= self.box[d]
+        return x
+
+    def halo_plan(self, x):
+        """For each direction (below, above): (peer rank, indices of owned atoms
+        within cutneigh of that face, z shift into the peer's frame)."""
+        z = x[:, 2]
+        below = (self.rank - 1) % self.world
+        above = (self.rank + 1) % self.world
+        sdown = self.box[2] if self.rank == 0 else 0.0
+        sup = -self.box[2] if self.rank == self.world - 1 else 0.0
+        down = np.nonzero(z < self.zlo + self.cut)[0]
+        up = np.nonzero(z >= self.zhi - self.cut)[0]
+        return [(below, down, sdown), (above, up, sup)]
+
+
+class DistTransport:
+    """Neighbour exchange over torch.distributed point-to-point calls (NCCL
+    with device tensors, gloo with host tensors). Every exchange runs in two
+    phases, all ranks sending down and receiving from above, then sending up
+    and receiving from below, so each phase has one message per direction
+    between any two ranks and NCCL's in-order matching pairs them correctly
+    even when the ranks below and above are the same (two ranks)."""
+
+    def __init__(self, torch, dist, device):
+        self.torch, self.dist, self.device = torch, dist, device
+
+    def wrap(self, rows):
+        return self.torch.from_numpy(np.ascontiguousarray(rows)).to(self.device)
+
+    def to_host(self, t):
+        return t.cpu().numpy()
+
+    def _phase(self, dest, t, src, shape_rows):
+        torch, dist = self.torch, self.dist
+        r = torch.empty((shape_rows, t.shape[1]), dtype=t.dtype, device=self.device)
+        ops = [dist.P2POp(dist.isend, t.contiguous(), dest), dist.P2POp(dist.irecv, r, src)]
+        for q in dist.batch_isend_irecv(ops):
+            q.wait()
+        return r
+
+    def exchange(self, down, up, below, above, sizes=None):
+        """down / up: rows for the rank below / above. Returns (rows from below,
+        rows from above); sizes: their row counts when known (between rebuilds)."""
+        torch = self.torch
+        if sizes is None:
+            n = []
+            for dest, t, src in ((below, down, above), (above, up, below)):
+                c = torch.tensor([[t.shape[0]]], dtype=torch.int64, device=self.device)
+                n.append(int(self._phase(dest, c, src, 1).item()))
+            sizes = (n[1], n[0])
+        from_above = self._phase(below, down, above, sizes[1])
+        from_below = self._phase(above, up, below, sizes[0])
+        return from_below, from_above
+
+    def sum(self, values):
+        t = self.torch.tensor(values, dtype=self.torch.float64, device=self.device)
+        self.dist.all_reduce(t)
+        return t.tolist()
+
+
+class SlabRun:
+    """One rank of a slab-decomposed run. ``engine`` holds this rank's atoms
+    (see MdbEngine for the interface); atoms carry global ids so that results
+    can be compared with an undivided run."""
+
+    def __init__(self, slabs, transport, engine, reneigh_every=20):
+        self.sl, self.tr, self.eng = slabs, transport, engine
+        self.every = int(reneigh_every)
+        w, r = slabs.world, slabs.rank
+        self.below, self.above = (r - 1) % w, (r + 1) % w
+
+    def start(self, x, v, t, gid):
+        """Every rank passes the full initial state; each keeps its slab."""
+        x = self.sl.wrap(x)
+        mine = self.sl.owner(x[:, 2]) == self.sl.rank
+        self._load(x[mine], np.asarray(v)[mine], np.asarray(t)[mine], np.asarray(gid)[mine])
+
+    def _load(self, x, v, t, gid):
+        order = np.argsort(gid, kind="stable")
+        x, v, t, gid = x[order], v[order], t[order], gid[order]
+        self.gid = gid
+        (_, down, sdown), (_, up, sup) = self.sl.halo_plan(x)
+        # halo rows: position shifted into the receiver's frame, type, global id
+        def rows(idx, sz):
+            return np.column_stack([x[idx, 0], x[idx, 1], x[idx, 2] + sz,
+                                    t[idx].astype(np.float64), gid[idx].astype(np.float64)])
+        fb, fa = self.tr.exchange(self.tr.wrap(rows(down, sdown)), self.tr.wrap(rows(up, sup)),
+                                  self.below, self.above)
+        fb, fa = self.tr.to_host(fb), self.tr.to_host(fa)
+        halo = np.concatenate([fb, fa])
+        self.send = ((down, sdown), (up, sup))
+        self.nhalo = (len(fb), len(fa))
+        self.halo_gid = halo[:, 4].astype(np.int64)
+        self.eng.load(x, v, t, halo[:, :3], halo[:, 3].astype(np.int32))
+
+    def _migrate(self):
+        """updateAtoms + reneighbour (verletlist/main.c:115-161): wrap, hand the
+        atoms that left the slab to the neighbour that owns them, then a new
+        halo and new lists."""
+        x, v, t = self.eng.owned_state()
+        x = self.sl.wrap(x)
+        dest = self.sl.owner(x[:, 2])
+        stay = dest == self.sl.rank
+        go_down, go_up = dest == self.below, (dest == self.above) & (dest != self.below)
+        if not np.all(stay | go_down | go_up):
+            raise RuntimeError("an atom moved past a whole slab in one rebuild period")
+        rows = np.column_stack([x, v, t.astype(np.float64), self.gid.astype(np.float64)])
+        fb, fa = self.tr.exchange(self.tr.wrap(rows[go_down]), self.tr.wrap(rows[go_up]),
+                                  self.below, self.above)
+        got = np.concatenate([rows[stay], self.tr.to_host(fb), self.tr.to_host(fa)])
+        self._load(got[:, 0:3], got[:, 3:6], got[:, 6].astype(np.int32),
+                   got[:, 7].astype(np.int64))
+
+    def _forward(self):
+        """The halo's positions of this step (forward(),
+        common/shell_methods.h:28-54)."""
+        (down, sdown), (up, sup) = self.send
+        fb, fa = self.tr.exchange(self.eng.positions(down, sdown), self.eng.positions(up, sup),
+                                  self.below, self.above, sizes=self.nhalo)
+        self.eng.set_halo_positions([fb, fa])
+
+    def step(self, n):
+        """Timestep n as verletlist/main.c:383-407 runs it."""
+        self.eng.initial_integrate()
+        if (n + 1) % self.every == 0:
+            self._migrate()
+        else:
+            self._forward()
+        self.eng.force()
+        self.eng.final_integrate()
+
+    def run(self, nsteps, first_step=0):
+        for n in range(first_step, first_step + nsteps):
+            self.step(n)
+
+    def temperature(self, natoms):
+        """T over all ranks (computeThermo, common/thermo.c:60-100, LJ units)."""
+        ke = self.tr.sum([self.eng.kinetic()])[0]
+        return ke / (3 * natoms - 3)
+
+    def gather(self):
+        """(gid, x, v, f) of this rank's owned atoms."""
+        x, v, _ = self.eng.owned_state()
+        return self.gid, x, v, self.eng.owned_forces()
+
+
+class MdbEngine:
+    """A rank's atoms in a libmdb Verlet-list context (FP64 or mixed, full
+    lists): owned atoms, then the halo; halo positions move on the device."""
+
+    def __init__(self, torch, mdb, hp, device, precision="fp64"):
+        self.torch, self.mdb, self.hp = torch, mdb, hp
+        self.device, self.precision = device, precision
+        self.sys = None
+
+    def load(self, x, v, t, hx, ht):
+        torch, mdb = self.torch, self.mdb
+        n, nh = len(t), len(ht)
+        if self.sys is None:
+            # periodic in x and y only: z neighbours come as halo atoms
+            self.sys = mdb.system_from_host(self.hp, n + nh, precision=self.precision,
+                                            device=self.device, pbc_z=0, half_neigh=0)
+        xa = np.concatenate([x, hx]) if nh else x
+        va = np.concatenate([v, np.zeros((nh, 3))]) if nh else v
+        ta = np.concatenate([t, ht]).astype(np.int32) if nh else t.astype(np.int32)
+        self.sys.set_atoms(xa, va, ta)
+        self.sys.set_owned(n)
+        self.n, self.nh = n, nh
+        self.sys.setup_pbc()
+        self.sys.update_pbc()
+        self.sys.build_neighbor()
+        self.sys.compute_force()
+
+    def positions(self, idx, sz):
+        torch = self.torch
+        d_idx = torch.as_tensor(np.ascontiguousarray(idx, dtype=np.int32), device="cuda")
+        out = torch.empty((len(idx), 3), dtype=torch.float64, device="cuda")
+        self.sys.gather_positions(d_idx.data_ptr(), len(idx), (0.0, 0.0, sz), out.data_ptr())
+        self.sys.synchronize()
+        return out
+
+    def set_halo_positions(self, recv):
+        torch = self.torch
+        buf = torch.cat([r.to("cuda") for r in recv]).contiguous()
+        self.sys.set_halo_positions(buf.data_ptr(), buf.shape[0])
+        self.sys.update_pbc()
+        self.sys.synchronize()
+
+    def initial_integrate(self):
+        self.sys.initial_integrate()
+
+    def force(self):
+        self.sys.compute_force()
+
+    def final_integrate(self):
+        self.sys.final_integrate()
+
+    def owned_state(self):
+        x, v, _, t = self.sys.atoms()
+        return x[:self.n], v[:self.n], t[:self.n]
+
+    def owned_forces(self):
+        return self.sys.atoms()[2][:self.n]
+
+    def kinetic(self):
+        _, v, _ = self.owned_state()
+        return float(np.sum(v * v) * self.hp.mass)

@@ -83,6 +83,7 @@ EXPORTS = [
     "mdb_initial_integrate", "mdb_final_integrate", "mdb_thermo", "mdb_setup", "mdb_run", "mdb_get_counts",
     "mdb_get_positions_all", "mdb_get_ghosts", "mdb_get_neighbor_list",
     "mdb_get_bin_geometry", "mdb_get_eam_fp", "mdb_launch_count", "mdb_kinetic_sum_noalloc",
+    "mdb_set_owned", "mdb_gather_positions", "mdb_set_halo_positions",
     "mdb_sort_atoms", "mdb_set_resort", "mdb_set_neighbor_list",
 ]
 # every symbol include/mdb_cp.h declares
@@ -145,6 +146,9 @@ def load():
         "mdb_get_eam_fp": ([vp, _dp], ip),
         "mdb_launch_count": ([vp], C.c_longlong),
         "mdb_kinetic_sum_noalloc": ([vp, ip, C.c_double, vp, vp], ip),
+        "mdb_set_owned": ([vp, ip], ip),
+        "mdb_gather_positions": ([vp, vp, ip, C.c_double, C.c_double, C.c_double, vp], ip),
+        "mdb_set_halo_positions": ([vp, vp, ip], ip),
     }
     for name in ("mdb_setup_pbc", "mdb_update_pbc", "mdb_update_atoms_pbc",
                  "mdb_build_neighbor", "mdb_compute_force", "mdb_compute_force_energy",
@@ -600,6 +604,24 @@ class System:
         self._ck(self.lib.mdb_run(self.h, first_step, nsteps, buf, max_samples, C.byref(ns)),
                  "mdb_run")
         return [buf[k].as_dict() for k in range(ns.value)]
+
+    # -- domain decomposition (halo atoms) ------------------------------------
+    def set_owned(self, nown):
+        """Atoms [nown, nlocal) of the last set_atoms are halo atoms."""
+        self._ck(self.lib.mdb_set_owned(self.h, int(nown)), "mdb_set_owned")
+
+    def gather_positions(self, d_idx, n, shift, d_out):
+        """Device AoS positions of atoms d_idx[0..n) plus shift into d_out
+        (device pointers as ints), on the context's stream."""
+        self._ck(self.lib.mdb_gather_positions(self.h, C.c_void_p(d_idx), int(n),
+                                               float(shift[0]), float(shift[1]),
+                                               float(shift[2]), C.c_void_p(d_out)),
+                 "mdb_gather_positions")
+
+    def set_halo_positions(self, d_x, n):
+        """The halo atoms' positions from device AoS triples, on the context's stream."""
+        self._ck(self.lib.mdb_set_halo_positions(self.h, C.c_void_p(d_x), int(n)),
+                 "mdb_set_halo_positions")
 
     def synchronize(self):
         self._ck(self.lib.mdb_synchronize(self.h), "mdb_synchronize")

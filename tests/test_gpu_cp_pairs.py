@@ -190,3 +190,65 @@ def test_pair_path_timing_and_buffer():
     with pytest.raises(mdb.MdbError):
         f64, _ = system(5, 4, 1, precision="fp64")
         f64.tune("force_path", 1)
+
+
+# ---- MDB_PREC_MIXED_COMP: compensated sums, exact cutoff decisions ------------
+
+def oracle_state(n, types=None, steps=150):
+    """A thermalised state from the Verlet-list oracle, with its parameters."""
+    kw = {}
+    okw = {}
+    if types is not None:
+        import workloads as W
+        kw = dict(types=types, cutforce=W.c5_cutoff(types[1]))
+        okw = dict(epsilon_per_type=types[0], sigma_per_type=types[1], ntypes=len(types[0]),
+                   cutforce=kw["cutforce"])
+    o = O.Oracle(nx=n, ny=n, nz=n, **okw)
+    o.lattice()
+    o.setup()
+    o.run(steps)
+    x, v, _, t = o.atoms()
+    hp = mdb.host_params(nx=n, ny=n, nz=n, **kw)
+    mdb.create_fcc(hp)
+    return hp, x, v, t
+
+
+@pytest.mark.parametrize("N,half", [(4, 1), (4, 0), (8, 1)])
+def test_comp_against_fp64_oracle_multitype(N, half):
+    """4 types, geometric mixing, cutoff 2.5 sigma_max: the compensated path
+    takes exactly the FP64 path's pairs (no outliers from pairs within an FP32
+    rounding of the cutoff, where the unshifted potential jumps) and carries
+    compensated sums, so both its RMS and its max per-atom error stay far
+    below the mixed path's budget."""
+    import workloads as W
+    types = W.c5_types()
+    hp, x, v, t = oracle_state(7, types)
+    common = dict(xprd=hp.xprd, yprd=hp.yprd, zprd=hp.zprd, cutforce=hp.cutforce,
+                  cutneigh=hp.cutneigh, dt=hp.dt, dtforce=hp.dtforce, mass=hp.mass,
+                  ntypes=4, epsilon_per_type=list(types[0]), sigma_per_type=list(types[1]))
+    o = O.OracleCP(x, v, t, M=4, N=N, half=half, natoms=len(t), **common)
+    o.setup()
+    o.force()
+    nat = o.iclusters()[0]
+    ok = np.concatenate([np.arange(4) < k for k in nat])
+    fo = o.slots()[2][:len(ok)][ok]
+    errs = {}
+    for prec in ("mixed", "mixed_comp"):
+        s = mdb.ClusterSystem(natoms=len(t), cluster_n=N, half_neigh=half, precision=prec,
+                              **common)
+        s.set_atoms(x, v, t)
+        s.setup()
+        errs[prec] = rel(valid_forces(s), fo)
+        s.close()
+    r, m = errs["mixed_comp"]
+    assert r <= 2e-6 and m <= 5e-5, errs
+    assert r <= errs["mixed"][0], errs
+
+
+def test_comp_runs_and_rejects_the_cluster_kernel():
+    s, _ = system(6, 4, 1, precision="mixed_comp")
+    with pytest.raises(mdb.MdbError):
+        s.tune("force_path", 0)
+    t0 = s.thermo()["T"]
+    samples = s.run(100)
+    assert samples and abs(samples[-1]["T"] - t0) < 0.5 * t0
