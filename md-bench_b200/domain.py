@@ -115,6 +115,50 @@ class DistTransport:
         return t.tolist()
 
 
+class ThreadTransport:
+    """Ranks as host threads of one process (tests, or a decomposition run on
+    fewer GPUs than ranks): messages pass through queues on the host, so no
+    kernel ever waits on another rank's kernel. One shared hub per run."""
+
+    class Hub:
+        def __init__(self, world):
+            import queue
+            import threading
+            self.world = world
+            self.q = {(r, k): queue.Queue() for r in range(world) for k in ("below", "above")}
+            self.barrier = threading.Barrier(world)
+            self.acc = [0.0]
+            self.lock = threading.Lock()
+
+    def __init__(self, hub, rank):
+        self.hub, self.rank = hub, rank
+
+    def wrap(self, rows):
+        return rows
+
+    def to_host(self, t):
+        return t.cpu().numpy() if hasattr(t, "cpu") else np.asarray(t)
+
+    def exchange(self, down, up, below, above, sizes=None):
+        h = self.hub
+        h.q[(below, "above")].put(down)
+        h.q[(above, "below")].put(up)
+        return h.q[(self.rank, "below")].get(timeout=120), h.q[(self.rank, "above")].get(timeout=120)
+
+    def sum(self, values):
+        h = self.hub
+        h.barrier.wait(timeout=120)
+        if self.rank == 0:
+            h.acc = [0.0] * len(values)
+        h.barrier.wait(timeout=120)
+        with h.lock:
+            h.acc = [a + float(v) for a, v in zip(h.acc, values)]
+        h.barrier.wait(timeout=120)
+        out = list(h.acc)
+        h.barrier.wait(timeout=120)
+        return out
+
+
 class SlabRun:
     """One rank of a slab-decomposed run. ``engine`` holds this rank's atoms
     (see MdbEngine for the interface); atoms carry global ids so that results
@@ -148,7 +192,8 @@ class SlabRun:
         self.send = ((down, sdown), (up, sup))
         self.nhalo = (len(fb), len(fa))
         self.halo_gid = halo[:, 4].astype(np.int64)
-        self.eng.load(x, v, t, halo[:, :3], halo[:, 3].astype(np.int32))
+        self.eng.load(x, v, t, halo[:, :3], halo[:, 3].astype(np.int32),
+                      ids=(gid, self.halo_gid))
 
     def _migrate(self):
         """updateAtoms + reneighbour (verletlist/main.c:115-161): wrap, hand the
@@ -210,13 +255,13 @@ class MdbEngine:
         self.device, self.precision = device, precision
         self.sys = None
 
-    def load(self, x, v, t, hx, ht):
+    def load(self, x, v, t, hx, ht, ids=None):
         torch, mdb = self.torch, self.mdb
         n, nh = len(t), len(ht)
         if self.sys is None:
             # periodic in x and y only: z neighbours come as halo atoms
             self.sys = mdb.system_from_host(self.hp, n + nh, precision=self.precision,
-                                            device=self.device, pbc_z=0, half_neigh=0)
+                                            device=self.device, pbc=(1, 1, 0), half_neigh=0)
         xa = np.concatenate([x, hx]) if nh else x
         va = np.concatenate([v, np.zeros((nh, 3))]) if nh else v
         ta = np.concatenate([t, ht]).astype(np.int32) if nh else t.astype(np.int32)
