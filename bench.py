@@ -43,7 +43,7 @@ REF_CP = {shape: os.path.join(ROOT, "oracle", "_ref", f"MDBench-CP-{shape}")
           for shape in ("4x4", "4x8")}
 METRIC = "atom-steps/s, LJ+EAM mixed-FP32 vs FP64 on 1 B200 at stated force error"
 # headline workload: GROMACS-style 4x4 cluster pairs, half lists, mixed precision
-HEAD = {"kind": "cp44", "precision": "mixed", "half": 1, "path": 1}
+HEAD = {"kind": "cp44", "precision": "mixed", "half": 1, "path": 0}
 HEAD_WORKLOAD = f"lj-fcc-{LJ_CELLS}^3-clusterpair-4x4-half-mixed"
 
 
