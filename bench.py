@@ -57,10 +57,11 @@ def parse():
     ap.add_argument("--profile", choices=[f"{k}_{p}{h}" for k in ("lj", "eam", "cp44", "cp48")
                                           for p in ("mixed", "fp64") for h in ("", "_half")]
                     + [f"{k}_mixed{h}_pairs" for k in ("cp44", "cp48") for h in ("", "_half")]
-                    + ["c5_mixed", "c5_mixed_pairs", "c5_fp64", "c4_mixed", "stub"],
+                    + ["c5_mixed", "c5_mixed_pairs", "c5_fp64", "c4_mixed", "stub"]
+                    + [k for k in VARIANT_SPEC if "mixedcomp" in k],
                     help="run one variant only (W+K bench steps + force timing), for ncu")
     ap.add_argument("--cells", type=int, default=None, help="fcc cells per side (profiling)")
-    ap.add_argument("--tune", default=None, help="key=value[,key=value] cluster-pair tuning")
+    ap.add_argument("--tune", default=None, help="key=value[,key=value] context tuning")
     ap.add_argument("--replicas", type=int, default=C4_REPLICAS, help="ensemble size")
     ap.add_argument("--no-autotune", action="store_true", help="ensemble with default choices")
     return ap.parse_args()
@@ -218,11 +219,11 @@ def make_system(mdb, kind, precision, args, device, half=0, path=0):
     else:
         make = lj_workload if kind == "lj" else eam_workload
         s, init = make(mdb, precision, device, args.cells, half)
-    if kind.startswith("c"):
-        if path:
-            s.tune("force_path", 1)
-        for kv in (args.tune.split(",") if getattr(args, "tune", None) else []):
-            k, val = kv.split("=")
+    if kind.startswith("c") and path:
+        s.tune("force_path", 1)
+    for kv in (args.tune.split(",") if getattr(args, "tune", None) else []):
+        k, val = kv.split("=")
+        if kind.startswith("c") != k.startswith("eam"):
             s.tune(k, int(val))
     return s, init
 
@@ -599,13 +600,25 @@ def _variant_spec():
         spec[f"eam_{prec}"] = ("eam", prec, 0, 0)
         spec[f"c5_{prec}"] = ("c5", prec, 1, 0)
     spec["c5_mixed_pairs"] = ("c5", "mixed", 1, 1)
+    # compensated sums (and, on the cluster-pair scheme, FP64 cutoff decisions
+    # near r_c on the pair-list kernel)
+    spec["cp44_mixedcomp_half"] = ("cp44", "mixed_comp", 1, 1)
+    spec["c5_mixedcomp"] = ("c5", "mixed_comp", 1, 1)
+    spec["vl_mixedcomp"] = ("lj", "mixed_comp", 0, 0)
+    spec["eam_mixedcomp"] = ("eam", "mixed_comp", 0, 0)
     return spec
 
 
 VARIANT_SPEC = _variant_spec()
+
+
+def _twin(key):
+    kind, prec, half, _ = VARIANT_SPEC[key]
+    return f"{key.split('_')[0]}_fp64{'_half' if half and kind != 'c5' else ''}"
+
+
 # the FP64 variant each mixed one is compared with
-FP64_TWIN = {k: k.replace("_mixed", "_fp64").replace("_pairs", "")
-             for k in VARIANT_SPEC if "_mixed" in k}
+FP64_TWIN = {k: _twin(k) for k in VARIANT_SPEC if "_mixed" in k}
 
 
 def drift_window(mdb, kind, precision, args, device, half=0, path=0, md_steps=DRIFT_STEPS):
@@ -679,9 +692,12 @@ def main():
             dist.destroy_process_group()
         return
     if args.profile:
-        kind, prec = args.profile.split("_")[:2]
-        half = 1 if "_half" in args.profile or kind == "c5" else 0
-        path = 1 if args.profile.endswith("_pairs") else 0
+        if args.profile in VARIANT_SPEC:
+            kind, prec, half, path = VARIANT_SPEC[args.profile]
+        else:
+            kind, prec = args.profile.split("_")[:2]
+            half = 1 if "_half" in args.profile or kind == "c5" else 0
+            path = 1 if args.profile.endswith("_pairs") else 0
         m = measure(torch, mdb, kind, prec, args, local, half, path=path)
         kt = force_kernel_time(torch, m["system"], reps=3)
         print(json.dumps({"profile": args.profile, "natoms": m["natoms"],
