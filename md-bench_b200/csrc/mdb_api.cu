@@ -72,6 +72,9 @@ struct MdbCtx {
     int nred_slots = 0;
     double* fp = nullptr;
     float4* xe = nullptr; // mixed EAM: (cell-relative position, F'(rho)) of every atom
+    // mixed EAM: the list entries inside the cutoff (laid out like the list)
+    // and their count per atom, written by the density pass
+    int *eam_cutlist = nullptr, *eam_ncut = nullptr;
     double* stage  = nullptr; // 9 * nlocal doubles: AoS x, v, f for host transfers
     int* stage_t   = nullptr; // nlocal types
     double *eam_frho = nullptr, *eam_rhor = nullptr, *eam_z2r = nullptr;
@@ -430,6 +433,8 @@ static void free_atom_buffers(MdbCtx* ctx)
     dfree(ctx->bin_xf);
     dfree(ctx->numneigh);
     dfree(ctx->neighbors);
+    dfree(ctx->eam_cutlist);
+    dfree(ctx->eam_ncut);
     dfree(ctx->scan_scratch);
     dfree(ctx->partials);
     dfree(ctx->red);
@@ -526,7 +531,10 @@ static int alloc_list(MdbCtx* ctx, int maxneighs)
     CK(cudaStreamSynchronize(ctx->s));
     drop_graphs(ctx);
     dfree(ctx->neighbors);
+    dfree(ctx->eam_cutlist);
     CK(dalloc(&ctx->neighbors, (size_t)maxneighs * ctx->ld));
+    if (ctx->p.force_field == MDB_FF_EAM && ctx->mixed)
+        CK(dalloc(&ctx->eam_cutlist, (size_t)maxneighs * ctx->ld));
     ctx->maxneighs = maxneighs;
     ctx->have_list = false;
     return MDB_OK;
@@ -565,6 +573,7 @@ extern "C" int mdb_set_atoms(MdbCtx* ctx, int nlocal, const double* x, const dou
         CK(dalloc(&ctx->ghost_cnt, nlocal + 1));
         CK(dalloc(&ctx->ghost_off, nlocal + 1));
         CK(dalloc(&ctx->numneigh, nlocal));
+        if (ctx->p.force_field == MDB_FF_EAM && ctx->mixed) CK(dalloc(&ctx->eam_ncut, nlocal));
         CK(dalloc(&ctx->local_order, nlocal));
         CK(dalloc(&ctx->stage, 9 * (size_t)nlocal));
         CK(dalloc(&ctx->stage_t, nlocal));
@@ -676,8 +685,9 @@ static void enq_force(MdbCtx* ctx, bool energy)
         if (ctx->mixed) {
             launch_eam_mixed(s, energy, ctx->p.precision == MDB_PREC_MIXED_COMP,
                 n, ctx->ghost_cap, ctx->xr, ctx->shift, ctx->numneigh, ctx->neighbors, ctx->ld,
-                (float)ctx->cutforcesq, ctx->eam, ctx->border_map, ctx->counters, ctx->fp,
-                ctx->xe, ctx->fx, ctx->fy, ctx->fz, ep0, ep1);
+                (float)ctx->cutforcesq, ctx->eam, ctx->border_map, ctx->counters,
+                ctx->eam_cutlist, ctx->eam_ncut, ctx->fp, ctx->xe, ctx->fx, ctx->fy, ctx->fz, ep0,
+                ep1);
         } else {
             launch_eam_fp64(s, energy, n, ctx->ghost_cap, nullptr,ctx->x,
                 ctx->numneigh, ctx->neighbors, ctx->ld, ctx->cutforcesq, ctx->eam,

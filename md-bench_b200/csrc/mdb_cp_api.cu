@@ -264,6 +264,7 @@ static int setup_types(MdbCp* ctx)
     t.force_block   = 128;
     t.force_variant = 2; // measured fastest on B200 at 1M atoms (4x4 and 4x8, full and half)
     t.force_swizzle = 0;
+    t.force_cpw     = 1;
     t.eps0        = t.sqrt_eps[0] * t.sqrt_eps[0];
     t.sigma6_0 = t.sigma3[0] * t.sigma3[0];
     // the pair-list path's constants (geometric mixing, in FP64 then rounded)
@@ -301,6 +302,12 @@ extern "C" int mdb_cp_tune(MdbCp* ctx, const char* key, int value)
         if (value < 0 || value > 1) return MDB_ERR_ARG;
         drop_graph(ctx);
         ctx->ty.force_swizzle = value;
+        return MDB_OK;
+    }
+    if (!strcmp(key, "force_cpw")) {
+        if (value != 1 && value != 2 && value != 4) return MDB_ERR_ARG;
+        drop_graph(ctx);
+        ctx->ty.force_cpw = value;
         return MDB_OK;
     }
     if (!strcmp(key, "force_variant")) {
@@ -2116,6 +2123,8 @@ extern "C" int mdb_cp_ensemble_create(MdbCp* const* members, int n, MdbCpEnsembl
         // the batched rebuild does not derive pair codes: members run the
         // cluster-pair kernel
         if (c->force_path != 0) return fail(c, MDB_ERR_ARG, "ensemble member on force_path 1");
+        if (c->ty.force_cpw != 1)
+            return fail(c, MDB_ERR_ARG, "ensemble member with force_cpw other than 1");
     }
     MdbCpEnsemble* e = new MdbCpEnsemble();
     e->m.assign(members, members + n);

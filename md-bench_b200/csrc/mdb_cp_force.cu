@@ -148,28 +148,31 @@ void launch_force_fp64(cudaStream_t s, int M, int N, int half, int energy, int n
 // over the 4 i atoms in the lane and add it with one atomic per component.
 // Padding slots sit at +1e18 (j) and invalid i atoms are moved to -1e18, so
 // they fall outside the cutoff without INF arithmetic.
-__device__ __forceinline__ void warp_reduce_12(float (&v)[12], int lane)
+// Sum of 12 partial sums over the L lanes of one i-cluster's segment (l =
+// the lane's index in it). Transpose-reduce: after the xor-L/2 and xor-L/4
+// steps each lane holds 3 partial sums of i atom l / (L/4); plain xor steps
+// L/8 .. 1 finish them.
+template <int L>
+__device__ __forceinline__ void seg_reduce_12(float (&v)[12], int l)
 {
-    // transpose-reduce: after the xor-16 and xor-8 steps each lane holds 3
-    // partial sums of the i atom (lane >> 3); three more steps finish them
     float h[6];
-    const bool up16 = lane & 16;
+    const bool up = l & (L / 2);
 #pragma unroll
     for (int i = 0; i < 6; i++) {
-        float send = up16 ? v[i] : v[i + 6];
-        float keep = up16 ? v[i + 6] : v[i];
-        h[i]       = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+        float send = up ? v[i] : v[i + 6];
+        float keep = up ? v[i + 6] : v[i];
+        h[i]       = keep + __shfl_xor_sync(0xffffffffu, send, L / 2);
     }
     float q[3];
-    const bool up8 = lane & 8;
+    const bool up2 = l & (L / 4);
 #pragma unroll
     for (int i = 0; i < 3; i++) {
-        float send = up8 ? h[i] : h[i + 3];
-        float keep = up8 ? h[i + 3] : h[i];
-        q[i]       = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+        float send = up2 ? h[i] : h[i + 3];
+        float keep = up2 ? h[i + 3] : h[i];
+        q[i]       = keep + __shfl_xor_sync(0xffffffffu, send, L / 4);
     }
 #pragma unroll
-    for (int o = 4; o > 0; o >>= 1)
+    for (int o = L / 8; o > 0; o >>= 1)
 #pragma unroll
         for (int i = 0; i < 3; i++)
             q[i] += __shfl_xor_sync(0xffffffffu, q[i], o);
@@ -281,38 +284,49 @@ __device__ __forceinline__ JEntry load_entry(int cj, int b, const float4* __rest
     return j;
 }
 
-// One warp per i-cluster (M = 4 atoms, held by every lane as two packed
-// pairs). The warp takes 32 / N list entries at a time; lane (e, b) owns atom b
-// of entry e and computes its pairs with the 4 i atoms, two per packed
-// instruction. The list is read in coalesced blocks of 32 entries (the next
-// block in flight) and the j data of the next iteration is loaded while the
-// current one computes. Full lists reduce the i forces across the warp once
-// per i-cluster; half lists also accumulate each j atom's reaction over the 4
-// i atoms in the lane and add it with one atomic per component. Padding slots
-// sit at +1e18 (j) and invalid i atoms are moved to -1e18, so they fall outside
-// the cutoff without INF arithmetic.
+// A segment of L = 32 / CPW lanes per i-cluster (M = 4 atoms, held by every
+// lane of the segment as two packed pairs): CPW i-clusters per warp. The
+// segment takes L / N list entries at a time; lane (e, b) owns atom b of entry
+// e and computes its pairs with the 4 i atoms, two per packed instruction. The
+// list is read in coalesced blocks of L entries (the next block in flight) and
+// the j data of the next iteration is loaded while the current one computes.
+// Full lists reduce the i forces across the segment once per i-cluster; half
+// lists also accumulate each j atom's reaction over the 4 i atoms in the lane
+// and add it with one atomic per component. Padding slots sit at +1e18 (j) and
+// invalid i atoms are moved to -1e18, so they fall outside the cutoff without
+// INF arithmetic.
+// CPW > 1 shares the per-cluster set-up (i atoms, row pointers, the first
+// loads) and the final reduction of a warp among CPW clusters, a fixed cost
+// per i-cluster that is otherwise as large as four or five iterations over
+// the row; a warp runs as many iterations as its longest row (the shorter
+// rows compute the padding cluster meanwhile). The split of a row among the
+// lanes, and so the FP32 rounding of the i sums, depends on CPW.
 // PF: j data prefetched 1 or 2 iterations ahead; MINB: minimum resident blocks
 // of 128 threads per SM asked of the register allocator (0: no request; 8
 // caps a thread at 64 registers, measured best against 6, 7, 9 and 10).
 // Both are launch-shape choices of the autotuner; results do not depend on them.
-// The work of block bid (warps = i-clusters); s_se / s_s3: the type tables in
-// shared memory.
-template <int N, bool HALF, bool ENERGY, bool UNIFORM, int PF>
+// The work of block bid (warps x CPW = i-clusters); s_se / s_s3: the type
+// tables in shared memory.
+template <int N, bool HALF, bool ENERGY, bool UNIFORM, int PF, int CPW>
 __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict__ cnt,
     const float4* __restrict__ xr, const float4* __restrict__ anchor, const Types& ty,
     float cutforcesq, const int* __restrict__ list, int ks, int cs,
     const int* __restrict__ numneigh, float4* cf32, double* epart, const float* s_se,
     const float* s_s3)
 {
-    constexpr int JPW = 32 / N; // entries per warp iteration
+    constexpr int L   = 32 / CPW; // lanes per i-cluster
+    constexpr int JPW = L / N;    // entries per segment iteration
     const int lane = threadIdx.x & 31;
-    const int ci   = (bid * blockDim.x + threadIdx.x) >> 5;
+    const int l    = lane & (L - 1);
+    const int ci   = ((bid * blockDim.x + threadIdx.x) >> 5) * CPW + lane / L;
     const int ncl  = cnt[CP_NCL];
+    const bool act = ci < ncl;
     double e       = 0.0;
-    if (ci < ncl) {
+    if (__any_sync(0xffffffffu, act)) {
+        const int cic    = act ? ci : 0; // address arithmetic of inactive segments
         const int jfac   = N / 4;
-        const int ci_cj0 = ci / jfac;
-        const int ai0    = 4 * (ci % jfac);
+        const int ci_cj0 = cic / jfac;
+        const int ai0    = 4 * (cic % jfac);
         const int nloc   = ncl * 4;
         // i atoms relative to their j-cluster's anchor; j positions are moved
         // into that frame by adding (anchor_j - anchor_i), exact in FP32
@@ -321,11 +335,11 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
         float sei[4], s3i[4];
 #pragma unroll
         for (int a = 0; a < 4; a++) {
-            xi[a] = xr[ci * 4 + a];
+            xi[a] = xr[cic * 4 + a];
             // padding: type -1, or (one type: .w carries the anchor) the
-            // +1e18 position
+            // +1e18 position; every atom of an inactive segment
             int t          = UNIFORM ? 0 : __float_as_int(xi[a].w);
-            const bool pad = UNIFORM ? !(xi[a].x < 0.1f * CP_PAD_F) : t < 0;
+            const bool pad = !act || (UNIFORM ? !(xi[a].x < 0.1f * CP_PAD_F) : t < 0);
             if (pad) {
                 xi[a].x = xi[a].y = xi[a].z = -CP_PAD_F;
                 t                           = 0;
@@ -347,7 +361,7 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
         const float sig6u = (float)ty.sigma6_0;
         const f2 A2 = f2_pack(cA, cA), mB2 = f2_pack(-cB, -cB);
         f2 fx[2] = {0, 0}, fy[2] = {0, 0}, fz[2] = {0, 0};
-        const int eidx = lane / N, b = lane - eidx * N;
+        const int eidx = l / N, b = l - eidx * N;
         // pairs of the diagonal entry (cj == ci_cj0) excluded as the
         // reference's cond (clusterpair/force_lj.c:108-123): the self pair, and
         // for half lists every pair with the i atom at or after the j atom
@@ -355,29 +369,28 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
 #pragma unroll
         for (int a = 0; a < 4; a++)
             if (HALF ? (ai0 + a >= b) : (ai0 + a == b)) diag_excl |= 1u << a;
-        const int nn    = numneigh[ci];
+        const int nn    = act ? numneigh[ci] : 0;
         const int dummy = cnt[CP_NCJ] + cnt[CP_NGC]; // the dummy j-cluster
-        const int* row  = list + (size_t)ci * cs;
-        int lst_cur = lane < nn ? __ldg(&row[(size_t)lane * ks]) : dummy;
-        int lst_nxt = 32 + lane < nn ? __ldg(&row[(size_t)(32 + lane) * ks]) : dummy;
-        JEntry cur =
-            load_entry<N, UNIFORM>(__shfl_sync(0xffffffffu, lst_cur, eidx), b, xr, anchor, ai);
+        const int* row  = list + (size_t)cic * cs;
+        int lst_cur = l < nn ? __ldg(&row[(size_t)l * ks]) : dummy;
+        int lst_nxt = L + l < nn ? __ldg(&row[(size_t)(L + l) * ks]) : dummy;
+        JEntry cur  = load_entry<N, UNIFORM>(__shfl_sync(0xffffffffu, lst_cur, eidx, L), b, xr,
+             anchor, ai);
         JEntry nx1;
         if (PF == 2) {
-            const int c1 = __shfl_sync(0xffffffffu, lst_cur, JPW + eidx);
+            const int c1 = __shfl_sync(0xffffffffu, lst_cur, JPW + eidx, L);
             nx1          = load_entry<N, UNIFORM>(JPW < nn ? c1 : dummy, b, xr, anchor, ai);
         }
-        // one warp iteration: JPW entries, lane (eidx, b) on atom b of entry
-        // kb + eidx; masked: the iteration may hold the diagonal entry
+        // one segment iteration: JPW entries, lane (eidx, b) on atom b of
+        // entry kb + eidx; masked: the iteration may hold the diagonal entry
         auto step = [&](int kb, bool masked) {
             // the entry block holding kn is rotated in when kn reaches it
             const int kn = kb + PF * JPW;
-            if ((kn & 31) == 0) {
+            if ((kn & (L - 1)) == 0) {
                 lst_cur = lst_nxt;
-                lst_nxt = kn + 32 + lane < nn ? __ldg(&row[(size_t)(kn + 32 + lane) * ks])
-                                              : dummy;
+                lst_nxt = kn + L + l < nn ? __ldg(&row[(size_t)(kn + L + l) * ks]) : dummy;
             }
-            const int cjn   = __shfl_sync(0xffffffffu, lst_cur, (kn & 31) + eidx);
+            const int cjn   = __shfl_sync(0xffffffffu, lst_cur, (kn & (L - 1)) + eidx, L);
             const JEntry nx = load_entry<N, UNIFORM>(kn < nn ? cjn : dummy, b, xr, anchor, ai);
             const int cj    = cur.cj;
             float4 xj       = cur.x;
@@ -420,13 +433,14 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
                 cur = nx;
             }
         };
-        // the diagonal entry is the first of its row (the list build swaps it
-        // to the front and pruning never removes it), so only the first
-        // iteration tests for it
-        if (nn > 0) {
+        // the warp runs its longest row; the diagonal entry is the first of
+        // its row (the list build swaps it to the front and pruning never
+        // removes it), so only the first iteration tests for it
+        const int nmax = CPW > 1 ? __reduce_max_sync(0xffffffffu, nn) : nn;
+        if (nmax > 0) {
             step(0, true);
 #pragma unroll(HALF ? 1 : 2)
-            for (int kb = JPW; kb < nn; kb += JPW) step(kb, false);
+            for (int kb = JPW; kb < nmax; kb += JPW) step(kb, false);
         }
         float f[12];
 #pragma unroll
@@ -435,9 +449,9 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
             f2_unpack(fy[h], f[6 * h + 1], f[6 * h + 4]);
             f2_unpack(fz[h], f[6 * h + 2], f[6 * h + 5]);
         }
-        warp_reduce_12(f, lane);
-        if ((lane & 7) == 0) {
-            const int a     = lane >> 3;
+        seg_reduce_12<L>(f, l);
+        if (act && (l & (L / 4 - 1)) == 0) {
+            const int a     = l / (L / 4);
             const float4 xa = xr[ci * 4 + a];
             if (UNIFORM ? xa.x < 0.1f * CP_PAD_F : __float_as_int(xa.w) >= 0) {
                 float4* dst = &cf32[ci * 4 + a];
@@ -465,7 +479,7 @@ __device__ __forceinline__ void load_type_tables(const Types& ty, float* s_se, f
 // (b % slots) * K + b / slots, so that the blocks one resident slot runs one
 // after another take neighbouring i-clusters, whose j data is then still in
 // that SM's L1 (blocks of a launch start in index order)
-template <int N, bool HALF, bool ENERGY, bool UNIFORM, int PF, int MINB>
+template <int N, bool HALF, bool ENERGY, bool UNIFORM, int PF, int MINB, int CPW>
 __global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_force_mixed(
     const int* __restrict__ cnt,
     const float4* __restrict__ xr, const float4* __restrict__ anchor, Types ty,
@@ -476,7 +490,7 @@ __global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_force_mix
     load_type_tables(ty, s_se, s_s3);
     int bid = blockIdx.x;
     if (slots > 0) bid = (blockIdx.x % slots) * (gridDim.x / slots) + blockIdx.x / slots;
-    force_mixed_block<N, HALF, ENERGY, UNIFORM, PF>(bid, cnt, xr, anchor, ty, cutforcesq,
+    force_mixed_block<N, HALF, ENERGY, UNIFORM, PF, CPW>(bid, cnt, xr, anchor, ty, cutforcesq,
         list, ks, cs, numneigh, cf32, epart, s_se, s_s3);
 }
 
@@ -491,7 +505,7 @@ __global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_force_mix
     if (bm.x < 0) return; // an unused entry of a map sized for the capacities
     load_type_tables(ty, s_se, s_s3);
     const CpForceMember& m = tab[bm.x];
-    force_mixed_block<N, HALF, ENERGY, UNIFORM, PF>(bm.y, m.cnt, m.xr, m.anchor, ty, cutforcesq,
+    force_mixed_block<N, HALF, ENERGY, UNIFORM, PF, 1>(bm.y, m.cnt, m.xr, m.anchor, ty, cutforcesq,
         m.list, 1, m.cs, m.numneigh, m.cf32, m.epart, s_se, s_s3);
 }
 
@@ -504,7 +518,7 @@ int force_mixed_threads(const Types& ty)
 int force_mixed_grid(int ncl_cap, const Types& ty)
 {
     const int nt = force_mixed_threads(ty);
-    return (int)(((long long)ncl_cap * 32 + nt - 1) / nt);
+    return (int)(((long long)ncl_cap * 32 / ty.force_cpw + nt - 1) / nt);
 }
 
 template <int N, bool HALF, bool ENERGY, bool UNIFORM>
@@ -573,14 +587,23 @@ static void run_mixed(cudaStream_t s, int blocks, const int* cnt, const float4* 
         if (nb > slots) nb = (nb + slots - 1) / slots * slots;
         else slots = 0;
     }
-#define CP_RUN(PF, MB)                                                                   \
-    k_force_mixed<N, HALF, ENERGY, UNIFORM, PF, MB><<<nb, nt, 0, s>>>(cnt, xr, anchor, ty,   \
+#define CP_RUN(PF, MB, C)                                                                \
+    k_force_mixed<N, HALF, ENERGY, UNIFORM, PF, MB, C><<<nb, nt, 0, s>>>(cnt, xr, anchor, ty, \
         cutforcesq, list, ks, cs, numneigh, cf32, epart, slots)
-    switch (v) {
-    case 1: CP_RUN(2, 0); break;
-    case 2: CP_RUN(1, 8); break;
-    case 3: CP_RUN(2, 8); break;
-    default: CP_RUN(1, 0); break;
+    // several clusters per warp: prefetch depth 1 (bit 0 of the variant unused)
+    if (ty.force_cpw == 2) {
+        if (v & 2) CP_RUN(1, 8, 2);
+        else CP_RUN(1, 0, 2);
+    } else if (ty.force_cpw == 4) {
+        if (v & 2) CP_RUN(1, 8, 4);
+        else CP_RUN(1, 0, 4);
+    } else {
+        switch (v) {
+        case 1: CP_RUN(2, 0, 1); break;
+        case 2: CP_RUN(1, 8, 1); break;
+        case 3: CP_RUN(2, 8, 1); break;
+        default: CP_RUN(1, 0, 1); break;
+        }
     }
 #undef CP_RUN
 }

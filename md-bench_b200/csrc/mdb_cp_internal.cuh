@@ -85,6 +85,7 @@ struct Types {
     int force_block;       // threads per block of the mixed force kernel (tunable)
     int force_variant;     // mixed force kernel: bit 0 prefetch 2 ahead, bit 1 register budget
     int force_swizzle;     // mixed force kernel: blocks walk contiguous cluster ranges (0/1)
+    int force_cpw;         // mixed force kernel: i-clusters per warp (1, 2, 4; single systems)
     int pair_variant;      // pair-list force kernel: launch shape (0..3)
 };
 

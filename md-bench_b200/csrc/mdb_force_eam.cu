@@ -160,51 +160,35 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_fp64(int nlocal,
 }
 
 // ---- mixed ------------------------------------------------------------------
-// Four threads per atom: lane u * 8 + a of a warp takes atom a of the warp's 8
-// atoms and its list entries k = u, u + 4, u + 8, ... (one warp load of a
-// list row then reads 8 consecutive atoms: one full 32-byte sector), and two
-// shuffles combine the four partial sums. At 131k atoms a thread per atom
-// fills under half of the GPU's warp slots and leaves each SM few gathers in
-// flight; four per atom give 4x both.
-// The density pass also writes xe = (position, F'(rho)) of every local atom
-// and k_eam_xe_ghost that of every ghost, so the force pass gathers position
-// and F'(rho_j) of a neighbour in one 16-byte load.
-static constexpr int EAM_TPA = 4;
-
-__device__ __forceinline__ int eam_atom(int& u)
-{
-    const int lane = threadIdx.x & 31;
-    u              = lane >> 3;
-    return ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 8 + (lane & 7);
-}
-
-// the four partial sums of an atom (lanes a, a + 8, a + 16, a + 24)
-__device__ __forceinline__ double eam_combine(double v)
-{
-    v += __shfl_xor_sync(0xffffffffu, v, 8);
-    v += __shfl_xor_sync(0xffffffffu, v, 16);
-    return v;
-}
-
-int eam_mixed_blocks(int nlocal) { return mdb_blocks((long long)nlocal * EAM_TPA, EAM_THREADS); }
+// Thread t handles atom t. The density pass also writes, per atom, the list
+// entries inside the cutoff in list order (cut, laid out like the list, and
+// their count ncut), and xe = (position, F'(rho)) of the atom; k_eam_xe_ghost
+// writes xe of every ghost. The force pass then runs over the in-cutoff
+// entries only and gathers a neighbour's position and F'(rho_j) in one
+// 16-byte load: the same pairs in the same order as a pass over the whole list
+// that skips the rest, without the skin entries (about 40 % of a list at
+// r_c + 1 A) and without a cutoff branch that diverges inside a warp. The two
+// passes compute rsq from the same FP32 values with the same operations, so
+// every entry of cut is inside the cutoff in the force pass too.
+int eam_mixed_blocks(int nlocal) { return mdb_blocks(nlocal, EAM_THREADS); }
 
 template <bool ENERGY>
 __global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_mixed(int nlocal,
     const float4* __restrict__ xr, CellShift sh, const int* __restrict__ numneigh,
     const int* __restrict__ neighbors, int ld, float cutforcesq, EamDev e,
-    double* __restrict__ fp, float4* __restrict__ xe, double* __restrict__ epart)
+    int* __restrict__ cut, int* __restrict__ ncut, double* __restrict__ fp,
+    float4* __restrict__ xe, double* __restrict__ epart)
 {
     const float cg = sh.g;
-    int u;
-    const int i    = eam_atom(u);
-    const bool act = i < nlocal;
-    double rhoi    = 0.0; // FP64 embedding (density) sum
+    const int i    = blockIdx.x * blockDim.x + threadIdx.x;
     double eng     = 0.0;
-    float4 pi      = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (act) {
-        pi              = xr[i];
+    if (i < nlocal) {
+        const float4 pi = xr[i];
         const int n     = numneigh[i];
         const int* nb   = neighbors + i;
+        int* out        = cut + i;
+        int c           = 0;
+        double rhoi     = 0.0; // FP64 embedding (density) sum
         const float rdr = (float)e.rdr;
         auto pair       = [&](int en, const float4& pj) {
             float dx, dy, dz;
@@ -216,19 +200,21 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_mixed(int nlocal,
                 m       = m < e.nr - 1 ? m : e.nr - 1;
                 p -= (float)m;
                 p              = p < 1.0f ? p : 1.0f;
-                const float4 c = __ldg(reinterpret_cast<const float4*>(e.rhor32 + 8 * m) + 0);
-                const float4 d = __ldg(reinterpret_cast<const float4*>(e.rhor32 + 8 * m) + 1);
-                // coefficients 3..6 are c.w, d.x, d.y, d.z
-                rhoi += (double)__fmaf_rn(__fmaf_rn(__fmaf_rn(c.w, p, d.x), p, d.y), p, d.z);
+                const float4 a = __ldg(reinterpret_cast<const float4*>(e.rhor32 + 8 * m) + 0);
+                const float4 b = __ldg(reinterpret_cast<const float4*>(e.rhor32 + 8 * m) + 1);
+                // coefficients 3..6 are a.w, b.x, b.y, b.z
+                rhoi += (double)__fmaf_rn(__fmaf_rn(__fmaf_rn(a.w, p, b.x), p, b.y), p, b.z);
+                __stcg(out + (size_t)c * ld, en);
+                c++;
             }
         };
-        int k = u;
-        for (; k + EAM_TPA * (EUNROLL - 1) < n; k += EAM_TPA * EUNROLL) {
+        int k = 0;
+        for (; k + EUNROLL <= n; k += EUNROLL) {
             int en[EUNROLL];
             float4 pj[EUNROLL];
 #pragma unroll
             for (int v = 0; v < EUNROLL; v++)
-                en[v] = __ldcs(nb + (size_t)(k + EAM_TPA * v) * ld);
+                en[v] = __ldcs(nb + (size_t)(k + v) * ld);
 #pragma unroll
             for (int v = 0; v < EUNROLL; v++)
                 pj[v] = __ldg(xr + (en[v] & MDB_IDX_MASK));
@@ -236,24 +222,22 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_mixed(int nlocal,
             for (int v = 0; v < EUNROLL; v++)
                 pair(en[v], pj[v]);
         }
-        for (; k < n; k += EAM_TPA) {
-            int en = __ldcs(nb + (size_t)k * ld);
+        for (; k < n; k++) {
+            const int en = __ldcs(nb + (size_t)k * ld);
             pair(en, __ldg(xr + (en & MDB_IDX_MASK)));
         }
-    }
-    rhoi = eam_combine(rhoi);
-    if (act && u == 0) {
+        ncut[i]   = c;
         double p = 1.0 * rhoi * e.rdrho + 1.0;
         int m    = (int)(p);
         m        = m < e.nrho - 1 ? m : e.nrho - 1;
         m        = m > 1 ? m : 1;
         p -= m;
         p                = p < 1.0 ? p : 1.0;
-        const double* c  = e.frho + 8 * m;
-        const double fpi = (__ldg(c + 0) * p + __ldg(c + 1)) * p + __ldg(c + 2);
+        const double* cf = e.frho + 8 * m;
+        const double fpi = (__ldg(cf + 0) * p + __ldg(cf + 1)) * p + __ldg(cf + 2);
         fp[i]            = fpi;
         xe[i]            = make_float4(pi.x, pi.y, pi.z, (float)fpi);
-        if (ENERGY) eng = ((__ldg(c + 3) * p + __ldg(c + 4)) * p + __ldg(c + 5)) * p + __ldg(c + 6);
+        if (ENERGY) eng = ((__ldg(cf + 3) * p + __ldg(cf + 4)) * p + __ldg(cf + 5)) * p + __ldg(cf + 6);
     }
     if (ENERGY) {
         double s = block_sum(eng);
@@ -278,24 +262,21 @@ __global__ void k_eam_xe_ghost(int nlocal, const float4* __restrict__ xr,
 // COMP: Knuth two-sum compensated force sums (MDB_PREC_MIXED_COMP)
 template <bool ENERGY, bool COMP>
 __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_mixed(int nlocal,
-    const float4* __restrict__ xe, CellShift sh, const int* __restrict__ numneigh,
-    const int* __restrict__ neighbors, int ld, float cutforcesq, EamDev e,
-    double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
-    double* __restrict__ epart)
+    const float4* __restrict__ xe, CellShift sh, const int* __restrict__ ncut,
+    const int* __restrict__ cut, int ld, EamDev e, double* __restrict__ fx,
+    double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ epart)
 {
     const float cg = sh.g;
-    int u;
-    const int i    = eam_atom(u);
-    const bool act = i < nlocal;
+    const int i    = blockIdx.x * blockDim.x + threadIdx.x;
     double eng     = 0.0;
-    float fix = 0.f, fiy = 0.f, fiz = 0.f;
-    float cx = 0.f, cy = 0.f, cz = 0.f; // compensation terms
-    if (act) {
+    if (i < nlocal) {
         const float4 pi = xe[i];
-        const int n     = numneigh[i];
-        const int* nb   = neighbors + i;
+        const int n     = ncut[i];
+        const int* nb   = cut + i;
         const float fpi = pi.w;
         const float rdr = (float)e.rdr;
+        float fix = 0.f, fiy = 0.f, fiz = 0.f;
+        float cx = 0.f, cy = 0.f, cz = 0.f; // compensation terms
         auto acc = [&](float& s, float& c, float d, float f) {
             if (COMP) { // s + c carries the running sum exactly
                 float v  = d * f;
@@ -311,38 +292,36 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_mixed(int nlocal,
         auto pair = [&](int en, const float4& pj) {
             float dx, dy, dz;
             cell_delta(pi, pj, (unsigned)en >> MDB_IDX_BITS, cg, dx, dy, dz);
-            float rsq = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
-            if (rsq < cutforcesq) {
-                float r = sqrtf(rsq);
-                float p = __fmaf_rn(r, rdr, 1.0f);
-                int m   = (int)p;
-                m       = m < e.nr - 1 ? m : e.nr - 1;
-                p -= (float)m;
-                p               = p < 1.0f ? p : 1.0f;
-                const float4 r0 = __ldg(reinterpret_cast<const float4*>(e.rhor32 + 8 * m));
-                const float4 z0 = __ldg(reinterpret_cast<const float4*>(e.z2r32 + 8 * m) + 0);
-                const float4 z1 = __ldg(reinterpret_cast<const float4*>(e.z2r32 + 8 * m) + 1);
-                float rhoip = __fmaf_rn(__fmaf_rn(r0.x, p, r0.y), p, r0.z);
-                float z2p   = __fmaf_rn(__fmaf_rn(z0.x, p, z0.y), p, z0.z);
-                float z2 = __fmaf_rn(__fmaf_rn(__fmaf_rn(z0.w, p, z1.x), p, z1.y), p, z1.z);
-                float recip = __fdividef(1.0f, r);
-                float phi   = z2 * recip;
-                float phip  = __fmaf_rn(z2p, recip, -phi * recip);
-                float psip  = __fmaf_rn(fpi + pj.w, rhoip, phip);
-                float fpair = -psip * recip;
-                acc(fix, cx, dx, fpair);
-                acc(fiy, cy, dy, fpair);
-                acc(fiz, cz, dz, fpair);
-                if (ENERGY) eng += 0.5 * (double)phi;
-            }
+            const float rsq = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
+            const float r   = sqrtf(rsq);
+            float p         = __fmaf_rn(r, rdr, 1.0f);
+            int m           = (int)p;
+            m               = m < e.nr - 1 ? m : e.nr - 1;
+            p -= (float)m;
+            p               = p < 1.0f ? p : 1.0f;
+            const float4 r0 = __ldg(reinterpret_cast<const float4*>(e.rhor32 + 8 * m));
+            const float4 z0 = __ldg(reinterpret_cast<const float4*>(e.z2r32 + 8 * m) + 0);
+            const float4 z1 = __ldg(reinterpret_cast<const float4*>(e.z2r32 + 8 * m) + 1);
+            float rhoip = __fmaf_rn(__fmaf_rn(r0.x, p, r0.y), p, r0.z);
+            float z2p   = __fmaf_rn(__fmaf_rn(z0.x, p, z0.y), p, z0.z);
+            float z2    = __fmaf_rn(__fmaf_rn(__fmaf_rn(z0.w, p, z1.x), p, z1.y), p, z1.z);
+            float recip = __fdividef(1.0f, r);
+            float phi   = z2 * recip;
+            float phip  = __fmaf_rn(z2p, recip, -phi * recip);
+            float psip  = __fmaf_rn(fpi + pj.w, rhoip, phip);
+            float fpair = -psip * recip;
+            acc(fix, cx, dx, fpair);
+            acc(fiy, cy, dy, fpair);
+            acc(fiz, cz, dz, fpair);
+            if (ENERGY) eng += 0.5 * (double)phi;
         };
-        int k = u;
-        for (; k + EAM_TPA * (EUNROLL - 1) < n; k += EAM_TPA * EUNROLL) {
+        int k = 0;
+        for (; k + EUNROLL <= n; k += EUNROLL) {
             int en[EUNROLL];
             float4 pj[EUNROLL];
 #pragma unroll
             for (int v = 0; v < EUNROLL; v++)
-                en[v] = __ldcs(nb + (size_t)(k + EAM_TPA * v) * ld);
+                en[v] = __ldcs(nb + (size_t)(k + v) * ld);
 #pragma unroll
             for (int v = 0; v < EUNROLL; v++)
                 pj[v] = __ldg(xe + (en[v] & MDB_IDX_MASK));
@@ -350,19 +329,13 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_mixed(int nlocal,
             for (int v = 0; v < EUNROLL; v++)
                 pair(en[v], pj[v]);
         }
-        for (; k < n; k += EAM_TPA) {
-            int en = __ldcs(nb + (size_t)k * ld);
+        for (; k < n; k++) {
+            const int en = __ldcs(nb + (size_t)k * ld);
             pair(en, __ldg(xe + (en & MDB_IDX_MASK)));
         }
-    }
-    // the four partial sums combined in FP64
-    const double sx = eam_combine((double)fix + (double)cx);
-    const double sy = eam_combine((double)fiy + (double)cy);
-    const double sz = eam_combine((double)fiz + (double)cz);
-    if (act && u == 0) {
-        fx[i] = sx;
-        fy[i] = sy;
-        fz[i] = sz;
+        fx[i] = (double)fix + (double)cx;
+        fy[i] = (double)fiy + (double)cy;
+        fz[i] = (double)fiz + (double)cz;
     }
     if (ENERGY) {
         double s = block_sum(eng);
@@ -405,17 +378,18 @@ void launch_eam_fp64(cudaStream_t s, int energy, int nlocal, int ghost_cap, cons
 
 int launch_eam_mixed(cudaStream_t s, int energy, int comp, int nlocal, int ghost_cap,
     const float4* xr, const CellShift& sh, const int* numneigh, const int* neighbors, int ld,
-    float cutforcesq, EamDev eam, const int* border_map, const int* counters, double* fp,
-    float4* xe, double* fx, double* fy, double* fz, double* epart_rho, double* epart_pair)
+    float cutforcesq, EamDev eam, const int* border_map, const int* counters, int* cut,
+    int* ncut, double* fp, float4* xe, double* fx, double* fy, double* fz, double* epart_rho,
+    double* epart_pair)
 {
     if (nlocal <= 0) return 0;
     const int nb = eam_mixed_blocks(nlocal);
     if (energy)
         k_eam_rho_mixed<true><<<nb, EAM_THREADS, 0, s>>>(nlocal, xr, sh, numneigh, neighbors,
-            ld, cutforcesq, eam, fp, xe, epart_rho);
+            ld, cutforcesq, eam, cut, ncut, fp, xe, epart_rho);
     else
         k_eam_rho_mixed<false><<<nb, EAM_THREADS, 0, s>>>(nlocal, xr, sh, numneigh, neighbors,
-            ld, cutforcesq, eam, fp, xe, epart_rho);
+            ld, cutforcesq, eam, cut, ncut, fp, xe, epart_rho);
     g_launches++;
     if (ghost_cap > 0) {
         k_eam_xe_ghost<<<mdb_blocks(ghost_cap, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(nlocal, xr,
@@ -423,8 +397,8 @@ int launch_eam_mixed(cudaStream_t s, int energy, int comp, int nlocal, int ghost
         g_launches++;
     }
 #define EAM_FM(E, C)                                                                     \
-    k_eam_force_mixed<E, C><<<nb, EAM_THREADS, 0, s>>>(nlocal, xe, sh, numneigh, neighbors, ld, \
-        cutforcesq, eam, fx, fy, fz, epart_pair)
+    k_eam_force_mixed<E, C><<<nb, EAM_THREADS, 0, s>>>(nlocal, xe, sh, ncut, cut, ld, eam, fx, \
+        fy, fz, epart_pair)
     if (energy) {
         if (comp) EAM_FM(true, true);
         else EAM_FM(true, false);

@@ -232,8 +232,9 @@ void launch_eam_fp64(cudaStream_t s, int energy, int nlocal, int ghost_cap, cons
 // compensated force sums; returns the energy partials written per pass
 int launch_eam_mixed(cudaStream_t s, int energy, int comp, int nlocal, int ghost_cap,
     const float4* xr, const CellShift& sh, const int* numneigh, const int* neighbors, int ld,
-    float cutforcesq, EamDev eam, const int* border_map, const int* counters, double* fp,
-    float4* xe, double* fx, double* fy, double* fz, double* epart_rho, double* epart_pair);
+    float cutforcesq, EamDev eam, const int* border_map, const int* counters, int* cut,
+    int* ncut, double* fp, float4* xe, double* fx, double* fy, double* fz, double* epart_rho,
+    double* epart_pair);
 int eam_mixed_blocks(int nlocal);
 
 // domain-decomposed runs: positions of atoms idx[0..n) plus a shift, AoS

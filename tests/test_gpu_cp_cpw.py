@@ -1,0 +1,95 @@
+"""Several i-clusters per warp in the mixed cluster-pair kernel (force_cpw).
+
+force_cpw 2 and 4 give each i-cluster a segment of 16 or 8 lanes instead of
+a warp. They evaluate the same pairs of the same list, so their forces equal
+force_cpw 1's up to FP32 summation order (the split of a row among lanes
+differs), for 4x4 and 4x8 clusters, half and full lists, one and four atom
+types, with energies; trajectories stay within the mixed path's budget of the
+FP64 oracle's forces. Ensembles run one cluster per warp and reject the
+setting.
+"""
+import numpy as np
+import pytest
+
+import mdb
+import oracle as O
+from test_gpu_cp_pairs import MIXED_RMS, SUM_ORDER, rel, system, valid_forces
+
+pytestmark = pytest.mark.gpu
+
+C5_TYPES = ([0.5, 1.5, 0.8, 1.2], [0.8, 1.2, 1.0, 0.9])
+
+
+def forces(s, cpw, energy=True):
+    s.tune("force_cpw", cpw)
+    s.compute_force(energy=energy)
+    return valid_forces(s), (s.thermo()["PE"] if energy else None)
+
+
+@pytest.mark.parametrize("N", [4, 8])
+@pytest.mark.parametrize("half", [0, 1])
+@pytest.mark.parametrize("types", [None, C5_TYPES], ids=["one_type", "four_types"])
+def test_cpw_matches_one_cluster_per_warp(N, half, types):
+    s, _ = system(7, N, half, steps=120, types=types)
+    f1, e1 = forces(s, 1)
+    for cpw in (2, 4):
+        f, e = forces(s, cpw)
+        r, m = rel(f, f1)
+        assert r <= SUM_ORDER and m <= 10 * SUM_ORDER, (cpw, r, m)
+        assert e == pytest.approx(e1, rel=1e-6)
+
+
+@pytest.mark.parametrize("half", [0, 1])
+def test_cpw_against_fp64_oracle(half):
+    """force_cpw 2 and 4 on a melted state against the FP64 oracle's forces."""
+    n = 8
+    o0 = O.Oracle(nx=n, ny=n, nz=n)
+    o0.lattice()
+    o0.setup()
+    o0.run(200)
+    x, v, _, t = o0.atoms()
+    hp = mdb.host_params(nx=n, ny=n, nz=n)
+    mdb.create_fcc(hp)
+    common = dict(xprd=hp.xprd, yprd=hp.yprd, zprd=hp.zprd, cutforce=hp.cutforce,
+                  cutneigh=hp.cutneigh, dt=hp.dt, dtforce=hp.dtforce, mass=hp.mass,
+                  epsilon=hp.epsilon, sigma=hp.sigma, ntypes=hp.ntypes)
+    o = O.OracleCP(x, v, t, M=4, N=4, half=half, natoms=len(t), **common)
+    o.setup()
+    o.force()
+    nat = o.iclusters()[0]
+    ok = np.concatenate([np.arange(4) < k for k in nat])
+    fo = o.slots()[2][:len(ok)][ok]
+    s = mdb.ClusterSystem(natoms=len(t), cluster_n=4, half_neigh=half, precision="mixed",
+                          **common)
+    s.set_atoms(x, v, t)
+    s.setup()
+    for cpw in (2, 4):
+        f, _ = forces(s, cpw, energy=False)
+        r, m = rel(f, fo)
+        assert r <= MIXED_RMS and m <= 20 * MIXED_RMS, (cpw, r, m)
+
+
+def test_cpw_trajectory_tracks_one_cluster_per_warp():
+    """100 steps from the lattice (five rebuilds) with force_cpw 2 and 1: the
+    temperatures agree as two mixed runs that differ in summation order."""
+    a, _ = system(6, 4, 1)
+    b, _ = system(6, 4, 1)
+    b.tune("force_cpw", 2)
+    a.run(100, max_samples=0)
+    b.run(100, max_samples=0)
+    assert b.thermo()["T"] == pytest.approx(a.thermo()["T"], rel=1e-3)
+
+
+def test_ensemble_rejects_cpw():
+    a, _ = system(5, 4, 1)
+    b, _ = system(6, 4, 1)
+    b.tune("force_cpw", 2)
+    with pytest.raises(mdb.MdbError):
+        mdb.Ensemble([a, b])
+
+
+def test_cpw_rejects_bad_values():
+    s, _ = system(4, 4, 0)
+    for bad in (0, 3, 8):
+        with pytest.raises(mdb.MdbError):
+            s.tune("force_cpw", bad)
