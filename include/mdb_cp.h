@@ -43,12 +43,19 @@ int mdb_cp_destroy(MdbCp* ctx);
 const char* mdb_cp_last_error(const MdbCp* ctx);
 void* mdb_cp_stream(MdbCp* ctx);
 int mdb_cp_synchronize(MdbCp* ctx);
-/* Launch tuning (no counterpart in the reference; results are unchanged):
+/* Launch tuning (no counterpart in the reference; results are unchanged
+ * except where noted):
+ * "force_cpw" = i-clusters per warp of the mixed cluster-pair kernel: 1, 2, 4,
+ * or 8 with 4x4 clusters (default 4). Each i-cluster gets 32 / force_cpw
+ * lanes; the rows of a warp's clusters run side by side. The same pairs are
+ * evaluated, but a row's split among the lanes, and so the FP32 rounding of
+ * the i sums, depends on the setting. Ensemble members keep theirs;
  * "force_block" = threads per block of the mixed force kernel (32..512, a
  * multiple of 32; default 128); "force_variant" = 0..3: 0 and 1 prefetch the
  * j data one or two list blocks ahead with no register budget, 2 and 3 the same
  * with a budget for 8 resident blocks of 128 threads per SM (these run blocks
- * of 128 threads; default 2); "force_swizzle" = 1: the blocks one resident
+ * of 128 threads; default 2; with force_cpw > 1, 1 and 3 run as 0 and 2);
+ * "force_swizzle" = 1: the blocks one resident
  * slot runs in turn take neighbouring i-clusters (L1 reuse of j data; default
  * 0, measured within 2 % either way); "force_path" (mixed contexts) = 0: the
  * cluster-pair kernel evaluates every pair slot of the listed cluster pairs,

@@ -10,8 +10,9 @@ chosen shape. The tuner picks, per system size:
 
 * cluster shape N = 4 or 8 (which also fixes the column size),
 * list form: full or half (half-list reactions use atomics),
-* the mixed force kernel's launch: threads per block (``force_block``) and
-  ``force_variant`` (prefetch depth, register budget),
+* the mixed force kernel's launch: threads per block (``force_block``),
+  ``force_variant`` (prefetch depth, register budget) and i-clusters per warp
+  (``force_cpw``: 1, 2, 4, or 8 with 4x4 clusters),
 
 by measurement on the device. A single large system is tuned on the force
 kernel's own time (``ClusterSystem.time_force``, CUDA events). Members of an
@@ -30,7 +31,16 @@ SHAPES = (4, 8)
 FORMS = (0, 1)
 BLOCKS = (64, 128, 256)
 VARIANTS = (0, 1, 2, 3)
-DEFAULT = {"cluster_n": 4, "half": 1, "force_block": 128, "force_variant": 2}
+CPWS = (1, 2, 4, 8)
+DEFAULT = {"cluster_n": 4, "half": 1, "force_block": 128, "force_variant": 2, "force_cpw": 4}
+
+
+def valid(choice):
+    """force_cpw 8 needs 4x4 clusters; several clusters per warp prefetch one
+    block ahead (variants 1 and 3 run as 0 and 2 there)."""
+    if choice.get("force_cpw", 1) == 8 and choice["cluster_n"] != 4:
+        return False
+    return not (choice.get("force_cpw", 1) > 1 and choice.get("force_variant", 0) in (1, 3))
 
 
 def size_class(natoms):
@@ -42,6 +52,7 @@ def apply_launch(system, choice):
     """Launch settings of a choice on a (mixed-precision) system."""
     system.tune("force_block", choice["force_block"])
     system.tune("force_variant", choice["force_variant"])
+    system.tune("force_cpw", choice["force_cpw"])
 
 
 def tune_system(build, precision="mixed", reps=20, shapes=SHAPES, forms=FORMS):
@@ -54,15 +65,17 @@ def tune_system(build, precision="mixed", reps=20, shapes=SHAPES, forms=FORMS):
             t = s.time_force(reps)
             trials.append(({"cluster_n": n, "half": half}, t))
             if precision == "mixed":
-                for blk in BLOCKS:
-                    for var in VARIANTS:
-                        c = {"cluster_n": n, "half": half, "force_block": blk,
-                             "force_variant": var}
-                        apply_launch(s, c)
-                        t = s.time_force(reps)
-                        trials.append((c, t))
-                        if best is None or t < best[1]:
-                            best = (c, t)
+                for blk, var, cpw in ((b, v, w) for b in BLOCKS for v in VARIANTS
+                                      for w in CPWS):
+                    c = {"cluster_n": n, "half": half, "force_block": blk,
+                         "force_variant": var, "force_cpw": cpw}
+                    if not valid(c):
+                        continue
+                    apply_launch(s, c)
+                    t = s.time_force(reps)
+                    trials.append((c, t))
+                    if best is None or t < best[1]:
+                        best = (c, t)
             elif best is None or t < best[1]:
                 best = ({"cluster_n": n, "half": half}, t)
             s.close()
@@ -123,6 +136,8 @@ def tune_ensemble(specs, build, steps=20, rounds=2, shapes=SHAPES, forms=FORMS, 
                 if (n, half) == (choice[c]["cluster_n"], choice[c]["half"]):
                     continue
                 trial = dict(choice[c], cluster_n=n, half=half)
+                if not valid(trial):
+                    continue
                 old, members[c] = members[c], [build(sp, n, half) for sp in classes[c]]
                 for m in members[c]:
                     apply_launch(m, trial)
@@ -135,11 +150,14 @@ def tune_ensemble(specs, build, steps=20, rounds=2, shapes=SHAPES, forms=FORMS, 
                     close(members[c])
                     members[c] = old
     for c in order:
-        for key, values in (("force_block", BLOCKS), ("force_variant", VARIANTS)):
+        for key, values in (("force_block", BLOCKS), ("force_variant", VARIANTS),
+                            ("force_cpw", CPWS)):
             for val in values:
                 if val == choice[c][key]:
                     continue
                 trial = dict(choice[c], **{key: val})
+                if not valid(trial):
+                    continue
                 for m in members[c]:
                     apply_launch(m, trial)
                 r = rate(everyone())

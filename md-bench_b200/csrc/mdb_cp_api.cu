@@ -264,7 +264,9 @@ static int setup_types(MdbCp* ctx)
     t.force_block   = 128;
     t.force_variant = 2; // measured fastest on B200 at 1M atoms (4x4 and 4x8, full and half)
     t.force_swizzle = 0;
-    t.force_cpw     = 1;
+    // four i-clusters per warp: measured fastest on B200 at 1M atoms (4x4 and
+    // 4x8, full and half; 170 us against 229 us per launch for one per warp)
+    t.force_cpw     = 4;
     t.eps0        = t.sqrt_eps[0] * t.sqrt_eps[0];
     t.sigma6_0 = t.sigma3[0] * t.sigma3[0];
     // the pair-list path's constants (geometric mixing, in FP64 then rounded)
@@ -305,7 +307,9 @@ extern "C" int mdb_cp_tune(MdbCp* ctx, const char* key, int value)
         return MDB_OK;
     }
     if (!strcmp(key, "force_cpw")) {
-        if (value != 1 && value != 2 && value != 4) return MDB_ERR_ARG;
+        // 8: 4x4 clusters only (a segment of 4 lanes holds one j-cluster)
+        if (value != 1 && value != 2 && value != 4 && !(value == 8 && ctx->N == 4))
+            return MDB_ERR_ARG;
         drop_graph(ctx);
         ctx->ty.force_cpw = value;
         return MDB_OK;
@@ -1772,7 +1776,7 @@ static bool same_types(const Types& a, const Types& b)
 {
     if (a.ntypes != b.ntypes || a.uniform != b.uniform || a.eps0 != b.eps0 ||
         a.sigma6_0 != b.sigma6_0 || a.force_block != b.force_block ||
-        a.force_variant != b.force_variant)
+        a.force_variant != b.force_variant || a.force_cpw != b.force_cpw)
         return false;
     for (int t = 0; t < MDB_MAX_TYPES; t++)
         if (a.sqrt_eps_f[t] != b.sqrt_eps_f[t] || a.sigma3_f[t] != b.sigma3_f[t]) return false;
@@ -2123,8 +2127,6 @@ extern "C" int mdb_cp_ensemble_create(MdbCp* const* members, int n, MdbCpEnsembl
         // the batched rebuild does not derive pair codes: members run the
         // cluster-pair kernel
         if (c->force_path != 0) return fail(c, MDB_ERR_ARG, "ensemble member on force_path 1");
-        if (c->ty.force_cpw != 1)
-            return fail(c, MDB_ERR_ARG, "ensemble member with force_cpw other than 1");
     }
     MdbCpEnsemble* e = new MdbCpEnsemble();
     e->m.assign(members, members + n);

@@ -316,6 +316,7 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
 {
     constexpr int L   = 32 / CPW; // lanes per i-cluster
     constexpr int JPW = L / N;    // entries per segment iteration
+    static_assert(JPW >= 1, "a segment holds at least one list entry");
     const int lane = threadIdx.x & 31;
     const int l    = lane & (L - 1);
     const int ci   = ((bid * blockDim.x + threadIdx.x) >> 5) * CPW + lane / L;
@@ -495,7 +496,7 @@ __global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_force_mix
 }
 
 // all members of an ensemble group (same shape, list form, types and launch)
-template <int N, bool HALF, bool ENERGY, bool UNIFORM, int PF, int MINB>
+template <int N, bool HALF, bool ENERGY, bool UNIFORM, int PF, int MINB, int CPW>
 __global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_force_mixed_batch(
     const CpForceMember* __restrict__ tab, const int2* __restrict__ bmap, Types ty,
     float cutforcesq)
@@ -505,7 +506,7 @@ __global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_force_mix
     if (bm.x < 0) return; // an unused entry of a map sized for the capacities
     load_type_tables(ty, s_se, s_s3);
     const CpForceMember& m = tab[bm.x];
-    force_mixed_block<N, HALF, ENERGY, UNIFORM, PF, 1>(bm.y, m.cnt, m.xr, m.anchor, ty, cutforcesq,
+    force_mixed_block<N, HALF, ENERGY, UNIFORM, PF, CPW>(bm.y, m.cnt, m.xr, m.anchor, ty, cutforcesq,
         m.list, 1, m.cs, m.numneigh, m.cf32, m.epart, s_se, s_s3);
 }
 
@@ -526,14 +527,28 @@ static void run_mixed_batch(cudaStream_t s, int nblocks, const CpForceMember* ta
     const int2* bmap, const Types& ty, float cutforcesq)
 {
     const int nt = force_mixed_threads(ty);
-#define CP_RUN(PF, MB)                                                                   \
-    k_force_mixed_batch<N, HALF, ENERGY, UNIFORM, PF, MB><<<nblocks, nt, 0, s>>>(tab, bmap, ty, \
-        cutforcesq)
-    switch (ty.force_variant) {
-    case 1: CP_RUN(2, 0); break;
-    case 2: CP_RUN(1, 8); break;
-    case 3: CP_RUN(2, 8); break;
-    default: CP_RUN(1, 0); break;
+#define CP_RUN(PF, MB, C)                                                                \
+    k_force_mixed_batch<N, HALF, ENERGY, UNIFORM, PF, MB, C><<<nblocks, nt, 0, s>>>(tab, bmap, \
+        ty, cutforcesq)
+    const int v = ty.force_variant;
+    if (ty.force_cpw == 2) {
+        if (v & 2) CP_RUN(1, 8, 2);
+        else CP_RUN(1, 0, 2);
+    } else if (ty.force_cpw == 4) {
+        if (v & 2) CP_RUN(1, 8, 4);
+        else CP_RUN(1, 0, 4);
+    } else if (ty.force_cpw == 8) {
+        if constexpr (N == 4) {
+            if (v & 2) CP_RUN(1, 8, 8);
+            else CP_RUN(1, 0, 8);
+        }
+    } else {
+        switch (v) {
+        case 1: CP_RUN(2, 0, 1); break;
+        case 2: CP_RUN(1, 8, 1); break;
+        case 3: CP_RUN(2, 8, 1); break;
+        default: CP_RUN(1, 0, 1); break;
+        }
     }
 #undef CP_RUN
 }
@@ -597,6 +612,12 @@ static void run_mixed(cudaStream_t s, int blocks, const int* cnt, const float4* 
     } else if (ty.force_cpw == 4) {
         if (v & 2) CP_RUN(1, 8, 4);
         else CP_RUN(1, 0, 4);
+    } else if (ty.force_cpw == 8) {
+        // a segment of 4 lanes: one entry of a 4-wide j-cluster at a time
+        if constexpr (N == 4) {
+            if (v & 2) CP_RUN(1, 8, 8);
+            else CP_RUN(1, 0, 8);
+        }
     } else {
         switch (v) {
         case 1: CP_RUN(2, 0, 1); break;

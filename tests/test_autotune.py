@@ -12,8 +12,7 @@ class FakeMember:
     def __init__(self, sp, n, half, log):
         self.natoms, self.nlocal = sp["natoms"], sp["natoms"]
         self.cluster_n, self.half = n, half
-        self.launch = {"force_block": AT.DEFAULT["force_block"],
-                       "force_variant": AT.DEFAULT["force_variant"]}
+        self.launch = {k: AT.DEFAULT[k] for k in ("force_block", "force_variant", "force_cpw")}
         self.closed = False
         log.append(self)
 
@@ -30,7 +29,8 @@ def model_rate(members):
     """Time of the ensemble = sum over members of natoms x cost, where the model
     rewards: 4x8 half lists for the 500-atom class (-20 %), full lists for the 4000-atom
     class (-1 %, inside the margin), 256 threads for the 4000-atom class
-    (-10 %); plus one launch per distinct (shape, form, launch) group."""
+    (-10 %), eight i-clusters per warp for the 32,000-atom class (-8 %); plus
+    one launch per distinct (shape, form, launch) group."""
     t, groups = 0.0, set()
     for m in members:
         assert not m.closed
@@ -42,10 +42,13 @@ def model_rate(members):
             c *= 0.99
         if cls == AT.size_class(4000) and m.launch["force_block"] == 256:
             c *= 0.9
+        if cls == AT.size_class(32000) and m.launch["force_cpw"] == 8:
+            c *= 0.92
         if m.launch["force_variant"] != AT.DEFAULT["force_variant"]:
             c *= 1.05
         t += m.natoms * c
-        groups.add((m.cluster_n, m.half, m.launch["force_block"], m.launch["force_variant"]))
+        groups.add((m.cluster_n, m.half, m.launch["force_block"], m.launch["force_variant"],
+                    m.launch["force_cpw"]))
     t += 50.0 * len(groups)
     return sum(m.natoms for m in members) / t
 
@@ -62,7 +65,9 @@ def test_coordinate_descent_finds_rewarded_choices():
     assert c512["force_block"] == AT.DEFAULT["force_block"]
     assert (c4k["cluster_n"], c4k["half"]) == (4, 1)      # full lists gain < margin
     assert c4k["force_block"] == 256
-    assert c32k == AT.DEFAULT
+    assert c32k == dict(AT.DEFAULT, force_cpw=8)
+    # force_cpw 8 was never tried on a 4x8 shape
+    assert all(t[1]["force_cpw"] != 8 or t[1]["cluster_n"] == 4 for t in trials)
     assert all(c["force_variant"] == AT.DEFAULT["force_variant"] for c in choice.values())
     # every system built was closed, and trials start from the default ensemble
     assert log and all(m.closed for m in log)
@@ -74,7 +79,8 @@ def test_coordinate_descent_finds_rewarded_choices():
 def test_no_change_within_noise():
     specs = [{"natoms": 1000}] * 3
     log = []
-    flat = iter([1.0, 1.01, 0.99, 1.015, 1.0, 1.019, 0.98, 1.0, 1.0, 1.0])
+    flat = iter([1.0, 1.01, 0.99, 1.015, 1.0, 1.019, 0.98, 1.0, 1.0, 1.0, 1.012, 1.0, 0.99,
+                 1.0])
     choice, trials = AT.tune_ensemble(specs, lambda sp, n, h: FakeMember(sp, n, h, log),
                                       rate=lambda ms: next(flat))
     assert choice == {AT.size_class(1000): AT.DEFAULT}
