@@ -348,6 +348,48 @@ def run_ensemble(torch, mdb, members, args, every=20):
     return secs, launches, np.array(drifts), n
 
 
+def sharded(torch, dist, mdb, rank, world, device, md_steps=40):
+    """The z-slab domain decomposition of the Verlet-list scheme (full lists,
+    mixed) on LJ fcc 64^3: every rank owns a slab of the same system and
+    exchanges its halo's positions every step and atoms at each rebuild
+    (md-bench_b200/domain.py). Several ranks exchange over torch.distributed
+    point-to-point calls (NCCL); one rank gets its slab's own z images
+    through host queues, as its own neighbour. One untimed rebuild period,
+    then md_steps steps timed with CUDA events after a device synchronisation
+    on both sides (the loop is host-driven: host work is inside), max over
+    ranks. value = all atoms x md_steps / that time."""
+    import domain as D
+    hp = mdb.host_params(nx=LJ_CELLS, ny=LJ_CELLS, nz=LJ_CELLS)
+    x, v, t = mdb.create_fcc(hp)
+    box = (hp.xprd, hp.yprd, hp.zprd)
+    tr = (D.DistTransport(torch, dist, "cuda") if world > 1
+          else D.ThreadTransport(D.ThreadTransport.Hub(1), 0))
+    eng = D.MdbEngine(torch, mdb, hp, device, "mixed")
+    run = D.SlabRun(D.Slabs(box, hp.cutneigh, world, rank), tr, eng, hp.reneigh_every)
+    run.start(x, v, t, np.arange(len(t)))
+    run.run(hp.reneigh_every)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    run.run(md_steps, first_step=hp.reneigh_every)
+    torch.cuda.synchronize()
+    e1.record()
+    e1.synchronize()
+    secs = reduce_scalar(torch, dist, e0.elapsed_time(e1) / 1e3, "max", "cuda")
+    temp = run.temperature(len(t))
+    owned = reduce_scalar(torch, dist, eng.n, "max", "cuda")
+    halo = reduce_scalar(torch, dist, eng.nh, "max", "cuda")
+    eng.sys.close()
+    return {"value": len(t) * md_steps / secs, "unit": "atom-steps/s", "ranks": world,
+            "scaling": "strong", "workload": HEAD_WORKLOAD.replace("clusterpair-4x4-half",
+                                                                  "verletlist-full-zslabs"),
+            "md_steps": md_steps, "max_owned_atoms": int(owned), "max_halo_atoms": int(halo),
+            "T_end": temp,
+            "exchange": "NCCL point-to-point" if world > 1 else "one slab: its own z images"}
+
+
 def reduce_scalar(torch, dist, x, op, device):
     """x reduced over all ranks (op "max" or "sum"); x itself without a group."""
     if dist is None:
@@ -828,6 +870,12 @@ def main():
     for es in extra_sys:
         es.close()
     e2["value"] = reduce_scalar(torch, dist, e2["value"], "sum", "cuda")
+    # the same LJ system split into z-slabs over all ranks
+    barrier()
+    try:
+        dd = sharded(torch, dist, mdb, rank, world, local)
+    except (mdb.MdbError, RuntimeError, ValueError) as e:
+        dd = {"error": str(e)[:300]}
     cb = cpu_baseline(half=HEAD["half"]) if (rank == 0 and world == 1) else None
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world,
@@ -850,7 +898,7 @@ def main():
                                     head["natoms"] * 96 / 1e6),
                            "parallelism": f"replicas{world}"},
                 "roofline": roof, "cpu_baseline": cb, "e2e": e2, "clocks": clocks,
-                "gpu_launches": head["launches"]}
+                "gpu_launches": head["launches"], "sharded": dd}
         line.update(extra)
         print(json.dumps(line), flush=True)
     if dist:

@@ -78,7 +78,8 @@ struct MdbCtx {
     double* stage  = nullptr; // 9 * nlocal doubles: AoS x, v, f for host transfers
     int* stage_t   = nullptr; // nlocal types
     double *eam_frho = nullptr, *eam_rhor = nullptr, *eam_z2r = nullptr;
-    float *eam_frho32 = nullptr, *eam_rhor32 = nullptr, *eam_z2r32 = nullptr;
+    float* eam_frho32 = nullptr;
+    float4 *eam_dens32 = nullptr, *eam_pair32 = nullptr;
     EamDev eam;
     double eam_cut = 0;
 
@@ -462,8 +463,8 @@ extern "C" int mdb_destroy(MdbCtx* ctx)
     dfree(ctx->eam_rhor);
     dfree(ctx->eam_z2r);
     dfree(ctx->eam_frho32);
-    dfree(ctx->eam_rhor32);
-    dfree(ctx->eam_z2r32);
+    dfree(ctx->eam_dens32);
+    dfree(ctx->eam_pair32);
     if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
     if (ctx->s) cudaStreamDestroy(ctx->s);
     delete ctx;
@@ -1275,24 +1276,36 @@ extern "C" int mdb_set_eam(MdbCtx* ctx, const MdbEamTables* t)
     relayout(t->frho_spline, t->nrho, t->nrho_tot, fr, fr32);
     relayout(t->rhor_spline, t->nr, t->nr_tot, rr, rr32);
     relayout(t->z2r_spline, t->nr, t->nr_tot, zr, zr32);
+    // the mixed passes' rows (see EamDev)
+    const size_t nrow = (size_t)t->nr + 1;
+    std::vector<float4> dens32(nrow), pair32(2 * nrow);
+    for (size_t m = 0; m < nrow; m++) {
+        const float* r = &rr32[m * 8];
+        const float* z = &zr32[m * 8];
+        dens32[m]         = make_float4(r[3], r[4], r[5], r[6]);
+        pair32[2 * m]     = make_float4(z[3], z[4], z[5], z[6]);
+        pair32[2 * m + 1] = make_float4(r[0], r[1], r[2], z[0]);
+    }
     dfree(ctx->eam_frho);
     dfree(ctx->eam_rhor);
     dfree(ctx->eam_z2r);
     dfree(ctx->eam_frho32);
-    dfree(ctx->eam_rhor32);
-    dfree(ctx->eam_z2r32);
+    dfree(ctx->eam_dens32);
+    dfree(ctx->eam_pair32);
     CK(dalloc(&ctx->eam_frho, fr.size()));
     CK(dalloc(&ctx->eam_rhor, rr.size()));
     CK(dalloc(&ctx->eam_z2r, zr.size()));
     CK(dalloc(&ctx->eam_frho32, fr32.size()));
-    CK(dalloc(&ctx->eam_rhor32, rr32.size()));
-    CK(dalloc(&ctx->eam_z2r32, zr32.size()));
+    CK(dalloc(&ctx->eam_dens32, dens32.size()));
+    CK(dalloc(&ctx->eam_pair32, pair32.size()));
     CK(cudaMemcpy(ctx->eam_frho, fr.data(), fr.size() * 8, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ctx->eam_rhor, rr.data(), rr.size() * 8, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ctx->eam_z2r, zr.data(), zr.size() * 8, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ctx->eam_frho32, fr32.data(), fr32.size() * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->eam_rhor32, rr32.data(), rr32.size() * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->eam_z2r32, zr32.data(), zr32.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->eam_dens32, dens32.data(), dens32.size() * sizeof(float4),
+        cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->eam_pair32, pair32.data(), pair32.size() * sizeof(float4),
+        cudaMemcpyHostToDevice));
     ctx->eam.nrho   = t->nrho;
     ctx->eam.nr     = t->nr;
     ctx->eam.rdr    = t->rdr;
@@ -1301,8 +1314,8 @@ extern "C" int mdb_set_eam(MdbCtx* ctx, const MdbEamTables* t)
     ctx->eam.rhor   = ctx->eam_rhor;
     ctx->eam.z2r    = ctx->eam_z2r;
     ctx->eam.frho32 = ctx->eam_frho32;
-    ctx->eam.rhor32 = ctx->eam_rhor32;
-    ctx->eam.z2r32  = ctx->eam_z2r32;
+    ctx->eam.dens32 = ctx->eam_dens32;
+    ctx->eam.pair32 = ctx->eam_pair32;
     ctx->have_eam   = true;
     return MDB_OK;
 }

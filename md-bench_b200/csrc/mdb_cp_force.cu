@@ -440,7 +440,7 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
         const int nmax = CPW > 1 ? __reduce_max_sync(0xffffffffu, nn) : nn;
         if (nmax > 0) {
             step(0, true);
-#pragma unroll(HALF ? 1 : 2)
+#pragma unroll((HALF && CPW == 1) ? 1 : 2)
             for (int kb = JPW; kb < nmax; kb += JPW) step(kb, false);
         }
         float f[12];

@@ -200,10 +200,8 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_mixed(int nlocal,
                 m       = m < e.nr - 1 ? m : e.nr - 1;
                 p -= (float)m;
                 p              = p < 1.0f ? p : 1.0f;
-                const float4 a = __ldg(reinterpret_cast<const float4*>(e.rhor32 + 8 * m) + 0);
-                const float4 b = __ldg(reinterpret_cast<const float4*>(e.rhor32 + 8 * m) + 1);
-                // coefficients 3..6 are a.w, b.x, b.y, b.z
-                rhoi += (double)__fmaf_rn(__fmaf_rn(__fmaf_rn(a.w, p, b.x), p, b.y), p, b.z);
+                const float4 a = __ldg(e.dens32 + m); // coefficients 3..6
+                rhoi += (double)__fmaf_rn(__fmaf_rn(__fmaf_rn(a.x, p, a.y), p, a.z), p, a.w);
                 __stcg(out + (size_t)c * ld, en);
                 c++;
             }
@@ -275,6 +273,7 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_mixed(int nlocal,
         const int* nb   = cut + i;
         const float fpi = pi.w;
         const float rdr = (float)e.rdr;
+        const float rdr2 = 2.0f * rdr;
         float fix = 0.f, fiy = 0.f, fiz = 0.f;
         float cx = 0.f, cy = 0.f, cz = 0.f; // compensation terms
         auto acc = [&](float& s, float& c, float d, float f) {
@@ -299,12 +298,13 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_mixed(int nlocal,
             m               = m < e.nr - 1 ? m : e.nr - 1;
             p -= (float)m;
             p               = p < 1.0f ? p : 1.0f;
-            const float4 r0 = __ldg(reinterpret_cast<const float4*>(e.rhor32 + 8 * m));
-            const float4 z0 = __ldg(reinterpret_cast<const float4*>(e.z2r32 + 8 * m) + 0);
-            const float4 z1 = __ldg(reinterpret_cast<const float4*>(e.z2r32 + 8 * m) + 1);
-            float rhoip = __fmaf_rn(__fmaf_rn(r0.x, p, r0.y), p, r0.z);
-            float z2p   = __fmaf_rn(__fmaf_rn(z0.x, p, z0.y), p, z0.z);
-            float z2    = __fmaf_rn(__fmaf_rn(__fmaf_rn(z0.w, p, z1.x), p, z1.y), p, z1.z);
+            // z2r coefficients 3..6, then rho 0..2 and z2r 0; z2r 1 and 2 are
+            // 2 c4 / dr and c5 / dr (spline7's derivative rows)
+            const float4 za = __ldg(e.pair32 + 2 * m);
+            const float4 rb = __ldg(e.pair32 + 2 * m + 1);
+            float rhoip = __fmaf_rn(__fmaf_rn(rb.x, p, rb.y), p, rb.z);
+            float z2p   = __fmaf_rn(__fmaf_rn(rb.w, p, za.y * rdr2), p, za.z * rdr);
+            float z2    = __fmaf_rn(__fmaf_rn(__fmaf_rn(za.x, p, za.y), p, za.z), p, za.w);
             float recip = __fdividef(1.0f, r);
             float phi   = z2 * recip;
             float phip  = __fmaf_rn(z2p, recip, -phi * recip);

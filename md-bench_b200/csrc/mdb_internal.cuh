@@ -97,8 +97,12 @@ struct EamDev {
     const double* rhor;
     const double* z2r;
     const float* frho32;
-    const float* rhor32;
-    const float* z2r32;
+    // mixed path, FP32 rows: dens32[m] = rho coefficients 3..6 (the density
+    // pass); pair32[2m], pair32[2m + 1] = z2r coefficients 3..6, then rho
+    // coefficients 0..2 and z2r coefficient 0 (the force pass: z2r 1 and 2
+    // are 2 c4 / dr and c5 / dr of the spline, formed in the kernel)
+    const float4* dens32;
+    const float4* pair32;
 };
 
 namespace mdb {

@@ -277,6 +277,7 @@ class MdbEngine:
         torch = self.torch
         d_idx = torch.as_tensor(np.ascontiguousarray(idx, dtype=np.int32), device="cuda")
         out = torch.empty((len(idx), 3), dtype=torch.float64, device="cuda")
+        torch.cuda.current_stream().synchronize()  # d_idx lands on torch's stream
         self.sys.gather_positions(d_idx.data_ptr(), len(idx), (0.0, 0.0, sz), out.data_ptr())
         self.sys.synchronize()
         return out
@@ -284,6 +285,9 @@ class MdbEngine:
     def set_halo_positions(self, recv):
         torch = self.torch
         buf = torch.cat([r.to("cuda") for r in recv]).contiguous()
+        # the received rows and buf come from torch's stream (NCCL receives
+        # complete there asynchronously); the context reads buf on its own
+        torch.cuda.current_stream().synchronize()
         self.sys.set_halo_positions(buf.data_ptr(), buf.shape[0])
         self.sys.update_pbc()
         self.sys.synchronize()
