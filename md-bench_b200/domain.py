@@ -203,7 +203,9 @@ class SlabRun:
         x = self.sl.wrap(x)
         dest = self.sl.owner(x[:, 2])
         stay = dest == self.sl.rank
-        go_down, go_up = dest == self.below, (dest == self.above) & (dest != self.below)
+        # one rank is its own neighbour: nothing leaves
+        go_down = (dest == self.below) & ~stay
+        go_up = (dest == self.above) & (dest != self.below) & ~stay
         if not np.all(stay | go_down | go_up):
             raise RuntimeError("an atom moved past a whole slab in one rebuild period")
         rows = np.column_stack([x, v, t.astype(np.float64), self.gid.astype(np.float64)])

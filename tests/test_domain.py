@@ -206,6 +206,38 @@ def test_two_slabs_bit_identical_to_one_domain():
     assert T == pytest.approx(float(np.sum(V * V)) / (3 * n - 3), rel=1e-14)
 
 
+def test_one_slab_is_its_own_neighbour():
+    """One rank: the halo is the slab's own z images (shifted by the box
+    length both ways), exchanged with itself through host queues; atoms never
+    leave. Bit-identical to the undivided periodic run, across two rebuilds."""
+    sys.path[:0] = [os.path.join(ROOT, "md-bench_b200")]
+    import domain as D
+    hp, x, v, t = initial_state()
+    box = (hp.xprd, hp.yprd, hp.zprd)
+    eng = NumpyLJ(box, hp.cutforce, hp.cutneigh, hp.dt, hp.dtforce, periodic_z=False)
+    run = D.SlabRun(D.Slabs(box, hp.cutneigh, 1, 0),
+                    D.ThreadTransport(D.ThreadTransport.Hub(1), 0), eng, EVERY)
+    run.start(x, v, t, np.arange(len(t)))
+    run.run(STEPS + EVERY)
+    g, xs, vs, fs = run.gather()
+    assert len(g) == len(t) and np.array_equal(np.sort(g), np.arange(len(t)))
+    ref = NumpyLJ(box, hp.cutforce, hp.cutneigh, hp.dt, hp.dtforce, periodic_z=True)
+    sl = D.Slabs(box, hp.cutneigh, 1, 0)
+    gid = np.arange(len(t))
+    ref.load(sl.wrap(x), v, t, np.zeros((0, 3)), np.zeros(0, np.int32), (gid, gid[:0]))
+    for n in range(STEPS + EVERY):
+        ref.initial_integrate()
+        if (n + 1) % EVERY == 0:
+            ref.load(sl.wrap(ref.x), ref.v, ref.t, np.zeros((0, 3)), np.zeros(0, np.int32),
+                     (gid, gid[:0]))
+        else:
+            ref.force()
+        ref.final_integrate()
+    order = np.argsort(g)
+    assert np.array_equal(xs[order], ref.x) and np.array_equal(vs[order], ref.v)
+    assert np.array_equal(fs[order], ref.f)
+
+
 def test_slab_geometry_and_halo_plan():
     sys.path[:0] = [os.path.join(ROOT, "md-bench_b200")]
     import domain as D
