@@ -256,6 +256,7 @@ class MdbEngine:
         self.torch, self.mdb, self.hp = torch, mdb, hp
         self.device, self.precision = device, precision
         self.sys = None
+        self._idx = {}  # device copies of the halo index arrays, per load
 
     def load(self, x, v, t, hx, ht, ids=None):
         torch, mdb = self.torch, self.mdb
@@ -269,6 +270,7 @@ class MdbEngine:
         ta = np.concatenate([t, ht]).astype(np.int32) if nh else t.astype(np.int32)
         self.sys.set_atoms(xa, va, ta)
         self.sys.set_owned(n)
+        self._idx = {}
         self.n, self.nh = n, nh
         self.sys.setup_pbc()
         self.sys.update_pbc()
@@ -277,9 +279,14 @@ class MdbEngine:
 
     def positions(self, idx, sz):
         torch = self.torch
-        d_idx = torch.as_tensor(np.ascontiguousarray(idx, dtype=np.int32), device="cuda")
+        # the same index arrays serve every step of a rebuild period
+        key = id(idx)
+        if key not in self._idx:
+            d = torch.as_tensor(np.ascontiguousarray(idx, dtype=np.int32), device="cuda")
+            self._idx[key] = (idx, d)
+        d_idx = self._idx[key][1]
         out = torch.empty((len(idx), 3), dtype=torch.float64, device="cuda")
-        torch.cuda.current_stream().synchronize()  # d_idx lands on torch's stream
+        torch.cuda.current_stream().synchronize()  # d_idx and out come from torch's stream
         self.sys.gather_positions(d_idx.data_ptr(), len(idx), (0.0, 0.0, sz), out.data_ptr())
         self.sys.synchronize()
         return out

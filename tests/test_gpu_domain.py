@@ -87,6 +87,35 @@ def test_two_slab_contexts_match_one(precision):
         assert out[0][-1] == pytest.approx(T, rel=1e-4)
 
 
+def test_one_slab_context_matches_undivided():
+    """One rank: the slab context's halo is its own z images, refreshed every
+    step through host queues; across two rebuilds it follows the periodic
+    context (FP64: same pairs, summation order differs at the box faces)."""
+    torch = pytest.importorskip("torch")
+    import domain as D
+    hp = mdb.host_params(nx=CELLS, ny=CELLS, nz=CELLS)
+    x, v, t = mdb.create_fcc(hp)
+    n = len(t)
+    one = mdb.system_from_host(hp, n, precision="fp64")
+    one.set_atoms(x, v, t)
+    one.setup()
+    for k in range(45):
+        one.step(k)
+    X, V, F, _ = one.atoms()
+    box = np.array([hp.xprd, hp.yprd, hp.zprd])
+    eng = D.MdbEngine(torch, mdb, hp, 0, "fp64")
+    run = D.SlabRun(D.Slabs(box, hp.cutneigh, 1, 0),
+                    D.ThreadTransport(D.ThreadTransport.Hub(1), 0), eng, hp.reneigh_every)
+    run.start(x, v, t, np.arange(n))
+    run.run(45)
+    g, xs, vs, fs = run.gather()
+    assert eng.n == n and np.array_equal(np.sort(g), np.arange(n))
+    d = np.abs((xs - X[g] + 0.5 * box) % box - 0.5 * box)
+    assert d.max() < 1e-10
+    assert np.abs(vs - V[g]).max() < 1e-10
+    assert np.abs(fs - F[g]).max() <= 1e-9 * scale(F)
+
+
 def test_halo_entry_points_reject_bad_use():
     torch = pytest.importorskip("torch")
     hp = mdb.host_params(nx=4, ny=4, nz=4, half_neigh=1)
