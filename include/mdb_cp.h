@@ -54,7 +54,8 @@ int mdb_cp_synchronize(MdbCp* ctx);
  * multiple of 32; default 128); "force_variant" = 0..3: 0 and 1 prefetch the
  * j data one or two list blocks ahead with no register budget, 2 and 3 the same
  * with a budget for 8 resident blocks of 128 threads per SM (these run blocks
- * of 128 threads; default 2; with force_cpw > 1, 1 and 3 run as 0 and 2);
+ * of 128 threads; default 2; with force_cpw > 1 the prefetch is one block,
+ * 1 runs as 0 and 3 asks a budget for 6 blocks instead of 8);
  * "force_swizzle" = 1: the blocks one resident
  * slot runs in turn take neighbouring i-clusters (L1 reuse of j data; default
  * 0, measured within 2 % either way); "force_path" (mixed contexts) = 0: the

@@ -37,10 +37,10 @@ DEFAULT = {"cluster_n": 4, "half": 1, "force_block": 128, "force_variant": 2, "f
 
 def valid(choice):
     """force_cpw 8 needs 4x4 clusters; several clusters per warp prefetch one
-    block ahead (variants 1 and 3 run as 0 and 2 there)."""
+    block ahead (variant 1 runs as 0 there; 3 is a budget for 6 blocks)."""
     if choice.get("force_cpw", 1) == 8 and choice["cluster_n"] != 4:
         return False
-    return not (choice.get("force_cpw", 1) > 1 and choice.get("force_variant", 0) in (1, 3))
+    return not (choice.get("force_cpw", 1) > 1 and choice.get("force_variant", 0) == 1)
 
 
 def size_class(natoms):

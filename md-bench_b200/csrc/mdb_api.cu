@@ -61,10 +61,7 @@ struct MdbCtx {
     float4* bin_xf = nullptr; // the same rounded to FP32 (list build prefilter)
     int *bin_lcount = nullptr, *loc_start = nullptr; // locals per bin, their offsets
     int* local_order = nullptr; // local atoms bin by bin (the order sortAtom gives)
-    // the stencil as rows of consecutive x: {flat offset of the first bin,
-    // bins in the row}, in stencil order
-    std::vector<int2> rows;
-    int2* rows_d = nullptr;
+    int4* stencil_d  = nullptr;                      // {flat offset, dx, dy, dz}
     int *numneigh = nullptr, *neighbors = nullptr;
     int* counters = nullptr;
     int* scan_scratch = nullptr;
@@ -241,17 +238,6 @@ static int setup_bins(MdbCtx* ctx)
                 }
     g.nstencil = (int)ctx->stencil.size();
     if (g.nstencil > MDB_MAX_STENCIL) return fail(ctx, MDB_ERR_ARG, "stencil too large");
-    // bindist grows with |dx| in a row of fixed (dy, dz), so a row's stencil
-    // bins are consecutive in x
-    ctx->rows.clear();
-    for (size_t k = 0; k < ctx->stencil4.size(); k++) {
-        const int4 e = ctx->stencil4[k];
-        if (k > 0 && ctx->stencil4[k - 1].z == e.z && ctx->stencil4[k - 1].w == e.w &&
-            ctx->stencil4[k - 1].y + 1 == e.y)
-            ctx->rows.back().y++;
-        else
-            ctx->rows.push_back(make_int2(e.x, 1));
-    }
     g.xlo = fabs(0.0 - g.pad_x * g.binsizex) + 1e-9;
     g.ylo = fabs(0.0 - g.pad_y * g.binsizey) + 1e-9;
     g.zlo = fabs(0.0 - g.pad_z * g.binsizez) + 1e-9;
@@ -396,7 +382,7 @@ extern "C" int mdb_create(const MdbParams* params, MdbCtx** out)
             goto bad;
         }
         if ((e = dalloc(&ctx->counters, CNT_SLOTS)) != cudaSuccess ||
-            (e = dalloc(&ctx->rows_d, std::max((int)ctx->rows.size(), 1))) != cudaSuccess ||
+            (e = dalloc(&ctx->stencil_d, ctx->g.nstencil)) != cudaSuccess ||
             (e = dalloc(&ctx->bin_count, ctx->g.mbins)) != cudaSuccess ||
             (e = dalloc(&ctx->bin_start, ctx->g.mbins + 1)) != cudaSuccess ||
             (e = cudaMallocHost((void**)&ctx->h_counters, CNT_SLOTS * sizeof(int))) !=
@@ -410,9 +396,8 @@ extern "C" int mdb_create(const MdbParams* params, MdbCtx** out)
             goto bad;
         }
         cudaMemset(ctx->counters, 0, CNT_SLOTS * sizeof(int));
-        if (!ctx->rows.empty())
-            cudaMemcpy(ctx->rows_d, ctx->rows.data(), sizeof(int2) * ctx->rows.size(),
-                cudaMemcpyHostToDevice);
+        cudaMemcpy(ctx->stencil_d, ctx->stencil4.data(), sizeof(int4) * ctx->g.nstencil,
+            cudaMemcpyHostToDevice);
         if ((e = cudaGetLastError()) != cudaSuccess) {
             rc = fail(ctx, MDB_ERR_CUDA, "setup copy", e);
             goto bad;
@@ -469,7 +454,7 @@ extern "C" int mdb_destroy(MdbCtx* ctx)
     drop_graphs(ctx);
     free_atom_buffers(ctx);
     dfree(ctx->counters);
-    dfree(ctx->rows_d);
+    dfree(ctx->stencil_d);
     dfree(ctx->bin_count);
     dfree(ctx->bin_start);
     dfree(ctx->bin_lcount);
@@ -760,9 +745,8 @@ static void enq_list(MdbCtx* ctx)
         ctx->local_order);
     launch_bin_positions(s, ctx->nall_cap, ctx->g.mbins, ctx->x, ctx->bin_start, ctx->bin_atoms,
         ctx->bin_x, ctx->bin_xf);
-    launch_build_list(s, ctx->nlocal, ctx->g, (int)ctx->rows.size(), ctx->rows_d,
-        ctx->bin_start, ctx->loc_start, ctx->local_order, ctx->x, ctx->bin_x, ctx->bin_xf,
-        ctx->cutneighsq, ctx->list_margin,
+    launch_build_list(s, ctx->nlocal, ctx->x, ctx->g, ctx->stencil_d, ctx->atom_bin,
+        ctx->bin_start, ctx->bin_x, ctx->bin_xf, ctx->cutneighsq, ctx->list_margin,
         ctx->p.half_neigh, ctx->maxneighs, ctx->ld, ctx->neighbors, ctx->numneigh,
         ctx->counters, ctx->mixed ? ctx->qcell : nullptr);
 }

@@ -532,14 +532,17 @@ static void run_mixed_batch(cudaStream_t s, int nblocks, const CpForceMember* ta
         ty, cutforcesq)
     const int v = ty.force_variant;
     if (ty.force_cpw == 2) {
-        if (v & 2) CP_RUN(1, 8, 2);
+        if (v == 3) CP_RUN(1, 6, 2);
+        else if (v & 2) CP_RUN(1, 8, 2);
         else CP_RUN(1, 0, 2);
     } else if (ty.force_cpw == 4) {
-        if (v & 2) CP_RUN(1, 8, 4);
+        if (v == 3) CP_RUN(1, 6, 4);
+        else if (v & 2) CP_RUN(1, 8, 4);
         else CP_RUN(1, 0, 4);
     } else if (ty.force_cpw == 8) {
         if constexpr (N == 4) {
-            if (v & 2) CP_RUN(1, 8, 8);
+            if (v == 3) CP_RUN(1, 6, 8);
+            else if (v & 2) CP_RUN(1, 8, 8);
             else CP_RUN(1, 0, 8);
         }
     } else {
@@ -597,7 +600,8 @@ static void run_mixed(cudaStream_t s, int blocks, const int* cnt, const float4* 
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         }
-        const int per_sm = (v & 2) ? 8 : std::max(1, 2048 / nt);
+        const int per_sm =
+            (v & 2) ? ((v == 3 && ty.force_cpw > 1) ? 6 : 8) : std::max(1, 2048 / nt);
         slots            = nsm * per_sm;
         if (nb > slots) nb = (nb + slots - 1) / slots * slots;
         else slots = 0;
@@ -605,17 +609,21 @@ static void run_mixed(cudaStream_t s, int blocks, const int* cnt, const float4* 
 #define CP_RUN(PF, MB, C)                                                                \
     k_force_mixed<N, HALF, ENERGY, UNIFORM, PF, MB, C><<<nb, nt, 0, s>>>(cnt, xr, anchor, ty, \
         cutforcesq, list, ks, cs, numneigh, cf32, epart, slots)
-    // several clusters per warp: prefetch depth 1 (bit 0 of the variant unused)
+    // several clusters per warp: prefetch depth 1; bit 0 of the variant
+    // lowers the register budget's block count from 8 to 6
     if (ty.force_cpw == 2) {
-        if (v & 2) CP_RUN(1, 8, 2);
+        if (v == 3) CP_RUN(1, 6, 2);
+        else if (v & 2) CP_RUN(1, 8, 2);
         else CP_RUN(1, 0, 2);
     } else if (ty.force_cpw == 4) {
-        if (v & 2) CP_RUN(1, 8, 4);
+        if (v == 3) CP_RUN(1, 6, 4);
+        else if (v & 2) CP_RUN(1, 8, 4);
         else CP_RUN(1, 0, 4);
     } else if (ty.force_cpw == 8) {
         // a segment of 4 lanes: one entry of a 4-wide j-cluster at a time
         if constexpr (N == 4) {
-            if (v & 2) CP_RUN(1, 8, 8);
+            if (v == 3) CP_RUN(1, 6, 8);
+            else if (v & 2) CP_RUN(1, 8, 8);
             else CP_RUN(1, 0, 8);
         }
     } else {

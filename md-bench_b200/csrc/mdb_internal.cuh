@@ -209,8 +209,8 @@ void launch_bin_positions(cudaStream_t s, int nall_cap, int mbins, const double4
     const int* bin_start, const int* bin_atoms, double4* bin_x, float4* bin_xf);
 // the Verlet list from the bin-ordered positions; margin bounds the FP32
 // prefilter's rsq error (only candidates within it take the exact FP64 test)
-void launch_build_list(cudaStream_t s, int nlocal, BinGeom g, int nrows, const int2* rows,
-    const int* bin_start, const int* loc_start, const int* local_order, const double4* x,
+void launch_build_list(cudaStream_t s, int nlocal, const double4* x, BinGeom g,
+    const int4* stencil, const int* atom_bin, const int* bin_start,
     const double4* bin_x, const float4* bin_xf, double cutneighsq, float margin, int half,
     int maxneighs, int ld, int* neighbors, int* numneigh, int* counters, const int* qcell);
 int ke_partial_blocks(int n);

@@ -481,8 +481,15 @@ void launch_bin_sort(cudaStream_t s, int mbins, const int* bin_start, int* bin_a
 }
 
 // ---- list build: buildNeighborCPU, verletlist/neighbor.c:260-352 -------------
-// Positions in bin order (a bin's atoms in index order), FP64 and FP32, with
-// the atom index in .w: the build's candidates.
+// One thread per local atom i (atom order, so the k-major row writes of a warp
+// are coalesced). The stencil is walked in the reference order and each bin's
+// atoms in index order, so row i holds exactly the reference's neighbours of i
+// in the reference's order. A stencil bin is skipped when its box lies farther
+// than cutneigh from the atom (a lower bound on every distance to its atoms,
+// with a relative margin: skipping only removes candidates that would fail the
+// test). The candidate loop handles two candidates per iteration so their
+// loads overlap. On the mixed path each entry also carries the cell offset of
+// the pair (2 bits per axis, bits 26-31).
 __global__ void k_bin_positions(int mbins, const double4* __restrict__ x,
     const int* __restrict__ bin_start, const int* __restrict__ bin_atoms,
     double4* __restrict__ bin_x, float4* __restrict__ bin_xf)
@@ -503,161 +510,110 @@ void launch_bin_positions(cudaStream_t s, int nall_cap, int mbins, const double4
     g_launches++;
 }
 
-// One warp per bin, for the bin's local atoms (up to 32 at a time). Every
-// atom of a bin has the same stencil, whose bins form rows of consecutive x
-// (rows: {flat offset of the row's first bin, its bin count}, in stencil
-// order); a row's candidates are therefore one contiguous range of the
-// bin-ordered arrays, a bin's atoms in index order. The warp walks the
-// concatenated ranges 32 candidates at a time, lane = candidate, and tests
-// each candidate against every i atom of the group; a ballot per i atom then
-// appends the accepted candidates in candidate order, which is the
-// reference's order: stencil bins in order, atoms of a bin in index order
-// (buildNeighborCPU, verletlist/neighbor.c:260-352). The candidate loop is the
-// same for all lanes (no divergence but the short append), and the candidate
-// loads are coalesced. The FP32 copy decides every candidate whose FP32
-// distance lies more than `margin` (a bound on its rounding error) from
-// cutneigh^2; the few within it take the reference's exact FP64 test. On the
-// mixed path each entry also carries the cell offset of the pair (2 bits per
-// axis, bits 26-31).
-static constexpr int BL_WARPS = 4;
-
-__global__ void __launch_bounds__(32 * BL_WARPS) k_build_list(int mbins, int nrows,
-    const int2* __restrict__ rows, const int* __restrict__ bin_start,
-    const int* __restrict__ loc_start, const int* __restrict__ local_order,
-    const double4* __restrict__ x, const double4* __restrict__ bin_x,
+// Candidates come from the bin-ordered copies (a bin's atoms contiguous, in
+// index order): the FP32 copy decides every candidate whose FP32 distance lies
+// more than `margin` (a bound on its rounding error) from cutneigh^2; the few
+// within it take the reference's exact FP64 test on the FP64 copy. Accepted
+// sets and their order are therefore exactly the reference's.
+__global__ void __launch_bounds__(128) k_build_list(int nlocal, const double4* __restrict__ x,
+    BinGeom g, const int4* __restrict__ stencil, const int* __restrict__ atom_bin,
+    const int* __restrict__ bin_start, const double4* __restrict__ bin_x,
     const float4* __restrict__ bin_xf, double cutneighsq, float margin, int half,
     int maxneighs, int ld, int* __restrict__ neighbors, int* __restrict__ numneigh,
     int* __restrict__ counters, const int* __restrict__ qcell)
 {
-    __shared__ float4 s_xf[BL_WARPS][32]; // i atoms: FP32 position, index in .w
-    __shared__ double4 s_xd[BL_WARPS][32]; // FP64 positions (exact tests)
-    __shared__ int s_qi[BL_WARPS][32];
-    __shared__ int s_lo[BL_WARPS][32], s_st[BL_WARPS][32];
-    const int w    = threadIdx.x >> 5;
-    const int lane = threadIdx.x & 31;
-    const int b    = blockIdx.x * BL_WARPS + w;
-    if (b >= mbins) return;
-    const int l0 = __ldg(&loc_start[b]), nl = __ldg(&loc_start[b + 1]) - l0;
+    extern __shared__ int4 st[];
+    for (int k = threadIdx.x; k < g.nstencil; k += blockDim.x)
+        st[k] = stencil[k];
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nlocal) return;
+    const double4 xi = x[i];
+    const int ibin   = atom_bin[i];
+    const int qi     = qcell ? qcell[i] : 0;
+    const double ux  = (xi.x + g.xlo) * g.bininvx;
+    const double uy  = (xi.y + g.ylo) * g.bininvy;
+    const double uz  = (xi.z + g.zlo) * g.bininvz;
+    const float fx   = (float)(ux - (double)(int)ux);
+    const float fy   = (float)(uy - (double)(int)uy);
+    const float fz   = (float)(uz - (double)(int)uz);
+    const float bx = (float)g.binsizex, by = (float)g.binsizey, bz = (float)g.binsizez;
+    const float skip2 = (float)cutneighsq * 1.0001f + 1e-4f;
+    const float xif = (float)xi.x, yif = (float)xi.y, zif = (float)xi.z;
     const float lo = (float)cutneighsq - margin, hi = (float)cutneighsq + margin;
-    const unsigned lt = (1u << lane) - 1u;
-    for (int g0 = 0; g0 < nl; g0 += 32) {
-        const int gn = nl - g0 < 32 ? nl - g0 : 32;
-        int n = 0, bad = 0, ia = -1; // lane a < gn: atom a's count and index
-        if (lane < gn) {
-            ia              = __ldg(&local_order[l0 + g0 + lane]);
-            const double4 p = x[ia];
-            s_xd[w][lane]   = p;
-            s_xf[w][lane]   = make_float4((float)p.x, (float)p.y, (float)p.z, __int_as_float(ia));
-            s_qi[w][lane]   = qcell ? qcell[ia] : 0;
+    int n = 0, bad = 0;
+
+    auto consider = [&](int m, const float4& c) {
+        const int j = __float_as_int(c.w);
+        if (j == i || (half && j < i)) return;
+        const float dx = xif - c.x, dy = yif - c.y, dz = zif - c.z;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 > hi) return;
+        if (r2 >= lo) {
+            // the reference's test, verletlist/neighbor.c:320-330
+            const double4 xj = ldg4(&bin_x[m]);
+            double delx      = xi.x - xj.x;
+            double dely      = xi.y - xj.y;
+            double delz      = xi.z - xj.z;
+            double rsq       = delx * delx + dely * dely + delz * delz;
+            if (!(rsq <= cutneighsq)) return;
         }
-        __syncwarp();
-        for (int r0 = 0; r0 < nrows; r0 += 32) {
-            // this block of rows: candidate ranges, flattened by a scan
-            int rlo = 0, rn = 0;
-            if (r0 + lane < nrows) {
-                // bins past either end of the grid hold no atoms
-                const int2 rw = __ldg(&rows[r0 + lane]);
-                const int b0  = max(b + rw.x, 0), b1 = min(b + rw.x + rw.y, mbins);
-                if (b1 > b0) {
-                    rlo = __ldg(&bin_start[b0]);
-                    rn  = __ldg(&bin_start[b1]) - rlo;
-                }
-            }
-            int incl = rn;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int t = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += t;
-            }
-            const int T   = __shfl_sync(0xffffffffu, incl, 31);
-            s_lo[w][lane] = rlo;
-            s_st[w][lane] = incl - rn;
-            __syncwarp();
-            for (int c0 = 0; c0 < T; c0 += 32) {
-                const int t = c0 + lane;
-                int m = 0, j = -1;
-                float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (t < T) {
-                    int u = 0, v = 31; // the last row whose range starts at or before t
-                    while (u < v) {
-                        const int mid = (u + v + 1) >> 1;
-                        if (s_st[w][mid] <= t) u = mid;
-                        else v = mid - 1;
-                    }
-                    m = s_lo[w][u] + (t - s_st[w][u]);
-                    c = __ldg(&bin_xf[m]);
-                    j = __float_as_int(c.w);
-                }
-                int qj = 0;
-                if (qcell && j >= 0) qj = __ldg(&qcell[j]);
-                for (int a = 0; a < gn; a++) {
-                    const float4 xi = s_xf[w][a];
-                    const int i     = __float_as_int(xi.w);
-                    bool ok         = j >= 0 && j != i && !(half && j < i);
-                    if (ok) {
-                        const float dx = xi.x - c.x, dy = xi.y - c.y, dz = xi.z - c.z;
-                        const float r2 = dx * dx + dy * dy + dz * dz;
-                        if (r2 > hi) ok = false;
-                        else if (r2 >= lo) {
-                            // the reference's test, verletlist/neighbor.c:320-330
-                            const double4 pi = s_xd[w][a];
-                            const double4 xj = ldg4(&bin_x[m]);
-                            double delx      = pi.x - xj.x;
-                            double dely      = pi.y - xj.y;
-                            double delz      = pi.z - xj.z;
-                            double rsq       = delx * delx + dely * dely + delz * delz;
-                            ok               = rsq <= cutneighsq;
-                        }
-                    }
-                    const unsigned bal = __ballot_sync(0xffffffffu, ok);
-                    if (bal) {
-                        const int na = __shfl_sync(0xffffffffu, n, a);
-                        if (ok) {
-                            const int p = na + __popc(bal & lt);
-                            int e       = j;
-                            if (qcell) {
-                                const int qi = s_qi[w][a];
-                                int cx       = cell_axis(qj, 0) - cell_axis(qi, 0);
-                                int cy       = cell_axis(qj, 1) - cell_axis(qi, 1);
-                                int cz       = cell_axis(qj, 2) - cell_axis(qi, 2);
-                                if (cx < -1 || cx > 1 || cy < -1 || cy > 1 || cz < -1 || cz > 1)
-                                    bad = 1;
-                                int code = ((cx + 1) & 3) | (((cy + 1) & 3) << 2) |
-                                           (((cz + 1) & 3) << 4);
-                                e = j | (code << MDB_IDX_BITS);
-                            }
-                            if (p < maxneighs) neighbors[(size_t)p * ld + i] = e;
-                        }
-                        if (lane == a) n += __popc(bal);
-                    }
-                }
-            }
-            __syncwarp();
+        int e = j;
+        if (qcell) {
+            int qj = __ldg(&qcell[j]);
+            int cx = cell_axis(qj, 0) - cell_axis(qi, 0);
+            int cy = cell_axis(qj, 1) - cell_axis(qi, 1);
+            int cz = cell_axis(qj, 2) - cell_axis(qi, 2);
+            if (cx < -1 || cx > 1 || cy < -1 || cy > 1 || cz < -1 || cz > 1) bad = 1;
+            int code = ((cx + 1) & 3) | (((cy + 1) & 3) << 2) | (((cz + 1) & 3) << 4);
+            e        = j | (code << MDB_IDX_BITS);
         }
-        // the stored count never exceeds the row capacity, so no consumer can
-        // read past the list; the true count of an overflowing row goes to
-        // the host, which grows the list and rebuilds before any force is
-        // computed
-        if (lane < gn) {
-            numneigh[ia] = n < maxneighs ? n : maxneighs;
-            if (n > maxneighs) atomicMax(&counters[CNT_MAXNEED], n);
+        if (n < maxneighs) neighbors[(size_t)n * ld + i] = e;
+        n++;
+    };
+
+    if (ibin >= 0) {
+        for (int k = 0; k < g.nstencil; k++) {
+            const int4 sk = st[k];
+            const int jbin = ibin + sk.x;
+            if (jbin < 0 || jbin >= g.mbins) continue;
+            float gx = sk.y > 0 ? (sk.y - fx) : (sk.y < 0 ? (fx - (sk.y + 1)) : 0.f);
+            float gy = sk.z > 0 ? (sk.z - fy) : (sk.z < 0 ? (fy - (sk.z + 1)) : 0.f);
+            float gz = sk.w > 0 ? (sk.w - fz) : (sk.w < 0 ? (fz - (sk.w + 1)) : 0.f);
+            gx *= bx;
+            gy *= by;
+            gz *= bz;
+            if (gx * gx + gy * gy + gz * gz > skip2) continue;
+            const int beg = __ldg(&bin_start[jbin]);
+            const int end = __ldg(&bin_start[jbin + 1]);
+            int m         = beg;
+            for (; m + 1 < end; m += 2) {
+                const float4 ca = __ldg(&bin_xf[m]);
+                const float4 cb = __ldg(&bin_xf[m + 1]);
+                consider(m, ca);
+                consider(m + 1, cb);
+            }
+            if (m < end) consider(m, __ldg(&bin_xf[m]));
         }
-        if (__any_sync(0xffffffffu, bad) && lane == 0) atomicAdd(&counters[CNT_BADCELL], 1);
-        __syncwarp();
     }
+    // the stored count never exceeds the row capacity, so no consumer can read
+    // past the list; the true count of an overflowing row goes to the host,
+    // which grows the list and rebuilds before any force is computed
+    numneigh[i] = n < maxneighs ? n : maxneighs;
+    if (n > maxneighs) atomicMax(&counters[CNT_MAXNEED], n);
+    if (bad) atomicAdd(&counters[CNT_BADCELL], 1);
 }
 
-void launch_build_list(cudaStream_t s, int nlocal, BinGeom g, int nrows, const int2* rows,
-    const int* bin_start, const int* loc_start, const int* local_order, const double4* x,
+void launch_build_list(cudaStream_t s, int nlocal, const double4* x, BinGeom g,
+    const int4* stencil, const int* atom_bin, const int* bin_start,
     const double4* bin_x, const float4* bin_xf, double cutneighsq, float margin, int half,
     int maxneighs, int ld, int* neighbors, int* numneigh, int* counters, const int* qcell)
 {
     if (nlocal <= 0) return;
-    // atoms outside the bin grid (reported by the binning) get empty rows
-    cudaMemsetAsync(numneigh, 0, sizeof(int) * nlocal, s);
-    k_build_list<<<(g.mbins + BL_WARPS - 1) / BL_WARPS, 32 * BL_WARPS, 0, s>>>(g.mbins, nrows,
-        rows, bin_start, loc_start, local_order, x, bin_x, bin_xf, cutneighsq, margin, half,
-        maxneighs, ld, neighbors, numneigh, counters, qcell);
+    size_t smem = sizeof(int4) * g.nstencil;
+    k_build_list<<<mdb_blocks(nlocal, 128), 128, smem, s>>>(nlocal, x, g, stencil, atom_bin,
+        bin_start, bin_x, bin_xf, cutneighsq, margin, half, maxneighs, ld, neighbors, numneigh,
+        counters, qcell);
     g_launches++;
 }
 
