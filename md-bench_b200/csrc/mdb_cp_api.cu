@@ -267,6 +267,10 @@ static int setup_types(MdbCp* ctx)
     // four i-clusters per warp: measured fastest on B200 at 1M atoms (4x4 and
     // 4x8, full and half; 170 us against 229 us per launch for one per warp)
     t.force_cpw     = 4;
+    // two j atoms per lane: 189 against 200 us per launch at 1M atoms for full
+    // lists, 167 against 163 us for half lists (their reactions take
+    // registers)
+    t.force_jpl     = ctx->p.half_neigh ? 1 : 2;
     t.eps0        = t.sqrt_eps[0] * t.sqrt_eps[0];
     t.sigma6_0 = t.sigma3[0] * t.sigma3[0];
     // the pair-list path's constants (geometric mixing, in FP64 then rounded)
@@ -312,6 +316,13 @@ extern "C" int mdb_cp_tune(MdbCp* ctx, const char* key, int value)
             return MDB_ERR_ARG;
         drop_graph(ctx);
         ctx->ty.force_cpw = value;
+        return MDB_OK;
+    }
+    if (!strcmp(key, "force_jpl")) {
+        // 2: single systems with force_cpw 4
+        if (value != 1 && value != 2) return MDB_ERR_ARG;
+        drop_graph(ctx);
+        ctx->ty.force_jpl = value;
         return MDB_OK;
     }
     if (!strcmp(key, "force_variant")) {

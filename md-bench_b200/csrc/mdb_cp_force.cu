@@ -250,8 +250,9 @@ __device__ __forceinline__ void mixed_entry(const IPack& ip, const float4& xj, f
 // anchor frame (the anchor difference is exact), its type bits in .w. Lanes
 // past the end of a row read the dummy j-cluster (padding at +1e18, anchor 0),
 // so no lane branches.
+template <int JPL>
 struct JEntry {
-    float4 x;
+    float4 x[JPL]; // atoms b0 .. b0 + JPL - 1 of the entry
     int cj;
 };
 
@@ -270,16 +271,20 @@ __device__ __forceinline__ void to_i_frame(float4& x, float ax, float ay, float 
 // AW (one atom type): the anchor travels in .w of the entry's slots 0..2 and
 // is applied when the entry is used (after its load has landed); otherwise
 // it is loaded here and applied at once.
-template <int N, bool AW>
-__device__ __forceinline__ JEntry load_entry(int cj, int b, const float4* __restrict__ xr,
+template <int N, bool AW, int JPL>
+__device__ __forceinline__ JEntry<JPL> load_entry(int cj, int b0, const float4* __restrict__ xr,
     const float4* __restrict__ anchor, const float4& ai)
 {
-    JEntry j;
+    JEntry<JPL> j;
     j.cj = cj;
-    j.x  = __ldg(&xr[cj * N + b]);
+#pragma unroll
+    for (int u = 0; u < JPL; u++)
+        j.x[u] = __ldg(&xr[cj * N + b0 + u]);
     if (!AW) {
         const float4 a = __ldg(&anchor[cj]);
-        to_i_frame(j.x, a.x, a.y, a.z, ai);
+#pragma unroll
+        for (int u = 0; u < JPL; u++)
+            to_i_frame(j.x[u], a.x, a.y, a.z, ai);
     }
     return j;
 }
@@ -305,17 +310,20 @@ __device__ __forceinline__ JEntry load_entry(int cj, int b, const float4* __rest
 // of 128 threads per SM asked of the register allocator (0: no request; 8
 // caps a thread at 64 registers, measured best against 6, 7, 9 and 10).
 // Both are launch-shape choices of the autotuner; results do not depend on them.
+// JPL: j atoms per lane (consecutive atoms of one entry; 2 shares a lane's
+// list handling, anchor and loop work between two atoms).
 // The work of block bid (warps x CPW = i-clusters); s_se / s_s3: the type
 // tables in shared memory.
-template <int N, bool HALF, bool ENERGY, bool UNIFORM, int PF, int CPW>
+template <int N, bool HALF, bool ENERGY, bool UNIFORM, int PF, int CPW, int JPL>
 __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict__ cnt,
     const float4* __restrict__ xr, const float4* __restrict__ anchor, const Types& ty,
     float cutforcesq, const int* __restrict__ list, int ks, int cs,
     const int* __restrict__ numneigh, float4* cf32, double* epart, const float* s_se,
     const float* s_s3)
 {
-    constexpr int L   = 32 / CPW; // lanes per i-cluster
-    constexpr int JPW = L / N;    // entries per segment iteration
+    constexpr int L   = 32 / CPW;  // lanes per i-cluster
+    constexpr int LPE = N / JPL;   // lanes per list entry
+    constexpr int JPW = L / LPE;   // entries per segment iteration
     static_assert(JPW >= 1, "a segment holds at least one list entry");
     const int lane = threadIdx.x & 31;
     const int l    = lane & (L - 1);
@@ -362,28 +370,33 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
         const float sig6u = (float)ty.sigma6_0;
         const f2 A2 = f2_pack(cA, cA), mB2 = f2_pack(-cB, -cB);
         f2 fx[2] = {0, 0}, fy[2] = {0, 0}, fz[2] = {0, 0};
-        const int eidx = l / N, b = l - eidx * N;
+        const int eidx = l / LPE, bq = l - eidx * LPE, b0 = bq * JPL;
         // pairs of the diagonal entry (cj == ci_cj0) excluded as the
         // reference's cond (clusterpair/force_lj.c:108-123): the self pair, and
         // for half lists every pair with the i atom at or after the j atom
-        unsigned diag_excl = 0;
+        unsigned diag_excl[JPL];
 #pragma unroll
-        for (int a = 0; a < 4; a++)
-            if (HALF ? (ai0 + a >= b) : (ai0 + a == b)) diag_excl |= 1u << a;
+        for (int u = 0; u < JPL; u++) {
+            diag_excl[u] = 0;
+#pragma unroll
+            for (int a = 0; a < 4; a++)
+                if (HALF ? (ai0 + a >= b0 + u) : (ai0 + a == b0 + u)) diag_excl[u] |= 1u << a;
+        }
         const int nn    = act ? numneigh[ci] : 0;
         const int dummy = cnt[CP_NCJ] + cnt[CP_NGC]; // the dummy j-cluster
         const int* row  = list + (size_t)cic * cs;
         int lst_cur = l < nn ? __ldg(&row[(size_t)l * ks]) : dummy;
         int lst_nxt = L + l < nn ? __ldg(&row[(size_t)(L + l) * ks]) : dummy;
-        JEntry cur  = load_entry<N, UNIFORM>(__shfl_sync(0xffffffffu, lst_cur, eidx, L), b, xr,
-             anchor, ai);
-        JEntry nx1;
+        JEntry<JPL> cur = load_entry<N, UNIFORM, JPL>(
+            __shfl_sync(0xffffffffu, lst_cur, eidx, L), b0, xr, anchor, ai);
+        JEntry<JPL> nx1;
         if (PF == 2) {
             const int c1 = __shfl_sync(0xffffffffu, lst_cur, JPW + eidx, L);
-            nx1          = load_entry<N, UNIFORM>(JPW < nn ? c1 : dummy, b, xr, anchor, ai);
+            nx1 = load_entry<N, UNIFORM, JPL>(JPW < nn ? c1 : dummy, b0, xr, anchor, ai);
         }
-        // one segment iteration: JPW entries, lane (eidx, b) on atom b of
-        // entry kb + eidx; masked: the iteration may hold the diagonal entry
+        // one segment iteration: JPW entries, lane (eidx, bq) on atoms b0 ..
+        // b0 + JPL - 1 of entry kb + eidx; masked: the iteration may hold the
+        // diagonal entry
         auto step = [&](int kb, bool masked) {
             // the entry block holding kn is rotated in when kn reaches it
             const int kn = kb + PF * JPW;
@@ -391,41 +404,48 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
                 lst_cur = lst_nxt;
                 lst_nxt = kn + L + l < nn ? __ldg(&row[(size_t)(kn + L + l) * ks]) : dummy;
             }
-            const int cjn   = __shfl_sync(0xffffffffu, lst_cur, (kn & (L - 1)) + eidx, L);
-            const JEntry nx = load_entry<N, UNIFORM>(kn < nn ? cjn : dummy, b, xr, anchor, ai);
-            const int cj    = cur.cj;
-            float4 xj       = cur.x;
+            const int cjn = __shfl_sync(0xffffffffu, lst_cur, (kn & (L - 1)) + eidx, L);
+            const JEntry<JPL> nx =
+                load_entry<N, UNIFORM, JPL>(kn < nn ? cjn : dummy, b0, xr, anchor, ai);
+            const int cj = cur.cj;
+            float ax = 0.f, ay = 0.f, az = 0.f;
             if (UNIFORM) {
-                // the anchor of this entry's j-cluster from .w of its slots 0..2
-                const int base = lane - b;
-                const float ax = __shfl_sync(0xffffffffu, xj.w, base);
-                const float ay = __shfl_sync(0xffffffffu, xj.w, base + 1);
-                const float az = __shfl_sync(0xffffffffu, xj.w, base + 2);
-                to_i_frame(xj, ax, ay, az, ai);
+                // the anchor of this entry's j-cluster from .w of its slots
+                // 0..2, held by the entry's lanes JPL slots each
+                const int base = lane - bq;
+                ax = __shfl_sync(0xffffffffu, cur.x[0 % JPL].w, base + 0 / JPL);
+                ay = __shfl_sync(0xffffffffu, cur.x[1 % JPL].w, base + 1 / JPL);
+                az = __shfl_sync(0xffffffffu, cur.x[2 % JPL].w, base + 2 / JPL);
             }
-            float sej = 0.f, s3j = 0.f;
-            if (!UNIFORM) {
-                int t = __float_as_int(cur.x.w);
-                t     = t < 0 ? 0 : t;
-                sej   = s_se[t];
-                s3j   = s_s3[t];
-            }
-            f2 gx = 0, gy = 0, gz = 0;
-            // energy weight: full lists see every pair twice; half lists once,
-            // except pairs with ghost atoms, which both owners list
-            const double ew = (!HALF || cj * N + b >= nloc) ? 0.5 : 1.0;
-            mixed_entry<HALF, ENERGY, UNIFORM>(ip, xj, sej, s3j,
-                (masked && cj == ci_cj0) ? diag_excl : 0u, cutforcesq, A2, mB2, sig6u, ty.eps0,
-                ew, fx, fy, fz, gx, gy, gz, e);
-            // reactions on local j atoms only (the reference drops ghost
-            // reactions; the dummy cluster lies past the ghosts); padding j
-            // slots get exact zeros
-            if (HALF && cj * N + b < nloc) {
-                float gx0, gx1, gy0, gy1, gz0, gz1;
-                f2_unpack(gx, gx0, gx1);
-                f2_unpack(gy, gy0, gy1);
-                f2_unpack(gz, gz0, gz1);
-                red_add4(&cf32[cj * N + b], -(gx0 + gx1), -(gy0 + gy1), -(gz0 + gz1));
+#pragma unroll
+            for (int u = 0; u < JPL; u++) {
+                const int b = b0 + u;
+                float4 xj   = cur.x[u];
+                if (UNIFORM) to_i_frame(xj, ax, ay, az, ai);
+                float sej = 0.f, s3j = 0.f;
+                if (!UNIFORM) {
+                    int t = __float_as_int(cur.x[u].w);
+                    t     = t < 0 ? 0 : t;
+                    sej   = s_se[t];
+                    s3j   = s_s3[t];
+                }
+                f2 gx = 0, gy = 0, gz = 0;
+                // energy weight: full lists see every pair twice; half lists
+                // once, except pairs with ghost atoms, which both owners list
+                const double ew = (!HALF || cj * N + b >= nloc) ? 0.5 : 1.0;
+                mixed_entry<HALF, ENERGY, UNIFORM>(ip, xj, sej, s3j,
+                    (masked && cj == ci_cj0) ? diag_excl[u] : 0u, cutforcesq, A2, mB2, sig6u,
+                    ty.eps0, ew, fx, fy, fz, gx, gy, gz, e);
+                // reactions on local j atoms only (the reference drops ghost
+                // reactions; the dummy cluster lies past the ghosts); padding
+                // j slots get exact zeros
+                if (HALF && cj * N + b < nloc) {
+                    float gx0, gx1, gy0, gy1, gz0, gz1;
+                    f2_unpack(gx, gx0, gx1);
+                    f2_unpack(gy, gy0, gy1);
+                    f2_unpack(gz, gz0, gz1);
+                    red_add4(&cf32[cj * N + b], -(gx0 + gx1), -(gy0 + gy1), -(gz0 + gz1));
+                }
             }
             if (PF == 2) {
                 cur = nx1;
@@ -440,7 +460,7 @@ __device__ __forceinline__ void force_mixed_block(int bid, const int* __restrict
         const int nmax = CPW > 1 ? __reduce_max_sync(0xffffffffu, nn) : nn;
         if (nmax > 0) {
             step(0, true);
-#pragma unroll((HALF && CPW == 1) ? 1 : 2)
+#pragma unroll((HALF && (CPW == 1 || JPL == 2)) ? 1 : 2)
             for (int kb = JPW; kb < nmax; kb += JPW) step(kb, false);
         }
         float f[12];
@@ -480,7 +500,7 @@ __device__ __forceinline__ void load_type_tables(const Types& ty, float* s_se, f
 // (b % slots) * K + b / slots, so that the blocks one resident slot runs one
 // after another take neighbouring i-clusters, whose j data is then still in
 // that SM's L1 (blocks of a launch start in index order)
-template <int N, bool HALF, bool ENERGY, bool UNIFORM, int PF, int MINB, int CPW>
+template <int N, bool HALF, bool ENERGY, bool UNIFORM, int PF, int MINB, int CPW, int JPL>
 __global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_force_mixed(
     const int* __restrict__ cnt,
     const float4* __restrict__ xr, const float4* __restrict__ anchor, Types ty,
@@ -491,12 +511,12 @@ __global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_force_mix
     load_type_tables(ty, s_se, s_s3);
     int bid = blockIdx.x;
     if (slots > 0) bid = (blockIdx.x % slots) * (gridDim.x / slots) + blockIdx.x / slots;
-    force_mixed_block<N, HALF, ENERGY, UNIFORM, PF, CPW>(bid, cnt, xr, anchor, ty, cutforcesq,
+    force_mixed_block<N, HALF, ENERGY, UNIFORM, PF, CPW, JPL>(bid, cnt, xr, anchor, ty, cutforcesq,
         list, ks, cs, numneigh, cf32, epart, s_se, s_s3);
 }
 
 // all members of an ensemble group (same shape, list form, types and launch)
-template <int N, bool HALF, bool ENERGY, bool UNIFORM, int PF, int MINB, int CPW>
+template <int N, bool HALF, bool ENERGY, bool UNIFORM, int PF, int MINB, int CPW, int JPL>
 __global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_force_mixed_batch(
     const CpForceMember* __restrict__ tab, const int2* __restrict__ bmap, Types ty,
     float cutforcesq)
@@ -506,7 +526,7 @@ __global__ void __launch_bounds__(MINB ? 128 : 512, MINB ? MINB : 1) k_force_mix
     if (bm.x < 0) return; // an unused entry of a map sized for the capacities
     load_type_tables(ty, s_se, s_s3);
     const CpForceMember& m = tab[bm.x];
-    force_mixed_block<N, HALF, ENERGY, UNIFORM, PF, CPW>(bm.y, m.cnt, m.xr, m.anchor, ty, cutforcesq,
+    force_mixed_block<N, HALF, ENERGY, UNIFORM, PF, CPW, JPL>(bm.y, m.cnt, m.xr, m.anchor, ty, cutforcesq,
         m.list, 1, m.cs, m.numneigh, m.cf32, m.epart, s_se, s_s3);
 }
 
@@ -528,8 +548,8 @@ static void run_mixed_batch(cudaStream_t s, int nblocks, const CpForceMember* ta
 {
     const int nt = force_mixed_threads(ty);
 #define CP_RUN(PF, MB, C)                                                                \
-    k_force_mixed_batch<N, HALF, ENERGY, UNIFORM, PF, MB, C><<<nblocks, nt, 0, s>>>(tab, bmap, \
-        ty, cutforcesq)
+    k_force_mixed_batch<N, HALF, ENERGY, UNIFORM, PF, MB, C, 1><<<nblocks, nt, 0, s>>>(tab,   \
+        bmap, ty, cutforcesq)
     const int v = ty.force_variant;
     if (ty.force_cpw == 2) {
         if (v == 3) CP_RUN(1, 6, 2);
@@ -606,15 +626,19 @@ static void run_mixed(cudaStream_t s, int blocks, const int* cnt, const float4* 
         if (nb > slots) nb = (nb + slots - 1) / slots * slots;
         else slots = 0;
     }
-#define CP_RUN(PF, MB, C)                                                                \
-    k_force_mixed<N, HALF, ENERGY, UNIFORM, PF, MB, C><<<nb, nt, 0, s>>>(cnt, xr, anchor, ty, \
-        cutforcesq, list, ks, cs, numneigh, cf32, epart, slots)
+#define CP_RUN(PF, MB, C) CP_RUNJ(PF, MB, C, 1)
+#define CP_RUNJ(PF, MB, C, J)                                                            \
+    k_force_mixed<N, HALF, ENERGY, UNIFORM, PF, MB, C, J><<<nb, nt, 0, s>>>(cnt, xr, anchor, \
+        ty, cutforcesq, list, ks, cs, numneigh, cf32, epart, slots)
     // several clusters per warp: prefetch depth 1; bit 0 of the variant
     // lowers the register budget's block count from 8 to 6
     if (ty.force_cpw == 2) {
         if (v == 3) CP_RUN(1, 6, 2);
         else if (v & 2) CP_RUN(1, 8, 2);
         else CP_RUN(1, 0, 2);
+    } else if (ty.force_cpw == 4 && ty.force_jpl == 2) {
+        if (v & 2) CP_RUNJ(1, 8, 4, 2);
+        else CP_RUNJ(1, 0, 4, 2);
     } else if (ty.force_cpw == 4) {
         if (v == 3) CP_RUN(1, 6, 4);
         else if (v & 2) CP_RUN(1, 8, 4);
@@ -635,6 +659,7 @@ static void run_mixed(cudaStream_t s, int blocks, const int* cnt, const float4* 
         }
     }
 #undef CP_RUN
+#undef CP_RUNJ
 }
 
 template <int N, bool HALF>

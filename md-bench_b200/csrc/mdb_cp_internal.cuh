@@ -85,7 +85,8 @@ struct Types {
     int force_block;       // threads per block of the mixed force kernel (tunable)
     int force_variant;     // mixed force kernel: bit 0 prefetch 2 ahead, bit 1 register budget
     int force_swizzle;     // mixed force kernel: blocks walk contiguous cluster ranges (0/1)
-    int force_cpw;         // mixed force kernel: i-clusters per warp (1, 2, 4; single systems)
+    int force_cpw;         // mixed force kernel: i-clusters per warp (1, 2, 4, 8)
+    int force_jpl;         // mixed force kernel: j atoms per lane (1, or 2 with force_cpw 4)
     int pair_variant;      // pair-list force kernel: launch shape (0..3)
 };
 

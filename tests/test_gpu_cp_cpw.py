@@ -20,8 +20,9 @@ pytestmark = pytest.mark.gpu
 C5_TYPES = ([0.5, 1.5, 0.8, 1.2], [0.8, 1.2, 1.0, 0.9])
 
 
-def forces(s, cpw, energy=True):
+def forces(s, cpw, energy=True, jpl=1):
     s.tune("force_cpw", cpw)
+    s.tune("force_jpl", jpl)
     s.compute_force(energy=energy)
     return valid_forces(s), (s.thermo()["PE"] if energy else None)
 
@@ -32,10 +33,10 @@ def forces(s, cpw, energy=True):
 def test_cpw_matches_one_cluster_per_warp(N, half, types):
     s, _ = system(7, N, half, steps=120, types=types)
     f1, e1 = forces(s, 1)
-    for cpw in ((2, 4, 8) if N == 4 else (2, 4)):
-        f, e = forces(s, cpw)
+    for cpw, jpl in ((2, 1), (4, 1), (4, 2)) + (((8, 1),) if N == 4 else ()):
+        f, e = forces(s, cpw, jpl=jpl)
         r, m = rel(f, f1)
-        assert r <= SUM_ORDER and m <= 10 * SUM_ORDER, (cpw, r, m)
+        assert r <= SUM_ORDER and m <= 10 * SUM_ORDER, (cpw, jpl, r, m)
         assert e == pytest.approx(e1, rel=1e-6)
 
 
@@ -63,10 +64,10 @@ def test_cpw_against_fp64_oracle(half):
                           **common)
     s.set_atoms(x, v, t)
     s.setup()
-    for cpw in (2, 4, 8):
-        f, _ = forces(s, cpw, energy=False)
+    for cpw, jpl in ((2, 1), (4, 1), (4, 2), (8, 1)):
+        f, _ = forces(s, cpw, energy=False, jpl=jpl)
         r, m = rel(f, fo)
-        assert r <= MIXED_RMS and m <= 20 * MIXED_RMS, (cpw, r, m)
+        assert r <= MIXED_RMS and m <= 20 * MIXED_RMS, (cpw, jpl, r, m)
 
 
 def test_cpw_trajectory_tracks_one_cluster_per_warp():
