@@ -1787,7 +1787,8 @@ static bool same_types(const Types& a, const Types& b)
 {
     if (a.ntypes != b.ntypes || a.uniform != b.uniform || a.eps0 != b.eps0 ||
         a.sigma6_0 != b.sigma6_0 || a.force_block != b.force_block ||
-        a.force_variant != b.force_variant || a.force_cpw != b.force_cpw)
+        a.force_variant != b.force_variant || a.force_cpw != b.force_cpw ||
+        a.force_jpl != b.force_jpl)
         return false;
     for (int t = 0; t < MDB_MAX_TYPES; t++)
         if (a.sqrt_eps_f[t] != b.sqrt_eps_f[t] || a.sigma3_f[t] != b.sigma3_f[t]) return false;

@@ -547,11 +547,15 @@ static void run_mixed_batch(cudaStream_t s, int nblocks, const CpForceMember* ta
     const int2* bmap, const Types& ty, float cutforcesq)
 {
     const int nt = force_mixed_threads(ty);
-#define CP_RUN(PF, MB, C)                                                                \
-    k_force_mixed_batch<N, HALF, ENERGY, UNIFORM, PF, MB, C, 1><<<nblocks, nt, 0, s>>>(tab,   \
+#define CP_RUN(PF, MB, C) CP_RUNJ(PF, MB, C, 1)
+#define CP_RUNJ(PF, MB, C, J)                                                            \
+    k_force_mixed_batch<N, HALF, ENERGY, UNIFORM, PF, MB, C, J><<<nblocks, nt, 0, s>>>(tab,   \
         bmap, ty, cutforcesq)
     const int v = ty.force_variant;
-    if (ty.force_cpw == 2) {
+    if (ty.force_cpw == 4 && ty.force_jpl == 2) {
+        if (v & 2) CP_RUNJ(1, 8, 4, 2);
+        else CP_RUNJ(1, 0, 4, 2);
+    } else if (ty.force_cpw == 2) {
         if (v == 3) CP_RUN(1, 6, 2);
         else if (v & 2) CP_RUN(1, 8, 2);
         else CP_RUN(1, 0, 2);
@@ -574,6 +578,7 @@ static void run_mixed_batch(cudaStream_t s, int nblocks, const CpForceMember* ta
         }
     }
 #undef CP_RUN
+#undef CP_RUNJ
 }
 
 template <int N, bool HALF>
