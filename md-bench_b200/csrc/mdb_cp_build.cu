@@ -6,6 +6,7 @@
 // j-clusters in columns and of entries in the lists.
 #include <math.h>
 
+#include "mdb_cp_f2.cuh"
 #include "mdb_cp_internal.cuh"
 
 namespace mdb {
@@ -948,28 +949,39 @@ __device__ __noinline__ bool exact_box(const double4* __restrict__ imn_p,
     return d < cutsq;
 }
 
+// the i-cluster's 4 FP32 positions as packed pairs (atoms 0,1 and 2,3)
+struct IPairs {
+    f2 x[2], y[2], z[2];
+};
+
 // The reference's pair test decided in FP32 where the rounding margin allows
 // (some pair surely inside cutneigh, or every pair surely outside), else by
 // the exact FP64 test on the i-cluster's slots ci*M.. and the j-cluster's.
+// Two pairs per packed instruction; each squared distance rounds exactly as
+// (dx dx + dy dy) + dz dz in scalar FP32, and "some pair below lo" / "some pair
+// at or below hi" are decided on the smallest of them.
 template <int M, int N>
-__device__ __forceinline__ bool any_pair_f(const float3* xif, const float4* __restrict__ cjf,
+__device__ __forceinline__ bool any_pair_f(const IPairs& ip, const float4* __restrict__ cjf,
     float lo, float hi, const double4* __restrict__ ci_x, const double4* __restrict__ cj_x,
     double cutsq)
 {
-    bool sure = false, maybe = false;
+    static_assert(M == 4, "i-clusters of 4 atoms");
+    float mn = 3.0e38f;
 #pragma unroll
     for (int b = 0; b < N; b++) {
         const float4 xj = __ldg(&cjf[b]);
+        const f2 XJ = f2_pack(xj.x, xj.x), YJ = f2_pack(xj.y, xj.y), ZJ = f2_pack(xj.z, xj.z);
 #pragma unroll
-        for (int a = 0; a < M; a++) {
-            const float dx = xif[a].x - xj.x, dy = xif[a].y - xj.y, dz = xif[a].z - xj.z;
-            const float r2 = dx * dx + dy * dy + dz * dz;
-            sure |= r2 < lo;
-            maybe |= r2 <= hi;
+        for (int h = 0; h < 2; h++) {
+            const f2 dx = f2_sub(ip.x[h], XJ), dy = f2_sub(ip.y[h], YJ), dz = f2_sub(ip.z[h], ZJ);
+            const f2 r2 = f2_add(f2_add(f2_mul(dx, dx), f2_mul(dy, dy)), f2_mul(dz, dz));
+            float r0, r1;
+            f2_unpack(r2, r0, r1);
+            mn = fminf(mn, fminf(r0, r1));
         }
     }
-    if (sure) return true;
-    if (!maybe) return false;
+    if (mn < lo) return true;
+    if (!(mn <= hi)) return false;
     return exact_any_pair<M, N>(ci_x, cj_x, cutsq);
 }
 
@@ -997,6 +1009,13 @@ __device__ __forceinline__ void build_list_blk(int bid, int half, int* cnt, Geom
     for (int a = 0; a < M; a++) {
         const float4 p = cxf[ci * M + a];
         xif[a]         = make_float3(p.x, p.y, p.z);
+    }
+    IPairs ipf;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        ipf.x[h] = f2_pack(xif[2 * h].x, xif[2 * h + 1].x);
+        ipf.y[h] = f2_pack(xif[2 * h].y, xif[2 * h + 1].y);
+        ipf.z[h] = f2_pack(xif[2 * h].z, xif[2 * h + 1].z);
     }
     // FP32 decisions are taken only outside +-margin of the thresholds
     const float mg     = g.list_margin;
@@ -1060,7 +1079,7 @@ __device__ __forceinline__ void build_list_blk(int bid, int half, int* cnt, Geom
                             in_cut = exact_box(&ibbmin[ci], &ibbmax[ci], &jcbbmin[m],
                                 &jcbbmax[m], g.cutneighsq, g.rbb_sq, &in_rbb);
                         if (in_cut)
-                            ok = in_rbb || any_pair_f<M, N>(xif, cxf + (size_t)cj * N, cut_lo,
+                            ok = in_rbb || any_pair_f<M, N>(ipf, cxf + (size_t)cj * N, cut_lo,
                                                cut_hi, cx + (size_t)ci * M,
                                                cx + (size_t)cj * N, g.cutneighsq);
                     }
