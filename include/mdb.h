@@ -154,6 +154,12 @@ int mdb_sort_atoms(MdbCtx* ctx);
  * every step n with (n+1) % resort_every == 0 and rebuilds in that step.
  * 0 (the default, as SORT_ATOMS ?= false) disables. */
 int mdb_set_resort(MdbCtx* ctx, int resort_every);
+/* Launch tuning (no counterpart in the reference): "eam_rho_lanes" = 1 or 2
+ * lanes per atom in the mixed EAM density pass (2: the lanes take alternate
+ * list entries and append the in-cutoff ones in list order; the force pass
+ * reads the same rows either way, only the FP64 density sum's order
+ * changes). */
+int mdb_tune(MdbCtx* ctx, const char* key, int value);
 
 /* A caller-made neighbour list (row-major, row i = numneigh[i] local atom
  * indices, leading dimension ld) for the force kernels, with no ghosts, as the

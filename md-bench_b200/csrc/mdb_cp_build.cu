@@ -852,6 +852,7 @@ __device__ __forceinline__ double bb_axis(double imin, double imax, double jmin,
 // build (latency-bound: occupancy pays more than registers for its rare
 // exact fallbacks)
 #define CP_LIST_MINB 8
+#define CP_LIST_EXPAND 256
 
 // FP32 copies for the prefilter: thread t rounds slot t's position and, if t
 // is a column entry, that entry's box. Window table: entry q of column c
@@ -998,6 +999,9 @@ __device__ __forceinline__ void build_list_blk(int bid, int half, int* cnt, Geom
 {
     __shared__ int s_lo[CP_LIST_WARPS][32];
     __shared__ int s_ws[CP_LIST_WARPS][32];
+    // the flattened windows' column-list indices, when they fit (else each
+    // candidate finds its column by a binary search over s_ws)
+    __shared__ int s_m[CP_LIST_WARPS][CP_LIST_EXPAND];
     const int w    = threadIdx.x >> 5;
     const int ci   = (bid * blockDim.x + threadIdx.x) >> 5;
     const int lane = lane_id();
@@ -1051,19 +1055,28 @@ __device__ __forceinline__ void build_list_blk(int bid, int half, int* cnt, Geom
         const int W     = __shfl_sync(0xffffffffu, incl, 31);
         s_lo[w][lane]   = lo;
         s_ws[w][lane]   = incl - wn;
+        const bool expanded = W <= CP_LIST_EXPAND;
+        if (expanded)
+            for (int q = 0; q < wn; q++)
+                s_m[w][incl - wn + q] = lo + q;
         __syncwarp();
         for (int t0 = 0; t0 < W; t0 += 32) {
             const int t = t0 + lane;
             bool ok     = false;
             int cj      = -1;
             if (t < W) {
-                int a = 0, z = 31; // last column whose window starts at or before t
-                while (a < z) {
-                    int mid = (a + z + 1) >> 1;
-                    if (s_ws[w][mid] <= t) a = mid;
-                    else z = mid - 1;
+                int m;
+                if (expanded) {
+                    m = s_m[w][t];
+                } else {
+                    int a = 0, z = 31; // last column whose window starts at or before t
+                    while (a < z) {
+                        int mid = (a + z + 1) >> 1;
+                        if (s_ws[w][mid] <= t) a = mid;
+                        else z = mid - 1;
+                    }
+                    m = s_lo[w][a] + (t - s_ws[w][a]);
                 }
-                const int m = s_lo[w][a] + (t - s_ws[w][a]);
                 cj          = jcol[m];
                 if (!(half && ci_cj0 > cj)) {
                     const float4 fn = __ldg(&jcbbf[2 * m]), fx = __ldg(&jcbbf[2 * m + 1]);

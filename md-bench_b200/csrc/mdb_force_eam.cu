@@ -243,6 +243,103 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_mixed(int nlocal,
     }
 }
 
+// The density pass with two lanes per atom (lanes 2q and 2q + 1 of a warp on
+// atom 16 w + q): the lanes take list entries k and k + 1 of each pair and
+// append the in-cutoff ones to cut in list order (the lower lane's first), so
+// the force pass reads the same rows as after the one-lane pass; the two FP64
+// partial densities are added at the end. Twice the warps of the one-lane pass
+// keep more gathers in flight on a 131k-atom system. Blocks of 2 x EAM_THREADS
+// threads cover the same EAM_THREADS atoms as a block of the one-lane pass, so
+// both write the same energy partials.
+template <bool ENERGY>
+__global__ void __launch_bounds__(2 * EAM_THREADS) k_eam_rho_mixed2(int nlocal,
+    const float4* __restrict__ xr, CellShift sh, const int* __restrict__ numneigh,
+    const int* __restrict__ neighbors, int ld, float cutforcesq, EamDev e,
+    int* __restrict__ cut, int* __restrict__ ncut, double* __restrict__ fp,
+    float4* __restrict__ xe, double* __restrict__ epart)
+{
+    const float cg  = sh.g;
+    const int lane  = threadIdx.x & 31;
+    const int u     = lane & 1;
+    const int i     = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 16 + (lane >> 1);
+    const bool act  = i < nlocal;
+    const int ia    = act ? i : 0;
+    const float4 pi = act ? xr[ia] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const int n     = act ? numneigh[ia] : 0;
+    const int* nb   = neighbors + ia;
+    int* out        = cut + ia;
+    int c           = 0;     // entries appended so far (both lanes)
+    double rhoi     = 0.0;   // this lane's FP64 partial density
+    double eng      = 0.0;
+    const float rdr = (float)e.rdr;
+    const unsigned pairmask = 3u << (lane & ~1);
+    auto pair = [&](int en, const float4& pj, bool valid) {
+        bool in = false;
+        if (valid) {
+            float dx, dy, dz;
+            cell_delta(pi, pj, (unsigned)en >> MDB_IDX_BITS, cg, dx, dy, dz);
+            const float rsq = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
+            in              = rsq < cutforcesq;
+            if (in) {
+                float p = __fmaf_rn(sqrtf(rsq), rdr, 1.0f);
+                int m   = (int)p;
+                m       = m < e.nr - 1 ? m : e.nr - 1;
+                p -= (float)m;
+                p              = p < 1.0f ? p : 1.0f;
+                const float4 a = __ldg(e.dens32 + m); // coefficients 3..6
+                rhoi += (double)__fmaf_rn(__fmaf_rn(__fmaf_rn(a.x, p, a.y), p, a.z), p, a.w);
+            }
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, in) & pairmask;
+        if (in) __stcg(out + (size_t)(c + (u ? __popc(bal) - 1 : 0)) * ld, en);
+        c += __popc(bal);
+    };
+    // a warp runs as many pair steps as its longest row
+    int nmax = n;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
+    int k = 0;
+    for (; k + 2 * EUNROLL <= nmax; k += 2 * EUNROLL) {
+        int en[EUNROLL];
+        float4 pj[EUNROLL];
+#pragma unroll
+        for (int v = 0; v < EUNROLL; v++) {
+            const int kk = k + 2 * v + u;
+            en[v]        = kk < n ? __ldcs(nb + (size_t)kk * ld) : 0;
+        }
+#pragma unroll
+        for (int v = 0; v < EUNROLL; v++)
+            pj[v] = k + 2 * v + u < n ? __ldg(xr + (en[v] & MDB_IDX_MASK)) : pi;
+#pragma unroll
+        for (int v = 0; v < EUNROLL; v++)
+            pair(en[v], pj[v], k + 2 * v + u < n);
+    }
+    for (; k < nmax; k += 2) {
+        const bool valid = k + u < n;
+        const int en     = valid ? __ldcs(nb + (size_t)(k + u) * ld) : 0;
+        pair(en, valid ? __ldg(xr + (en & MDB_IDX_MASK)) : pi, valid);
+    }
+    rhoi += __shfl_xor_sync(0xffffffffu, rhoi, 1);
+    if (act && u == 0) {
+        ncut[i]  = c;
+        double p = 1.0 * rhoi * e.rdrho + 1.0;
+        int m    = (int)(p);
+        m        = m < e.nrho - 1 ? m : e.nrho - 1;
+        m        = m > 1 ? m : 1;
+        p -= m;
+        p                = p < 1.0 ? p : 1.0;
+        const double* cf = e.frho + 8 * m;
+        const double fpi = (__ldg(cf + 0) * p + __ldg(cf + 1)) * p + __ldg(cf + 2);
+        fp[i]            = fpi;
+        xe[i]            = make_float4(pi.x, pi.y, pi.z, (float)fpi);
+        if (ENERGY) eng = ((__ldg(cf + 3) * p + __ldg(cf + 4)) * p + __ldg(cf + 5)) * p + __ldg(cf + 6);
+    }
+    if (ENERGY) {
+        double s = block_sum(eng);
+        if (threadIdx.x == 0) epart[blockIdx.x] = s;
+    }
+}
+
 // F'(rho) of the ghosts from their owners (the mid-step halo of
 // computeForceEam, verletlist/force_eam.c:120-130), with their positions
 __global__ void k_eam_xe_ghost(int nlocal, const float4* __restrict__ xr,
@@ -376,7 +473,8 @@ void launch_eam_fp64(cudaStream_t s, int energy, int nlocal, int ghost_cap, cons
     g_launches++;
 }
 
-int launch_eam_mixed(cudaStream_t s, int energy, int comp, int nlocal, int ghost_cap,
+int launch_eam_mixed(cudaStream_t s, int energy, int comp, int rho_lanes, int nlocal,
+    int ghost_cap,
     const float4* xr, const CellShift& sh, const int* numneigh, const int* neighbors, int ld,
     float cutforcesq, EamDev eam, const int* border_map, const int* counters, int* cut,
     int* ncut, double* fp, float4* xe, double* fx, double* fy, double* fz, double* epart_rho,
@@ -384,7 +482,14 @@ int launch_eam_mixed(cudaStream_t s, int energy, int comp, int nlocal, int ghost
 {
     if (nlocal <= 0) return 0;
     const int nb = eam_mixed_blocks(nlocal);
-    if (energy)
+    if (rho_lanes == 2) {
+        if (energy)
+            k_eam_rho_mixed2<true><<<nb, 2 * EAM_THREADS, 0, s>>>(nlocal, xr, sh, numneigh,
+                neighbors, ld, cutforcesq, eam, cut, ncut, fp, xe, epart_rho);
+        else
+            k_eam_rho_mixed2<false><<<nb, 2 * EAM_THREADS, 0, s>>>(nlocal, xr, sh, numneigh,
+                neighbors, ld, cutforcesq, eam, cut, ncut, fp, xe, epart_rho);
+    } else if (energy)
         k_eam_rho_mixed<true><<<nb, EAM_THREADS, 0, s>>>(nlocal, xr, sh, numneigh, neighbors,
             ld, cutforcesq, eam, cut, ncut, fp, xe, epart_rho);
     else

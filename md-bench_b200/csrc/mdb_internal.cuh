@@ -234,7 +234,8 @@ void launch_eam_fp64(cudaStream_t s, int energy, int nlocal, int ghost_cap, cons
 // mixed EAM: four threads per atom; xe (nlocal + ghost_cap) receives
 // (position, F'(rho)) of every atom for the force pass; comp: two-sum
 // compensated force sums; returns the energy partials written per pass
-int launch_eam_mixed(cudaStream_t s, int energy, int comp, int nlocal, int ghost_cap,
+int launch_eam_mixed(cudaStream_t s, int energy, int comp, int rho_lanes, int nlocal,
+    int ghost_cap,
     const float4* xr, const CellShift& sh, const int* numneigh, const int* neighbors, int ld,
     float cutforcesq, EamDev eam, const int* border_map, const int* counters, int* cut,
     int* ncut, double* fp, float4* xe, double* fx, double* fy, double* fz, double* epart_rho,

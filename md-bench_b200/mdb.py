@@ -84,7 +84,7 @@ EXPORTS = [
     "mdb_get_positions_all", "mdb_get_ghosts", "mdb_get_neighbor_list",
     "mdb_get_bin_geometry", "mdb_get_eam_fp", "mdb_launch_count", "mdb_kinetic_sum_noalloc",
     "mdb_set_owned", "mdb_gather_positions", "mdb_set_halo_positions",
-    "mdb_sort_atoms", "mdb_set_resort", "mdb_set_neighbor_list",
+    "mdb_sort_atoms", "mdb_set_resort", "mdb_tune", "mdb_set_neighbor_list",
 ]
 # every symbol include/mdb_cp.h declares
 CP_EXPORTS = [
@@ -156,6 +156,7 @@ def load():
                  "mdb_sort_atoms"):
         sig[name] = ([vp], ip)
     sig["mdb_set_resort"] = ([vp, ip], ip)
+    sig["mdb_tune"] = ([vp, C.c_char_p, ip], ip)
     sig["mdb_set_neighbor_list"] = ([vp, _ip, _ip, ip], ip)
     sig.update({
         "mdb_cp_create": ([C.POINTER(MdbParams), ip, ip, C.POINTER(vp)], ip),
@@ -562,6 +563,10 @@ class System:
 
     def set_resort(self, every):
         self._ck(self.lib.mdb_set_resort(self.h, int(every)), "mdb_set_resort")
+
+    def tune(self, key, value):
+        """Launch tuning (``eam_rho_lanes``: 1 or 2)."""
+        self._ck(self.lib.mdb_tune(self.h, key.encode(), int(value)), "mdb_tune")
 
     def build_neighbor(self):
         self._ck(self.lib.mdb_build_neighbor(self.h), "mdb_build_neighbor")

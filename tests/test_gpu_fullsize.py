@@ -278,9 +278,11 @@ def test_c3_eam_copper_against_oracle():
 
 @pytest.mark.parametrize("precision", ["mixed", "mixed_comp"])
 def test_c3_eam_copper_mixed_against_oracle(precision):
-    """The mixed EAM passes (four threads per atom, F'(rho) gathered with the
-    position) on the copper state after 100 FP64 steps, against the oracle's
-    FP64 forces on the same state: within the mixed path's budget."""
+    """The mixed EAM passes (in-cutoff rows from the density pass, F'(rho)
+    gathered with the position) on the copper state after 100 FP64 steps,
+    against the oracle's FP64 forces on the same state: within the mixed
+    path's budget, with one and with two lanes per atom in the density pass
+    (the same rows; only the FP64 density sum's order differs)."""
     tab, hp, x, v, t = copper()
     s = mdb.system_from_host(hp, len(t), eam=tab)
     s.set_atoms(x, v, t)
@@ -296,9 +298,17 @@ def test_c3_eam_copper_mixed_against_oracle(precision):
     m = mdb.system_from_host(hp, len(t), eam=tab, precision=precision)
     m.set_atoms(xa, va, ta)
     m.setup()
-    assert rel_rms(m.atoms()[2], o.atoms()[2]) <= MIXED_RMS
+    f1 = m.atoms()[2]
+    assert rel_rms(f1, o.atoms()[2]) <= MIXED_RMS
     m.compute_force(energy=True)
     assert m.thermo()["PE"] == pytest.approx(o.thermo()["PE"], rel=1e-6)
+    m.tune("eam_rho_lanes", 2)
+    m.compute_force(energy=True)
+    assert m.thermo()["PE"] == pytest.approx(o.thermo()["PE"], rel=1e-6)
+    f2 = m.atoms()[2]
+    assert rel_rms(f2, f1) <= 1e-6 and rel_rms(f2, o.atoms()[2]) <= MIXED_RMS
+    with pytest.raises(mdb.MdbError):
+        m.tune("eam_rho_lanes", 3)
     m.close()
 
 
