@@ -158,7 +158,7 @@ int mdb_set_resort(MdbCtx* ctx, int resort_every);
  * lanes per atom in the mixed EAM density pass (2: the lanes take alternate
  * list entries and append the in-cutoff ones in list order; the force pass
  * reads the same rows either way, only the FP64 density sum's order
- * changes). */
+ * changes; default 1, measured faster at 131k atoms). */
 int mdb_tune(MdbCtx* ctx, const char* key, int value);
 
 /* A caller-made neighbour list (row-major, row i = numneigh[i] local atom
