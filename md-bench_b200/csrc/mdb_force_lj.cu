@@ -127,11 +127,7 @@ __global__ void __launch_bounds__(LJ_THREADS) k_lj_mixed(int nlocal,
 {
     __shared__ float s_eps[MDB_MAX_TYPES * MDB_MAX_TYPES];
     __shared__ float s_sig6[MDB_MAX_TYPES * MDB_MAX_TYPES];
-    // offset * G of every cell-offset code (2 bits per axis, bits 26-31 of an
-    // entry): one shared load per pair instead of decoding three fields. The
-    // products are exact, so (p_i - p_j) - offset * G rounds as cell_delta's
-    // fused form does.
-    __shared__ float4 s_off[64];
+    __shared__ float4 s_off[64]; // offset * G per cell-offset code
     const int nt = tab.ntypes;
     const float cg = sh.g;
     if (!UNIFORM) {
@@ -140,10 +136,7 @@ __global__ void __launch_bounds__(LJ_THREADS) k_lj_mixed(int nlocal,
             s_sig6[k] = tab.sig6[k];
         }
     }
-    for (int c = threadIdx.x; c < 64; c += blockDim.x)
-        s_off[c] = make_float4(cell_offset(c & 3u) * cg, cell_offset((c >> 2) & 3u) * cg,
-            cell_offset((c >> 4) & 3u) * cg, 0.f);
-    __syncthreads();
+    fill_offset_table(s_off, cg);
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double epot = 0.0;
     if (t < nlocal) {
@@ -170,11 +163,9 @@ __global__ void __launch_bounds__(LJ_THREADS) k_lj_mixed(int nlocal,
         };
 
         auto pair = [&](int e, const float4& pj) {
-            const int j    = e & MDB_IDX_MASK;
-            const float4 o = s_off[(unsigned)e >> MDB_IDX_BITS];
-            const float delx = (pi.x - pj.x) - o.x;
-            const float dely = (pi.y - pj.y) - o.y;
-            const float delz = (pi.z - pj.z) - o.z;
+            const int j = e & MDB_IDX_MASK;
+            float delx, dely, delz;
+            table_delta(pi, pj, (unsigned)e >> MDB_IDX_BITS, s_off, delx, dely, delz);
             float rsq = __fmaf_rn(delx, delx, __fmaf_rn(dely, dely, delz * delz));
             float sigma6 = sig0, epsilon = eps0;
             if (!UNIFORM) {
