@@ -91,7 +91,6 @@ struct MdbCtx {
     bool energy_valid = false;
     int resort_every  = 0; // SORT_ATOMS builds: sortAtom every resort_every steps
     int eam_rho_lanes = 1; // mixed EAM density pass: lanes per atom (1 or 2)
-    int eam_offsets   = 0; // mixed EAM: cell offsets from a shared table (bit 0 density, bit 1 force)
 };
 
 // ---------------------------------------------------------------------------
@@ -687,7 +686,7 @@ static void enq_force(MdbCtx* ctx, bool energy)
     if (ctx->p.force_field == MDB_FF_EAM) {
         if (ctx->mixed) {
             launch_eam_mixed(s, energy, ctx->p.precision == MDB_PREC_MIXED_COMP,
-                ctx->eam_rho_lanes, ctx->eam_offsets, n, ctx->ghost_cap, ctx->xr, ctx->shift, ctx->numneigh, ctx->neighbors, ctx->ld,
+                ctx->eam_rho_lanes, n, ctx->ghost_cap, ctx->xr, ctx->shift, ctx->numneigh, ctx->neighbors, ctx->ld,
                 (float)ctx->cutforcesq, ctx->eam, ctx->border_map, ctx->counters,
                 ctx->eam_cutlist, ctx->eam_ncut, ctx->fp, ctx->xe, ctx->fx, ctx->fy, ctx->fz, ep0,
                 ep1);
@@ -1128,12 +1127,6 @@ extern "C" int mdb_tune(MdbCtx* ctx, const char* key, int value)
         if (value != 1 && value != 2) return MDB_ERR_ARG;
         drop_graphs(ctx);
         ctx->eam_rho_lanes = value;
-        return MDB_OK;
-    }
-    if (!strcmp(key, "eam_offsets")) {
-        if (value < 0 || value > 3) return MDB_ERR_ARG;
-        drop_graphs(ctx);
-        ctx->eam_offsets = value;
         return MDB_OK;
     }
     return fail(ctx, MDB_ERR_ARG, "unknown tuning key");

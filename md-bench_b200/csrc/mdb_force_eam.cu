@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_fp64(int nlocal,
 // every entry of cut is inside the cutoff in the force pass too.
 int eam_mixed_blocks(int nlocal) { return mdb_blocks(nlocal, EAM_THREADS); }
 
-template <bool ENERGY, bool OT>
+template <bool ENERGY>
 __global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_mixed(int nlocal,
     const float4* __restrict__ xr, CellShift sh, const int* __restrict__ numneigh,
     const int* __restrict__ neighbors, int ld, float cutforcesq, EamDev e,
@@ -180,8 +180,6 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_mixed(int nlocal,
     float4* __restrict__ xe, double* __restrict__ epart)
 {
     const float cg = sh.g;
-    __shared__ float4 s_off[64]; // offset * G per cell-offset code (OT)
-    if (OT) fill_offset_table(s_off, cg);
     const int i    = blockIdx.x * blockDim.x + threadIdx.x;
     double eng     = 0.0;
     if (i < nlocal) {
@@ -194,8 +192,7 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_mixed(int nlocal,
         const float rdr = (float)e.rdr;
         auto pair       = [&](int en, const float4& pj) {
             float dx, dy, dz;
-            if (OT) table_delta(pi, pj, (unsigned)en >> MDB_IDX_BITS, s_off, dx, dy, dz);
-            else cell_delta(pi, pj, (unsigned)en >> MDB_IDX_BITS, cg, dx, dy, dz);
+            cell_delta(pi, pj, (unsigned)en >> MDB_IDX_BITS, cg, dx, dy, dz);
             float rsq = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
             if (rsq < cutforcesq) {
                 float p = __fmaf_rn(sqrtf(rsq), rdr, 1.0f);
@@ -254,7 +251,7 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_rho_mixed(int nlocal,
 // keep more gathers in flight on a 131k-atom system. Blocks of 2 x EAM_THREADS
 // threads cover the same EAM_THREADS atoms as a block of the one-lane pass, so
 // both write the same energy partials.
-template <bool ENERGY, bool OT>
+template <bool ENERGY>
 __global__ void __launch_bounds__(2 * EAM_THREADS) k_eam_rho_mixed2(int nlocal,
     const float4* __restrict__ xr, CellShift sh, const int* __restrict__ numneigh,
     const int* __restrict__ neighbors, int ld, float cutforcesq, EamDev e,
@@ -262,8 +259,6 @@ __global__ void __launch_bounds__(2 * EAM_THREADS) k_eam_rho_mixed2(int nlocal,
     float4* __restrict__ xe, double* __restrict__ epart)
 {
     const float cg  = sh.g;
-    __shared__ float4 s_off[64]; // offset * G per cell-offset code (OT)
-    if (OT) fill_offset_table(s_off, cg);
     const int lane  = threadIdx.x & 31;
     const int u     = lane & 1;
     const int i     = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 16 + (lane >> 1);
@@ -282,8 +277,7 @@ __global__ void __launch_bounds__(2 * EAM_THREADS) k_eam_rho_mixed2(int nlocal,
         bool in = false;
         if (valid) {
             float dx, dy, dz;
-            if (OT) table_delta(pi, pj, (unsigned)en >> MDB_IDX_BITS, s_off, dx, dy, dz);
-            else cell_delta(pi, pj, (unsigned)en >> MDB_IDX_BITS, cg, dx, dy, dz);
+            cell_delta(pi, pj, (unsigned)en >> MDB_IDX_BITS, cg, dx, dy, dz);
             const float rsq = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
             in              = rsq < cutforcesq;
             if (in) {
@@ -361,15 +355,13 @@ __global__ void k_eam_xe_ghost(int nlocal, const float4* __restrict__ xr,
 }
 
 // COMP: Knuth two-sum compensated force sums (MDB_PREC_MIXED_COMP)
-template <bool ENERGY, bool COMP, bool OT>
+template <bool ENERGY, bool COMP>
 __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_mixed(int nlocal,
     const float4* __restrict__ xe, CellShift sh, const int* __restrict__ ncut,
     const int* __restrict__ cut, int ld, EamDev e, double* __restrict__ fx,
     double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ epart)
 {
     const float cg = sh.g;
-    __shared__ float4 s_off[64]; // offset * G per cell-offset code (OT)
-    if (OT) fill_offset_table(s_off, cg);
     const int i    = blockIdx.x * blockDim.x + threadIdx.x;
     double eng     = 0.0;
     if (i < nlocal) {
@@ -395,8 +387,7 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_mixed(int nlocal,
         };
         auto pair = [&](int en, const float4& pj) {
             float dx, dy, dz;
-            if (OT) table_delta(pi, pj, (unsigned)en >> MDB_IDX_BITS, s_off, dx, dy, dz);
-            else cell_delta(pi, pj, (unsigned)en >> MDB_IDX_BITS, cg, dx, dy, dz);
+            cell_delta(pi, pj, (unsigned)en >> MDB_IDX_BITS, cg, dx, dy, dz);
             const float rsq = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
             const float r   = sqrtf(rsq);
             float p         = __fmaf_rn(r, rdr, 1.0f);
@@ -482,8 +473,8 @@ void launch_eam_fp64(cudaStream_t s, int energy, int nlocal, int ghost_cap, cons
     g_launches++;
 }
 
-int launch_eam_mixed(cudaStream_t s, int energy, int comp, int rho_lanes, int ot,
-    int nlocal, int ghost_cap,
+int launch_eam_mixed(cudaStream_t s, int energy, int comp, int rho_lanes, int nlocal,
+    int ghost_cap,
     const float4* xr, const CellShift& sh, const int* numneigh, const int* neighbors, int ld,
     float cutforcesq, EamDev eam, const int* border_map, const int* counters, int* cut,
     int* ncut, double* fp, float4* xe, double* fx, double* fy, double* fz, double* epart_rho,
@@ -491,44 +482,34 @@ int launch_eam_mixed(cudaStream_t s, int energy, int comp, int rho_lanes, int ot
 {
     if (nlocal <= 0) return 0;
     const int nb = eam_mixed_blocks(nlocal);
-    // ot: bit 0 the density pass, bit 1 the force pass decode cell offsets
-    // from a shared table
-#define EAM_RHO(K, T, E, O)                                                              \
-    K<E, O><<<nb, T, 0, s>>>(nlocal, xr, sh, numneigh, neighbors, ld, cutforcesq, eam, cut, \
-        ncut, fp, xe, epart_rho)
-    const bool orho = ot & 1;
     if (rho_lanes == 2) {
-        if (energy) {
-            if (orho) EAM_RHO(k_eam_rho_mixed2, 2 * EAM_THREADS, true, true);
-            else EAM_RHO(k_eam_rho_mixed2, 2 * EAM_THREADS, true, false);
-        } else {
-            if (orho) EAM_RHO(k_eam_rho_mixed2, 2 * EAM_THREADS, false, true);
-            else EAM_RHO(k_eam_rho_mixed2, 2 * EAM_THREADS, false, false);
-        }
-    } else if (energy) {
-        if (orho) EAM_RHO(k_eam_rho_mixed, EAM_THREADS, true, true);
-        else EAM_RHO(k_eam_rho_mixed, EAM_THREADS, true, false);
-    } else {
-        if (orho) EAM_RHO(k_eam_rho_mixed, EAM_THREADS, false, true);
-        else EAM_RHO(k_eam_rho_mixed, EAM_THREADS, false, false);
-    }
-#undef EAM_RHO
+        if (energy)
+            k_eam_rho_mixed2<true><<<nb, 2 * EAM_THREADS, 0, s>>>(nlocal, xr, sh, numneigh,
+                neighbors, ld, cutforcesq, eam, cut, ncut, fp, xe, epart_rho);
+        else
+            k_eam_rho_mixed2<false><<<nb, 2 * EAM_THREADS, 0, s>>>(nlocal, xr, sh, numneigh,
+                neighbors, ld, cutforcesq, eam, cut, ncut, fp, xe, epart_rho);
+    } else if (energy)
+        k_eam_rho_mixed<true><<<nb, EAM_THREADS, 0, s>>>(nlocal, xr, sh, numneigh, neighbors,
+            ld, cutforcesq, eam, cut, ncut, fp, xe, epart_rho);
+    else
+        k_eam_rho_mixed<false><<<nb, EAM_THREADS, 0, s>>>(nlocal, xr, sh, numneigh, neighbors,
+            ld, cutforcesq, eam, cut, ncut, fp, xe, epart_rho);
     g_launches++;
     if (ghost_cap > 0) {
         k_eam_xe_ghost<<<mdb_blocks(ghost_cap, MDB_NTHREADS), MDB_NTHREADS, 0, s>>>(nlocal, xr,
             fp, xe, border_map, counters);
         g_launches++;
     }
-#define EAM_FM(E, C, O)                                                                  \
-    k_eam_force_mixed<E, C, O><<<nb, EAM_THREADS, 0, s>>>(nlocal, xe, sh, ncut, cut, ld, eam, \
-        fx, fy, fz, epart_pair)
-    const bool ofor = ot & 2;
+#define EAM_FM(E, C)                                                                     \
+    k_eam_force_mixed<E, C><<<nb, EAM_THREADS, 0, s>>>(nlocal, xe, sh, ncut, cut, ld, eam, fx, \
+        fy, fz, epart_pair)
     if (energy) {
-        if (comp) ofor ? EAM_FM(true, true, true) : EAM_FM(true, true, false);
-        else ofor ? EAM_FM(true, false, true) : EAM_FM(true, false, false);
+        if (comp) EAM_FM(true, true);
+        else EAM_FM(true, false);
     } else {
-        if (comp) ofor ? EAM_FM(false, true, true) : EAM_FM(false, true, false);
-        else ofor ? EAM_FM(false, false, true) : EAM_FM(false, false, false);
+        if (comp) EAM_FM(false, true);
+        else EAM_FM(false, false);
     }
 #undef EAM_FM
     g_launches++;

@@ -127,16 +127,15 @@ __global__ void __launch_bounds__(LJ_THREADS) k_lj_mixed(int nlocal,
 {
     __shared__ float s_eps[MDB_MAX_TYPES * MDB_MAX_TYPES];
     __shared__ float s_sig6[MDB_MAX_TYPES * MDB_MAX_TYPES];
-    __shared__ float4 s_off[64]; // offset * G per cell-offset code
     const int nt = tab.ntypes;
-    const float cg = sh.g;
     if (!UNIFORM) {
         for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) {
             s_eps[k]  = tab.eps[k];
             s_sig6[k] = tab.sig6[k];
         }
+        __syncthreads();
     }
-    fill_offset_table(s_off, cg);
+    const float cg = sh.g;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double epot = 0.0;
     if (t < nlocal) {
@@ -165,7 +164,7 @@ __global__ void __launch_bounds__(LJ_THREADS) k_lj_mixed(int nlocal,
         auto pair = [&](int e, const float4& pj) {
             const int j = e & MDB_IDX_MASK;
             float delx, dely, delz;
-            table_delta(pi, pj, (unsigned)e >> MDB_IDX_BITS, s_off, delx, dely, delz);
+            cell_delta(pi, pj, (unsigned)e >> MDB_IDX_BITS, cg, delx, dely, delz);
             float rsq = __fmaf_rn(delx, delx, __fmaf_rn(dely, dely, delz * delz));
             float sigma6 = sig0, epsilon = eps0;
             if (!UNIFORM) {

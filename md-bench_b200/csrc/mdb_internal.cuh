@@ -90,28 +90,6 @@ __device__ __forceinline__ void cell_delta(const float4& pi, const float4& pj, u
     dz = __fmaf_rn(-cell_offset((code >> 4) & 3u), g, pi.z - pj.z);
 }
 
-// offset * G of every cell-offset code (2 bits per axis, bits 26-31 of an
-// entry), filled into a block's shared table of 64 entries (all threads call,
-// then a barrier): one shared load per pair instead of decoding three fields.
-// The products are exact, so (p_i - p_j) - offset * G rounds as cell_delta's
-// fused form does.
-__device__ __forceinline__ void fill_offset_table(float4* t, float g)
-{
-    for (int c = threadIdx.x; c < 64; c += blockDim.x)
-        t[c] = make_float4(cell_offset(c & 3u) * g, cell_offset((c >> 2) & 3u) * g,
-            cell_offset((c >> 4) & 3u) * g, 0.f);
-    __syncthreads();
-}
-
-__device__ __forceinline__ void table_delta(const float4& pi, const float4& pj, unsigned code,
-    const float4* t, float& dx, float& dy, float& dz)
-{
-    const float4 o = t[code];
-    dx             = (pi.x - pj.x) - o.x;
-    dy             = (pi.y - pj.y) - o.y;
-    dz             = (pi.z - pj.z) - o.z;
-}
-
 struct EamDev {
     int nrho, nr;
     double rdr, rdrho;
@@ -256,8 +234,8 @@ void launch_eam_fp64(cudaStream_t s, int energy, int nlocal, int ghost_cap, cons
 // mixed EAM: four threads per atom; xe (nlocal + ghost_cap) receives
 // (position, F'(rho)) of every atom for the force pass; comp: two-sum
 // compensated force sums; returns the energy partials written per pass
-int launch_eam_mixed(cudaStream_t s, int energy, int comp, int rho_lanes, int ot,
-    int nlocal, int ghost_cap,
+int launch_eam_mixed(cudaStream_t s, int energy, int comp, int rho_lanes, int nlocal,
+    int ghost_cap,
     const float4* xr, const CellShift& sh, const int* numneigh, const int* neighbors, int ld,
     float cutforcesq, EamDev eam, const int* border_map, const int* counters, int* cut,
     int* ncut, double* fp, float4* xe, double* fx, double* fy, double* fz, double* epart_rho,
