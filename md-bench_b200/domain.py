@@ -88,12 +88,17 @@ class DistTransport:
         return t.cpu().numpy()
 
     def _phase(self, dest, t, src, shape_rows):
+        """Send t to dest, receive shape_rows rows from src. Empty messages
+        travel as one padding row (dropped on arrival), so no point-to-point
+        call ever moves zero elements."""
         torch, dist = self.torch, self.dist
-        r = torch.empty((shape_rows, t.shape[1]), dtype=t.dtype, device=self.device)
+        if t.shape[0] == 0:
+            t = torch.zeros((1, t.shape[1]), dtype=t.dtype, device=self.device)
+        r = torch.empty((max(shape_rows, 1), t.shape[1]), dtype=t.dtype, device=self.device)
         ops = [dist.P2POp(dist.isend, t.contiguous(), dest), dist.P2POp(dist.irecv, r, src)]
         for q in dist.batch_isend_irecv(ops):
             q.wait()
-        return r
+        return r[:shape_rows]
 
     def exchange(self, down, up, below, above, sizes=None):
         """down / up: rows for the rank below / above. Returns (rows from below,

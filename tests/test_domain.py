@@ -206,6 +206,48 @@ def test_two_slabs_bit_identical_to_one_domain():
     assert T == pytest.approx(float(np.sum(V * V)) / (3 * n - 3), rel=1e-14)
 
 
+def _empty_worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path[:0] = [os.path.join(ROOT, "md-bench_b200")]
+    import datetime
+
+    import domain as D
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        tr = D.DistTransport(torch, dist, "cpu")
+        other = 1 - rank
+        # rank 0 sends nothing down and three rows up; rank 1 the reverse
+        down = np.zeros((0, 3)) if rank == 0 else np.arange(9.0).reshape(3, 3) + 100 * rank
+        up = np.arange(9.0).reshape(3, 3) + 100 * rank if rank == 0 else np.zeros((0, 3))
+        fb, fa = tr.exchange(tr.wrap(down), tr.wrap(up), other, other)
+        q.put((rank, tr.to_host(fb).tolist(), tr.to_host(fa).tolist()))
+    finally:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(120)
+def test_exchange_with_empty_messages():
+    """Empty halves of an exchange (no atom leaving in one direction) travel
+    as padding and arrive as zero rows."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_empty_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict((r, (fb, fa)) for r, fb, fa in [q.get(timeout=90) for _ in range(2)])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    rows = np.arange(9.0).reshape(3, 3)
+    # rank 0: from below (rank 1's up) nothing; from above (rank 1's down) 3 rows
+    assert res[0][0] == [] and res[0][1] == (rows + 100).tolist()
+    # rank 1: from below (rank 0's up) 3 rows; from above (rank 0's down) nothing
+    assert res[1][0] == rows.tolist() and res[1][1] == []
+
+
 def test_one_slab_is_its_own_neighbour():
     """One rank: the halo is the slab's own z images (shifted by the box
     length both ways), exchanged with itself through host queues; atoms never
