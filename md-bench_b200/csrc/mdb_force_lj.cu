@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(LJ_THREADS) k_lj_fp64(int nlocal,
 }
 
 template <bool HALF, bool UNIFORM, bool ENERGY, bool COMP>
-__global__ void __launch_bounds__(LJ_THREADS) k_lj_mixed(int nlocal,
+__global__ void __launch_bounds__(LJ_THREADS, 10) k_lj_mixed(int nlocal,
     const int* __restrict__ order, const float4* __restrict__ xr, CellShift sh,
     const int* __restrict__ numneigh, const int* __restrict__ neighbors, int ld,
     float cutforcesq, LJTableF tab, double* __restrict__ fx, double* __restrict__ fy,
@@ -147,6 +147,9 @@ __global__ void __launch_bounds__(LJ_THREADS) k_lj_mixed(int nlocal,
         float fix = 0.f, fiy = 0.f, fiz = 0.f;
         float cx = 0.f, cy = 0.f, cz = 0.f; // compensation terms
         const float eps0 = tab.eps[0], sig0 = tab.sig6[0];
+        // one type: force / r = sr2 s (A s - B), s = 1 / r^6, A = 48 eps sigma^12,
+        // B = 24 eps sigma^6
+        const float cA = 48.0f * eps0 * sig0 * sig0, cB = 24.0f * eps0 * sig0;
 
         auto acc = [&](float& s, float& c, float d, float f) {
             if (COMP) { // Knuth two-sum: s + c carries the running sum exactly
@@ -173,9 +176,16 @@ __global__ void __launch_bounds__(LJ_THREADS) k_lj_mixed(int nlocal,
                 epsilon = s_eps[tij];
             }
             if (rsq < cutforcesq) {
-                float sr2   = __fdividef(1.0f, rsq);
-                float sr6   = sr2 * sr2 * sr2 * sigma6;
-                float force = 48.0f * sr6 * (sr6 - 0.5f) * sr2 * epsilon;
+                float sr2 = __fdividef(1.0f, rsq);
+                float sr6, force;
+                if (UNIFORM) {
+                    const float s3 = sr2 * sr2 * sr2;
+                    sr6            = s3 * sigma6;
+                    force          = sr2 * s3 * __fmaf_rn(cA, s3, -cB);
+                } else {
+                    sr6   = sr2 * sr2 * sr2 * sigma6;
+                    force = 48.0f * sr6 * (sr6 - 0.5f) * sr2 * epsilon;
+                }
                 acc(fix, cx, delx, force);
                 acc(fiy, cy, dely, force);
                 acc(fiz, cz, delz, force);
