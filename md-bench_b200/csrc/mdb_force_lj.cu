@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(LJ_THREADS) k_lj_fp64(int nlocal,
 }
 
 template <bool HALF, bool UNIFORM, bool ENERGY, bool COMP>
-__global__ void __launch_bounds__(LJ_THREADS, 10) k_lj_mixed(int nlocal,
+__global__ void __launch_bounds__(LJ_THREADS) k_lj_mixed(int nlocal,
     const int* __restrict__ order, const float4* __restrict__ xr, CellShift sh,
     const int* __restrict__ numneigh, const int* __restrict__ neighbors, int ld,
     float cutforcesq, LJTableF tab, double* __restrict__ fx, double* __restrict__ fy,
