@@ -16,6 +16,15 @@ __device__ __forceinline__ void red_add4(float4* dst, float x, float y, float z)
                  : "memory");
 }
 
+// two consecutive float4 in one 256-bit load (sm_100); p 32-byte aligned
+__device__ __forceinline__ void ldg_pair4(const float4* p, float4& a, float4& b)
+{
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z),
+          "=f"(b.w)
+        : "l"(p));
+}
+
 // PTX rcp.approx.ftz.f32: at most 1 ulp from 1/x, one MUFU operation
 __device__ __forceinline__ float rcp_approx(float x)
 {

@@ -277,9 +277,14 @@ __device__ __forceinline__ JEntry<JPL> load_entry(int cj, int b0, const float4* 
 {
     JEntry<JPL> j;
     j.cj = cj;
+    if (JPL == 2) {
+        // slots cj * N + b0, b0 even: a 32-byte aligned pair
+        ldg_pair4(&xr[cj * N + b0], j.x[0], j.x[JPL - 1]);
+    } else {
 #pragma unroll
-    for (int u = 0; u < JPL; u++)
-        j.x[u] = __ldg(&xr[cj * N + b0 + u]);
+        for (int u = 0; u < JPL; u++)
+            j.x[u] = __ldg(&xr[cj * N + b0 + u]);
+    }
     if (!AW) {
         const float4 a = __ldg(&anchor[cj]);
 #pragma unroll

@@ -15,6 +15,15 @@
 namespace mdb {
 
 static constexpr int EAM_THREADS = 128;
+
+// one 32-byte row (two float4) in one 256-bit load (sm_100); p 32-byte aligned
+__device__ __forceinline__ void ldg_row32(const float4* p, float4& a, float4& b)
+{
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z),
+          "=f"(b.w)
+        : "l"(p));
+}
 static constexpr int EUNROLL     = 4;
 
 template <bool ENERGY>
@@ -397,8 +406,8 @@ __global__ void __launch_bounds__(EAM_THREADS) k_eam_force_mixed(int nlocal,
             p               = p < 1.0f ? p : 1.0f;
             // z2r coefficients 3..6, then rho 0..2 and z2r 0; z2r 1 and 2 are
             // 2 c4 / dr and c5 / dr (spline7's derivative rows)
-            const float4 za = __ldg(e.pair32 + 2 * m);
-            const float4 rb = __ldg(e.pair32 + 2 * m + 1);
+            float4 za, rb;
+            ldg_row32(e.pair32 + 2 * m, za, rb);
             float rhoip = __fmaf_rn(__fmaf_rn(rb.x, p, rb.y), p, rb.z);
             float z2p   = __fmaf_rn(__fmaf_rn(rb.w, p, za.y * rdr2), p, za.z * rdr);
             float z2    = __fmaf_rn(__fmaf_rn(__fmaf_rn(za.x, p, za.y), p, za.z), p, za.w);
