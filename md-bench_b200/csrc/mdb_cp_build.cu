@@ -968,17 +968,24 @@ __device__ __forceinline__ bool any_pair_f(const IPairs& ip, const float4* __res
 {
     static_assert(M == 4, "i-clusters of 4 atoms");
     float mn = 3.0e38f;
+    // the j-cluster's slots two per 256-bit load (cjf is 32-byte aligned: N even)
 #pragma unroll
-    for (int b = 0; b < N; b++) {
-        const float4 xj = __ldg(&cjf[b]);
-        const f2 XJ = f2_pack(xj.x, xj.x), YJ = f2_pack(xj.y, xj.y), ZJ = f2_pack(xj.z, xj.z);
+    for (int b = 0; b < N; b += 2) {
+        float4 xjp[2];
+        ldg_pair4(&cjf[b], xjp[0], xjp[1]);
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const f2 dx = f2_sub(ip.x[h], XJ), dy = f2_sub(ip.y[h], YJ), dz = f2_sub(ip.z[h], ZJ);
-            const f2 r2 = f2_add(f2_add(f2_mul(dx, dx), f2_mul(dy, dy)), f2_mul(dz, dz));
-            float r0, r1;
-            f2_unpack(r2, r0, r1);
-            mn = fminf(mn, fminf(r0, r1));
+        for (int u = 0; u < 2; u++) {
+            const float4 xj = xjp[u];
+            const f2 XJ = f2_pack(xj.x, xj.x), YJ = f2_pack(xj.y, xj.y), ZJ = f2_pack(xj.z, xj.z);
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const f2 dx = f2_sub(ip.x[h], XJ), dy = f2_sub(ip.y[h], YJ),
+                         dz = f2_sub(ip.z[h], ZJ);
+                const f2 r2 = f2_add(f2_add(f2_mul(dx, dx), f2_mul(dy, dy)), f2_mul(dz, dz));
+                float r0, r1;
+                f2_unpack(r2, r0, r1);
+                mn = fminf(mn, fminf(r0, r1));
+            }
         }
     }
     if (mn < lo) return true;
@@ -1079,7 +1086,8 @@ __device__ __forceinline__ void build_list_blk(int bid, int half, int* cnt, Geom
                 }
                 cj          = jcol[m];
                 if (!(half && ci_cj0 > cj)) {
-                    const float4 fn = __ldg(&jcbbf[2 * m]), fx = __ldg(&jcbbf[2 * m + 1]);
+                    float4 fn, fx;
+                    ldg_pair4(&jcbbf[2 * m], fn, fx); // the box's min and max
                     float df = bb_axis_f(imnzf, imxzf, fn.z, fx.z);
                     df       = df * df;
                     float ef = bb_axis_f(imnyf, imxyf, fn.y, fx.y);
