@@ -890,7 +890,7 @@ def main():
                            "force_path": "pair list (listed cluster pairs' pairs within "
                                          "r_c + skin, re-derived when an atom moves past "
                                          "skin / 2)" if HEAD["path"] else "cluster pair",
-                           "i_clusters_per_warp": 4,
+                           "i_clusters_per_warp": 4, "j_atoms_per_lane": 2,
                            "lists": "half" if HEAD["half"] else "full",
                            "l2": "inputs larger than L2 (cluster list %.0f MB, "
                                  "positions and velocities %.0f MB)"

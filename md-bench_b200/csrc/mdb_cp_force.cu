@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(CP_FORCE_THREADS) k_force_fp64(const int* __re
                     const bool cond = HALF ? (ci_cj0 != cj || ai < b) : (ci_cj0 != cj || ai != b);
                     if (!cond) continue;
                     const int sj     = cj * N + b;
-                    const double4 pj = cx[sj];
+                    const double4 pj = ldg4(&cx[sj]);
                     const double delx = pi.x - pj.x;
                     const double dely = pi.y - pj.y;
                     const double delz = pi.z - pj.z;

@@ -111,11 +111,15 @@ namespace mdb {
 __device__ __forceinline__ int type_of(const double4& p) { return (int)__double_as_longlong(p.w); }
 
 // read-only 32-byte position load as two 16-byte non-coherent loads of one sector
+// a double4 in one 256-bit read-only load (sm_100; p 32-byte aligned, as
+// every double4 array from cudaMalloc is)
 __device__ __forceinline__ double4 ldg4(const double4* p)
 {
-    const double2* q = reinterpret_cast<const double2*>(p);
-    double2 a = __ldg(q), b = __ldg(q + 1);
-    return make_double4(a.x, a.y, b.x, b.y);
+    double4 r;
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+        : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w)
+        : "l"(p));
+    return r;
 }
 
 __device__ __forceinline__ int pack_cell(int cx, int cy, int cz)
