@@ -14,9 +14,10 @@ mixed variant with its force error against FP64 and the energy drifts.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
-With N > 1 (torchrun) every rank runs one independent replica (the path has
-no data-path collective on one node); value is the sum over ranks, timing the
-max over ranks.
+With N > 1 (torchrun) every rank runs one independent replica for the
+headline (value is the sum over ranks, timing the max over ranks), and the
+line's ``sharded`` key runs the Verlet-list LJ system decomposed into z-slabs
+over all ranks (halo exchange every step, atoms migrating at rebuilds).
 """
 import argparse
 import json
