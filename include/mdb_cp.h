@@ -52,8 +52,9 @@ int mdb_cp_synchronize(MdbCp* ctx);
  * the i sums, depends on the setting. Ensemble members keep theirs;
  * "force_jpl" = j atoms per lane of the mixed cluster-pair kernel: 1, or 2
  * with force_cpw 4 (two consecutive atoms of an entry share a lane's list,
- * anchor and loop work; FP32 rounding changes as for force_cpw; default 2,
- * 1 for 4x8 half lists; ensemble members keep theirs);
+ * anchor and loop work; FP32 rounding changes as for force_cpw; default 2
+ * for one atom type, 1 for several types and for 4x8 half lists; ensemble
+ * members keep theirs);
  * "force_block" = threads per block of the mixed force kernel (32..512, a
  * multiple of 32; default 128); "force_variant" = 0..3: 0 and 1 prefetch the
  * j data one or two list blocks ahead with no register budget, 2 and 3 the same

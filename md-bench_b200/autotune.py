@@ -11,8 +11,9 @@ chosen shape. The tuner picks, per system size:
 * cluster shape N = 4 or 8 (which also fixes the column size),
 * list form: full or half (half-list reactions use atomics),
 * the mixed force kernel's launch: threads per block (``force_block``),
-  ``force_variant`` (prefetch depth, register budget) and i-clusters per warp
-  (``force_cpw``: 1, 2, 4, or 8 with 4x4 clusters),
+  ``force_variant`` (prefetch depth, register budget), i-clusters per warp
+  (``force_cpw``: 1, 2, 4, or 8 with 4x4 clusters) and j atoms per lane
+  (``force_jpl``: 1, or 2 with four i-clusters per warp),
 
 by measurement on the device. A single large system is tuned on the force
 kernel's own time (``ClusterSystem.time_force``, CUDA events). Members of an
@@ -32,13 +33,17 @@ FORMS = (0, 1)
 BLOCKS = (64, 128, 256)
 VARIANTS = (0, 1, 2, 3)
 CPWS = (1, 2, 4, 8)
-DEFAULT = {"cluster_n": 4, "half": 1, "force_block": 128, "force_variant": 2, "force_cpw": 4}
+JPLS = (1, 2)
+DEFAULT = {"cluster_n": 4, "half": 1, "force_block": 128, "force_variant": 2, "force_cpw": 4,
+           "force_jpl": 1}
 
 
 def valid(choice):
     """force_cpw 8 needs 4x4 clusters; several clusters per warp prefetch one
     block ahead (variant 1 runs as 0 there; 3 is a budget for 6 blocks)."""
     if choice.get("force_cpw", 1) == 8 and choice["cluster_n"] != 4:
+        return False
+    if choice.get("force_jpl", 1) == 2 and choice.get("force_cpw", 1) != 4:
         return False
     return not (choice.get("force_cpw", 1) > 1 and choice.get("force_variant", 0) == 1)
 
@@ -53,6 +58,7 @@ def apply_launch(system, choice):
     system.tune("force_block", choice["force_block"])
     system.tune("force_variant", choice["force_variant"])
     system.tune("force_cpw", choice["force_cpw"])
+    system.tune("force_jpl", choice.get("force_jpl", 1))
 
 
 def tune_system(build, precision="mixed", reps=20, shapes=SHAPES, forms=FORMS):
@@ -65,10 +71,10 @@ def tune_system(build, precision="mixed", reps=20, shapes=SHAPES, forms=FORMS):
             t = s.time_force(reps)
             trials.append(({"cluster_n": n, "half": half}, t))
             if precision == "mixed":
-                for blk, var, cpw in ((b, v, w) for b in BLOCKS for v in VARIANTS
-                                      for w in CPWS):
+                for blk, var, cpw, jpl in ((b, v, w, p) for b in BLOCKS for v in VARIANTS
+                                           for w in CPWS for p in JPLS):
                     c = {"cluster_n": n, "half": half, "force_block": blk,
-                         "force_variant": var, "force_cpw": cpw}
+                         "force_variant": var, "force_cpw": cpw, "force_jpl": jpl}
                     if not valid(c):
                         continue
                     apply_launch(s, c)
@@ -151,7 +157,7 @@ def tune_ensemble(specs, build, steps=20, rounds=2, shapes=SHAPES, forms=FORMS, 
                     members[c] = old
     for c in order:
         for key, values in (("force_block", BLOCKS), ("force_variant", VARIANTS),
-                            ("force_cpw", CPWS)):
+                            ("force_cpw", CPWS), ("force_jpl", JPLS)):
             for val in values:
                 if val == choice[c][key]:
                     continue

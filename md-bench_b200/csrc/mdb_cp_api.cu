@@ -267,10 +267,12 @@ static int setup_types(MdbCp* ctx)
     // four i-clusters per warp: measured fastest on B200 at 1M atoms (4x4 and
     // 4x8, full and half; 170 us against 229 us per launch for one per warp)
     t.force_cpw     = 4;
-    // two j atoms per lane (one 256-bit load): at 1M atoms 189 against 200 us
-    // per launch for 4x4 full lists, 159 against 164 us for 4x4 half lists;
-    // 4x8 half lists 188 against 182 us
-    t.force_jpl     = (ctx->N == 4 || !ctx->p.half_neigh) ? 2 : 1;
+    // two j atoms per lane (one 256-bit load), one atom type: at 1M atoms 189
+    // against 200 us per launch for 4x4 full lists, 159 against 164 us for
+    // 4x4 half lists; 4x8 half lists 188 against 182 us; several types (their
+    // per-atom tables take the registers) 2.83e9 against 3.65e9 atom-steps/s
+    // on the 4-type liquid
+    t.force_jpl     = (t.uniform && (ctx->N == 4 || !ctx->p.half_neigh)) ? 2 : 1;
     t.eps0        = t.sqrt_eps[0] * t.sqrt_eps[0];
     t.sigma6_0 = t.sigma3[0] * t.sigma3[0];
     // the pair-list path's constants (geometric mixing, in FP64 then rounded)

@@ -12,7 +12,8 @@ class FakeMember:
     def __init__(self, sp, n, half, log):
         self.natoms, self.nlocal = sp["natoms"], sp["natoms"]
         self.cluster_n, self.half = n, half
-        self.launch = {k: AT.DEFAULT[k] for k in ("force_block", "force_variant", "force_cpw")}
+        self.launch = {k: AT.DEFAULT[k]
+                       for k in ("force_block", "force_variant", "force_cpw", "force_jpl")}
         self.closed = False
         log.append(self)
 
@@ -48,7 +49,7 @@ def model_rate(members):
             c *= 1.05
         t += m.natoms * c
         groups.add((m.cluster_n, m.half, m.launch["force_block"], m.launch["force_variant"],
-                    m.launch["force_cpw"]))
+                    m.launch["force_cpw"], m.launch["force_jpl"]))
     t += 50.0 * len(groups)
     return sum(m.natoms for m in members) / t
 
@@ -80,7 +81,7 @@ def test_no_change_within_noise():
     specs = [{"natoms": 1000}] * 3
     log = []
     flat = iter([1.0, 1.01, 0.99, 1.015, 1.0, 1.019, 0.98, 1.0, 1.0, 1.0, 1.012, 1.0, 0.99,
-                 1.0])
+                 1.0, 1.005])
     choice, trials = AT.tune_ensemble(specs, lambda sp, n, h: FakeMember(sp, n, h, log),
                                       rate=lambda ms: next(flat))
     assert choice == {AT.size_class(1000): AT.DEFAULT}
