@@ -57,23 +57,30 @@ void launch_gather(cudaStream_t s, int M, int ncl_cap, const int* cnt, const dou
 }
 
 // ---- binAtoms (clusterpair/neighbor.c:1409-1449) -----------------------------
+// Atoms arrive in cluster order from the last build, so the lanes of a warp
+// mostly share a column: one atomic per distinct column of the warp
+// (__match_any_sync). The order in which a column's atoms are appended does
+// not matter: the column sort orders them by z and atom index.
 __device__ __forceinline__ void bin_atoms_blk(int bid, int n, const double4* __restrict__ ax,
     Geom g, int* atom_col,
     int* col_count, int* cnt)
 {
     const int i = bid * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double4 p = ax[i];
-    int ix, iy;
-    coord2bin2d(g, p.x, p.y, ix, iy);
-    int b = iy * g.mbinx + ix + 1;
-    if (b < 0 || b >= g.mbins) {
-        atomicAdd(&cnt[CP_BADBIN], 1);
-        atom_col[i] = -1;
-        return;
+    int b       = -1;
+    if (i < n) {
+        double4 p = ax[i];
+        int ix, iy;
+        coord2bin2d(g, p.x, p.y, ix, iy);
+        b = iy * g.mbinx + ix + 1;
+        if (b < 0 || b >= g.mbins) {
+            atomicAdd(&cnt[CP_BADBIN], 1);
+            b = -1;
+        }
+        atom_col[i] = b;
     }
-    atom_col[i] = b;
-    atomicAdd(&col_count[b], 1);
+    const unsigned peers = __match_any_sync(0xffffffffu, b);
+    if (b >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1)
+        atomicAdd(&col_count[b], __popc(peers));
 }
 
 __global__ void k_bin_atoms(int n, const double4* __restrict__ ax, Geom g, int* atom_col,
@@ -94,11 +101,15 @@ void launch_bin_atoms(cudaStream_t s, int n, const double4* ax, const Geom& g, i
 __device__ __forceinline__ void scatter_atoms_blk(int bid, int n, const int* __restrict__ atom_col,
     const int* __restrict__ col_start, int* col_fill, int* col_atoms)
 {
-    const int i = bid * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int b = atom_col[i];
-    if (b < 0) return;
-    col_atoms[col_start[b] + atomicAdd(&col_fill[b], 1)] = i;
+    const int i          = bid * blockDim.x + threadIdx.x;
+    const int lane       = threadIdx.x & 31;
+    const int b          = i < n ? atom_col[i] : -1;
+    const unsigned peers = __match_any_sync(0xffffffffu, b);
+    const int leader     = __ffs(peers) - 1;
+    int base             = 0;
+    if (b >= 0 && lane == leader) base = atomicAdd(&col_fill[b], __popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (b >= 0) col_atoms[col_start[b] + base + __popc(peers & ((1u << lane) - 1u))] = i;
 }
 
 __global__ void k_scatter_atoms(int n, const int* __restrict__ atom_col,
