@@ -162,76 +162,6 @@ __device__ void bitonic(int* idx, double* z, int P)
     }
 }
 
-// (z, index) order of the bitonic sort by z
-__device__ __forceinline__ bool zgreater(double za, int a, double zb, int b)
-{
-    return za > zb || (za == zb && a > b);
-}
-
-// The same sort by (z, index) with the column in registers: lane l holds
-// elements l * E .. l * E + E - 1 (E = P / 32), strides below E are exchanges
-// between a lane's registers, larger ones between lanes (shuffles); no shared
-// memory round trip per stage. The result goes back to idx / z.
-template <int E>
-__device__ void bitonic_regs(int* idx, double* z)
-{
-    const int lane = lane_id();
-    int ri[E];
-    double rz[E];
-#pragma unroll
-    for (int r = 0; r < E; r++) {
-        ri[r] = idx[lane * E + r];
-        rz[r] = z[lane * E + r];
-    }
-#pragma unroll
-    for (int size = 2; size <= 32 * E; size <<= 1) {
-#pragma unroll
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            if (stride >= E) {
-                const int lx = stride / E; // partner lane = lane ^ lx, same register
-#pragma unroll
-                for (int r = 0; r < E; r++) {
-                    const int i      = lane * E + r;
-                    const bool up    = (i & size) == 0;
-                    const bool lower = (lane & lx) == 0; // holds the smaller index
-                    const int oi     = __shfl_xor_sync(0xffffffffu, ri[r], lx);
-                    const double oz  = __shfl_xor_sync(0xffffffffu, rz[r], lx);
-                    // the pair (lower, upper) swaps when gt(lower, upper) == up
-                    const bool gt = lower ? zgreater(rz[r], ri[r], oz, oi)
-                                          : zgreater(oz, oi, rz[r], ri[r]);
-                    if (gt == up) {
-                        ri[r] = oi;
-                        rz[r] = oz;
-                    }
-                }
-            } else {
-#pragma unroll
-                for (int r = 0; r < E; r++) {
-                    const int q = r ^ stride;
-                    if (q > r) {
-                        const int i   = lane * E + r;
-                        const bool up = (i & size) == 0;
-                        if (zgreater(rz[r], ri[r], rz[q], ri[q]) == up) {
-                            const int ti    = ri[r];
-                            const double tz = rz[r];
-                            ri[r]           = ri[q];
-                            rz[r]           = rz[q];
-                            ri[q]           = ti;
-                            rz[q]           = tz;
-                        }
-                    }
-                }
-            }
-        }
-    }
-#pragma unroll
-    for (int r = 0; r < E; r++) {
-        idx[lane * E + r] = ri[r];
-        z[lane * E + r]   = rz[r];
-    }
-    __syncwarp();
-}
-
 __device__ void sort_column(int* idx, double* z, int c, int P, const double4* __restrict__ ax)
 {
     const int lane = lane_id();
@@ -240,9 +170,7 @@ __device__ void sort_column(int* idx, double* z, int c, int P, const double4* __
         z[k] = k < c ? ax[idx[k]].z : INFINITY;
     }
     __syncwarp();
-    if (P == 256) bitonic_regs<8>(idx, z);
-    else if (P == 512) bitonic_regs<16>(idx, z);
-    else bitonic<true>(idx, z, P);
+    bitonic<true>(idx, z, P);
     bool tie = false;
     for (int k = lane; k + 1 < c; k += 32)
         tie |= z[k] == z[k + 1];
