@@ -302,10 +302,11 @@ class Replicas:
             self.cache[key] = (hp, x, v, t)
         return self.cache[key]
 
-    def build(self, sp, cluster_n, half, choice=None, precision="mixed"):
+    def build(self, sp, cluster_n, half, column_edge=100, choice=None, precision="mixed"):
         import autotune as AT
         hp, x, v, t = self.state(sp)
         s = self.mdb.ClusterSystem(natoms=len(t), cluster_n=cluster_n, half_neigh=half,
+                                   column_edge=column_edge,
                                    precision=precision, device=self.device, xprd=hp.xprd,
                                    yprd=hp.yprd, zprd=hp.zprd, cutforce=hp.cutforce,
                                    cutneigh=hp.cutneigh, dt=hp.dt, dtforce=hp.dtforce,
@@ -419,12 +420,13 @@ def c4_ensemble(torch, mdb, args, device, rank=0, world=1, dist=None):
     if args.no_autotune:
         choice, trials = {}, []
     else:
-        choice, trials = AT.tune_ensemble(specs, lambda sp, n, h: pool.build(sp, n, h),
+        choice, trials = AT.tune_ensemble(specs, lambda sp, n, h, e: pool.build(sp, n, h, e),
                                           rounds=2)
     tune_secs = time.perf_counter() - t0
     pick = [choice.get(AT.size_class(sp["natoms"]), AT.DEFAULT) for sp in specs]
     every = 20
-    members = [pool.build(sp, c["cluster_n"], c["half"], c) for sp, c in zip(specs, pick)]
+    members = [pool.build(sp, c["cluster_n"], c["half"], c["column_edge"], c)
+               for sp, c in zip(specs, pick)]
     secs, launches, d32, n = run_ensemble(torch, mdb, members, args, every)
     secs = reduce_scalar(torch, dist, secs, "max", "cuda")
     # the same replicas advanced one after another (each its own graph loop)
@@ -434,7 +436,7 @@ def c4_ensemble(torch, mdb, args, device, rank=0, world=1, dist=None):
     serial = time.perf_counter() - t1
     for m in members:
         m.close()
-    members = [pool.build(sp, c["cluster_n"], c["half"], None, "fp64")
+    members = [pool.build(sp, c["cluster_n"], c["half"], c["column_edge"], None, "fp64")
                for sp, c in zip(specs, pick)]
     secs64, _, d64, _ = run_ensemble(torch, mdb, members, args, every)
     secs64 = reduce_scalar(torch, dist, secs64, "max", "cuda")
@@ -444,7 +446,7 @@ def c4_ensemble(torch, mdb, args, device, rank=0, world=1, dist=None):
     nat = total_atoms
     shapes = {}
     for c in pick:
-        key = f"4x{c['cluster_n']}-{'half' if c['half'] else 'full'}"
+        key = f"4x{c['cluster_n']}-{'half' if c['half'] else 'full'}-edge{c['column_edge']}"
         shapes[key] = shapes.get(key, 0) + 1
     return {"value": nat * every * args.steps / secs, "ms_per_step": 1e3 * secs / args.steps,
             "natoms": nat, "replicas": len(specs), "md_steps": every * args.steps,

@@ -73,7 +73,13 @@ int mdb_cp_synchronize(MdbCp* ctx);
  * same forces up to FP32 summation order; "pair_variant" = 0..3: launch
  * shape of the pair-list kernel (j loads in flight per lane and register
  * budget: 0 = 4 loads, 1 = 2, 2 = 3 with a budget for 6 blocks of 128
- * threads per SM, 3 = 2 with a budget for 8; default 0). */
+ * threads per SM, 3 = 2 with a budget for 8; default 0);
+ * "column_edge" = 50..200: the xy edge of the column grid in percent of
+ * setupNeighbor's (max(M, N) / rho)^(1/3) (clusterpair/neighbor.c:128-145),
+ * the scheme's bin size; accepted only before mdb_cp_set_atoms. 100 (the
+ * default) is the reference's grid and lists; any other value gives other
+ * clusters and lists with the same pairs inside cutneigh, so the same forces
+ * up to summation order. */
 int mdb_cp_tune(MdbCp* ctx, const char* key, int value);
 /* Buffer of the pair-list path (force_path 1; no counterpart in the
  * reference): pairs are kept within r_c + buffer, and any atom moving more

@@ -34,6 +34,9 @@ struct MdbCp {
     long long launches = 0;
 
     int nlocal = 0, maxneighs = 200;
+    // column edge in percent of setupNeighbor's (max(M, N) / rho)^(1/3); 100
+    // keeps the reference's grid, so its lists (tuning key "column_edge")
+    int col_edge_pct = 100;
     Geom g;
     std::vector<int> stencil;
     Types ty;
@@ -148,6 +151,8 @@ static void drop_graph(MdbCp* ctx)
 
 static int ensure_pairs(MdbCp* ctx);
 static int mark_derive(MdbCp* ctx);
+static void setup_columns(MdbCp* ctx);
+static int alloc_columns(MdbCp* ctx);
 
 static long long mark() { return mdb::g_launches; }
 static void account(MdbCp* ctx, long long m) { ctx->launches += mdb::g_launches - m; }
@@ -175,6 +180,10 @@ static void setup_columns(MdbCp* ctx)
     double in_cell  = (double)std::max(ctx->M, ctx->N);
     double tx       = cbrt(in_cell / density);
     double ty       = cbrt(in_cell / density);
+    if (ctx->col_edge_pct != 100) {
+        tx *= ctx->col_edge_pct / 100.0;
+        ty *= ctx->col_edge_pct / 100.0;
+    }
     g.nbinx         = std::max(1, (int)ceil((xprd - 0.0) / tx));
     g.nbiny         = std::max(1, (int)ceil((yprd - 0.0) / ty));
     g.binsizex      = (xprd - 0.0) / g.nbinx;
@@ -339,6 +348,17 @@ extern "C" int mdb_cp_tune(MdbCp* ctx, const char* key, int value)
         ctx->ty.pair_variant = value;
         return MDB_OK;
     }
+    if (!strcmp(key, "column_edge")) {
+        // the column grid sizes the atom and cluster buffers: only before atoms
+        if (value < 50 || value > 200) return fail(ctx, MDB_ERR_ARG, "column_edge: 50..200");
+        if (ctx->atom_cap != 0)
+            return fail(ctx, MDB_ERR_ARG, "column_edge is set before mdb_cp_set_atoms");
+        CK(cudaSetDevice(ctx->dev));
+        drop_graph(ctx);
+        ctx->col_edge_pct = value;
+        setup_columns(ctx);
+        return alloc_columns(ctx);
+    }
     if (!strcmp(key, "force_path")) {
         // compensated contexts run the pair-list kernel only
         if (value < 0 || value > 1 || (value == 1 && !ctx->mixed) || (value == 0 && ctx->comp))
@@ -433,6 +453,32 @@ extern "C" int mdb_cp_destroy(MdbCp* ctx)
     return MDB_OK;
 }
 
+// arrays sized by the column grid (setup_columns), with the stencil copied
+static int alloc_columns(MdbCp* ctx)
+{
+    cudaError_t e;
+    const int mb1 = ctx->g.mbins + 1;
+    dfree(ctx->stencil_d), dfree(ctx->col_count), dfree(ctx->col_start), dfree(ctx->col_fill);
+    dfree(ctx->ncl_col), dfree(ctx->cl_start), dfree(ctx->gcol_count), dfree(ctx->gfill);
+    dfree(ctx->jcol_n), dfree(ctx->jcol_start), dfree(ctx->ztab);
+    if ((e = dalloc(&ctx->stencil_d, ctx->g.nstencil)) != cudaSuccess ||
+        (e = dalloc(&ctx->col_count, mb1)) != cudaSuccess ||
+        (e = dalloc(&ctx->col_start, mb1 + 1)) != cudaSuccess ||
+        (e = dalloc(&ctx->col_fill, mb1)) != cudaSuccess ||
+        (e = dalloc(&ctx->ncl_col, mb1)) != cudaSuccess ||
+        (e = dalloc(&ctx->cl_start, mb1 + 1)) != cudaSuccess ||
+        (e = dalloc(&ctx->gcol_count, mb1)) != cudaSuccess ||
+        (e = dalloc(&ctx->gfill, mb1)) != cudaSuccess ||
+        (e = dalloc(&ctx->jcol_n, mb1)) != cudaSuccess ||
+        (e = dalloc(&ctx->jcol_start, mb1 + 1)) != cudaSuccess ||
+        (e = dalloc(&ctx->ztab, (size_t)ctx->g.mbins * (ctx->g.zq + 2))) != cudaSuccess)
+        return fail(ctx, MDB_ERR_NOMEM, "device allocation (columns)", e);
+    if ((e = cudaMemcpy(ctx->stencil_d, ctx->stencil.data(), sizeof(int) * ctx->g.nstencil,
+             cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(ctx, MDB_ERR_CUDA, "stencil copy", e);
+    return MDB_OK;
+}
+
 extern "C" int mdb_cp_create(const MdbParams* params, int cluster_n, int prune_every, MdbCp** out)
 {
     if (!params || !out) return MDB_ERR_ARG;
@@ -486,20 +532,8 @@ extern "C" int mdb_cp_create(const MdbParams* params, int cluster_n, int prune_e
             rc = fail(ctx, MDB_ERR_CUDA, "cudaStreamCreate", e);
             goto bad;
         }
-        const int mb1 = ctx->g.mbins + 1;
         if ((e = dalloc(&ctx->cnt, CP_SLOTS)) != cudaSuccess ||
             (e = dalloc(&ctx->zext, 1)) != cudaSuccess ||
-            (e = dalloc(&ctx->stencil_d, ctx->g.nstencil)) != cudaSuccess ||
-            (e = dalloc(&ctx->col_count, mb1)) != cudaSuccess ||
-            (e = dalloc(&ctx->col_start, mb1 + 1)) != cudaSuccess ||
-            (e = dalloc(&ctx->col_fill, mb1)) != cudaSuccess ||
-            (e = dalloc(&ctx->ncl_col, mb1)) != cudaSuccess ||
-            (e = dalloc(&ctx->cl_start, mb1 + 1)) != cudaSuccess ||
-            (e = dalloc(&ctx->gcol_count, mb1)) != cudaSuccess ||
-            (e = dalloc(&ctx->gfill, mb1)) != cudaSuccess ||
-            (e = dalloc(&ctx->jcol_n, mb1)) != cudaSuccess ||
-            (e = dalloc(&ctx->jcol_start, mb1 + 1)) != cudaSuccess ||
-            (e = dalloc(&ctx->ztab, (size_t)ctx->g.mbins * (ctx->g.zq + 2))) != cudaSuccess ||
             (e = dalloc(&ctx->red, 4 * RED_SLOTS)) != cudaSuccess ||
             (e = cudaMallocHost((void**)&ctx->h_cnt, CP_SLOTS * sizeof(int))) != cudaSuccess ||
             (e = cudaMallocHost((void**)&ctx->h_red, 4 * RED_SLOTS * sizeof(double))) !=
@@ -508,12 +542,7 @@ extern "C" int mdb_cp_create(const MdbParams* params, int cluster_n, int prune_e
             goto bad;
         }
         cudaMemset(ctx->cnt, 0, CP_SLOTS * sizeof(int));
-        cudaMemcpy(ctx->stencil_d, ctx->stencil.data(), sizeof(int) * ctx->g.nstencil,
-            cudaMemcpyHostToDevice);
-        if ((e = cudaGetLastError()) != cudaSuccess) {
-            rc = fail(ctx, MDB_ERR_CUDA, "setup copy", e);
-            goto bad;
-        }
+        if ((rc = alloc_columns(ctx)) != MDB_OK) goto bad;
     }
     *out = ctx;
     return MDB_OK;

@@ -651,7 +651,8 @@ class ClusterSystem:
     def __init__(self, *, xprd, yprd, zprd, cutforce, cutneigh, dt, dtforce, natoms,
                  cluster_n=4, prune_every=0, mass=1.0, half_neigh=0, precision=PREC_FP64,
                  ntypes=1, epsilon=1.0, sigma=1.0, epsilon_per_type=None, sigma_per_type=None,
-                 reneigh_every=20, nstat=100, maxneighs=0, device=0, **_ignored):
+                 reneigh_every=20, nstat=100, maxneighs=0, device=0, column_edge=100,
+                 **_ignored):
         self.lib = load()
         if isinstance(precision, str):
             precision = PRECISIONS[precision]
@@ -676,6 +677,10 @@ class ClusterSystem:
         self.params = p
         self.M, self.N = 4, cluster_n
         self.nlocal = 0
+        self.column_edge = column_edge
+        if column_edge != 100:
+            # the column grid (bin size) in percent of the reference's
+            self._ck(self.lib.mdb_cp_tune(h, b"column_edge", int(column_edge)), "column_edge")
 
     def close(self):
         if getattr(self, "h", None):

@@ -3,15 +3,17 @@ throughput), run on fake members with a throughput model in place of the
 device: it must find the choices the model rewards beyond the noise margin,
 keep the defaults where a change gains less, and close every system it
 builds (the tuned members too: the caller builds its own from the choice)."""
+import itertools
+
 import pytest
 
 import autotune as AT
 
 
 class FakeMember:
-    def __init__(self, sp, n, half, log):
+    def __init__(self, sp, n, half, edge, log):
         self.natoms, self.nlocal = sp["natoms"], sp["natoms"]
-        self.cluster_n, self.half = n, half
+        self.cluster_n, self.half, self.edge = n, half, edge
         self.launch = {k: AT.DEFAULT[k]
                        for k in ("force_block", "force_variant", "force_cpw", "force_jpl")}
         self.closed = False
@@ -30,7 +32,8 @@ def model_rate(members):
     """Time of the ensemble = sum over members of natoms x cost, where the model
     rewards: 4x8 half lists for the 500-atom class (-20 %), full lists for the 4000-atom
     class (-1 %, inside the margin), 256 threads for the 4000-atom class
-    (-10 %), eight i-clusters per warp for the 32,000-atom class (-8 %); plus
+    (-10 %), eight i-clusters per warp for the 32,000-atom class (-8 %), a
+    column edge of 125 % for the 32,000-atom class (-6 %; 80 % costs +5 %); plus
     one launch per distinct (shape, form, launch) group."""
     t, groups = 0.0, set()
     for m in members:
@@ -45,6 +48,8 @@ def model_rate(members):
             c *= 0.9
         if cls == AT.size_class(32000) and m.launch["force_cpw"] == 8:
             c *= 0.92
+        if cls == AT.size_class(32000):
+            c *= {80: 1.05, 100: 1.0, 125: 0.94}[m.edge]
         if m.launch["force_variant"] != AT.DEFAULT["force_variant"]:
             c *= 1.05
         t += m.natoms * c
@@ -59,14 +64,18 @@ def test_coordinate_descent_finds_rewarded_choices():
     # 5.5 % and 2.7 % of the ensemble, the full-list gain 0.3 %
     specs = [{"natoms": 500}] * 40 + [{"natoms": 4000}] * 5 + [{"natoms": 32000}]
     log = []
-    choice, trials = AT.tune_ensemble(specs, lambda sp, n, h: FakeMember(sp, n, h, log),
+    choice, trials = AT.tune_ensemble(specs, lambda sp, n, h, e: FakeMember(sp, n, h, e, log),
                                       rate=model_rate)
     c512, c4k, c32k = (choice[AT.size_class(n)] for n in (500, 4000, 32000))
     assert (c512["cluster_n"], c512["half"]) == (8, 1)
     assert c512["force_block"] == AT.DEFAULT["force_block"]
     assert (c4k["cluster_n"], c4k["half"]) == (4, 1)      # full lists gain < margin
     assert c4k["force_block"] == 256
-    assert c32k == dict(AT.DEFAULT, force_cpw=8)
+    assert c32k == dict(AT.DEFAULT, force_cpw=8, column_edge=125)
+    # the bin size stays the reference's where nothing rewards another
+    assert c512["column_edge"] == c4k["column_edge"] == 100
+    # the tuned members were built with their bin size
+    assert any(m.edge == 125 for m in log) and any(m.edge == 80 for m in log)
     # force_cpw 8 was never tried on a 4x8 shape
     assert all(t[1]["force_cpw"] != 8 or t[1]["cluster_n"] == 4 for t in trials)
     assert all(c["force_variant"] == AT.DEFAULT["force_variant"] for c in choice.values())
@@ -80,9 +89,9 @@ def test_coordinate_descent_finds_rewarded_choices():
 def test_no_change_within_noise():
     specs = [{"natoms": 1000}] * 3
     log = []
-    flat = iter([1.0, 1.01, 0.99, 1.015, 1.0, 1.019, 0.98, 1.0, 1.0, 1.0, 1.012, 1.0, 0.99,
-                 1.0, 1.005])
-    choice, trials = AT.tune_ensemble(specs, lambda sp, n, h: FakeMember(sp, n, h, log),
+    flat = itertools.cycle([1.0, 1.01, 0.99, 1.015, 1.0, 1.019, 0.98, 1.0, 1.0, 1.0, 1.012,
+                            1.0, 0.99, 1.0, 1.005])
+    choice, trials = AT.tune_ensemble(specs, lambda sp, n, h, e: FakeMember(sp, n, h, e, log),
                                       rate=lambda ms: next(flat))
     assert choice == {AT.size_class(1000): AT.DEFAULT}
     assert all(m.closed for m in log)
