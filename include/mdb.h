@@ -190,9 +190,13 @@ int mdb_run(MdbCtx* ctx, int first_step, int nsteps, MdbThermo* samples, int max
  * Halo atoms are binned, listed and imaged by the periodic directions like
  * owned atoms but get no force row, no integration and no thermo; the caller
  * refreshes their positions before every force evaluation and runs the
- * per-step hooks (mdb_run refuses a context with halo atoms). Full lists and
- * LJ only: half lists would need the reverse force exchange and EAM the
- * mid-step F'(rho) exchange. */
+ * per-step hooks (mdb_run refuses a context with halo atoms). LJ only (EAM
+ * would need a mid-step F'(rho) exchange, which the reference's EAM does not
+ * have either). Full and half lists: the halo covers both z faces, as the
+ * reference's fullShell method, whose reverse() moves nothing
+ * (common/shell_methods.h:59-88): with half lists a halo atom is listed like
+ * a ghost and gets no reaction, so each domain computes the pairs across its
+ * faces for its own atoms. */
 /* Atoms [nown, nlocal) of the last mdb_set_atoms are halo atoms (nown =
  * nlocal: none); mdb_set_atoms resets it. */
 int mdb_set_owned(MdbCtx* ctx, int nown);

@@ -1144,8 +1144,11 @@ extern "C" int mdb_set_owned(MdbCtx* ctx, int nown)
 {
     NEED_ATOMS();
     if (nown < 1 || nown > ctx->nlocal) return fail(ctx, MDB_ERR_ARG, "owned count out of range");
-    if (nown < ctx->nlocal && (ctx->p.half_neigh || ctx->p.force_field != MDB_FF_LJ))
-        return fail(ctx, MDB_ERR_ARG, "halo atoms need full lists and LJ forces");
+    // half lists: a halo atom is listed like a ghost (index past every owned
+    // atom) and gets no reaction, so each domain computes the pairs across its
+    // faces for its own atoms, with no reverse exchange of forces
+    if (nown < ctx->nlocal && ctx->p.force_field != MDB_FF_LJ)
+        return fail(ctx, MDB_ERR_ARG, "halo atoms need LJ forces");
     ctx->nown = nown == ctx->nlocal ? 0 : nown;
     drop_graphs(ctx);
     return MDB_OK;

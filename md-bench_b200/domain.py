@@ -18,8 +18,12 @@ period:
   the initial integration and before the force (``mdb_gather_positions`` /
   ``mdb_set_halo_positions``).
 
-Full lists, so no reverse exchange: each rank computes the forces of its own
-atoms from owned and halo neighbours. Thermo sums are reduced over ranks.
+The halo covers both z faces, as the reference's fullShell method, whose
+reverse() moves nothing (common/shell_methods.h:59-88): each rank computes the
+forces of its own atoms from owned and halo neighbours. With half lists a
+halo atom is listed like a ghost and gets no reaction, so a pair across a slab
+face is computed on both ranks, each for its own atom; there is no reverse
+exchange of forces. Thermo sums are reduced over ranks.
 
 The exchange goes through a ``Transport``: ``DistTransport`` uses
 torch.distributed point-to-point calls (NCCL with device tensors between
@@ -254,12 +258,13 @@ class SlabRun:
 
 
 class MdbEngine:
-    """A rank's atoms in a libmdb Verlet-list context (FP64 or mixed, full
-    lists): owned atoms, then the halo; halo positions move on the device."""
+    """A rank's atoms in a libmdb Verlet-list context (FP64 or mixed, full or
+    half lists): owned atoms, then the halo; halo positions move on the
+    device."""
 
-    def __init__(self, torch, mdb, hp, device, precision="fp64"):
+    def __init__(self, torch, mdb, hp, device, precision="fp64", half_neigh=0):
         self.torch, self.mdb, self.hp = torch, mdb, hp
-        self.device, self.precision = device, precision
+        self.device, self.precision, self.half_neigh = device, precision, half_neigh
         self.sys = None
         self._idx = {}  # device copies of the halo index arrays, per load
 
@@ -269,7 +274,8 @@ class MdbEngine:
         if self.sys is None:
             # periodic in x and y only: z neighbours come as halo atoms
             self.sys = mdb.system_from_host(self.hp, n + nh, precision=self.precision,
-                                            device=self.device, pbc=(1, 1, 0), half_neigh=0)
+                                            device=self.device, pbc=(1, 1, 0),
+                                            half_neigh=self.half_neigh)
         xa = np.concatenate([x, hx]) if nh else x
         va = np.concatenate([v, np.zeros((nh, 3))]) if nh else v
         ta = np.concatenate([t, ht]).astype(np.int32) if nh else t.astype(np.int32)
