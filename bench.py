@@ -58,7 +58,8 @@ def parse():
     ap.add_argument("--profile", choices=[f"{k}_{p}{h}" for k in ("lj", "eam", "cp44", "cp48")
                                           for p in ("mixed", "fp64") for h in ("", "_half")]
                     + [f"{k}_mixed{h}_pairs" for k in ("cp44", "cp48") for h in ("", "_half")]
-                    + ["c5_mixed", "c5_mixed_pairs", "c5_fp64", "c4_mixed", "stub"]
+                    + ["c5_mixed", "c5_mixed_pairs", "c5_fp64", "c4_mixed", "stub",
+                       "cp44_mixed_half_checked"]
                     + [k for k in VARIANT_SPEC if "mixedcomp" in k],
                     help="run one variant only (W+K bench steps + force timing), for ncu")
     ap.add_argument("--cells", type=int, default=None, help="fcc cells per side (profiling)")
@@ -251,6 +252,30 @@ def measure(torch, mdb, kind, precision, args, device, half=0, steps=None, path=
         out["pair_stats"] = {"pair_derivations": d1 - d0,
                              "pair_md_steps": (args.warmup + steps) * every,
                              "pair_slots_per_atom": round(2.0 * codes / nat, 2)}
+    return out
+
+
+def checked_rebuilds(torch, mdb, args, device, limit=0.15):
+    """The headline workload with displacement-checked rebuilds (any atom
+    moving farther than skin / 2 since the last build also rebuilds, besides
+    the fixed schedule), the decision taken on the device (a conditional CUDA
+    graph per step) and on the host (one synchronisation per step); W + K
+    bench steps of 20 MD steps each, device-timed like the headline."""
+    out = {"max_displacement": limit}
+    for mode, host in (("device", 0), ("host", 1)):
+        s, (x, v, t) = make_system(mdb, HEAD["kind"], HEAD["precision"], args, device,
+                                   HEAD["half"], HEAD["path"])
+        s.tune("check_on_host", host)
+        s.set_rebuild_check(limit)
+        s.set_atoms(x, v, t)
+        s.setup()
+        secs, launches, _, _ = time_run(torch, s, args.steps, args.warmup, 20)
+        sched, trig = s.rebuilds()
+        out[mode] = {"value": len(t) * 20 * args.steps / secs,
+                     "ms_per_step": 1e3 * secs / args.steps, "rebuilds_scheduled": sched,
+                     "rebuilds_checked": trig, "device_decided_steps": s.check_stats()[0],
+                     "gpu_launches": launches}
+        s.close()
     return out
 
 
@@ -728,6 +753,10 @@ def main():
         print(json.dumps(dict(profile=args.profile, **stub_bench(torch, mdb, local))),
               flush=True)
         return
+    if args.profile == "cp44_mixed_half_checked":
+        print(json.dumps(dict(profile=args.profile, **checked_rebuilds(torch, mdb, args, local))),
+              flush=True)
+        return
     if args.profile == "c4_mixed":
         res = c4_ensemble(torch, mdb, args, local, rank, world, dist)
         if rank == 0:
@@ -862,6 +891,7 @@ def main():
                                "cutoff, so the FP64 path itself drifts past 1e-4 per 1000 "
                                "steps on these workloads; excess_drift_vs_fp64 is the mixed "
                                "path's part"}
+        var["cp44_mixed_half_checked"] = checked_rebuilds(torch, mdb, args, local)
         var["c4_ensemble_mixed"] = c4_ensemble(torch, mdb, args, local)
         var["stub_gather_fp64"] = stub_bench(torch, mdb, local)
 

@@ -151,13 +151,27 @@ int mdb_cp_run(MdbCp* ctx, int first_step, int nsteps, MdbThermo* samples, int m
  * rebuilds every reneigh_every steps). With max_displacement > 0, mdb_cp_run
  * also rebuilds in any step in which some atom has moved farther than
  * max_displacement since the last build (skin / 2 keeps every list complete
- * whatever the motion); the integrator tests the displacement and the host
- * reads one flag per step. 0 (the default) restores the fixed schedule alone.
- * After a change the next step rebuilds first. */
+ * whatever the motion); the integrator tests the displacement and raises a
+ * device flag. The decision is taken on the device: each such step is one
+ * CUDA graph whose conditional nodes run updateAtoms and the whole rebuild
+ * when the flag is up, else updatePbc, then the force, with no host
+ * synchronisation. A rebuild there that overflows a buffer stops the call's
+ * later steps on the device; the host then grows the buffer, replays that
+ * build and resumes from the next step, so the result is that of growing
+ * the buffer at once. Scheduled rebuilds, pruning, thermo samples, a call's
+ * first and last step, the pair-list path and the tuning key
+ * "check_on_host" = 1 read the flag on the host after the integration
+ * instead (the same decisions, so the same trajectory). 0 (the default)
+ * restores the fixed schedule alone. After a change the next step rebuilds
+ * first. */
 int mdb_cp_set_rebuild_check(MdbCp* ctx, double max_displacement);
 /* Rebuilds performed by mdb_cp_run with the check on: on the fixed schedule,
  * and triggered by the displacement test. */
 int mdb_cp_get_rebuilds(MdbCp* ctx, long long* scheduled, long long* checked);
+/* Checked steps decided on the device so far, and rebuilds among them that
+ * overflowed a buffer and were replayed by the host (no counterpart in the
+ * reference). */
+int mdb_cp_get_check_stats(MdbCp* ctx, long long* graph_steps, long long* replays);
 
 /* ---- ensembles ----------------------------------------------------------------
  * No counterpart in the reference (which runs one system per process). Many

@@ -96,6 +96,21 @@ struct MdbCp {
     int* h_dflag       = nullptr;
     bool snap_valid    = false;
     long long rebuilds_sched = 0, rebuilds_check = 0;
+    // the check decided on the device (default; "check_on_host" 1: the host
+    // reads the flag every step): one graph per step with conditional nodes
+    // that rebuild when the flag is up, and skip the force and every later
+    // step of the call once such a rebuild overflowed a buffer (the host
+    // grows it, replays that build and resumes). dstate: {stopped, steps
+    // run, rebuilds} on the device, h_dstate its pinned copy
+    bool check_host    = false;
+    int* dstate        = nullptr;
+    int* h_dstate      = nullptr;
+    cudaStream_t s_cap[2] = {nullptr, nullptr}; // capture streams of the bodies
+    CpGraph g_chk;
+    // kernels of the checked step graph's parts, for the launch count: the
+    // step's fixed part, the ghost update, the rebuild, the force
+    long long chk_k[4] = {0, 0, 0, 0};
+    long long chk_steps = 0, chk_replays = 0; // graph steps run, overflowed rebuilds replayed
     // pair-list force path of the mixed scheme (force_path 1, mdb_cp_pairs.cu):
     // codes per (i pair, chunk), their counts, the positions they were
     // derived from, and {derive flag, derivations run}
@@ -147,6 +162,9 @@ static void drop_graph(MdbCp* ctx)
     if (ctx->g_plain.exec) cudaGraphExecDestroy(ctx->g_plain.exec);
     ctx->g_plain.exec    = nullptr;
     ctx->g_plain.kernels = 0;
+    if (ctx->g_chk.exec) cudaGraphExecDestroy(ctx->g_chk.exec);
+    ctx->g_chk.exec    = nullptr;
+    ctx->g_chk.kernels = 0;
 }
 
 static int ensure_pairs(MdbCp* ctx);
@@ -348,6 +366,13 @@ extern "C" int mdb_cp_tune(MdbCp* ctx, const char* key, int value)
         ctx->ty.pair_variant = value;
         return MDB_OK;
     }
+    if (!strcmp(key, "check_on_host")) {
+        // 1: the displacement check's flag is read by the host every step
+        if (value < 0 || value > 1) return MDB_ERR_ARG;
+        drop_graph(ctx);
+        ctx->check_host = value != 0;
+        return MDB_OK;
+    }
     if (!strcmp(key, "column_edge")) {
         // the column grid sizes the atom and cluster buffers: only before atoms
         if (value < 50 || value > 200) return fail(ctx, MDB_ERR_ARG, "column_edge: 50..200");
@@ -432,6 +457,9 @@ static void free_all(MdbCp* ctx)
     ctx->pair_ncl = ctx->pair_chmax = 0;
     if (ctx->h_dflag) cudaFreeHost(ctx->h_dflag);
     ctx->h_dflag  = nullptr;
+    dfree(ctx->dstate);
+    if (ctx->h_dstate) cudaFreeHost(ctx->h_dstate);
+    ctx->h_dstate = nullptr;
     ctx->xbuild_n = 0;
     dfree(ctx->cnt), dfree(ctx->zext), dfree(ctx->scan_scratch), dfree(ctx->partials);
     dfree(ctx->red), dfree(ctx->stage), dfree(ctx->stage_i);
@@ -449,6 +477,8 @@ extern "C" int mdb_cp_destroy(MdbCp* ctx)
     drop_graph(ctx);
     free_all(ctx);
     if (ctx->s) cudaStreamDestroy(ctx->s);
+    for (cudaStream_t c : ctx->s_cap)
+        if (c) cudaStreamDestroy(c);
     delete ctx;
     return MDB_OK;
 }
@@ -1332,24 +1362,255 @@ static int capture_plain(MdbCp* ctx)
     return MDB_OK;
 }
 
+// ---- displacement check decided on the device --------------------------------
+// dstate = {stopped, steps run, rebuilds}: a step's graph opens with a gate
+// (the step runs unless a rebuild earlier in the call overflowed a buffer),
+// rebuilds when the integrator raised the displacement flag, and runs the
+// force unless that rebuild overflowed.
+__global__ void k_chk_gate(cudaGraphConditionalHandle h, int* st)
+{
+    const bool go = st[0] == 0;
+    if (go) st[1]++;
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+__global__ void k_chk_reb(cudaGraphConditionalHandle h, const int* dflag, int* st)
+{
+    const bool reb = *dflag != 0;
+    if (reb) st[2]++;
+    cudaGraphSetConditional(h, reb ? 1u : 0u);
+}
+
+// what eval_build would grow (or reject) stops the call
+__global__ void k_chk_built(const int* cnt, int ngc_cap, int maxneighs, int* st)
+{
+    if (cnt[CP_BADBIN] > 0 || cnt[CP_NGC_TOTAL] > ngc_cap || cnt[CP_MAXNEED] >= maxneighs)
+        st[0] = 1;
+}
+
+__global__ void k_chk_force(cudaGraphConditionalHandle h, const int* st)
+{
+    cudaGraphSetConditional(h, st[0] == 0 ? 1u : 0u);
+}
+
+// An "if" node (size 2: if / else) on handle h after the current capture
+// point of stream s; its body graphs in bodies[0..size).
+static cudaError_t cap_conditional(cudaStream_t s, cudaGraphConditionalHandle h, unsigned size,
+    cudaGraph_t* bodies)
+{
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g                = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd                    = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd);
+    if (e != cudaSuccess) return e;
+    cudaGraphNodeParams p = {};
+    p.type                = cudaGraphNodeTypeConditional;
+    p.conditional.handle  = h;
+    p.conditional.type    = cudaGraphCondTypeIf;
+    p.conditional.size    = size;
+    cudaGraphNode_t node;
+    if ((e = cudaGraphAddNode(&node, g, deps, nd, &p)) != cudaSuccess) return e;
+    for (unsigned k = 0; k < size; k++) bodies[k] = p.conditional.phGraph_out[k];
+    return cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+}
+
+static cudaError_t cap_handle(cudaStream_t s, cudaGraphConditionalHandle* h)
+{
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamGetCaptureInfo(s, &st, nullptr, &g, nullptr, nullptr);
+    if (e != cudaSuccess) return e;
+    return cudaGraphConditionalHandleCreate(h, g, 0, 0);
+}
+
+// One checked step as a graph: finalIntegrate(n-1) + initialIntegrate(n) with
+// the displacement test, then either updateAtoms + the whole rebuild (an atom
+// moved past the limit) or updatePbc, then the force; all of it only while no
+// rebuild of this call has overflowed a buffer. The bodies are captured on two
+// further streams (enq_* enqueue on ctx->s, which points at the capturing one).
+static int capture_chk(MdbCp* ctx)
+{
+    cudaError_t e = cudaSuccess;
+    for (cudaStream_t& c : ctx->s_cap)
+        if (!c && (e = cudaStreamCreateWithFlags(&c, cudaStreamNonBlocking)) != cudaSuccess)
+            return fail(ctx, MDB_ERR_CUDA, "capture stream", e);
+    const cudaStream_t s0 = ctx->s, s1 = ctx->s_cap[0], s2 = ctx->s_cap[1];
+    const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+    cudaGraphConditionalHandle h_step = 0, h_reb = 0, h_force = 0;
+    cudaGraph_t step[1] = {nullptr}, reb[2] = {nullptr, nullptr}, frc[1] = {nullptr};
+    cudaGraph_t graph = nullptr;
+    const long long m0 = mark();
+    long long* k = ctx->chk_k;
+    bool cap1 = false, cap2 = false;
+    auto body2 = [&](cudaGraph_t g, int what) -> cudaError_t {
+        // one body of the inner conditionals, captured on s2
+        cudaError_t r = cudaStreamBeginCaptureToGraph(s2, g, nullptr, nullptr, 0, mode);
+        if (r != cudaSuccess) return r;
+        cap2 = true;
+        ctx->s = s2;
+        long long m = mark();
+        if (what == 0) {
+            enq_gather(ctx, 1);
+            enq_build(ctx);
+            k_chk_built<<<1, 1, 0, s2>>>(ctx->cnt, ctx->ngc_cap, ctx->maxneighs, ctx->dstate);
+            cudaMemcpyAsync(ctx->xbuild, ctx->cx, sizeof(double4) * ctx->ncl_cap * ctx->M,
+                cudaMemcpyDeviceToDevice, s2);
+            cudaMemsetAsync(ctx->dflag, 0, sizeof(int), s2);
+            k[2] = mark() - m + 1;
+        } else if (what == 1) {
+            enq_ghost_update(ctx);
+            k[1] = mark() - m;
+        } else {
+            enq_force(ctx, false);
+            k[3] = mark() - m;
+        }
+        ctx->s = s1;
+        r = cudaGetLastError();
+        cudaGraph_t out = nullptr;
+        cudaError_t r2 = cudaStreamEndCapture(s2, &out);
+        cap2 = false;
+        return r != cudaSuccess ? r : r2;
+    };
+    e = cudaStreamBeginCapture(s0, mode);
+    if (e == cudaSuccess) e = cap_handle(s0, &h_step);
+    if (e == cudaSuccess) {
+        k_chk_gate<<<1, 1, 0, s0>>>(h_step, ctx->dstate);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cap_conditional(s0, h_step, 1, step);
+    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(s1, step[0], nullptr, nullptr, 0, mode);
+    if (e == cudaSuccess) {
+        cap1   = true;
+        ctx->s = s1;
+        long long m = mark();
+        enq_final_initial(ctx);
+        k[0] = mark() - m + 2;
+        e = cap_handle(s1, &h_reb);
+    }
+    if (e == cudaSuccess) {
+        k_chk_reb<<<1, 1, 0, s1>>>(h_reb, ctx->dflag, ctx->dstate);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cap_conditional(s1, h_reb, 2, reb);
+    if (e == cudaSuccess) e = body2(reb[0], 0);
+    if (e == cudaSuccess) e = body2(reb[1], 1);
+    if (e == cudaSuccess) e = cap_handle(s1, &h_force);
+    if (e == cudaSuccess) {
+        k_chk_force<<<1, 1, 0, s1>>>(h_force, ctx->dstate);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cap_conditional(s1, h_force, 1, frc);
+    if (e == cudaSuccess) e = body2(frc[0], 2);
+    ctx->s = s0;
+    mdb::g_launches = m0;
+    if (cap2) {
+        cudaGraph_t g2 = nullptr;
+        cudaStreamEndCapture(s2, &g2);
+    }
+    if (cap1) {
+        cudaGraph_t g1       = nullptr;
+        const cudaError_t e1 = cudaStreamEndCapture(s1, &g1);
+        if (e == cudaSuccess) e = e1;
+    }
+    const cudaError_t e0 = cudaStreamEndCapture(s0, &graph);
+    if (e == cudaSuccess) e = e0;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&ctx->g_chk.exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, MDB_ERR_CUDA, "checked step graph", e);
+    }
+    ctx->g_chk.kernels = 1;
+    return MDB_OK;
+}
+
+// The device's record of the graph steps launched since the last call (their
+// step indices in `launched`): counts their rebuilds and kernels and, when a
+// rebuild overflowed a buffer, grows it, replays that build (from the atom
+// arrays its updateAtoms wrote: the build is idempotent) and evaluates that
+// step's force. *resume = that step (the later ones did nothing), else -1.
+static int chk_resolve(MdbCp* ctx, std::vector<int>& launched, int* resume)
+{
+    *resume = -1;
+    if (launched.empty()) return MDB_OK;
+    CK(cudaMemcpyAsync(ctx->h_dstate, ctx->dstate, 3 * sizeof(int), cudaMemcpyDeviceToHost,
+        ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    const int stopped = ctx->h_dstate[0], ran = ctx->h_dstate[1], reb = ctx->h_dstate[2];
+    CK(cudaMemsetAsync(ctx->dstate, 0, 3 * sizeof(int), ctx->s));
+    const long long* k = ctx->chk_k;
+    ctx->rebuilds_check += reb;
+    ctx->chk_steps += ran;
+    ctx->chk_replays += stopped ? 1 : 0;
+    ctx->launches += (long long)launched.size() + ran * k[0] + (ran - reb) * k[1] + reb * k[2] +
+                     (ran - stopped) * k[3];
+    if (stopped) {
+        if (ran < 1 || ran > (int)launched.size())
+            return fail(ctx, MDB_ERR_CUDA, "checked steps: inconsistent device record");
+        const int n = launched[ran - 1];
+        CK(cudaMemcpyAsync(ctx->h_cnt, ctx->cnt, CP_SLOTS * sizeof(int), cudaMemcpyDeviceToHost,
+            ctx->s));
+        CK(cudaStreamSynchronize(ctx->s));
+        const int r = eval_build(ctx, CHK_ALL);
+        if (r < 0) return -r;
+        int rc = do_build(ctx);
+        if (rc) return rc;
+        long long m = mark();
+        enq_force(ctx, false);
+        account(ctx, m);
+        *resume = n;
+    }
+    launched.clear();
+    return MDB_OK;
+}
+
 // The timestep loop with the displacement check: each step's initial
-// integration also tests every atom's displacement since the last build; the
-// host reads the flag (one synchronisation per step) and rebuilds in that
-// step when an atom moved farther than disp_max, besides the reference's
-// fixed schedule. Lists are then complete at every step for any motion.
+// integration also tests every atom's displacement since the last build, and
+// the step rebuilds when an atom moved farther than disp_max, besides the
+// reference's fixed schedule. Lists are then complete at every step for any
+// motion. The decision is taken on the device (a conditional graph per step,
+// no host synchronisation) except at scheduled rebuilds, pruning, thermo
+// samples, a call's first and last step and with the pair-list path, where
+// (as with "check_on_host") the host reads the flag after the integration.
 static int run_checked(MdbCp* ctx, int first_step, int nsteps, MdbThermo* samples,
     int max_samples, int* nsamples)
 {
     int nslot = 0;
-    std::vector<int> slot_step;
-    const int last     = first_step + nsteps - 1;
-    bool pending_final = false;
+    std::vector<int> slot_step, launched;
+    const int last       = first_step + nsteps - 1;
+    bool pending_final   = false;
+    const bool on_device = !ctx->check_host && !pair_path(ctx);
+    if (on_device && !ctx->dstate) {
+        CK(dalloc(&ctx->dstate, 3));
+        CK(cudaMallocHost((void**)&ctx->h_dstate, 3 * sizeof(int)));
+        CK(cudaMemsetAsync(ctx->dstate, 0, 3 * sizeof(int), ctx->s));
+    }
     for (int n = first_step; n <= last; n++) {
         const bool sched  = (n + 1) % ctx->p.reneigh_every == 0;
         const bool prune  = !sched && (n + 1) % ctx->prune_every == 0;
         const bool sample = max_samples > 0 && (n + 1) % ctx->p.nstat == 0;
-        const bool had    = ctx->snap_valid;
-        long long m       = mark();
+        if (on_device && pending_final && ctx->snap_valid && !sched && !prune && !sample &&
+            n != last) {
+            if (!ctx->g_chk.exec) {
+                int rc = capture_chk(ctx);
+                if (rc) return rc;
+            }
+            CK(cudaGraphLaunch(ctx->g_chk.exec, ctx->s));
+            launched.push_back(n);
+            continue; // the step leaves its final integration pending
+        }
+        if (!launched.empty()) {
+            int resume = -1;
+            int rc     = chk_resolve(ctx, launched, &resume);
+            if (rc) return rc;
+            if (resume >= 0) {
+                n = resume; // steps after it did nothing: run them again
+                continue;
+            }
+        }
+        const bool had = ctx->snap_valid;
+        long long m    = mark();
         if (pending_final) enq_final_initial(ctx);
         else enq_initial(ctx);
         pending_final = false;
@@ -1407,6 +1668,14 @@ extern "C" int mdb_cp_set_rebuild_check(MdbCp* ctx, double max_displacement)
     drop_graph(ctx);
     ctx->disp_max   = max_displacement;
     ctx->snap_valid = false; // the next step rebuilds (and snapshots) first
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_get_check_stats(MdbCp* ctx, long long* graph_steps, long long* replays)
+{
+    if (!ctx) return MDB_ERR_ARG;
+    if (graph_steps) *graph_steps = ctx->chk_steps;
+    if (replays) *replays = ctx->chk_replays;
     return MDB_OK;
 }
 

@@ -100,7 +100,7 @@ CP_EXPORTS = [
     "mdb_cp_ensemble_destroy", "mdb_cp_ensemble_last_error", "mdb_cp_ensemble_stream",
     "mdb_cp_ensemble_launch_count", "mdb_cp_ensemble_run", "mdb_cp_ensemble_tune",
     "mdb_cp_set_rebuild_check", "mdb_cp_get_rebuilds", "mdb_cp_set_pair_buffer",
-    "mdb_cp_get_pair_stats",
+    "mdb_cp_get_pair_stats", "mdb_cp_get_check_stats",
 ]
 # every symbol include/mdb_host.h declares
 HOST_EXPORTS = [
@@ -182,6 +182,7 @@ def load():
         "mdb_cp_set_pair_buffer": ([vp, C.c_double], ip),
         "mdb_cp_get_pair_stats": ([vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], ip),
         "mdb_cp_get_rebuilds": ([vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], ip),
+        "mdb_cp_get_check_stats": ([vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], ip),
         "mdb_cp_ensemble_create": ([C.POINTER(vp), ip, C.POINTER(vp)], ip),
         "mdb_cp_ensemble_destroy": ([vp], ip),
         "mdb_cp_ensemble_last_error": ([vp], C.c_char_p),
@@ -888,6 +889,14 @@ class ClusterSystem:
         a, b = C.c_longlong(), C.c_longlong()
         self._ck(self.lib.mdb_cp_get_rebuilds(self.h, C.byref(a), C.byref(b)),
                  "mdb_cp_get_rebuilds")
+        return a.value, b.value
+
+    def check_stats(self):
+        """(checked steps decided on the device, overflowed rebuilds among them
+        replayed by the host)."""
+        a, b = C.c_longlong(), C.c_longlong()
+        self._ck(self.lib.mdb_cp_get_check_stats(self.h, C.byref(a), C.byref(b)),
+                 "mdb_cp_get_check_stats")
         return a.value, b.value
 
     def time_force(self, reps=20):
