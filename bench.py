@@ -327,7 +327,8 @@ class Replicas:
             self.cache[key] = (hp, x, v, t)
         return self.cache[key]
 
-    def build(self, sp, cluster_n, half, column_edge=100, choice=None, precision="mixed"):
+    def build(self, sp, cluster_n, half, column_edge=100, choice=None, precision="mixed",
+              check=0.0):
         import autotune as AT
         hp, x, v, t = self.state(sp)
         s = self.mdb.ClusterSystem(natoms=len(t), cluster_n=cluster_n, half_neigh=half,
@@ -339,15 +340,19 @@ class Replicas:
                                    nstat=hp.nstat, ntypes=hp.ntypes)
         if choice is not None and precision == "mixed":
             AT.apply_launch(s, choice)
+        if check > 0.0:
+            s.set_rebuild_check(check)
         s.set_atoms(x, v, t)
         s.setup()
         return s
 
 
-def run_ensemble(torch, mdb, members, args, every=20):
+def run_ensemble(torch, mdb, members, args, every=20, check_on_host=None):
     """Device time of args.steps rebuild periods of an ensemble (after
     args.warmup untimed ones) and the energy drift of every member."""
     ens = mdb.Ensemble(members)
+    if check_on_host is not None:
+        ens.tune("check_on_host", check_on_host)
     th0 = [m.thermo() for m in members]
     stream = torch.cuda.ExternalStream(ens.stream)
     n = 0
@@ -468,6 +473,20 @@ def c4_ensemble(torch, mdb, args, device, rank=0, world=1, dist=None):
     serial = reduce_scalar(torch, dist, serial, "max", "cuda")
     for m in members:
         m.close()
+    # displacement-checked rebuilds (limit skin / 2, every member rebuilds when
+    # one trips), decided on the device (a conditional graph per step) and on
+    # the host (one synchronisation per step)
+    checked = {"max_displacement": 0.15}
+    for mode, host in (("device", 0), ("host", 1)):
+        members = [pool.build(sp, c["cluster_n"], c["half"], c["column_edge"], c, check=0.15)
+                   for sp, c in zip(specs, pick)]
+        sc, _, _, _ = run_ensemble(torch, mdb, members, args, every, check_on_host=host)
+        sc = reduce_scalar(torch, dist, sc, "max", "cuda")
+        checked[mode] = {"value": total_atoms * every * args.steps / sc,
+                         "rebuilds_scheduled": members[0].rebuilds()[0],
+                         "rebuilds_checked": members[0].rebuilds()[1]}
+        for m in members:
+            m.close()
     nat = total_atoms
     shapes = {}
     for c in pick:
@@ -483,6 +502,7 @@ def c4_ensemble(torch, mdb, args, device, rank=0, world=1, dist=None):
                                                           "max", "cuda"),
             "excess_drift_vs_fp64_median_abs": float(np.median(np.abs(d32 - d64))),
             "fp64_value": nat * every * args.steps / secs64,
+            "checked_rebuilds": checked,
             "serial_value": nat * every / serial,
             "autotune": {"seconds": round(tune_secs, 2), "trials": len(trials),
                          "choice_per_size_class": {str(k): v for k, v in choice.items()},

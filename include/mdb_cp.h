@@ -195,10 +195,20 @@ long long mdb_cp_ensemble_launch_count(const MdbCpEnsemble* ens);
  * integrator, the ghost update and the force kernel each run as one launch
  * over all members (members grouped by cluster shape, list form, types and
  * launch settings); 0: every member runs its own kernel sequence on its own
- * graph branch. Results are the same either way. */
+ * graph branch. Results are the same either way.
+ * "check_on_host" = 1: members with the displacement check
+ * (mdb_cp_set_rebuild_check; batched ensembles only) have the host read their
+ * flags after every integration; 0 (the default): each checked step is one
+ * CUDA graph launch whose conditional nodes rebuild every member when one
+ * member's flag is up, with no host synchronisation, and a rebuild there that
+ * overflows a member's buffer is replayed by the host at its next
+ * synchronisation, as for a single system. The same decisions either way. */
 int mdb_cp_ensemble_tune(MdbCpEnsemble* ens, const char* key, int value);
 int mdb_cp_ensemble_run(MdbCpEnsemble* ens, int first_step, int nsteps, MdbThermo* samples,
     int max_samples, int* nsamples);
+/* Checked steps decided on the device so far, and overflowed rebuilds among
+ * them replayed by the host (no counterpart in the reference). */
+int mdb_cp_ensemble_check_stats(MdbCpEnsemble* ens, long long* graph_steps, long long* replays);
 
 /* ---- introspection (tests, tools) ----------------------------------------- */
 /* counts: Nlocal Natoms Nclusters_local ncj Nclusters_ghost Nghost dummy_cj

@@ -1988,6 +1988,16 @@ struct MdbCpEnsemble {
     // displacement check: one flag per member (set by the batched integrator)
     int* d_flags = nullptr;
     int* h_flags = nullptr;
+    // the check decided on the device (default; "check_on_host" 1: the host
+    // reads the flags every step): one graph per step whose conditional nodes
+    // rebuild every member when one flag is up; dstate = {stopped, steps run,
+    // rebuilds} as for a single system
+    bool check_host = false;
+    int* dstate     = nullptr;
+    int* h_dstate   = nullptr;
+    cudaStream_t s_cap[2] = {nullptr, nullptr};
+    long long chk_k[4]    = {0, 0, 0, 0}; // kernels: fixed part, ghost update, rebuild, force
+    long long chk_steps = 0, chk_replays = 0;
     struct Group { // members sharing cluster shape, list form, types and launch shape
         int N, half;
         Types ty;
@@ -2023,6 +2033,7 @@ enum {
     EG_CK_I,      // I with the check, flags to the host
     EG_REB_NOINT, // the rebuild of EG_REB_* without the integration
     EG_GHOST,     // ghost update
+    EG_CHK,       // a whole checked step, the rebuild decided on the device
     EG_COUNT
 };
 static_assert(EG_COUNT <= 16, "graph slots of MdbCpEnsemble");
@@ -2313,6 +2324,46 @@ template <class F> static void ens_fork(MdbCpEnsemble* e, F&& body)
     }
 }
 
+// updateAtoms + the whole rebuild of every member, stage by stage (block maps
+// of the capacities), then every member's counters into d_cnt_all
+static void ens_rebuild_stages(MdbCpEnsemble* e)
+{
+    const int n = (int)e->m.size();
+    auto stage  = [e](int st) {
+        launch_build_stage_batch(e->s, st, e->nb_stage[st], e->d_build,
+            e->d_bmap + e->off_stage[st]);
+    };
+    stage(CB_RESET);
+    stage(CB_GATHER);
+    stage(CB_BIN);
+    launch_scan_batch(e->s, 0, n, e->d_build);
+    stage(CB_SCATTER);
+    stage(CB_SORT);
+    launch_scan_batch(e->s, 1, n, e->d_build);
+    stage(CB_CLUSTERS);
+    stage(CB_GCOUNT);
+    launch_scan_batch(e->s, 2, n, e->d_build);
+    stage(CB_GWRITE);
+    stage(CB_GFIRST);
+    stage(CB_GCOLS);
+    stage(CB_CSIZES);
+    launch_scan_batch(e->s, 3, n, e->d_build);
+    stage(CB_GSCATTER);
+    stage(CB_MERGE);
+    stage(CB_PREP);
+    stage(CB_LIST);
+    launch_counters_batch(e->s, n, e->d_build, e->d_cnt_all);
+}
+
+// positions as built, for the members' displacement checks
+static void ens_snapshots(MdbCpEnsemble* e)
+{
+    for (MdbCp* c : e->m)
+        if (c->disp_max > 0.0 && c->xbuild)
+            cudaMemcpyAsync(c->xbuild, c->cx, sizeof(double4) * c->ncl_cap * c->M,
+                cudaMemcpyDeviceToDevice, e->s);
+}
+
 static void ens_body_batched(MdbCpEnsemble* e, int kind)
 {
     const bool fi = kind == EG_PLAIN_FI || kind == EG_FRONT_FI || kind == EG_REB_FI;
@@ -2330,39 +2381,12 @@ static void ens_body_batched(MdbCpEnsemble* e, int kind)
     case EG_REB_NOINT: {
         // updateAtoms + the whole rebuild of every member, stage by stage
         if (kind != EG_REB_NOINT) ens_integ(e, fi, true);
-        const int n = (int)e->m.size();
-        auto stage  = [e](int st) {
-            launch_build_stage_batch(e->s, st, e->nb_stage[st], e->d_build,
-                e->d_bmap + e->off_stage[st]);
-        };
-        stage(CB_RESET);
-        stage(CB_GATHER);
-        stage(CB_BIN);
-        launch_scan_batch(e->s, 0, n, e->d_build);
-        stage(CB_SCATTER);
-        stage(CB_SORT);
-        launch_scan_batch(e->s, 1, n, e->d_build);
-        stage(CB_CLUSTERS);
-        stage(CB_GCOUNT);
-        launch_scan_batch(e->s, 2, n, e->d_build);
-        stage(CB_GWRITE);
-        stage(CB_GFIRST);
-        stage(CB_GCOLS);
-        stage(CB_CSIZES);
-        launch_scan_batch(e->s, 3, n, e->d_build);
-        stage(CB_GSCATTER);
-        stage(CB_MERGE);
-        stage(CB_PREP);
-        stage(CB_LIST);
-        launch_counters_batch(e->s, n, e->d_build, e->d_cnt_all);
-        cudaMemcpyAsync(e->h_cnt_all, e->d_cnt_all, sizeof(int) * CP_SLOTS * n,
+        ens_rebuild_stages(e);
+        cudaMemcpyAsync(e->h_cnt_all, e->d_cnt_all, sizeof(int) * CP_SLOTS * e->m.size(),
             cudaMemcpyDeviceToHost, e->s);
         // positions as built, for the members' displacement checks (the
         // flags are cleared by the host after the rebuild)
-        for (MdbCp* c : e->m)
-            if (c->disp_max > 0.0 && c->xbuild)
-                cudaMemcpyAsync(c->xbuild, c->cx, sizeof(double4) * c->ncl_cap * c->M,
-                    cudaMemcpyDeviceToDevice, e->s);
+        ens_snapshots(e);
         break;
     }
     case EG_CK_FI:
@@ -2387,6 +2411,136 @@ static void ens_body_batched(MdbCpEnsemble* e, int kind)
     }
 }
 
+// rebuild every member when some member's displacement flag is up
+__global__ void k_ens_chk_reb(cudaGraphConditionalHandle h, const int* flags, int n, int* st)
+{
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    for (int k = threadIdx.x; k < n; k += blockDim.x)
+        if (flags[k]) any = 1;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (any) st[2]++;
+        cudaGraphSetConditional(h, any ? 1u : 0u);
+    }
+}
+
+// after a device rebuild: a member whose counters eval_build would grow (or
+// reject) stops the call
+__global__ void k_ens_chk_built(const CpBuildMember* __restrict__ tab, int n, int* st)
+{
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const int* c = tab[k].cnt;
+        if (c[CP_BADBIN] > 0 || c[CP_NGC_TOTAL] > tab[k].ngc_cap ||
+            c[CP_MAXNEED] >= tab[k].maxneighs)
+            st[0] = 1;
+    }
+}
+
+// One checked step of a batched ensemble as a graph, as capture_chk for a
+// single system: gate; the fused integration with every member's test; if a
+// flag is up, updateAtoms + the rebuild of every member, the overflow test,
+// the snapshots and the flags cleared, else the ghost update; then the force.
+// Every launch uses the block maps of the capacities (a rebuild inside the
+// graph changes the members' cluster counts).
+static int ens_capture_chk(MdbCpEnsemble* e)
+{
+    cudaError_t ce = cudaSuccess;
+    for (cudaStream_t& c : e->s_cap)
+        if (!c && (ce = cudaStreamCreateWithFlags(&c, cudaStreamNonBlocking)) != cudaSuccess)
+            return ens_fail(e, MDB_ERR_CUDA, "capture stream", ce);
+    const cudaStream_t s0 = e->s, s1 = e->s_cap[0], s2 = e->s_cap[1];
+    const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+    const int n = (int)e->m.size();
+    cudaGraphConditionalHandle h_step = 0, h_reb = 0, h_force = 0;
+    cudaGraph_t step[1] = {nullptr}, reb[2] = {nullptr, nullptr}, frc[1] = {nullptr};
+    cudaGraph_t graph = nullptr;
+    const long long m0 = mark();
+    long long* k = e->chk_k;
+    bool cap1 = false, cap2 = false;
+    auto body2 = [&](cudaGraph_t g, int what) -> cudaError_t {
+        cudaError_t r = cudaStreamBeginCaptureToGraph(s2, g, nullptr, nullptr, 0, mode);
+        if (r != cudaSuccess) return r;
+        cap2 = true;
+        e->s = s2;
+        long long m = mark();
+        if (what == 0) {
+            ens_rebuild_stages(e);
+            k_ens_chk_built<<<1, 128, 0, s2>>>(e->d_build, n, e->dstate);
+            ens_snapshots(e);
+            cudaMemsetAsync(e->d_flags, 0, sizeof(int) * n, s2);
+            k[2] = mark() - m + 1;
+        } else if (what == 1) {
+            launch_ghost_update_batch(s2, e->nb_ghost, e->d_step, e->d_bmap + e->off_ghost);
+            k[1] = mark() - m;
+        } else {
+            launch_zero_forces_batch(s2, e->nb_integ, e->d_step, e->d_bmap + e->off_integ);
+            for (const auto& gr : e->groups)
+                launch_force_mixed_batch(s2, gr.N, gr.half, false, gr.ty, gr.cutsq, gr.nblocks,
+                    e->d_force, e->d_bmap + gr.off);
+            k[3] = mark() - m;
+        }
+        e->s = s1;
+        r = cudaGetLastError();
+        cudaGraph_t out = nullptr;
+        cudaError_t r2  = cudaStreamEndCapture(s2, &out);
+        cap2            = false;
+        return r != cudaSuccess ? r : r2;
+    };
+    ce = cudaStreamBeginCapture(s0, mode);
+    if (ce == cudaSuccess) ce = cap_handle(s0, &h_step);
+    if (ce == cudaSuccess) {
+        k_chk_gate<<<1, 1, 0, s0>>>(h_step, e->dstate);
+        ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess) ce = cap_conditional(s0, h_step, 1, step);
+    if (ce == cudaSuccess) ce = cudaStreamBeginCaptureToGraph(s1, step[0], nullptr, nullptr, 0, mode);
+    if (ce == cudaSuccess) {
+        cap1 = true;
+        long long m = mark();
+        launch_cp_integrate_batch(s1, true, true, e->nb_integ, e->d_step,
+            e->d_bmap + e->off_integ);
+        k[0] = mark() - m + 2;
+        ce   = cap_handle(s1, &h_reb);
+    }
+    if (ce == cudaSuccess) {
+        k_ens_chk_reb<<<1, 128, 0, s1>>>(h_reb, e->d_flags, n, e->dstate);
+        ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess) ce = cap_conditional(s1, h_reb, 2, reb);
+    if (ce == cudaSuccess) ce = body2(reb[0], 0);
+    if (ce == cudaSuccess) ce = body2(reb[1], 1);
+    if (ce == cudaSuccess) ce = cap_handle(s1, &h_force);
+    if (ce == cudaSuccess) {
+        k_chk_force<<<1, 1, 0, s1>>>(h_force, e->dstate);
+        ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess) ce = cap_conditional(s1, h_force, 1, frc);
+    if (ce == cudaSuccess) ce = body2(frc[0], 2);
+    e->s            = s0;
+    mdb::g_launches = m0;
+    if (cap2) {
+        cudaGraph_t g2 = nullptr;
+        cudaStreamEndCapture(s2, &g2);
+    }
+    if (cap1) {
+        cudaGraph_t g1        = nullptr;
+        const cudaError_t ce1 = cudaStreamEndCapture(s1, &g1);
+        if (ce == cudaSuccess) ce = ce1;
+    }
+    const cudaError_t ce0 = cudaStreamEndCapture(s0, &graph);
+    if (ce == cudaSuccess) ce = ce0;
+    if (ce == cudaSuccess) ce = cudaGraphInstantiate(&e->g[EG_CHK].exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) {
+        cudaGetLastError();
+        return ens_fail(e, MDB_ERR_CUDA, "checked ensemble step graph", ce);
+    }
+    e->g[EG_CHK].kernels = 1;
+    return MDB_OK;
+}
+
 static int ens_capture(MdbCpEnsemble* e, int kind)
 {
     CpGraph& g = e->g[kind];
@@ -2395,6 +2549,7 @@ static int ens_capture(MdbCpEnsemble* e, int kind)
         int rc = ens_tables(e);
         if (rc) return rc;
     }
+    if (kind == EG_CHK) return ens_capture_chk(e);
     cudaGraph_t graph;
     long long m0 = mark();
     cudaError_t ce = cudaStreamBeginCapture(e->s, cudaStreamCaptureModeThreadLocal);
@@ -2481,6 +2636,10 @@ extern "C" int mdb_cp_ensemble_destroy(MdbCpEnsemble* e)
     if (e->h_dyn) cudaFreeHost(e->h_dyn);
     if (e->d_flags) cudaFree(e->d_flags);
     if (e->h_flags) cudaFreeHost(e->h_flags);
+    if (e->dstate) cudaFree(e->dstate);
+    if (e->h_dstate) cudaFreeHost(e->h_dstate);
+    for (cudaStream_t c : e->s_cap)
+        if (c) cudaStreamDestroy(c);
     if (e->s) cudaStreamDestroy(e->s);
     delete e;
     return MDB_OK;
@@ -2502,6 +2661,11 @@ extern "C" int mdb_cp_ensemble_tune(MdbCpEnsemble* e, const char* key, int value
         cudaStreamSynchronize(e->s);
         e->batched = value != 0;
         ens_drop(e);
+        return MDB_OK;
+    }
+    if (!strcmp(key, "check_on_host")) {
+        if (value < 0 || value > 1) return MDB_ERR_ARG;
+        e->check_host = value != 0;
         return MDB_OK;
     }
     return ens_fail(e, MDB_ERR_ARG, "unknown tuning key");
@@ -2532,11 +2696,76 @@ static int ens_rebuild(MdbCpEnsemble* e, int kind)
             // grown buffers bump the member's generation: graphs are recaptured
             rc = do_build(c);
             if (rc) return ens_fail(e, rc, c->err.c_str());
+            // its snapshot copy ran on the member's stream
+            ce = cudaStreamSynchronize(c->s);
+            if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "member rebuild", ce);
         }
         c->have_clusters = c->have_ghosts = c->have_list = true;
         if (c->disp_max > 0.0 && c->xbuild) c->snap_valid = true;
     }
     return ens_dyn_maps(e);
+}
+
+// The device's record of the checked step graphs launched since the last call
+// (their steps in `launched`), as chk_resolve for a single system: counts
+// rebuilds and kernels, refreshes the counters and block maps after device
+// rebuilds, and when a rebuild overflowed a member's buffer grows it, replays
+// that member's build, runs the step's force and sets *resume to the step.
+static int ens_chk_resolve(MdbCpEnsemble* e, std::vector<int>& launched, int* resume)
+{
+    *resume = -1;
+    if (launched.empty()) return MDB_OK;
+    const int n    = (int)e->m.size();
+    cudaError_t ce = cudaMemcpyAsync(e->h_dstate, e->dstate, 3 * sizeof(int),
+        cudaMemcpyDeviceToHost, e->s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->s);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(e->dstate, 0, 3 * sizeof(int), e->s);
+    if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "checked steps", ce);
+    const int stopped = e->h_dstate[0], ran = e->h_dstate[1], reb = e->h_dstate[2];
+    const long long* k = e->chk_k;
+    e->launches += (long long)launched.size() + ran * k[0] + (ran - reb) * k[1] + reb * k[2] +
+                   (ran - stopped) * k[3];
+    e->chk_steps += ran;
+    e->chk_replays += stopped ? 1 : 0;
+    for (MdbCp* c : e->m) c->rebuilds_check += reb;
+    int rc = MDB_OK;
+    if (reb > 0) {
+        ce = cudaMemcpyAsync(e->h_cnt_all, e->d_cnt_all, sizeof(int) * CP_SLOTS * n,
+            cudaMemcpyDeviceToHost, e->s);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->s);
+        if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "checked steps (counters)", ce);
+        for (int q = 0; q < n; q++)
+            memcpy(e->m[q]->h_cnt, e->h_cnt_all + (size_t)q * CP_SLOTS, sizeof(int) * CP_SLOTS);
+    }
+    if (stopped) {
+        if (ran < 1 || ran > (int)launched.size())
+            return ens_fail(e, MDB_ERR_CUDA, "checked steps: inconsistent device record");
+        for (MdbCp* c : e->m) {
+            const int r = eval_build(c, CHK_ALL);
+            if (r < 0) return ens_fail(e, -r, c->err.c_str());
+            if (r > 0) {
+                // grown buffers bump the member's generation: graphs are recaptured
+                if ((rc = do_build(c))) return ens_fail(e, rc, c->err.c_str());
+                if ((ce = cudaStreamSynchronize(c->s)) != cudaSuccess)
+                    return ens_fail(e, MDB_ERR_CUDA, "member rebuild", ce);
+            }
+        }
+        if ((rc = ens_dyn_maps(e)) || (rc = ens_launch(e, EG_FORCE))) return rc;
+        *resume = launched[ran - 1];
+    } else if (reb > 0 && (rc = ens_dyn_maps(e))) {
+        return rc;
+    }
+    launched.clear();
+    return MDB_OK;
+}
+
+extern "C" int mdb_cp_ensemble_check_stats(MdbCpEnsemble* e, long long* graph_steps,
+    long long* replays)
+{
+    if (!e) return MDB_ERR_ARG;
+    if (graph_steps) *graph_steps = e->chk_steps;
+    if (replays) *replays = e->chk_replays;
+    return MDB_OK;
 }
 
 extern "C" int mdb_cp_ensemble_run(MdbCpEnsemble* e, int first_step, int nsteps,
@@ -2569,12 +2798,35 @@ extern "C" int mdb_cp_ensemble_run(MdbCpEnsemble* e, int first_step, int nsteps,
     }
     // members may have been rebuilt on their own since the last run
     if ((rc = ens_dyn_maps(e))) return rc;
+    const bool on_device = checked && !e->check_host;
+    if (on_device && !e->dstate) {
+        cudaError_t ce = cudaMalloc((void**)&e->dstate, 3 * sizeof(int));
+        if (ce == cudaSuccess) ce = cudaMallocHost((void**)&e->h_dstate, 3 * sizeof(int));
+        if (ce == cudaSuccess) ce = cudaMemsetAsync(e->dstate, 0, 3 * sizeof(int), e->s);
+        if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_NOMEM, "checked steps", ce);
+    }
+    std::vector<int> launched;
     const int last     = first_step + nsteps - 1;
     bool pending_final = false;
     for (int step = first_step; step <= last; step++) {
         const bool reneigh = (step + 1) % c0->p.reneigh_every == 0;
         const bool prune   = !reneigh && (step + 1) % c0->prune_every == 0;
         const bool sample  = max_samples > 0 && (step + 1) % c0->p.nstat == 0 && nslot < max_samples;
+        // a checked step decided on the device: one graph launch, no synchronisation
+        if (on_device && pending_final && !prune && !reneigh && !force_reb && !sample &&
+            step != last) {
+            if ((rc = ens_launch(e, EG_CHK))) return rc;
+            launched.push_back(step);
+            continue;
+        }
+        if (!launched.empty()) {
+            int resume = -1;
+            if ((rc = ens_chk_resolve(e, launched, &resume))) return rc;
+            if (resume >= 0) {
+                step = resume; // the steps after it did nothing: run them again
+                continue;
+            }
+        }
         if (checked && !prune && !reneigh && !force_reb) {
             if ((rc = ens_launch(e, pending_final ? EG_CK_FI : EG_CK_I))) return rc;
             pending_final  = false;

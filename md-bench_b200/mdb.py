@@ -100,7 +100,7 @@ CP_EXPORTS = [
     "mdb_cp_ensemble_destroy", "mdb_cp_ensemble_last_error", "mdb_cp_ensemble_stream",
     "mdb_cp_ensemble_launch_count", "mdb_cp_ensemble_run", "mdb_cp_ensemble_tune",
     "mdb_cp_set_rebuild_check", "mdb_cp_get_rebuilds", "mdb_cp_set_pair_buffer",
-    "mdb_cp_get_pair_stats", "mdb_cp_get_check_stats",
+    "mdb_cp_get_pair_stats", "mdb_cp_get_check_stats", "mdb_cp_ensemble_check_stats",
 ]
 # every symbol include/mdb_host.h declares
 HOST_EXPORTS = [
@@ -183,6 +183,8 @@ def load():
         "mdb_cp_get_pair_stats": ([vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], ip),
         "mdb_cp_get_rebuilds": ([vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], ip),
         "mdb_cp_get_check_stats": ([vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], ip),
+        "mdb_cp_ensemble_check_stats": ([vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)],
+                                        ip),
         "mdb_cp_ensemble_create": ([C.POINTER(vp), ip, C.POINTER(vp)], ip),
         "mdb_cp_ensemble_destroy": ([vp], ip),
         "mdb_cp_ensemble_last_error": ([vp], C.c_char_p),
@@ -936,6 +938,14 @@ class Ensemble:
         if rc:
             msg = self.lib.mdb_cp_ensemble_last_error(self.h)
             raise MdbError(f"mdb_cp_ensemble_tune: {msg.decode() if msg else rc}")
+
+    def check_stats(self):
+        """(checked steps decided on the device, overflowed rebuilds replayed)."""
+        a, b = C.c_longlong(), C.c_longlong()
+        rc = self.lib.mdb_cp_ensemble_check_stats(self.h, C.byref(a), C.byref(b))
+        if rc:
+            raise MdbError("mdb_cp_ensemble_check_stats")
+        return a.value, b.value
 
     def close(self):
         if getattr(self, "h", None):

@@ -98,3 +98,54 @@ def test_cold_system_never_rebuilds_on_the_device():
     assert_same_state(a, b)
     a.close()
     b.close()
+
+
+def ensemble_members(host_check, maxneighs=None):
+    """A hot dense replica, a mild one and a cold one (mixed, full lists), all
+    with the displacement check; maxneighs: list capacity of the hot one."""
+    specs = [(6, 0.95, 2.0), (4, 0.8, 0.5), (5, 0.8442, 0.02)]
+    out = []
+    for k, (n, rho, temp) in enumerate(specs):
+        s, _ = hot(0.05, host_check, "mixed", maxneighs if (k == 0 and maxneighs) else 0,
+                   n, rho, temp)
+        out.append(s)
+    return out
+
+
+@pytest.mark.parametrize("squeeze", [False, True])
+def test_ensemble_device_decisions_match_host_decisions(squeeze):
+    """Batched ensemble with the check decided on the device (one conditional
+    graph per step over all replicas) against the host reading the flags every
+    step: the same samples, rebuild counts and end states, bit for bit. With
+    the hot replica's list capacity one more than its lattice's longest row,
+    a device rebuild overflows it and is replayed by the host."""
+    maxneighs = None
+    if squeeze:
+        probe, _ = hot(0.05, 1, "mixed")
+        maxneighs = int(probe.numneigh().max()) + 1
+        probe.close()
+    a = ensemble_members(0, maxneighs)
+    b = ensemble_members(1, maxneighs)
+    ea, eb = mdb.Ensemble(a), mdb.Ensemble(b)
+    ea.tune("check_on_host", 0)
+    eb.tune("check_on_host", 1)
+    ga = ea.run(57, max_samples=8)
+    gb = eb.run(57, max_samples=8)
+    assert ga == gb
+    steps, replays = ea.check_stats()
+    assert steps > 20 and eb.check_stats() == (0, 0)
+    assert replays >= 1 if squeeze else replays == 0
+    for u, w in zip(a, b):
+        assert u.rebuilds() == w.rebuilds()
+        assert u.rebuilds()[1] > 0
+        assert_same_state(u, w)
+    if squeeze:
+        assert a[0].counts()["maxneighs"] == b[0].counts()["maxneighs"] > maxneighs
+    ga = ea.run(23, first_step=57, max_samples=0)
+    gb = eb.run(23, first_step=57, max_samples=0)
+    for u, w in zip(a, b):
+        assert_same_state(u, w)
+    ea.close()
+    eb.close()
+    for s in a + b:
+        s.close()
