@@ -134,11 +134,16 @@ int mdb_cp_initial_integrate(MdbCp* ctx);
 int mdb_cp_final_integrate(MdbCp* ctx);
 /* computeThermo (common/thermo.c:60-100): T and P from the atom arrays, as
  * the reference prints them (velocities as of the last updateSingleAtoms); ke,
- * pe and etotal from the cluster state (pe of the last energy evaluation). */
+ * pe and etotal from the cluster state. pe: of the last energy evaluation; when
+ * the last force evaluation (mdb_cp_setup, mdb_cp_compute_force, the last step
+ * of mdb_cp_run) had none and the slots have not moved since, one force
+ * evaluation with the energy runs first (the same forces; half lists sum them
+ * in another atomic order); otherwise NaN. */
 int mdb_cp_thermo(MdbCp* ctx, MdbThermo* out);
 
 /* setup() of clusterpair/main.c:44-97 for atoms already set: buildClusters,
- * defineJClusters, setupPbc, binJClusters, buildNeighbor, then computeForce. */
+ * defineJClusters, setupPbc, binJClusters, buildNeighbor, then computeForce
+ * (no energy: mdb_cp_thermo evaluates it when asked). */
 int mdb_cp_setup(MdbCp* ctx);
 /* The timestep loop of clusterpair/main.c:326-362 for steps first_step ..
  * first_step+nsteps-1 (prune every prune_every steps, rebuild every

@@ -84,6 +84,10 @@ struct MdbCp {
 
     bool have_atoms = false, have_clusters = false, have_ghosts = false, have_list = false;
     bool energy_valid = false;
+    // the slot forces belong to the current slot positions (a force evaluation
+    // since the last integration or cluster build), so thermo can evaluate
+    // the energy on demand
+    bool force_current = false;
     int energy_blocks = 0; // partial-energy blocks of the last energy evaluation
     CpGraph g_plain;
     unsigned gen = 0; // bumped whenever buffers move (graphs that hold them are stale)
@@ -788,7 +792,7 @@ extern "C" int mdb_cp_set_atoms(MdbCp* ctx, int nlocal, const double* x, const d
     if (hbad) return fail(ctx, MDB_ERR_ARG, "atom type out of range");
     ctx->have_atoms    = true;
     ctx->have_clusters = ctx->have_ghosts = ctx->have_list = false;
-    ctx->energy_valid  = false;
+    ctx->energy_valid = ctx->force_current = false;
     return MDB_OK;
 }
 
@@ -958,6 +962,7 @@ static int snapshot(MdbCp* ctx)
 
 static int do_build(MdbCp* ctx)
 {
+    ctx->force_current = false;
     for (int attempt = 0; attempt < 8; attempt++) {
         long long m = mark();
         enq_build(ctx);
@@ -1121,6 +1126,7 @@ extern "C" int mdb_cp_build_clusters(MdbCp* ctx)
     if (r < 0) return -r;
     ctx->have_clusters = true;
     ctx->have_ghosts = ctx->have_list = false;
+    ctx->force_current = false;
     return MDB_OK;
 }
 
@@ -1245,7 +1251,8 @@ static int compute_force(MdbCp* ctx, bool energy)
     enq_force(ctx, energy);
     account(ctx, m);
     CK(cudaGetLastError());
-    ctx->energy_valid = energy;
+    ctx->energy_valid  = energy;
+    ctx->force_current = true;
     return MDB_OK;
 }
 
@@ -1259,6 +1266,7 @@ extern "C" int mdb_cp_initial_integrate(MdbCp* ctx)
     long long m = mark();
     enq_initial(ctx);
     account(ctx, m);
+    ctx->force_current = false;
     return MDB_OK;
 }
 
@@ -1311,6 +1319,12 @@ extern "C" int mdb_cp_thermo(MdbCp* ctx, MdbThermo* out)
     NEED_ATOMS();
     if (!out) return MDB_ERR_ARG;
     long long m = mark();
+    if (!ctx->energy_valid && ctx->force_current && ctx->have_list) {
+        // the energy of the current state: one force evaluation with it (the
+        // same forces; half lists sum them in another atomic order)
+        enq_force(ctx, true);
+        ctx->energy_valid = true;
+    }
     bool pe     = ctx->energy_valid && ctx->have_clusters;
     if (ctx->have_clusters) {
         enq_thermo(ctx, 0, pe);
@@ -1334,7 +1348,8 @@ extern "C" int mdb_cp_setup(MdbCp* ctx)
     CK(cudaSetDevice(ctx->dev));
     int rc = do_build(ctx);
     if (rc) return rc;
-    return compute_force(ctx, true);
+    // the energy is evaluated when mdb_cp_thermo asks for it
+    return compute_force(ctx, false);
 }
 
 // A plain step whose predecessor left its final integration pending:
@@ -1649,6 +1664,7 @@ static int run_checked(MdbCp* ctx, int first_step, int nsteps, MdbThermo* sample
         account(ctx, m);
     }
     ctx->energy_valid = nsteps > 0 && max_samples > 0 && ((last + 1) % ctx->p.nstat == 0);
+    if (nsteps > 0) ctx->force_current = true;
     CK(cudaGetLastError());
     if (nslot > 0)
         CK(cudaMemcpyAsync(ctx->h_red, ctx->red, 4 * sizeof(double) * nslot,
@@ -1751,6 +1767,7 @@ extern "C" int mdb_cp_run(MdbCp* ctx, int first_step, int nsteps, MdbThermo* sam
         account(ctx, m);
     }
     ctx->energy_valid = nsteps > 0 && max_samples > 0 && ((last + 1) % ctx->p.nstat == 0);
+    if (nsteps > 0) ctx->force_current = true;
     CK(cudaGetLastError());
     if (nslot > 0)
         CK(cudaMemcpyAsync(ctx->h_red, ctx->red, 4 * sizeof(double) * nslot,
