@@ -2015,6 +2015,11 @@ struct MdbCpEnsemble {
     cudaStream_t s_cap[2] = {nullptr, nullptr};
     long long chk_k[4]    = {0, 0, 0, 0}; // kernels: fixed part, ghost update, rebuild, force
     long long chk_steps = 0, chk_replays = 0;
+    // per member {M, N, force group, i-clusters per warp, force threads}, for
+    // the block maps that a rebuild inside the checked step graph refreshes
+    int* d_mapinfo = nullptr;
+    size_t* d_goff = nullptr; // per force group: its region of the maps and size
+    int* d_gnb     = nullptr;
     struct Group { // members sharing cluster shape, list form, types and launch shape
         int N, half;
         Types ty;
@@ -2455,14 +2460,103 @@ __global__ void k_ens_chk_built(const CpBuildMember* __restrict__ tab, int n, in
     }
 }
 
+// The block maps of the members' current clusters (ens_dyn_maps' layout: per
+// region the members in order, each with its blocks, then unused entries),
+// from the device counters after a rebuild inside the checked step graph.
+// One block; a member's block count as launch_* computes it.
+template <class F>
+__device__ void fill_map_region(int2* out, int cap, int n, F blocks_of)
+{
+    __shared__ int s_scan[256];
+    __shared__ int s_carry;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    for (int base = 0; base < n; base += blockDim.x) {
+        const int k = base + threadIdx.x;
+        const int c = k < n ? blocks_of(k) : 0;
+        s_scan[threadIdx.x] = c;
+        __syncthreads();
+        for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+            const int v = threadIdx.x >= o ? s_scan[threadIdx.x - o] : 0;
+            __syncthreads();
+            s_scan[threadIdx.x] += v;
+            __syncthreads();
+        }
+        const int start = s_carry + s_scan[threadIdx.x] - c;
+        for (int b = 0; b < c && start + b < cap; b++) out[start + b] = make_int2(k, b);
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) s_carry += s_scan[threadIdx.x];
+        __syncthreads();
+    }
+    for (int w = min(s_carry, cap) + threadIdx.x; w < cap; w += blockDim.x)
+        out[w] = make_int2(-1, 0);
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) k_ens_dyn_maps(const CpBuildMember* __restrict__ tab,
+    const int* __restrict__ info, int n, int2* bmap, size_t off_integ, int nb_integ,
+    size_t off_ghost, int nb_ghost, const size_t* __restrict__ goff,
+    const int* __restrict__ gnb, int ngroups)
+{
+    fill_map_region(bmap + off_integ, nb_integ, n, [&](int k) {
+        return (int)(((long long)tab[k].cnt[CP_NCL] * info[5 * k] + MDB_NTHREADS - 1) /
+                     MDB_NTHREADS);
+    });
+    fill_map_region(bmap + off_ghost, nb_ghost, n, [&](int k) {
+        return (int)(((long long)tab[k].cnt[CP_NGC] * info[5 * k + 1] + MDB_NTHREADS - 1) /
+                     MDB_NTHREADS);
+    });
+    for (int q = 0; q < ngroups; q++)
+        fill_map_region(bmap + goff[q], gnb[q], n, [&](int k) {
+            if (info[5 * k + 2] != q) return 0;
+            const int nt = info[5 * k + 4];
+            return (int)(((long long)tab[k].cnt[CP_NCL] * 32 / info[5 * k + 3] + nt - 1) / nt);
+        });
+}
+
+// the member table of k_ens_dyn_maps for the current groups
+static int ens_map_info(MdbCpEnsemble* e)
+{
+    const int n = (int)e->m.size(), ng = (int)e->groups.size();
+    std::vector<int> info(5 * (size_t)n);
+    for (int k = 0; k < n; k++) {
+        const MdbCp* c = e->m[k];
+        info[5 * k]     = c->M;
+        info[5 * k + 1] = c->N;
+        info[5 * k + 2] = e->gid[k];
+        info[5 * k + 3] = c->ty.force_cpw;
+        info[5 * k + 4] = force_mixed_threads(c->ty);
+    }
+    std::vector<size_t> goff(std::max(ng, 1));
+    std::vector<int> gnb(std::max(ng, 1));
+    for (int q = 0; q < ng; q++) goff[q] = e->groups[q].off_dyn, gnb[q] = e->groups[q].nblocks;
+    cudaError_t ce = cudaSuccess;
+    if (!e->d_mapinfo) {
+        ce = cudaMalloc((void**)&e->d_mapinfo, sizeof(int) * info.size());
+        if (ce == cudaSuccess) ce = cudaMalloc((void**)&e->d_goff, sizeof(size_t) * 64);
+        if (ce == cudaSuccess) ce = cudaMalloc((void**)&e->d_gnb, sizeof(int) * 64);
+        if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_NOMEM, "ensemble map table", ce);
+    }
+    if (ng > 64) return ens_fail(e, MDB_ERR_ARG, "more than 64 force groups");
+    ce = cudaMemcpy(e->d_mapinfo, info.data(), sizeof(int) * info.size(), cudaMemcpyHostToDevice);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpy(e->d_goff, goff.data(), sizeof(size_t) * goff.size(), cudaMemcpyHostToDevice);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpy(e->d_gnb, gnb.data(), sizeof(int) * gnb.size(), cudaMemcpyHostToDevice);
+    if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "ensemble map table", ce);
+    return MDB_OK;
+}
+
 // One checked step of a batched ensemble as a graph, as capture_chk for a
 // single system: gate; the fused integration with every member's test; if a
 // flag is up, updateAtoms + the rebuild of every member, the overflow test,
 // the snapshots and the flags cleared, else the ghost update; then the force.
-// Every launch uses the block maps of the capacities (a rebuild inside the
-// graph changes the members' cluster counts).
+// Every launch uses the block maps of the current clusters, which the rebuild
+// refreshes on the device from the members' new counters.
 static int ens_capture_chk(MdbCpEnsemble* e)
 {
+    int rc = ens_map_info(e);
+    if (rc) return rc;
     cudaError_t ce = cudaSuccess;
     for (cudaStream_t& c : e->s_cap)
         if (!c && (ce = cudaStreamCreateWithFlags(&c, cudaStreamNonBlocking)) != cudaSuccess)
@@ -2485,17 +2579,17 @@ static int ens_capture_chk(MdbCpEnsemble* e)
         if (what == 0) {
             ens_rebuild_stages(e);
             k_ens_chk_built<<<1, 128, 0, s2>>>(e->d_build, n, e->dstate);
+            k_ens_dyn_maps<<<1, 256, 0, s2>>>(e->d_build, e->d_mapinfo, n, e->d_bmap,
+                e->off_integ_dyn, e->nb_integ, e->off_ghost_dyn, e->nb_ghost, e->d_goff,
+                e->d_gnb, (int)e->groups.size());
             ens_snapshots(e);
             cudaMemsetAsync(e->d_flags, 0, sizeof(int) * n, s2);
-            k[2] = mark() - m + 1;
+            k[2] = mark() - m + 2;
         } else if (what == 1) {
-            launch_ghost_update_batch(s2, e->nb_ghost, e->d_step, e->d_bmap + e->off_ghost);
+            launch_ghost_update_batch(s2, e->nb_ghost, e->d_step, e->d_bmap + e->off_ghost_dyn);
             k[1] = mark() - m;
         } else {
-            launch_zero_forces_batch(s2, e->nb_integ, e->d_step, e->d_bmap + e->off_integ);
-            for (const auto& gr : e->groups)
-                launch_force_mixed_batch(s2, gr.N, gr.half, false, gr.ty, gr.cutsq, gr.nblocks,
-                    e->d_force, e->d_bmap + gr.off);
+            ens_forces(e, false);
             k[3] = mark() - m;
         }
         e->s = s1;
@@ -2514,10 +2608,10 @@ static int ens_capture_chk(MdbCpEnsemble* e)
     if (ce == cudaSuccess) ce = cap_conditional(s0, h_step, 1, step);
     if (ce == cudaSuccess) ce = cudaStreamBeginCaptureToGraph(s1, step[0], nullptr, nullptr, 0, mode);
     if (ce == cudaSuccess) {
-        cap1 = true;
+        cap1   = true;
+        e->s   = s1;
         long long m = mark();
-        launch_cp_integrate_batch(s1, true, true, e->nb_integ, e->d_step,
-            e->d_bmap + e->off_integ);
+        ens_integ(e, true, true);
         k[0] = mark() - m + 2;
         ce   = cap_handle(s1, &h_reb);
     }
@@ -2655,6 +2749,9 @@ extern "C" int mdb_cp_ensemble_destroy(MdbCpEnsemble* e)
     if (e->h_flags) cudaFreeHost(e->h_flags);
     if (e->dstate) cudaFree(e->dstate);
     if (e->h_dstate) cudaFreeHost(e->h_dstate);
+    if (e->d_mapinfo) cudaFree(e->d_mapinfo);
+    if (e->d_goff) cudaFree(e->d_goff);
+    if (e->d_gnb) cudaFree(e->d_gnb);
     for (cudaStream_t c : e->s_cap)
         if (c) cudaStreamDestroy(c);
     if (e->s) cudaStreamDestroy(e->s);
