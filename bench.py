@@ -644,16 +644,24 @@ def reference_arm(args, rank):
     print(json.dumps(line), flush=True)
 
 
-def fp32_peak():
-    """FP32 SIMT peak from the measured max SM clock: 148 SMs x 128 FP32 lanes x
-    2 flops per FMA (no FP32 figure is measured by the pool)."""
+def fp32_peak(mdb=None, device=0):
+    """FP32 peak: measured in this run by mdb_fp32_fma_rate (packed FMA chains
+    on all SMs; the pool's MEASURED_PEAKS.json has no FP32 figure), with the
+    figure derived from its max SM clock (148 SMs x 128 FP32 lanes x 2 flops
+    per FMA) beside it."""
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             mhz = float(json.load(f)["sm_max_mhz"])
-        src = "derived from sm_max_mhz of MEASURED_PEAKS.json"
+        dsrc = "sm_max_mhz of MEASURED_PEAKS.json"
     except Exception:
-        mhz, src = 1965.0, "derived from the nominal 1965 MHz"
-    return 148 * 128 * 2 * mhz * 1e6 / 1e12, src
+        mhz, dsrc = 1965.0, "the nominal 1965 MHz"
+    derived = 148 * 128 * 2 * mhz * 1e6 / 1e12
+    if mdb is not None:
+        measured = mdb.fp32_fma_rate(device) / 1e12
+        if measured > 0:
+            return measured, ("measured in this run: mdb_fp32_fma_rate, packed FP32 FMA "
+                              f"chains on all SMs (derived from {dsrc}: {derived:.1f})")
+    return derived, f"derived from {dsrc}"
 
 
 def pairs_in_cutoff(x, box, rc):
@@ -816,7 +824,7 @@ def main():
     box = np.array([s.params.xprd, s.params.yprd, s.params.zprd])
     pc = pairs_in_cutoff(xh, box, s.params.cutforce)
     fpa = cp_flops_per_atom(pc, HEAD["half"])
-    peak, src = fp32_peak()
+    peak, src = fp32_peak(mdb, local)
     achieved = fpa * head["natoms"] / kt / 1e12
     # DRAM bytes of one launch from the ncu capture recorded in profiles/ (not
     # a counter of this run)

@@ -229,6 +229,16 @@ int mdb_set_halo_positions(MdbCtx* ctx, const double* d_x, int n);
  * any capture too. */
 int mdb_kinetic_sum_noalloc(const double* d_v, int n, double mass, double* d_out, void* stream);
 
+/* ---- device probe -------------------------------------------------------------
+ * No counterpart in the reference. The packed FP32 FMA rate of a device, in
+ * FP32 flops per second (one fused multiply-add = 2 flops): every thread of a
+ * grid filling all SMs runs eight independent chains of fma.rn.f32x2, timed
+ * with CUDA events on a stream of its own, best of five launches after a
+ * warm-up. The roofline denominator of the mixed cluster-pair force kernels,
+ * whose pair arithmetic runs on that pipe. Synchronous; allocates and frees a
+ * small output buffer. */
+int mdb_fp32_fma_rate(int device, double* flops_per_s);
+
 /* ---- introspection (tests, tools) ----------------------------------------- */
 int mdb_get_counts(MdbCtx* ctx, int* nlocal, int* nghost, int* maxneighs);
 int mdb_get_positions_all(MdbCtx* ctx, double* x); /* (nlocal+nghost) x 3 */

@@ -83,6 +83,7 @@ EXPORTS = [
     "mdb_initial_integrate", "mdb_final_integrate", "mdb_thermo", "mdb_setup", "mdb_run", "mdb_get_counts",
     "mdb_get_positions_all", "mdb_get_ghosts", "mdb_get_neighbor_list",
     "mdb_get_bin_geometry", "mdb_get_eam_fp", "mdb_launch_count", "mdb_kinetic_sum_noalloc",
+    "mdb_fp32_fma_rate",
     "mdb_set_owned", "mdb_gather_positions", "mdb_set_halo_positions",
     "mdb_sort_atoms", "mdb_set_resort", "mdb_tune", "mdb_set_neighbor_list",
 ]
@@ -146,6 +147,7 @@ def load():
         "mdb_get_eam_fp": ([vp, _dp], ip),
         "mdb_launch_count": ([vp], C.c_longlong),
         "mdb_kinetic_sum_noalloc": ([vp, ip, C.c_double, vp, vp], ip),
+        "mdb_fp32_fma_rate": ([ip, C.POINTER(C.c_double)], ip),
         "mdb_set_owned": ([vp, ip], ip),
         "mdb_gather_positions": ([vp, vp, ip, C.c_double, C.c_double, C.c_double, vp], ip),
         "mdb_set_halo_positions": ([vp, vp, ip], ip),
@@ -394,6 +396,16 @@ def system_from_host(hp, natoms, eam=None, device=0, **overrides):
         kw["sigma_per_type"] = list(hp.sigma_per_type)[:hp.ntypes]
     kw.update(overrides)
     return System(eam=eam, **kw)
+
+
+def fp32_fma_rate(device=0):
+    """The device's packed FP32 FMA rate in flops per second (mdb_fp32_fma_rate)."""
+    lib = load()
+    r = C.c_double()
+    rc = lib.mdb_fp32_fma_rate(int(device), C.byref(r))
+    if rc:
+        raise MdbError(f"mdb_fp32_fma_rate: {lib.mdb_status_string(rc).decode()}")
+    return r.value
 
 
 def read_funcfl(path):
