@@ -115,8 +115,11 @@ int mdb_set_eam(MdbCtx* ctx, const MdbEamTables* tables);
 int mdb_eam_read_funcfl(const char* path, MdbEamTables* out);
 void mdb_eam_free(MdbEamTables* t);
 
-/* Local atoms, AoS host arrays. Replaces copyDataToCUDADevice /
- * copyDataFromCUDADevice (verletlist/forceCuda.cu:331-343). */
+/* Local atoms, AoS arrays. Replaces copyDataToCUDADevice /
+ * copyDataFromCUDADevice (verletlist/forceCuda.cu:331-343). The arrays may be
+ * host or device memory of the context's device (unified addressing), so a
+ * caller that keeps its atoms on the GPU moves them without a host copy (the
+ * types of device arrays are copied to the host once, to be checked). */
 int mdb_set_atoms(MdbCtx* ctx, int nlocal, const double* x, const double* v, const int* type);
 int mdb_get_atoms(MdbCtx* ctx, double* x, double* v, double* f, int* type);
 

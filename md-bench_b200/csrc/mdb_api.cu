@@ -30,7 +30,10 @@ struct MdbCtx {
     // (binned, imaged and listed, but without force row, integration or
     // thermo); nown = 0: every atom is owned
     int nlocal = 0, ntypes = 1, nown = 0;
-    int ghost_cap = 0, nall_cap = 0;
+    // capacities: atom_cap local atoms (the atom-sized arrays and the list's
+    // leading dimension), nall_cap positions (locals then ghosts), border_cap
+    // ghost maps; ghost_cap = the ghosts the current nlocal leaves room for
+    int ghost_cap = 0, nall_cap = 0, atom_cap = 0, border_cap = 0;
     int maxneighs = 100, ld = 0;
     bool have_atoms = false, have_list = false, have_ghosts = false, mixed = false;
     bool have_eam = false;
@@ -514,6 +517,7 @@ static int alloc_ghost_sized(MdbCtx* ctx, int ghost_cap)
     dfree(ctx->xe);
     CK(dalloc(&ctx->border_map, ghost_cap));
     CK(dalloc(&ctx->pbc_code, ghost_cap));
+    ctx->border_cap = ghost_cap;
     CK(dalloc(&ctx->atom_bin, nall));
     CK(dalloc(&ctx->atom_slot, nall));
     CK(dalloc(&ctx->bin_atoms, nall));
@@ -548,42 +552,65 @@ extern "C" int mdb_set_atoms(MdbCtx* ctx, int nlocal, const double* x, const dou
     if (!ctx || nlocal < 0 || (nlocal > 0 && (!x || !v || !type))) return MDB_ERR_ARG;
     CK(cudaSetDevice(ctx->dev));
     ctx->nown = 0; // new atoms: all owned until mdb_set_owned
-    int maxt  = 0;
+    // host or device arrays (unified addressing); the types are checked here
+    std::vector<int> htype;
+    const int* th = type;
+    if (nlocal > 0) {
+        cudaPointerAttributes pa;
+        if (cudaPointerGetAttributes(&pa, type) == cudaSuccess &&
+            (pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged)) {
+            htype.resize(nlocal);
+            CK(cudaMemcpy(htype.data(), type, sizeof(int) * nlocal, cudaMemcpyDefault));
+            th = htype.data();
+        }
+        cudaGetLastError();
+    }
+    int maxt = 0;
     for (int i = 0; i < nlocal; i++) {
-        if (type[i] < 0) return fail(ctx, MDB_ERR_ARG, "negative atom type");
-        maxt = std::max(maxt, type[i] + 1);
+        if (th[i] < 0) return fail(ctx, MDB_ERR_ARG, "negative atom type");
+        maxt = std::max(maxt, th[i] + 1);
     }
     int rc = setup_types(ctx, std::max(ctx->p.ntypes, maxt));
     if (rc) return rc;
-    bool realloc_all = nlocal != ctx->nlocal || !ctx->x;
+    // the buffers are kept while the atom count stays within the capacity
+    // (a domain's atom count changes a little at every rebuild)
+    bool realloc_all = nlocal > ctx->atom_cap || !ctx->x;
+    if (!realloc_all && nlocal != ctx->nlocal) {
+        CK(cudaStreamSynchronize(ctx->s));
+        drop_graphs(ctx);
+        ctx->nlocal      = nlocal;
+        ctx->ghost_cap   = std::min(ctx->border_cap, ctx->nall_cap - nlocal);
+        ctx->have_ghosts = ctx->have_list = false;
+    }
     if (realloc_all) {
         CK(cudaStreamSynchronize(ctx->s));
         drop_graphs(ctx);
         free_atom_buffers(ctx);
-        ctx->nlocal = nlocal;
-        ctx->ld     = ((nlocal + 31) / 32) * 32;
-        if (ctx->ld == 0) ctx->ld = 32;
-        CK(dalloc(&ctx->vx, nlocal));
-        CK(dalloc(&ctx->vy, nlocal));
-        CK(dalloc(&ctx->vz, nlocal));
-        CK(dalloc(&ctx->fx, nlocal));
-        CK(dalloc(&ctx->fy, nlocal));
-        CK(dalloc(&ctx->fz, nlocal));
-        CK(cudaMemset(ctx->fx, 0, sizeof(double) * std::max(nlocal, 1)));
-        CK(cudaMemset(ctx->fy, 0, sizeof(double) * std::max(nlocal, 1)));
-        CK(cudaMemset(ctx->fz, 0, sizeof(double) * std::max(nlocal, 1)));
-        CK(dalloc(&ctx->ghost_cnt, nlocal + 1));
-        CK(dalloc(&ctx->ghost_off, nlocal + 1));
-        CK(dalloc(&ctx->numneigh, nlocal));
-        if (ctx->p.force_field == MDB_FF_EAM && ctx->mixed) CK(dalloc(&ctx->eam_ncut, nlocal));
-        CK(dalloc(&ctx->local_order, nlocal));
-        CK(dalloc(&ctx->stage, 9 * (size_t)nlocal));
-        CK(dalloc(&ctx->stage_t, nlocal));
-        int nscan         = std::max(scan_scratch_ints(nlocal), scan_scratch_ints(ctx->g.mbins));
+        ctx->nlocal   = nlocal;
+        const int cap = nlocal + nlocal / 32 + 64;
+        ctx->atom_cap = cap;
+        ctx->ld       = ((cap + 31) / 32) * 32;
+        CK(dalloc(&ctx->vx, cap));
+        CK(dalloc(&ctx->vy, cap));
+        CK(dalloc(&ctx->vz, cap));
+        CK(dalloc(&ctx->fx, cap));
+        CK(dalloc(&ctx->fy, cap));
+        CK(dalloc(&ctx->fz, cap));
+        CK(cudaMemset(ctx->fx, 0, sizeof(double) * cap));
+        CK(cudaMemset(ctx->fy, 0, sizeof(double) * cap));
+        CK(cudaMemset(ctx->fz, 0, sizeof(double) * cap));
+        CK(dalloc(&ctx->ghost_cnt, cap + 1));
+        CK(dalloc(&ctx->ghost_off, cap + 1));
+        CK(dalloc(&ctx->numneigh, cap));
+        if (ctx->p.force_field == MDB_FF_EAM && ctx->mixed) CK(dalloc(&ctx->eam_ncut, cap));
+        CK(dalloc(&ctx->local_order, cap));
+        CK(dalloc(&ctx->stage, 9 * (size_t)cap));
+        CK(dalloc(&ctx->stage_t, cap));
+        int nscan         = std::max(scan_scratch_ints(cap), scan_scratch_ints(ctx->g.mbins));
         ctx->scan_scratch_n = nscan;
         CK(dalloc(&ctx->scan_scratch, nscan));
-        ctx->npart = std::max(std::max(force_partial_blocks(nlocal), ke_partial_blocks(nlocal)),
-            eam_mixed_blocks(nlocal));
+        ctx->npart = std::max(std::max(force_partial_blocks(cap), ke_partial_blocks(cap)),
+            eam_mixed_blocks(cap));
         CK(dalloc(&ctx->partials, 3 * (size_t)ctx->npart));
         ctx->nred_slots = 64;
         CK(dalloc(&ctx->red, 4 * (size_t)ctx->nred_slots));
@@ -603,9 +630,9 @@ extern "C" int mdb_set_atoms(MdbCtx* ctx, int nlocal, const double* x, const dou
     // layout (double4 with the type bits in .w, SoA velocities)
     cudaStream_t s = ctx->s;
     size_t n3      = 3 * (size_t)nlocal;
-    CK(cudaMemcpyAsync(ctx->stage, x, sizeof(double) * n3, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(ctx->stage + n3, v, sizeof(double) * n3, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(ctx->stage_t, type, sizeof(int) * nlocal, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->stage, x, sizeof(double) * n3, cudaMemcpyDefault, s));
+    CK(cudaMemcpyAsync(ctx->stage + n3, v, sizeof(double) * n3, cudaMemcpyDefault, s));
+    CK(cudaMemcpyAsync(ctx->stage_t, type, sizeof(int) * nlocal, cudaMemcpyDefault, s));
     {
         long long m = launch_mark();
         launch_pack_atoms(s, nlocal, ctx->stage, ctx->stage + n3, ctx->stage_t, ctx->x, ctx->vx,
@@ -636,11 +663,10 @@ extern "C" int mdb_get_atoms(MdbCtx* ctx, double* x, double* v, double* f, int* 
     launch_unpack_atoms(s, n, ctx->x, ctx->vx, ctx->vy, ctx->vz, ctx->fx, ctx->fy, ctx->fz,
         ctx->stage, ctx->stage + n3, ctx->stage + 2 * n3, ctx->stage_t);
     launch_account(ctx, m);
-    if (x) CK(cudaMemcpyAsync(x, ctx->stage, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
-    if (v) CK(cudaMemcpyAsync(v, ctx->stage + n3, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
-    if (f)
-        CK(cudaMemcpyAsync(f, ctx->stage + 2 * n3, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
-    if (type) CK(cudaMemcpyAsync(type, ctx->stage_t, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+    if (x) CK(cudaMemcpyAsync(x, ctx->stage, sizeof(double) * n3, cudaMemcpyDefault, s));
+    if (v) CK(cudaMemcpyAsync(v, ctx->stage + n3, sizeof(double) * n3, cudaMemcpyDefault, s));
+    if (f) CK(cudaMemcpyAsync(f, ctx->stage + 2 * n3, sizeof(double) * n3, cudaMemcpyDefault, s));
+    if (type) CK(cudaMemcpyAsync(type, ctx->stage_t, sizeof(int) * n, cudaMemcpyDefault, s));
     CK(cudaStreamSynchronize(s));
     return MDB_OK;
 }

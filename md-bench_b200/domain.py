@@ -33,6 +33,10 @@ same for any engine with the small interface of ``MdbEngine``.
 import numpy as np
 
 
+def _is_tensor(a):
+    return type(a).__module__.startswith("torch")
+
+
 class Slabs:
     """Slab geometry: rank r owns z in [r * Lz / P, (r + 1) * Lz / P)."""
 
@@ -46,14 +50,29 @@ class Slabs:
         self.zlo = self.rank * self.lz
         self.zhi = self.box[2] if self.rank == self.world - 1 else (self.rank + 1) * self.lz
 
+    # NumPy arrays or torch tensors (on the host or a GPU): the same FP64
+    # operations either way
+
     def owner(self, z):
         """The rank owning each z (wrapped positions)."""
+        if _is_tensor(z):
+            import torch
+            return torch.clamp(torch.floor(z / self.lz).long(), 0, self.world - 1)
         r = np.floor(np.asarray(z) / self.lz).astype(np.int64)
         return np.clip(r, 0, self.world - 1)
 
     def wrap(self, x):
         """updateAtomsPbcCPU (verletlist/pbc.c:62-87): one box length back
-        into [0, L) per coordinate."""
+        into [0, L) per coordinate (both tests on the unwrapped value)."""
+        if _is_tensor(x):
+            import torch
+            x = x.clone()
+            for d in range(3):
+                c = x[:, d]
+                lo, hi = c < 0.0, c >= float(self.box[d])
+                x[:, d] = torch.where(lo, c + float(self.box[d]),
+                                      torch.where(hi, c - float(self.box[d]), c))
+            return x
         x = np.array(x, dtype=np.float64, copy=True)
         for d in range(3):
             lo, hi = x[:, d] < 0.0, x[:, d] >= self.box[d]
@@ -67,10 +86,15 @@ class Slabs:
         z = x[:, 2]
         below = (self.rank - 1) % self.world
         above = (self.rank + 1) % self.world
-        sdown = self.box[2] if self.rank == 0 else 0.0
-        sup = -self.box[2] if self.rank == self.world - 1 else 0.0
-        down = np.nonzero(z < self.zlo + self.cut)[0]
-        up = np.nonzero(z >= self.zhi - self.cut)[0]
+        sdown = float(self.box[2]) if self.rank == 0 else 0.0
+        sup = -float(self.box[2]) if self.rank == self.world - 1 else 0.0
+        if _is_tensor(x):
+            import torch
+            down = torch.nonzero(z < self.zlo + self.cut).flatten()
+            up = torch.nonzero(z >= self.zhi - self.cut).flatten()
+        else:
+            down = np.nonzero(z < self.zlo + self.cut)[0]
+            up = np.nonzero(z >= self.zhi - self.cut)[0]
         return [(below, down, sdown), (above, up, sup)]
 
 
@@ -86,6 +110,8 @@ class DistTransport:
         self.torch, self.dist, self.device = torch, dist, device
 
     def wrap(self, rows):
+        if _is_tensor(rows):
+            return rows.contiguous().to(self.device)
         return self.torch.from_numpy(np.ascontiguousarray(rows)).to(self.device)
 
     def to_host(self, t):
@@ -171,58 +197,80 @@ class ThreadTransport:
 class SlabRun:
     """One rank of a slab-decomposed run. ``engine`` holds this rank's atoms
     (see MdbEngine for the interface); atoms carry global ids so that results
-    can be compared with an undivided run."""
+    can be compared with an undivided run. The atom state between the engine
+    and the transport stays in torch tensors on the engine's device
+    (``engine.tensor_device``, the host when the engine has none): a GPU
+    engine's migration, halo selection and exchange never pass through host
+    memory."""
 
     def __init__(self, slabs, transport, engine, reneigh_every=20):
         self.sl, self.tr, self.eng = slabs, transport, engine
         self.every = int(reneigh_every)
         w, r = slabs.world, slabs.rank
         self.below, self.above = (r - 1) % w, (r + 1) % w
+        self.dev = getattr(engine, "tensor_device", "cpu")
+
+    def _t(self, a, dtype):
+        import torch
+        if _is_tensor(a):
+            return a.to(device=self.dev, dtype=dtype)
+        return torch.as_tensor(np.asarray(a), dtype=dtype, device=self.dev)
 
     def start(self, x, v, t, gid):
         """Every rank passes the full initial state; each keeps its slab."""
-        x = self.sl.wrap(x)
+        import torch
+        x = self.sl.wrap(self._t(x, torch.float64).reshape(-1, 3))
+        v = self._t(v, torch.float64).reshape(-1, 3)
+        t, gid = self._t(t, torch.int32), self._t(gid, torch.int64)
         mine = self.sl.owner(x[:, 2]) == self.sl.rank
-        self._load(x[mine], np.asarray(v)[mine], np.asarray(t)[mine], np.asarray(gid)[mine])
+        self._load(x[mine], v[mine], t[mine], gid[mine])
 
     def _load(self, x, v, t, gid):
-        order = np.argsort(gid, kind="stable")
+        import torch
+        order = torch.argsort(gid, stable=True)
         x, v, t, gid = x[order], v[order], t[order], gid[order]
         self.gid = gid
         (_, down, sdown), (_, up, sup) = self.sl.halo_plan(x)
+
         # halo rows: position shifted into the receiver's frame, type, global id
         def rows(idx, sz):
-            return np.column_stack([x[idx, 0], x[idx, 1], x[idx, 2] + sz,
-                                    t[idx].astype(np.float64), gid[idx].astype(np.float64)])
+            return torch.stack([x[idx, 0], x[idx, 1], x[idx, 2] + sz, t[idx].double(),
+                                gid[idx].double()], dim=1)
         fb, fa = self.tr.exchange(self.tr.wrap(rows(down, sdown)), self.tr.wrap(rows(up, sup)),
                                   self.below, self.above)
-        fb, fa = self.tr.to_host(fb), self.tr.to_host(fa)
-        halo = np.concatenate([fb, fa])
+        halo = torch.cat([self._t(fb, torch.float64).reshape(-1, 5),
+                          self._t(fa, torch.float64).reshape(-1, 5)])
         self.send = ((down, sdown), (up, sup))
-        self.nhalo = (len(fb), len(fa))
-        self.halo_gid = halo[:, 4].astype(np.int64)
-        self.eng.load(x, v, t, halo[:, :3], halo[:, 3].astype(np.int32),
+        self.nhalo = (int(fb.shape[0]), int(fa.shape[0]))
+        self.halo_gid = halo[:, 4].long()
+        self.eng.load(x, v, t, halo[:, :3].contiguous(), halo[:, 3].int(),
                       ids=(gid, self.halo_gid))
 
     def _migrate(self):
         """updateAtoms + reneighbour (verletlist/main.c:115-161): wrap, hand the
         atoms that left the slab to the neighbour that owns them, then a new
         halo and new lists."""
+        import torch
         x, v, t = self.eng.owned_state()
-        x = self.sl.wrap(x)
+        x = self.sl.wrap(self._t(x, torch.float64))
+        v, t = self._t(v, torch.float64), self._t(t, torch.int32)
         dest = self.sl.owner(x[:, 2])
         stay = dest == self.sl.rank
         # one rank is its own neighbour: nothing leaves
         go_down = (dest == self.below) & ~stay
         go_up = (dest == self.above) & (dest != self.below) & ~stay
-        if not np.all(stay | go_down | go_up):
+        if not bool(torch.all(stay | go_down | go_up)):
             raise RuntimeError("an atom moved past a whole slab in one rebuild period")
-        rows = np.column_stack([x, v, t.astype(np.float64), self.gid.astype(np.float64)])
-        fb, fa = self.tr.exchange(self.tr.wrap(rows[go_down]), self.tr.wrap(rows[go_up]),
-                                  self.below, self.above)
-        got = np.concatenate([rows[stay], self.tr.to_host(fb), self.tr.to_host(fa)])
-        self._load(got[:, 0:3], got[:, 3:6], got[:, 6].astype(np.int32),
-                   got[:, 7].astype(np.int64))
+        rows = torch.cat([x, v, t.double()[:, None], self.gid.double()[:, None]], dim=1)
+        if self.sl.world == 1:
+            got = rows
+        else:
+            fb, fa = self.tr.exchange(self.tr.wrap(rows[go_down]), self.tr.wrap(rows[go_up]),
+                                      self.below, self.above)
+            got = torch.cat([rows[stay], self._t(fb, torch.float64).reshape(-1, 8),
+                             self._t(fa, torch.float64).reshape(-1, 8)])
+        self._load(got[:, 0:3].contiguous(), got[:, 3:6].contiguous(), got[:, 6].int(),
+                   got[:, 7].long())
 
     def _forward(self):
         """The halo's positions of this step (forward(),
@@ -252,34 +300,42 @@ class SlabRun:
         return ke / (3 * natoms - 3)
 
     def gather(self):
-        """(gid, x, v, f) of this rank's owned atoms."""
+        """(gid, x, v, f) of this rank's owned atoms, as NumPy arrays."""
+        def host(a):
+            return a.cpu().numpy() if _is_tensor(a) else np.asarray(a)
         x, v, _ = self.eng.owned_state()
-        return self.gid, x, v, self.eng.owned_forces()
+        return host(self.gid), host(x), host(v), host(self.eng.owned_forces())
 
 
 class MdbEngine:
     """A rank's atoms in a libmdb Verlet-list context (FP64 or mixed, full or
-    half lists): owned atoms, then the halo; halo positions move on the
-    device."""
+    half lists): owned atoms, then the halo. The atom state moves between the
+    context and torch tensors on the GPU (mdb_set_atoms / mdb_get_atoms take
+    device arrays), halo positions with mdb_gather_positions /
+    mdb_set_halo_positions; nothing passes through host memory."""
+
+    tensor_device = "cuda"
 
     def __init__(self, torch, mdb, hp, device, precision="fp64", half_neigh=0):
         self.torch, self.mdb, self.hp = torch, mdb, hp
         self.device, self.precision, self.half_neigh = device, precision, half_neigh
         self.sys = None
-        self._idx = {}  # device copies of the halo index arrays, per load
+        self._idx = {}  # int32 copies of the halo index tensors, per load
 
     def load(self, x, v, t, hx, ht, ids=None):
         torch, mdb = self.torch, self.mdb
-        n, nh = len(t), len(ht)
+        n, nh = int(t.shape[0]), int(ht.shape[0])
         if self.sys is None:
             # periodic in x and y only: z neighbours come as halo atoms
             self.sys = mdb.system_from_host(self.hp, n + nh, precision=self.precision,
                                             device=self.device, pbc=(1, 1, 0),
                                             half_neigh=self.half_neigh)
-        xa = np.concatenate([x, hx]) if nh else x
-        va = np.concatenate([v, np.zeros((nh, 3))]) if nh else v
-        ta = np.concatenate([t, ht]).astype(np.int32) if nh else t.astype(np.int32)
-        self.sys.set_atoms(xa, va, ta)
+        xa = torch.cat([x, hx.to(x.device)]).contiguous()
+        va = torch.cat([v, torch.zeros((nh, 3), dtype=v.dtype, device=v.device)]).contiguous()
+        ta = torch.cat([t.int(), ht.to(t.device).int()]).contiguous()
+        # xa, va, ta come from torch's stream; the context copies them on its own
+        torch.cuda.current_stream().synchronize()
+        self.sys.set_atoms_ptr(n + nh, xa.data_ptr(), va.data_ptr(), ta.data_ptr())
         self.sys.set_owned(n)
         self._idx = {}
         self.n, self.nh = n, nh
@@ -290,15 +346,16 @@ class MdbEngine:
 
     def positions(self, idx, sz):
         torch = self.torch
-        # the same index arrays serve every step of a rebuild period
+        # the same index tensors serve every step of a rebuild period
         key = id(idx)
         if key not in self._idx:
-            d = torch.as_tensor(np.ascontiguousarray(idx, dtype=np.int32), device="cuda")
-            self._idx[key] = (idx, d)
+            self._idx[key] = (idx, torch.as_tensor(idx, device="cuda").to(torch.int32)
+                              .contiguous())
         d_idx = self._idx[key][1]
-        out = torch.empty((len(idx), 3), dtype=torch.float64, device="cuda")
+        out = torch.empty((int(d_idx.shape[0]), 3), dtype=torch.float64, device="cuda")
         torch.cuda.current_stream().synchronize()  # d_idx and out come from torch's stream
-        self.sys.gather_positions(d_idx.data_ptr(), len(idx), (0.0, 0.0, sz), out.data_ptr())
+        self.sys.gather_positions(d_idx.data_ptr(), int(d_idx.shape[0]), (0.0, 0.0, sz),
+                                  out.data_ptr())
         self.sys.synchronize()
         return out
 
@@ -321,13 +378,25 @@ class MdbEngine:
     def final_integrate(self):
         self.sys.final_integrate()
 
+    def _state(self, what):
+        torch = self.torch
+        nl = self.n + self.nh
+        bufs = {k: torch.empty((nl, 3), dtype=torch.float64, device="cuda") for k in what
+                if k != "t"}
+        if "t" in what:
+            bufs["t"] = torch.empty(nl, dtype=torch.int32, device="cuda")
+        torch.cuda.current_stream().synchronize()
+        self.sys.atoms_ptr(*(bufs[k].data_ptr() if k in bufs else None
+                             for k in ("x", "v", "f", "t")))
+        return bufs
+
     def owned_state(self):
-        x, v, _, t = self.sys.atoms()
-        return x[:self.n], v[:self.n], t[:self.n]
+        b = self._state(("x", "v", "t"))
+        return b["x"][:self.n], b["v"][:self.n], b["t"][:self.n]
 
     def owned_forces(self):
-        return self.sys.atoms()[2][:self.n]
+        return self._state(("f",))["f"][:self.n]
 
     def kinetic(self):
         _, v, _ = self.owned_state()
-        return float(np.sum(v * v) * self.hp.mass)
+        return float((v * v).sum()) * self.hp.mass

@@ -499,6 +499,23 @@ class System:
                  "mdb_get_atoms")
         return x, v, f, t
 
+    def set_atoms_ptr(self, n, x, v, type_):
+        """set_atoms from raw pointers (host or device memory of the context's
+        device): n AoS position and velocity triples, n int32 types."""
+        if not hasattr(self, "_set_ptr"):
+            fn = self.lib._FuncPtr(("mdb_set_atoms", self.lib))
+            fn.argtypes, fn.restype = [C.c_void_p, C.c_int] + [C.c_void_p] * 3, C.c_int
+            type(self)._set_ptr = fn
+        self._ck(self._set_ptr(self.h, int(n), C.c_void_p(x), C.c_void_p(v),
+                               C.c_void_p(type_)), "mdb_set_atoms")
+        self.nlocal = int(n)
+
+    def atoms_ptr(self, x=None, v=None, f=None, type_=None):
+        """mdb_get_atoms into raw pointers (host or device memory; None: skipped)."""
+        cv = lambda p: C.c_void_p(p) if p else None
+        self._ck(self.lib.mdb_get_atoms(self.h, cv(x), cv(v), cv(f), cv(type_)),
+                 "mdb_get_atoms")
+
     def counts(self):
         nl, ng, mx = C.c_int(), C.c_int(), C.c_int()
         self._ck(self.lib.mdb_get_counts(self.h, C.byref(nl), C.byref(ng), C.byref(mx)),

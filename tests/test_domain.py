@@ -26,6 +26,10 @@ STEPS = 26        # one rebuild (step 19) with migration, then 6 more steps
 EVERY = 20
 
 
+def _np(a):
+    return a.numpy() if hasattr(a, "numpy") else np.asarray(a)
+
+
 class NumpyLJ:
     """LJ full lists (epsilon = sigma = 1) and the velocity Verlet of
     verletlist/integrate.c:21-42 on NumPy; periodic in x, y and, without
@@ -40,10 +44,12 @@ class NumpyLJ:
                                dtype=np.float64) * self.box
 
     def load(self, x, v, t, hx, ht, ids):
+        # the driver hands over torch tensors on the host (NumPy arrays here)
+        x, v, t, hx = (_np(a) for a in (x, v, t, hx))
         self.x, self.v = np.array(x, dtype=np.float64), np.array(v, dtype=np.float64)
         self.t = np.asarray(t)
         self.hx = np.array(hx, dtype=np.float64).reshape(-1, 3)
-        self.gall = np.concatenate([ids[0], ids[1]]).astype(np.int64)
+        self.gall = np.concatenate([_np(ids[0]), _np(ids[1])]).astype(np.int64)
         self.n = len(self.x)
         self._build()
         self.force()
@@ -85,13 +91,12 @@ class NumpyLJ:
             self.f[i] = np.sum(d[a:b] * fpair[a:b, None], axis=0)
 
     def positions(self, idx, sz):
-        p = self.x[idx].copy()
+        p = self.x[np.asarray(idx)].copy()
         p[:, 2] += sz
         return torch.from_numpy(p)
 
     def set_halo_positions(self, recv):
-        self.hx = np.concatenate([np.asarray(r, dtype=np.float64).reshape(-1, 3)
-                                  for r in recv])
+        self.hx = np.concatenate([_np(r).astype(np.float64).reshape(-1, 3) for r in recv])
 
     def initial_integrate(self):
         self.v += self.dtf * self.f
