@@ -175,7 +175,17 @@ __global__ void __launch_bounds__(LJ_THREADS) k_lj_mixed(int nlocal,
                 sigma6  = s_sig6[tij];
                 epsilon = s_eps[tij];
             }
-            if (rsq < cutforcesq) {
+            if (UNIFORM && !HALF && !ENERGY && !COMP) {
+                // one type, full lists: no branch; pairs outside the cutoff
+                // add exact zeros (the same sums as the branch)
+                const float sr2 = __fdividef(1.0f, rsq);
+                const float s3  = sr2 * sr2 * sr2;
+                float force     = sr2 * s3 * __fmaf_rn(cA, s3, -cB);
+                force           = rsq < cutforcesq ? force : 0.0f;
+                fix             = __fmaf_rn(delx, force, fix);
+                fiy             = __fmaf_rn(dely, force, fiy);
+                fiz             = __fmaf_rn(delz, force, fiz);
+            } else if (rsq < cutforcesq) {
                 float sr2 = __fdividef(1.0f, rsq);
                 float sr6, force;
                 if (UNIFORM) {
