@@ -11,10 +11,9 @@ import numpy as np
 import pytest
 
 import mdb
-import oracle as O
 
-from test_gpu_cp import FP64_REL, MIXED_RMS, SHAPES, assert_forces_close, local_forces, \
-    pair, thermalised, valid_slots
+from test_gpu_cp import MIXED_RMS, SHAPES, assert_forces_close, local_forces, pair, \
+    thermalised, valid_slots
 
 pytestmark = pytest.mark.gpu
 
