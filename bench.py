@@ -473,9 +473,9 @@ def c4_ensemble(torch, mdb, args, device, rank=0, world=1, dist=None):
     serial = reduce_scalar(torch, dist, serial, "max", "cuda")
     for m in members:
         m.close()
-    # displacement-checked rebuilds (limit skin / 2, every member rebuilds when
-    # one trips), decided on the device (a conditional graph per step) and on
-    # the host (one synchronisation per step)
+    # displacement-checked rebuilds (limit skin / 2, a member rebuilds when its
+    # own flag trips), decided on the device (a conditional graph per step) and
+    # on the host (one synchronisation per step)
     checked = {"max_displacement": 0.15}
     for mode, host in (("device", 0), ("host", 1)):
         members = [pool.build(sp, c["cluster_n"], c["half"], c["column_edge"], c, check=0.15)

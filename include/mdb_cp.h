@@ -204,8 +204,9 @@ long long mdb_cp_ensemble_launch_count(const MdbCpEnsemble* ens);
  * "check_on_host" = 1: members with the displacement check
  * (mdb_cp_set_rebuild_check; batched ensembles only) have the host read their
  * flags after every integration; 0 (the default): each checked step is one
- * CUDA graph launch whose conditional nodes rebuild every member when one
- * member's flag is up, with no host synchronisation, and a rebuild there that
+ * CUDA graph launch whose conditional nodes rebuild the members whose flag is
+ * up (the others update their ghosts, so each member follows its own checked
+ * run alone), with no host synchronisation, and a rebuild there that
  * overflows a member's buffer is replayed by the host at its next
  * synchronisation, as for a single system. The same decisions either way. */
 int mdb_cp_ensemble_tune(MdbCpEnsemble* ens, const char* key, int value);

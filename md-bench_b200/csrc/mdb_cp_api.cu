@@ -2007,11 +2007,14 @@ struct MdbCpEnsemble {
     int* h_flags = nullptr;
     // the check decided on the device (default; "check_on_host" 1: the host
     // reads the flags every step): one graph per step whose conditional nodes
-    // rebuild every member when one flag is up; dstate = {stopped, steps run,
-    // rebuilds} as for a single system
+    // rebuild the members whose flag is up (the others update their ghosts);
+    // dstate = {stopped, steps run, steps with a rebuild} as for a single
+    // system
     bool check_host = false;
     int* dstate     = nullptr;
     int* h_dstate   = nullptr;
+    int* d_rebcnt   = nullptr; // per member: checked rebuilds on the device
+    int* h_rebcnt   = nullptr;
     cudaStream_t s_cap[2] = {nullptr, nullptr};
     long long chk_k[4]    = {0, 0, 0, 0}; // kernels: fixed part, ghost update, rebuild, force
     long long chk_steps = 0, chk_replays = 0;
@@ -2346,30 +2349,31 @@ template <class F> static void ens_fork(MdbCpEnsemble* e, F&& body)
     }
 }
 
-// updateAtoms + the whole rebuild of every member, stage by stage (block maps
-// of the capacities), then every member's counters into d_cnt_all
-static void ens_rebuild_stages(MdbCpEnsemble* e)
+// updateAtoms + the whole rebuild of the members (every member, or with only
+// those whose flag in only is set), stage by stage (block maps of the
+// capacities), then every member's counters into d_cnt_all
+static void ens_rebuild_stages(MdbCpEnsemble* e, const int* only)
 {
     const int n = (int)e->m.size();
-    auto stage  = [e](int st) {
+    auto stage  = [e, only](int st) {
         launch_build_stage_batch(e->s, st, e->nb_stage[st], e->d_build,
-            e->d_bmap + e->off_stage[st]);
+            e->d_bmap + e->off_stage[st], only);
     };
     stage(CB_RESET);
     stage(CB_GATHER);
     stage(CB_BIN);
-    launch_scan_batch(e->s, 0, n, e->d_build);
+    launch_scan_batch(e->s, 0, n, e->d_build, only);
     stage(CB_SCATTER);
     stage(CB_SORT);
-    launch_scan_batch(e->s, 1, n, e->d_build);
+    launch_scan_batch(e->s, 1, n, e->d_build, only);
     stage(CB_CLUSTERS);
     stage(CB_GCOUNT);
-    launch_scan_batch(e->s, 2, n, e->d_build);
+    launch_scan_batch(e->s, 2, n, e->d_build, only);
     stage(CB_GWRITE);
     stage(CB_GFIRST);
     stage(CB_GCOLS);
     stage(CB_CSIZES);
-    launch_scan_batch(e->s, 3, n, e->d_build);
+    launch_scan_batch(e->s, 3, n, e->d_build, only);
     stage(CB_GSCATTER);
     stage(CB_MERGE);
     stage(CB_PREP);
@@ -2395,20 +2399,32 @@ static void ens_body_batched(MdbCpEnsemble* e, int kind)
     case EG_FRONT_FI:
     case EG_FRONT_I:
         ens_integ(e, fi, true);
-        launch_ghost_update_batch(e->s, e->nb_ghost, e->d_step, e->d_bmap + e->off_ghost_dyn);
+        launch_ghost_update_batch(e->s, e->nb_ghost, e->d_step, e->d_bmap + e->off_ghost_dyn,
+            nullptr);
         if (kind == EG_PLAIN_FI || kind == EG_PLAIN_I) ens_forces(e, false);
         break;
     case EG_REB_FI:
     case EG_REB_I:
     case EG_REB_NOINT: {
-        // updateAtoms + the whole rebuild of every member, stage by stage
-        if (kind != EG_REB_NOINT) ens_integ(e, fi, true);
-        ens_rebuild_stages(e);
+        // updateAtoms + the whole rebuild, stage by stage: of every member on
+        // the schedule; of the members whose displacement flag is up in a
+        // checked step (EG_REB_NOINT), the others' ghosts updated instead
+        if (kind != EG_REB_NOINT) {
+            ens_integ(e, fi, true);
+            ens_rebuild_stages(e, nullptr);
+        } else {
+            launch_ghost_update_batch(e->s, e->nb_ghost, e->d_step,
+                e->d_bmap + e->off_ghost_dyn, e->d_flags);
+            ens_rebuild_stages(e, e->d_flags);
+        }
         cudaMemcpyAsync(e->h_cnt_all, e->d_cnt_all, sizeof(int) * CP_SLOTS * e->m.size(),
             cudaMemcpyDeviceToHost, e->s);
         // positions as built, for the members' displacement checks (the
         // flags are cleared by the host after the rebuild)
-        ens_snapshots(e);
+        if (kind != EG_REB_NOINT) ens_snapshots(e);
+        else
+            launch_snapshot_batch(e->s, e->nb_integ, e->d_step, e->d_bmap + e->off_integ,
+                e->d_flags);
         break;
     }
     case EG_CK_FI:
@@ -2418,7 +2434,8 @@ static void ens_body_batched(MdbCpEnsemble* e, int kind)
             cudaMemcpyDeviceToHost, e->s);
         break;
     case EG_GHOST:
-        launch_ghost_update_batch(e->s, e->nb_ghost, e->d_step, e->d_bmap + e->off_ghost_dyn);
+        launch_ghost_update_batch(e->s, e->nb_ghost, e->d_step, e->d_bmap + e->off_ghost_dyn,
+            nullptr);
         break;
     case EG_FORCE: ens_forces(e, false); break;
     case EG_SAMPLE:
@@ -2434,13 +2451,17 @@ static void ens_body_batched(MdbCpEnsemble* e, int kind)
 }
 
 // rebuild every member when some member's displacement flag is up
-__global__ void k_ens_chk_reb(cudaGraphConditionalHandle h, const int* flags, int n, int* st)
+__global__ void k_ens_chk_reb(cudaGraphConditionalHandle h, const int* flags, int n, int* st,
+    int* rebuilds)
 {
     __shared__ int any;
     if (threadIdx.x == 0) any = 0;
     __syncthreads();
     for (int k = threadIdx.x; k < n; k += blockDim.x)
-        if (flags[k]) any = 1;
+        if (flags[k]) {
+            any = 1;
+            if (st[0] == 0) rebuilds[k]++; // the member's own rebuild count
+        }
     __syncthreads();
     if (threadIdx.x == 0) {
         if (any) st[2]++;
@@ -2577,16 +2598,22 @@ static int ens_capture_chk(MdbCpEnsemble* e)
         e->s = s2;
         long long m = mark();
         if (what == 0) {
-            ens_rebuild_stages(e);
+            // the members whose flag is up rebuild, the others update their
+            // ghosts as in a plain step
+            launch_ghost_update_batch(s2, e->nb_ghost, e->d_step, e->d_bmap + e->off_ghost_dyn,
+                e->d_flags);
+            ens_rebuild_stages(e, e->d_flags);
             k_ens_chk_built<<<1, 128, 0, s2>>>(e->d_build, n, e->dstate);
             k_ens_dyn_maps<<<1, 256, 0, s2>>>(e->d_build, e->d_mapinfo, n, e->d_bmap,
                 e->off_integ_dyn, e->nb_integ, e->off_ghost_dyn, e->nb_ghost, e->d_goff,
                 e->d_gnb, (int)e->groups.size());
-            ens_snapshots(e);
+            launch_snapshot_batch(s2, e->nb_integ, e->d_step, e->d_bmap + e->off_integ,
+                e->d_flags);
             cudaMemsetAsync(e->d_flags, 0, sizeof(int) * n, s2);
             k[2] = mark() - m + 2;
         } else if (what == 1) {
-            launch_ghost_update_batch(s2, e->nb_ghost, e->d_step, e->d_bmap + e->off_ghost_dyn);
+            launch_ghost_update_batch(s2, e->nb_ghost, e->d_step, e->d_bmap + e->off_ghost_dyn,
+                nullptr);
             k[1] = mark() - m;
         } else {
             ens_forces(e, false);
@@ -2616,7 +2643,7 @@ static int ens_capture_chk(MdbCpEnsemble* e)
         ce   = cap_handle(s1, &h_reb);
     }
     if (ce == cudaSuccess) {
-        k_ens_chk_reb<<<1, 128, 0, s1>>>(h_reb, e->d_flags, n, e->dstate);
+        k_ens_chk_reb<<<1, 128, 0, s1>>>(h_reb, e->d_flags, n, e->dstate, e->d_rebcnt);
         ce = cudaGetLastError();
     }
     if (ce == cudaSuccess) ce = cap_conditional(s1, h_reb, 2, reb);
@@ -2749,6 +2776,8 @@ extern "C" int mdb_cp_ensemble_destroy(MdbCpEnsemble* e)
     if (e->h_flags) cudaFreeHost(e->h_flags);
     if (e->dstate) cudaFree(e->dstate);
     if (e->h_dstate) cudaFreeHost(e->h_dstate);
+    if (e->d_rebcnt) cudaFree(e->d_rebcnt);
+    if (e->h_rebcnt) cudaFreeHost(e->h_rebcnt);
     if (e->d_mapinfo) cudaFree(e->d_mapinfo);
     if (e->d_goff) cudaFree(e->d_goff);
     if (e->d_gnb) cudaFree(e->d_gnb);
@@ -2841,7 +2870,14 @@ static int ens_chk_resolve(MdbCpEnsemble* e, std::vector<int>& launched, int* re
                    (ran - stopped) * k[3];
     e->chk_steps += ran;
     e->chk_replays += stopped ? 1 : 0;
-    for (MdbCp* c : e->m) c->rebuilds_check += reb;
+    if (reb > 0) {
+        ce = cudaMemcpyAsync(e->h_rebcnt, e->d_rebcnt, sizeof(int) * n, cudaMemcpyDeviceToHost,
+            e->s);
+        if (ce == cudaSuccess) ce = cudaMemsetAsync(e->d_rebcnt, 0, sizeof(int) * n, e->s);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->s);
+        if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_CUDA, "checked steps (rebuilds)", ce);
+        for (int q = 0; q < n; q++) e->m[q]->rebuilds_check += e->h_rebcnt[q];
+    }
     int rc = MDB_OK;
     if (reb > 0) {
         ce = cudaMemcpyAsync(e->h_cnt_all, e->d_cnt_all, sizeof(int) * CP_SLOTS * n,
@@ -2916,7 +2952,10 @@ extern "C" int mdb_cp_ensemble_run(MdbCpEnsemble* e, int first_step, int nsteps,
     if (on_device && !e->dstate) {
         cudaError_t ce = cudaMalloc((void**)&e->dstate, 3 * sizeof(int));
         if (ce == cudaSuccess) ce = cudaMallocHost((void**)&e->h_dstate, 3 * sizeof(int));
+        if (ce == cudaSuccess) ce = cudaMalloc((void**)&e->d_rebcnt, n * sizeof(int));
+        if (ce == cudaSuccess) ce = cudaMallocHost((void**)&e->h_rebcnt, n * sizeof(int));
         if (ce == cudaSuccess) ce = cudaMemsetAsync(e->dstate, 0, 3 * sizeof(int), e->s);
+        if (ce == cudaSuccess) ce = cudaMemsetAsync(e->d_rebcnt, 0, n * sizeof(int), e->s);
         if (ce != cudaSuccess) return ens_fail(e, MDB_ERR_NOMEM, "checked steps", ce);
     }
     std::vector<int> launched;
@@ -2949,8 +2988,10 @@ extern "C" int mdb_cp_ensemble_run(MdbCpEnsemble* e, int first_step, int nsteps,
             bool any = false;
             for (int k = 0; k < n; k++) any = any || e->h_flags[k] != 0;
             if (any) {
+                // the members whose flag is up rebuild, the others update ghosts
                 if ((rc = ens_rebuild(e, EG_REB_NOINT))) return rc;
-                for (MdbCp* c : e->m) c->rebuilds_check++;
+                for (int k = 0; k < n; k++)
+                    if (e->h_flags[k]) e->m[k]->rebuilds_check++;
             } else if ((rc = ens_launch(e, EG_GHOST))) {
                 return rc;
             }

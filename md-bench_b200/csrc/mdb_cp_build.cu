@@ -631,21 +631,22 @@ __global__ void k_ghost_update(int N, int mixed, const int* __restrict__ cnt,
         g.xprd, g.yprd, g.zprd, cx, anchor, xr);
 }
 
+// skip: null, or a flag per member (the members whose flag is set skip it)
 __global__ void k_ghost_update_batch(const CpStepMember* __restrict__ tab,
-    const int2* __restrict__ bmap)
+    const int2* __restrict__ bmap, const int* __restrict__ skip)
 {
     const int2 bm = __ldg(&bmap[blockIdx.x]);
-    if (bm.x < 0) return;
+    if (bm.x < 0 || (skip && skip[bm.x])) return;
     const CpStepMember& m = tab[bm.x];
     ghost_update_slot(bm.y * blockDim.x + threadIdx.x, m.N, m.mixed, m.cnt, m.border, m.pbc,
         m.jnat, m.xprd, m.yprd, m.zprd, m.cx, m.anchor, m.xr);
 }
 
 void launch_ghost_update_batch(cudaStream_t s, int nblocks, const CpStepMember* tab,
-    const int2* bmap)
+    const int2* bmap, const int* skip)
 {
     if (nblocks <= 0) return;
-    k_ghost_update_batch<<<nblocks, MDB_NTHREADS, 0, s>>>(tab, bmap);
+    k_ghost_update_batch<<<nblocks, MDB_NTHREADS, 0, s>>>(tab, bmap, skip);
     g_launches++;
 }
 
@@ -1289,12 +1290,14 @@ __device__ __forceinline__ void reset_blk(int bid, const CpBuildMember& m)
     }
 }
 
+// only: null, or a flag per member (the members whose flag is 0 skip the stage)
 template <int STAGE>
 __global__ void __launch_bounds__(256, STAGE == CB_LIST ? 3 : 1)
     k_build_stage_batch(const CpBuildMember* __restrict__ tab,
-    const int2* __restrict__ bmap)
+    const int2* __restrict__ bmap, const int* __restrict__ only)
 {
     const int2 bm          = __ldg(&bmap[blockIdx.x]);
+    if (only && !only[bm.x]) return;
     const CpBuildMember& m = tab[bm.x];
     const int b            = bm.y;
     switch (STAGE) {
@@ -1363,7 +1366,7 @@ __global__ void __launch_bounds__(256, STAGE == CB_LIST ? 3 : 1)
 }
 
 void launch_build_stage_batch(cudaStream_t s, int stage, int nblocks, const CpBuildMember* tab,
-    const int2* bmap)
+    const int2* bmap, const int* only)
 {
     if (nblocks <= 0) return;
     CpBuildMember probe{};
@@ -1372,7 +1375,7 @@ void launch_build_stage_batch(cudaStream_t s, int stage, int nblocks, const CpBu
     cp_build_stage_blocks(stage, probe, &T);
     switch (stage) {
 #define CP_STAGE(S)                                                                      \
-    case S: k_build_stage_batch<S><<<nblocks, T, 0, s>>>(tab, bmap); break;
+    case S: k_build_stage_batch<S><<<nblocks, T, 0, s>>>(tab, bmap, only); break;
         CP_STAGE(CB_RESET)
         CP_STAGE(CB_GATHER)
         CP_STAGE(CB_BIN)
@@ -1398,9 +1401,10 @@ void launch_build_stage_batch(cudaStream_t s, int stage, int nblocks, const CpBu
 // per thread per pass), out[n] = total
 #define CP_SCAN_T 1024
 __global__ void __launch_bounds__(CP_SCAN_T) k_scan_batch(const CpBuildMember* __restrict__ tab,
-    int which)
+    int which, const int* __restrict__ only)
 {
     __shared__ int s_w[CP_SCAN_T / 32];
+    if (only && !only[blockIdx.x]) return;
     const CpBuildMember& m = tab[blockIdx.x];
     const int* in;
     int* out;
@@ -1449,16 +1453,37 @@ __global__ void __launch_bounds__(CP_SCAN_T) k_scan_batch(const CpBuildMember* _
     if (threadIdx.x == 0) out[n] = carry;
 }
 
-void launch_scan_batch(cudaStream_t s, int which, int nmem, const CpBuildMember* tab)
+void launch_scan_batch(cudaStream_t s, int which, int nmem, const CpBuildMember* tab,
+    const int* only)
 {
     if (nmem <= 0) return;
-    k_scan_batch<<<nmem, CP_SCAN_T, 0, s>>>(tab, which);
+    k_scan_batch<<<nmem, CP_SCAN_T, 0, s>>>(tab, which, only);
     g_launches++;
 }
 
 __global__ void k_counters_batch(const CpBuildMember* __restrict__ tab, int* out)
 {
     if (threadIdx.x < CP_SLOTS) out[blockIdx.x * CP_SLOTS + threadIdx.x] = tab[blockIdx.x].cnt[threadIdx.x];
+}
+
+// the displacement check's reference positions (slots as built) of the
+// members whose flag is set, over the integrator's block map
+__global__ void k_snapshot_batch(const CpStepMember* __restrict__ tab,
+    const int2* __restrict__ bmap, const int* __restrict__ only)
+{
+    const int2 bm = __ldg(&bmap[blockIdx.x]);
+    if (bm.x < 0 || !only[bm.x]) return;
+    const CpStepMember& m = tab[bm.x];
+    const int k           = bm.y * blockDim.x + threadIdx.x;
+    if (m.xb && k < m.cnt[CP_NCL] * m.M) const_cast<double4*>(m.xb)[k] = m.cx[k];
+}
+
+void launch_snapshot_batch(cudaStream_t s, int nblocks, const CpStepMember* tab,
+    const int2* bmap, const int* only)
+{
+    if (nblocks <= 0) return;
+    k_snapshot_batch<<<nblocks, MDB_NTHREADS, 0, s>>>(tab, bmap, only);
+    g_launches++;
 }
 
 void launch_counters_batch(cudaStream_t s, int nmem, const CpBuildMember* tab, int* out)

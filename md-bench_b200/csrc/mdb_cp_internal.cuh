@@ -318,12 +318,18 @@ enum CpBuildStage {
 };
 // blocks (and threads per block) of a stage for one member
 int cp_build_stage_blocks(int stage, const CpBuildMember& m, int* threads);
-// the stage over all members: nblocks entries of bmap
+// the stage over all members: nblocks entries of bmap (only: null, or a flag
+// per member, 0 = the member skips it)
 void launch_build_stage_batch(cudaStream_t s, int stage, int nblocks,
-    const CpBuildMember* tab, const int2* bmap);
+    const CpBuildMember* tab, const int2* bmap, const int* only);
 // the column scans of the rebuild (which: 0 col_count, 1 ncl_col, 2 gcount,
-// 3 jcol_n), one block per member
-void launch_scan_batch(cudaStream_t s, int which, int nmem, const CpBuildMember* tab);
+// 3 jcol_n), one block per member (only: as above)
+void launch_scan_batch(cudaStream_t s, int which, int nmem, const CpBuildMember* tab,
+    const int* only);
+// the displacement check's reference positions of the members whose flag in
+// only is set (slots as built), over the integrator's block map
+void launch_snapshot_batch(cudaStream_t s, int nblocks, const CpStepMember* tab,
+    const int2* bmap, const int* only);
 // every member's CP_SLOTS counters into out[member * CP_SLOTS + k]
 void launch_counters_batch(cudaStream_t s, int nmem, const CpBuildMember* tab, int* out);
 
@@ -333,8 +339,9 @@ void launch_cp_integrate_batch(cudaStream_t s, bool final_, bool initial, int nb
 // integrator's block map; launched right before the force evaluation
 void launch_zero_forces_batch(cudaStream_t s, int nblocks, const CpStepMember* tab,
     const int2* bmap);
+// skip: null, or a flag per member (set = the member skips the update)
 void launch_ghost_update_batch(cudaStream_t s, int nblocks, const CpStepMember* tab,
-    const int2* bmap);
+    const int2* bmap, const int* skip);
 void launch_force_mixed_batch(cudaStream_t s, int N, int half, int energy, const Types& ty,
     float cutforcesq, int nblocks, const CpForceMember* tab, const int2* bmap);
 void launch_ke_atoms(cudaStream_t s, int n, const double4* av, double mass, double* partials);

@@ -535,8 +535,9 @@ def test_rebuild_check_idle_when_atoms_barely_move():
 def test_ensemble_rebuild_check():
     """Batched ensemble with the displacement check: cold replicas never trip it
     and follow the fixed schedule bit for bit; with a hot replica in the set
-    every member rebuilds when it trips, and each member's forces 17 steps
-    after the last scheduled rebuild agree with a fresh build (mixed
+    each member rebuilds when its own flag trips, so every member follows its
+    own checked run alone bit for bit (full lists), and each member's forces
+    17 steps after the last scheduled rebuild agree with a fresh build (mixed
     precision: RMS 1e-5 of the force scale)."""
     cold = [(4, 0.8442, 0.02), (5, 0.8, 0.05)]
     a = [_hot_system(0.15, n, rho, T, "mixed")[0] for n, rho, T in cold]
@@ -550,13 +551,22 @@ def test_ensemble_rebuild_check():
         assert np.array_equal(xu, xw) and np.array_equal(vu, vw)
     ea.close()
     eb.close()
-    hot = [(6, 0.95, 2.0), (4, 0.8, 0.5)]
+    hot = [(6, 0.95, 2.0), (4, 0.8, 0.5), (5, 0.8442, 0.02)]
     sys_kw = [_hot_system(0.15, n, rho, T, "mixed")[:2] for n, rho, T in hot]
     members = [s for s, _ in sys_kw]
+    solo = [_hot_system(0.15, n, rho, T, "mixed")[0] for n, rho, T in hot]
     ens = mdb.Ensemble(members)
     ens.run(57, max_samples=0)
-    sched, trig = members[1].rebuilds()
+    for s in solo:
+        s.run(57, max_samples=0)
+    sched, trig = members[0].rebuilds()
     assert sched == 2 and trig > 0
+    assert members[2].rebuilds() == (2, 0)  # the cold replica never trips
+    for u, w in zip(members, solo):
+        assert u.rebuilds() == w.rebuilds()
+        xu, vu, _, _ = _local_state(u)
+        xw, vw, _, _ = _local_state(w)
+        assert np.array_equal(xu, xw) and np.array_equal(vu, vw)
     for s, kw in sys_kw:
         x, v, f, t = _local_state(s)
         ref = mdb.ClusterSystem(**kw)
@@ -570,6 +580,8 @@ def test_ensemble_rebuild_check():
         assert np.sqrt(np.mean(np.sum(d * d, axis=1))) <= 1e-5 * rms
         ref.close()
     ens.close()
+    for s in solo:
+        s.close()
 
 
 def thermalised_box(nx, ny, nz, steps=150):
