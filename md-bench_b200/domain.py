@@ -344,6 +344,14 @@ class MdbEngine:
         self.sys.build_neighbor()
         self.sys.compute_force()
 
+    def _streams(self):
+        # the context's own stream as a torch stream, and torch's current one:
+        # the halo moves between them by stream order, with no host wait
+        if getattr(self, "_es", None) is None or self._es_sys is not self.sys:
+            self._es = self.torch.cuda.ExternalStream(self.sys.stream)
+            self._es_sys = self.sys
+        return self._es, self.torch.cuda.current_stream()
+
     def positions(self, idx, sz):
         torch = self.torch
         # the same index tensors serve every step of a rebuild period
@@ -353,21 +361,24 @@ class MdbEngine:
                               .contiguous())
         d_idx = self._idx[key][1]
         out = torch.empty((int(d_idx.shape[0]), 3), dtype=torch.float64, device="cuda")
-        torch.cuda.current_stream().synchronize()  # d_idx and out come from torch's stream
+        es, cur = self._streams()
+        es.wait_stream(cur)   # d_idx and out exist on torch's stream first
         self.sys.gather_positions(d_idx.data_ptr(), int(d_idx.shape[0]), (0.0, 0.0, sz),
                                   out.data_ptr())
-        self.sys.synchronize()
+        out.record_stream(es)
+        cur.wait_stream(es)   # torch's later uses of out follow the gather
         return out
 
     def set_halo_positions(self, recv):
         torch = self.torch
         buf = torch.cat([r.to("cuda") for r in recv]).contiguous()
         # the received rows and buf come from torch's stream (NCCL receives
-        # complete there asynchronously); the context reads buf on its own
-        torch.cuda.current_stream().synchronize()
+        # complete there); the context reads buf on its own stream, after it
+        es, cur = self._streams()
+        es.wait_stream(cur)
         self.sys.set_halo_positions(buf.data_ptr(), buf.shape[0])
         self.sys.update_pbc()
-        self.sys.synchronize()
+        buf.record_stream(es)  # not reused before the context has read it
 
     def initial_integrate(self):
         self.sys.initial_integrate()
