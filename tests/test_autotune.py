@@ -95,3 +95,40 @@ def test_no_change_within_noise():
                                       rate=lambda ms: next(flat))
     assert choice == {AT.size_class(1000): AT.DEFAULT}
     assert all(m.closed for m in log)
+
+
+class FakeSystem:
+    """A single system whose force time the model below gives."""
+
+    def __init__(self, n, half, edge, log):
+        self.cluster_n, self.half, self.edge = n, half, edge
+        self.launch = {}
+        self.closed = False
+        log.append(self)
+
+    def tune(self, key, value):
+        self.launch[key] = value
+
+    def time_force(self, reps):
+        # 4x4 half lists with a 125 % column edge and four i-clusters per warp
+        # are fastest; everything else costs more
+        t = 1.0
+        t *= 1.0 if (self.cluster_n, self.half) == (4, 1) else 1.3
+        t *= {80: 1.1, 100: 1.0, 125: 0.95}[self.edge]
+        t *= 1.0 if self.launch.get("force_cpw", 4) == 4 else 1.2
+        return t
+
+    def close(self):
+        self.closed = True
+
+
+def test_single_system_search_covers_bin_sizes():
+    log = []
+    choice, trials = AT.tune_system(lambda n, h, e: FakeSystem(n, h, e, log))
+    assert (choice["cluster_n"], choice["half"], choice["column_edge"]) == (4, 1, 125)
+    assert choice["force_cpw"] == 4
+    # every shape, list form and bin size was built once, and closed
+    assert sorted((m.cluster_n, m.half, m.edge) for m in log) == sorted(
+        (n, h, e) for n in AT.SHAPES for h in AT.FORMS for e in AT.EDGES)
+    assert all(m.closed for m in log)
+    assert all(AT.valid(c) for c, _ in trials if "force_cpw" in c)
